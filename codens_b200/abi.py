@@ -1,0 +1,112 @@
+"""ctypes bindings of libcodens_b200.so (include/cns_abi.h).
+
+The product path has no CPU fallback: if the CUDA library is missing or no
+GPU is visible, loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+c_i32, c_i64, c_f64 = C.c_int32, C.c_int64, C.c_double
+P = C.POINTER
+
+ERRORS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-positive temperature",
+    4: "time step below dt1min", 5: "unknown boundary condition",
+    6: "not ready", 7: "non-finite residual norm",
+}
+
+
+class Layout_t(C.Structure):
+    _fields_ = [("nblk", c_i32), ("dims", P(c_i32)), ("ld", c_i64)]
+
+
+class Phys_t(C.Structure):
+    _fields_ = [(n, c_f64) for n in
+                ("gam", "pinfl", "pr", "prt", "reynz", "suth_a", "pa1", "aa1", "omg")]
+
+
+class Scheme_t(C.Structure):
+    _fields_ = [("ns", c_i32), ("muscl", c_i32), ("xk", c_f64), ("ilim", c_i32),
+                ("eta", c_f64), ("kdtl", c_i32), ("dt1min", c_f64), ("lmax", c_i32),
+                ("qfix_dfez", c_i32)]
+
+
+class Bnd_t(C.Structure):
+    _fields_ = [("nbnd", c_i32), ("type", P(c_i32)), ("blk", P(c_i32)),
+                ("face", P(c_i32)), ("mpb", P(c_i64)), ("mmb", P(c_i32)),
+                ("partner", P(c_i32)), ("cosr", P(c_f64)), ("sinr", P(c_f64)),
+                ("nlist", c_i64), ("ncbd", P(c_i64)), ("ncin", P(c_i64)),
+                ("bceqt", P(c_f64))]
+
+
+class State_t(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ("v", "u", "d", "dt", "sn", "vol", "pression", "ztemp", "cson",
+                 "mu", "mut", "tau")]
+
+
+EXPORTS = [
+    "cns_create", "cns_destroy", "cns_set_stream", "cns_set_scheme",
+    "cns_last_error", "cns_scratch_bytes", "cns_metric", "cns_boundary_geom",
+    "cns_zpres", "cns_zvismo", "cns_chronos", "cns_rbord", "cns_sch_roe_euler",
+    "cns_sch_roe", "cns_zvisqc", "cns_implimf_eu", "cns_implimf_3d",
+    "cns_rscpsv", "cns_bind_state", "cns_atsch_num_step",
+    "cns_atsch_num_launch", "cns_last_norms", "cns_atsch_num_step_host",
+]
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load the CUDA library (building it in-tree if needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise RuntimeError(f"{path} is missing; build it with codens_b200/build.py")
+        _build.build()
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.cns_create.argtypes = [P(Layout_t), P(Phys_t), P(Scheme_t), P(Bnd_t), P(vp)]
+    L.cns_destroy.argtypes = [vp]
+    L.cns_set_stream.argtypes = [vp, vp]
+    L.cns_set_scheme.argtypes = [vp, P(Scheme_t)]
+    L.cns_last_error.argtypes = [vp]
+    L.cns_last_error.restype = C.c_char_p
+    L.cns_scratch_bytes.argtypes = [vp]
+    L.cns_scratch_bytes.restype = c_i64
+    L.cns_metric.argtypes = [vp] * 6
+    L.cns_boundary_geom.argtypes = [vp] + [P(c_f64)] * 5
+    L.cns_zpres.argtypes = [vp, C.c_int] + [vp] * 4
+    L.cns_zvismo.argtypes = [vp, C.c_int] + [vp] * 3
+    L.cns_chronos.argtypes = [vp, C.c_int] + [vp] * 7
+    L.cns_rbord.argtypes = [vp] * 5
+    L.cns_sch_roe_euler.argtypes = [vp, C.c_int] + [vp] * 4
+    L.cns_sch_roe.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_zvisqc.argtypes = [vp] * 8
+    L.cns_implimf_eu.argtypes = [vp, C.c_int] + [vp] * 8 + [C.c_int]
+    L.cns_implimf_3d.argtypes = [vp, C.c_int] + [vp] * 10 + [C.c_int]
+    L.cns_rscpsv.argtypes = [vp] * 4 + [P(c_f64)]
+    L.cns_bind_state.argtypes = [vp, P(State_t)]
+    L.cns_atsch_num_step.argtypes = [vp, C.c_int, P(c_f64)]
+    L.cns_atsch_num_launch.argtypes = [vp, C.c_int]
+    L.cns_last_norms.argtypes = [vp, P(c_f64)]
+    L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
+    for f in EXPORTS:
+        getattr(L, f).restype = getattr(L, f).restype or C.c_int
+    L.cns_last_error.restype = C.c_char_p
+    L.cns_scratch_bytes.restype = c_i64
+    _lib = L
+    return L
+
+
+class CnsError(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str = ""):
+        super().__init__(f"{where}: {ERRORS.get(code, code)} ({code}) {detail}".strip())
+        self.code = code

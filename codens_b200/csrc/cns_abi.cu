@@ -1,0 +1,633 @@
+// cns_abi.cu -- C ABI of the CodeNS hot path: context (the reference's module
+// state), tile work lists, per-routine entry points and the graph-captured
+// fused pseudo-time step.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cns_abi.h"
+#include "cns_kernels.cuh"
+
+
+using namespace cns;
+
+struct cns_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;      // stream the work is issued on
+  cudaStream_t own_st = nullptr;  // stream created by the context
+  HostLayout lay;
+  Blk* d_blks = nullptr;
+  Phys ph{};
+  Scheme sc{};
+  SpaceBuf cells, faces[3], lines[3];
+  int* d_cells_tile0 = nullptr;  // cells.blk_tile0 on the device
+  // boundaries
+  Bnd bd{};
+  std::vector<int> h_btype;
+  int n_idd = 0;
+  int* d_idd_list = nullptr;
+  double* clidd_scratch = nullptr;
+  // scratch
+  Work w;
+  std::vector<void*> allocs;
+  long long scratch_bytes = 0;
+  double* h_norms = nullptr;  // pinned [16]
+  int* h_status = nullptr;    // pinned
+  // fast path
+  cns_state_t state{};
+  bool bound = false;
+  bool metric_done = false;
+  cudaGraphExec_t gexec = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int fail(cns_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(cns_ctx* c, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return CNS_OK;
+  return fail(c, CNS_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e__ = (call);                                      \
+    if (e__ != cudaSuccess) return cuda_fail(c, e__, #call);       \
+  } while (0)
+
+template <typename T>
+cudaError_t dev_alloc(cns_ctx* c, T** p, size_t n, bool zero = true) {
+  void* q = nullptr;
+  const size_t bytes = sizeof(T) * (n > 0 ? n : 1);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) return e;
+  c->allocs.push_back(q);
+  c->scratch_bytes += (long long)bytes;
+  if (zero) e = cudaMemset(q, 0, bytes);
+  *p = static_cast<T*>(q);
+  return e;
+}
+
+template <typename T>
+cudaError_t upload(cns_ctx* c, T** p, const T* h, size_t n) {
+  cudaError_t e = dev_alloc(c, p, n, false);
+  if (e != cudaSuccess) return e;
+  if (n > 0) e = cudaMemcpy(*p, h, sizeof(T) * n, cudaMemcpyHostToDevice);
+  return e;
+}
+
+// index space with extent ext(B) per block and its tile work list
+template <typename F>
+cudaError_t build_space(cns_ctx* c, SpaceBuf& s, F ext_of) {
+  std::vector<int> tb, ext;
+  std::vector<long long> ts;
+  s.blk_tile0.assign(c->lay.blks.size() + 1, 0);
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    int e[3];
+    ext_of(c->lay.blks[b], e);
+    ext.push_back(e[0]);
+    ext.push_back(e[1]);
+    ext.push_back(e[2]);
+    const long long cnt = (long long)e[0] * e[1] * e[2];
+    s.blk_tile0[b] = (int)tb.size();
+    for (long long t = 0; t < cnt; t += kTile) {
+      tb.push_back((int)b);
+      ts.push_back(t);
+    }
+  }
+  s.blk_tile0.back() = (int)tb.size();
+  s.ntiles = (int)tb.size();
+  cudaError_t e = upload(c, &s.d_tile_blk, tb.data(), tb.size());
+  if (e == cudaSuccess) e = upload(c, &s.d_tile_start, ts.data(), ts.size());
+  if (e == cudaSuccess) e = upload(c, &s.d_ext, ext.data(), ext.size());
+  return e;
+}
+
+bool bad_block(cns_ctx* c, int l) { return l < 0 || l > (int)c->lay.blks.size(); }
+
+// [first, last) flat range of block l (0 = every block)
+void block_range(cns_ctx* c, int l, long long& n0, long long& n1) {
+  if (l == 0) {
+    n0 = 0;
+    n1 = c->lay.ncells;
+  } else {
+    const Blk& B = c->lay.blks[l - 1];
+    n0 = B.npc;
+    n1 = B.npc + B.nnn;
+  }
+}
+
+cudaError_t zero_cols(cns_ctx* c, double* a, int ncol, int l) {
+  long long n0, n1;
+  block_range(c, l, n0, n1);
+  for (int col = 0; col < ncol; ++col) {
+    cudaError_t e = cudaMemsetAsync(a + col * c->lay.ld + n0, 0,
+                                    sizeof(double) * (n1 - n0), c->st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int check_status(cns_ctx* c) {
+  CK(cudaMemcpyAsync(c->h_status, c->w.status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (*c->h_status & 1) {
+    *c->h_status = 0;
+    CK(cudaMemsetAsync(c->w.status, 0, sizeof(int), c->st));
+    return fail(c, CNS_ETEMP, "non-positive temperature (zvismo)");
+  }
+  return CNS_OK;
+}
+
+// the residual of one block set: (optional) limiter ratios, face fluxes,
+// accumulation into u
+cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
+                     const double* tau, const double* sn, const double* ps) {
+  const long long ld = c->lay.ld;
+  cudaError_t e = cudaSuccess;
+  if (c->sc.ns && c->sc.ilim == 1)
+    e = launch_ratio(c->d_blks, c->lines, l0, v, ld, ps, c->w.R, c->st);
+  if (e == cudaSuccess)
+    e = launch_face_flux(c->d_blks, c->faces, l0, c->ph, c->sc, v, ld, ps, tau, sn,
+                         c->w.R, c->w.G, c->st);
+  if (e == cudaSuccess)
+    e = launch_accumulate(c->d_blks, c->cells.view(l0), c->w.G, ld, u, c->st);
+  return e;
+}
+
+// one pseudo-time iteration on the bound state (atsch_num.f90:245-1134 for
+// ischema = 7, kmf = 1, steady, dt recomputed every iteration)
+cudaError_t enqueue_step(cns_ctx* c) {
+  const cns_state_t& s = c->state;
+  const long long ld = c->lay.ld;
+  const Space all = c->cells.view(-1);
+  cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
+                               s.ztemp, s.cson, s.mu, c->w.status, c->st);
+  if (e == cudaSuccess)
+    e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
+                       s.vol, s.cson, c->st);
+  if (e == cudaSuccess)
+    e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd,
+                     c->d_idd_list, c->clidd_scratch, c->st);
+  if (e == cudaSuccess && c->sc.ns) {
+    e = launch_grad(c->d_blks, all, c->ph, s.v, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
+                    s.ztemp, c->st);
+    if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
+  }
+  if (e == cudaSuccess) e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
+  if (e == cudaSuccess)
+    e = launch_implicit(c->d_blks, all, c->faces, -1, c->ph, c->sc, !c->sc.ns,
+                        c->sc.lmax, s.u, s.dt, s.v, nullptr, s.mu, s.mut, s.sn, s.vol,
+                        s.pression, s.cson, c->w, 1, c->st);
+  if (e == cudaSuccess)
+    e = launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
+                             c->w.normpart, c->w.norms, c->st);
+  return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
+               const cns_scheme_t* scheme, const cns_bnd_t* bnd, cns_ctx** out) {
+  if (!layout || !phys || !scheme || !bnd || !out || layout->nblk < 1 ||
+      layout->nblk > kMaxBlocks || !layout->dims)
+    return CNS_EINVAL;
+  cns_ctx* c = new cns_ctx();
+  *out = nullptr;
+  CK(cudaGetDevice(&c->device));
+  // layout (crdms.f90:125-158)
+  long long off = 0, nreal = 0;
+  for (int l = 0; l < layout->nblk; ++l) {
+    Blk B{};
+    B.ni = layout->dims[3 * l];
+    B.nj = layout->dims[3 * l + 1];
+    B.nk = layout->dims[3 * l + 2];
+    if (B.ni < 2 || B.nj < 2 || B.nk < 2) {
+      delete c;
+      return CNS_EINVAL;
+    }
+    B.nid = B.ni + 2;
+    B.njd = B.nj + 2;
+    B.nkd = B.nk + 2;
+    B.nijd = (long long)B.nid * B.njd;
+    B.nnn = B.nijd * B.nkd;
+    B.npc = off;
+    off += B.nnn;
+    nreal += (long long)(B.ni - 1) * (B.nj - 1) * (B.nk - 1);
+    c->lay.blks.push_back(B);
+  }
+  c->lay.ncells = off;
+  c->lay.nreal = nreal;
+  c->lay.ld = layout->ld > 0 ? layout->ld : off;
+  if (c->lay.ld < off) {
+    delete c;
+    return CNS_EINVAL;
+  }
+  c->ph.gam = phys->gam;
+  c->ph.gam1 = phys->gam - 1.;
+  c->ph.pinfl = phys->pinfl;
+  c->ph.pr = phys->pr;
+  c->ph.prt = phys->prt;
+  c->ph.cp = 1. / (phys->gam - 1.);
+  c->ph.reynz = phys->reynz;
+  c->ph.suth_a = phys->suth_a;
+  c->ph.pa1 = phys->pa1;
+  c->ph.aa1 = phys->aa1;
+  c->ph.omg = phys->omg;
+  int rc = cns_set_scheme(c, scheme);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  auto cleanup_fail = [&](cudaError_t e, const char* what) {
+    int r = cuda_fail(c, e, what);
+    cns_destroy(c);
+    return r;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cleanup_fail(e, "stream");
+  c->st = c->own_st;
+  e = upload(c, &c->d_blks, c->lay.blks.data(), c->lay.blks.size());
+  if (e != cudaSuccess) return cleanup_fail(e, "blocks");
+  e = build_space(c, c->cells, [](const Blk& B, int x[3]) {
+    x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = B.nk - 1; });
+  for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
+    e = build_space(c, c->faces[dir], [dir](const Blk& B, int x[3]) {
+      x[0] = dir == 0 ? B.ni : B.ni - 1;
+      x[1] = dir == 1 ? B.nj : B.nj - 1;
+      x[2] = dir == 2 ? B.nk : B.nk - 1; });
+    if (e == cudaSuccess)
+      e = build_space(c, c->lines[dir], [dir](const Blk& B, int x[3]) {
+        x[0] = dir == 0 ? 1 : B.ni - 1;
+        x[1] = dir == 1 ? 1 : B.nj - 1;
+        x[2] = dir == 2 ? 1 : B.nk - 1; });
+  }
+  if (e != cudaSuccess) return cleanup_fail(e, "index spaces");
+  e = upload(c, &c->d_cells_tile0, c->cells.blk_tile0.data(), c->cells.blk_tile0.size());
+  if (e != cudaSuccess) return cleanup_fail(e, "tiles");
+  // boundaries
+  const int nb = bnd->nbnd;
+  const long long nl = bnd->nlist;
+  if (nb < 0 || nl < 0) {
+    cns_destroy(c);
+    return CNS_EINVAL;
+  }
+  std::vector<int> ent_bnd((size_t)nl), blk0(nb), idd;
+  for (int b = 0; b < nb; ++b) {
+    const int t = bnd->type[b];
+    if (t < CNS_BC_EXTR || t > CNS_BC_PRD) {
+      cns_destroy(c);
+      return CNS_EBC;
+    }
+    if (bnd->blk[b] < 1 || bnd->blk[b] > layout->nblk || bnd->face[b] < 0 ||
+        bnd->face[b] > 5 || bnd->mpb[b] < 0 || bnd->mpb[b] + bnd->mmb[b] > nl) {
+      cns_destroy(c);
+      return CNS_EINVAL;
+    }
+    if (t == CNS_BC_RC) {
+      const int p = bnd->partner[b];
+      if (p < 0 || p >= nb || bnd->mmb[p] != bnd->mmb[b]) {
+        cns_destroy(c);
+        return CNS_EINVAL;
+      }
+    }
+    blk0[b] = bnd->blk[b] - 1;
+    for (int m = 0; m < bnd->mmb[b]; ++m) ent_bnd[(size_t)(bnd->mpb[b] + m)] = b;
+    if (t == CNS_BC_IDD) idd.push_back(b);
+    c->h_btype.push_back(t);
+  }
+  for (long long q = 0; q < nl; ++q) {
+    if (bnd->ncbd[q] < 0 || bnd->ncbd[q] >= off || bnd->ncin[q] < 0 || bnd->ncin[q] >= off) {
+      cns_destroy(c);
+      return CNS_EINVAL;
+    }
+  }
+  c->bd.nbnd = nb;
+  c->bd.nlist = nl;
+  c->n_idd = (int)idd.size();
+  {
+    int *t_, *b_, *f_, *m_, *p_, *eb_;
+    long long *mpb_, *ncbd_, *ncin_;
+    double *cr_, *sr_, *bc_;
+    e = upload(c, &t_, bnd->type, nb);
+    if (e == cudaSuccess) e = upload(c, &b_, blk0.data(), nb);
+    if (e == cudaSuccess) e = upload(c, &f_, bnd->face, nb);
+    if (e == cudaSuccess) e = upload(c, &mpb_, (const long long*)bnd->mpb, nb);
+    if (e == cudaSuccess) e = upload(c, &m_, bnd->mmb, nb);
+    if (e == cudaSuccess) e = upload(c, &p_, bnd->partner, nb);
+    if (e == cudaSuccess) e = upload(c, &cr_, bnd->cosr, nb);
+    if (e == cudaSuccess) e = upload(c, &sr_, bnd->sinr, nb);
+    if (e == cudaSuccess) e = upload(c, &eb_, ent_bnd.data(), (size_t)nl);
+    if (e == cudaSuccess) e = upload(c, &ncbd_, (const long long*)bnd->ncbd, (size_t)nl);
+    if (e == cudaSuccess) e = upload(c, &ncin_, (const long long*)bnd->ncin, (size_t)nl);
+    if (e == cudaSuccess) e = upload(c, &bc_, bnd->bceqt, (size_t)(5 * nl));
+    if (e == cudaSuccess) e = upload(c, &c->d_idd_list, idd.data(), idd.size());
+    if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nxn, (size_t)nl);
+    if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nyn, (size_t)nl);
+    if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nzn, (size_t)nl);
+    if (e == cudaSuccess) e = dev_alloc(c, &c->bd.ym, (size_t)nl);
+    if (e == cudaSuccess) e = dev_alloc(c, &c->bd.zm, (size_t)nl);
+    if (e == cudaSuccess) e = dev_alloc(c, &c->clidd_scratch, (size_t)(3 * nl));
+    if (e != cudaSuccess) return cleanup_fail(e, "boundary tables");
+    c->bd.type = t_;
+    c->bd.blk = b_;
+    c->bd.face = f_;
+    c->bd.mpb = mpb_;
+    c->bd.mmb = m_;
+    c->bd.partner = p_;
+    c->bd.cosr = cr_;
+    c->bd.sinr = sr_;
+    c->bd.ent_bnd = eb_;
+    c->bd.ncbd = ncbd_;
+    c->bd.ncin = ncin_;
+    c->bd.bceqt = bc_;
+  }
+  // scratch (zeroed: ghost entries of the Jacobi iterates and of rv stay 0)
+  const long long ld = c->lay.ld;
+  c->w.ld = ld;
+  e = dev_alloc(c, &c->w.G, (size_t)(15 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.R, (size_t)(15 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.coefe, (size_t)(3 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.coefdiag, (size_t)ld);
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.rv, (size_t)ld);
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+    e = dev_alloc(c, &c->w.dpp[q], (size_t)(5 * ld));
+    if (e == cudaSuccess) e = dev_alloc(c, &c->w.dfpp[q], (size_t)(9 * ld));
+  }
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.normpart, (size_t)(15 * c->cells.ntiles));
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.norms, 16);
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.status, 1);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->h_norms, 16 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->h_status, sizeof(int));
+  if (e != cudaSuccess) return cleanup_fail(e, "scratch");
+  *c->h_status = 0;
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cleanup_fail(e, "create");
+  *out = c;
+  return CNS_OK;
+}
+
+int cns_destroy(cns_ctx* c) {
+  if (!c) return CNS_OK;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->h_norms) cudaFreeHost(c->h_norms);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->own_st) cudaStreamDestroy(c->own_st);
+  delete c;
+  return CNS_OK;
+}
+
+int cns_set_stream(cns_ctx* c, void* stream) {
+  if (!c) return CNS_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  // work is issued on the caller's stream from now on (NULL: back to the
+  // context's own stream)
+  c->st = stream ? (cudaStream_t)stream : c->own_st;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return CNS_OK;
+}
+
+int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
+  if (!c || !s) return CNS_EINVAL;
+  if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1))
+    return fail(c, CNS_EINVAL, "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}");
+  c->sc.ns = s->ns;
+  c->sc.muscl = s->muscl;
+  c->sc.xk = s->xk;
+  c->sc.ilim = s->ilim;
+  c->sc.eta = s->eta;
+  c->sc.kdtl = s->kdtl;
+  c->sc.dt1min = s->dt1min;
+  c->sc.lmax = s->lmax;
+  c->sc.qfix_dfez = s->qfix_dfez;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return CNS_OK;
+}
+
+const char* cns_last_error(cns_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int64_t cns_scratch_bytes(cns_ctx* c) { return c ? c->scratch_bytes : 0; }
+
+int cns_metric(cns_ctx* c, double* x, double* y, double* z, double* sn,
+               double* vol) {
+  if (!c || !x || !y || !z || !sn || !vol) return CNS_EINVAL;
+  CK(launch_metric(c->lay, c->d_blks, c->bd, x, y, z, sn, vol, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->metric_done = true;
+  return CNS_OK;
+}
+
+int cns_boundary_geom(cns_ctx* c, double* nxn, double* nyn, double* nzn,
+                      double* ym, double* zm) {
+  if (!c) return CNS_EINVAL;
+  if (!c->metric_done) return fail(c, CNS_ENOTREADY, "cns_metric has not run");
+  const size_t n = sizeof(double) * (size_t)c->bd.nlist;
+  if (n == 0) return CNS_OK;
+  CK(cudaMemcpyAsync(nxn, c->bd.nxn, n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(nyn, c->bd.nyn, n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(nzn, c->bd.nzn, n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(ym, c->bd.ym, n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(zm, c->bd.zm, n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CNS_OK;
+}
+
+int cns_zpres(cns_ctx* c, int l, const double* v, double* ps, double* temp,
+              double* cson) {
+  if (!c || bad_block(c, l) || !v || !ps || !temp || !cson) return CNS_EINVAL;
+  CK(launch_zpres(c->d_blks, c->cells.view(l - 1), c->ph, 0, v, c->lay.ld, ps, temp,
+                  cson, nullptr, c->w.status, c->st));
+  return CNS_OK;
+}
+
+int cns_zvismo(cns_ctx* c, int l, double* mu, const double* v, const double* temp) {
+  (void)v;
+  if (!c || bad_block(c, l) || !mu || !temp) return CNS_EINVAL;
+  CK(launch_zvismo(c->d_blks, c->cells.view(l - 1), c->ph, mu, temp, c->w.status, c->st));
+  return check_status(c);
+}
+
+int cns_chronos(cns_ctx* c, int l, const double* mu, const double* mut,
+                const double* v, double* dt, const double* sn, const double* vol,
+                const double* cson) {
+  if (!c || bad_block(c, l) || !v || !dt || !sn || !vol || !cson) return CNS_EINVAL;
+  if (c->sc.ns && (!mu || !mut)) return CNS_EINVAL;
+  // chronos.f90:138-141 zeroes dt from cell (1,1,1) to cell (ni,nj,nk)
+  const int b0 = l == 0 ? 0 : l - 1, b1 = l == 0 ? (int)c->lay.blks.size() : l;
+  for (int b = b0; b < b1; ++b) {
+    const Blk& B = c->lay.blks[b];
+    const long long n1 = B.npc + 1 + B.nid + B.nijd;
+    const long long n2 = B.npc + B.ni + (long long)B.nj * B.nid + (long long)B.nk * B.nijd;
+    CK(cudaMemsetAsync(dt + n1, 0, sizeof(double) * (n2 - n1 + 1), c->st));
+  }
+  CK(launch_chronos(c->d_blks, c->cells.view(l - 1), c->ph, c->sc, mu, mut, v,
+                    c->lay.ld, dt, sn, vol, cson, c->st));
+  return CNS_OK;
+}
+
+int cns_rbord(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
+  if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
+  if (!c->metric_done) return fail(c, CNS_ENOTREADY, "cns_metric has not run");
+  CK(launch_rbord(c->bd, c->ph, v, c->lay.ld, ps, temp, cson, c->n_idd, c->d_idd_list,
+                  c->clidd_scratch, c->st));
+  return CNS_OK;
+}
+
+int cns_sch_roe_euler(cns_ctx* c, int l, double* u, const double* v,
+                      const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || !u || !v || !sn || !ps) return CNS_EINVAL;
+  const Scheme keep = c->sc;
+  c->sc.ns = 0;
+  CK(zero_cols(c, u, 5, l));
+  cudaError_t e = residual(c, l - 1, u, v, nullptr, sn, ps);
+  c->sc = keep;
+  CK(e);
+  return CNS_OK;
+}
+
+int cns_sch_roe(cns_ctx* c, int l, double* u, const double* v, const double* tau,
+                const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  const Scheme keep = c->sc;
+  c->sc.ns = 1;
+  CK(zero_cols(c, u, 5, l));
+  cudaError_t e = residual(c, l - 1, u, v, tau, sn, ps);
+  c->sc = keep;
+  CK(e);
+  return CNS_OK;
+}
+
+int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,
+               double* tau, const double* sn, const double* vol,
+               const double* temp) {
+  if (!c || !v || !mu || !mut || !tau || !sn || !vol || !temp) return CNS_EINVAL;
+  CK(launch_grad(c->d_blks, c->cells.view(-1), c->ph, v, c->lay.ld, mu, mut, tau, sn,
+                 vol, temp, c->st));
+  CK(launch_tau_ghosts(c->bd, tau, c->lay.ld, c->st));
+  return CNS_OK;
+}
+
+static int implimf(cns_ctx* c, int l, int eu, const double* u, const double* dt,
+                   double* v, double* d, const double* mu, const double* mut,
+                   const double* sn, const double* vol, const double* ps,
+                   const double* cson, int lmx) {
+  if (lmx < 0) return CNS_EINVAL;
+  CK(zero_cols(c, d, 5, l));
+  CK(launch_implicit(c->d_blks, c->cells.view(l - 1), c->faces, l - 1, c->ph, c->sc, eu,
+                     lmx, u, dt, v, d, mu, mut, sn, vol, ps, cson, c->w, 0, c->st));
+  return CNS_OK;
+}
+
+int cns_implimf_eu(cns_ctx* c, int l, const double* u, const double* dt, double* v,
+                   double* d, const double* sn, const double* vol, const double* ps,
+                   const double* cson, int lmx) {
+  if (!c || bad_block(c, l) || !u || !dt || !v || !d || !sn || !vol || !ps || !cson)
+    return CNS_EINVAL;
+  return implimf(c, l, 1, u, dt, v, d, nullptr, nullptr, sn, vol, ps, cson, lmx);
+}
+
+int cns_implimf_3d(cns_ctx* c, int l, const double* u, const double* dt, double* v,
+                   double* d, const double* mu, const double* mut, const double* sn,
+                   const double* vol, const double* ps, const double* cson, int lmx) {
+  if (!c || bad_block(c, l) || !u || !dt || !v || !d || !mu || !mut || !sn || !vol ||
+      !ps || !cson)
+    return CNS_EINVAL;
+  return implimf(c, l, 0, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx);
+}
+
+int cns_rscpsv(cns_ctx* c, const double* u0, const double* v, const double* dt,
+               double* norms) {
+  if (!c || !u0 || !v || !dt || !norms) return CNS_EINVAL;
+  CK(launch_norm_partials(c->d_blks, c->cells.view(-1), c->lay.ld, u0, v, dt,
+                          c->w.normpart, c->st));
+  CK(launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
+                          c->w.normpart, c->w.norms, c->st));
+  CK(cudaMemcpyAsync(c->h_norms, c->w.norms, 15 * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  std::memcpy(norms, c->h_norms, 15 * sizeof(double));
+  return CNS_OK;
+}
+
+int cns_bind_state(cns_ctx* c, const cns_state_t* s) {
+  if (!c || !s || !s->v || !s->u || !s->d || !s->dt || !s->sn || !s->vol ||
+      !s->pression || !s->ztemp || !s->cson || !s->mu || !s->mut || !s->tau)
+    return CNS_EINVAL;
+  c->state = *s;
+  c->bound = true;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return CNS_OK;
+}
+
+int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return CNS_EINVAL;
+  if (!c->bound || !c->metric_done)
+    return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
+  if (c->sc.kdtl == 0)
+    return fail(c, CNS_EINVAL, "the fused step runs with local time steps (kdtl != 0)");
+  if (!c->gexec) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(c);
+    cudaError_t e2 = cudaStreamEndCapture(c->st, &g);
+    CK(e);
+    CK(e2);
+    e = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
+  return CNS_OK;
+}
+
+int cns_last_norms(cns_ctx* c, double* norms) {
+  if (!c) return CNS_EINVAL;
+  CK(cudaMemcpyAsync(c->h_norms, c->w.norms, 15 * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->st));
+  int rc = check_status(c);
+  if (rc) return rc;
+  if (norms) std::memcpy(norms, c->h_norms, 15 * sizeof(double));
+  for (int q = 0; q < 15; ++q)
+    if (!std::isfinite(c->h_norms[q])) return fail(c, CNS_ENONFINITE, "non-finite residual norm");
+  return CNS_OK;
+}
+
+int cns_atsch_num_step(cns_ctx* c, int nsteps, double* norms) {
+  int rc = cns_atsch_num_launch(c, nsteps);
+  if (rc) return rc;
+  if (nsteps == 0) return check_status(c);
+  return cns_last_norms(c, norms);
+}
+
+int cns_atsch_num_step_host(cns_ctx* c, double* v_host, int nsteps, double* norms) {
+  if (!c || !v_host) return CNS_EINVAL;
+  if (!c->bound) return fail(c, CNS_ENOTREADY, "bind the state first");
+  const size_t bytes = sizeof(double) * 5 * (size_t)c->lay.ld;
+  CK(cudaMemcpyAsync(c->state.v, v_host, bytes, cudaMemcpyHostToDevice, c->st));
+  int rc = cns_atsch_num_step(c, nsteps, norms);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(v_host, c->state.v, bytes, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CNS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// cns_common.cuh -- device-side layout, index spaces and shared helpers of
+// the CodeNS hot path on sm_100a.
+//
+// Layout (the reference's per-block arrays, crdms.f90:125-158): every block
+// has real nodes 1..ni (one ghost layer on each side, id1 = 0), nodes and
+// cells share one flat index space, block l starts at npc(l).  Cell
+// (i,j,k) is npc + i + j*nid + k*nid*njd.  State arrays are column-major
+// (ld, ncol); the normals of a block sit at sn[9*npc ...] as
+// sn(nnn, 3 directions, 3 components).
+//
+// Work decomposition: every kernel walks an "index space" (real cells, the
+// faces of one direction, the lines of one direction, a boundary list)
+// through a tile work list built once on the host: tile t covers elements
+// [start, start+TILE) of one block, so uneven blocks and many independent
+// cases share a single launch with no per-thread block search.
+//
+// Arithmetic: the parity build compiles with --fmad=false and evaluates the
+// reference expressions in the reference's left-to-right order, so every
+// FP64 result is bit-identical to the reference semantics (IEEE add, mul,
+// div and sqrt are correctly rounded on both sides).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cns {
+
+constexpr int kMaxBlocks = 4096;
+
+struct Blk {
+  int ni, nj, nk;           // real node counts (ii2, jj2, kk2)
+  int nid, njd, nkd;        // with the ghost layer
+  long long npc;            // flat offset of the block
+  long long nijd, nnn;
+};
+
+// index space over all blocks: element e of block b has extents ext[3b..3b+2]
+// and maps to (i,j,k) = (1,1,1) + unflatten(e)
+struct Space {
+  const int* tile_blk;          // [ntiles]
+  const long long* tile_start;  // [ntiles]
+  const int* ext;               // [3*nblk]
+  int tile0;                    // first tile of this launch
+  int ntiles;
+};
+
+struct Phys {
+  double gam, gam1, pinfl, pr, prt, cp, reynz, suth_a, pa1, aa1, omg;
+};
+
+struct Scheme {
+  int ns, muscl, ilim, kdtl, lmax, qfix_dfez;
+  double xk, eta, dt1min;
+};
+
+// boundary tables (per boundary, then per list entry)
+struct Bnd {
+  int nbnd;
+  long long nlist;
+  const int* type;        // [nbnd]
+  const int* blk;         // [nbnd] 0-based
+  const int* face;        // [nbnd] 0..5 = i1,i2,j1,j2,k1,k2
+  const long long* mpb;   // [nbnd]
+  const int* mmb;         // [nbnd]
+  const int* partner;     // [nbnd]
+  const double* cosr;     // [nbnd]
+  const double* sinr;     // [nbnd]
+  const int* ent_bnd;     // [nlist] owning boundary of each entry
+  const long long* ncbd;  // [nlist]
+  const long long* ncin;  // [nlist]
+  const double* bceqt;    // [5*nlist] column-major
+  double* nxn;            // [nlist] filled by the metric
+  double* nyn;
+  double* nzn;
+  double* ym;
+  double* zm;
+};
+
+enum BcKind { BC_EXTR = 1, BC_RC = 2, BC_PARA = 3, BC_IDD = 4, BC_PRD = 5 };
+
+__device__ __forceinline__ double sq(double a) { return a * a; }
+
+// element of the tile handled by this thread; false when past the block end
+__device__ __forceinline__ bool space_elem(const Space& sp, int lane, int& b,
+                                           int& i, int& j, int& k) {
+  const int t = sp.tile0 + blockIdx.x;
+  b = sp.tile_blk[t];
+  const long long e = sp.tile_start[t] + lane;
+  const int ex = sp.ext[3 * b], ey = sp.ext[3 * b + 1], ez = sp.ext[3 * b + 2];
+  if (e >= (long long)ex * ey * ez) return false;
+  const int ee = (int)e;
+  i = ee % ex;
+  const int r = ee / ex;
+  j = r % ey;
+  k = r / ey;
+  i += 1;
+  j += 1;
+  k += 1;
+  return true;
+}
+
+__device__ __forceinline__ long long cell_index(const Blk& B, int i, int j, int k) {
+  return B.npc + (long long)i + (long long)j * B.nid + (long long)k * B.nijd;
+}
+__device__ __forceinline__ long long ninc_of(const Blk& B, int dir) {
+  return dir == 0 ? 1LL : (dir == 1 ? (long long)B.nid : B.nijd);
+}
+__device__ __forceinline__ int nd_of(const Blk& B, int dir) {
+  return dir == 0 ? B.ni : (dir == 1 ? B.nj : B.nk);
+}
+// sn(m, dir, c) of the block (m local index = n - npc)
+__device__ __forceinline__ const double* sn_ptr(const double* sn, const Blk& B,
+                                                int dir, int c) {
+  return sn + 9 * B.npc + (long long)c * 3 * B.nnn + (long long)dir * B.nnn - B.npc;
+}
+
+}  // namespace cns

@@ -1,0 +1,239 @@
+"""Host-side mirror of the reference's call surface for the hot path.
+
+``CodeNS`` holds one case on one GPU: the context (what the Fortran reference
+keeps in its modules) and the device arrays of the reference's flat layout,
+allocated through torch (device memory and streams only).  Its methods carry
+the reference routine names and argument meaning:
+
+    zpres(l, v, pression, ztemp, cson)              zpres.f90
+    zvismo(l, mu, v, ztemp)                         zvismo.f90
+    chronos(l, mu, mut, v, dt, sn, vol, cson)       chronos.f90
+    rbord(v, pression, ztemp, cson)                 rbord.f90
+    sch_roe_euler(l, u, v, sn, ps)                  sch_roe_euler.f90
+    sch_roe(l, u, v, tau, sn, ps)                   sch_roe.f90
+    zvisqc(v, mu, mut, tau, sn, vol, ztemp)         zvisqc.f90
+    implimf_eu(l, u, dt, v, d, sn, vol, ps, cson, lmx)
+    implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx)
+    rscpsv(u0, v, dt) -> (3, 5) L1/L2/Linf         rscpsv.f90 + residu.f90
+    atsch_num(nsteps) -> norms of the last step     atsch_num.f90 (fused, graph)
+
+Block numbers are 1-based like the reference; ``l = 0`` runs every block in
+one launch.  Every array argument is a float64 CUDA tensor in the reference
+layout (column-major (ld, ncol) flattened).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .cases import Case
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype.is_floating_point and t.is_contiguous()):
+        raise ValueError("arrays must be contiguous float64 CUDA tensors")
+    return C.c_void_p(t.data_ptr())
+
+
+class CodeNS:
+    def __init__(self, case: Case, device: int | None = None):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("codens_b200 needs a CUDA device: there is no CPU path")
+        self.torch = torch
+        if device is not None:
+            torch.cuda.set_device(device)
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.lib = abi.load()
+        self.case = case
+        lay = case.layout
+        self.ld = ld = lay.ld
+        self.nreal = lay.nreal
+        # host copies kept alive for the lifetime of the context
+        self._dims = np.ascontiguousarray(lay.dims_array())
+        ba = case.boundary_arrays()
+        self._ba = {k: np.ascontiguousarray(v) for k, v in ba.items()}
+        self._ba["bceqt"] = np.ascontiguousarray(ba["bceqt"].reshape(-1))
+        self.nlist = len(self._ba["ncbd"])
+        self._layout = abi.Layout_t(lay.nblk, self._dims.ctypes.data_as(C.POINTER(C.c_int32)), ld)
+        p = case.phys
+        self._phys = abi.Phys_t(p.gam, p.pinfl, p.pr, p.prt, p.reynz, p.suth_a, p.pa1,
+                                p.aa1, p.omg)
+        self._scheme = self._scheme_t(case.scheme)
+        b = self._ba
+
+        def ip(a, t):
+            return a.ctypes.data_as(C.POINTER(t))
+
+        self._bnd = abi.Bnd_t(len(b["type"]), ip(b["type"], C.c_int32), ip(b["blk"], C.c_int32),
+                              ip(b["face"], C.c_int32), ip(b["mpb"], C.c_int64),
+                              ip(b["mmb"], C.c_int32), ip(b["partner"], C.c_int32),
+                              ip(b["cosr"], C.c_double), ip(b["sinr"], C.c_double),
+                              self.nlist, ip(b["ncbd"], C.c_int64), ip(b["ncin"], C.c_int64),
+                              ip(b["bceqt"], C.c_double))
+        ctx = C.c_void_p()
+        rc = self.lib.cns_create(C.byref(self._layout), C.byref(self._phys),
+                                 C.byref(self._scheme), C.byref(self._bnd), C.byref(ctx))
+        if rc:
+            raise abi.CnsError(rc, "cns_create")
+        self.ctx = ctx
+        self.stream = torch.cuda.Stream()
+        self._check(self.lib.cns_set_stream(ctx, C.c_void_p(self.stream.cuda_stream)),
+                    "cns_set_stream")
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        self.x = torch.as_tensor(case.x, **f64).contiguous()
+        self.y = torch.as_tensor(case.y, **f64).contiguous()
+        self.z = torch.as_tensor(case.z, **f64).contiguous()
+        self.v = torch.as_tensor(case.v0.reshape(-1), **f64).contiguous()
+        self.u = torch.zeros(5 * ld, **f64)
+        self.d = torch.zeros(5 * ld, **f64)
+        self.dt = torch.zeros(ld, **f64)
+        self.sn = torch.zeros(9 * ld, **f64)
+        self.vol = torch.zeros(ld, **f64)
+        self.pression = torch.zeros(ld, **f64)
+        self.ztemp = torch.zeros(ld, **f64)
+        self.cson = torch.zeros(ld, **f64)
+        self.mu = torch.zeros(ld, **f64)
+        self.mut = torch.zeros(ld, **f64)
+        self.tau = torch.zeros(9 * ld, **f64)
+        torch.cuda.synchronize()
+        st = abi.State_t(*[C.c_void_p(t.data_ptr()) for t in
+                           (self.v, self.u, self.d, self.dt, self.sn, self.vol,
+                            self.pression, self.ztemp, self.cson, self.mu, self.mut,
+                            self.tau)])
+        self._check(self.lib.cns_bind_state(ctx, C.byref(st)), "cns_bind_state")
+        self._metric_done = False
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def _scheme_t(s, qfix_dfez: int = 0):
+        return abi.Scheme_t(int(s.ns), int(s.muscl), float(s.xk), int(s.ilim), float(s.eta),
+                            int(s.kdtl), float(s.dt1min), int(s.lmax),
+                            int(getattr(s, "qfix_dfez", qfix_dfez)))
+
+    def _check(self, rc: int, where: str):
+        if rc:
+            detail = self.lib.cns_last_error(self.ctx).decode() if getattr(self, "ctx", None) else ""
+            raise abi.CnsError(rc, where, detail)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.stream.synchronize()
+            self.lib.cns_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_scheme(self, scheme, qfix_dfez: int = 0):
+        self._scheme = self._scheme_t(scheme, qfix_dfez)
+        self._check(self.lib.cns_set_scheme(self.ctx, C.byref(self._scheme)), "cns_set_scheme")
+
+    def sync(self):
+        self.stream.synchronize()
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self.lib.cns_scratch_bytes(self.ctx))
+
+    # ---- set-up -------------------------------------------------------
+    def metric(self):
+        """metric.f90: ghost nodes, sn, vol and the boundary-entry geometry."""
+        self._check(self.lib.cns_metric(self.ctx, _ptr(self.x), _ptr(self.y), _ptr(self.z),
+                                        _ptr(self.sn), _ptr(self.vol)), "cns_metric")
+        self._metric_done = True
+
+    def boundary_geom(self):
+        out = [np.zeros(max(self.nlist, 1)) for _ in range(5)]
+        self._check(self.lib.cns_boundary_geom(
+            self.ctx, *[o.ctypes.data_as(C.POINTER(C.c_double)) for o in out]),
+            "cns_boundary_geom")
+        return [o[: self.nlist] for o in out]
+
+    # ---- reference call surface ----------------------------------------
+    def zpres(self, l, v, pression, ztemp, cson):
+        self._check(self.lib.cns_zpres(self.ctx, l, _ptr(v), _ptr(pression), _ptr(ztemp),
+                                       _ptr(cson)), "cns_zpres")
+
+    def zvismo(self, l, mu, v, ztemp):
+        self._check(self.lib.cns_zvismo(self.ctx, l, _ptr(mu), _ptr(v), _ptr(ztemp)),
+                    "cns_zvismo")
+
+    def chronos(self, l, mu, mut, v, dt, sn, vol, cson):
+        self._check(self.lib.cns_chronos(self.ctx, l, _ptr(mu), _ptr(mut), _ptr(v), _ptr(dt),
+                                         _ptr(sn), _ptr(vol), _ptr(cson)), "cns_chronos")
+
+    def rbord(self, v, pression, ztemp, cson):
+        self._check(self.lib.cns_rbord(self.ctx, _ptr(v), _ptr(pression), _ptr(ztemp),
+                                       _ptr(cson)), "cns_rbord")
+
+    def sch_roe_euler(self, l, u, v, sn, ps):
+        self._check(self.lib.cns_sch_roe_euler(self.ctx, l, _ptr(u), _ptr(v), _ptr(sn),
+                                               _ptr(ps)), "cns_sch_roe_euler")
+
+    def sch_roe(self, l, u, v, tau, sn, ps):
+        self._check(self.lib.cns_sch_roe(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
+                                         _ptr(ps)), "cns_sch_roe")
+
+    def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
+        self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
+                                        _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")
+
+    def implimf_eu(self, l, u, dt, v, d, sn, vol, ps, cson, lmx):
+        self._check(self.lib.cns_implimf_eu(self.ctx, l, _ptr(u), _ptr(dt), _ptr(v), _ptr(d),
+                                            _ptr(sn), _ptr(vol), _ptr(ps), _ptr(cson), lmx),
+                    "cns_implimf_eu")
+
+    def implimf_3d(self, l, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx):
+        self._check(self.lib.cns_implimf_3d(self.ctx, l, _ptr(u), _ptr(dt), _ptr(v), _ptr(d),
+                                            _ptr(mu), _ptr(mut), _ptr(sn), _ptr(vol), _ptr(ps),
+                                            _ptr(cson), lmx), "cns_implimf_3d")
+
+    def rscpsv(self, u0, v, dt) -> np.ndarray:
+        out = (C.c_double * 15)()
+        self._check(self.lib.cns_rscpsv(self.ctx, _ptr(u0), _ptr(v), _ptr(dt), out),
+                    "cns_rscpsv")
+        return np.array(out).reshape(3, 5)
+
+    # ---- fused fast path ------------------------------------------------
+    def atsch_num(self, nsteps: int = 1) -> np.ndarray:
+        """nsteps pseudo-time iterations on the device-resident state (one
+        CUDA graph per iteration); returns the L1/L2/Linf of the last one."""
+        if not self._metric_done:
+            self.metric()
+        out = (C.c_double * 15)()
+        self._check(self.lib.cns_atsch_num_step(self.ctx, int(nsteps), out),
+                    "cns_atsch_num_step")
+        return np.array(out).reshape(3, 5)
+
+    def atsch_num_launch(self, nsteps: int = 1):
+        """enqueue nsteps iterations on self.stream without waiting"""
+        if not self._metric_done:
+            self.metric()
+        self._check(self.lib.cns_atsch_num_launch(self.ctx, int(nsteps)), "cns_atsch_num_launch")
+
+    def last_norms(self) -> np.ndarray:
+        out = (C.c_double * 15)()
+        self._check(self.lib.cns_last_norms(self.ctx, out), "cns_last_norms")
+        return np.array(out).reshape(3, 5)
+
+    def atsch_num_host(self, v_host, nsteps: int = 1) -> np.ndarray:
+        """Same through the host-array entry point: v_host (a pinned CPU
+        float64 tensor of 5*ld) is copied in, advanced and copied back."""
+        if not self._metric_done:
+            self.metric()
+        if v_host.is_cuda or v_host.dtype != self.torch.float64 or not v_host.is_contiguous():
+            raise ValueError("v_host must be a contiguous float64 CPU tensor")
+        out = (C.c_double * 15)()
+        self._check(self.lib.cns_atsch_num_step_host(self.ctx, C.c_void_p(v_host.data_ptr()),
+                                                     int(nsteps), out),
+                    "cns_atsch_num_step_host")
+        return np.array(out).reshape(3, 5)

@@ -1,0 +1,192 @@
+/*
+ * cns_abi.h -- C ABI of the B200 implementation of the CodeNS per-iteration
+ * hot path (residual evaluation and matrix-free implicit update on
+ * structured multi-block grids).
+ *
+ * The entry points keep the reference's call surface: one function per
+ * reference subroutine, the same argument meaning and order, prefixed
+ * "cns_", plus a context handle that carries what the reference reads from
+ * its Fortran modules (maillage: block layout; proprieteflu/definition:
+ * physical constants; schemanum: scheme keys; boundary: boundary lists).
+ *
+ * Data contract (identical to the reference's arrays, crdms.f90:125-158):
+ *   - blocks l = 1..nblk with real nodes 1..ni, 1..nj, 1..nk and one ghost
+ *     layer; nodes and cells share one flat index space; block l starts at
+ *     npc(l) = sum of (ni+2)(nj+2)(nk+2) of the blocks before it;
+ *   - cell (i,j,k) of block l is element npc(l) + i + j*(ni+2) + k*(ni+2)*(nj+2)
+ *     (0-based storage of sch_roe.f90:1487-1491);
+ *   - v, u, d are column-major (ld, 5) double arrays (ip11 x ip60, columns
+ *     1..5 = rho, rho u, rho v, rho w, rho E); scalar cell arrays are (ld);
+ *   - sn holds, for block l at offset 9*npc(l), sn(nnn, 3 face directions,
+ *     3 components), the area vector of the lower face of each cell oriented
+ *     towards increasing index (norm.f90);
+ *   - tau is (ld, 9): toxx, toxy, toxz, toyy, toyz, tozz, qcx, qcy, qcz.
+ * All array pointers given to kernel entry points are DEVICE pointers on the
+ * context's device; the *_host entry points take host pointers.
+ *
+ * Errors: every function returns 0 on success or a CNS_E* code.  The
+ * reference prints and stops instead (zvismo.f90:123-127, chrono.f90:134-142,
+ * rbord.f90:417-421); a Fortran shim turns a nonzero code into that message
+ * and STOP.
+ *
+ * Threading: a context is used from one host thread; work is ordered on the
+ * context's CUDA stream (cns_set_stream).
+ */
+#ifndef CNS_ABI_H
+#define CNS_ABI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CNS_OK = 0,
+  CNS_EINVAL = 1,      /* bad argument (block number, sizes, pointers) */
+  CNS_ECUDA = 2,       /* CUDA runtime error */
+  CNS_ETEMP = 3,       /* non-positive temperature (zvismo.f90:123-127) */
+  CNS_EDT = 4,         /* global time step below dt1min (chrono.f90:134-142) */
+  CNS_EBC = 5,         /* unknown boundary condition (rbord.f90:417-421) */
+  CNS_ENOTREADY = 6,   /* state arrays not bound / metric not computed */
+  CNS_ENONFINITE = 7   /* non-finite residual norm after a step */
+};
+
+/* boundary kinds (rbord.f90:144-424) */
+enum { CNS_BC_EXTR = 1, CNS_BC_RC = 2, CNS_BC_PARA = 3, CNS_BC_IDD = 4,
+       CNS_BC_PRD = 5 };
+
+typedef struct cns_ctx cns_ctx;
+
+/* maillage: block dimensions (ii2, jj2, kk2 = real node counts) */
+typedef struct {
+  int32_t nblk;
+  const int32_t *dims;   /* [3*nblk]: ni, nj, nk of each block */
+  int64_t ld;            /* ip11: leading dimension of the state arrays */
+} cns_layout_t;
+
+/* proprieteflu / definition (dfph.f90, c_nzst.f90, zvismo.f90:79) */
+typedef struct {
+  double gam, pinfl, pr, prt, reynz;
+  double suth_a;         /* Sutherland 110.4/tnz */
+  double pa1, aa1, omg;  /* reference pressure, sound speed, rotation speed */
+} cns_phys_t;
+
+/* schemanum keys of the path (tcmd_dfnm.f90, defdf*.f90) */
+typedef struct {
+  int32_t ns;            /* equat(1:2) == 'ns' */
+  int32_t muscl;
+  double xk;
+  int32_t ilim;          /* 1: minmod limiter with the in-place ratio recurrence */
+  double eta;            /* CFL */
+  int32_t kdtl;          /* 0: global time step (chrono.f90:113-151) */
+  double dt1min;
+  int32_t lmax;          /* Jacobi sub-iterations */
+  int32_t qfix_dfez;     /* non-reference option: restore the missing *wi of
+                            implimf_eu.f90:312 (0 = reference behaviour) */
+} cns_scheme_t;
+
+/* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
+typedef struct {
+  int32_t nbnd;
+  const int32_t *type;    /* [nbnd] CNS_BC_* */
+  const int32_t *blk;     /* [nbnd] owning block, 1-based */
+  const int32_t *face;    /* [nbnd] 0..5 = i1,i2,j1,j2,k1,k2 */
+  const int64_t *mpb;     /* [nbnd] first list entry */
+  const int32_t *mmb;     /* [nbnd] entry count */
+  const int32_t *partner; /* [nbnd] coincident partner boundary (0-based), -1 */
+  const double *cosr;     /* [nbnd] cos of the boundary's periodic angle */
+  const double *sinr;     /* [nbnd] sin of the boundary's periodic angle */
+  int64_t nlist;
+  const int64_t *ncbd;    /* [nlist] ghost cell (0-based flat index) */
+  const int64_t *ncin;    /* [nlist] adjacent interior cell */
+  const double *bceqt;    /* [5*nlist] column-major: idd rpi,rti,d0x,d0y,d0z;
+                             prd p */
+} cns_bnd_t;
+
+/* device-resident arrays of the fast path (all device pointers, same layout
+ * as above); the context never frees them */
+typedef struct {
+  double *v, *u, *d, *dt, *sn, *vol;
+  double *pression, *ztemp, *cson, *mu, *mut, *tau;
+} cns_state_t;
+
+/* ---- context ---------------------------------------------------------- */
+int cns_create(const cns_layout_t *layout, const cns_phys_t *phys,
+               const cns_scheme_t *scheme, const cns_bnd_t *bnd,
+               cns_ctx **out);
+int cns_destroy(cns_ctx *ctx);
+int cns_set_stream(cns_ctx *ctx, void *cuda_stream);
+int cns_set_scheme(cns_ctx *ctx, const cns_scheme_t *scheme);
+const char *cns_last_error(cns_ctx *ctx);
+int64_t cns_scratch_bytes(cns_ctx *ctx);
+
+/* ---- set-up ------------------------------------------------------------ */
+/* metric.f90 -> metrics.f90: ghost nodes (extmhg), sn (norm), vol (svol),
+ * coincident ghost volumes (rfsc) and the boundary-entry geometry (initns,
+ * clidd ghost centres) kept in the context.  x, y, z: node coordinates,
+ * ghost nodes overwritten. */
+int cns_metric(cns_ctx *ctx, double *x, double *y, double *z, double *sn,
+               double *vol);
+/* copy the boundary-entry geometry to host arrays of nlist doubles */
+int cns_boundary_geom(cns_ctx *ctx, double *nxn, double *nyn, double *nzn,
+                      double *ym, double *zm);
+
+/* ---- per-routine entry points (l = 1..nblk; l = 0: every block) ---------- */
+/* zpres.f90:4-101 */
+int cns_zpres(cns_ctx *ctx, int l, const double *v, double *pression,
+              double *ztemp, double *cson);
+/* zvismo.f90:4-136 (iflu = 1) */
+int cns_zvismo(cns_ctx *ctx, int l, double *mu, const double *v,
+               const double *ztemp);
+/* chronos.f90:4-213 (kprec = 0) with the scheme's eta */
+int cns_chronos(cns_ctx *ctx, int l, const double *mu, const double *mut,
+                const double *v, double *dt, const double *sn,
+                const double *vol, const double *cson);
+/* rbord.f90:4-433 restricted to extr, rc, para, idd, prd */
+int cns_rbord(cns_ctx *ctx, double *v, double *pression, double *ztemp,
+              double *cson);
+/* sch_roe_euler.f90:106-1009 (ityprk = 0) */
+int cns_sch_roe_euler(cns_ctx *ctx, int l, double *u, const double *v,
+                      const double *sn, const double *ps);
+/* sch_roe.f90:4-1505 (ityprk = 0) */
+int cns_sch_roe(cns_ctx *ctx, int l, double *u, const double *v,
+                const double *tau, const double *sn, const double *ps);
+/* zvisqc.f90:4-210: zgrad2 + zfluto on every block, then rbte/rbtc */
+int cns_zvisqc(cns_ctx *ctx, const double *v, const double *mu,
+               const double *mut, double *tau, const double *sn,
+               const double *vol, const double *ztemp);
+/* implimf_eu.f90:6-347 (kfmg != 3, ityprk = 0) */
+int cns_implimf_eu(cns_ctx *ctx, int l, const double *u, const double *dt,
+                   double *v, double *d, const double *sn, const double *vol,
+                   const double *ps, const double *cson, int lmx);
+/* implimf_3d.f90:4-502 (kfmg != 3, ityprk = 0) */
+int cns_implimf_3d(cns_ctx *ctx, int l, const double *u, const double *dt,
+                   double *v, double *d, const double *mu, const double *mut,
+                   const double *sn, const double *vol, const double *ps,
+                   const double *cson, int lmx);
+/* rscpsv.f90 + residu.f90: L1, L2, Linf of (v-u0)/dt over all blocks;
+ * norms: host array of 15 doubles (L1[5], L2[5], Linf[5]) */
+int cns_rscpsv(cns_ctx *ctx, const double *u0, const double *v,
+               const double *dt, double *norms);
+
+/* ---- fast path ---------------------------------------------------------- */
+int cns_bind_state(cns_ctx *ctx, const cns_state_t *state);
+/* nsteps pseudo-time iterations of atsch_num.f90 (Roe, implicit) on the bound
+ * state; the step sequence is captured once in a CUDA graph and replayed.
+ * norms (host, may be NULL): 15 doubles of the LAST step. */
+int cns_atsch_num_step(cns_ctx *ctx, int nsteps, double *norms);
+/* enqueue nsteps iterations without waiting (stream-ordered); the norms of
+ * the last enqueued iteration are read back by cns_last_norms, which waits
+ * for the stream and checks the device status word */
+int cns_atsch_num_launch(cns_ctx *ctx, int nsteps);
+int cns_last_norms(cns_ctx *ctx, double *norms);
+/* drop-in call with host arrays: copies the real+ghost state v (host, ld x 5)
+ * in, runs nsteps iterations, copies v back and returns the last norms */
+int cns_atsch_num_step_host(cns_ctx *ctx, double *v_host, int nsteps,
+                            double *norms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CNS_ABI_H */

@@ -1,0 +1,1628 @@
+/*
+ * cns_oracle.c -- CPU oracle for the CodeNS hot path (test infrastructure).
+ *
+ * This file is the checker that tests/ and bench.py's CPU-baseline leg run
+ * against the CUDA product; the product never loads it.  Each routine names
+ * the reference file and lines it restates.  Parity is UNPINNED (no
+ * reference outputs exist; see cns_oracle.h).
+ *
+ * Build: gcc -O2 -ffp-contract=off -fno-fast-math -shared -fPIC (oracle/Makefile).
+ */
+#include "cns_oracle.h"
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAXB 1024
+
+typedef struct {
+  int ni, nj, nk;        /* ii2, jj2, kk2: real node counts (ii1=jj1=kk1=1) */
+  int64_t npc;           /* 0-based offset of the block (crdms.f90:150-157) */
+  int nid, njd, nkd;     /* id2-id1+1 ... with nfi=1 */
+  int64_t nijd, nnn;
+} blk_t;
+
+static struct {
+  int nblk;
+  blk_t b[MAXB];
+  int64_t ld, ncells;
+  /* proprieteflu / definition */
+  double gam, gam1, pinfl, pr, prt, cp, reynz, suth_a, pa1, aa1, omg;
+  /* schemanum */
+  int ns, muscl, ilim, kdtl, lmax;
+  double xk, eta, dt1min;
+  /* boundary */
+  int nbnd;
+  int32_t *btype, *bblk, *bface, *bmmb, *bpart;
+  int64_t *bmpb;
+  double *bcos, *bsin;
+  int64_t nlist;
+  int64_t *ncbd, *ncin;
+  double *nxn, *nyn, *nzn, *bceqt, *bym, *bzm;
+} G;
+
+static inline double sq(double a) { return a * a; }
+
+/* cell (or node) (i,j,k), Fortran index values, ghost layer starting at 0 */
+static inline int64_t IC(const blk_t *b, int i, int j, int k) {
+  return b->npc + (int64_t)i + (int64_t)j * b->nid + (int64_t)k * b->nijd;
+}
+static inline int64_t ML(const blk_t *b, int i, int j, int k) {
+  return (int64_t)i + (int64_t)j * b->nid + (int64_t)k * b->nijd;
+}
+/* sn(m,kdir,c) of the block slice starting at 9*npc (atsch_num.f90:470) */
+static inline double SN(const double *sn, const blk_t *b, int64_t m, int kdir,
+                        int c) {
+  return sn[9 * b->npc + (int64_t)c * 3 * b->nnn + (int64_t)kdir * b->nnn + m];
+}
+static inline double *SNW(double *sn, const blk_t *b, int64_t m, int kdir,
+                          int c) {
+  return &sn[9 * b->npc + (int64_t)c * 3 * b->nnn + (int64_t)kdir * b->nnn + m];
+}
+static inline int64_t NINC(const blk_t *b, int dir) {
+  return dir == 0 ? 1 : (dir == 1 ? (int64_t)b->nid : b->nijd);
+}
+static inline int NDIR(const blk_t *b, int dir) {
+  return dir == 0 ? b->ni : (dir == 1 ? b->nj : b->nk);
+}
+
+int orc_setup(int nblk, const int32_t *dims, int64_t ld) {
+  if (nblk < 1 || nblk > MAXB) return 1;
+  G.nblk = nblk;
+  int64_t off = 0;
+  for (int l = 0; l < nblk; ++l) {
+    blk_t *b = &G.b[l];
+    b->ni = dims[3 * l];
+    b->nj = dims[3 * l + 1];
+    b->nk = dims[3 * l + 2];
+    if (b->ni < 2 || b->nj < 2 || b->nk < 2) return 2;
+    b->nid = b->ni + 2;
+    b->njd = b->nj + 2;
+    b->nkd = b->nk + 2;
+    b->nijd = (int64_t)b->nid * b->njd;
+    b->nnn = b->nijd * b->nkd;
+    b->npc = off;
+    off += b->nnn;
+  }
+  G.ncells = off;
+  G.ld = ld > 0 ? ld : off;
+  if (G.ld < off) return 3;
+  return 0;
+}
+int64_t orc_npc(int l) { return G.b[l - 1].npc; }
+int64_t orc_ncells(void) { return G.ncells; }
+
+/* dfph.f90:31-35, dfnzst.f90:67 (cp=1/(gam-1)), c_nzst.f90 */
+void orc_set_phys(double gam, double pinfl, double pr, double prt,
+                  double reynz, double suth_a, double pa1, double aa1,
+                  double omg) {
+  G.gam = gam;
+  G.gam1 = gam - 1.;
+  G.pinfl = pinfl;
+  G.pr = pr;
+  G.prt = prt;
+  G.cp = 1. / (gam - 1.);
+  G.reynz = reynz;
+  G.suth_a = suth_a;
+  G.pa1 = pa1;
+  G.aa1 = aa1;
+  G.omg = omg;
+}
+
+void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
+                    int kdtl, double dt1min, int lmax) {
+  G.ns = ns;
+  G.muscl = muscl;
+  G.xk = xk;
+  G.ilim = ilim;
+  G.eta = eta;
+  G.kdtl = kdtl;
+  G.dt1min = dt1min;
+  G.lmax = lmax;
+}
+
+#define DUP(dst, src, n, T)                                   \
+  do {                                                        \
+    free(dst);                                                \
+    dst = (T *)malloc(sizeof(T) * ((n) > 0 ? (n) : 1));       \
+    if ((n) > 0 && (src)) memcpy(dst, src, sizeof(T) * (n));  \
+  } while (0)
+
+int orc_set_boundaries(int nbnd, const int32_t *type, const int32_t *blk,
+                       const int32_t *face, const int64_t *mpb,
+                       const int32_t *mmb, const int32_t *partner,
+                       const double *cosr, const double *sinr, int64_t nlist,
+                       const int64_t *ncbd, const int64_t *ncin,
+                       const double *bceqt) {
+  G.nbnd = nbnd;
+  DUP(G.btype, type, nbnd, int32_t);
+  DUP(G.bblk, blk, nbnd, int32_t);
+  DUP(G.bface, face, nbnd, int32_t);
+  DUP(G.bmpb, mpb, nbnd, int64_t);
+  DUP(G.bmmb, mmb, nbnd, int32_t);
+  DUP(G.bpart, partner, nbnd, int32_t);
+  DUP(G.bcos, cosr, nbnd, double);
+  DUP(G.bsin, sinr, nbnd, double);
+  G.nlist = nlist;
+  DUP(G.ncbd, ncbd, nlist, int64_t);
+  DUP(G.ncin, ncin, nlist, int64_t);
+  DUP(G.bceqt, bceqt, 5 * nlist, double);
+  double **geo[5] = {&G.nxn, &G.nyn, &G.nzn, &G.bym, &G.bzm};
+  for (int a = 0; a < 5; ++a) {
+    free(*geo[a]);
+    *geo[a] = calloc((size_t)(nlist > 0 ? nlist : 1), sizeof(double));
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* geometry                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* extmhg.f90:51-100 with ex1=exs1=1, ex2=exs2=0 (solve.f90:384-385) */
+static void extmhg(const blk_t *b, double *x, double *y, double *z) {
+  const double ex1 = 1., ex2 = 0.;
+  const int64_t nci = 1, ncj = b->nid, nck = b->nijd;
+  const int i1 = 1, i2 = b->ni, j1 = 1, j2 = b->nj, k1 = 1, k2 = b->nk;
+  int ks = -1;
+  for (int k = k1 - 1; k <= k2 + 1; k += (k2 + 1) - (k1 - 1)) {
+    ks = -ks;
+    for (int j = j1; j <= j2; ++j)
+      for (int i = i1; i <= i2; ++i) {
+        int64_t n = IC(b, i, j, k);
+        x[n] = ex1 * x[n + ks * nck] + ex2 * x[n + ks * 2 * nck];
+        y[n] = ex1 * y[n + ks * nck] + ex2 * y[n + ks * 2 * nck];
+        z[n] = ex1 * z[n + ks * nck] + ex2 * z[n + ks * 2 * nck];
+      }
+  }
+  for (int k = k1 - 1; k <= k2 + 1; ++k)
+    for (int j = j1; j <= j2; ++j) {
+      int is = -1;
+      for (int i = i1 - 1; i <= i2 + 1; i += (i2 + 1) - (i1 - 1)) {
+        is = -is;
+        int64_t n = IC(b, i, j, k);
+        x[n] = ex1 * x[n + is * nci] + ex2 * x[n + is * 2 * nci];
+        y[n] = ex1 * y[n + is * nci] + ex2 * y[n + is * 2 * nci];
+        z[n] = ex1 * z[n + is * nci] + ex2 * z[n + is * 2 * nci];
+      }
+    }
+  for (int k = k1 - 1; k <= k2 + 1; ++k) {
+    int js = -1;
+    for (int j = j1 - 1; j <= j2 + 1; j += (j2 + 1) - (j1 - 1)) {
+      js = -js;
+      for (int i = i1 - 1; i <= i2 + 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        x[n] = ex1 * x[n + js * ncj] + ex2 * x[n + js * 2 * ncj];
+        y[n] = ex1 * y[n + js * ncj] + ex2 * y[n + js * 2 * ncj];
+        z[n] = ex1 * z[n + js * ncj] + ex2 * z[n + js * 2 * ncj];
+      }
+    }
+  }
+}
+
+/* norm.f90:57-271 called from snorm.f90 with imin=i1-1 ... imax=i2+1 */
+static void snorm(const blk_t *b, const double *x, const double *y,
+                  const double *z, double *sn) {
+  const int64_t n0 = b->npc;
+#define INC(a, bb, c) ((int64_t)(a) + (int64_t)(bb) * b->nid + (int64_t)(c) * b->nijd)
+  const int imin = 0, imax = b->ni + 1, jmin = 0, jmax = b->nj + 1, kmin = 0,
+            kmax = b->nk + 1;
+  const int64_t nor = IC(b, 2, 2, 2);
+  double dx1, dy1, dz1, dx2, dy2, dz2, vx, vy, vz, tx, ty, tz;
+  /* k faces */
+  dx1 = x[nor + INC(1, 1, 0)] - x[nor];
+  dy1 = y[nor + INC(1, 1, 0)] - y[nor];
+  dz1 = z[nor + INC(1, 1, 0)] - z[nor];
+  dx2 = x[nor + INC(0, 1, 0)] - x[nor + INC(1, 0, 0)];
+  dy2 = y[nor + INC(0, 1, 0)] - y[nor + INC(1, 0, 0)];
+  dz2 = z[nor + INC(0, 1, 0)] - z[nor + INC(1, 0, 0)];
+  tx = dy1 * dz2 - dz1 * dy2;
+  ty = dz1 * dx2 - dx1 * dz2;
+  tz = dx1 * dy2 - dy1 * dx2;
+  vx = x[nor + INC(0, 0, 1)] - x[nor] + x[nor + INC(1, 0, 1)] - x[nor + INC(1, 0, 0)] +
+       x[nor + INC(0, 1, 1)] - x[nor + INC(0, 1, 0)] + x[nor + INC(1, 1, 1)] - x[nor + INC(1, 1, 0)];
+  vy = y[nor + INC(0, 0, 1)] - y[nor] + y[nor + INC(1, 0, 1)] - y[nor + INC(1, 0, 0)] +
+       y[nor + INC(0, 1, 1)] - y[nor + INC(0, 1, 0)] + y[nor + INC(1, 1, 1)] - y[nor + INC(1, 1, 0)];
+  vz = z[nor + INC(0, 0, 1)] - z[nor] + z[nor + INC(1, 0, 1)] - z[nor + INC(1, 0, 0)] +
+       z[nor + INC(0, 1, 1)] - z[nor + INC(0, 1, 0)] + z[nor + INC(1, 1, 1)] - z[nor + INC(1, 1, 0)];
+  const double psk = tx * vx + ty * vy + tz * vz;
+  for (int k = kmin; k <= kmax; ++k)
+    for (int j = jmin; j <= jmax - 1; ++j)
+      for (int i = imin; i <= imax - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        dx1 = x[n + INC(1, 1, 0)] - x[n];
+        dy1 = y[n + INC(1, 1, 0)] - y[n];
+        dz1 = z[n + INC(1, 1, 0)] - z[n];
+        dx2 = x[n + INC(0, 1, 0)] - x[n + INC(1, 0, 0)];
+        dy2 = y[n + INC(0, 1, 0)] - y[n + INC(1, 0, 0)];
+        dz2 = z[n + INC(0, 1, 0)] - z[n + INC(1, 0, 0)];
+        *SNW(sn, b, m, 2, 0) = copysign(.5, psk) * (dy1 * dz2 - dz1 * dy2);
+        *SNW(sn, b, m, 2, 1) = copysign(.5, psk) * (dz1 * dx2 - dx1 * dz2);
+        *SNW(sn, b, m, 2, 2) = copysign(.5, psk) * (dx1 * dy2 - dy1 * dx2);
+      }
+  /* j faces */
+  dx1 = x[nor + INC(1, 0, 1)] - x[nor];
+  dy1 = y[nor + INC(1, 0, 1)] - y[nor];
+  dz1 = z[nor + INC(1, 0, 1)] - z[nor];
+  dx2 = x[nor + INC(0, 0, 1)] - x[nor + INC(1, 0, 0)];
+  dy2 = y[nor + INC(0, 0, 1)] - y[nor + INC(1, 0, 0)];
+  dz2 = z[nor + INC(0, 0, 1)] - z[nor + INC(1, 0, 0)];
+  tx = dy1 * dz2 - dz1 * dy2;
+  ty = dz1 * dx2 - dx1 * dz2;
+  tz = dx1 * dy2 - dy1 * dx2;
+  vx = x[nor + INC(0, 1, 0)] - x[nor] + x[nor + INC(1, 1, 0)] - x[nor + INC(1, 0, 0)] +
+       x[nor + INC(0, 1, 1)] - x[nor + INC(0, 0, 1)] + x[nor + INC(1, 1, 1)] - x[nor + INC(1, 0, 1)];
+  vy = y[nor + INC(0, 1, 0)] - y[nor] + y[nor + INC(1, 1, 0)] - y[nor + INC(1, 0, 0)] +
+       y[nor + INC(0, 1, 1)] - y[nor + INC(0, 0, 1)] + y[nor + INC(1, 1, 1)] - y[nor + INC(1, 0, 1)];
+  vz = z[nor + INC(0, 1, 0)] - z[nor] + z[nor + INC(1, 1, 0)] - z[nor + INC(1, 0, 0)] +
+       z[nor + INC(0, 1, 1)] - z[nor + INC(0, 0, 1)] + z[nor + INC(1, 1, 1)] - z[nor + INC(1, 0, 1)];
+  const double psj = tx * vx + ty * vy + tz * vz;
+  for (int j = jmin; j <= jmax; ++j)
+    for (int k = kmin; k <= kmax - 1; ++k)
+      for (int i = imin; i <= imax - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        dx1 = x[n + INC(1, 0, 1)] - x[n];
+        dy1 = y[n + INC(1, 0, 1)] - y[n];
+        dz1 = z[n + INC(1, 0, 1)] - z[n];
+        dx2 = x[n + INC(0, 0, 1)] - x[n + INC(1, 0, 0)];
+        dy2 = y[n + INC(0, 0, 1)] - y[n + INC(1, 0, 0)];
+        dz2 = z[n + INC(0, 0, 1)] - z[n + INC(1, 0, 0)];
+        *SNW(sn, b, m, 1, 0) = copysign(.5, psj) * (dy1 * dz2 - dz1 * dy2);
+        *SNW(sn, b, m, 1, 1) = copysign(.5, psj) * (dz1 * dx2 - dx1 * dz2);
+        *SNW(sn, b, m, 1, 2) = copysign(.5, psj) * (dx1 * dy2 - dy1 * dx2);
+      }
+  /* i faces */
+  dx1 = x[nor + INC(0, 1, 1)] - x[nor];
+  dy1 = y[nor + INC(0, 1, 1)] - y[nor];
+  dz1 = z[nor + INC(0, 1, 1)] - z[nor];
+  dx2 = x[nor + INC(0, 0, 1)] - x[nor + INC(0, 1, 0)];
+  dy2 = y[nor + INC(0, 0, 1)] - y[nor + INC(0, 1, 0)];
+  dz2 = z[nor + INC(0, 0, 1)] - z[nor + INC(0, 1, 0)];
+  tx = dy1 * dz2 - dz1 * dy2;
+  ty = dz1 * dx2 - dx1 * dz2;
+  tz = dx1 * dy2 - dy1 * dx2;
+  vx = x[nor + INC(1, 0, 0)] - x[nor] + x[nor + INC(1, 1, 0)] - x[nor + INC(0, 1, 0)] +
+       x[nor + INC(1, 0, 1)] - x[nor + INC(0, 0, 1)] + x[nor + INC(1, 1, 1)] - x[nor + INC(0, 1, 1)];
+  vy = y[nor + INC(1, 0, 0)] - y[nor] + y[nor + INC(1, 1, 0)] - y[nor + INC(0, 1, 0)] +
+       y[nor + INC(1, 0, 1)] - y[nor + INC(0, 0, 1)] + y[nor + INC(1, 1, 1)] - y[nor + INC(0, 1, 1)];
+  vz = z[nor + INC(1, 0, 0)] - z[nor] + z[nor + INC(1, 1, 0)] - z[nor + INC(0, 1, 0)] +
+       z[nor + INC(1, 0, 1)] - z[nor + INC(0, 0, 1)] + z[nor + INC(1, 1, 1)] - z[nor + INC(0, 1, 1)];
+  const double psi = tx * vx + ty * vy + tz * vz;
+  for (int i = imin; i <= imax; ++i)
+    for (int k = kmin; k <= kmax - 1; ++k)
+      for (int j = jmin; j <= jmax - 1; ++j) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        dx1 = x[n + INC(0, 1, 1)] - x[n];
+        dy1 = y[n + INC(0, 1, 1)] - y[n];
+        dz1 = z[n + INC(0, 1, 1)] - z[n];
+        dx2 = x[n + INC(0, 0, 1)] - x[n + INC(0, 1, 0)];
+        dy2 = y[n + INC(0, 0, 1)] - y[n + INC(0, 1, 0)];
+        dz2 = z[n + INC(0, 0, 1)] - z[n + INC(0, 1, 0)];
+        *SNW(sn, b, m, 0, 0) = copysign(.5, psi) * (dy1 * dz2 - dz1 * dy2);
+        *SNW(sn, b, m, 0, 1) = copysign(.5, psi) * (dz1 * dx2 - dx1 * dz2);
+        *SNW(sn, b, m, 0, 2) = copysign(.5, psi) * (dx1 * dy2 - dy1 * dx2);
+      }
+#undef INC
+}
+
+/* svol.f90:62-150 */
+static void svol(const blk_t *b, const double *x, const double *y,
+                 const double *z, const double *sn, double *vol) {
+  const int64_t n0 = b->npc, nci = 1, ncj = b->nid, nck = b->nijd;
+  double *siv = calloc(b->nnn, sizeof(double));
+  double *sjv = calloc(b->nnn, sizeof(double));
+  double *skv = calloc(b->nnn, sizeof(double));
+  const int i1m1 = 0, i2 = b->ni, i2p1 = b->ni + 1, j1m1 = 0, j2 = b->nj,
+            j2p1 = b->nj + 1, k1m1 = 0, k2 = b->nk, k2p1 = b->nk + 1;
+  for (int k = k1m1; k <= k2p1; ++k)
+    for (int j = j1m1; j <= j2; ++j)
+      for (int i = i1m1; i <= i2; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        skv[m] = (x[n] + x[n + nci] + x[n + ncj] + x[n + nci + ncj]) * SN(sn, b, m, 2, 0) +
+                 (y[n] + y[n + nci] + y[n + ncj] + y[n + nci + ncj]) * SN(sn, b, m, 2, 1) +
+                 (z[n] + z[n + nci] + z[n + ncj] + z[n + nci + ncj]) * SN(sn, b, m, 2, 2);
+      }
+  for (int j = j1m1; j <= j2p1; ++j)
+    for (int k = k1m1; k <= k2; ++k)
+      for (int i = i1m1; i <= i2; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        sjv[m] = (x[n] + x[n + nci] + x[n + nck] + x[n + nci + nck]) * SN(sn, b, m, 1, 0) +
+                 (y[n] + y[n + nci] + y[n + nck] + y[n + nci + nck]) * SN(sn, b, m, 1, 1) +
+                 (z[n] + z[n + nci] + z[n + nck] + z[n + nci + nck]) * SN(sn, b, m, 1, 2);
+      }
+  for (int i = i1m1; i <= i2p1; ++i)
+    for (int k = k1m1; k <= k2; ++k)
+      for (int j = j1m1; j <= j2; ++j) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        siv[m] = (x[n] + x[n + ncj] + x[n + nck] + x[n + ncj + nck]) * SN(sn, b, m, 0, 0) +
+                 (y[n] + y[n + ncj] + y[n + nck] + y[n + ncj + nck]) * SN(sn, b, m, 0, 1) +
+                 (z[n] + z[n + ncj] + z[n + nck] + z[n + ncj + nck]) * SN(sn, b, m, 0, 2);
+      }
+  for (int k = k1m1; k <= k2; ++k)
+    for (int j = j1m1; j <= j2; ++j)
+      for (int i = i1m1; i <= i2; ++i) {
+        int64_t n = IC(b, i, j, k), m1 = n - n0;
+        vol[n] = 0.25 * (siv[m1 + nci] - siv[m1] + sjv[m1 + ncj] - sjv[m1] +
+                         skv[m1 + nck] - skv[m1]) / 3.;
+      }
+  free(siv);
+  free(sjv);
+  free(skv);
+}
+
+/* rfsc.f90:26-57: ghost volume of a coincident boundary = partner interior */
+static void rfsc(double *t) {
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    int p = G.bpart[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m)
+      t[G.ncbd[G.bmpb[bb] + m]] = t[G.ncin[G.bmpb[p] + m]];
+  }
+}
+
+/* per boundary entry: inward unit normal of the boundary face (initns.f90:
+ * 63-150: +/- the face area vector of norm.f90, then normalised) and the
+ * centre of the ghost cell (clidd.f90:64-71) */
+static void boundary_geom(const double *x, const double *y, const double *z,
+                          const double *sn) {
+  const double eps = 1.e-10;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    const blk_t *b = &G.b[G.bblk[bb] - 1];
+    const int f = G.bface[bb], dir = f / 2, upper = f % 2;
+    const double is = upper ? -1. : 1.;
+    const int64_t nci = 1, ncj = b->nid, nck = b->nijd;
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m;
+      int64_t face_cell = upper ? G.ncbd[mb] : G.ncin[mb];
+      int64_t mm = face_cell - b->npc;
+      double nx = is * SN(sn, b, mm, dir, 0);
+      double ny = is * SN(sn, b, mm, dir, 1);
+      double nz = is * SN(sn, b, mm, dir, 2);
+      double nn = sqrt(nx * nx + ny * ny + nz * nz);
+      nn = nn + (copysign(1., -fabs(nn)) + 1.) * eps;
+      G.nxn[mb] = nx / nn;
+      G.nyn[mb] = ny / nn;
+      G.nzn[mb] = nz / nn;
+      int64_t n = G.ncbd[mb];
+      G.bym[mb] = 0.125 * (y[n] + y[n + nci] + y[n + ncj] + y[n + nci + ncj] + y[n + nck] +
+                           y[n + nci + nck] + y[n + ncj + nck] + y[n + nci + ncj + nck]);
+      G.bzm[mb] = 0.125 * (z[n] + z[n + nci] + z[n + ncj] + z[n + nci + ncj] + z[n + nck] +
+                           z[n + nci + nck] + z[n + ncj + nck] + z[n + nci + ncj + nck]);
+    }
+  }
+}
+
+/* metric.f90:24-51 -> metrics.f90:52-66 */
+void orc_metric(double *x, double *y, double *z, double *sn, double *vol) {
+  for (int l = 0; l < G.nblk; ++l) {
+    const blk_t *b = &G.b[l];
+    extmhg(b, x, y, z);
+    snorm(b, x, y, z, sn);
+    svol(b, x, y, z, sn, vol);
+  }
+  rfsc(vol);
+  boundary_geom(x, y, z, sn);
+}
+
+void orc_boundary_geom(double *nxn, double *nyn, double *nzn, double *ym,
+                       double *zm) {
+  size_t n = sizeof(double) * (size_t)G.nlist;
+  memcpy(nxn, G.nxn, n);
+  memcpy(nyn, G.nyn, n);
+  memcpy(nzn, G.nzn, n);
+  memcpy(ym, G.bym, n);
+  memcpy(zm, G.bzm, n);
+}
+
+/* ------------------------------------------------------------------------ */
+/* thermodynamics and time step                                             */
+/* ------------------------------------------------------------------------ */
+
+/* zpres.f90:66-79 */
+void orc_zpres(int l, const double *v, double *ps, double *temp, double *cson) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        double rhoe = v[4 * L + n] -
+                      0.5 * (sq(v[L + n]) + sq(v[2 * L + n]) + sq(v[3 * L + n])) / v[n];
+        ps[n] = G.gam1 * (rhoe - G.pinfl);
+        temp[n] = G.gam * ps[n] / v[n];
+        cson[n] = sqrt(temp[n]);
+      }
+}
+
+/* zvismo.f90:77-104 (iflu=1, Sutherland; a = 110.4/tnz is passed in) */
+void orc_zvismo(int l, double *mu, const double *temp) {
+  const blk_t *b = &G.b[l - 1];
+  const double usrey = 1. / G.reynz, a = G.suth_a;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        if (temp[n] <= 0.)
+          mu[n] = 0.;
+        else
+          mu[n] = usrey * temp[n] * sqrt(temp[n]) * (1. + a) / (temp[n] + a);
+      }
+}
+
+/* chronos.f90:110-194 (kprec=0) */
+void orc_chronos(int l, const double *mu, const double *mut, const double *t,
+                 double *dt, const double *sn, const double *vol,
+                 const double *cson) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nci = 1, ncj = b->nid, nck = b->nijd;
+  const int i1 = 1, i2 = b->ni, j1 = 1, j2 = b->nj, k1 = 1, k2 = b->nk;
+  double *sfsi = calloc(b->nnn, sizeof(double));
+  double *sfsj = calloc(b->nnn, sizeof(double));
+  double *sfsk = calloc(b->nnn, sizeof(double));
+  double *dism = calloc(b->nnn, sizeof(double));
+  for (int64_t n = IC(b, i1, j1, k1); n <= IC(b, i2, j2, k2); ++n) dt[n] = 0.;
+  for (int k = k1; k <= k2 - 1; ++k) {
+    for (int j = j1; j <= j2 - 1; ++j)
+      for (int i = i1; i <= i2; ++i) {
+        int64_t m = ML(b, i, j, k);
+        sfsi[m] = SN(sn, b, m, 0, 0) * SN(sn, b, m, 0, 0) +
+                  SN(sn, b, m, 0, 1) * SN(sn, b, m, 0, 1) +
+                  SN(sn, b, m, 0, 2) * SN(sn, b, m, 0, 2);
+      }
+    for (int j = j1; j <= j2; ++j)
+      for (int i = i1; i <= i2 - 1; ++i) {
+        int64_t m = ML(b, i, j, k);
+        sfsj[m] = SN(sn, b, m, 1, 0) * SN(sn, b, m, 1, 0) +
+                  SN(sn, b, m, 1, 1) * SN(sn, b, m, 1, 1) +
+                  SN(sn, b, m, 1, 2) * SN(sn, b, m, 1, 2);
+      }
+  }
+  for (int k = k1; k <= k2; ++k)
+    for (int j = j1; j <= j2 - 1; ++j)
+      for (int i = i1; i <= i2 - 1; ++i) {
+        int64_t m = ML(b, i, j, k);
+        sfsk[m] = SN(sn, b, m, 2, 0) * SN(sn, b, m, 2, 0) +
+                  SN(sn, b, m, 2, 1) * SN(sn, b, m, 2, 1) +
+                  SN(sn, b, m, 2, 2) * SN(sn, b, m, 2, 2);
+      }
+  for (int k = k1; k <= k2 - 1; ++k)
+    for (int j = j1; j <= j2 - 1; ++j)
+      for (int i = i1; i <= i2 - 1; ++i) {
+        int64_t mn = ML(b, i, j, k), nc = n0 + mn;
+        double simax = fmax(sfsi[mn + nci], sfsi[mn]);
+        double sjmax = fmax(sfsj[mn + ncj], sfsj[mn]);
+        double skmax = fmax(sfsk[mn + nck], sfsk[mn]);
+        double smoy = sqrt(simax + sjmax + skmax);
+        dism[mn] = vol[nc] / smoy;
+      }
+  const double etal = G.eta;
+  for (int k = k1; k <= k2 - 1; ++k)
+    for (int j = j1; j <= j2 - 1; ++j)
+      for (int i = i1; i <= i2 - 1; ++i) {
+        int64_t nc = IC(b, i, j, k), mc = nc - n0;
+        double ro = t[nc];
+        double qq = (sq(t[L + nc]) + sq(t[2 * L + nc]) + sq(t[3 * L + nc])) / sq(ro);
+        double q = sqrt(qq);
+        double dte = dism[mc] / (q + cson[nc]);
+        dt[nc] = etal * dte;
+      }
+  if (G.ns) {
+    for (int k = k1; k <= k2 - 1; ++k)
+      for (int j = j1; j <= j2 - 1; ++j)
+        for (int i = i1; i <= i2 - 1; ++i) {
+          int64_t nc = IC(b, i, j, k), mc = nc - n0;
+          double rv1 = G.gam * (mu[nc] / G.pr + mut[nc] / G.prt) / t[nc];
+          double rv = fmax(rv1, 4. / 3. * (mu[nc] + mut[nc]) / t[nc]);
+          double dtv = etal * 0.25 * sq(dism[mc]) / rv;
+          dt[nc] = fmin(dt[nc], dtv);
+        }
+  }
+  free(sfsi);
+  free(sfsj);
+  free(sfsk);
+  free(dism);
+}
+
+/* chrono.f90:113-151 (kdtl=0): dt = min(dt1min, min over real cells); a
+ * value below dt1min stops the reference, here dt is left untouched and the
+ * caller sees the minimum through the return of orc_step */
+void orc_chrono_global(double *dt) {
+  double dtmin = DBL_MAX;
+  for (int l = 0; l < G.nblk; ++l) {
+    const blk_t *b = &G.b[l];
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) dtmin = fmin(dtmin, dt[IC(b, i, j, k)]);
+  }
+  dtmin = fmin(G.dt1min, dtmin);
+  for (int l = 0; l < G.nblk; ++l) {
+    const blk_t *b = &G.b[l];
+    for (int64_t n = b->npc; n < b->npc + b->nnn; ++n) dt[n] = dtmin;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* boundary conditions                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* rbvc.f90:34-92: ghost = 0.5*(own interior + partner interior rotated by the
+ * partner's periodic angle) for every coincident boundary */
+static void rbvc(double *t, double *ps, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  int64_t tot = 0;
+  for (int bb = 0; bb < G.nbnd; ++bb)
+    if (G.btype[bb] == ORC_BC_RC) tot += G.bmmb[bb];
+  if (tot == 0) return;
+  /* pack (buff(:,:,:,1)) */
+  double *buff = malloc(sizeof(double) * 8 * (size_t)G.nlist);
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    const double c = G.bcos[bb], s = G.bsin[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nc = G.ncin[mb];
+      double *bf = &buff[8 * mb];
+      bf[0] = t[nc];
+      bf[1] = t[L + nc];
+      bf[2] = t[2 * L + nc] * c + t[3 * L + nc] * s;
+      bf[3] = t[3 * L + nc] * c - t[2 * L + nc] * s;
+      bf[4] = t[4 * L + nc];
+      bf[5] = ps[nc];
+      bf[6] = temp[nc];
+      bf[7] = cson[nc];
+    }
+  }
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    const int p = G.bpart[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ndm = G.ncin[mb];
+      const double *bf = &buff[8 * (G.bmpb[p] + m)];
+      t[nd] = 0.5 * (t[ndm] + bf[0]);
+      t[L + nd] = 0.5 * (t[L + ndm] + bf[1]);
+      t[2 * L + nd] = 0.5 * (t[2 * L + ndm] + bf[2]);
+      t[3 * L + nd] = 0.5 * (t[3 * L + ndm] + bf[3]);
+      t[4 * L + nd] = 0.5 * (t[4 * L + ndm] + bf[4]);
+      ps[nd] = 0.5 * (ps[ndm] + bf[5]);
+      temp[nd] = 0.5 * (temp[ndm] + bf[6]);
+      cson[nd] = 0.5 * (cson[ndm] + bf[7]);
+    }
+  }
+  free(buff);
+}
+
+/* rbve.f90:21-33 */
+static void rbve(int bb, double *t) {
+  const int64_t L = G.ld;
+  for (int m = 0; m < G.bmmb[bb]; ++m) {
+    int64_t ml = G.bmpb[bb] + m, n = G.ncbd[ml], ni = G.ncin[ml];
+    for (int c = 0; c < 5; ++c) t[c * L + n] = t[c * L + ni];
+  }
+}
+
+/* clextr.f90:23-37 */
+static void clextr(int bb, double *v, double *ps, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  for (int m = 0; m < G.bmmb[bb]; ++m) {
+    int64_t mb = G.bmpb[bb] + m, nl = G.ncbd[mb], ni = G.ncin[mb];
+    for (int c = 0; c < 5; ++c) v[c * L + nl] = v[c * L + ni];
+    ps[nl] = ps[ni];
+    temp[nl] = temp[ni];
+    cson[nl] = cson[ni];
+  }
+}
+
+/* clpara.f90:24-40: adiabatic wall, ghost at rest with the interior rho e */
+static void clpara(int bb, double *v, double *ps, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  for (int m = 0; m < G.bmmb[bb]; ++m) {
+    int64_t mb = G.bmpb[bb] + m, nc = G.ncbd[mb], ni = G.ncin[mb];
+    double rhoe1 = v[4 * L + ni] -
+                   0.5 * (sq(v[L + ni]) + sq(v[2 * L + ni]) + sq(v[3 * L + ni])) / v[ni];
+    v[nc] = v[ni];
+    v[L + nc] = 0.;
+    v[2 * L + nc] = 0.;
+    v[3 * L + nc] = 0.;
+    v[4 * L + nc] = rhoe1;
+    ps[nc] = ps[ni];
+    temp[nc] = temp[ni];
+    cson[nc] = cson[ni];
+  }
+}
+
+/* utidd.f90 + clidd.f90:50-170: subsonic injection at imposed total pressure,
+ * total temperature and flow direction (Newton on the normal velocity, at
+ * most 20 sweeps, the stop test is the maximum over the whole boundary) */
+static void clidd(int bb, double *v, double *ps_, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  const int mt = G.bmmb[bb];
+  const int64_t m0 = G.bmpb[bb];
+  const double eps = 0.0000001;
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl, omg = G.omg;
+  const double gam6 = gam / gam1;
+  const double gamt = gam / sq(G.aa1);
+  const double gam2t = 0.5 * gam1 / sq(G.aa1);
+  double *usdn = malloc(sizeof(double) * mt), *usdn2 = malloc(sizeof(double) * mt);
+  double *un = malloc(sizeof(double) * mt), *qn = malloc(sizeof(double) * mt);
+  double *roc0 = malloc(sizeof(double) * mt), *am0 = malloc(sizeof(double) * mt);
+  for (int m = 0; m < mt; ++m) {
+    int64_t mb = m0 + m, nc = G.ncbd[mb];
+    const double *bc = &G.bceqt[mb];
+    double d0x = bc[G.nlist * 2], d0y = bc[G.nlist * 3], d0z = bc[G.nlist * 4];
+    double nx = G.nxn[mb], ny = G.nyn[mb], nz = G.nzn[mb];
+    double ym = G.bym[mb], zm = G.bzm[mb];
+    usdn[m] = 1. / (d0x * nx + d0y * ny + d0z * nz);
+    usdn2[m] = sq(usdn[m]);
+    un[m] = omg * (ym * nz - zm * ny);
+    double qxs = v[L + nc] / v[nc], qys = v[2 * L + nc] / v[nc], qzs = v[3 * L + nc] / v[nc];
+    qn[m] = qxs * nx + qys * ny + qzs * nz;
+    double ps = gam1 * (v[4 * L + nc] -
+                        0.5 * (qxs * v[L + nc] + qys * v[2 * L + nc] + qzs * v[3 * L + nc]) - pinfl);
+    roc0[m] = -sqrt(gam * ps * v[nc]);
+    am0[m] = ps + roc0[m] * qn[m];
+  }
+  int nitn = 0;
+  double residu = 1.;
+  while (residu > eps && nitn < 20) {
+    residu = 0.;
+    for (int m = 0; m < mt; ++m) {
+      int64_t mb = m0 + m;
+      double rpi = G.bceqt[mb], rti = G.bceqt[G.nlist + mb];
+      double b = 1. / (1. + gam2t / rti * usdn2[m] * sq(qn[m] + un[m]));
+      double p = G.pa1 * rpi * pow(b, gam6);
+      double ro = gamt * p / (b * rti);
+      double f = p + roc0[m] * qn[m] - am0[m];
+      double df = roc0[m] - ro * (qn[m] + un[m]) * usdn2[m];
+      double dqn = -f / df;
+      double resi = fabs(dqn) / qn[m];
+      qn[m] = qn[m] + dqn;
+      residu = fmax(residu, resi);
+    }
+    nitn = nitn + 1;
+  }
+  for (int m = 0; m < mt; ++m) {
+    int64_t mb = m0 + m, nc = G.ncbd[mb];
+    double rpi = G.bceqt[mb], rti = G.bceqt[G.nlist + mb];
+    double d0x = G.bceqt[G.nlist * 2 + mb], d0y = G.bceqt[G.nlist * 3 + mb],
+           d0z = G.bceqt[G.nlist * 4 + mb];
+    double ym = G.bym[mb], zm = G.bzm[mb];
+    double b = 1. / (1. + gam2t / rti * usdn2[m] * sq(qn[m] + un[m]));
+    double p = G.pa1 * rpi * pow(b, gam6);
+    double ro = gamt * p / (b * rti);
+    double wn = qn[m] + un[m];
+    double w = wn * usdn[m];
+    v[nc] = ro;
+    v[L + nc] = ro * (w * d0x);
+    v[2 * L + nc] = ro * (w * d0y + zm * omg);
+    v[3 * L + nc] = ro * (w * d0z - ym * omg);
+    v[4 * L + nc] = p / gam1 + pinfl +
+                    0.5 * (sq(v[L + nc]) + sq(v[2 * L + nc]) + sq(v[3 * L + nc])) / ro;
+    ps_[nc] = p;
+    temp[nc] = gam * p / ro;
+    cson[nc] = sqrt(temp[nc]);
+  }
+  free(usdn);
+  free(usdn2);
+  free(un);
+  free(qn);
+  free(roc0);
+  free(am0);
+}
+
+/* utprd.f90 + clprd.f90:31-59: imposed static pressure, compatibility
+ * relation along the inward normal */
+static void clprd(int bb, double *v, double *ps_, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  for (int m = 0; m < G.bmmb[bb]; ++m) {
+    int64_t mb = G.bmpb[bb] + m, nl = G.ncbd[mb];
+    double pres = G.bceqt[mb];
+    double rho = v[nl];
+    double qxs = v[L + nl] / v[nl], qys = v[2 * L + nl] / v[nl], qzs = v[3 * L + nl] / v[nl];
+    double ps = gam1 * (v[4 * L + nl] - 0.5 * rho * (sq(qxs) + sq(qys) + sq(qzs)) - pinfl);
+    double cs2 = gam * ps / rho;
+    double roc0 = sqrt(gam * ps * rho);
+    double dqn = (pres - ps) / roc0;
+    double qx = qxs + dqn * G.nxn[mb];
+    double qy = qys + dqn * G.nyn[mb];
+    double qz = qzs + dqn * G.nzn[mb];
+    double drho = (pres - ps) / cs2;
+    v[nl] = v[nl] + drho;
+    v[L + nl] = v[nl] * qx;
+    v[2 * L + nl] = v[nl] * qy;
+    v[3 * L + nl] = v[nl] * qz;
+    v[4 * L + nl] = pres / gam1 + pinfl + 0.5 * v[nl] * (sq(qx) + sq(qy) + sq(qz));
+    ps_[nl] = pres;
+    temp[nl] = gam * ps_[nl] / v[nl];
+    cson[nl] = sqrt(temp[nl]);
+  }
+}
+
+/* rbord.f90:137-429: coincident halo, physical conditions, coincident halo */
+void orc_rbord(double *v, double *ps, double *temp, double *cson) {
+  rbvc(v, ps, temp, cson);
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    switch (G.btype[bb]) {
+      case ORC_BC_EXTR: clextr(bb, v, ps, temp, cson); break;
+      case ORC_BC_PARA: clpara(bb, v, ps, temp, cson); break;
+      case ORC_BC_IDD:
+        rbve(bb, v);
+        clidd(bb, v, ps, temp, cson);
+        break;
+      case ORC_BC_PRD:
+        rbve(bb, v);
+        clprd(bb, v, ps, temp, cson);
+        break;
+      default: break;
+    }
+  }
+  rbvc(v, ps, temp, cson);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Roe flux                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Roe dissipation |A|dW and the convective part of the face flux
+ * (sch_roe_euler.f90:284-422, sch_roe.f90:326-461).  W = rho,u,v,w,p. */
+static void roe_core(const double *WL, const double *WR, double sx, double sy,
+                     double sz, int absam, double di[5], double *el_,
+                     double *er_) {
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  double cnds = sqrt(sx * sx + sy * sy + sz * sz);
+  double nx = sx / cnds, ny = sy / cnds, nz = sz / cnds;
+  double al = sqrt(gam * pl / rhol);
+  double ar = sqrt(gam * prr / rhor);
+  double q2l = sq(ul) + sq(vl) + sq(wl);
+  double q2r = sq(ur) + sq(vr) + sq(wr);
+  double hl = al * al / gam1 + 0.5 * q2l;
+  double hr = ar * ar / gam1 + 0.5 * q2r;
+  double el = pl / (gam1 * rhol) + 0.5 * q2l + pinfl / rhol;
+  double er = prr / (gam1 * rhor) + 0.5 * q2r + pinfl / rhor;
+  double gd = sqrt(rhor / rhol);
+  double gd1 = 1. / (1. + gd);
+  double gd2 = gd * gd1;
+  double rhom = sqrt(rhol * rhor);
+  double rhomi = 1. / rhom;
+  double um = gd1 * ul + gd2 * ur;
+  double vm = gd1 * vl + gd2 * vr;
+  double wm = gd1 * wl + gd2 * wr;
+  double hm = gd1 * hl + gd2 * hr;
+  double vitm2 = 0.5 * (sq(um) + sq(vm) + sq(wm));
+  double am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
+  double am2i = 1. / (am * am);
+  double vn = um * nx + vm * ny + wm * nz;
+  double rhoiam = rhom / am;
+  double rhoami = am2i / rhoiam;
+  double lam[5];
+  lam[0] = fabs(vn * cnds);
+  lam[1] = lam[0];
+  lam[2] = lam[0];
+  lam[3] = fabs(vn * cnds + am * cnds);
+  lam[4] = fabs(vn * cnds - am * cnds);
+  double q[5][5], p[5][5];
+  q[0][0] = (1. - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi;
+  q[0][1] = gam1 * um * nx * am2i;
+  q[0][2] = gam1 * vm * nx * am2i + nz * rhomi;
+  q[0][3] = gam1 * wm * nx * am2i - ny * rhomi;
+  q[0][4] = -gam1 * nx * am2i;
+  q[1][0] = (1. - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi;
+  q[1][1] = gam1 * um * ny * am2i - nz * rhomi;
+  q[1][2] = gam1 * vm * ny * am2i;
+  q[1][3] = gam1 * wm * ny * am2i + nx * rhomi;
+  q[1][4] = -gam1 * ny * am2i;
+  q[2][0] = (1. - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi;
+  q[2][1] = gam1 * um * nz * am2i + ny * rhomi;
+  q[2][2] = gam1 * vm * nz * am2i - nx * rhomi;
+  q[2][3] = gam1 * wm * nz * am2i;
+  q[2][4] = -gam1 * nz * am2i;
+  q[3][0] = gam1 * vitm2 * rhoami - vn * rhomi;
+  q[3][1] = nx * rhomi - gam1 * um * rhoami;
+  q[3][2] = ny * rhomi - gam1 * vm * rhoami;
+  q[3][3] = nz * rhomi - gam1 * wm * rhoami;
+  q[3][4] = gam1 * rhoami;
+  q[4][0] = gam1 * vitm2 * rhoami + vn * rhomi;
+  q[4][1] = -nx * rhomi - gam1 * um * rhoami;
+  q[4][2] = -ny * rhomi - gam1 * vm * rhoami;
+  q[4][3] = -nz * rhomi - gam1 * wm * rhoami;
+  q[4][4] = gam1 * rhoami;
+  p[0][0] = nx;
+  p[0][1] = ny;
+  p[0][2] = nz;
+  p[0][3] = 0.5 * rhoiam;
+  p[0][4] = 0.5 * rhoiam;
+  p[1][0] = um * nx;
+  p[1][1] = um * ny - rhom * nz;
+  p[1][2] = um * nz + rhom * ny;
+  p[1][3] = 0.5 * rhoiam * (um + nx * am);
+  p[1][4] = 0.5 * rhoiam * (um - nx * am);
+  p[2][0] = vm * nx + rhom * nz;
+  p[2][1] = vm * ny;
+  p[2][2] = vm * nz - rhom * nx;
+  p[2][3] = 0.5 * rhoiam * (vm + ny * am);
+  p[2][4] = 0.5 * rhoiam * (vm - ny * am);
+  p[3][0] = wm * nx - rhom * ny;
+  p[3][1] = wm * ny + rhom * nx;
+  p[3][2] = wm * nz;
+  p[3][3] = 0.5 * rhoiam * (wm + nz * am);
+  p[3][4] = 0.5 * rhoiam * (wm - nz * am);
+  p[4][0] = vitm2 * nx + rhom * (vm * nz - wm * ny);
+  p[4][1] = vitm2 * ny + rhom * (wm * nx - um * nz);
+  p[4][2] = vitm2 * nz + rhom * (um * ny - vm * nx);
+  p[4][3] = 0.5 * rhoiam * (hm + am * vn);
+  p[4][4] = 0.5 * rhoiam * (hm - am * vn);
+  double dw[5];
+  dw[0] = rhor - rhol;
+  dw[1] = rhor * ur - rhol * ul;
+  dw[2] = rhor * vr - rhol * vl;
+  dw[3] = rhor * wr - rhol * wl;
+  dw[4] = rhor * er - rhol * el;
+  for (int r = 0; r < 5; ++r) {
+    double acc = 0.;
+    for (int c = 0; c < 5; ++c) {
+      double a = p[r][0] * lam[0] * q[0][c];
+      for (int kk = 1; kk < 5; ++kk) a = a + p[r][kk] * lam[kk] * q[kk][c];
+      acc = (c == 0) ? a * dw[0] : acc + a * dw[c];
+    }
+    di[r] = acc;
+  }
+  *el_ = el;
+  *er_ = er;
+}
+
+/* primitive extrapolation with the kappa-MUSCL formula, no limiter
+ * (sch_roe_euler.f90:245-273).  vv: rho,rhou,rhov,rhow,rhoE columns at cells
+ * n-2,n-1,n,n+1 (index 0..3), pp: pressure at the same cells */
+static void muscl_plain(const double vv[4][5], const double pp[4], double WL[5],
+                        double WR[5]) {
+  const double c = 0.25 * G.muscl, xk = G.xk;
+  double uu[4][3];
+  for (int s = 0; s < 4; ++s)
+    for (int a = 0; a < 3; ++a) uu[s][a] = vv[s][a + 1] / vv[s][0];
+  WL[0] = vv[1][0] + c * ((1. - xk) * (vv[1][0] - vv[0][0]) + (1. + xk) * (vv[2][0] - vv[1][0]));
+  for (int a = 0; a < 3; ++a)
+    WL[1 + a] = uu[1][a] + c * ((1. - xk) * (uu[1][a] - uu[0][a]) + (1. + xk) * (uu[2][a] - uu[1][a]));
+  WL[4] = pp[1] + c * ((1. - xk) * (pp[1] - pp[0]) + (1. + xk) * (pp[2] - pp[1]));
+  WR[0] = vv[2][0] - c * ((1. + xk) * (vv[2][0] - vv[1][0]) + (1. - xk) * (vv[3][0] - vv[2][0]));
+  for (int a = 0; a < 3; ++a)
+    WR[1 + a] = uu[2][a] - c * ((1. + xk) * (uu[2][a] - uu[1][a]) + (1. - xk) * (uu[3][a] - uu[2][a]));
+  WR[4] = pp[2] - c * ((1. + xk) * (pp[2] - pp[1]) + (1. - xk) * (pp[3] - pp[2]));
+}
+
+/* minmod limiter of sch_roe.f90:1500-1504 */
+static inline double phi(double a) {
+  double m = (a < 1.) ? a : 1.;
+  return (m > 0.) ? m : 0.;
+}
+
+/* limited extrapolation of sch_roe.f90:196-227 given the slope ratios at the
+ * face (rm) and at the next face (rp) for the five primitive variables */
+static void muscl_limited(const double vv[4][5], const double pp[4],
+                          const double rm[5], const double rp[5], double WL[5],
+                          double WR[5]) {
+  const double c = 0.25 * G.muscl, xk = G.xk;
+  double uu[4][3];
+  for (int s = 0; s < 4; ++s)
+    for (int a = 0; a < 3; ++a) uu[s][a] = vv[s][a + 1] / vv[s][0];
+  WL[0] = vv[1][0] + c * phi(rm[0]) * (1. - xk) * (vv[1][0] - vv[0][0]) +
+          c * phi(1. / rm[0]) * (1. + xk) * (vv[2][0] - vv[1][0]);
+  for (int a = 0; a < 3; ++a)
+    WL[1 + a] = uu[1][a] + c * phi(rm[1 + a]) * (1. - xk) * (uu[1][a] - uu[0][a]) +
+                (1. + xk) * (uu[2][a] - uu[1][a]) * 0.25 * G.muscl * phi(1. / rm[1 + a]);
+  WL[4] = pp[1] + c * phi(rm[4]) * (1. - xk) * (pp[1] - pp[0]) +
+          c * phi(1. / rm[4]) * (1. + xk) * (pp[2] - pp[1]);
+  WR[0] = vv[2][0] - c * phi(rp[0]) * (1. + xk) * (vv[2][0] - vv[1][0]) -
+          c * phi(1. / rp[0]) * (1. - xk) * (vv[3][0] - vv[2][0]);
+  for (int a = 0; a < 3; ++a)
+    WR[1 + a] = uu[2][a] - c * phi(rp[1 + a]) * (1. + xk) * (uu[2][a] - uu[1][a]) -
+                (1. - xk) * (uu[3][a] - uu[2][a]) * 0.25 * G.muscl * phi(1. / rp[1 + a]);
+  WR[4] = pp[2] - c * phi(rp[4]) * (1. + xk) * (pp[2] - pp[1]) -
+          c * phi(1. / rp[4]) * (1. - xk) * (pp[3] - pp[2]);
+}
+
+/* interior face flux f1..f5 (before the 0.5) of sch_roe_euler.f90:403-422 and
+ * sch_roe.f90:437-461 (tau = NULL for the Euler form) */
+static void face_flux(const double WL[5], const double WR[5], double sx,
+                      double sy, double sz, int absam, const double *tau,
+                      int64_t L, int64_t nR, int64_t nL, double f[5]) {
+  const double pinfl = G.pinfl;
+  double di[5], el, er;
+  roe_core(WL, WR, sx, sy, sz, absam, di, &el, &er);
+  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  double dfxx, dfxy, dfxz, dfyy, dfyz, dfzz, dfex, dfey, dfez;
+  if (!tau) {
+    dfxx = rhor * sq(ur) + prr - pinfl + rhol * sq(ul) + pl - pinfl;
+    dfxy = rhor * ur * vr + rhol * ul * vl;
+    dfxz = rhor * ur * wr + rhol * ul * wl;
+    dfyy = rhor * sq(vr) + prr - pinfl + rhol * sq(vl) + pl - pinfl;
+    dfyz = rhor * vr * wr + rhol * vl * wl;
+    dfzz = rhor * sq(wr) + prr - pinfl + rhol * sq(wl) + pl - pinfl;
+    dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul;
+    dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl;
+    dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl;
+  } else {
+    const double *txx = tau, *txy = tau + L, *txz = tau + 2 * L, *tyy = tau + 3 * L,
+                 *tyz = tau + 4 * L, *tzz = tau + 5 * L, *qx = tau + 6 * L,
+                 *qy = tau + 7 * L, *qz = tau + 8 * L;
+    dfxx = rhor * sq(ur) + prr - pinfl - txx[nR] + rhol * sq(ul) + pl - pinfl - txx[nL];
+    dfxy = rhor * ur * vr - txy[nR] + rhol * ul * vl - txy[nL];
+    dfxz = rhor * ur * wr - txz[nR] + rhol * ul * wl - txz[nL];
+    dfyy = rhor * sq(vr) + prr - pinfl - tyy[nR] + rhol * sq(vl) + pl - pinfl - tyy[nL];
+    dfyz = rhor * vr * wr - tyz[nR] + rhol * vl * wl - tyz[nL];
+    dfzz = rhor * sq(wr) + prr - pinfl - tzz[nR] + rhol * sq(wl) + pl - pinfl - tzz[nL];
+    dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul -
+           (txx[nR] * ur + txy[nR] * vr + txz[nR] * wr) -
+           (txx[nL] * ul + txy[nL] * vl + txz[nL] * wl) - qx[nR] - qx[nL];
+    dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl -
+           (txy[nR] * ur + tyy[nR] * vr + tyz[nR] * wr) -
+           (txy[nL] * ul + tyy[nL] * vl + tyz[nL] * wl) - qy[nR] - qy[nL];
+    dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl -
+           (txz[nR] * ur + tyz[nR] * vr + tzz[nR] * wr) -
+           (txz[nL] * ul + tyz[nL] * vl + tzz[nL] * wl) - qz[nR] - qz[nL];
+  }
+  f[0] = (rhor * ur + rhol * ul) * sx + (rhor * vr + rhol * vl) * sy +
+         (rhor * wr + rhol * wl) * sz - di[0];
+  f[1] = dfxx * sx + dfxy * sy + dfxz * sz - di[1];
+  f[2] = dfxy * sx + dfyy * sy + dfyz * sz - di[2];
+  f[3] = dfxz * sx + dfyz * sy + dfzz * sz - di[3];
+  f[4] = dfex * sx + dfey * sy + dfez * sz - di[4];
+}
+
+/* physical flux of a ghost cell through a boundary face (sch_roe_euler.f90:
+ * 438-513, sch_roe.f90:497-580).  ng: ghost cell; nrho: the cell whose
+ * density divides the energy flux (the ghost, except the j/k lower faces of
+ * sch_roe_euler, which use the interior cell: sch_roe_euler.f90:630-632). */
+static void bnd_flux(const double *v, const double *ps, const double *tau,
+                     int64_t L, int64_t ng, int64_t nrho, double sx, double sy,
+                     double sz, double s[5]) {
+  const double pinfl = G.pinfl;
+  const double v1 = v[ng], v2 = v[L + ng], v3 = v[2 * L + ng], v4 = v[3 * L + ng],
+               v5 = v[4 * L + ng], p = ps[ng];
+  double fxx, fxy, fxz, fyy, fyz, fzz, fex, fey, fez;
+  if (!tau) {
+    fxx = v2 * (v2 / v1) + p - pinfl;
+    fxy = v3 * (v2 / v1);
+    fxz = v4 * (v2 / v1);
+    fyy = v3 * (v3 / v1) + p - pinfl;
+    fyz = v4 * (v3 / v1);
+    fzz = v4 * (v4 / v1) + p - pinfl;
+    fex = (v5 + p - pinfl) * v2 / v[nrho];
+    fey = (v5 + p - pinfl) * v3 / v[nrho];
+    fez = (v5 + p - pinfl) * v4 / v[nrho];
+  } else {
+    const double txx = tau[ng], txy = tau[L + ng], txz = tau[2 * L + ng],
+                 tyy = tau[3 * L + ng], tyz = tau[4 * L + ng], tzz = tau[5 * L + ng],
+                 qx = tau[6 * L + ng], qy = tau[7 * L + ng], qz = tau[8 * L + ng];
+    fxx = v2 * (v2 / v1) + p - pinfl - txx;
+    fxy = v3 * (v2 / v1) - txy;
+    fxz = v4 * (v2 / v1) - txz;
+    fyy = v3 * (v3 / v1) + p - pinfl - tyy;
+    fyz = v4 * (v3 / v1) - tyz;
+    fzz = v4 * (v4 / v1) + p - pinfl - tzz;
+    fex = ((v5 + p - pinfl - txx) * v2 - txy * v3 - txz * v4) / v1 - qx;
+    fey = ((v5 + p - pinfl - tyy) * v3 - txy * v2 - tyz * v4) / v1 - qy;
+    fez = ((v5 + p - pinfl - tzz) * v4 - txz * v2 - tyz * v3) / v1 - qz;
+  }
+  s[0] = v2 * sx + v3 * sy + v4 * sz;
+  s[1] = fxx * sx + fxy * sy + fxz * sz;
+  s[2] = fxy * sx + fyy * sy + fyz * sz;
+  s[3] = fxz * sx + fyz * sy + fzz * sz;
+  s[4] = fex * sx + fey * sy + fez * sz;
+}
+
+static void gather_cells(const double *v, const double *ps, int64_t L,
+                         int64_t n, int64_t ninc, double vv[4][5], double pp[4]) {
+  for (int s = 0; s < 4; ++s) {
+    int64_t c = n + (s - 2) * ninc;
+    for (int a = 0; a < 5; ++a) vv[s][a] = v[a * L + c];
+    pp[s] = ps[c];
+  }
+}
+
+/* ranges of the (k,j,i) loop nest of one direction: real cells on the
+ * tangential axes, [flo, fhi] on the face axis */
+static void dir_ranges(const blk_t *b, int dir, int flo, int fhi, int lo[3],
+                       int hi[3]) {
+  lo[0] = 1; hi[0] = b->ni - 1;
+  lo[1] = 1; hi[1] = b->nj - 1;
+  lo[2] = 1; hi[2] = b->nk - 1;
+  lo[dir] = flo;
+  hi[dir] = fhi;
+}
+
+/* one direction of sch_roe_euler / sch_roe: interior faces (optionally with
+ * the in-place limiter recurrence), then lower and upper boundary faces */
+static void roe_direction(const blk_t *b, int dir, int ns, double *u,
+                          const double *v, const double *tau, const double *sn,
+                          const double *ps) {
+  const int64_t L = G.ld, n0 = b->npc, ninc = NINC(b, dir);
+  const int nd = NDIR(b, dir); /* node count along dir: faces 1..nd */
+  const int absam = (!ns) && dir > 0;
+  int lo[3], hi[3], idx[3];
+  double *r = NULL;
+  const int limited = ns && G.ilim == 1;
+  if (limited) {
+    r = calloc((size_t)5 * b->nnn, sizeof(double));
+    /* slope differences at faces 1..nd (sch_roe.f90:146-159) */
+    dir_ranges(b, dir, 1, nd, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          r[m] = v[n] - v[n - ninc];
+          r[b->nnn + m] = v[L + n] / v[n] - v[L + n - ninc] / v[n - ninc];
+          r[2 * b->nnn + m] = v[2 * L + n] / v[n] - v[2 * L + n - ninc] / v[n - ninc];
+          r[3 * b->nnn + m] = v[3 * L + n] / v[n] - v[3 * L + n - ninc] / v[n - ninc];
+          r[4 * b->nnn + m] = ps[n] - ps[n - ninc];
+        }
+    /* in-place ratio recurrence along each line (sch_roe.f90:161-194) */
+    dir_ranges(b, dir, 2, nd - 1, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t m = ML(b, idx[0], idx[1], idx[2]);
+          for (int a = 0; a < 5; ++a) {
+            double *ra = r + (int64_t)a * b->nnn;
+            if (fabs(ra[m - ninc] * ra[m] * ra[m + ninc]) <= DBL_MIN)
+              ra[m] = 1.;
+            else
+              ra[m] = ra[m] / ra[m - ninc];
+          }
+        }
+  }
+  /* interior faces 2..nd-1 */
+  dir_ranges(b, dir, 2, nd - 1, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double vv[4][5], pp[4], WL[5], WR[5], f[5];
+        gather_cells(v, ps, L, n, ninc, vv, pp);
+        if (limited && idx[dir] <= nd - 2) {
+          double rm[5], rp[5];
+          for (int a = 0; a < 5; ++a) {
+            rm[a] = r[(int64_t)a * b->nnn + m];
+            rp[a] = r[(int64_t)a * b->nnn + m + ninc];
+          }
+          muscl_limited(vv, pp, rm, rp, WL, WR);
+        } else {
+          muscl_plain(vv, pp, WL, WR);
+        }
+        face_flux(WL, WR, SN(sn, b, m, dir, 0), SN(sn, b, m, dir, 1),
+                  SN(sn, b, m, dir, 2), absam, ns ? tau : NULL, L, n, n - ninc, f);
+        for (int a = 0; a < 5; ++a) {
+          u[a * L + n] = u[a * L + n] - 0.5 * f[a];
+          u[a * L + n - ninc] = u[a * L + n - ninc] + 0.5 * f[a];
+        }
+      }
+  /* lower boundary face 1 */
+  dir_ranges(b, dir, 1, 1, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double s[5];
+        int64_t nrho = (!ns && dir > 0) ? n : n - ninc;
+        bnd_flux(v, ps, ns ? tau : NULL, L, n - ninc, nrho, SN(sn, b, m, dir, 0),
+                 SN(sn, b, m, dir, 1), SN(sn, b, m, dir, 2), s);
+        for (int a = 0; a < 5; ++a) u[a * L + n] = u[a * L + n] - s[a];
+      }
+  /* upper boundary face nd */
+  dir_ranges(b, dir, nd, nd, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double s[5];
+        bnd_flux(v, ps, ns ? tau : NULL, L, n, n, SN(sn, b, m, dir, 0),
+                 SN(sn, b, m, dir, 1), SN(sn, b, m, dir, 2), s);
+        for (int a = 0; a < 5; ++a) u[a * L + n - ninc] = u[a * L + n - ninc] + s[a];
+      }
+  free(r);
+}
+
+static void zero_u(const blk_t *b, double *u) {
+  for (int a = 0; a < 5; ++a)
+    for (int64_t n = b->npc; n < b->npc + b->nnn; ++n) u[a * G.ld + n] = 0.;
+}
+
+/* sch_roe_euler.f90:205-1000 (ityprk=0, 3-D) */
+void orc_sch_roe_euler(int l, double *u, const double *v, const double *sn,
+                       const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) roe_direction(b, dir, 0, u, v, NULL, sn, ps);
+}
+
+/* sch_roe.f90:102-1462 (ityprk=0, 3-D) */
+void orc_sch_roe(int l, double *u, const double *v, const double *tau,
+                 const double *sn, const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) roe_direction(b, dir, 1, u, v, tau, sn, ps);
+}
+
+/* ------------------------------------------------------------------------ */
+/* viscous stresses                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* zgrad2.f90:62-497 with unit weights (inivec.f90:110; metric3 only runs for
+ * the weighted schemes, cpfw.f90:235) then zfluto.f90:38-57 */
+static void zgrad2_zfluto(const blk_t *b, const double *s, const double *mu,
+                          const double *mut, double *tau, const double *sn,
+                          const double *vol, const double *temp) {
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  double *vx = calloc(nnn, sizeof(double)), *vy = calloc(nnn, sizeof(double)),
+         *vz = calloc(nnn, sizeof(double));
+  double *g = calloc((size_t)12 * nnn, sizeof(double)); /* dvxx..dvzz, dtx..dtz */
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 0; j <= b->nj; ++j)
+      for (int i = 0; i <= b->ni; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        vx[m] = s[L + n] / s[n];
+        vy[m] = s[2 * L + n] / s[n];
+        vz[m] = s[3 * L + n] / s[n];
+      }
+  /* component order in g: xx,xy,xz,yx,yy,yz,zx,zy,zz,tx,ty,tz */
+  const int order[3] = {2, 1, 0}; /* k faces, then j, then i */
+  for (int oi = 0; oi < 3; ++oi) {
+    const int dir = order[oi];
+    const int64_t ninc = NINC(b, dir);
+    const int nd = NDIR(b, dir);
+    int lo[3], hi[3], idx[3];
+    dir_ranges(b, dir, 2, nd - 1, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          double sv[3] = {SN(sn, b, m, dir, 0), SN(sn, b, m, dir, 1), SN(sn, b, m, dir, 2)};
+          double fv[4] = {vx[m] + vx[m - ninc], vy[m] + vy[m - ninc],
+                          vz[m] + vz[m - ninc], temp[n] + temp[n - ninc]};
+          for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 3; ++c) {
+              double sk = fv[a] * sv[c];
+              g[(3 * a + c) * nnn + m] = g[(3 * a + c) * nnn + m] - sk;
+              g[(3 * a + c) * nnn + m - ninc] = g[(3 * a + c) * nnn + m - ninc] + sk;
+            }
+        }
+    dir_ranges(b, dir, 1, 1, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          double fv[4] = {vx[m - ninc], vy[m - ninc], vz[m - ninc], temp[n - ninc]};
+          for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 3; ++c)
+              g[(3 * a + c) * nnn + m] =
+                  g[(3 * a + c) * nnn + m] - SN(sn, b, m, dir, c) * 2 * fv[a];
+        }
+    dir_ranges(b, dir, nd, nd, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          double fv[4] = {vx[m], vy[m], vz[m], temp[n]};
+          for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 3; ++c)
+              g[(3 * a + c) * nnn + m - ninc] =
+                  g[(3 * a + c) * nnn + m - ninc] + SN(sn, b, m, dir, c) * 2 * fv[a];
+        }
+  }
+  const double eps = 0.00001, ds3 = 2. / 3.;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        double ts = copysign(0.5, -vol[n]);
+        double vols = (0.5 + ts) * eps + (0.5 - ts) * vol[n];
+        double c0 = .5 / (vols + DBL_MIN);
+        double gg[12];
+        for (int a = 0; a < 12; ++a) gg[a] = g[a * nnn + m] * c0;
+        const double dvxx = gg[0], dvxy = gg[1], dvxz = gg[2], dvyx = gg[3],
+                     dvyy = gg[4], dvyz = gg[5], dvzx = gg[6], dvzy = gg[7],
+                     dvzz = gg[8], dtx = gg[9], dty = gg[10], dtz = gg[11];
+        double mm = mu[n] + mut[n];
+        tau[n] = ds3 * (mu[n] + mut[n]) * (2 * dvxx - dvyy - dvzz);
+        tau[3 * L + n] = ds3 * (mu[n] + mut[n]) * (2 * dvyy - dvxx - dvzz);
+        tau[5 * L + n] = ds3 * (mu[n] + mut[n]) * (2 * dvzz - dvxx - dvyy);
+        tau[L + n] = mm * (dvxy + dvyx);
+        tau[2 * L + n] = mm * (dvxz + dvzx);
+        tau[4 * L + n] = mm * (dvyz + dvzy);
+        double kq = G.cp * (mu[n] / G.pr + mut[n] / G.prt);
+        tau[6 * L + n] = kq * dtx;
+        tau[7 * L + n] = kq * dty;
+        tau[8 * L + n] = kq * dtz;
+      }
+  free(vx);
+  free(vy);
+  free(vz);
+  free(g);
+}
+
+/* zvisqc.f90:134-205: gradients + stresses per block, then ghost values:
+ * rbte.f90 (copy of the interior cell) on every non-coincident boundary and
+ * rbtc.f90:30-100 (average with the rotated partner) on coincident ones */
+void orc_zvisqc(const double *v, const double *mu, const double *mut,
+                double *tau, const double *sn, const double *vol,
+                const double *temp) {
+  const int64_t L = G.ld;
+  for (int l = 0; l < G.nblk; ++l)
+    zgrad2_zfluto(&G.b[l], v, mu, mut, tau, sn, vol, temp);
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] == ORC_BC_RC) continue;
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ndm = G.ncin[mb];
+      for (int a = 0; a < 9; ++a) tau[a * L + nd] = tau[a * L + ndm];
+    }
+  }
+  double *buff = malloc(sizeof(double) * 9 * (size_t)(G.nlist > 0 ? G.nlist : 1));
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    const double sr = -G.bsin[bb], cr = G.bcos[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nc = G.ncin[mb];
+      double *bf = &buff[9 * mb];
+      const double txx = tau[nc], txy = tau[L + nc], txz = tau[2 * L + nc],
+                   tyy = tau[3 * L + nc], tyz = tau[4 * L + nc], tzz = tau[5 * L + nc];
+      bf[0] = txx;
+      bf[1] = cr * txy - sr * txz;
+      bf[2] = cr * txz + sr * txy;
+      bf[3] = cr * cr * tyy - 2. * cr * sr * tyz + sr * sr * tzz;
+      bf[4] = -cr * sr * (tzz - tyy) + (2. * cr * cr - 1.) * tyz;
+      bf[5] = sr * sr * tyy + 2. * cr * sr * tyz + cr * cr * tzz;
+      bf[6] = tau[6 * L + nc];
+      bf[7] = cr * tau[7 * L + nc] - sr * tau[8 * L + nc];
+      bf[8] = cr * tau[8 * L + nc] + sr * tau[7 * L + nc];
+    }
+  }
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    const int p = G.bpart[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ndm = G.ncin[mb];
+      const double *bf = &buff[9 * (G.bmpb[p] + m)];
+      for (int a = 0; a < 9; ++a) tau[a * L + nd] = 0.5 * (tau[a * L + ndm] + bf[a]);
+    }
+  }
+  free(buff);
+}
+
+/* ------------------------------------------------------------------------ */
+/* implicit phase                                                            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  double *coefe[3], *coefdiag, *d2w[5], *df[9], *rv;
+} impl_work;
+
+static void impl_alloc(const blk_t *b, impl_work *w) {
+  for (int a = 0; a < 3; ++a) w->coefe[a] = calloc(b->nnn, sizeof(double));
+  w->coefdiag = calloc(b->nnn, sizeof(double));
+  for (int a = 0; a < 5; ++a) w->d2w[a] = calloc(b->nnn, sizeof(double));
+  for (int a = 0; a < 9; ++a) w->df[a] = calloc(b->nnn, sizeof(double));
+  w->rv = calloc(b->nnn, sizeof(double));
+}
+static void impl_free(impl_work *w) {
+  for (int a = 0; a < 3; ++a) free(w->coefe[a]);
+  free(w->coefdiag);
+  for (int a = 0; a < 5; ++a) free(w->d2w[a]);
+  for (int a = 0; a < 9; ++a) free(w->df[a]);
+  free(w->rv);
+}
+
+/* df index: 0 xx, 1 xy, 2 xz, 3 ex, 4 yy, 5 yz, 6 ey, 7 zz, 8 ez */
+enum { DXX = 0, DXY, DXZ, DEX, DYY, DYZ, DEY, DZZ, DEZ };
+
+/* face loop of one Jacobi sub-iteration (implimf_eu.f90:269-313,
+ * implimf_3d.f90:236-420); eu selects the implimf_eu form of tn */
+static void jacobi_faces(const blk_t *b, int eu, const double *d,
+                         const double *sn, impl_work *w) {
+  const int64_t L = G.ld, n0 = b->npc;
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    int lo[3], hi[3], idx[3];
+    dir_ranges(b, dir, 1, NDIR(b, dir), lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          const double sx = SN(sn, b, m, dir, 0), sy = SN(sn, b, m, dir, 1),
+                       sz = SN(sn, b, m, dir, 2);
+          double tn[5];
+          double **df = w->df;
+#define AV(arr, mm) ((arr)[mm] + (arr)[(mm) - ninc])
+          if (eu) {
+            tn[0] = 0.5 * ((d[L + n] + d[L + n - ninc]) * sx +
+                           (d[2 * L + n] + d[2 * L + n - ninc]) * sy +
+                           (d[3 * L + n] + d[3 * L + n - ninc]) * sz);
+            tn[1] = 0.5 * (AV(df[DXX], m) * sx + AV(df[DXY], m) * sy + AV(df[DXZ], m) * sz);
+            tn[2] = 0.5 * (AV(df[DXY], m) * sx + AV(df[DYY], m) * sy + AV(df[DYZ], m) * sz);
+            tn[3] = 0.5 * (AV(df[DXZ], m) * sx + AV(df[DYZ], m) * sy + AV(df[DZZ], m) * sz);
+            tn[4] = 0.5 * (AV(df[DEX], m) * sx + AV(df[DEY], m) * sy + AV(df[DEZ], m) * sz);
+          } else {
+            tn[0] = 0.5 * (d[L + n] + d[L + n - ninc]) * sx +
+                    0.5 * (d[2 * L + n] + d[2 * L + n - ninc]) * sy +
+                    0.5 * (d[3 * L + n] + d[3 * L + n - ninc]) * sz;
+            tn[1] = 0.5 * AV(df[DXX], m) * sx + 0.5 * AV(df[DXY], m) * sy + 0.5 * AV(df[DXZ], m) * sz;
+            tn[2] = 0.5 * AV(df[DXY], m) * sx + 0.5 * AV(df[DYY], m) * sy + 0.5 * AV(df[DYZ], m) * sz;
+            tn[3] = 0.5 * AV(df[DXZ], m) * sx + 0.5 * AV(df[DYZ], m) * sy + 0.5 * AV(df[DZZ], m) * sz;
+            tn[4] = 0.5 * AV(df[DEX], m) * sx + 0.5 * AV(df[DEY], m) * sy + 0.5 * AV(df[DEZ], m) * sz;
+          }
+#undef AV
+          const double ce = w->coefe[dir][m], cep = w->coefe[dir][m + ninc];
+          for (int a = 0; a < 5; ++a) {
+            w->d2w[a][m] = w->d2w[a][m] + tn[a] + ce * d[a * L + n - ninc] +
+                           cep * d[a * L + n + ninc];
+            w->d2w[a][m - ninc] = w->d2w[a][m - ninc] - tn[a];
+          }
+        }
+  }
+}
+
+/* implimf_eu.f90:79-330 (kfmg!=3, ityprk=0) */
+void orc_implimf_eu(int l, const double *u, const double *dt, double *v,
+                    double *d, const double *sn, const double *vol,
+                    const double *ps, const double *cson, int lmx) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  const double gam1 = G.gam1, pinfl = G.pinfl, fact = 0.;
+  impl_work w;
+  impl_alloc(b, &w);
+  for (int a = 0; a < 5; ++a)
+    for (int64_t n = n0; n < n0 + b->nnn; ++n) d[a * L + n] = 0.;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        w.coefdiag[m] = vol[n] * (fact + 1. / dt[n]);
+      }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    int lo[3], hi[3], idx[3];
+    dir_ranges(b, dir, 1, NDIR(b, dir), lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          const double sx = SN(sn, b, m, dir, 0), sy = SN(sn, b, m, dir, 1),
+                       sz = SN(sn, b, m, dir, 2);
+          double cnds = sx * sx + sy * sy + sz * sz;
+          double norm = 1. / v[n], norm1 = 1. / v[n - ninc];
+          double uu = 0.5 * (v[L + n] * norm + v[L + n - ninc] * norm1);
+          double vv = 0.5 * (v[2 * L + n] * norm + v[2 * L + n - ninc] * norm1);
+          double ww = 0.5 * (v[3 * L + n] * norm + v[3 * L + n - ninc] * norm1);
+          double cc = 0.5 * (cson[n] + cson[n - ninc]);
+          w.coefe[dir][m] = 0.5 * (fabs(uu * sx + vv * sy + ww * sz)) + sqrt(cnds) * cc;
+        }
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t m = ML(b, idx[0], idx[1], idx[2]);
+          w.coefdiag[m] = w.coefdiag[m] + w.coefe[dir][m] + w.coefe[dir][m + ninc];
+        }
+  }
+  for (int ls = 1; ls <= lmx; ++ls) {
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          for (int a = 0; a < 5; ++a) w.d2w[a][m] = -u[a * L + n];
+        }
+    jacobi_faces(b, 1, d, sn, &w);
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          for (int a = 0; a < 5; ++a) d[a * L + n] = w.d2w[a][m] / w.coefdiag[m];
+          double wi1 = 1. / (v[n] + d[n]);
+          double ui = v[L + n] + d[L + n];
+          double vi = v[2 * L + n] + d[2 * L + n];
+          double wi = v[3 * L + n] + d[3 * L + n];
+          double wi5 = v[4 * L + n] + d[4 * L + n];
+          double pres = gam1 * (wi5 - .5 * wi1 * (sq(ui) + sq(vi) + sq(wi)) - pinfl);
+          double norm = 1. / v[n];
+          const double v2 = v[L + n], v3 = v[2 * L + n], v4 = v[3 * L + n],
+                       v5 = v[4 * L + n], p = ps[n];
+          double fxx = v2 * (v2 * norm) + p;
+          double fxy = v3 * (v2 * norm);
+          double fxz = v4 * (v2 * norm);
+          double fyy = v3 * (v3 * norm) + p;
+          double fyz = v4 * (v3 * norm);
+          double fzz = v4 * (v4 * norm) + p;
+          double fex = (v5 + p - pinfl) * v2 * norm;
+          double fey = (v5 + p - pinfl) * v3 * norm;
+          double fez = (v5 + p - pinfl) * v4 * norm;
+          w.df[DXX][m] = wi1 * sq(ui) + pres - fxx;
+          w.df[DXY][m] = wi1 * ui * vi - fxy;
+          w.df[DXZ][m] = wi1 * ui * wi - fxz;
+          w.df[DEX][m] = wi1 * ui * (wi5 + pres - pinfl) - fex;
+          w.df[DYY][m] = wi1 * sq(vi) + pres - fyy;
+          w.df[DYZ][m] = wi1 * vi * wi - fyz;
+          w.df[DEY][m] = wi1 * vi * (wi5 + pres - pinfl) - fey;
+          w.df[DZZ][m] = wi1 * sq(wi) + pres - fzz;
+          /* implimf_eu.f90:312: the *wi factor of the z energy flux is
+           * missing in the reference and is reproduced here */
+          w.df[DEZ][m] = wi1 * (wi5 + pres - pinfl) - fez;
+        }
+  }
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        for (int a = 0; a < 5; ++a) v[a * L + n] = v[a * L + n] + d[a * L + n];
+      }
+  impl_free(&w);
+}
+
+/* implimf_3d.f90:64-490 (kfmg!=3, ityprk=0) */
+void orc_implimf_3d(int l, const double *u, const double *dt, double *v,
+                    double *d, const double *mu, const double *mut,
+                    const double *sn, const double *vol, const double *ps,
+                    const double *cson, int lmx) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  impl_work w;
+  impl_alloc(b, &w);
+  for (int a = 0; a < 5; ++a)
+    for (int64_t n = n0; n < n0 + b->nnn; ++n) d[a * L + n] = 0.;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        w.rv[m] = gam * (mu[n] / G.pr + mut[n] / G.prt) / v[n];
+        w.coefdiag[m] = vol[n] / dt[n];
+      }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    int lo[3], hi[3], idx[3];
+    dir_ranges(b, dir, 1, NDIR(b, dir), lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          const double sx = SN(sn, b, m, dir, 0), sy = SN(sn, b, m, dir, 1),
+                       sz = SN(sn, b, m, dir, 2);
+          double cnds = sx * sx + sy * sy + sz * sz;
+          double uu = 0.5 * (v[L + n] / v[n] + v[L + n - ninc] / v[n - ninc]);
+          double vv = 0.5 * (v[2 * L + n] / v[n] + v[2 * L + n - ninc] / v[n - ninc]);
+          double ww = 0.5 * (v[3 * L + n] / v[n] + v[3 * L + n - ninc] / v[n - ninc]);
+          double vn = uu * sx + vv * sy + ww * sz;
+          double cc = 0.5 * (cson[n] + cson[n - ninc]);
+          w.coefe[dir][m] = 0.5 * (fabs(vn) + sqrt(cnds) * cc) +
+                            (w.rv[m] + w.rv[m - ninc]) * cnds / (vol[n] + vol[n - ninc]);
+        }
+  }
+  const int64_t nci = 1, ncj = b->nid, nck = b->nijd;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t m = ML(b, i, j, k);
+        w.coefdiag[m] = w.coefdiag[m] + w.coefe[0][m] + w.coefe[0][m + nci] +
+                        w.coefe[1][m] + w.coefe[1][m + ncj] + w.coefe[2][m] +
+                        w.coefe[2][m + nck];
+      }
+  for (int ls = 1; ls <= lmx; ++ls) {
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          for (int a = 0; a < 5; ++a) w.d2w[a][m] = -u[a * L + n];
+        }
+    jacobi_faces(b, 0, d, sn, &w);
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          for (int a = 0; a < 5; ++a) d[a * L + n] = w.d2w[a][m] / w.coefdiag[m];
+          double wi1 = v[n] + d[n];
+          double wi2 = v[L + n] + d[L + n];
+          double wi3 = v[2 * L + n] + d[2 * L + n];
+          double wi4 = v[3 * L + n] + d[3 * L + n];
+          double wi5 = v[4 * L + n] + d[4 * L + n];
+          double ui = wi2 / wi1, vi = wi3 / wi1, wi = wi4 / wi1;
+          double pres = gam1 * (wi5 - .5 * wi1 * (sq(ui) + sq(vi) + sq(wi)) - pinfl);
+          const double v1 = v[n], v2 = v[L + n], v3 = v[2 * L + n], v4 = v[3 * L + n],
+                       v5 = v[4 * L + n], p = ps[n];
+          double fxx = v2 * (v2 / v1) + p;
+          double fxy = v3 * (v2 / v1);
+          double fxz = v4 * (v2 / v1);
+          double fyy = v3 * (v3 / v1) + p;
+          double fyz = v4 * (v3 / v1);
+          double fzz = v4 * (v4 / v1) + p;
+          double fex = (v5 + p - pinfl) * v2 / v1;
+          double fey = (v5 + p - pinfl) * v3 / v1;
+          double fez = (v5 + p - pinfl) * v4 / v1;
+          w.df[DXX][m] = wi1 * sq(ui) + pres - fxx;
+          w.df[DXY][m] = wi1 * ui * vi - fxy;
+          w.df[DXZ][m] = wi1 * ui * wi - fxz;
+          w.df[DEX][m] = ui * (wi5 + pres - pinfl) - fex;
+          w.df[DYY][m] = wi1 * sq(vi) + pres - fyy;
+          w.df[DYZ][m] = wi1 * vi * wi - fyz;
+          w.df[DEY][m] = vi * (wi5 + pres - pinfl) - fey;
+          w.df[DZZ][m] = wi1 * sq(wi) + pres - fzz;
+          w.df[DEZ][m] = wi * (wi5 + pres - pinfl) - fez;
+        }
+  }
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        for (int a = 0; a < 5; ++a) v[a * L + n] = v[a * L + n] + d[a * L + n];
+      }
+  impl_free(&w);
+}
+
+/* ------------------------------------------------------------------------ */
+/* residual norms                                                            */
+/* ------------------------------------------------------------------------ */
+
+/* residu.f90:89-241 per block, combined as in rscpsv.f90:79-150 */
+void orc_rscpsv(const double *u0, const double *v, const double *dt,
+                double *out) {
+  const int64_t L = G.ld;
+  double g1[5] = {0}, g2[5] = {0}, gmax[5] = {0};
+  int64_t npts = 0;
+  for (int l = 0; l < G.nblk; ++l) {
+    const blk_t *b = &G.b[l];
+    double d1[5] = {0}, d2[5] = {0}, dmax[5] = {0};
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k);
+          for (int a = 0; a < 5; ++a) {
+            double res = (v[a * L + n] - u0[a * L + n]) / dt[n];
+            d1[a] = d1[a] + fabs(res);
+            d2[a] = d2[a] + res * res;
+            dmax[a] = fmax(dmax[a], fabs(res));
+          }
+        }
+    const int64_t nmax = (int64_t)(b->ni - 1) * (b->nj - 1) * (b->nk - 1);
+    const double coef = 1. / (double)nmax;
+    for (int a = 0; a < 5; ++a) {
+      d1[a] = coef * d1[a];
+      d2[a] = sqrt(coef * d2[a]);
+      g1[a] = g1[a] + (double)nmax * d1[a];
+      g2[a] = g2[a] + (double)nmax * sq(d2[a]);
+      gmax[a] = fmax(gmax[a], fabs(dmax[a]));
+    }
+    npts += nmax;
+  }
+  for (int a = 0; a < 5; ++a) {
+    out[a] = g1[a] / (double)npts;
+    out[5 + a] = sqrt(g2[a] / (double)npts);
+    out[10 + a] = gmax[a];
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* one iteration                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* atsch_num.f90:245-1134 for ischema=7 (Roe), kmf=1 (implicit), steady */
+int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
+             const double *vol, double *ps, double *temp, double *cson,
+             double *mu, double *mut, double *tau, int compute_dt) {
+  for (int l = 1; l <= G.nblk; ++l) orc_zpres(l, v, ps, temp, cson);
+  if (G.ns)
+    for (int l = 1; l <= G.nblk; ++l) orc_zvismo(l, mu, temp);
+  if (compute_dt) {
+    for (int l = 1; l <= G.nblk; ++l) orc_chronos(l, mu, mut, v, dt, sn, vol, cson);
+    if (G.kdtl == 0) orc_chrono_global(dt);
+  }
+  orc_rbord(v, ps, temp, cson);
+  if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+  for (int l = 1; l <= G.nblk; ++l) {
+    if (G.ns) {
+      orc_sch_roe(l, u, v, tau, sn, ps);
+      orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
+    } else {
+      orc_sch_roe_euler(l, u, v, sn, ps);
+      orc_implimf_eu(l, u, dt, v, d, sn, vol, ps, cson, G.lmax);
+    }
+  }
+  return 0;
+}

@@ -1,0 +1,109 @@
+/*
+ * cns_oracle.h -- CPU oracle (test infrastructure only).
+ *
+ * A plain-C restatement of the CodeNS per-iteration hot path, used by the
+ * test-suite and by bench.py's CPU-baseline leg as the checker for the CUDA
+ * product.  It is NOT part of the product: nothing in codens_b200/ links,
+ * loads or calls it.
+ *
+ * Parity status: UNPINNED.  The reference is Fortran 90 with no tests, golden
+ * vectors or sample decks, and no Fortran compiler exists in this image, so
+ * the restatement cannot be checked against reference outputs.  It is pinned
+ * instead by line-by-line review against the cited reference lines and by the
+ * analytic invariants exercised in tests/ (freestream preservation, Roe
+ * consistency F(W,W)=F(W).S, telescoping conservation, Jacobi fixed point).
+ *
+ * Conventions (mirroring the reference's Fortran module globals):
+ *   - blocks are numbered l = 1..nblk;
+ *   - node and cell arrays share one flat index space; block l starts at the
+ *     0-based offset npc(l) (crdms.f90:150-157);
+ *   - within a block, cell (i,j,k) with Fortran index values i=0..ni+1
+ *     (ghost layer nfi=1, id1=0) sits at npc + i + j*nid + k*nid*njd
+ *     (sch_roe.f90:1487-1491 with 0-based storage);
+ *   - v/u/d are column-major (ld, ncol) arrays: v[c*ld + n];
+ *   - the normals of block l occupy sn[9*npc(l) ...] viewed as
+ *     sn(nnn, 3 face directions, 3 components) (atsch_num.f90:470-479).
+ * Arithmetic follows the reference expressions left to right with all
+ * literals in double precision (CMake build, -fdefault-real-8) and no FMA
+ * contraction (built with -ffp-contract=off).
+ */
+#ifndef CNS_ORACLE_H
+#define CNS_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* boundary condition kinds (rbord.f90:144-424) */
+enum { ORC_BC_EXTR = 1, ORC_BC_RC = 2, ORC_BC_PARA = 3, ORC_BC_IDD = 4,
+       ORC_BC_PRD = 5 };
+
+int  orc_setup(int nblk, const int32_t *dims /* 3*nblk: ni,nj,nk nodes */, int64_t ld);
+int64_t orc_npc(int l);
+int64_t orc_ncells(void);
+
+void orc_set_phys(double gam, double pinfl, double pr, double prt,
+                  double reynz, double suth_a, double pa1, double aa1,
+                  double omg);
+void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
+                    int kdtl, double dt1min, int lmax);
+
+/* boundaries: per boundary b: type, block (1-based), face (0..5 = i1,i2,j1,j2,
+ * k1,k2), first list entry mpb and count mmb, partner boundary (RC) and the
+ * boundary's own periodic rotation (cos, sin).  Per list entry: ghost cell
+ * ncbd, interior cell ncin (0-based global) and bc values (nlist x 5, column
+ * major: idd rpi,rti,d0x,d0y,d0z; prd p). */
+int orc_set_boundaries(int nbnd, const int32_t *type, const int32_t *blk,
+                       const int32_t *face, const int64_t *mpb,
+                       const int32_t *mmb, const int32_t *partner,
+                       const double *cosr, const double *sinr,
+                       int64_t nlist, const int64_t *ncbd, const int64_t *ncin,
+                       const double *bceqt);
+
+/* geometry (metrics.f90, extmhg.f90, norm.f90, svol.f90, rfsc.f90) and the
+ * boundary-entry geometry: inward unit normals (initns.f90) and ghost-cell
+ * centres (clidd.f90:64-71), stored internally and returned by
+ * orc_boundary_geom */
+void orc_metric(double *x, double *y, double *z, double *sn, double *vol);
+void orc_boundary_geom(double *nxn, double *nyn, double *nzn, double *ym,
+                       double *zm);
+
+/* per-block kernels (l = 1..nblk) */
+void orc_zpres(int l, const double *v, double *ps, double *temp, double *cson);
+void orc_zvismo(int l, double *mu, const double *temp);
+void orc_chronos(int l, const double *mu, const double *mut, const double *v,
+                 double *dt, const double *sn, const double *vol,
+                 const double *cson);
+void orc_chrono_global(double *dt);
+void orc_rbord(double *v, double *ps, double *temp, double *cson);
+void orc_sch_roe_euler(int l, double *u, const double *v, const double *sn,
+                       const double *ps);
+void orc_zvisqc(const double *v, const double *mu, const double *mut,
+                double *tau /* 9 x ld: toxx,toxy,toxz,toyy,toyz,tozz,qcx,qcy,qcz */,
+                const double *sn, const double *vol, const double *temp);
+void orc_sch_roe(int l, double *u, const double *v, const double *tau,
+                 const double *sn, const double *ps);
+void orc_implimf_eu(int l, const double *u, const double *dt, double *v,
+                    double *d, const double *sn, const double *vol,
+                    const double *ps, const double *cson, int lmx);
+void orc_implimf_3d(int l, const double *u, const double *dt, double *v,
+                    double *d, const double *mu, const double *mut,
+                    const double *sn, const double *vol, const double *ps,
+                    const double *cson, int lmx);
+/* residual norms (residu.f90, rscpsv.f90): out[0..4]=L1, [5..9]=L2,
+ * [10..14]=Linf over all blocks */
+void orc_rscpsv(const double *u0, const double *v, const double *dt,
+                double *out);
+
+/* one pseudo-time iteration over all blocks (atsch_num.f90:245-1134 for the
+ * ischema=7, kmf=1 Roe/implicit path); work holds ld*(9+5) doubles for
+ * ps,temp,cson,mu,mut,dt,...; returns 0 */
+int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
+             const double *vol, double *ps, double *temp, double *cson,
+             double *mu, double *mut, double *tau, int compute_dt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,129 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker of the CUDA product.  Parity status: UNPINNED (see
+cns_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "libcns_oracle.so")
+_lib = None
+
+_d = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        L.orc_setup.argtypes = [C.c_int, _i32, C.c_int64]
+        L.orc_setup.restype = C.c_int
+        L.orc_set_phys.argtypes = [C.c_double] * 9
+        L.orc_set_scheme.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int,
+                                     C.c_double, C.c_int, C.c_double, C.c_int]
+        L.orc_set_boundaries.argtypes = [C.c_int, _i32, _i32, _i32, _i64, _i32,
+                                         _i32, _d, _d, C.c_int64, _i64, _i64, _d]
+        L.orc_metric.argtypes = [_d] * 5
+        L.orc_boundary_geom.argtypes = [_d] * 5
+        L.orc_zpres.argtypes = [C.c_int, _d, _d, _d, _d]
+        L.orc_zvismo.argtypes = [C.c_int, _d, _d]
+        L.orc_chronos.argtypes = [C.c_int, _d, _d, _d, _d, _d, _d, _d]
+        L.orc_chrono_global.argtypes = [_d]
+        L.orc_rbord.argtypes = [_d, _d, _d, _d]
+        L.orc_sch_roe_euler.argtypes = [C.c_int, _d, _d, _d, _d]
+        L.orc_zvisqc.argtypes = [_d, _d, _d, _d, _d, _d, _d]
+        L.orc_sch_roe.argtypes = [C.c_int, _d, _d, _d, _d, _d]
+        L.orc_implimf_eu.argtypes = [C.c_int, _d, _d, _d, _d, _d, _d, _d, _d, C.c_int]
+        L.orc_implimf_3d.argtypes = [C.c_int, _d, _d, _d, _d, _d, _d, _d, _d, _d,
+                                     _d, C.c_int]
+        L.orc_rscpsv.argtypes = [_d, _d, _d, _d]
+        L.orc_step.argtypes = [_d] * 12 + [C.c_int]
+        L.orc_step.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+class OracleState:
+    """Host arrays of one case, in the reference's flat layout."""
+
+    def __init__(self, case):
+        ld = case.layout.ld
+        self.ld = ld
+        self.x = case.x.copy()
+        self.y = case.y.copy()
+        self.z = case.z.copy()
+        self.sn = np.zeros(9 * ld)
+        self.vol = np.zeros(ld)
+        self.v = np.ascontiguousarray(case.v0.reshape(-1)).copy()
+        self.u = np.zeros(5 * ld)
+        self.d = np.zeros(5 * ld)
+        self.dt = np.zeros(ld)
+        self.ps = np.zeros(ld)
+        self.temp = np.zeros(ld)
+        self.cson = np.zeros(ld)
+        self.mu = np.zeros(ld)
+        self.mut = np.zeros(ld)
+        self.tau = np.zeros(9 * ld)
+
+
+class Oracle:
+    """The reference hot path on the CPU, one case at a time (the library keeps
+    module-global state like the Fortran reference, so only one Oracle is
+    active at a time)."""
+
+    def __init__(self, case):
+        self.case = case
+        L = lib()
+        lay = case.layout
+        rc = L.orc_setup(lay.nblk, lay.dims_array(), lay.ld)
+        if rc:
+            raise ValueError(f"orc_setup failed ({rc})")
+        p = case.phys
+        L.orc_set_phys(p.gam, p.pinfl, p.pr, p.prt, p.reynz, p.suth_a, p.pa1,
+                       p.aa1, p.omg)
+        self.set_scheme(case.scheme)
+        ba = case.boundary_arrays()
+        self._ba = ba
+        L.orc_set_boundaries(len(ba["type"]), ba["type"], ba["blk"], ba["face"],
+                             ba["mpb"], ba["mmb"], ba["partner"], ba["cosr"],
+                             ba["sinr"], len(ba["ncbd"]), ba["ncbd"], ba["ncin"],
+                             np.ascontiguousarray(ba["bceqt"].reshape(-1)))
+
+    def set_scheme(self, s):
+        lib().orc_set_scheme(s.ns, s.muscl, s.xk, s.ilim, s.eta, s.kdtl,
+                             s.dt1min, s.lmax)
+
+    def metric(self, st: OracleState):
+        lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)
+
+    def boundary_geom(self):
+        n = len(self._ba["ncbd"])
+        out = [np.zeros(max(n, 1)) for _ in range(5)]
+        lib().orc_boundary_geom(*out)
+        return [o[:n] for o in out]
+
+    def step(self, st: OracleState, compute_dt: bool = True):
+        return lib().orc_step(st.v, st.u, st.d, st.dt, st.sn, st.vol, st.ps,
+                              st.temp, st.cson, st.mu, st.mut, st.tau,
+                              int(compute_dt))
+
+    def norms(self, u0, st: OracleState):
+        out = np.zeros(15)
+        lib().orc_rscpsv(u0, st.v, st.dt, out)
+        return out.reshape(3, 5)

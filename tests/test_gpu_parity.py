@@ -1,0 +1,270 @@
+"""GPU parity of every hot-path routine against the oracle, through the C ABI.
+
+FP64 results are compared bit for bit (the kernels evaluate the reference
+expressions in the reference's order with separately rounded multiplies and
+adds), except where a libm power is involved (the injection condition,
+clidd.f90:128 b**gam6): there the tolerance is 1e-13 relative per routine.
+"""
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+from oracle.oracle import lib as orc_lib
+
+from ._helpers import SMALL, assert_equal_bits, max_rel, oracle_prepared, real
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(case):
+    from codens_b200.solver import CodeNS
+    s = CodeNS(case)
+    s.metric()
+    s.sync()
+    return s
+
+
+def _t(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+def _n(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_metric_parity(cuda, name):
+    case = SMALL[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    n = case.layout.ncells
+    assert_equal_bits(_n(s.sn), st.sn, "sn")
+    assert_equal_bits(_n(s.vol)[:n], st.vol[:n], "vol")
+    for a, b, w in zip(s.boundary_geom(), orc.boundary_geom(), "nx ny nz ym zm".split()):
+        assert_equal_bits(a, b, w)
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_zpres_zvismo_chronos_rbord(cuda, name):
+    torch = cuda
+    case = SMALL[name]()
+    orc, st = oracle_prepared(case)
+    L = orc_lib()
+    s = _gpu(case)
+    rc = real(case)
+    nb = case.layout.nblk
+    for l in range(1, nb + 1):
+        L.orc_zpres(l, st.v, st.ps, st.temp, st.cson)
+    s.zpres(0, s.v, s.pression, s.ztemp, s.cson)
+    s.sync()
+    for nm in ("pression", "ztemp", "cson"):
+        a = _n(getattr(s, nm))[rc]
+        b = {"pression": st.ps, "ztemp": st.temp, "cson": st.cson}[nm][rc]
+        assert_equal_bits(a, b, nm)
+    if case.scheme.ns:
+        for l in range(1, nb + 1):
+            L.orc_zvismo(l, st.mu, st.temp)
+        s.zvismo(0, s.mu, s.v, s.ztemp)
+        s.sync()
+        assert_equal_bits(_n(s.mu)[rc], st.mu[rc], "mu")
+    for l in range(1, nb + 1):
+        L.orc_chronos(l, st.mu, st.mut, st.v, st.dt, st.sn, st.vol, st.cson)
+    s.chronos(0, s.mu, s.mut, s.v, s.dt, s.sn, s.vol, s.cson)
+    s.sync()
+    assert_equal_bits(_n(s.dt)[rc], st.dt[rc], "dt")
+    # boundary conditions: ghost values of every list entry
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    s.rbord(s.v, s.pression, s.ztemp, s.cson)
+    s.sync()
+    g = case.boundary_arrays()["ncbd"]
+    has_idd = any(b.kind == cases.BC_IDD for b in case.boundaries)
+    v_g = _n(s.v).reshape(5, -1)[:, g]
+    v_o = st.v.reshape(5, -1)[:, g]
+    if has_idd:
+        assert max_rel(v_g, v_o) <= 1e-13
+        assert max_rel(_n(s.pression)[g], st.ps[g]) <= 1e-13
+    else:
+        assert_equal_bits(v_g, v_o, "ghost v")
+        assert_equal_bits(_n(s.pression)[g], st.ps[g], "ghost p")
+        assert_equal_bits(_n(s.cson)[g], st.cson[g], "ghost c")
+    s.close()
+
+
+def _prepared_flow(case):
+    """oracle state after zpres, zvismo, chronos, rbord and zvisqc"""
+    orc, st = oracle_prepared(case)
+    L = orc_lib()
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_zpres(l, st.v, st.ps, st.temp, st.cson)
+        if case.scheme.ns:
+            L.orc_zvismo(l, st.mu, st.temp)
+        L.orc_chronos(l, st.mu, st.mut, st.v, st.dt, st.sn, st.vol, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    if case.scheme.ns:
+        L.orc_zvisqc(st.v, st.mu, st.mut, st.tau, st.sn, st.vol, st.temp)
+    return orc, st
+
+
+def _load_state(torch, s, st):
+    for nm, a in (("v", st.v), ("pression", st.ps), ("ztemp", st.temp), ("cson", st.cson),
+                  ("mu", st.mu), ("mut", st.mut), ("dt", st.dt), ("tau", st.tau)):
+        getattr(s, nm).copy_(_t(torch, a))
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("name", ["box_ns", "channel", "box_pinfl"])
+def test_zvisqc_parity(cuda, name):
+    torch = cuda
+    case = SMALL[name]()
+    orc, st = _prepared_flow(case)
+    s = _gpu(case)
+    _load_state(torch, s, st)
+    s.tau.zero_()
+    torch.cuda.synchronize()
+    s.zvisqc(s.v, s.mu, s.mut, s.tau, s.sn, s.vol, s.ztemp)
+    s.sync()
+    ld = case.layout.ld
+    idx = np.concatenate([real(case), case.boundary_arrays()["ncbd"]])
+    assert_equal_bits(_n(s.tau).reshape(9, ld)[:, idx], st.tau.reshape(9, ld)[:, idx], "tau")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_residual_parity(cuda, name):
+    torch = cuda
+    case = SMALL[name]()
+    orc, st = _prepared_flow(case)
+    s = _gpu(case)
+    _load_state(torch, s, st)
+    L = orc_lib()
+    u_o = np.zeros_like(st.u)
+    for l in range(1, case.layout.nblk + 1):
+        if case.scheme.ns:
+            L.orc_sch_roe(l, u_o, st.v, st.tau, st.sn, st.ps)
+        else:
+            L.orc_sch_roe_euler(l, u_o, st.v, st.sn, st.ps)
+    ld = case.layout.ld
+    rc = real(case)
+    # all blocks in one launch, then block by block as the reference calls it
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        s.u.fill_(7.0)
+        torch.cuda.synchronize()
+        if l == 0:
+            if case.scheme.ns:
+                s.sch_roe(0, s.u, s.v, s.tau, s.sn, s.pression)
+            else:
+                s.sch_roe_euler(0, s.u, s.v, s.sn, s.pression)
+            sel = rc
+        else:
+            if case.scheme.ns:
+                s.sch_roe(l, s.u, s.v, s.tau, s.sn, s.pression)
+            else:
+                s.sch_roe_euler(l, s.u, s.v, s.sn, s.pression)
+            sel = case.layout.blocks[l - 1].real_cells()
+        s.sync()
+        assert_equal_bits(_n(s.u).reshape(5, ld)[:, sel], u_o.reshape(5, ld)[:, sel],
+                          f"u (l={l})")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("lmx", [0, 1, 4])
+def test_implicit_parity(cuda, name, lmx):
+    torch = cuda
+    case = SMALL[name]()
+    orc, st = _prepared_flow(case)
+    L = orc_lib()
+    for l in range(1, case.layout.nblk + 1):
+        if case.scheme.ns:
+            L.orc_sch_roe(l, st.u, st.v, st.tau, st.sn, st.ps)
+        else:
+            L.orc_sch_roe_euler(l, st.u, st.v, st.sn, st.ps)
+    s = _gpu(case)
+    _load_state(torch, s, st)
+    s.u.copy_(_t(torch, st.u))
+    torch.cuda.synchronize()
+    for l in range(1, case.layout.nblk + 1):
+        if case.scheme.ns:
+            L.orc_implimf_3d(l, st.u, st.dt, st.v, st.d, st.mu, st.mut, st.sn, st.vol,
+                             st.ps, st.cson, lmx)
+            s.implimf_3d(l, s.u, s.dt, s.v, s.d, s.mu, s.mut, s.sn, s.vol, s.pression,
+                         s.cson, lmx)
+        else:
+            L.orc_implimf_eu(l, st.u, st.dt, st.v, st.d, st.sn, st.vol, st.ps, st.cson, lmx)
+            s.implimf_eu(l, s.u, s.dt, s.v, s.d, s.sn, s.vol, s.pression, s.cson, lmx)
+    s.sync()
+    ld = case.layout.ld
+    rc = real(case)
+    assert_equal_bits(_n(s.d).reshape(5, ld)[:, rc], st.d.reshape(5, ld)[:, rc], "d")
+    assert_equal_bits(_n(s.v).reshape(5, ld)[:, rc], st.v.reshape(5, ld)[:, rc], "v")
+    s.close()
+
+
+@pytest.mark.parametrize("name,nsteps", [("box_eu", 4), ("box_ns", 6), ("channel", 6),
+                                         ("batch", 4), ("box_pinfl", 5)])
+def test_fused_steps_parity(cuda, name, nsteps):
+    """the graph-captured iteration against the oracle's atsch_num sequence,
+    state and L2 history after several iterations"""
+    case = SMALL[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    rc = real(case)
+    has_idd = any(b.kind == cases.BC_IDD for b in case.boundaries)
+    for it in range(nsteps):
+        u0 = st.v.copy()
+        orc.step(st)
+        no = orc.norms(u0, st)
+        ng = s.atsch_num(1)
+        v_g = _n(s.v).reshape(5, ld)[:, rc]
+        v_o = st.v.reshape(5, ld)[:, rc]
+        if has_idd:
+            assert max_rel(v_g, v_o) <= 1e-12, f"step {it}"
+        else:
+            assert_equal_bits(v_g, v_o, f"v after step {it}")
+        np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0, err_msg=f"norms step {it}")
+    s.close()
+
+
+def test_host_entry_point_matches_device(cuda):
+    torch = cuda
+    case = SMALL["box_ns"]()
+    a = _gpu(case)
+    b = _gpu(case)
+    na = a.atsch_num(3)
+    vh = torch.as_tensor(case.v0.reshape(-1).copy()).pin_memory()
+    nb = b.atsch_num_host(vh, 3)
+    assert_equal_bits(vh.numpy(), _n(a.v), "v host vs device")
+    np.testing.assert_array_equal(na, nb)
+    a.close()
+    b.close()
+
+
+def test_rscpsv_parity(cuda):
+    torch = cuda
+    case = SMALL["channel"]()
+    orc, st = oracle_prepared(case)
+    u0 = st.v.copy()
+    orc.step(st)
+    no = orc.norms(u0, st)
+    s = _gpu(case)
+    ng = s.rscpsv(_t(torch, u0), _t(torch, st.v), _t(torch, st.dt))
+    np.testing.assert_allclose(ng, no, rtol=1e-13)
+    s.close()
+
+
+def test_errors_are_codes(cuda):
+    from codens_b200 import abi
+    case = SMALL["box_ns"]()
+    s = _gpu(case)
+    with pytest.raises(abi.CnsError) as ei:
+        s.zpres(case.layout.nblk + 1, s.v, s.pression, s.ztemp, s.cson)
+    assert ei.value.code == 1
+    # a non-positive temperature is reported, not trapped (zvismo.f90:123-127)
+    s.ztemp.fill_(-1.0)
+    with pytest.raises(abi.CnsError) as ei:
+        s.zvismo(0, s.mu, s.v, s.ztemp)
+    assert ei.value.code == 3
+    s.close()

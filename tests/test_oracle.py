@@ -1,0 +1,136 @@
+"""CPU tests of the oracle: the analytic invariants that pin the restatement
+of the reference (no reference outputs exist to pin it against)."""
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+from oracle.oracle import Oracle, OracleState, lib
+
+from ._helpers import SMALL, oracle_prepared, real
+
+
+def test_box_volumes_and_normals():
+    case = cases.box_case((8, 6, 5), seed=1)
+    orc, st = oracle_prepared(case)
+    rc = real(case)
+    assert np.all(st.vol[rc] > 0)
+    assert st.vol[rc].sum() == pytest.approx(2.0, rel=1e-13)  # 2 x 1 x 1 box
+    b = case.layout.blocks[0]
+    # extrapolation ghost cells are degenerate (ghost nodes = boundary nodes)
+    g = b.ic(0, 3, 2)
+    assert st.vol[g] == 0.0
+    # coincident ghost volume = partner interior volume (rfsc.f90)
+    assert st.vol[b.ic(3, 0, 2)] == st.vol[b.ic(3, b.nj - 1, 2)]
+    # sn points towards increasing index: i-faces have +x area on a box
+    sn = st.sn[9 * b.npc: 9 * b.npc + 9 * b.nnn].reshape(3, 3, b.nnn)  # [comp][dir][m]
+    m = b.ic(3, 2, 2) - b.npc
+    assert sn[0, 0, m] > 0 and sn[1, 1, m] > 0 and sn[2, 2, m] > 0
+
+
+def test_skewed_volume_conservation():
+    """the closed-surface identity: sum of cell volumes equals the box volume
+    for a perturbed grid whose boundary is the box"""
+    case = cases.box_case((10, 8, 6), seed=1, skew=0.02)
+    orc, st = oracle_prepared(case)
+    assert st.vol[real(case)].sum() == pytest.approx(2.0, rel=1e-12)
+
+
+@pytest.mark.parametrize("ns", [False, True])
+def test_freestream_preservation(ns):
+    """a uniform state gives a zero residual on a curved grid (Roe
+    consistency F(W,W) = F(W).S plus the closed-cell metric identity)"""
+    case = cases.box_case((10, 7, 6), seed=3, noise=0.0, ns=ns, ilim=int(ns),
+                          skew=0.03, alpha=4.0)
+    orc, st = oracle_prepared(case)
+    L = lib()
+    L.orc_zpres(1, st.v, st.ps, st.temp, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    if ns:
+        L.orc_zvismo(1, st.mu, st.temp)
+        L.orc_zvisqc(st.v, st.mu, st.mut, st.tau, st.sn, st.vol, st.temp)
+        L.orc_sch_roe(1, st.u, st.v, st.tau, st.sn, st.ps)
+    else:
+        L.orc_sch_roe_euler(1, st.u, st.v, st.sn, st.ps)
+    u = st.u.reshape(5, -1)[:, real(case)]
+    scale = np.abs(case.v0[:, 0]).max()
+    assert np.abs(u).max() < 1e-13 * scale
+
+
+def test_ns_channel_converges():
+    case = SMALL["channel"]()
+    orc, st = oracle_prepared(case)
+    l2 = []
+    for _ in range(25):
+        u0 = st.v.copy()
+        orc.step(st)
+        l2.append(orc.norms(u0, st)[1, 0])
+    assert np.all(np.isfinite(l2))
+    assert l2[-1] < 0.5 * l2[0]
+
+
+def test_euler_reference_defect_diverges():
+    """implimf_eu.f90:312 drops the *wi factor of the z energy increment; on a
+    3-D noisy box the reference Euler implicit path (reproduced here) blows up
+    within a few dozen iterations even at CFL 1 -- documented behaviour the
+    parity path keeps."""
+    case = cases.box_case((12, 6, 6), seed=1, eta=1.0)
+    orc, st = oracle_prepared(case)
+    with np.errstate(all="ignore"):
+        for _ in range(60):
+            orc.step(st)
+    assert not np.all(np.isfinite(st.v[real(case)]))
+
+
+def test_jacobi_fixed_point():
+    """with many sub-iterations the point-Jacobi increment satisfies its own
+    linear system: a second implicit pass on the same residual with lmax and
+    2*lmax agrees to the contraction error"""
+    case = cases.box_case((8, 6, 5), seed=5, ns=True, ilim=0, lmax=40)
+    orc, st = oracle_prepared(case)
+    L = lib()
+    L.orc_zpres(1, st.v, st.ps, st.temp, st.cson)
+    L.orc_zvismo(1, st.mu, st.temp)
+    L.orc_chronos(1, st.mu, st.mut, st.v, st.dt, st.sn, st.vol, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    L.orc_zvisqc(st.v, st.mu, st.mut, st.tau, st.sn, st.vol, st.temp)
+    L.orc_sch_roe(1, st.u, st.v, st.tau, st.sn, st.ps)
+    v0 = st.v.copy()
+    d40 = np.zeros_like(st.d)
+    va = v0.copy()
+    L.orc_implimf_3d(1, st.u, st.dt, va, d40, st.mu, st.mut, st.sn, st.vol, st.ps,
+                     st.cson, 40)
+    d80 = np.zeros_like(st.d)
+    vb = v0.copy()
+    L.orc_implimf_3d(1, st.u, st.dt, vb, d80, st.mu, st.mut, st.sn, st.vol, st.ps,
+                     st.cson, 80)
+    rc = real(case)
+    a, b = d40.reshape(5, -1)[:, rc], d80.reshape(5, -1)[:, rc]
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+
+
+def test_norms_match_numpy():
+    case = SMALL["box_ns"]()
+    orc, st = oracle_prepared(case)
+    u0 = st.v.copy()
+    orc.step(st)
+    nr = orc.norms(u0, st)
+    rc = real(case)
+    res = (st.v.reshape(5, -1)[:, rc] - u0.reshape(5, -1)[:, rc]) / st.dt[rc]
+    np.testing.assert_allclose(nr[0], np.abs(res).mean(axis=1), rtol=1e-12)
+    np.testing.assert_allclose(nr[1], np.sqrt((res ** 2).mean(axis=1)), rtol=1e-12)
+    np.testing.assert_allclose(nr[2], np.abs(res).max(axis=1), rtol=0)
+
+
+def test_boundary_geometry():
+    case = SMALL["channel"]()
+    orc, st = oracle_prepared(case)
+    nx, ny, nz, ym, zm = orc.boundary_geom()
+    ba = case.boundary_arrays()
+    np.testing.assert_allclose(nx ** 2 + ny ** 2 + nz ** 2, 1.0, rtol=1e-14)
+    # the inlet (idd, face i1) normal points into the domain: +x
+    ib = [i for i, b in enumerate(case.boundaries) if b.kind == cases.BC_IDD][0]
+    sl = slice(ba["mpb"][ib], ba["mpb"][ib] + ba["mmb"][ib])
+    assert np.all(nx[sl] > 0.999)
+    ob = [i for i, b in enumerate(case.boundaries) if b.kind == cases.BC_PRD][0]
+    sl = slice(ba["mpb"][ob], ba["mpb"][ob] + ba["mmb"][ob])
+    assert np.all(nx[sl] < -0.999)
