@@ -70,6 +70,7 @@ class Scheme:
     kdtl: int = 1        # local time step
     dt1min: float = 0.0
     lmax: int = 10
+    qfix_dfez: int = 0   # non-reference: restore the *wi of implimf_eu.f90:312
 
 
 @dataclass
@@ -240,12 +241,12 @@ def box_case(cells=(64, 32, 32), mach: float = 0.8, seed: int = 1,
              noise: float = 0.01, ns: bool = False, ilim: int = 0,
              skew: float = 0.0, lmax: int = 10, eta: float = 5.0,
              pinfl: float = 0.0, reynz: float = 1.0e12, alpha: float = 0.0,
-             name: str = "box") -> Case:
+             qfix_dfez: int = 0, name: str = "box") -> Case:
     """Single stretched box: extr on i faces, self-periodic j and k."""
     ni, nj, nk = (c + 1 for c in cells)
     lay = Layout.from_dims([(ni, nj, nk)])
     phys = Phys(pinfl=pinfl, reynz=reynz)
-    scheme = Scheme(ns=int(ns), ilim=ilim, lmax=lmax, eta=eta)
+    scheme = Scheme(ns=int(ns), ilim=ilim, lmax=lmax, eta=eta, qfix_dfez=qfix_dfez)
     x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
     idx, X, Y, Z = _box_coords(lay, 0, skew=skew)
     x[idx], y[idx], z[idx] = X, Y, Z
@@ -261,7 +262,8 @@ def box_case(cells=(64, 32, 32), mach: float = 0.8, seed: int = 1,
 
 def batch_case(ncase: int = 64, side=(16, 96), seed: int = 4,
                noise: float = 0.01, lmax: int = 10, eta: float = 5.0,
-               mach_range=(0.3, 2.0), alpha_range=(-5.0, 5.0)) -> Case:
+               mach_range=(0.3, 2.0), alpha_range=(-5.0, 5.0),
+               qfix_dfez: int = 0) -> Case:
     """Independent single-block Euler boxes run as one multi-block layout."""
     r = splitmix64_uniform(seed, 5 * ncase).reshape(ncase, 5)
     lo, hi = side
@@ -270,7 +272,7 @@ def batch_case(ncase: int = 64, side=(16, 96), seed: int = 4,
     alphas = alpha_range[0] + r[:, 4] * (alpha_range[1] - alpha_range[0])
     lay = Layout.from_dims([tuple(int(s) + 1 for s in sd) for sd in sides])
     phys = Phys()
-    scheme = Scheme(ns=0, lmax=lmax, eta=eta)
+    scheme = Scheme(ns=0, lmax=lmax, eta=eta, qfix_dfez=qfix_dfez)
     x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
     states = {}
     bnd: List[Boundary] = []

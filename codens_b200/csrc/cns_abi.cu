@@ -26,9 +26,9 @@ struct cns_ctx {
   // boundaries
   Bnd bd{};
   std::vector<int> h_btype;
-  int n_idd = 0;
-  int* d_idd_list = nullptr;
-  double* clidd_scratch = nullptr;
+  long long n_idd_ent = 0;
+  long long* d_idd_ents = nullptr;  // list entries of injection boundaries
+  unsigned* d_idd_masks = nullptr;  // per boundary sweep masks
   // scratch
   Work w;
   std::vector<void*> allocs;
@@ -145,17 +145,24 @@ int check_status(cns_ctx* c) {
   return CNS_OK;
 }
 
+// primitive velocities of the cells of block l (0: every block)
+cudaError_t prim_of(cns_ctx* c, int l, const double* v) {
+  long long n0, n1;
+  block_range(c, l, n0, n1);
+  return launch_prim(n0, n1, v, c->lay.ld, c->w.prim, c->st);
+}
+
 // the residual of one block set: (optional) limiter ratios, face fluxes,
-// accumulation into u
+// accumulation into u; the primitive velocities must be current
 cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
                      const double* tau, const double* sn, const double* ps) {
   const long long ld = c->lay.ld;
   cudaError_t e = cudaSuccess;
   if (c->sc.ns && c->sc.ilim == 1)
-    e = launch_ratio(c->d_blks, c->lines, l0, v, ld, ps, c->w.R, c->st);
+    e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
   if (e == cudaSuccess)
-    e = launch_face_flux(c->d_blks, c->faces, l0, c->ph, c->sc, v, ld, ps, tau, sn,
-                         c->w.R, c->w.G, c->st);
+    e = launch_face_flux(c->d_blks, c->faces, l0, c->ph, c->sc, v, c->w.prim, ld, ps, tau,
+                         sn, c->w.R, c->w.G, c->st);
   if (e == cudaSuccess)
     e = launch_accumulate(c->d_blks, c->cells.view(l0), c->w.G, ld, u, c->st);
   return e;
@@ -173,11 +180,12 @@ cudaError_t enqueue_step(cns_ctx* c) {
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
   if (e == cudaSuccess)
-    e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd,
-                     c->d_idd_list, c->clidd_scratch, c->st);
+    e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
+                     c->d_idd_ents, c->d_idd_masks, c->st);
+  if (e == cudaSuccess) e = launch_prim(0, c->lay.ncells, s.v, ld, c->w.prim, c->st);
   if (e == cudaSuccess && c->sc.ns) {
-    e = launch_grad(c->d_blks, all, c->ph, s.v, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
-                    s.ztemp, c->st);
+    e = launch_grad(c->d_blks, all, c->ph, s.v, c->w.prim, ld, s.mu, s.mut, s.tau, s.sn,
+                    s.vol, s.ztemp, c->st);
     if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
   }
   if (e == cudaSuccess) e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
@@ -280,7 +288,8 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     cns_destroy(c);
     return CNS_EINVAL;
   }
-  std::vector<int> ent_bnd((size_t)nl), blk0(nb), idd;
+  std::vector<int> ent_bnd((size_t)nl), blk0(nb);
+  std::vector<long long> idd_ents;
   for (int b = 0; b < nb; ++b) {
     const int t = bnd->type[b];
     if (t < CNS_BC_EXTR || t > CNS_BC_PRD) {
@@ -300,8 +309,10 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
       }
     }
     blk0[b] = bnd->blk[b] - 1;
-    for (int m = 0; m < bnd->mmb[b]; ++m) ent_bnd[(size_t)(bnd->mpb[b] + m)] = b;
-    if (t == CNS_BC_IDD) idd.push_back(b);
+    for (int m = 0; m < bnd->mmb[b]; ++m) {
+      ent_bnd[(size_t)(bnd->mpb[b] + m)] = b;
+      if (t == CNS_BC_IDD) idd_ents.push_back(bnd->mpb[b] + m);
+    }
     c->h_btype.push_back(t);
   }
   for (long long q = 0; q < nl; ++q) {
@@ -312,7 +323,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   }
   c->bd.nbnd = nb;
   c->bd.nlist = nl;
-  c->n_idd = (int)idd.size();
+  c->n_idd_ent = (long long)idd_ents.size();
   {
     int *t_, *b_, *f_, *m_, *p_, *eb_;
     long long *mpb_, *ncbd_, *ncin_;
@@ -329,13 +340,13 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     if (e == cudaSuccess) e = upload(c, &ncbd_, (const long long*)bnd->ncbd, (size_t)nl);
     if (e == cudaSuccess) e = upload(c, &ncin_, (const long long*)bnd->ncin, (size_t)nl);
     if (e == cudaSuccess) e = upload(c, &bc_, bnd->bceqt, (size_t)(5 * nl));
-    if (e == cudaSuccess) e = upload(c, &c->d_idd_list, idd.data(), idd.size());
+    if (e == cudaSuccess) e = upload(c, &c->d_idd_ents, idd_ents.data(), idd_ents.size());
+    if (e == cudaSuccess) e = dev_alloc(c, &c->d_idd_masks, (size_t)nb);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nxn, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nyn, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nzn, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.ym, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.zm, (size_t)nl);
-    if (e == cudaSuccess) e = dev_alloc(c, &c->clidd_scratch, (size_t)(3 * nl));
     if (e != cudaSuccess) return cleanup_fail(e, "boundary tables");
     c->bd.type = t_;
     c->bd.blk = b_;
@@ -353,7 +364,8 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   // scratch (zeroed: ghost entries of the Jacobi iterates and of rv stay 0)
   const long long ld = c->lay.ld;
   c->w.ld = ld;
-  e = dev_alloc(c, &c->w.G, (size_t)(15 * ld));
+  e = dev_alloc(c, &c->w.prim, (size_t)(3 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.G, (size_t)(15 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.R, (size_t)(15 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.coefe, (size_t)(3 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.coefdiag, (size_t)ld);
@@ -484,8 +496,8 @@ int cns_chronos(cns_ctx* c, int l, const double* mu, const double* mut,
 int cns_rbord(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
   if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
   if (!c->metric_done) return fail(c, CNS_ENOTREADY, "cns_metric has not run");
-  CK(launch_rbord(c->bd, c->ph, v, c->lay.ld, ps, temp, cson, c->n_idd, c->d_idd_list,
-                  c->clidd_scratch, c->st));
+  CK(launch_rbord(c->bd, c->ph, v, c->lay.ld, ps, temp, cson, c->n_idd_ent, c->d_idd_ents,
+                  c->d_idd_masks, c->st));
   return CNS_OK;
 }
 
@@ -495,7 +507,8 @@ int cns_sch_roe_euler(cns_ctx* c, int l, double* u, const double* v,
   const Scheme keep = c->sc;
   c->sc.ns = 0;
   CK(zero_cols(c, u, 5, l));
-  cudaError_t e = residual(c, l - 1, u, v, nullptr, sn, ps);
+  cudaError_t e = prim_of(c, l, v);
+  if (e == cudaSuccess) e = residual(c, l - 1, u, v, nullptr, sn, ps);
   c->sc = keep;
   CK(e);
   return CNS_OK;
@@ -507,7 +520,8 @@ int cns_sch_roe(cns_ctx* c, int l, double* u, const double* v, const double* tau
   const Scheme keep = c->sc;
   c->sc.ns = 1;
   CK(zero_cols(c, u, 5, l));
-  cudaError_t e = residual(c, l - 1, u, v, tau, sn, ps);
+  cudaError_t e = prim_of(c, l, v);
+  if (e == cudaSuccess) e = residual(c, l - 1, u, v, tau, sn, ps);
   c->sc = keep;
   CK(e);
   return CNS_OK;
@@ -517,8 +531,9 @@ int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,
                double* tau, const double* sn, const double* vol,
                const double* temp) {
   if (!c || !v || !mu || !mut || !tau || !sn || !vol || !temp) return CNS_EINVAL;
-  CK(launch_grad(c->d_blks, c->cells.view(-1), c->ph, v, c->lay.ld, mu, mut, tau, sn,
-                 vol, temp, c->st));
+  CK(prim_of(c, 0, v));
+  CK(launch_grad(c->d_blks, c->cells.view(-1), c->ph, v, c->w.prim, c->lay.ld, mu, mut, tau,
+                 sn, vol, temp, c->st));
   CK(launch_tau_ghosts(c->bd, tau, c->lay.ld, c->st));
   return CNS_OK;
 }
@@ -529,6 +544,7 @@ static int implimf(cns_ctx* c, int l, int eu, const double* u, const double* dt,
                    const double* cson, int lmx) {
   if (lmx < 0) return CNS_EINVAL;
   CK(zero_cols(c, d, 5, l));
+  CK(prim_of(c, l, v));
   CK(launch_implicit(c->d_blks, c->cells.view(l - 1), c->faces, l - 1, c->ph, c->sc, eu,
                      lmx, u, dt, v, d, mu, mut, sn, vol, ps, cson, c->w, 0, c->st));
   return CNS_OK;

@@ -73,6 +73,22 @@ __global__ void __launch_bounds__(kTile) k_zvismo(const Blk* __restrict__ blks,
   }
 }
 
+// primitive velocities u = rho u / rho (and v, w) of every cell of a flat
+// range, once per iteration after the boundary conditions: the face fluxes,
+// the limiter ratios, the gradients and the implicit phase all use these very
+// quotients (the reference recomputes them at every use, with identical
+// results), so sharing them changes no bit
+__global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
+                                             const double* __restrict__ v,
+                                             long long ld, double* __restrict__ prim) {
+  const long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= n1) return;
+  const double r = v[n];
+  prim[n] = v[ld + n] / r;
+  prim[ld + n] = v[2 * ld + n] / r;
+  prim[2 * ld + n] = v[3 * ld + n] / r;
+}
+
 // chronos.f90:110-194 (kprec = 0)
 __global__ void __launch_bounds__(kTile) k_chronos(
     const Blk* __restrict__ blks, Space sp, Phys ph, Scheme sc,
@@ -188,111 +204,113 @@ __global__ void __launch_bounds__(256) k_rbord(Bnd bd, Phys ph, double* v,
   }
 }
 
-// utidd.f90 + rbve.f90 + clidd.f90:50-170 for one injection boundary per CTA:
-// Newton on the normal velocity until the largest relative update over the
-// whole boundary is below 1e-7, at most 20 sweeps
-__global__ void __launch_bounds__(256) k_clidd(Bnd bd, Phys ph, const int* idd_list,
-                                              double* v, long long ld, double* ps_,
-                                              double* temp, double* cson,
-                                              double* scratch /* [4*nlist] */) {
-  __shared__ double red[256 / 32];
-  __shared__ double residu_sh;
-  const int bb = idd_list[blockIdx.x];
-  const long long m0 = bd.mpb[bb];
-  const int mt = bd.mmb[bb];
-  const double eps = 0.0000001;
+// utidd.f90 + rbve.f90 + clidd.f90:50-170: injection at imposed total
+// pressure, total temperature and flow direction.  The reference iterates a
+// Newton method on the normal velocity of every boundary cell, sweep after
+// sweep, until the largest relative update over the whole boundary is below
+// 1e-7 (at most 20 sweeps).  Each cell's iterate depends on that cell only;
+// only the number of sweeps is global.  So pass 1 runs every cell's 20 sweeps
+// and ORs into a per-boundary word which sweeps still had an update above
+// 1e-7; pass 2 reads the sweep count (the first sweep whose bit is clear) and
+// replays exactly that many sweeps: the same values as the sequential loop.
+struct IddCell {
+  double usdn, usdn2, un, qn, roc0, am0, rpi, rti;
+};
+
+__device__ __forceinline__ void idd_setup(const Bnd& bd, const Phys& ph,
+                                          const double* __restrict__ v,
+                                          long long ld, long long e, IddCell& c) {
+  const long long nl = bd.nlist, ni = bd.ncin[e];
+  const double d0x = bd.bceqt[2 * nl + e], d0y = bd.bceqt[3 * nl + e],
+               d0z = bd.bceqt[4 * nl + e];
+  const double nx = bd.nxn[e], ny = bd.nyn[e], nz = bd.nzn[e];
+  c.rpi = bd.bceqt[e];
+  c.rti = bd.bceqt[nl + e];
+  c.usdn = 1. / (d0x * nx + d0y * ny + d0z * nz);
+  c.usdn2 = sq(c.usdn);
+  c.un = ph.omg * (bd.ym[e] * nz - bd.zm[e] * ny);
+  // the ghost cell holds the interior state (rbve) when clidd reads it
+  const double r1 = v[ni], r2 = v[ld + ni], r3 = v[2 * ld + ni], r4 = v[3 * ld + ni];
+  const double qxs = r2 / r1, qys = r3 / r1, qzs = r4 / r1;
+  c.qn = qxs * nx + qys * ny + qzs * nz;
+  const double p = ph.gam1 * (v[4 * ld + ni] - 0.5 * (qxs * r2 + qys * r3 + qzs * r4) - ph.pinfl);
+  c.roc0 = -sqrt(ph.gam * p * r1);
+  c.am0 = p + c.roc0 * c.qn;
+}
+
+// one Newton sweep of clidd.f90:96-113 on one cell; returns resi
+__device__ __forceinline__ double idd_sweep(const Phys& ph, IddCell& c) {
+  const double gam6 = ph.gam / ph.gam1;
+  const double gamt = ph.gam / sq(ph.aa1);
+  const double gam2t = 0.5 * ph.gam1 / sq(ph.aa1);
+  const double b = 1. / (1. + gam2t / c.rti * c.usdn2 * sq(c.qn + c.un));
+  const double p = ph.pa1 * c.rpi * pow(b, gam6);
+  const double ro = gamt * p / (b * c.rti);
+  const double f = p + c.roc0 * c.qn - c.am0;
+  const double df = c.roc0 - ro * (c.qn + c.un) * c.usdn2;
+  const double dqn = -f / df;
+  const double resi = fabs(dqn) / c.qn;
+  c.qn = c.qn + dqn;
+  return resi;
+}
+
+__global__ void __launch_bounds__(256) k_clidd_mask(Bnd bd, Phys ph, const long long* ents,
+                                                   long long nent, const double* v,
+                                                   long long ld, unsigned* masks) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nent) return;
+  const long long e = ents[q];
+  IddCell c;
+  idd_setup(bd, ph, v, ld, e, c);
+  unsigned bits = 0u;
+  for (int t = 0; t < 20; ++t) {
+    const double resi = idd_sweep(ph, c);
+    if (resi > 0.0000001) bits |= 1u << t;
+  }
+  atomicOr(&masks[bd.ent_bnd[e]], bits);
+}
+
+__global__ void __launch_bounds__(256) k_clidd_apply(Bnd bd, Phys ph, const long long* ents,
+                                                    long long nent, double* v, long long ld,
+                                                    double* ps_, double* temp, double* cson,
+                                                    const unsigned* masks) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nent) return;
+  const long long e = ents[q], nl = bd.nlist, nc = bd.ncbd[e];
+  const unsigned bits = masks[bd.ent_bnd[e]];
+  int nsweep = 20;
+  for (int t = 0; t < 20; ++t)
+    if (!(bits & (1u << t))) {
+      nsweep = t + 1;
+      break;
+    }
+  IddCell c;
+  idd_setup(bd, ph, v, ld, e, c);
+  for (int t = 0; t < nsweep; ++t) idd_sweep(ph, c);
   const double gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl, omg = ph.omg;
   const double gam6 = gam / gam1;
   const double gamt = gam / sq(ph.aa1);
   const double gam2t = 0.5 * gam1 / sq(ph.aa1);
-  const long long nl = bd.nlist;
-  double* qn_ = scratch + m0;                // per entry Newton iterate
-  double* roc0_ = scratch + nl + m0;
-  double* am0_ = scratch + 2 * nl + m0;
-  for (int m = threadIdx.x; m < mt; m += blockDim.x) {
-    const long long e = m0 + m, ni = bd.ncin[e];
-    const double d0x = bd.bceqt[2 * nl + e], d0y = bd.bceqt[3 * nl + e],
-                 d0z = bd.bceqt[4 * nl + e];
-    const double nx = bd.nxn[e], ny = bd.nyn[e], nz = bd.nzn[e];
-    const double r1 = v[ni], r2 = v[ld + ni], r3 = v[2 * ld + ni], r4 = v[3 * ld + ni];
-    const double qxs = r2 / r1, qys = r3 / r1, qzs = r4 / r1;
-    const double qn = qxs * nx + qys * ny + qzs * nz;
-    const double p = gam1 * (v[4 * ld + ni] - 0.5 * (qxs * r2 + qys * r3 + qzs * r4) - pinfl);
-    const double roc0 = -sqrt(gam * p * r1);
-    qn_[m] = qn;
-    roc0_[m] = roc0;
-    am0_[m] = p + roc0 * qn;
-    (void)d0x; (void)d0y; (void)d0z;
-  }
-  __syncthreads();
-  int nitn = 0;
-  double residu = 1.;
-  while (residu > eps && nitn < 20) {
-    double rmax = 0.;
-    for (int m = threadIdx.x; m < mt; m += blockDim.x) {
-      const long long e = m0 + m;
-      const double rpi = bd.bceqt[e], rti = bd.bceqt[nl + e];
-      const double d0x = bd.bceqt[2 * nl + e], d0y = bd.bceqt[3 * nl + e],
-                   d0z = bd.bceqt[4 * nl + e];
-      const double nx = bd.nxn[e], ny = bd.nyn[e], nz = bd.nzn[e];
-      const double usdn = 1. / (d0x * nx + d0y * ny + d0z * nz);
-      const double usdn2 = sq(usdn);
-      const double un = omg * (bd.ym[e] * nz - bd.zm[e] * ny);
-      const double qn = qn_[m];
-      const double bb_ = 1. / (1. + gam2t / rti * usdn2 * sq(qn + un));
-      const double p = ph.pa1 * rpi * pow(bb_, gam6);
-      const double ro = gamt * p / (bb_ * rti);
-      const double f = p + roc0_[m] * qn - am0_[m];
-      const double df = roc0_[m] - ro * (qn + un) * usdn2;
-      const double dqn = -f / df;
-      const double resi = fabs(dqn) / qn;
-      qn_[m] = qn + dqn;
-      rmax = fmax(rmax, resi);
-    }
-    // block-wide maximum (exact, order independent)
-    for (int off = 16; off > 0; off >>= 1)
-      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rmax;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double r = 0.;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, red[w]);
-      residu_sh = r;
-    }
-    __syncthreads();
-    residu = residu_sh;
-    __syncthreads();
-    nitn = nitn + 1;
-  }
-  for (int m = threadIdx.x; m < mt; m += blockDim.x) {
-    const long long e = m0 + m, nc = bd.ncbd[e];
-    const double rpi = bd.bceqt[e], rti = bd.bceqt[nl + e];
-    const double d0x = bd.bceqt[2 * nl + e], d0y = bd.bceqt[3 * nl + e],
-                 d0z = bd.bceqt[4 * nl + e];
-    const double nx = bd.nxn[e], ny = bd.nyn[e], nz = bd.nzn[e];
-    const double ym = bd.ym[e], zm = bd.zm[e];
-    const double usdn = 1. / (d0x * nx + d0y * ny + d0z * nz);
-    const double usdn2 = sq(usdn);
-    const double un = omg * (ym * nz - zm * ny);
-    const double qn = qn_[m];
-    const double bb_ = 1. / (1. + gam2t / rti * usdn2 * sq(qn + un));
-    const double p = ph.pa1 * rpi * pow(bb_, gam6);
-    const double ro = gamt * p / (bb_ * rti);
-    const double wn = qn + un;
-    const double w = wn * usdn;
-    const double m2 = ro * (w * d0x);
-    const double m3 = ro * (w * d0y + zm * omg);
-    const double m4 = ro * (w * d0z - ym * omg);
-    v[nc] = ro;
-    v[ld + nc] = m2;
-    v[2 * ld + nc] = m3;
-    v[3 * ld + nc] = m4;
-    v[4 * ld + nc] = p / gam1 + pinfl + 0.5 * (sq(m2) + sq(m3) + sq(m4)) / ro;
-    ps_[nc] = p;
-    const double tt = gam * p / ro;
-    temp[nc] = tt;
-    cson[nc] = sqrt(tt);
-  }
+  const double d0x = bd.bceqt[2 * nl + e], d0y = bd.bceqt[3 * nl + e],
+               d0z = bd.bceqt[4 * nl + e];
+  const double ym = bd.ym[e], zm = bd.zm[e];
+  const double b = 1. / (1. + gam2t / c.rti * c.usdn2 * sq(c.qn + c.un));
+  const double p = ph.pa1 * c.rpi * pow(b, gam6);
+  const double ro = gamt * p / (b * c.rti);
+  const double wn = c.qn + c.un;
+  const double w = wn * c.usdn;
+  const double m2 = ro * (w * d0x);
+  const double m3 = ro * (w * d0y + zm * omg);
+  const double m4 = ro * (w * d0z - ym * omg);
+  v[nc] = ro;
+  v[ld + nc] = m2;
+  v[2 * ld + nc] = m3;
+  v[3 * ld + nc] = m4;
+  v[4 * ld + nc] = p / gam1 + pinfl + 0.5 * (sq(m2) + sq(m3) + sq(m4)) / ro;
+  ps_[nc] = p;
+  const double tt = gam * p / ro;
+  temp[nc] = tt;
+  cson[nc] = sqrt(tt);
 }
 
 // rbte.f90:15-31 (non-coincident boundaries: copy of the interior cell) and
@@ -332,6 +350,7 @@ __global__ void __launch_bounds__(256) k_tau_ghosts(Bnd bd, double* tau, long lo
 __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
                                                 Space sp, Phys ph,
                                                 const double* __restrict__ s,
+                                                const double* __restrict__ prim,
                                                 long long ld,
                                                 const double* __restrict__ mu,
                                                 const double* __restrict__ mut,
@@ -346,8 +365,8 @@ __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
   double g[12];
 #pragma unroll
   for (int a = 0; a < 12; ++a) g[a] = 0.;
-  const double r0 = s[n];
-  const double fc[4] = {s[ld + n] / r0, s[2 * ld + n] / r0, s[3 * ld + n] / r0, temp[n]};
+  (void)s;
+  const double fc[4] = {prim[n], prim[ld + n], prim[2 * ld + n], temp[n]};
   // directions in the reference's order: k faces, then j, then i
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi) {
@@ -358,9 +377,8 @@ __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
     const double *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
                  *s2 = sn_ptr(sn, B, dir, 2);
     const long long nl = n - inc, nu = n + inc;
-    const double rl = s[nl], ru = s[nu];
-    const double fl[4] = {s[ld + nl] / rl, s[2 * ld + nl] / rl, s[3 * ld + nl] / rl, temp[nl]};
-    const double fu[4] = {s[ld + nu] / ru, s[2 * ld + nu] / ru, s[3 * ld + nu] / ru, temp[nu]};
+    const double fl[4] = {prim[nl], prim[ld + nl], prim[2 * ld + nl], temp[nl]};
+    const double fu[4] = {prim[nu], prim[ld + nu], prim[2 * ld + nu], temp[nu]};
     const double sl[3] = {s0[n], s1[n], s2[n]};
     const double su[3] = {s0[nu], s1[nu], s2[nu]};
     const bool lower_bnd = (p == 1), upper_bnd = (p + 1 == nd);
@@ -419,48 +437,43 @@ __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
 
 // slope-ratio recurrence of sch_roe.f90:146-194 along one grid line: the
 // ratio at face m divides by the ALREADY UPDATED ratio at face m-1, with a
-// reset to 1 when |r(m-1) r(m) r(m+1)| <= tiny.  One thread walks one line.
+// reset to 1 when |r(m-1) r(m) r(m+1)| <= tiny.  One thread walks one line
+// for one of the five variables (blockIdx.y: rho, u, v, w, p); lines of the
+// j and k directions are adjacent in i, so those walks are coalesced.
 __global__ void __launch_bounds__(kTile) k_ratio(const Blk* __restrict__ blks,
                                                  Space sp, int dir,
                                                  const double* __restrict__ v,
+                                                 const double* __restrict__ prim,
                                                  long long ld,
                                                  const double* __restrict__ ps,
                                                  double* __restrict__ R) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
-  const long long inc = ninc_of(B, dir);
   const int nd = nd_of(B, dir);
-  // (i,j,k) has the line position 1 on axis dir
-  const long long n1 = cell_index(B, i, j, k);
-  double* Rd = R + (long long)dir * 5 * ld;
-  // differences at faces 1 and 2
-  auto delta = [&](long long n, double out[5]) {
-    const double a = v[n], c = v[n - inc];
-    out[0] = a - c;
-    out[1] = v[ld + n] / a - v[ld + n - inc] / c;
-    out[2] = v[2 * ld + n] / a - v[2 * ld + n - inc] / c;
-    out[3] = v[3 * ld + n] / a - v[3 * ld + n - inc] / c;
-    out[4] = ps[n] - ps[n - inc];
-  };
   if (nd < 3) return;
-  double rprev[5], dcur[5], dnext[5];
-  delta(n1, rprev);
-  delta(n1 + inc, dcur);
+  const long long inc = ninc_of(B, dir);
+  const int a = blockIdx.y;
+  const double* x = a == 0 ? v : (a == 4 ? ps : prim + (long long)(a - 1) * ld);
+  double* Ra = R + ((long long)dir * 5 + a) * ld;
+  // (i,j,k) is position 1 of the line: cells 0 .. nd along dir
+  const long long n0 = cell_index(B, i, j, k) - inc;
+  double x0 = x[n0], x1 = x[n0 + inc], x2 = x[n0 + 2 * inc];
+  double rprev = x1 - x0;   // face 1 (never updated)
+  double dcur = x2 - x1;    // face 2
   for (int f = 2; f <= nd - 1; ++f) {
-    const long long n = n1 + (long long)(f - 1) * inc;
-    delta(n + inc, dnext);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      double r;
-      if (fabs(rprev[a] * dcur[a] * dnext[a]) <= 2.2250738585072014e-308)
-        r = 1.;
-      else
-        r = dcur[a] / rprev[a];
-      Rd[a * ld + n] = r;
-      rprev[a] = r;
-      dcur[a] = dnext[a];
-    }
+    const long long n = n0 + (long long)f * inc;
+    const double x3 = x[n + inc];
+    const double dnext = x3 - x2;
+    double r;
+    if (fabs(rprev * dcur * dnext) <= 2.2250738585072014e-308)
+      r = 1.;
+    else
+      r = dcur / rprev;
+    Ra[n] = r;
+    rprev = r;
+    dcur = dnext;
+    x2 = x3;
   }
 }
 
@@ -628,14 +641,14 @@ __device__ __forceinline__ void roe_dissipation(const double WL[5],
 
 // primitive (rho, u, v, w, p) of cell n
 __device__ __forceinline__ void load_prim(const double* __restrict__ v,
+                                          const double* __restrict__ prim,
                                           const double* __restrict__ ps,
                                           long long ld, long long n,
                                           double c[5]) {
-  const double r = v[n];
-  c[0] = r;
-  c[1] = v[ld + n] / r;
-  c[2] = v[2 * ld + n] / r;
-  c[3] = v[3 * ld + n] / r;
+  c[0] = v[n];
+  c[1] = prim[n];
+  c[2] = prim[ld + n];
+  c[3] = prim[2 * ld + n];
   c[4] = ps[n];
 }
 
@@ -644,11 +657,12 @@ __device__ __forceinline__ void load_prim(const double* __restrict__ v,
 // (lower face 1, upper face nd).  Results go to G[dir][a][n] where n is the
 // cell above the face.
 template <bool NS>
-__global__ void __launch_bounds__(kTile) k_face_flux(
+__global__ void __launch_bounds__(kTile, 3) k_face_flux(
     const Blk* __restrict__ blks, Space sp, int dir, Phys ph, Scheme sc,
-    const double* __restrict__ v, long long ld, const double* __restrict__ ps,
-    const double* __restrict__ tau, const double* __restrict__ sn,
-    const double* __restrict__ R, double* __restrict__ G) {
+    const double* __restrict__ v, const double* __restrict__ prim, long long ld,
+    const double* __restrict__ ps, const double* __restrict__ tau,
+    const double* __restrict__ sn, const double* __restrict__ R,
+    double* __restrict__ G) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -668,15 +682,16 @@ __global__ void __launch_bounds__(kTile) k_face_flux(
     const long long nrho = (!NS && p == 1 && dir > 0) ? n : ng;
     const double v1 = v[ng], v2 = v[ld + ng], v3 = v[2 * ld + ng],
                  v4 = v[3 * ld + ng], v5 = v[4 * ld + ng], pg = ps[ng];
+    const double qu = prim[ng], qv = prim[ld + ng], qw = prim[2 * ld + ng];
     double fxx, fxy, fxz, fyy, fyz, fzz, fex, fey, fez;
     if (!NS) {
       const double rr = v[nrho];
-      fxx = v2 * (v2 / v1) + pg - pinfl;
-      fxy = v3 * (v2 / v1);
-      fxz = v4 * (v2 / v1);
-      fyy = v3 * (v3 / v1) + pg - pinfl;
-      fyz = v4 * (v3 / v1);
-      fzz = v4 * (v4 / v1) + pg - pinfl;
+      fxx = v2 * qu + pg - pinfl;
+      fxy = v3 * qu;
+      fxz = v4 * qu;
+      fyy = v3 * qv + pg - pinfl;
+      fyz = v4 * qv;
+      fzz = v4 * qw + pg - pinfl;
       fex = (v5 + pg - pinfl) * v2 / rr;
       fey = (v5 + pg - pinfl) * v3 / rr;
       fez = (v5 + pg - pinfl) * v4 / rr;
@@ -685,12 +700,12 @@ __global__ void __launch_bounds__(kTile) k_face_flux(
                    tyy = tau[3 * ld + ng], tyz = tau[4 * ld + ng],
                    tzz = tau[5 * ld + ng], qx = tau[6 * ld + ng],
                    qy = tau[7 * ld + ng], qz = tau[8 * ld + ng];
-      fxx = v2 * (v2 / v1) + pg - pinfl - txx;
-      fxy = v3 * (v2 / v1) - txy;
-      fxz = v4 * (v2 / v1) - txz;
-      fyy = v3 * (v3 / v1) + pg - pinfl - tyy;
-      fyz = v4 * (v3 / v1) - tyz;
-      fzz = v4 * (v4 / v1) + pg - pinfl - tzz;
+      fxx = v2 * qu + pg - pinfl - txx;
+      fxy = v3 * qu - txy;
+      fxz = v4 * qu - txz;
+      fyy = v3 * qv + pg - pinfl - tyy;
+      fyz = v4 * qv - tyz;
+      fzz = v4 * qw + pg - pinfl - tzz;
       fex = ((v5 + pg - pinfl - txx) * v2 - txy * v3 - txz * v4) / v1 - qx;
       fey = ((v5 + pg - pinfl - tyy) * v3 - txy * v2 - tyz * v4) / v1 - qy;
       fez = ((v5 + pg - pinfl - tzz) * v4 - txz * v2 - tyz * v3) / v1 - qz;
@@ -703,7 +718,7 @@ __global__ void __launch_bounds__(kTile) k_face_flux(
   } else {
     double c[4][5];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) load_prim(v, ps, ld, n + (long long)(s - 2) * inc, c[s]);
+    for (int s = 0; s < 4; ++s) load_prim(v, prim, ps, ld, n + (long long)(s - 2) * inc, c[s]);
     double WL[5], WR[5];
     const double c4 = 0.25 * sc.muscl;
     if (NS && sc.ilim == 1 && p <= nd - 2) {
@@ -835,7 +850,8 @@ __global__ void __launch_bounds__(kTile) k_impl_cell0(
 // implimf_3d.f90:110-190)
 __global__ void __launch_bounds__(kTile) k_impl_coefe(
     const Blk* __restrict__ blks, Space sp, int dir, int eu,
-    const double* __restrict__ v, long long ld, const double* __restrict__ sn,
+    const double* __restrict__ v, const double* __restrict__ prim, long long ld,
+    const double* __restrict__ sn,
     const double* __restrict__ vol, const double* __restrict__ cson,
     const double* __restrict__ rv, double* coefe) {
   int b, i, j, k;
@@ -855,9 +871,9 @@ __global__ void __launch_bounds__(kTile) k_impl_coefe(
     const double ww = 0.5 * (v[3 * ld + n] * norm + v[3 * ld + nl] * norm1);
     ce = 0.5 * (fabs(uu * sx + vv * sy + ww * sz)) + sqrt(cnds) * cc;
   } else {
-    const double uu = 0.5 * (v[ld + n] / v[n] + v[ld + nl] / v[nl]);
-    const double vv = 0.5 * (v[2 * ld + n] / v[n] + v[2 * ld + nl] / v[nl]);
-    const double ww = 0.5 * (v[3 * ld + n] / v[n] + v[3 * ld + nl] / v[nl]);
+    const double uu = 0.5 * (prim[n] + prim[nl]);
+    const double vv = 0.5 * (prim[ld + n] + prim[ld + nl]);
+    const double ww = 0.5 * (prim[2 * ld + n] + prim[2 * ld + nl]);
     const double vn = uu * sx + vv * sy + ww * sz;
     ce = 0.5 * (fabs(vn) + sqrt(cnds) * cc) + (rv[n] + rv[nl]) * cnds / (vol[n] + vol[nl]);
   }
@@ -935,6 +951,7 @@ template <bool EU, bool FIRST>
 __global__ void __launch_bounds__(kTile) k_jacobi(
     const Blk* __restrict__ blks, Space sp, Phys ph, int qfix, long long ld,
     const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ prim,
     const double* __restrict__ ps, const double* __restrict__ sn,
     const double* __restrict__ coefe, const double* __restrict__ coefdiag,
     const double* __restrict__ d_in, const double* __restrict__ df_in,
@@ -1008,12 +1025,13 @@ __global__ void __launch_bounds__(kTile) k_jacobi(
     const double ui = (v2 + dn[1]) / wi1, vi = (v3 + dn[2]) / wi1, wi = (v4 + dn[3]) / wi1;
     const double wi5 = v5 + dn[4];
     const double pres = gam1 * (wi5 - .5 * wi1 * (sq(ui) + sq(vi) + sq(wi)) - pinfl);
-    const double fxx = v2 * (v2 / v1) + p;
-    const double fxy = v3 * (v2 / v1);
-    const double fxz = v4 * (v2 / v1);
-    const double fyy = v3 * (v3 / v1) + p;
-    const double fyz = v4 * (v3 / v1);
-    const double fzz = v4 * (v4 / v1) + p;
+    const double qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
+    const double fxx = v2 * qu + p;
+    const double fxy = v3 * qu;
+    const double fxz = v4 * qu;
+    const double fyy = v3 * qv + p;
+    const double fyz = v4 * qv;
+    const double fzz = v4 * qw + p;
     const double fex = (v5 + p - pinfl) * v2 / v1;
     const double fey = (v5 + p - pinfl) * v3 / v1;
     const double fez = (v5 + p - pinfl) * v4 / v1;
@@ -1192,6 +1210,13 @@ cudaError_t launch_zvismo(const Blk* blks, Space sp, Phys ph, double* mu,
   return cudaGetLastError();
 }
 
+cudaError_t launch_prim(long long n0, long long n1, const double* v, long long ld,
+                        double* prim, cudaStream_t st) {
+  if (n1 > n0)
+    k_prim<<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(n0, n1, v, ld, prim);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
                            const double* mu, const double* mut, const double* v,
                            long long ld, double* dt, const double* sn,
@@ -1203,12 +1228,18 @@ cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
 }
 
 cudaError_t launch_rbord(const Bnd& bd, Phys ph, double* v, long long ld,
-                         double* ps, double* temp, double* cson, int n_idd,
-                         const int* idd_list, double* scratch, cudaStream_t st) {
+                         double* ps, double* temp, double* cson, long long n_idd_ent,
+                         const long long* idd_ents, unsigned* masks, cudaStream_t st) {
   if (bd.nlist > 0)
     k_rbord<<<(int)((bd.nlist + 255) / 256), 256, 0, st>>>(bd, ph, v, ld, ps, temp, cson);
-  if (n_idd > 0)
-    k_clidd<<<n_idd, 256, 0, st>>>(bd, ph, idd_list, v, ld, ps, temp, cson, scratch);
+  if (n_idd_ent > 0) {
+    cudaError_t e = cudaMemsetAsync(masks, 0, sizeof(unsigned) * bd.nbnd, st);
+    if (e != cudaSuccess) return e;
+    const int g = (int)((n_idd_ent + 255) / 256);
+    k_clidd_mask<<<g, 256, 0, st>>>(bd, ph, idd_ents, n_idd_ent, v, ld, masks);
+    k_clidd_apply<<<g, 256, 0, st>>>(bd, ph, idd_ents, n_idd_ent, v, ld, ps, temp, cson,
+                                     masks);
+  }
   return cudaGetLastError();
 }
 
@@ -1220,40 +1251,40 @@ cudaError_t launch_tau_ghosts(const Bnd& bd, double* tau, long long ld,
 }
 
 cudaError_t launch_grad(const Blk* blks, Space sp, Phys ph, const double* v,
-                        long long ld, const double* mu, const double* mut,
-                        double* tau, const double* sn, const double* vol,
-                        const double* temp, cudaStream_t st) {
+                        const double* prim, long long ld, const double* mu,
+                        const double* mut, double* tau, const double* sn,
+                        const double* vol, const double* temp, cudaStream_t st) {
   if (sp.ntiles > 0)
-    k_grad<<<grid_of(sp), kTile, 0, st>>>(blks, sp, ph, v, ld, mu, mut, tau, sn,
+    k_grad<<<grid_of(sp), kTile, 0, st>>>(blks, sp, ph, v, prim, ld, mu, mut, tau, sn,
                                           vol, temp);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
-                         const double* v, long long ld, const double* ps,
-                         double* R, cudaStream_t st) {
+                         const double* v, const double* prim, long long ld,
+                         const double* ps, double* R, cudaStream_t st) {
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = lines[dir].view(l0);
     if (sp.ntiles > 0)
-      k_ratio<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, v, ld, ps, R);
+      k_ratio<<<dim3(grid_of(sp), 5), kTile, 0, st>>>(blks, sp, dir, v, prim, ld, ps, R);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
-                             Phys ph, Scheme sc, const double* v, long long ld,
-                             const double* ps, const double* tau,
-                             const double* sn, const double* R, double* G,
-                             cudaStream_t st) {
+                             Phys ph, Scheme sc, const double* v,
+                             const double* prim, long long ld, const double* ps,
+                             const double* tau, const double* sn, const double* R,
+                             double* G, cudaStream_t st) {
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = faces[dir].view(l0);
     if (sp.ntiles == 0) continue;
     if (sc.ns)
-      k_face_flux<true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, ld,
-                                                       ps, tau, sn, R, G);
+      k_face_flux<true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                       ld, ps, tau, sn, R, G);
     else
-      k_face_flux<false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, ld,
-                                                        ps, tau, sn, R, G);
+      k_face_flux<false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                        ld, ps, tau, sn, R, G);
   }
   return cudaGetLastError();
 }
@@ -1271,6 +1302,7 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
                             const double* sn, const double* vol,
                             const double* ps, const double* cson, Work& w,
                             int want_norms, cudaStream_t st) {
+  const double* prim = w.prim;
   const long long ld = w.ld;
   if (cells.ntiles == 0) return cudaSuccess;
   const int g = grid_of(cells);
@@ -1279,8 +1311,8 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
   for (int dir = 0; dir < 3; ++dir) {
     const Space fs = faces[dir].view(l0);
     if (fs.ntiles > 0)
-      k_impl_coefe<<<fs.ntiles, kTile, 0, st>>>(blks, fs, dir, eu, v, ld, sn, vol,
-                                                cson, w.rv, w.coefe);
+      k_impl_coefe<<<fs.ntiles, kTile, 0, st>>>(blks, fs, dir, eu, v, prim, ld, sn,
+                                                vol, cson, w.rv, w.coefe);
   }
   k_impl_diag<<<g, kTile, 0, st>>>(blks, cells, ld, w.coefe, w.coefdiag);
   int cur = 0;  // index of the buffer holding the latest iterate
@@ -1297,19 +1329,19 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
     if (eu) {
       if (ls == 1)
         k_jacobi<true, true><<<g, kTile, 0, st>>>(blks, cells, ph, sc.qfix_dfez, ld, u, v,
-                                                  ps, sn, w.coefe, w.coefdiag, din,
+                                                  prim, ps, sn, w.coefe, w.coefdiag, din,
                                                   dfin, dout, dfout);
       else
         k_jacobi<true, false><<<g, kTile, 0, st>>>(blks, cells, ph, sc.qfix_dfez, ld, u, v,
-                                                   ps, sn, w.coefe, w.coefdiag, din,
+                                                   prim, ps, sn, w.coefe, w.coefdiag, din,
                                                    dfin, dout, dfout);
     } else {
       if (ls == 1)
-        k_jacobi<false, true><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, ps,
+        k_jacobi<false, true><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, prim, ps,
                                                    sn, w.coefe, w.coefdiag, din,
                                                    dfin, dout, dfout);
       else
-        k_jacobi<false, false><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, ps,
+        k_jacobi<false, false><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, prim, ps,
                                                     sn, w.coefe, w.coefdiag, din,
                                                     dfin, dout, dfout);
     }

@@ -44,6 +44,7 @@ struct SpaceBuf {
 // per-step scratch (device)
 struct Work {
   long long ld = 0;
+  double* prim = nullptr;     // primitive velocities u, v, w, [3][ld]
   double* G = nullptr;        // face fluxes, [3][5][ld]
   double* R = nullptr;        // limiter ratios, [3][5][ld]
   double* coefe = nullptr;    // [3][ld]
@@ -74,27 +75,32 @@ cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
                            const double* vol, const double* cson,
                            cudaStream_t st);
 
+// rbord: every list entry, then the injection entries (two passes)
 cudaError_t launch_rbord(const Bnd& bd, Phys ph, double* v, long long ld,
-                         double* ps, double* temp, double* cson, int n_idd,
-                         const int* idd_list, double* scratch, cudaStream_t st);
+                         double* ps, double* temp, double* cson, long long n_idd_ent,
+                         const long long* idd_ents, unsigned* masks, cudaStream_t st);
 
 cudaError_t launch_tau_ghosts(const Bnd& bd, double* tau, long long ld,
                               cudaStream_t st);
 
+// primitive velocities of the flat cell range [n0, n1)
+cudaError_t launch_prim(long long n0, long long n1, const double* v, long long ld,
+                        double* prim, cudaStream_t st);
+
 cudaError_t launch_grad(const Blk* blks, Space sp, Phys ph, const double* v,
-                        long long ld, const double* mu, const double* mut,
-                        double* tau, const double* sn, const double* vol,
-                        const double* temp, cudaStream_t st);
+                        const double* prim, long long ld, const double* mu,
+                        const double* mut, double* tau, const double* sn,
+                        const double* vol, const double* temp, cudaStream_t st);
 
 cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
-                         const double* v, long long ld, const double* ps,
-                         double* R, cudaStream_t st);
+                         const double* v, const double* prim, long long ld,
+                         const double* ps, double* R, cudaStream_t st);
 
 cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
-                             Phys ph, Scheme sc, const double* v, long long ld,
-                             const double* ps, const double* tau,
-                             const double* sn, const double* R, double* G,
-                             cudaStream_t st);
+                             Phys ph, Scheme sc, const double* v,
+                             const double* prim, long long ld, const double* ps,
+                             const double* tau, const double* sn, const double* R,
+                             double* G, cudaStream_t st);
 
 cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
                               long long ld, double* u, cudaStream_t st);

@@ -30,7 +30,7 @@ static struct {
   /* proprieteflu / definition */
   double gam, gam1, pinfl, pr, prt, cp, reynz, suth_a, pa1, aa1, omg;
   /* schemanum */
-  int ns, muscl, ilim, kdtl, lmax;
+  int ns, muscl, ilim, kdtl, lmax, qfix_dfez;
   double xk, eta, dt1min;
   /* boundary */
   int nbnd;
@@ -111,7 +111,8 @@ void orc_set_phys(double gam, double pinfl, double pr, double prt,
 }
 
 void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
-                    int kdtl, double dt1min, int lmax) {
+                    int kdtl, double dt1min, int lmax, int qfix_dfez) {
+  G.qfix_dfez = qfix_dfez;
   G.ns = ns;
   G.muscl = muscl;
   G.xk = xk;
@@ -1444,8 +1445,10 @@ void orc_implimf_eu(int l, const double *u, const double *dt, double *v,
           w.df[DEY][m] = wi1 * vi * (wi5 + pres - pinfl) - fey;
           w.df[DZZ][m] = wi1 * sq(wi) + pres - fzz;
           /* implimf_eu.f90:312: the *wi factor of the z energy flux is
-           * missing in the reference and is reproduced here */
-          w.df[DEZ][m] = wi1 * (wi5 + pres - pinfl) - fez;
+           * missing in the reference and is reproduced here unless the
+           * flagged non-reference option asks for it */
+          w.df[DEZ][m] = G.qfix_dfez ? wi1 * wi * (wi5 + pres - pinfl) - fez
+                                     : wi1 * (wi5 + pres - pinfl) - fez;
         }
   }
   for (int k = 1; k <= b->nk - 1; ++k)

@@ -46,8 +46,10 @@ int64_t orc_ncells(void);
 void orc_set_phys(double gam, double pinfl, double pr, double prt,
                   double reynz, double suth_a, double pa1, double aa1,
                   double omg);
+/* qfix_dfez: non-reference option restoring the *wi factor missing from
+ * implimf_eu.f90:312 (0 keeps the reference behaviour) */
 void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
-                    int kdtl, double dt1min, int lmax);
+                    int kdtl, double dt1min, int lmax, int qfix_dfez);
 
 /* boundaries: per boundary b: type, block (1-based), face (0..5 = i1,i2,j1,j2,
  * k1,k2), first list entry mpb and count mmb, partner boundary (RC) and the

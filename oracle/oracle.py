@@ -36,7 +36,7 @@ def lib():
         L.orc_setup.restype = C.c_int
         L.orc_set_phys.argtypes = [C.c_double] * 9
         L.orc_set_scheme.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int,
-                                     C.c_double, C.c_int, C.c_double, C.c_int]
+                                     C.c_double, C.c_int, C.c_double, C.c_int, C.c_int]
         L.orc_set_boundaries.argtypes = [C.c_int, _i32, _i32, _i32, _i64, _i32,
                                          _i32, _d, _d, C.c_int64, _i64, _i64, _d]
         L.orc_metric.argtypes = [_d] * 5
@@ -107,7 +107,7 @@ class Oracle:
 
     def set_scheme(self, s):
         lib().orc_set_scheme(s.ns, s.muscl, s.xk, s.ilim, s.eta, s.kdtl,
-                             s.dt1min, s.lmax)
+                             s.dt1min, s.lmax, int(getattr(s, "qfix_dfez", 0)))
 
     def metric(self, st: OracleState):
         lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)

@@ -17,7 +17,10 @@ SMALL = {
     # config-2 form: laminar bump channel, 3 blocks, idd/prd/para/rc
     "channel": lambda: cases.channel_case([9, 6, 7], 8, 5, seed=13, reynz=1.0e3),
     # config-4 form: independent boxes in one layout
-    "batch": lambda: cases.batch_case(ncase=4, side=(3, 9), seed=14),
+    "batch": lambda: cases.batch_case(ncase=4, side=(3, 9), seed=14, qfix_dfez=1),
+    # Euler with the flagged non-reference fix of implimf_eu.f90:312
+    "box_eu_qfix": lambda: cases.box_case((12, 7, 6), seed=16, skew=0.02, alpha=2.0,
+                                          qfix_dfez=1),
     # stiffened gas (pinfl != 0) exercises every pinfl term
     "box_pinfl": lambda: cases.box_case((8, 6, 5), seed=15, ns=True, ilim=1, pinfl=0.3,
                                         reynz=500.0, skew=0.01),
@@ -43,6 +46,15 @@ def max_rel(a, b):
     den = np.maximum(np.abs(a), np.abs(b))
     den[den == 0] = 1.0
     return float(np.max(np.abs(a - b) / den)) if a.size else 0.0
+
+
+def max_rel_cols(a, b):
+    """largest difference of each component relative to that component's
+    largest magnitude (a state comparison insensitive to near-zero entries)"""
+    a = np.asarray(a).reshape(a.shape[0], -1)
+    b = np.asarray(b).reshape(b.shape[0], -1)
+    scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), 1e-300)
+    return float((np.abs(a - b) / scale).max())
 
 
 def assert_equal_bits(a, b, what):

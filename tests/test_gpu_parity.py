@@ -11,7 +11,7 @@ import pytest
 from codens_b200 import cases
 from oracle.oracle import lib as orc_lib
 
-from ._helpers import SMALL, assert_equal_bits, max_rel, oracle_prepared, real
+from ._helpers import SMALL, assert_equal_bits, max_rel, max_rel_cols, oracle_prepared, real
 
 pytestmark = pytest.mark.gpu
 
@@ -83,7 +83,7 @@ def test_zpres_zvismo_chronos_rbord(cuda, name):
     v_g = _n(s.v).reshape(5, -1)[:, g]
     v_o = st.v.reshape(5, -1)[:, g]
     if has_idd:
-        assert max_rel(v_g, v_o) <= 1e-13
+        assert max_rel_cols(v_g, v_o) <= 1e-13
         assert max_rel(_n(s.pression)[g], st.ps[g]) <= 1e-13
     else:
         assert_equal_bits(v_g, v_o, "ghost v")
@@ -202,11 +202,14 @@ def test_implicit_parity(cuda, name, lmx):
     s.close()
 
 
-@pytest.mark.parametrize("name,nsteps", [("box_eu", 4), ("box_ns", 6), ("channel", 6),
-                                         ("batch", 4), ("box_pinfl", 5)])
+@pytest.mark.parametrize("name,nsteps", [("box_eu", 2), ("box_ns", 6), ("channel", 6),
+                                         ("batch", 6), ("box_pinfl", 5),
+                                         ("box_eu_qfix", 8)])
 def test_fused_steps_parity(cuda, name, nsteps):
     """the graph-captured iteration against the oracle's atsch_num sequence,
-    state and L2 history after several iterations"""
+    state and L2 history after several iterations (the reference Euler form
+    diverges after a few iterations because of implimf_eu.f90:312, so its
+    cases run two)"""
     case = SMALL[name]()
     orc, st = oracle_prepared(case)
     s = _gpu(case)
@@ -221,7 +224,7 @@ def test_fused_steps_parity(cuda, name, nsteps):
         v_g = _n(s.v).reshape(5, ld)[:, rc]
         v_o = st.v.reshape(5, ld)[:, rc]
         if has_idd:
-            assert max_rel(v_g, v_o) <= 1e-12, f"step {it}"
+            assert max_rel_cols(v_g, v_o) <= 1e-12, f"step {it}"
         else:
             assert_equal_bits(v_g, v_o, f"v after step {it}")
         np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0, err_msg=f"norms step {it}")
