@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcodens_b200.so")
-SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_abi.cu"]
+SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_abi.cu", "cns_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [

@@ -186,6 +186,26 @@ int cns_last_norms(cns_ctx *ctx, double *norms);
 int cns_atsch_num_step_host(cns_ctx *ctx, double *v_host, int nsteps,
                             double *norms);
 
+/* ---- no-allocation variant -------------------------------------------- */
+/* No counterpart in the reference.  The Euler Roe residual of ONE block
+ * (what cns_sch_roe_euler(ctx, 1, ...) computes for a layout of a single
+ * block starting at offset 0), for callers that cannot let the library
+ * allocate device memory -- a driver that owns every device array in its own
+ * pre-sized pool or runs under a hard memory cap.  Needs no context: the
+ * intermediates live in a 20 MiB static device array that every GPU loading
+ * the library holds until exit, which limits ld to 131072 (larger calls
+ * return CNS_EINVAL and launch nothing).  The first call on a device looks up
+ * that array's address; make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race, so order them on one stream.
+ * ni, nj, nk: real node counts; ld: leading dimension of u, v; gam, pinfl,
+ * muscl, xk: as in cns_phys_t / cns_scheme_t; u, v, sn, ps: device arrays;
+ * stream: CUDA stream (NULL = legacy default stream). */
+int cns_sch_roe_euler_noalloc(int32_t ni, int32_t nj, int32_t nk, int64_t ld,
+                              double gam, double pinfl, int32_t muscl,
+                              double xk, double *u, const double *v,
+                              const double *sn, const double *ps,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif
