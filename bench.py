@@ -4,11 +4,17 @@
 One step = one pseudo-time iteration of the Roe-MUSCL / viscous residual and
 the matrix-free point-Jacobi implicit update over every block (atsch_num),
 graph-captured, on the laminar Navier-Stokes bump channel: 8 blocks of
-seeded uneven sizes (48..128 cells per side, ~4M cells), Mach 0.5, Re 1e4,
-minmod-limited MUSCL, lmax = 10 Jacobi sweeps, injection / outlet pressure /
+seeded uneven sizes (48..128 cells per side, ~4.4M cells), Mach 0.5, Re 1e4,
+kappa = -1 MUSCL, lmax = 10 Jacobi sweeps, injection / outlet pressure /
 adiabatic walls / periodic span and coincident inter-block joins handled on
 the device.  The state (~0.2 GB per field) is far larger than L2, so no L2
 flush is needed between steps.
+
+The headline value is the mixed form (FP64 residual, boundary conditions,
+update and norms; FP32 Jacobi sweeps), whose fixed point is the FP64 steady
+state; the plain FP64 iteration is timed in the same run beside it, and a
+small viscous box is converged in both forms to state the equal-error claim
+(`steady_state`).
 
 Arms:
   default            the CUDA path (device-resident state, CUDA events on the
@@ -35,10 +41,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-iters/s, mixed-prec vs FP64 GPU at equal L2 error; adjoint/primal cost"
 UNIT = "Mcell-iters/s"
-# algorithmic bytes per real cell (FP64): read W, S(3 faces), vol, write R
-# for the residual; read dW, W, S, R, vol and write dW per Jacobi sweep
+# algorithmic bytes per real cell: read W, S (3 owned faces), vol, write R
+# for the residual (FP64); read dW, W, S, R, vol and write dW per Jacobi
+# sweep, at the stored element size (FP64: 240 B, FP32: 120 B)
 BYTES_RESIDUAL = 160
-BYTES_JACOBI = 240
+BYTES_JACOBI = {"fp64": 240, "mixed": 120, "defect": 120}
+PRECISION = {"fp64": 0, "mixed": 1, "defect": 2}
+DTYPE = {"fp64": "f64", "mixed": "f64 residual/update, f32 sweeps",
+         "defect": "f32 fluxes/sweeps, f64 accumulate/update"}
+SWEEP_KERNEL = {"fp64": "k_jacobi<double> (point-Jacobi sweep, stored flux increments)",
+                "mixed": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)",
+                "defect": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)"}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -53,31 +66,44 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--small", action="store_true",
-                   help="a 3-block ~0.1M-cell channel (profiling, smoke runs)")
+                   help="a 3-block 1.18M-cell channel (profiling captures)")
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "defect"])
+    p.add_argument("--kdefect", type=int, default=4, help="defect form: FP64 refresh period")
+    p.add_argument("--no-fp64-arm", action="store_true",
+                   help="skip timing the plain FP64 iteration beside the mixed one")
+    p.add_argument("--no-steady-check", action="store_true")
+    p.add_argument("--ilim", type=int, default=0,
+                   help="0: plain kappa=-1 MUSCL (default: the reference's limiter "
+                        "recurrence stalls this channel at L2 ~1e-3); 1: minmod limiter")
     return p.parse_args()
 
 
 def make_case(args):
     from codens_b200 import cases
     if args.small:
-        case = cases.channel_case([40, 24, 32], 48, 40, seed=2)
+        case = cases.channel_case([64, 64, 64], 64, 96, seed=2)
     else:
         case = cases.channel_case(seed=2)
     case.scheme.lmax = args.lmax
+    case.scheme.ilim = args.ilim
+    case.scheme.precision = PRECISION[args.precision]
+    case.scheme.kdefect = args.kdefect
     return case
 
 
 def config_of(case, args, n):
     m = case.meta
     return {
-        "workload": "laminar NS bump channel, 8 uneven blocks, Roe-MUSCL minmod + viscous, "
-                    f"implicit point-Jacobi lmax={args.lmax}, FP64"
-        if not args.small else "small laminar NS bump channel (3 blocks)",
+        "workload": "laminar NS bump channel, 8 uneven blocks, Roe-MUSCL"
+                    f"{' minmod' if args.ilim else ''} + viscous, "
+                    f"implicit point-Jacobi lmax={args.lmax}, {args.precision}"
+        if not args.small else "laminar NS bump channel, 3 blocks of 64x64x96 cells",
         "cells": case.layout.nreal,
         "blocks": case.layout.nblk,
         "block_ni": m.get("ni"), "nj": m.get("nj"), "nk": m.get("nk"),
         "mach": m.get("mach"), "reynolds": m.get("reynz"), "seed": m.get("seed"),
-        "precision": "fp64",
+        "precision": args.precision,
+        "ilim": args.ilim,
         "l2_flush": "inputs larger than L2 (state and scratch ~GBs)",
         "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
     }
@@ -193,6 +219,77 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def _timed_steps(s, torch, steps):
+    """CUDA-event time of `steps` graph-launched iterations on the solver's
+    stream (ms), with the kernels they launched"""
+    s.sync()
+    k0 = s.kernels_launched
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(s.stream)
+    s.atsch_num_launch(steps)
+    b.record(s.stream)
+    b.synchronize()
+    return a.elapsed_time(b), s.kernels_launched - k0
+
+
+def _sweep_ms(s, torch, scheme, lmax, steps):
+    """one Jacobi sweep, timed live on the solver's stream as the difference
+    of the fused iteration with lmax sweeps and with none, over `steps`
+    iterations each (ms per sweep)"""
+    t_l, _ = _timed_steps(s, torch, steps)
+    scheme.lmax = 0
+    s.set_scheme(scheme)
+    s.atsch_num_launch(3)
+    t_0, _ = _timed_steps(s, torch, steps)
+    scheme.lmax = lmax
+    s.set_scheme(scheme)
+    s.atsch_num_launch(3)
+    return max((t_l - t_0) / steps / max(lmax, 1), 1e-9)
+
+
+def _residual_ms(s, torch, reps=5):
+    """the FP64 residual of every block (sch_roe / sch_roe_euler), ms"""
+    s.sync()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(s.stream)
+    for _ in range(reps):
+        if s.case.scheme.ns:
+            s.sch_roe(0, s.u, s.v, s.tau, s.sn, s.pression)
+        else:
+            s.sch_roe_euler(0, s.u, s.v, s.sn, s.pression)
+    b.record(s.stream)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def steady_state_check(iters=2400):
+    """converge a small viscous box in the FP64 and the selected reduced-
+    precision form; the largest component-relative state difference"""
+    import numpy as np
+    from codens_b200 import cases
+    from codens_b200.solver import CodeNS
+
+    out = {}
+    states = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        case = cases.box_case((8, 6, 5), seed=12, ns=True, ilim=0, reynz=100.0, skew=0.02)
+        case.scheme.precision = prec
+        s = CodeNS(case)
+        s.metric()
+        n = s.atsch_num(iters)
+        states[name] = s.v.cpu().numpy().reshape(5, case.layout.ld)[:, case.layout.real_cells()]
+        out[f"l2_rho_{name}"] = float(n[1, 0])
+        s.close()
+    a, r = states["mixed"], states["fp64"]
+    scale = np.maximum(np.abs(r).max(axis=1, keepdims=True), 1e-300)
+    out["err_vs_fp64"] = float((np.abs(a - r) / scale).max())
+    out["case"] = "viscous box 8x6x5 cells, Re 100, seed 12"
+    out["iters"] = iters
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -207,16 +304,21 @@ def run_ours(args):
         if ws > 1:
             dist.barrier()
 
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     from codens_b200.solver import CodeNS
 
     case = make_case(args)
     s = CodeNS(case, device=local)
     s.metric()
     nreal = case.layout.nreal
-    # warm-up (also instantiates the step graph)
-    s.atsch_num(max(args.warmup, 3))
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    warm = max(args.warmup, 3)
+    # warm-up (also instantiates the step graphs)
+    s.atsch_num(warm)
     prop = torch.cuda.get_device_properties(local)
     try:
         bus = "%08X:%02X:%02X.0" % (prop.pci_domain_id, prop.pci_bus_id, prop.pci_device_id)
@@ -226,57 +328,43 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    ev0.record(s.stream)
-    s.atsch_num_launch(args.steps)
-    ev1.record(s.stream)
-    ev1.synchronize()
+    ms, kernels = _timed_steps(s, torch, args.steps)
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier()
-    ms = ev0.elapsed_time(ev1)
     norms = s.last_norms()
-    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms = float(t_max.item())
+    ms = max_over_ranks(ms)
     value = ws * nreal * args.steps / (ms * 1e-3) / 1e6
-    launches_per_step = 15 + args.lmax + (3 if case.scheme.ilim else 0) + (
-        1 if any(b.kind == 4 for b in case.boundaries) else 0)
 
-    # dominant-kernel roofline: one Jacobi sweep, timed live on the solver's
-    # stream as (implicit phase with lmax sweeps - with 0 sweeps) / lmax
-    def time_implicit(lmx, reps=3):
-        s.sync()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(s.stream)
-        for _ in range(reps):
-            s.implimf_3d(0, s.u, s.dt, s.v, s.d, s.mu, s.mut, s.sn,
-                         s.vol, s.pression, s.cson, lmx)
-        b.record(s.stream)
-        b.synchronize()
-        return a.elapsed_time(b) / reps
+    # the plain FP64 iteration on the same solver, same step count
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64_arm:
+        sch = case.scheme
+        keep = sch.precision
+        sch.precision = 0
+        s.set_scheme(sch)
+        s.atsch_num(warm)
+        barrier()
+        ms64, _ = _timed_steps(s, torch, args.steps)
+        barrier()
+        ms64 = max_over_ranks(ms64)
+        fp64 = {"value": ws * nreal * args.steps / (ms64 * 1e-3) / 1e6,
+                "ms_per_step": ms64 / args.steps}
+        sch.precision = keep
+        s.set_scheme(sch)
+        s.atsch_num(warm)
 
-    def time_residual(reps=3):
-        s.sync()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(s.stream)
-        for _ in range(reps):
-            s.sch_roe(0, s.u, s.v, s.tau, s.sn, s.pression)
-        b.record(s.stream)
-        b.synchronize()
-        return a.elapsed_time(b) / reps
-
+    # dominant-kernel roofline (the Jacobi sweep of the selected form) and
+    # the FP64 residual, timed live on the solver's stream
+    hbm, hbm_kind = peaks()
     v_keep = s.v.clone()
-    t_res = time_residual()
-    t_i0 = time_implicit(0)
-    t_il = time_implicit(args.lmax)
+    nsw = max(5, min(args.steps, 20))
+    t_sweep = _sweep_ms(s, torch, case.scheme, args.lmax, nsw)
+    t_res = _residual_ms(s, torch)
     s.v.copy_(v_keep)
     torch.cuda.synchronize()
-    t_sweep = max((t_il - t_i0) / max(args.lmax, 1), 1e-9)
-    hbm, hbm_kind = peaks()
-    ach_sweep = BYTES_JACOBI * nreal / (t_sweep * 1e-3) / 1e9
+    bj = BYTES_JACOBI[args.precision]
+    ach_sweep = bj * nreal / (t_sweep * 1e-3) / 1e9
     ach_res = BYTES_RESIDUAL * nreal / (t_res * 1e-3) / 1e9
 
     # end to end through the host-array entry point (pinned host state)
@@ -288,13 +376,13 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(ne):
         s.atsch_num_host(vh, 1)
-    te = time.perf_counter() - t0
-    te_t = torch.tensor([te], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
-    te = float(te_t.item())
+    te = max_over_ranks(time.perf_counter() - t0)
     e2e = ws * nreal * ne / te / 1e6
     bytes_v = 5 * case.layout.ld * 8
+
+    steady = None
+    if rank == 0 and args.precision == "mixed" and not args.no_steady_check:
+        steady = steady_state_check()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -305,24 +393,31 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": max(args.warmup, 3),
+            "steps": args.steps, "warmup": warm,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "vs_baseline": None, "dtype": DTYPE[args.precision],
+            "data": "synthetic (seeded)",
             "config": config_of(case, args, ws),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_v,
                     "d2h_bytes_per_step": bytes_v + 15 * 8},
-            "gpu_launches": launches_per_step * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "Jacobi sweep (k_jacobi)",
+            "gpu_launches": kernels,
+            "roofline": {"bound": "hbm", "kernel": SWEEP_KERNEL[args.precision],
                          "achieved": ach_sweep, "peak": hbm, "unit": "GB/s",
                          "frac": ach_sweep / hbm, "peak_source": hbm_kind,
                          "traffic": None, "ms_per_launch": t_sweep,
-                         "bytes_per_launch": BYTES_JACOBI * nreal},
-            "roofline_residual": {"bound": "hbm", "achieved": ach_res, "peak": hbm,
-                                  "unit": "GB/s", "frac": ach_res / hbm,
-                                  "ms_per_launch": t_res},
+                         "bytes_per_launch": bj * nreal, "bytes_per_cell": bj},
+            "roofline_residual": {"bound": "hbm", "kernels": "FP64 residual (all blocks)",
+                                  "achieved": ach_res, "peak": hbm, "unit": "GB/s",
+                                  "frac": ach_res / hbm, "ms_per_launch": t_res,
+                                  "bytes_per_cell": BYTES_RESIDUAL},
             "clocks": clocks,
             "final_l2_rho": float(norms[1, 0]),
         }
+        if fp64:
+            line["fp64"] = fp64
+            line["mixed_over_fp64"] = value / fp64["value"]
+        if steady:
+            line["steady_state"] = steady
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

@@ -18,6 +18,8 @@ ERRORS = {
     4: "time step below dt1min", 5: "unknown boundary condition",
     6: "not ready", 7: "non-finite residual norm",
 }
+(CNS_OK, CNS_EINVAL, CNS_ECUDA, CNS_ETEMP, CNS_EDT, CNS_EBC, CNS_ENOTREADY,
+ CNS_ENONFINITE) = range(8)
 
 
 class Layout_t(C.Structure):
@@ -32,7 +34,7 @@ class Phys_t(C.Structure):
 class Scheme_t(C.Structure):
     _fields_ = [("ns", c_i32), ("muscl", c_i32), ("xk", c_f64), ("ilim", c_i32),
                 ("eta", c_f64), ("kdtl", c_i32), ("dt1min", c_f64), ("lmax", c_i32),
-                ("qfix_dfez", c_i32)]
+                ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32)]
 
 
 class Bnd_t(C.Structure):
@@ -51,7 +53,7 @@ class State_t(C.Structure):
 
 EXPORTS = [
     "cns_create", "cns_destroy", "cns_set_stream", "cns_set_scheme",
-    "cns_last_error", "cns_scratch_bytes", "cns_metric", "cns_boundary_geom",
+    "cns_last_error", "cns_scratch_bytes", "cns_kernels_launched", "cns_metric", "cns_boundary_geom",
     "cns_zpres", "cns_zvismo", "cns_chronos", "cns_rbord", "cns_sch_roe_euler",
     "cns_sch_roe", "cns_zvisqc", "cns_implimf_eu", "cns_implimf_3d",
     "cns_rscpsv", "cns_bind_state", "cns_atsch_num_step",
@@ -82,6 +84,8 @@ def load(build_if_missing: bool = True):
     L.cns_last_error.restype = C.c_char_p
     L.cns_scratch_bytes.argtypes = [vp]
     L.cns_scratch_bytes.restype = c_i64
+    L.cns_kernels_launched.argtypes = [vp]
+    L.cns_kernels_launched.restype = c_i64
     L.cns_metric.argtypes = [vp] * 6
     L.cns_boundary_geom.argtypes = [vp] + [P(c_f64)] * 5
     L.cns_zpres.argtypes = [vp, C.c_int] + [vp] * 4
@@ -105,6 +109,7 @@ def load(build_if_missing: bool = True):
         getattr(L, f).restype = getattr(L, f).restype or C.c_int
     L.cns_last_error.restype = C.c_char_p
     L.cns_scratch_bytes.restype = c_i64
+    L.cns_kernels_launched.restype = c_i64
     _lib = L
     return L
 

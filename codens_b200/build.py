@@ -16,19 +16,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcodens_b200.so")
+# FP64 parity sources: no FMA contraction, every product and sum rounded as
+# written.  The FP32 half of the mixed-precision form (cns_mixed.cu) is not a
+# parity path and is built with contraction.
 SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_abi.cu", "cns_noalloc.cu"]
+SOURCES_FMA = ["cns_mixed.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+OBJDIR = os.path.join(HERE, "_build")
 
-FLAGS = [
+COMMON = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
     "-I" + os.path.join(ROOT, "include"),
 ]
+FLAGS = COMMON + ["--fmad=false"]
+FLAGS_FMA = COMMON + ["--fmad=true"]
 
 
 def sources():
-    return [os.path.join(CSRC, s) for s in SOURCES]
+    return [os.path.join(CSRC, s) for s in SOURCES + SOURCES_FMA]
 
 
 def up_to_date() -> bool:
@@ -41,16 +47,28 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + sources() + ["-o", LIB]
+def _run(cmd, verbose):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed building libcodens_b200.so")
     if verbose:
         sys.stderr.write(r.stderr)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+    extra = ["-Xptxas", "-v"] if verbose else []
+    objs = []
+    for names, flags in ((SOURCES, FLAGS), (SOURCES_FMA, FLAGS_FMA)):
+        for s in names:
+            o = os.path.join(OBJDIR, s.replace(".cu", ".o"))
+            _run([NVCC] + flags + extra + ["-c", os.path.join(CSRC, s), "-o", o], verbose)
+            objs.append(o)
+    _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + objs
+         + ["-o", LIB], verbose)
     return LIB
 
 

@@ -71,6 +71,8 @@ class Scheme:
     dt1min: float = 0.0
     lmax: int = 10
     qfix_dfez: int = 0   # non-reference: restore the *wi of implimf_eu.f90:312
+    precision: int = 0   # fused step: 0 FP64, 1 mixed (FP32 sweeps), 2 defect correction
+    kdefect: int = 4     # precision 2: FP64 residual / defect refresh period
 
 
 @dataclass
@@ -313,7 +315,7 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
                  nk_cells: int = 0, seed: int = 2, mach: float = 0.5,
                  reynz: float = 1.0e4, noise: float = 0.01, lmax: int = 10,
                  eta: float = 5.0, ilim: int = 1, bump: float = 0.1,
-                 length: float = 8.0, span: float = 0.5,
+                 length: float = 8.0, span: float = 0.5, walls: bool = True,
                  name: str = "channel") -> Case:
     """Bump channel: blocks along x joined by coincident faces.
 
@@ -322,7 +324,9 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     mild tanh clustering at both walls; z periodic over ``span``.
     Boundary kinds: idd at the inlet face (total pressure / temperature of the
     freestream, flow along +x), prd at the outlet (freestream static
-    pressure), para on both walls, periodic k on every block.
+    pressure), para on both walls, periodic k on every block.  walls=False
+    makes j periodic too (a duct with inlet and outlet only; with bump=0 its
+    steady state is the uniform flow set by the inlet and outlet values).
     """
     if ni_cells is None:
         ni_cells, nj_cells, nk_cells, seed = channel_dims(seed=seed)
@@ -365,8 +369,13 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     bnd.append(Boundary(0, "i1", BC_IDD, values=(1.0, 1.0, 1.0, 0.0, 0.0)))
     bnd.append(Boundary(nblk - 1, "i2", BC_PRD, values=(p_inf,)))
     for ib in range(nblk):
-        bnd.append(Boundary(ib, "j1", BC_PARA))
-        bnd.append(Boundary(ib, "j2", BC_PARA))
+        if walls:
+            bnd.append(Boundary(ib, "j1", BC_PARA))
+            bnd.append(Boundary(ib, "j2", BC_PARA))
+        else:
+            a = len(bnd)
+            bnd.append(Boundary(ib, "j1", BC_RC, partner=a + 1))
+            bnd.append(Boundary(ib, "j2", BC_RC, partner=a))
         a = len(bnd)
         bnd.append(Boundary(ib, "k1", BC_RC, partner=a + 1))
         bnd.append(Boundary(ib, "k2", BC_RC, partner=a))

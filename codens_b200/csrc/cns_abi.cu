@@ -21,7 +21,7 @@ struct cns_ctx {
   Blk* d_blks = nullptr;
   Phys ph{};
   Scheme sc{};
-  SpaceBuf cells, faces[3], lines[3];
+  SpaceBuf cells, cols, faces[3], lines[3];
   int* d_cells_tile0 = nullptr;  // cells.blk_tile0 on the device
   // boundaries
   Bnd bd{};
@@ -39,7 +39,12 @@ struct cns_ctx {
   cns_state_t state{};
   bool bound = false;
   bool metric_done = false;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr;       // FP64 iteration
+  cudaGraphExec_t gexec_mref = nullptr;  // mixed, or defect iteration with refresh
+  cudaGraphExec_t gexec_mreg = nullptr;  // defect iteration without refresh
+  int nk_gexec = 0, nk_mref = 0, nk_mreg = 0;  // kernel nodes of each graph
+  long long kernels_launched = 0;        // kernels of every fused-step graph launched
+  long long mixed_iter = 0;              // mixed iterations since the last reset
   std::string err;
 };
 
@@ -134,6 +139,15 @@ cudaError_t zero_cols(cns_ctx* c, double* a, int ncol, int l) {
   return cudaSuccess;
 }
 
+void drop_graphs(cns_ctx* c) {
+  for (cudaGraphExec_t* g : {&c->gexec, &c->gexec_mref, &c->gexec_mreg})
+    if (*g) {
+      cudaGraphExecDestroy(*g);
+      *g = nullptr;
+    }
+  c->mixed_iter = 0;
+}
+
 int check_status(cns_ctx* c) {
   CK(cudaMemcpyAsync(c->h_status, c->w.status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -195,7 +209,139 @@ cudaError_t enqueue_step(cns_ctx* c) {
                         s.pression, s.cson, c->w, 1, c->st);
   if (e == cudaSuccess)
     e = launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
-                             c->w.normpart, c->w.norms, c->st);
+                             c->w.normpart, c->w.blocksum, c->w.norms, c->st);
+  return e;
+}
+
+// the single-precision scratch of the mixed form, allocated on first use
+cudaError_t ensure_mixed(cns_ctx* c) {
+  Work& w = c->w;
+  if (w.mixed_ready) return cudaSuccess;
+  const long long ld = c->lay.ld;
+  cudaError_t e = dev_alloc(c, &w.v32, (size_t)(5 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.prim32, (size_t)(3 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.ps32, (size_t)ld);
+  if (e == cudaSuccess) e = dev_alloc(c, &w.tau32, (size_t)(9 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.sn32, (size_t)(9 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.G32, (size_t)(15 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.R32, (size_t)(15 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.u32, (size_t)(5 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.coefe32, (size_t)(3 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.coefdiag32, (size_t)ld);
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+    e = dev_alloc(c, &w.d32pp[q], (size_t)(5 * ld));
+    if (e == cudaSuccess) e = dev_alloc(c, &w.df32pp[q], (size_t)(9 * ld));
+  }
+  if (e == cudaSuccess) e = dev_alloc(c, &w.corr, (size_t)(5 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.ur32, (size_t)(5 * ld));
+  if (e == cudaSuccess) w.mixed_ready = true;
+  return e;
+}
+
+// one reduced-precision iteration on the bound state.  kMixed: FP64 residual,
+// FP32 sweeps (precision 1).  kDefectRefresh / kDefectRegular (precision 2):
+// FP32 face fluxes; the refresh iteration also evaluates the FP64 residual,
+// advances with it and stores corr = R64 - R32 for the regular iterations.
+enum MixedMode { kMixed, kDefectRefresh, kDefectRegular };
+
+cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode) {
+  const cns_state_t& s = c->state;
+  Work& w = c->w;
+  const long long ld = c->lay.ld;
+  const Space all = c->cells.view(-1);
+  const bool lim = c->sc.ns && c->sc.ilim == 1;
+  cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
+                               s.ztemp, s.cson, s.mu, w.status, c->st);
+  if (e == cudaSuccess)
+    e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
+                       s.vol, s.cson, c->st);
+  if (e == cudaSuccess)
+    e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
+                     c->d_idd_ents, c->d_idd_masks, c->st);
+  if (e == cudaSuccess)
+    e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression, w.v32, w.prim32,
+                           w.ps32, c->st);
+  if (e == cudaSuccess && c->sc.ns) {
+    e = launch_grad(c->d_blks, all, c->ph, s.v, w.prim, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
+                    s.ztemp, c->st);
+    if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
+  }
+  if (mode != kMixed) {
+    // single-precision face fluxes
+    if (e == cudaSuccess && c->sc.ns) e = launch_to_float(s.tau, w.tau32, 9 * ld, c->st);
+    if (e == cudaSuccess && lim)
+      e = launch_ratio_t<float>(c->d_blks, c->lines, -1, w.v32, w.prim32, ld, w.ps32, w.R32,
+                                c->st);
+    if (e == cudaSuccess)
+      e = launch_face_flux_t<float>(c->d_blks, c->faces, -1, c->ph, c->sc, w.v32, w.prim32,
+                                    ld, w.ps32, w.tau32, w.sn32, w.R32, w.G32, c->st);
+  }
+  if (mode == kDefectRegular) {
+    if (e == cudaSuccess)
+      e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, w.corr, s.u, w.u32, c->st);
+  } else {
+    // the FP64 residual; the defect refresh also keeps R32 alone for corr
+    if (e == cudaSuccess && mode == kDefectRefresh)
+      e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, nullptr, w.ur32, nullptr,
+                                     c->st);
+    if (e == cudaSuccess && lim)
+      e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
+    if (e == cudaSuccess)
+      e = launch_face_flux(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld, s.pression,
+                           s.tau, s.sn, w.R, w.G, c->st);
+    if (e == cudaSuccess)
+      e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st);
+    if (e == cudaSuccess && mode == kDefectRefresh)
+      e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
+  }
+  // single-precision implicit sweeps, FP64 update
+  if (e == cudaSuccess)
+    e = launch_implicit_coefficients(c->d_blks, all, c->faces, -1, c->ph, !c->sc.ns, s.dt,
+                                     s.v, w.prim, s.mu, s.mut, s.sn, s.vol, s.cson, w,
+                                     w.coefe32, w.coefdiag32, c->st);
+  int cur = 0;
+  if (e == cudaSuccess)
+    e = launch_sweeps_t<float>(c->d_blks, all, c->ph, c->sc, !c->sc.ns, c->sc.lmax, ld, w.u32,
+                               w.v32, w.prim32, w.ps32, w.sn32, w.coefe32, w.coefdiag32,
+                               w.d32pp, w.df32pp, &cur, c->st);
+  if (e == cudaSuccess)
+    e = launch_update_t<float>(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, nullptr,
+                               w.normpart, c->st);
+  if (e == cudaSuccess)
+    e = launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
+                             w.normpart, w.blocksum, w.norms, c->st);
+  return e;
+}
+
+// the kernel nodes of a captured graph (the launch count of one iteration)
+int kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+  int k = 0;
+  for (size_t q = 0; q < n; ++q) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+template <class F>
+cudaError_t capture(cns_ctx* c, cudaGraphExec_t* out, int* nkernels, F enqueue) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t e1 = enqueue();
+  cudaError_t e2 = cudaStreamEndCapture(c->st, &g);
+  if (e1 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return e1;
+  }
+  if (e2 != cudaSuccess) return e2;
+  *nkernels = kernel_nodes(g);
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
   return e;
 }
 
@@ -267,6 +413,9 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   if (e != cudaSuccess) return cleanup_fail(e, "blocks");
   e = build_space(c, c->cells, [](const Blk& B, int x[3]) {
     x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = B.nk - 1; });
+  if (e == cudaSuccess)
+    e = build_space(c, c->cols, [](const Blk& B, int x[3]) {
+      x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = (B.nk - 1 + kJacCol - 1) / kJacCol; });
   for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
     e = build_space(c, c->faces[dir], [dir](const Blk& B, int x[3]) {
       x[0] = dir == 0 ? B.ni : B.ni - 1;
@@ -376,6 +525,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   }
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.normpart, (size_t)(15 * c->cells.ntiles));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.norms, 16);
+  if (e == cudaSuccess) e = dev_alloc(c, &c->w.blocksum, (size_t)(15 * c->lay.blks.size()));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.status, 1);
   if (e == cudaSuccess) e = cudaMallocHost(&c->h_norms, 16 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&c->h_status, sizeof(int));
@@ -389,7 +539,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
 
 int cns_destroy(cns_ctx* c) {
   if (!c) return CNS_OK;
-  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  drop_graphs(c);
   if (c->st) cudaStreamSynchronize(c->st);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_norms) cudaFreeHost(c->h_norms);
@@ -405,17 +555,17 @@ int cns_set_stream(cns_ctx* c, void* stream) {
   // work is issued on the caller's stream from now on (NULL: back to the
   // context's own stream)
   c->st = stream ? (cudaStream_t)stream : c->own_st;
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-  }
+  drop_graphs(c);
   return CNS_OK;
 }
 
 int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (!c || !s) return CNS_EINVAL;
-  if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1))
-    return fail(c, CNS_EINVAL, "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}");
+  if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
+      s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1))
+    return fail(c, CNS_EINVAL,
+                "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
+                "kdefect >= 1");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
   c->sc.xk = s->xk;
@@ -425,10 +575,9 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.dt1min = s->dt1min;
   c->sc.lmax = s->lmax;
   c->sc.qfix_dfez = s->qfix_dfez;
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-  }
+  c->sc.precision = s->precision;
+  c->sc.kdefect = s->kdefect;
+  drop_graphs(c);
   return CNS_OK;
 }
 
@@ -436,12 +585,17 @@ const char* cns_last_error(cns_ctx* c) { return c ? c->err.c_str() : "no context
 
 int64_t cns_scratch_bytes(cns_ctx* c) { return c ? c->scratch_bytes : 0; }
 
+int64_t cns_kernels_launched(cns_ctx* c) { return c ? c->kernels_launched : 0; }
+
 int cns_metric(cns_ctx* c, double* x, double* y, double* z, double* sn,
                double* vol) {
   if (!c || !x || !y || !z || !sn || !vol) return CNS_EINVAL;
   CK(launch_metric(c->lay, c->d_blks, c->bd, x, y, z, sn, vol, c->st));
+  if (c->w.mixed_ready && c->bound && c->state.sn == sn)
+    CK(launch_to_float(sn, c->w.sn32, 9 * c->lay.ld, c->st));
   CK(cudaStreamSynchronize(c->st));
   c->metric_done = true;
+  c->mixed_iter = 0;
   return CNS_OK;
 }
 
@@ -573,7 +727,7 @@ int cns_rscpsv(cns_ctx* c, const double* u0, const double* v, const double* dt,
   CK(launch_norm_partials(c->d_blks, c->cells.view(-1), c->lay.ld, u0, v, dt,
                           c->w.normpart, c->st));
   CK(launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
-                          c->w.normpart, c->w.norms, c->st));
+                          c->w.normpart, c->w.blocksum, c->w.norms, c->st));
   CK(cudaMemcpyAsync(c->h_norms, c->w.norms, 15 * sizeof(double), cudaMemcpyDeviceToHost,
                      c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -587,10 +741,7 @@ int cns_bind_state(cns_ctx* c, const cns_state_t* s) {
     return CNS_EINVAL;
   c->state = *s;
   c->bound = true;
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-  }
+  drop_graphs(c);
   return CNS_OK;
 }
 
@@ -600,18 +751,35 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
   if (c->sc.kdtl == 0)
     return fail(c, CNS_EINVAL, "the fused step runs with local time steps (kdtl != 0)");
-  if (!c->gexec) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = enqueue_step(c);
-    cudaError_t e2 = cudaStreamEndCapture(c->st, &g);
-    CK(e);
-    CK(e2);
-    e = cudaGraphInstantiate(&c->gexec, g, 0);
-    cudaGraphDestroy(g);
-    CK(e);
+  if (c->sc.precision == 0) {
+    if (!c->gexec) CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c); }));
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
+    c->kernels_launched += (long long)nsteps * c->nk_gexec;
+    return CNS_OK;
   }
-  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
+  if (!c->w.mixed_ready) {
+    CK(ensure_mixed(c));
+    CK(launch_to_float(c->state.sn, c->w.sn32, 9 * c->lay.ld, c->st));
+  }
+  if (c->sc.precision == 1) {
+    if (!c->gexec_mref)
+      CK(capture(c, &c->gexec_mref, &c->nk_mref, [&] { return enqueue_step_mixed(c, kMixed); }));
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec_mref, c->st));
+    c->kernels_launched += (long long)nsteps * c->nk_mref;
+    return CNS_OK;
+  }
+  if (!c->gexec_mref)
+    CK(capture(c, &c->gexec_mref, &c->nk_mref,
+               [&] { return enqueue_step_mixed(c, kDefectRefresh); }));
+  if (!c->gexec_mreg)
+    CK(capture(c, &c->gexec_mreg, &c->nk_mreg,
+               [&] { return enqueue_step_mixed(c, kDefectRegular); }));
+  for (int s = 0; s < nsteps; ++s) {
+    const bool refresh = (c->mixed_iter % c->sc.kdefect) == 0;
+    CK(cudaGraphLaunch(refresh ? c->gexec_mref : c->gexec_mreg, c->st));
+    c->kernels_launched += refresh ? c->nk_mref : c->nk_mreg;
+    ++c->mixed_iter;
+  }
   return CNS_OK;
 }
 

@@ -48,7 +48,7 @@ struct Phys {
 };
 
 struct Scheme {
-  int ns, muscl, ilim, kdtl, lmax, qfix_dfez;
+  int ns, muscl, ilim, kdtl, lmax, qfix_dfez, precision, kdefect;
   double xk, eta, dt1min;
 };
 
@@ -108,8 +108,8 @@ __device__ __forceinline__ int nd_of(const Blk& B, int dir) {
   return dir == 0 ? B.ni : (dir == 1 ? B.nj : B.nk);
 }
 // sn(m, dir, c) of the block (m local index = n - npc)
-__device__ __forceinline__ const double* sn_ptr(const double* sn, const Blk& B,
-                                                int dir, int c) {
+template <class T>
+__device__ __forceinline__ const T* sn_ptr(const T* sn, const Blk& B, int dir, int c) {
   return sn + 9 * B.npc + (long long)c * 3 * B.nnn + (long long)dir * B.nnn - B.npc;
 }
 

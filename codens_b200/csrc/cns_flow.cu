@@ -12,6 +12,7 @@
 // order, then the lower and the upper boundary face), which keeps the FP64
 // result bit-identical.
 #include "cns_kernels.cuh"
+#include "cns_hot.cuh"
 
 namespace cns {
 
@@ -78,15 +79,32 @@ __global__ void __launch_bounds__(kTile) k_zvismo(const Blk* __restrict__ blks,
 // the limiter ratios, the gradients and the implicit phase all use these very
 // quotients (the reference recomputes them at every use, with identical
 // results), so sharing them changes no bit
+template <bool SHADOW>
 __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
                                              const double* __restrict__ v,
-                                             long long ld, double* __restrict__ prim) {
+                                             long long ld, double* __restrict__ prim,
+                                             const double* __restrict__ ps,
+                                             float* __restrict__ v32,
+                                             float* __restrict__ prim32,
+                                             float* __restrict__ ps32) {
   const long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= n1) return;
   const double r = v[n];
-  prim[n] = v[ld + n] / r;
-  prim[ld + n] = v[2 * ld + n] / r;
-  prim[2 * ld + n] = v[3 * ld + n] / r;
+  const double q0 = v[ld + n] / r, q1 = v[2 * ld + n] / r, q2 = v[3 * ld + n] / r;
+  prim[n] = q0;
+  prim[ld + n] = q1;
+  prim[2 * ld + n] = q2;
+  if (SHADOW) {
+    // single-precision copies of the state, velocities and pressure for
+    // the reduced-precision sweeps
+    v32[n] = (float)r;
+#pragma unroll
+    for (int a = 1; a < 5; ++a) v32[a * ld + n] = (float)v[a * ld + n];
+    prim32[n] = (float)q0;
+    prim32[ld + n] = (float)q1;
+    prim32[2 * ld + n] = (float)q2;
+    ps32[n] = (float)ps[n];
+  }
 }
 
 // chronos.f90:110-194 (kprec = 0)
@@ -431,402 +449,6 @@ __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
   tau[8 * ld + n] = kq * g[11];
 }
 
-// ---------------------------------------------------------------------------
-// Roe-MUSCL face flux
-// ---------------------------------------------------------------------------
-
-// slope-ratio recurrence of sch_roe.f90:146-194 along one grid line: the
-// ratio at face m divides by the ALREADY UPDATED ratio at face m-1, with a
-// reset to 1 when |r(m-1) r(m) r(m+1)| <= tiny.  One thread walks one line
-// for one of the five variables (blockIdx.y: rho, u, v, w, p); lines of the
-// j and k directions are adjacent in i, so those walks are coalesced.
-__global__ void __launch_bounds__(kTile) k_ratio(const Blk* __restrict__ blks,
-                                                 Space sp, int dir,
-                                                 const double* __restrict__ v,
-                                                 const double* __restrict__ prim,
-                                                 long long ld,
-                                                 const double* __restrict__ ps,
-                                                 double* __restrict__ R) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const int nd = nd_of(B, dir);
-  if (nd < 3) return;
-  const long long inc = ninc_of(B, dir);
-  const int a = blockIdx.y;
-  const double* x = a == 0 ? v : (a == 4 ? ps : prim + (long long)(a - 1) * ld);
-  double* Ra = R + ((long long)dir * 5 + a) * ld;
-  // (i,j,k) is position 1 of the line: cells 0 .. nd along dir
-  const long long n0 = cell_index(B, i, j, k) - inc;
-  double x0 = x[n0], x1 = x[n0 + inc], x2 = x[n0 + 2 * inc];
-  double rprev = x1 - x0;   // face 1 (never updated)
-  double dcur = x2 - x1;    // face 2
-  for (int f = 2; f <= nd - 1; ++f) {
-    const long long n = n0 + (long long)f * inc;
-    const double x3 = x[n + inc];
-    const double dnext = x3 - x2;
-    double r;
-    if (fabs(rprev * dcur * dnext) <= 2.2250738585072014e-308)
-      r = 1.;
-    else
-      r = dcur / rprev;
-    Ra[n] = r;
-    rprev = r;
-    dcur = dnext;
-    x2 = x3;
-  }
-}
-
-__device__ __forceinline__ double phi_mm(double a) {  // sch_roe.f90:1500-1504
-  const double m = (a < 1.) ? a : 1.;
-  return (m > 0.) ? m : 0.;
-}
-
-// kappa-MUSCL without limiter (sch_roe_euler.f90:245-273); cells c[0..3] are
-// n-2, n-1, n, n+1 as (rho, u, v, w, p)
-__device__ __forceinline__ void muscl_plain(const double c[4][5], double c4,
-                                            double xk, double WL[5],
-                                            double WR[5]) {
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-    WL[a] = c[1][a] + c4 * ((1. - xk) * (c[1][a] - c[0][a]) + (1. + xk) * (c[2][a] - c[1][a]));
-    WR[a] = c[2][a] - c4 * ((1. + xk) * (c[2][a] - c[1][a]) + (1. - xk) * (c[3][a] - c[2][a]));
-  }
-}
-
-// limited MUSCL (sch_roe.f90:196-227): rho and p use one product order,
-// the velocities another; rm are the ratios at this face, rp at the next
-__device__ __forceinline__ void muscl_limited(const double c[4][5], double c4,
-                                              int muscl, double xk,
-                                              const double rm[5],
-                                              const double rp[5], double WL[5],
-                                              double WR[5]) {
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-    if (a == 0 || a == 4) {
-      WL[a] = c[1][a] + c4 * phi_mm(rm[a]) * (1. - xk) * (c[1][a] - c[0][a]) +
-              c4 * phi_mm(1. / rm[a]) * (1. + xk) * (c[2][a] - c[1][a]);
-      WR[a] = c[2][a] - c4 * phi_mm(rp[a]) * (1. + xk) * (c[2][a] - c[1][a]) -
-              c4 * phi_mm(1. / rp[a]) * (1. - xk) * (c[3][a] - c[2][a]);
-    } else {
-      WL[a] = c[1][a] + c4 * phi_mm(rm[a]) * (1. - xk) * (c[1][a] - c[0][a]) +
-              (1. + xk) * (c[2][a] - c[1][a]) * 0.25 * muscl * phi_mm(1. / rm[a]);
-      WR[a] = c[2][a] - c4 * phi_mm(rp[a]) * (1. + xk) * (c[2][a] - c[1][a]) -
-              (1. - xk) * (c[3][a] - c[2][a]) * 0.25 * muscl * phi_mm(1. / rp[a]);
-    }
-  }
-}
-
-// row r of the right eigenvector matrix P at the Roe state
-__device__ __forceinline__ void p_row(int r, double nx, double ny, double nz,
-                                      double um, double vm, double wm,
-                                      double hm, double am, double vn,
-                                      double vitm2, double rhom, double rhoiam,
-                                      double p[5]) {
-  switch (r) {
-    case 0:
-      p[0] = nx; p[1] = ny; p[2] = nz;
-      p[3] = 0.5 * rhoiam; p[4] = 0.5 * rhoiam;
-      break;
-    case 1:
-      p[0] = um * nx; p[1] = um * ny - rhom * nz; p[2] = um * nz + rhom * ny;
-      p[3] = 0.5 * rhoiam * (um + nx * am); p[4] = 0.5 * rhoiam * (um - nx * am);
-      break;
-    case 2:
-      p[0] = vm * nx + rhom * nz; p[1] = vm * ny; p[2] = vm * nz - rhom * nx;
-      p[3] = 0.5 * rhoiam * (vm + ny * am); p[4] = 0.5 * rhoiam * (vm - ny * am);
-      break;
-    case 3:
-      p[0] = wm * nx - rhom * ny; p[1] = wm * ny + rhom * nx; p[2] = wm * nz;
-      p[3] = 0.5 * rhoiam * (wm + nz * am); p[4] = 0.5 * rhoiam * (wm - nz * am);
-      break;
-    default:
-      p[0] = vitm2 * nx + rhom * (vm * nz - wm * ny);
-      p[1] = vitm2 * ny + rhom * (wm * nx - um * nz);
-      p[2] = vitm2 * nz + rhom * (um * ny - vm * nx);
-      p[3] = 0.5 * rhoiam * (hm + am * vn);
-      p[4] = 0.5 * rhoiam * (hm - am * vn);
-  }
-}
-
-// Roe dissipation |A|(W_R - W_L) of sch_roe_euler.f90:284-402 (di), plus the
-// specific total energies el, er used by the centred part
-__device__ __forceinline__ void roe_dissipation(const double WL[5],
-                                                const double WR[5], double sx,
-                                                double sy, double sz, bool absam,
-                                                const Phys& ph, double di[5],
-                                                double& el, double& er) {
-  const double gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl;
-  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
-  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
-  const double cnds = sqrt(sx * sx + sy * sy + sz * sz);
-  const double nx = sx / cnds, ny = sy / cnds, nz = sz / cnds;
-  const double al = sqrt(gam * pl / rhol);
-  const double ar = sqrt(gam * prr / rhor);
-  const double q2l = sq(ul) + sq(vl) + sq(wl);
-  const double q2r = sq(ur) + sq(vr) + sq(wr);
-  const double hl = al * al / gam1 + 0.5 * q2l;
-  const double hr = ar * ar / gam1 + 0.5 * q2r;
-  el = pl / (gam1 * rhol) + 0.5 * q2l + pinfl / rhol;
-  er = prr / (gam1 * rhor) + 0.5 * q2r + pinfl / rhor;
-  const double gd = sqrt(rhor / rhol);
-  const double gd1 = 1. / (1. + gd);
-  const double gd2 = gd * gd1;
-  const double rhom = sqrt(rhol * rhor);
-  const double rhomi = 1. / rhom;
-  const double um = gd1 * ul + gd2 * ur;
-  const double vm = gd1 * vl + gd2 * vr;
-  const double wm = gd1 * wl + gd2 * wr;
-  const double hm = gd1 * hl + gd2 * hr;
-  const double vitm2 = 0.5 * (sq(um) + sq(vm) + sq(wm));
-  const double am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
-  const double am2i = 1. / (am * am);
-  const double vn = um * nx + vm * ny + wm * nz;
-  const double rhoiam = rhom / am;
-  const double rhoami = am2i / rhoiam;
-  const double lam1 = fabs(vn * cnds);
-  const double lam4 = fabs(vn * cnds + am * cnds);
-  const double lam5 = fabs(vn * cnds - am * cnds);
-  double q[5][5];
-  q[0][0] = (1. - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi;
-  q[0][1] = gam1 * um * nx * am2i;
-  q[0][2] = gam1 * vm * nx * am2i + nz * rhomi;
-  q[0][3] = gam1 * wm * nx * am2i - ny * rhomi;
-  q[0][4] = -gam1 * nx * am2i;
-  q[1][0] = (1. - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi;
-  q[1][1] = gam1 * um * ny * am2i - nz * rhomi;
-  q[1][2] = gam1 * vm * ny * am2i;
-  q[1][3] = gam1 * wm * ny * am2i + nx * rhomi;
-  q[1][4] = -gam1 * ny * am2i;
-  q[2][0] = (1. - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi;
-  q[2][1] = gam1 * um * nz * am2i + ny * rhomi;
-  q[2][2] = gam1 * vm * nz * am2i - nx * rhomi;
-  q[2][3] = gam1 * wm * nz * am2i;
-  q[2][4] = -gam1 * nz * am2i;
-  q[3][0] = gam1 * vitm2 * rhoami - vn * rhomi;
-  q[3][1] = nx * rhomi - gam1 * um * rhoami;
-  q[3][2] = ny * rhomi - gam1 * vm * rhoami;
-  q[3][3] = nz * rhomi - gam1 * wm * rhoami;
-  q[3][4] = gam1 * rhoami;
-  q[4][0] = gam1 * vitm2 * rhoami + vn * rhomi;
-  q[4][1] = -nx * rhomi - gam1 * um * rhoami;
-  q[4][2] = -ny * rhomi - gam1 * vm * rhoami;
-  q[4][3] = -nz * rhomi - gam1 * wm * rhoami;
-  q[4][4] = gam1 * rhoami;
-  double dw[5];
-  dw[0] = rhor - rhol;
-  dw[1] = rhor * ur - rhol * ul;
-  dw[2] = rhor * vr - rhol * vl;
-  dw[3] = rhor * wr - rhol * wl;
-  dw[4] = rhor * er - rhol * el;
-  const double lam[5] = {lam1, lam1, lam1, lam4, lam5};
-#pragma unroll
-  for (int r = 0; r < 5; ++r) {
-    double p[5];
-    p_row(r, nx, ny, nz, um, vm, wm, hm, am, vn, vitm2, rhom, rhoiam, p);
-    double pl_[5];
-#pragma unroll
-    for (int kk = 0; kk < 5; ++kk) pl_[kk] = p[kk] * lam[kk];
-    double acc = 0.;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      double a = pl_[0] * q[0][c];
-#pragma unroll
-      for (int kk = 1; kk < 5; ++kk) a = a + pl_[kk] * q[kk][c];
-      acc = (c == 0) ? a * dw[0] : acc + a * dw[c];
-    }
-    di[r] = acc;
-  }
-}
-
-// primitive (rho, u, v, w, p) of cell n
-__device__ __forceinline__ void load_prim(const double* __restrict__ v,
-                                          const double* __restrict__ prim,
-                                          const double* __restrict__ ps,
-                                          long long ld, long long n,
-                                          double c[5]) {
-  c[0] = v[n];
-  c[1] = prim[n];
-  c[2] = prim[ld + n];
-  c[3] = prim[2 * ld + n];
-  c[4] = ps[n];
-}
-
-// one face per thread, direction dir: interior faces give 0.5*f (sch_roe*
-// interior loops), boundary faces give the ghost-cell physical flux s
-// (lower face 1, upper face nd).  Results go to G[dir][a][n] where n is the
-// cell above the face.
-template <bool NS>
-__global__ void __launch_bounds__(kTile, 3) k_face_flux(
-    const Blk* __restrict__ blks, Space sp, int dir, Phys ph, Scheme sc,
-    const double* __restrict__ v, const double* __restrict__ prim, long long ld,
-    const double* __restrict__ ps, const double* __restrict__ tau,
-    const double* __restrict__ sn, const double* __restrict__ R,
-    double* __restrict__ G) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long inc = ninc_of(B, dir);
-  const int nd = nd_of(B, dir);
-  const int p = dir == 0 ? i : (dir == 1 ? j : k);
-  const long long n = cell_index(B, i, j, k);
-  const double sx = sn_ptr(sn, B, dir, 0)[n], sy = sn_ptr(sn, B, dir, 1)[n],
-               sz = sn_ptr(sn, B, dir, 2)[n];
-  const double pinfl = ph.pinfl;
-  double out[5];
-  if (p == 1 || p == nd) {
-    // boundary face: physical flux of the ghost cell (sch_roe_euler.f90:
-    // 438-513, sch_roe.f90:497-580); the Euler j/k lower faces divide the
-    // energy flux by the interior density (sch_roe_euler.f90:630-632)
-    const long long ng = (p == 1) ? n - inc : n;
-    const long long nrho = (!NS && p == 1 && dir > 0) ? n : ng;
-    const double v1 = v[ng], v2 = v[ld + ng], v3 = v[2 * ld + ng],
-                 v4 = v[3 * ld + ng], v5 = v[4 * ld + ng], pg = ps[ng];
-    const double qu = prim[ng], qv = prim[ld + ng], qw = prim[2 * ld + ng];
-    double fxx, fxy, fxz, fyy, fyz, fzz, fex, fey, fez;
-    if (!NS) {
-      const double rr = v[nrho];
-      fxx = v2 * qu + pg - pinfl;
-      fxy = v3 * qu;
-      fxz = v4 * qu;
-      fyy = v3 * qv + pg - pinfl;
-      fyz = v4 * qv;
-      fzz = v4 * qw + pg - pinfl;
-      fex = (v5 + pg - pinfl) * v2 / rr;
-      fey = (v5 + pg - pinfl) * v3 / rr;
-      fez = (v5 + pg - pinfl) * v4 / rr;
-    } else {
-      const double txx = tau[ng], txy = tau[ld + ng], txz = tau[2 * ld + ng],
-                   tyy = tau[3 * ld + ng], tyz = tau[4 * ld + ng],
-                   tzz = tau[5 * ld + ng], qx = tau[6 * ld + ng],
-                   qy = tau[7 * ld + ng], qz = tau[8 * ld + ng];
-      fxx = v2 * qu + pg - pinfl - txx;
-      fxy = v3 * qu - txy;
-      fxz = v4 * qu - txz;
-      fyy = v3 * qv + pg - pinfl - tyy;
-      fyz = v4 * qv - tyz;
-      fzz = v4 * qw + pg - pinfl - tzz;
-      fex = ((v5 + pg - pinfl - txx) * v2 - txy * v3 - txz * v4) / v1 - qx;
-      fey = ((v5 + pg - pinfl - tyy) * v3 - txy * v2 - tyz * v4) / v1 - qy;
-      fez = ((v5 + pg - pinfl - tzz) * v4 - txz * v2 - tyz * v3) / v1 - qz;
-    }
-    out[0] = v2 * sx + v3 * sy + v4 * sz;
-    out[1] = fxx * sx + fxy * sy + fxz * sz;
-    out[2] = fxy * sx + fyy * sy + fyz * sz;
-    out[3] = fxz * sx + fyz * sy + fzz * sz;
-    out[4] = fex * sx + fey * sy + fez * sz;
-  } else {
-    double c[4][5];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) load_prim(v, prim, ps, ld, n + (long long)(s - 2) * inc, c[s]);
-    double WL[5], WR[5];
-    const double c4 = 0.25 * sc.muscl;
-    if (NS && sc.ilim == 1 && p <= nd - 2) {
-      const double* Rd = R + (long long)dir * 5 * ld;
-      double rm[5], rp[5];
-#pragma unroll
-      for (int a = 0; a < 5; ++a) {
-        rm[a] = Rd[a * ld + n];
-        rp[a] = Rd[a * ld + n + inc];
-      }
-      muscl_limited(c, c4, sc.muscl, sc.xk, rm, rp, WL, WR);
-    } else {
-      muscl_plain(c, c4, sc.xk, WL, WR);
-    }
-    double di[5], el, er;
-    roe_dissipation(WL, WR, sx, sy, sz, (!NS) && dir > 0, ph, di, el, er);
-    const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
-    const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
-    double dfxx, dfxy, dfxz, dfyy, dfyz, dfzz, dfex, dfey, dfez;
-    if (!NS) {
-      dfxx = rhor * sq(ur) + prr - pinfl + rhol * sq(ul) + pl - pinfl;
-      dfxy = rhor * ur * vr + rhol * ul * vl;
-      dfxz = rhor * ur * wr + rhol * ul * wl;
-      dfyy = rhor * sq(vr) + prr - pinfl + rhol * sq(vl) + pl - pinfl;
-      dfyz = rhor * vr * wr + rhol * vl * wl;
-      dfzz = rhor * sq(wr) + prr - pinfl + rhol * sq(wl) + pl - pinfl;
-      dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul;
-      dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl;
-      dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl;
-    } else {
-      const long long nR = n, nL = n - inc;
-      const double txxR = tau[nR], txyR = tau[ld + nR], txzR = tau[2 * ld + nR],
-                   tyyR = tau[3 * ld + nR], tyzR = tau[4 * ld + nR],
-                   tzzR = tau[5 * ld + nR];
-      const double txxL = tau[nL], txyL = tau[ld + nL], txzL = tau[2 * ld + nL],
-                   tyyL = tau[3 * ld + nL], tyzL = tau[4 * ld + nL],
-                   tzzL = tau[5 * ld + nL];
-      dfxx = rhor * sq(ur) + prr - pinfl - txxR + rhol * sq(ul) + pl - pinfl - txxL;
-      dfxy = rhor * ur * vr - txyR + rhol * ul * vl - txyL;
-      dfxz = rhor * ur * wr - txzR + rhol * ul * wl - txzL;
-      dfyy = rhor * sq(vr) + prr - pinfl - tyyR + rhol * sq(vl) + pl - pinfl - tyyL;
-      dfyz = rhor * vr * wr - tyzR + rhol * vl * wl - tyzL;
-      dfzz = rhor * sq(wr) + prr - pinfl - tzzR + rhol * sq(wl) + pl - pinfl - tzzL;
-      dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul -
-             (txxR * ur + txyR * vr + txzR * wr) - (txxL * ul + txyL * vl + txzL * wl) -
-             tau[6 * ld + nR] - tau[6 * ld + nL];
-      dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl -
-             (txyR * ur + tyyR * vr + tyzR * wr) - (txyL * ul + tyyL * vl + tyzL * wl) -
-             tau[7 * ld + nR] - tau[7 * ld + nL];
-      dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl -
-             (txzR * ur + tyzR * vr + tzzR * wr) - (txzL * ul + tyzL * vl + tzzL * wl) -
-             tau[8 * ld + nR] - tau[8 * ld + nL];
-    }
-    const double f1 = (rhor * ur + rhol * ul) * sx + (rhor * vr + rhol * vl) * sy +
-                      (rhor * wr + rhol * wl) * sz - di[0];
-    const double f2 = dfxx * sx + dfxy * sy + dfxz * sz - di[1];
-    const double f3 = dfxy * sx + dfyy * sy + dfyz * sz - di[2];
-    const double f4 = dfxz * sx + dfyz * sy + dfzz * sz - di[3];
-    const double f5 = dfex * sx + dfey * sy + dfez * sz - di[4];
-    out[0] = 0.5 * f1;
-    out[1] = 0.5 * f2;
-    out[2] = 0.5 * f3;
-    out[3] = 0.5 * f4;
-    out[4] = 0.5 * f5;
-  }
-  double* Gd = G + (long long)dir * 5 * ld;
-#pragma unroll
-  for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
-}
-
-// u(n) from the six faces of the cell, in the reference's summation order
-__global__ void __launch_bounds__(kTile) k_accumulate(const Blk* __restrict__ blks,
-                                                      Space sp,
-                                                      const double* __restrict__ G,
-                                                      long long ld,
-                                                      double* __restrict__ u) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
-  double acc[5] = {0., 0., 0., 0., 0.};
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long inc = ninc_of(B, dir);
-    const int nd = nd_of(B, dir);
-    const int p = dir == 0 ? i : (dir == 1 ? j : k);
-    const bool upper_first = (p == 1) && nd >= 3;
-    const double* Gd = G + (long long)dir * 5 * ld;
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      const double gl = Gd[a * ld + n], gu = Gd[a * ld + n + inc];
-      if (upper_first) {
-        acc[a] = acc[a] + gu;
-        acc[a] = acc[a] - gl;
-      } else {
-        acc[a] = acc[a] - gl;
-        acc[a] = acc[a] + gu;
-      }
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 5; ++a) u[a * ld + n] = acc[a];
-}
-
-// ---------------------------------------------------------------------------
-// implicit phase: matrix-free point Jacobi (implimf_eu.f90, implimf_3d.f90)
-// ---------------------------------------------------------------------------
-
 // per real cell: coefdiag seed (vol/dt or vol*(0+1/dt)) and the viscous
 // spectral factor rv (implimf_3d.f90:95-105, implimf_eu.f90:124-134)
 __global__ void __launch_bounds__(kTile) k_impl_cell0(
@@ -848,12 +470,13 @@ __global__ void __launch_bounds__(kTile) k_impl_cell0(
 
 // per face: spectral radius coefe (implimf_eu.f90:141-159,
 // implimf_3d.f90:110-190)
+template <class TO>
 __global__ void __launch_bounds__(kTile) k_impl_coefe(
     const Blk* __restrict__ blks, Space sp, int dir, int eu,
     const double* __restrict__ v, const double* __restrict__ prim, long long ld,
     const double* __restrict__ sn,
     const double* __restrict__ vol, const double* __restrict__ cson,
-    const double* __restrict__ rv, double* coefe) {
+    const double* __restrict__ rv, double* coefe, TO* coefe_out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -878,14 +501,16 @@ __global__ void __launch_bounds__(kTile) k_impl_coefe(
     ce = 0.5 * (fabs(vn) + sqrt(cnds) * cc) + (rv[n] + rv[nl]) * cnds / (vol[n] + vol[nl]);
   }
   coefe[(long long)dir * ld + n] = ce;
+  if (coefe_out) coefe_out[(long long)dir * ld + n] = (TO)ce;
 }
 
 // per real cell: coefdiag += coefe of the six faces (implimf_eu.f90:161-170,
 // implimf_3d.f90:192-203: the same left-to-right chain)
+template <class TO>
 __global__ void __launch_bounds__(kTile) k_impl_diag(const Blk* __restrict__ blks,
                                                      Space sp, long long ld,
                                                      const double* __restrict__ coefe,
-                                                     double* coefdiag) {
+                                                     double* coefdiag, TO* coefdiag_out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -898,220 +523,9 @@ __global__ void __launch_bounds__(kTile) k_impl_diag(const Blk* __restrict__ blk
     c = c + coefe[(long long)dir * ld + n + inc];
   }
   coefdiag[n] = c;
+  if (coefdiag_out) coefdiag_out[n] = (TO)c;
 }
 
-// df index: 0 xx, 1 xy, 2 xz, 3 ex, 4 yy, 5 yz, 6 ey, 7 zz, 8 ez
-
-// flux-increment projections tn(1..5) on the face between cells nu (above)
-// and nl (below)
-template <bool EU, bool FIRST>
-__device__ __forceinline__ void jacobi_tn(const double* __restrict__ d,
-                                          const double* __restrict__ df,
-                                          long long ld, long long nu,
-                                          long long nl, double sx, double sy,
-                                          double sz, double tn[5]) {
-  double a2, a3, a4, fxx, fxy, fxz, fex, fyy, fyz, fey, fzz, fez;
-  if (FIRST) {
-    a2 = a3 = a4 = 0. + 0.;
-    fxx = fxy = fxz = fex = fyy = fyz = fey = fzz = fez = 0. + 0.;
-  } else {
-    a2 = d[ld + nu] + d[ld + nl];
-    a3 = d[2 * ld + nu] + d[2 * ld + nl];
-    a4 = d[3 * ld + nu] + d[3 * ld + nl];
-    fxx = df[nu] + df[nl];
-    fxy = df[ld + nu] + df[ld + nl];
-    fxz = df[2 * ld + nu] + df[2 * ld + nl];
-    fex = df[3 * ld + nu] + df[3 * ld + nl];
-    fyy = df[4 * ld + nu] + df[4 * ld + nl];
-    fyz = df[5 * ld + nu] + df[5 * ld + nl];
-    fey = df[6 * ld + nu] + df[6 * ld + nl];
-    fzz = df[7 * ld + nu] + df[7 * ld + nl];
-    fez = df[8 * ld + nu] + df[8 * ld + nl];
-  }
-  if (EU) {
-    tn[0] = 0.5 * (a2 * sx + a3 * sy + a4 * sz);
-    tn[1] = 0.5 * (fxx * sx + fxy * sy + fxz * sz);
-    tn[2] = 0.5 * (fxy * sx + fyy * sy + fyz * sz);
-    tn[3] = 0.5 * (fxz * sx + fyz * sy + fzz * sz);
-    tn[4] = 0.5 * (fex * sx + fey * sy + fez * sz);
-  } else {
-    tn[0] = 0.5 * a2 * sx + 0.5 * a3 * sy + 0.5 * a4 * sz;
-    tn[1] = 0.5 * fxx * sx + 0.5 * fxy * sy + 0.5 * fxz * sz;
-    tn[2] = 0.5 * fxy * sx + 0.5 * fyy * sy + 0.5 * fyz * sz;
-    tn[3] = 0.5 * fxz * sx + 0.5 * fyz * sy + 0.5 * fzz * sz;
-    tn[4] = 0.5 * fex * sx + 0.5 * fey * sy + 0.5 * fez * sz;
-  }
-}
-
-// one Jacobi sub-iteration on one real cell: d2w = -u + sum over the faces,
-// d = d2w / coefdiag, then the flux increments of v+d (implimf_eu.f90:
-// 176-323, implimf_3d.f90:222-466).  Reads the previous iterate (d_in,
-// df_in), writes the next one; FIRST: the previous iterate is zero.
-template <bool EU, bool FIRST>
-__global__ void __launch_bounds__(kTile) k_jacobi(
-    const Blk* __restrict__ blks, Space sp, Phys ph, int qfix, long long ld,
-    const double* __restrict__ u, const double* __restrict__ v,
-    const double* __restrict__ prim,
-    const double* __restrict__ ps, const double* __restrict__ sn,
-    const double* __restrict__ coefe, const double* __restrict__ coefdiag,
-    const double* __restrict__ d_in, const double* __restrict__ df_in,
-    double* __restrict__ d_out, double* __restrict__ df_out) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
-  double d2w[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long inc = ninc_of(B, dir);
-    const double *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
-                 *s2 = sn_ptr(sn, B, dir, 2);
-    const double* ce = coefe + (long long)dir * ld;
-    double tn[5];
-    jacobi_tn<EU, FIRST>(d_in, df_in, ld, n, n - inc, s0[n], s1[n], s2[n], tn);
-    const double cel = ce[n], ceu = ce[n + inc];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      const double dl = FIRST ? 0. : d_in[a * ld + n - inc];
-      const double du = FIRST ? 0. : d_in[a * ld + n + inc];
-      d2w[a] = d2w[a] + tn[a] + cel * dl + ceu * du;
-    }
-    const long long nu = n + inc;
-    jacobi_tn<EU, FIRST>(d_in, df_in, ld, nu, n, s0[nu], s1[nu], s2[nu], tn);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
-  }
-  const double cd = coefdiag[n];
-  double dn[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-    dn[a] = d2w[a] / cd;
-    d_out[a * ld + n] = dn[a];
-  }
-  const double gam1 = ph.gam1, pinfl = ph.pinfl;
-  const double v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n],
-               v5 = v[4 * ld + n], p = ps[n];
-  double f[9];
-  if (EU) {
-    const double wi1 = 1. / (v1 + dn[0]);
-    const double ui = v2 + dn[1], vi = v3 + dn[2], wi = v4 + dn[3], wi5 = v5 + dn[4];
-    const double pres = gam1 * (wi5 - .5 * wi1 * (sq(ui) + sq(vi) + sq(wi)) - pinfl);
-    const double norm = 1. / v1;
-    const double fxx = v2 * (v2 * norm) + p;
-    const double fxy = v3 * (v2 * norm);
-    const double fxz = v4 * (v2 * norm);
-    const double fyy = v3 * (v3 * norm) + p;
-    const double fyz = v4 * (v3 * norm);
-    const double fzz = v4 * (v4 * norm) + p;
-    const double fex = (v5 + p - pinfl) * v2 * norm;
-    const double fey = (v5 + p - pinfl) * v3 * norm;
-    const double fez = (v5 + p - pinfl) * v4 * norm;
-    f[0] = wi1 * sq(ui) + pres - fxx;
-    f[1] = wi1 * ui * vi - fxy;
-    f[2] = wi1 * ui * wi - fxz;
-    f[3] = wi1 * ui * (wi5 + pres - pinfl) - fex;
-    f[4] = wi1 * sq(vi) + pres - fyy;
-    f[5] = wi1 * vi * wi - fyz;
-    f[6] = wi1 * vi * (wi5 + pres - pinfl) - fey;
-    f[7] = wi1 * sq(wi) + pres - fzz;
-    // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
-    // parity path keeps it, qfix (a flagged non-reference option) restores it
-    f[8] = qfix ? wi1 * wi * (wi5 + pres - pinfl) - fez
-                : wi1 * (wi5 + pres - pinfl) - fez;
-  } else {
-    const double wi1 = v1 + dn[0];
-    const double ui = (v2 + dn[1]) / wi1, vi = (v3 + dn[2]) / wi1, wi = (v4 + dn[3]) / wi1;
-    const double wi5 = v5 + dn[4];
-    const double pres = gam1 * (wi5 - .5 * wi1 * (sq(ui) + sq(vi) + sq(wi)) - pinfl);
-    const double qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
-    const double fxx = v2 * qu + p;
-    const double fxy = v3 * qu;
-    const double fxz = v4 * qu;
-    const double fyy = v3 * qv + p;
-    const double fyz = v4 * qv;
-    const double fzz = v4 * qw + p;
-    const double fex = (v5 + p - pinfl) * v2 / v1;
-    const double fey = (v5 + p - pinfl) * v3 / v1;
-    const double fez = (v5 + p - pinfl) * v4 / v1;
-    f[0] = wi1 * sq(ui) + pres - fxx;
-    f[1] = wi1 * ui * vi - fxy;
-    f[2] = wi1 * ui * wi - fxz;
-    f[3] = ui * (wi5 + pres - pinfl) - fex;
-    f[4] = wi1 * sq(vi) + pres - fyy;
-    f[5] = wi1 * vi * wi - fyz;
-    f[6] = vi * (wi5 + pres - pinfl) - fey;
-    f[7] = wi1 * sq(wi) + pres - fzz;
-    f[8] = wi * (wi5 + pres - pinfl) - fez;
-  }
-#pragma unroll
-  for (int a = 0; a < 9; ++a) df_out[a * ld + n] = f[a];
-}
-
-// per-tile partial residual norms of (v_new - v_old)/dt (residu.f90:127-182)
-__device__ __forceinline__ void norm_tile_reduce(const double res[5], bool valid,
-                                                 double* out15) {
-  __shared__ double sh[kTile / 32][15];
-  double a1[5], a2[5], am[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-    a1[a] = valid ? fabs(res[a]) : 0.;
-    a2[a] = valid ? res[a] * res[a] : 0.;
-    am[a] = a1[a];
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      a1[a] = a1[a] + __shfl_down_sync(0xffffffffu, a1[a], off);
-      a2[a] = a2[a] + __shfl_down_sync(0xffffffffu, a2[a], off);
-      am[a] = fmax(am[a], __shfl_down_sync(0xffffffffu, am[a], off));
-    }
-  }
-  const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      sh[w][a] = a1[a];
-      sh[w][5 + a] = a2[a];
-      sh[w][10 + a] = am[a];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 15) {
-    const int q = threadIdx.x;
-    double s = sh[0][q];
-    for (int ww = 1; ww < kTile / 32; ++ww) s = (q >= 10) ? fmax(s, sh[ww][q]) : s + sh[ww][q];
-    out15[q] = s;
-  }
-}
-
-// v += d on the real cells (implimf_*.f90 final update), the residual norm
-// partials and, when requested, the final increment copied to d_out
-__global__ void __launch_bounds__(kTile) k_update(const Blk* __restrict__ blks,
-                                                  Space sp, long long ld,
-                                                  const double* __restrict__ d,
-                                                  double* __restrict__ v,
-                                                  const double* __restrict__ dt,
-                                                  double* d_out, double* normpart) {
-  int b, i, j, k;
-  const bool valid = space_elem(sp, threadIdx.x, b, i, j, k);
-  double res[5] = {0., 0., 0., 0., 0.};
-  if (valid) {
-    const long long n = cell_index(blks[b], i, j, k);
-    const double t = dt[n];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      const double vo = v[a * ld + n], dd = d[a * ld + n];
-      const double vn = vo + dd;
-      v[a * ld + n] = vn;
-      if (d_out) d_out[a * ld + n] = dd;
-      res[a] = (vn - vo) / t;
-    }
-  }
-  if (normpart) norm_tile_reduce(res, valid, normpart + (long long)(sp.tile0 + blockIdx.x) * 15);
-}
 
 // standalone residual partials from stored arrays (rscpsv.f90 called with u0)
 __global__ void __launch_bounds__(kTile) k_norm_partials(
@@ -1129,62 +543,60 @@ __global__ void __launch_bounds__(kTile) k_norm_partials(
   norm_tile_reduce(res, valid, normpart + (long long)(sp.tile0 + blockIdx.x) * 15);
 }
 
-// per-block sums of the tile partials in a fixed tree order, then the
-// rscpsv.f90:79-150 combination over blocks; one CTA
-__global__ void __launch_bounds__(256) k_norm_finalize(
-    const Blk* __restrict__ blks, const int* __restrict__ blk_tile0, int b0,
-    int b1, const double* __restrict__ normpart, double* norms) {
+// per-block sums of the tile partials in a fixed tree order (one CTA per
+// block), then the rscpsv.f90:79-150 combination over blocks (one thread)
+__global__ void __launch_bounds__(256) k_norm_blocks(const int* __restrict__ blk_tile0,
+                                                    int b0, const double* __restrict__ normpart,
+                                                    double* __restrict__ blocksum) {
   __shared__ double red[256][15];
-  __shared__ double blocksum[15];
-  __shared__ double g[15];
-  __shared__ long long npts;
-  if (threadIdx.x < 15) g[threadIdx.x] = 0.;
-  if (threadIdx.x == 0) npts = 0;
-  __syncthreads();
-  for (int b = b0; b < b1; ++b) {
-    const int t0 = blk_tile0[b], t1 = blk_tile0[b + 1];
-    double loc[15];
+  const int b = b0 + blockIdx.x;
+  const int t0 = blk_tile0[b], t1 = blk_tile0[b + 1];
+  double loc[15];
 #pragma unroll
-    for (int q = 0; q < 15; ++q) loc[q] = 0.;
-    for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x)
+  for (int q = 0; q < 15; ++q) loc[q] = 0.;
+  for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 15; ++q)
+      loc[q] = (q >= 10) ? fmax(loc[q], normpart[(long long)t * 15 + q])
+                         : loc[q] + normpart[(long long)t * 15 + q];
+#pragma unroll
+  for (int q = 0; q < 15; ++q) red[threadIdx.x][q] = loc[q];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
 #pragma unroll
       for (int q = 0; q < 15; ++q)
-        loc[q] = (q >= 10) ? fmax(loc[q], normpart[(long long)t * 15 + q])
-                           : loc[q] + normpart[(long long)t * 15 + q];
-#pragma unroll
-    for (int q = 0; q < 15; ++q) red[threadIdx.x][q] = loc[q];
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if ((int)threadIdx.x < s)
-#pragma unroll
-        for (int q = 0; q < 15; ++q)
-          red[threadIdx.x][q] = (q >= 10) ? fmax(red[threadIdx.x][q], red[threadIdx.x + s][q])
-                                          : red[threadIdx.x][q] + red[threadIdx.x + s][q];
-      __syncthreads();
-    }
-    if (threadIdx.x < 15) blocksum[threadIdx.x] = red[0][threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const Blk& B = blks[b];
-      const long long nmax = (long long)(B.ni - 1) * (B.nj - 1) * (B.nk - 1);
-      const double coef = 1. / (double)nmax;
-      for (int a = 0; a < 5; ++a) {
-        const double d1 = coef * blocksum[a];
-        const double d2 = sqrt(coef * blocksum[5 + a]);
-        g[a] = g[a] + (double)nmax * d1;
-        g[5 + a] = g[5 + a] + (double)nmax * sq(d2);
-        g[10 + a] = fmax(g[10 + a], fabs(blocksum[10 + a]));
-      }
-      npts += nmax;
-    }
+        red[threadIdx.x][q] = (q >= 10) ? fmax(red[threadIdx.x][q], red[threadIdx.x + s][q])
+                                        : red[threadIdx.x][q] + red[threadIdx.x + s][q];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 15) blocksum[(long long)blockIdx.x * 15 + threadIdx.x] = red[0][threadIdx.x];
+}
+
+__global__ void k_norm_combine(const Blk* __restrict__ blks, int b0, int b1,
+                               const double* __restrict__ blocksum, double* norms) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double g[15];
+  for (int q = 0; q < 15; ++q) g[q] = 0.;
+  long long npts = 0;
+  for (int b = b0; b < b1; ++b) {
+    const Blk& B = blks[b];
+    const double* bs = blocksum + (long long)(b - b0) * 15;
+    const long long nmax = (long long)(B.ni - 1) * (B.nj - 1) * (B.nk - 1);
+    const double coef = 1. / (double)nmax;
     for (int a = 0; a < 5; ++a) {
-      norms[a] = g[a] / (double)npts;
-      norms[5 + a] = sqrt(g[5 + a] / (double)npts);
-      norms[10 + a] = g[10 + a];
+      const double d1 = coef * bs[a];
+      const double d2 = sqrt(coef * bs[5 + a]);
+      g[a] = g[a] + (double)nmax * d1;
+      g[5 + a] = g[5 + a] + (double)nmax * sq(d2);
+      g[10 + a] = fmax(g[10 + a], fabs(bs[10 + a]));
     }
+    npts += nmax;
+  }
+  for (int a = 0; a < 5; ++a) {
+    norms[a] = g[a] / (double)npts;
+    norms[5 + a] = sqrt(g[5 + a] / (double)npts);
+    norms[10 + a] = g[10 + a];
   }
 }
 
@@ -1213,7 +625,17 @@ cudaError_t launch_zvismo(const Blk* blks, Space sp, Phys ph, double* mu,
 cudaError_t launch_prim(long long n0, long long n1, const double* v, long long ld,
                         double* prim, cudaStream_t st) {
   if (n1 > n0)
-    k_prim<<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(n0, n1, v, ld, prim);
+    k_prim<false><<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(n0, n1, v, ld, prim, nullptr,
+                                                                nullptr, nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
+                               const double* ps, float* v32, float* prim32, float* ps32,
+                               cudaStream_t st) {
+  if (ncells > 0)
+    k_prim<true><<<(int)((ncells + 255) / 256), 256, 0, st>>>(0, ncells, v, ld, prim, ps, v32,
+                                                              prim32, ps32);
   return cudaGetLastError();
 }
 
@@ -1260,39 +682,138 @@ cudaError_t launch_grad(const Blk* blks, Space sp, Phys ph, const double* v,
   return cudaGetLastError();
 }
 
-cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
-                         const double* v, const double* prim, long long ld,
-                         const double* ps, double* R, cudaStream_t st) {
+template <>
+cudaError_t launch_ratio_t<double>(const Blk* blks, const SpaceBuf* lines, int l0,
+                                   const double* v, const double* prim, long long ld,
+                                   const double* ps, double* R, cudaStream_t st) {
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = lines[dir].view(l0);
     if (sp.ntiles > 0)
-      k_ratio<<<dim3(grid_of(sp), 5), kTile, 0, st>>>(blks, sp, dir, v, prim, ld, ps, R);
+      k_ratio<double><<<dim3(grid_of(sp), 5), kTile, 0, st>>>(blks, sp, dir, v, prim, ld, ps, R);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
-                             Phys ph, Scheme sc, const double* v,
-                             const double* prim, long long ld, const double* ps,
-                             const double* tau, const double* sn, const double* R,
-                             double* G, cudaStream_t st) {
+template <>
+cudaError_t launch_face_flux_t<double>(const Blk* blks, const SpaceBuf* faces, int l0,
+                                       Phys ph, Scheme sc, const double* v,
+                                       const double* prim, long long ld,
+                                       const double* ps, const double* tau,
+                                       const double* sn, const double* R, double* G,
+                                       cudaStream_t st) {
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = faces[dir].view(l0);
     if (sp.ntiles == 0) continue;
     if (sc.ns)
-      k_face_flux<true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
-                                                       ld, ps, tau, sn, R, G);
+      k_face_flux<double, true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                               prim, ld, ps, tau, sn, R, G);
     else
-      k_face_flux<false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
-                                                        ld, ps, tau, sn, R, G);
+      k_face_flux<double, false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                                prim, ld, ps, tau, sn, R, G);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
-                              long long ld, double* u, cudaStream_t st) {
-  if (sp.ntiles > 0) k_accumulate<<<grid_of(sp), kTile, 0, st>>>(blks, sp, G, ld, u);
+template <>
+cudaError_t launch_accumulate_t<double>(const Blk* blks, Space sp, const double* G,
+                                        long long ld, const double* corr, double* u,
+                                        float* u32, cudaStream_t st) {
+  if (sp.ntiles > 0)
+    k_accumulate<double><<<grid_of(sp), kTile, 0, st>>>(blks, sp, G, ld, corr, u, u32);
   return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_sweeps_t<double>(const Blk* blks, Space cells, Phys ph, Scheme sc,
+                                    int eu, int lmx, long long ld, const double* u,
+                                    const double* v, const double* prim,
+                                    const double* ps, const double* sn,
+                                    const double* coefe, const double* coefdiag,
+                                    double* const dpp[2], double* const dfpp[2],
+                                    int* cur_out, cudaStream_t st) {
+  const int g = grid_of(cells);
+  int cur = 0;
+  if (lmx == 0) {
+    cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(double) * 5 * ld, st);
+    if (e0 != cudaSuccess) return e0;
+  }
+  for (int ls = 1; ls <= lmx; ++ls) {
+    const int nxt = (ls == 1) ? 0 : 1 - cur;
+    const double* din = dpp[cur];
+    const double* dfin = dfpp[cur];
+    double* dout = dpp[nxt];
+    double* dfout = dfpp[nxt];
+    const int q = eu ? sc.qfix_dfez : 0;
+    if (eu) {
+      if (ls == 1)
+        k_jacobi<double, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                          ps, sn, coefe, coefdiag, din, dfin,
+                                                          dout, dfout);
+      else
+        k_jacobi<double, true, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                           ps, sn, coefe, coefdiag, din, dfin,
+                                                           dout, dfout);
+    } else {
+      if (ls == 1)
+        k_jacobi<double, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                           ps, sn, coefe, coefdiag, din, dfin,
+                                                           dout, dfout);
+      else
+        k_jacobi<double, false, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                            prim, ps, sn, coefe, coefdiag, din,
+                                                            dfin, dout, dfout);
+    }
+    cur = nxt;
+  }
+  *cur_out = cur;
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_update_t<double>(const Blk* blks, Space cells, long long ld,
+                                    const double* d, double* v, const double* dt,
+                                    double* d_out, double* normpart, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_update<double><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, d, v, dt, d_out,
+                                                       normpart);
+  return cudaGetLastError();
+}
+
+// implicit coefficients computed in FP64 (coefdiag seed, face spectral radii,
+// diagonal); TO copies for the reduced-precision sweeps when given
+template <class TO>
+static cudaError_t implicit_coefficients(const Blk* blks, Space cells,
+                                         const SpaceBuf* faces, int l0, Phys ph, int eu,
+                                         const double* dt, const double* v,
+                                         const double* prim, const double* mu,
+                                         const double* mut, const double* sn,
+                                         const double* vol, const double* cson, Work& w,
+                                         TO* coefe_out, TO* coefdiag_out, cudaStream_t st) {
+  const long long ld = w.ld;
+  const int g = grid_of(cells);
+  k_impl_cell0<<<g, kTile, 0, st>>>(blks, cells, ph, eu, v, dt, mu, mut, vol, w.coefdiag,
+                                    w.rv);
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space fs = faces[dir].view(l0);
+    if (fs.ntiles > 0)
+      k_impl_coefe<TO><<<fs.ntiles, kTile, 0, st>>>(blks, fs, dir, eu, v, prim, ld, sn, vol,
+                                                    cson, w.rv, w.coefe, coefe_out);
+  }
+  k_impl_diag<TO><<<g, kTile, 0, st>>>(blks, cells, ld, w.coefe, w.coefdiag, coefdiag_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
+                                         const SpaceBuf* faces, int l0, Phys ph, int eu,
+                                         const double* dt, const double* v,
+                                         const double* prim, const double* mu,
+                                         const double* mut, const double* sn,
+                                         const double* vol, const double* cson, Work& w,
+                                         float* coefe32, float* coefdiag32,
+                                         cudaStream_t st) {
+  if (cells.ntiles == 0) return cudaSuccess;
+  return implicit_coefficients<float>(blks, cells, faces, l0, ph, eu, dt, v, prim, mu, mut,
+                                      sn, vol, cson, w, coefe32, coefdiag32, st);
 }
 
 cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
@@ -1302,54 +823,19 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
                             const double* sn, const double* vol,
                             const double* ps, const double* cson, Work& w,
                             int want_norms, cudaStream_t st) {
-  const double* prim = w.prim;
   const long long ld = w.ld;
   if (cells.ntiles == 0) return cudaSuccess;
-  const int g = grid_of(cells);
-  k_impl_cell0<<<g, kTile, 0, st>>>(blks, cells, ph, eu, v, dt, mu, mut, vol,
-                                    w.coefdiag, w.rv);
-  for (int dir = 0; dir < 3; ++dir) {
-    const Space fs = faces[dir].view(l0);
-    if (fs.ntiles > 0)
-      k_impl_coefe<<<fs.ntiles, kTile, 0, st>>>(blks, fs, dir, eu, v, prim, ld, sn,
-                                                vol, cson, w.rv, w.coefe);
-  }
-  k_impl_diag<<<g, kTile, 0, st>>>(blks, cells, ld, w.coefe, w.coefdiag);
-  int cur = 0;  // index of the buffer holding the latest iterate
-  if (lmx == 0) {
-    cudaError_t e0 = cudaMemsetAsync(w.dpp[0], 0, sizeof(double) * 5 * ld, st);
-    if (e0 != cudaSuccess) return e0;
-  }
-  for (int ls = 1; ls <= lmx; ++ls) {
-    const int nxt = (ls == 1) ? 0 : 1 - cur;
-    const double* din = w.dpp[cur];
-    const double* dfin = w.dfpp[cur];
-    double* dout = w.dpp[nxt];
-    double* dfout = w.dfpp[nxt];
-    if (eu) {
-      if (ls == 1)
-        k_jacobi<true, true><<<g, kTile, 0, st>>>(blks, cells, ph, sc.qfix_dfez, ld, u, v,
-                                                  prim, ps, sn, w.coefe, w.coefdiag, din,
-                                                  dfin, dout, dfout);
-      else
-        k_jacobi<true, false><<<g, kTile, 0, st>>>(blks, cells, ph, sc.qfix_dfez, ld, u, v,
-                                                   prim, ps, sn, w.coefe, w.coefdiag, din,
-                                                   dfin, dout, dfout);
-    } else {
-      if (ls == 1)
-        k_jacobi<false, true><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, prim, ps,
-                                                   sn, w.coefe, w.coefdiag, din,
-                                                   dfin, dout, dfout);
-      else
-        k_jacobi<false, false><<<g, kTile, 0, st>>>(blks, cells, ph, 0, ld, u, v, prim, ps,
-                                                    sn, w.coefe, w.coefdiag, din,
-                                                    dfin, dout, dfout);
-    }
-    cur = nxt;
-  }
-  k_update<<<g, kTile, 0, st>>>(blks, cells, ld, w.dpp[cur], v, dt, d_out,
-                                want_norms ? w.normpart : nullptr);
-  return cudaGetLastError();
+  cudaError_t e = implicit_coefficients<double>(blks, cells, faces, l0, ph, eu, dt, v, w.prim,
+                                                mu, mut, sn, vol, cson, w, nullptr, nullptr,
+                                                st);
+  int cur = 0;
+  if (e == cudaSuccess)
+    e = launch_sweeps_t<double>(blks, cells, ph, sc, eu, lmx, ld, u, v, w.prim, ps, sn,
+                                w.coefe, w.coefdiag, w.dpp, w.dfpp, &cur, st);
+  if (e == cudaSuccess)
+    e = launch_update_t<double>(blks, cells, ld, w.dpp[cur], v, dt, d_out,
+                                want_norms ? w.normpart : nullptr, st);
+  return e;
 }
 
 cudaError_t launch_norm_partials(const Blk* blks, Space cells, long long ld,
@@ -1363,8 +849,10 @@ cudaError_t launch_norm_partials(const Blk* blks, Space cells, long long ld,
 
 cudaError_t launch_norm_finalize(const Blk* blks, const int* blk_tile0_dev,
                                  int b0, int b1, const double* normpart,
-                                 double* norms, cudaStream_t st) {
-  k_norm_finalize<<<1, 256, 0, st>>>(blks, blk_tile0_dev, b0, b1, normpart, norms);
+                                 double* blocksum, double* norms, cudaStream_t st) {
+  if (b1 <= b0) return cudaSuccess;
+  k_norm_blocks<<<b1 - b0, 256, 0, st>>>(blk_tile0_dev, b0, normpart, blocksum);
+  k_norm_combine<<<1, 32, 0, st>>>(blks, b0, b1, blocksum, norms);
   return cudaGetLastError();
 }
 

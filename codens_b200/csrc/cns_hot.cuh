@@ -1,0 +1,955 @@
+// cns_hot.cuh -- the hot kernels of the iteration, templated on the real type
+// T of their arithmetic and storage:
+//   k_ratio       limiter slope-ratio recurrence (sch_roe.f90:146-194)
+//   k_face_flux   Roe-MUSCL face flux, Euler or Navier-Stokes (sch_roe*.f90)
+//   k_accumulate  face-owned residual accumulation, always summed in FP64
+//   k_jacobi      one point-Jacobi sweep (implimf_eu.f90, implimf_3d.f90)
+//   k_update      v += d in FP64 and the residual-norm partials
+//
+// The FP64 instantiations (cns_flow.cu, built with --fmad=false) evaluate the
+// reference expressions in the reference's order and are bit-identical to
+// the reference semantics.  The FP32 instantiations (cns_mixed.cu, built with
+// FMA contraction) are the reduced-precision half of the mixed-precision
+// form, where FP64 stays for metrics, the residual accumulation, the state
+// update and the norms.  Every literal is written T(...) so that the FP32
+// instantiation never promotes to double.
+//
+// Included by exactly one translation unit per precision; all kernels live in
+// an anonymous namespace.
+#pragma once
+#include <cfloat>
+
+#include "cns_kernels.cuh"
+
+namespace cns {
+namespace {
+
+template <class T>
+struct PhysT {
+  T gam, gam1, pinfl;
+  __device__ explicit PhysT(const Phys& p) : gam(T(p.gam)), gam1(T(p.gam1)), pinfl(T(p.pinfl)) {}
+};
+
+template <class T>
+__device__ __forceinline__ T sqT(T a) { return a * a; }
+
+template <class T>
+__device__ __forceinline__ T tinyT();
+template <>
+__device__ __forceinline__ double tinyT<double>() { return 2.2250738585072014e-308; }
+template <>
+__device__ __forceinline__ float tinyT<float>() { return FLT_MIN; }
+
+// ---------------------------------------------------------------------------
+// limiter ratios
+// ---------------------------------------------------------------------------
+
+// One thread walks one grid line for one of the five variables (blockIdx.y:
+// rho, u, v, w, p).  The ratio at face m divides by the ALREADY UPDATED ratio
+// of face m-1 and resets to 1 when |r(m-1) r(m) r(m+1)| <= tiny: a
+// sequential line recurrence, kept as such.
+template <class T>
+__global__ void __launch_bounds__(kTile) k_ratio(const Blk* __restrict__ blks,
+                                                 Space sp, int dir,
+                                                 const T* __restrict__ v,
+                                                 const T* __restrict__ prim,
+                                                 long long ld,
+                                                 const T* __restrict__ ps,
+                                                 T* __restrict__ R) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const int nd = nd_of(B, dir);
+  if (nd < 3) return;
+  const long long inc = ninc_of(B, dir);
+  const int a = blockIdx.y;
+  const T* x = a == 0 ? v : (a == 4 ? ps : prim + (long long)(a - 1) * ld);
+  T* Ra = R + ((long long)dir * 5 + a) * ld;
+  const long long n0 = cell_index(B, i, j, k) - inc;   // position 0 of the line
+  T x0 = x[n0], x1 = x[n0 + inc], x2 = x[n0 + 2 * inc];
+  T rprev = x1 - x0;   // face 1 (never updated)
+  T dcur = x2 - x1;    // face 2
+  for (int f = 2; f <= nd - 1; ++f) {
+    const long long n = n0 + (long long)f * inc;
+    const T x3 = x[n + inc];
+    const T dnext = x3 - x2;
+    T r;
+    if (fabs(rprev * dcur * dnext) <= tinyT<T>())
+      r = T(1.);
+    else
+      r = dcur / rprev;
+    Ra[n] = r;
+    rprev = r;
+    dcur = dnext;
+    x2 = x3;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Roe-MUSCL face flux
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ T phi_mm(T a) {  // minmod, sch_roe.f90:1500-1504
+  const T m = (a < T(1.)) ? a : T(1.);
+  return (m > T(0.)) ? m : T(0.);
+}
+
+// kappa-MUSCL without limiter (sch_roe_euler.f90:245-273); cells c[0..3] are
+// n-2, n-1, n, n+1 as (rho, u, v, w, p)
+template <class T>
+__device__ __forceinline__ void muscl_plain(const T c[4][5], T c4, T xk, T WL[5],
+                                            T WR[5]) {
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    WL[a] = c[1][a] + c4 * ((T(1.) - xk) * (c[1][a] - c[0][a]) +
+                            (T(1.) + xk) * (c[2][a] - c[1][a]));
+    WR[a] = c[2][a] - c4 * ((T(1.) + xk) * (c[2][a] - c[1][a]) +
+                            (T(1.) - xk) * (c[3][a] - c[2][a]));
+  }
+}
+
+// limited MUSCL (sch_roe.f90:196-227): rho and p use one product order, the
+// velocities another; rm are the ratios at this face, rp at the next
+template <class T>
+__device__ __forceinline__ void muscl_limited(const T c[4][5], T c4, int muscl,
+                                              T xk, const T rm[5], const T rp[5],
+                                              T WL[5], T WR[5]) {
+  const T mu = T(muscl);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    if (a == 0 || a == 4) {
+      WL[a] = c[1][a] + c4 * phi_mm(rm[a]) * (T(1.) - xk) * (c[1][a] - c[0][a]) +
+              c4 * phi_mm(T(1.) / rm[a]) * (T(1.) + xk) * (c[2][a] - c[1][a]);
+      WR[a] = c[2][a] - c4 * phi_mm(rp[a]) * (T(1.) + xk) * (c[2][a] - c[1][a]) -
+              c4 * phi_mm(T(1.) / rp[a]) * (T(1.) - xk) * (c[3][a] - c[2][a]);
+    } else {
+      WL[a] = c[1][a] + c4 * phi_mm(rm[a]) * (T(1.) - xk) * (c[1][a] - c[0][a]) +
+              (T(1.) + xk) * (c[2][a] - c[1][a]) * T(0.25) * mu * phi_mm(T(1.) / rm[a]);
+      WR[a] = c[2][a] - c4 * phi_mm(rp[a]) * (T(1.) + xk) * (c[2][a] - c[1][a]) -
+              (T(1.) - xk) * (c[3][a] - c[2][a]) * T(0.25) * mu * phi_mm(T(1.) / rp[a]);
+    }
+  }
+}
+
+// row r of the right eigenvector matrix P at the Roe state
+template <class T>
+__device__ __forceinline__ void p_row(int r, T nx, T ny, T nz, T um, T vm, T wm,
+                                      T hm, T am, T vn, T vitm2, T rhom, T rhoiam,
+                                      T p[5]) {
+  const T h = T(0.5);
+  switch (r) {
+    case 0:
+      p[0] = nx; p[1] = ny; p[2] = nz;
+      p[3] = h * rhoiam; p[4] = h * rhoiam;
+      break;
+    case 1:
+      p[0] = um * nx; p[1] = um * ny - rhom * nz; p[2] = um * nz + rhom * ny;
+      p[3] = h * rhoiam * (um + nx * am); p[4] = h * rhoiam * (um - nx * am);
+      break;
+    case 2:
+      p[0] = vm * nx + rhom * nz; p[1] = vm * ny; p[2] = vm * nz - rhom * nx;
+      p[3] = h * rhoiam * (vm + ny * am); p[4] = h * rhoiam * (vm - ny * am);
+      break;
+    case 3:
+      p[0] = wm * nx - rhom * ny; p[1] = wm * ny + rhom * nx; p[2] = wm * nz;
+      p[3] = h * rhoiam * (wm + nz * am); p[4] = h * rhoiam * (wm - nz * am);
+      break;
+    default:
+      p[0] = vitm2 * nx + rhom * (vm * nz - wm * ny);
+      p[1] = vitm2 * ny + rhom * (wm * nx - um * nz);
+      p[2] = vitm2 * nz + rhom * (um * ny - vm * nx);
+      p[3] = h * rhoiam * (hm + am * vn);
+      p[4] = h * rhoiam * (hm - am * vn);
+  }
+}
+
+// Roe dissipation |A|(W_R - W_L) of sch_roe_euler.f90:284-402 (di), plus the
+// specific total energies el, er used by the centred part
+template <class T>
+__device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T sx,
+                                                T sy, T sz, bool absam,
+                                                const PhysT<T>& ph, T di[5],
+                                                T& el, T& er) {
+  const T gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl;
+  const T one = T(1.), h = T(0.5);
+  const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const T cnds = sqrt(sx * sx + sy * sy + sz * sz);
+  const T nx = sx / cnds, ny = sy / cnds, nz = sz / cnds;
+  const T al = sqrt(gam * pl / rhol);
+  const T ar = sqrt(gam * prr / rhor);
+  const T q2l = sqT(ul) + sqT(vl) + sqT(wl);
+  const T q2r = sqT(ur) + sqT(vr) + sqT(wr);
+  const T hl = al * al / gam1 + h * q2l;
+  const T hr = ar * ar / gam1 + h * q2r;
+  el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
+  er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
+  const T gd = sqrt(rhor / rhol);
+  const T gd1 = one / (one + gd);
+  const T gd2 = gd * gd1;
+  const T rhom = sqrt(rhol * rhor);
+  const T rhomi = one / rhom;
+  const T um = gd1 * ul + gd2 * ur;
+  const T vm = gd1 * vl + gd2 * vr;
+  const T wm = gd1 * wl + gd2 * wr;
+  const T hm = gd1 * hl + gd2 * hr;
+  const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
+  const T am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
+  const T am2i = one / (am * am);
+  const T vn = um * nx + vm * ny + wm * nz;
+  const T rhoiam = rhom / am;
+  const T rhoami = am2i / rhoiam;
+  const T lam1 = fabs(vn * cnds);
+  const T lam4 = fabs(vn * cnds + am * cnds);
+  const T lam5 = fabs(vn * cnds - am * cnds);
+  T q[5][5];
+  q[0][0] = (one - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi;
+  q[0][1] = gam1 * um * nx * am2i;
+  q[0][2] = gam1 * vm * nx * am2i + nz * rhomi;
+  q[0][3] = gam1 * wm * nx * am2i - ny * rhomi;
+  q[0][4] = -gam1 * nx * am2i;
+  q[1][0] = (one - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi;
+  q[1][1] = gam1 * um * ny * am2i - nz * rhomi;
+  q[1][2] = gam1 * vm * ny * am2i;
+  q[1][3] = gam1 * wm * ny * am2i + nx * rhomi;
+  q[1][4] = -gam1 * ny * am2i;
+  q[2][0] = (one - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi;
+  q[2][1] = gam1 * um * nz * am2i + ny * rhomi;
+  q[2][2] = gam1 * vm * nz * am2i - nx * rhomi;
+  q[2][3] = gam1 * wm * nz * am2i;
+  q[2][4] = -gam1 * nz * am2i;
+  q[3][0] = gam1 * vitm2 * rhoami - vn * rhomi;
+  q[3][1] = nx * rhomi - gam1 * um * rhoami;
+  q[3][2] = ny * rhomi - gam1 * vm * rhoami;
+  q[3][3] = nz * rhomi - gam1 * wm * rhoami;
+  q[3][4] = gam1 * rhoami;
+  q[4][0] = gam1 * vitm2 * rhoami + vn * rhomi;
+  q[4][1] = -nx * rhomi - gam1 * um * rhoami;
+  q[4][2] = -ny * rhomi - gam1 * vm * rhoami;
+  q[4][3] = -nz * rhomi - gam1 * wm * rhoami;
+  q[4][4] = gam1 * rhoami;
+  T dw[5];
+  dw[0] = rhor - rhol;
+  dw[1] = rhor * ur - rhol * ul;
+  dw[2] = rhor * vr - rhol * vl;
+  dw[3] = rhor * wr - rhol * wl;
+  dw[4] = rhor * er - rhol * el;
+  const T lam[5] = {lam1, lam1, lam1, lam4, lam5};
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    T p[5];
+    p_row(r, nx, ny, nz, um, vm, wm, hm, am, vn, vitm2, rhom, rhoiam, p);
+    T pl_[5];
+#pragma unroll
+    for (int kk = 0; kk < 5; ++kk) pl_[kk] = p[kk] * lam[kk];
+    T acc = T(0.);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      T a = pl_[0] * q[0][c];
+#pragma unroll
+      for (int kk = 1; kk < 5; ++kk) a = a + pl_[kk] * q[kk][c];
+      acc = (c == 0) ? a * dw[0] : acc + a * dw[c];
+    }
+    di[r] = acc;
+  }
+}
+
+// primitive (rho, u, v, w, p) of cell n
+template <class T>
+__device__ __forceinline__ void load_prim(const T* __restrict__ v,
+                                          const T* __restrict__ prim,
+                                          const T* __restrict__ ps, long long ld,
+                                          long long n, T c[5]) {
+  c[0] = v[n];
+  c[1] = prim[n];
+  c[2] = prim[ld + n];
+  c[3] = prim[2 * ld + n];
+  c[4] = ps[n];
+}
+
+// one face per thread, direction dir: interior faces give 0.5*f (sch_roe*
+// interior loops), boundary faces give the ghost-cell physical flux s (lower
+// face 1, upper face nd).  Results go to G[dir][a][n], n the cell above the
+// face.
+template <class T, bool NS>
+__global__ void __launch_bounds__(kTile, 3) k_face_flux(
+    const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
+    const T* __restrict__ v, const T* __restrict__ prim, long long ld,
+    const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
+    const T* __restrict__ R, T* __restrict__ G) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const PhysT<T> ph(ph64);
+  const Blk& B = blks[b];
+  const long long inc = ninc_of(B, dir);
+  const int nd = nd_of(B, dir);
+  const int p = dir == 0 ? i : (dir == 1 ? j : k);
+  const long long n = cell_index(B, i, j, k);
+  const T sx = sn_ptr(sn, B, dir, 0)[n], sy = sn_ptr(sn, B, dir, 1)[n],
+          sz = sn_ptr(sn, B, dir, 2)[n];
+  const T pinfl = ph.pinfl;
+  T out[5];
+  if (p == 1 || p == nd) {
+    // boundary face: physical flux of the ghost cell (sch_roe_euler.f90:
+    // 438-513, sch_roe.f90:497-580); the Euler j/k lower faces divide the
+    // energy flux by the interior density (sch_roe_euler.f90:630-632)
+    const long long ng = (p == 1) ? n - inc : n;
+    const long long nrho = (!NS && p == 1 && dir > 0) ? n : ng;
+    const T v1 = v[ng], v2 = v[ld + ng], v3 = v[2 * ld + ng], v4 = v[3 * ld + ng],
+            v5 = v[4 * ld + ng], pg = ps[ng];
+    const T qu = prim[ng], qv = prim[ld + ng], qw = prim[2 * ld + ng];
+    T fxx, fxy, fxz, fyy, fyz, fzz, fex, fey, fez;
+    if (!NS) {
+      const T rr = v[nrho];
+      fxx = v2 * qu + pg - pinfl;
+      fxy = v3 * qu;
+      fxz = v4 * qu;
+      fyy = v3 * qv + pg - pinfl;
+      fyz = v4 * qv;
+      fzz = v4 * qw + pg - pinfl;
+      fex = (v5 + pg - pinfl) * v2 / rr;
+      fey = (v5 + pg - pinfl) * v3 / rr;
+      fez = (v5 + pg - pinfl) * v4 / rr;
+    } else {
+      const T txx = tau[ng], txy = tau[ld + ng], txz = tau[2 * ld + ng],
+              tyy = tau[3 * ld + ng], tyz = tau[4 * ld + ng], tzz = tau[5 * ld + ng],
+              qx = tau[6 * ld + ng], qy = tau[7 * ld + ng], qz = tau[8 * ld + ng];
+      fxx = v2 * qu + pg - pinfl - txx;
+      fxy = v3 * qu - txy;
+      fxz = v4 * qu - txz;
+      fyy = v3 * qv + pg - pinfl - tyy;
+      fyz = v4 * qv - tyz;
+      fzz = v4 * qw + pg - pinfl - tzz;
+      fex = ((v5 + pg - pinfl - txx) * v2 - txy * v3 - txz * v4) / v1 - qx;
+      fey = ((v5 + pg - pinfl - tyy) * v3 - txy * v2 - tyz * v4) / v1 - qy;
+      fez = ((v5 + pg - pinfl - tzz) * v4 - txz * v2 - tyz * v3) / v1 - qz;
+    }
+    out[0] = v2 * sx + v3 * sy + v4 * sz;
+    out[1] = fxx * sx + fxy * sy + fxz * sz;
+    out[2] = fxy * sx + fyy * sy + fyz * sz;
+    out[3] = fxz * sx + fyz * sy + fzz * sz;
+    out[4] = fex * sx + fey * sy + fez * sz;
+  } else {
+    T c[4][5];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) load_prim(v, prim, ps, ld, n + (long long)(s - 2) * inc, c[s]);
+    T WL[5], WR[5];
+    const T c4 = T(0.25) * T(sc.muscl);
+    const T xk = T(sc.xk);
+    if (NS && sc.ilim == 1 && p <= nd - 2) {
+      const T* Rd = R + (long long)dir * 5 * ld;
+      T rm[5], rp[5];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        rm[a] = Rd[a * ld + n];
+        rp[a] = Rd[a * ld + n + inc];
+      }
+      muscl_limited(c, c4, sc.muscl, xk, rm, rp, WL, WR);
+    } else {
+      muscl_plain(c, c4, xk, WL, WR);
+    }
+    T di[5], el, er;
+    roe_dissipation(WL, WR, sx, sy, sz, (!NS) && dir > 0, ph, di, el, er);
+    const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+    const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+    T dfxx, dfxy, dfxz, dfyy, dfyz, dfzz, dfex, dfey, dfez;
+    if (!NS) {
+      dfxx = rhor * sqT(ur) + prr - pinfl + rhol * sqT(ul) + pl - pinfl;
+      dfxy = rhor * ur * vr + rhol * ul * vl;
+      dfxz = rhor * ur * wr + rhol * ul * wl;
+      dfyy = rhor * sqT(vr) + prr - pinfl + rhol * sqT(vl) + pl - pinfl;
+      dfyz = rhor * vr * wr + rhol * vl * wl;
+      dfzz = rhor * sqT(wr) + prr - pinfl + rhol * sqT(wl) + pl - pinfl;
+      dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul;
+      dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl;
+      dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl;
+    } else {
+      const long long nR = n, nL = n - inc;
+      const T txxR = tau[nR], txyR = tau[ld + nR], txzR = tau[2 * ld + nR],
+              tyyR = tau[3 * ld + nR], tyzR = tau[4 * ld + nR], tzzR = tau[5 * ld + nR];
+      const T txxL = tau[nL], txyL = tau[ld + nL], txzL = tau[2 * ld + nL],
+              tyyL = tau[3 * ld + nL], tyzL = tau[4 * ld + nL], tzzL = tau[5 * ld + nL];
+      dfxx = rhor * sqT(ur) + prr - pinfl - txxR + rhol * sqT(ul) + pl - pinfl - txxL;
+      dfxy = rhor * ur * vr - txyR + rhol * ul * vl - txyL;
+      dfxz = rhor * ur * wr - txzR + rhol * ul * wl - txzL;
+      dfyy = rhor * sqT(vr) + prr - pinfl - tyyR + rhol * sqT(vl) + pl - pinfl - tyyL;
+      dfyz = rhor * vr * wr - tyzR + rhol * vl * wl - tyzL;
+      dfzz = rhor * sqT(wr) + prr - pinfl - tzzR + rhol * sqT(wl) + pl - pinfl - tzzL;
+      dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul -
+             (txxR * ur + txyR * vr + txzR * wr) - (txxL * ul + txyL * vl + txzL * wl) -
+             tau[6 * ld + nR] - tau[6 * ld + nL];
+      dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl -
+             (txyR * ur + tyyR * vr + tyzR * wr) - (txyL * ul + tyyL * vl + tyzL * wl) -
+             tau[7 * ld + nR] - tau[7 * ld + nL];
+      dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl -
+             (txzR * ur + tyzR * vr + tzzR * wr) - (txzL * ul + tyzL * vl + tzzL * wl) -
+             tau[8 * ld + nR] - tau[8 * ld + nL];
+    }
+    const T f1 = (rhor * ur + rhol * ul) * sx + (rhor * vr + rhol * vl) * sy +
+                 (rhor * wr + rhol * wl) * sz - di[0];
+    const T f2 = dfxx * sx + dfxy * sy + dfxz * sz - di[1];
+    const T f3 = dfxy * sx + dfyy * sy + dfyz * sz - di[2];
+    const T f4 = dfxz * sx + dfyz * sy + dfzz * sz - di[3];
+    const T f5 = dfex * sx + dfey * sy + dfez * sz - di[4];
+    out[0] = T(0.5) * f1;
+    out[1] = T(0.5) * f2;
+    out[2] = T(0.5) * f3;
+    out[3] = T(0.5) * f4;
+    out[4] = T(0.5) * f5;
+  }
+  T* Gd = G + (long long)dir * 5 * ld;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
+}
+
+// u(n) from the six faces of the cell, summed in FP64 in the reference's
+// order; with corr (defect correction, FP64) u = that sum + corr; with u32 a
+// single-precision copy of u is written too
+template <class T>
+__global__ void __launch_bounds__(kTile) k_accumulate(const Blk* __restrict__ blks,
+                                                      Space sp, const T* __restrict__ G,
+                                                      long long ld,
+                                                      const double* __restrict__ corr,
+                                                      double* __restrict__ u,
+                                                      float* __restrict__ u32) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  double acc[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long inc = ninc_of(B, dir);
+    const int nd = nd_of(B, dir);
+    const int p = dir == 0 ? i : (dir == 1 ? j : k);
+    const bool upper_first = (p == 1) && nd >= 3;
+    const T* Gd = G + (long long)dir * 5 * ld;
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      const double gl = (double)Gd[a * ld + n], gu = (double)Gd[a * ld + n + inc];
+      if (upper_first) {
+        acc[a] = acc[a] + gu;
+        acc[a] = acc[a] - gl;
+      } else {
+        acc[a] = acc[a] - gl;
+        acc[a] = acc[a] + gu;
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const double r = corr ? acc[a] + corr[a * ld + n] : acc[a];
+    if (u) u[a * ld + n] = r;
+    if (u32) u32[a * ld + n] = (float)r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// implicit phase: matrix-free point Jacobi
+// ---------------------------------------------------------------------------
+
+// df index: 0 xx, 1 xy, 2 xz, 3 ex, 4 yy, 5 yz, 6 ey, 7 zz, 8 ez
+
+// flux-increment projections tn(1..5) on the face between cells nu (above)
+// and nl (below) (implimf_eu.f90:272-291, implimf_3d.f90:243-262)
+template <class T, bool EU, bool FIRST>
+__device__ __forceinline__ void jacobi_tn(const T* __restrict__ d,
+                                          const T* __restrict__ df, long long ld,
+                                          long long nu, long long nl, T sx, T sy,
+                                          T sz, T tn[5]) {
+  T a2, a3, a4, fxx, fxy, fxz, fex, fyy, fyz, fey, fzz, fez;
+  if (FIRST) {
+    a2 = a3 = a4 = T(0.) + T(0.);
+    fxx = fxy = fxz = fex = fyy = fyz = fey = fzz = fez = T(0.) + T(0.);
+  } else {
+    a2 = d[ld + nu] + d[ld + nl];
+    a3 = d[2 * ld + nu] + d[2 * ld + nl];
+    a4 = d[3 * ld + nu] + d[3 * ld + nl];
+    fxx = df[nu] + df[nl];
+    fxy = df[ld + nu] + df[ld + nl];
+    fxz = df[2 * ld + nu] + df[2 * ld + nl];
+    fex = df[3 * ld + nu] + df[3 * ld + nl];
+    fyy = df[4 * ld + nu] + df[4 * ld + nl];
+    fyz = df[5 * ld + nu] + df[5 * ld + nl];
+    fey = df[6 * ld + nu] + df[6 * ld + nl];
+    fzz = df[7 * ld + nu] + df[7 * ld + nl];
+    fez = df[8 * ld + nu] + df[8 * ld + nl];
+  }
+  const T h = T(0.5);
+  if (EU) {
+    tn[0] = h * (a2 * sx + a3 * sy + a4 * sz);
+    tn[1] = h * (fxx * sx + fxy * sy + fxz * sz);
+    tn[2] = h * (fxy * sx + fyy * sy + fyz * sz);
+    tn[3] = h * (fxz * sx + fyz * sy + fzz * sz);
+    tn[4] = h * (fex * sx + fey * sy + fez * sz);
+  } else {
+    tn[0] = h * a2 * sx + h * a3 * sy + h * a4 * sz;
+    tn[1] = h * fxx * sx + h * fxy * sy + h * fxz * sz;
+    tn[2] = h * fxy * sx + h * fyy * sy + h * fyz * sz;
+    tn[3] = h * fxz * sx + h * fyz * sy + h * fzz * sz;
+    tn[4] = h * fex * sx + h * fey * sy + h * fez * sz;
+  }
+}
+
+// one Jacobi sub-iteration on one real cell: d2w = -u + sum over the faces,
+// d = d2w / coefdiag, then the flux increments of v+d (implimf_eu.f90:
+// 176-323, implimf_3d.f90:222-466).  Reads the previous iterate (d_in,
+// df_in), writes the next one; FIRST: the previous iterate is zero.
+template <class T, bool EU, bool FIRST>
+__global__ void __launch_bounds__(kTile) k_jacobi(
+    const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
+    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
+    const T* __restrict__ coefdiag, const T* __restrict__ d_in,
+    const T* __restrict__ df_in, T* __restrict__ d_out, T* __restrict__ df_out) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  T d2w[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long inc = ninc_of(B, dir);
+    const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
+            *s2 = sn_ptr(sn, B, dir, 2);
+    const T* ce = coefe + (long long)dir * ld;
+    T tn[5];
+    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - inc, s0[n], s1[n], s2[n], tn);
+    const T cel = ce[n], ceu = ce[n + inc];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      const T dl = FIRST ? T(0.) : d_in[a * ld + n - inc];
+      const T du = FIRST ? T(0.) : d_in[a * ld + n + inc];
+      d2w[a] = d2w[a] + tn[a] + cel * dl + ceu * du;
+    }
+    const long long nu = n + inc;
+    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, s0[nu], s1[nu], s2[nu], tn);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
+  }
+  const T cd = coefdiag[n];
+  T dn[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    dn[a] = d2w[a] / cd;
+    d_out[a * ld + n] = dn[a];
+  }
+  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl), h = T(0.5);
+  const T v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n],
+          v5 = v[4 * ld + n], p = ps[n];
+  T f[9];
+  if (EU) {
+    const T wi1 = T(1.) / (v1 + dn[0]);
+    const T ui = v2 + dn[1], vi = v3 + dn[2], wi = v4 + dn[3], wi5 = v5 + dn[4];
+    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
+    const T norm = T(1.) / v1;
+    const T fxx = v2 * (v2 * norm) + p;
+    const T fxy = v3 * (v2 * norm);
+    const T fxz = v4 * (v2 * norm);
+    const T fyy = v3 * (v3 * norm) + p;
+    const T fyz = v4 * (v3 * norm);
+    const T fzz = v4 * (v4 * norm) + p;
+    const T fex = (v5 + p - pinfl) * v2 * norm;
+    const T fey = (v5 + p - pinfl) * v3 * norm;
+    const T fez = (v5 + p - pinfl) * v4 * norm;
+    f[0] = wi1 * sqT(ui) + pres - fxx;
+    f[1] = wi1 * ui * vi - fxy;
+    f[2] = wi1 * ui * wi - fxz;
+    f[3] = wi1 * ui * (wi5 + pres - pinfl) - fex;
+    f[4] = wi1 * sqT(vi) + pres - fyy;
+    f[5] = wi1 * vi * wi - fyz;
+    f[6] = wi1 * vi * (wi5 + pres - pinfl) - fey;
+    f[7] = wi1 * sqT(wi) + pres - fzz;
+    // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
+    // parity path keeps it, qfix (a flagged non-reference option) restores it
+    f[8] = qfix ? wi1 * wi * (wi5 + pres - pinfl) - fez
+                : wi1 * (wi5 + pres - pinfl) - fez;
+  } else {
+    const T wi1 = v1 + dn[0];
+    const T ui = (v2 + dn[1]) / wi1, vi = (v3 + dn[2]) / wi1, wi = (v4 + dn[3]) / wi1;
+    const T wi5 = v5 + dn[4];
+    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
+    const T qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
+    const T fxx = v2 * qu + p;
+    const T fxy = v3 * qu;
+    const T fxz = v4 * qu;
+    const T fyy = v3 * qv + p;
+    const T fyz = v4 * qv;
+    const T fzz = v4 * qw + p;
+    const T fex = (v5 + p - pinfl) * v2 / v1;
+    const T fey = (v5 + p - pinfl) * v3 / v1;
+    const T fez = (v5 + p - pinfl) * v4 / v1;
+    f[0] = wi1 * sqT(ui) + pres - fxx;
+    f[1] = wi1 * ui * vi - fxy;
+    f[2] = wi1 * ui * wi - fxz;
+    f[3] = ui * (wi5 + pres - pinfl) - fex;
+    f[4] = wi1 * sqT(vi) + pres - fyy;
+    f[5] = wi1 * vi * wi - fyz;
+    f[6] = vi * (wi5 + pres - pinfl) - fey;
+    f[7] = wi1 * sqT(wi) + pres - fzz;
+    f[8] = wi * (wi5 + pres - pinfl) - fez;
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a) df_out[a * ld + n] = f[a];
+}
+
+// flux increments of v+d minus those of v (implimf_eu.f90:301-312,
+// implimf_3d.f90:430-463) for one cell
+template <class T, bool EU>
+__device__ __forceinline__ void jacobi_df(const T dn[5], T v1, T v2, T v3, T v4, T v5,
+                                          T p, T qu, T qv, T qw, T gam1, T pinfl,
+                                          int qfix, T f[9]) {
+  const T h = T(0.5);
+  if (EU) {
+    const T wi1 = T(1.) / (v1 + dn[0]);
+    const T ui = v2 + dn[1], vi = v3 + dn[2], wi = v4 + dn[3], wi5 = v5 + dn[4];
+    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
+    const T norm = T(1.) / v1;
+    const T fxx = v2 * (v2 * norm) + p;
+    const T fxy = v3 * (v2 * norm);
+    const T fxz = v4 * (v2 * norm);
+    const T fyy = v3 * (v3 * norm) + p;
+    const T fyz = v4 * (v3 * norm);
+    const T fzz = v4 * (v4 * norm) + p;
+    const T fex = (v5 + p - pinfl) * v2 * norm;
+    const T fey = (v5 + p - pinfl) * v3 * norm;
+    const T fez = (v5 + p - pinfl) * v4 * norm;
+    f[0] = wi1 * sqT(ui) + pres - fxx;
+    f[1] = wi1 * ui * vi - fxy;
+    f[2] = wi1 * ui * wi - fxz;
+    f[3] = wi1 * ui * (wi5 + pres - pinfl) - fex;
+    f[4] = wi1 * sqT(vi) + pres - fyy;
+    f[5] = wi1 * vi * wi - fyz;
+    f[6] = wi1 * vi * (wi5 + pres - pinfl) - fey;
+    f[7] = wi1 * sqT(wi) + pres - fzz;
+    f[8] = qfix ? wi1 * wi * (wi5 + pres - pinfl) - fez : wi1 * (wi5 + pres - pinfl) - fez;
+  } else {
+    const T wi1 = v1 + dn[0];
+    const T ui = (v2 + dn[1]) / wi1, vi = (v3 + dn[2]) / wi1, wi = (v4 + dn[3]) / wi1;
+    const T wi5 = v5 + dn[4];
+    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
+    const T fxx = v2 * qu + p;
+    const T fxy = v3 * qu;
+    const T fxz = v4 * qu;
+    const T fyy = v3 * qv + p;
+    const T fyz = v4 * qv;
+    const T fzz = v4 * qw + p;
+    const T fex = (v5 + p - pinfl) * v2 / v1;
+    const T fey = (v5 + p - pinfl) * v3 / v1;
+    const T fez = (v5 + p - pinfl) * v4 / v1;
+    f[0] = wi1 * sqT(ui) + pres - fxx;
+    f[1] = wi1 * ui * vi - fxy;
+    f[2] = wi1 * ui * wi - fxz;
+    f[3] = ui * (wi5 + pres - pinfl) - fex;
+    f[4] = wi1 * sqT(vi) + pres - fyy;
+    f[5] = wi1 * vi * wi - fyz;
+    f[6] = vi * (wi5 + pres - pinfl) - fey;
+    f[7] = wi1 * sqT(wi) + pres - fzz;
+    f[8] = wi * (wi5 + pres - pinfl) - fez;
+  }
+}
+
+// The same sweep with each thread walking a column of up to KC cells along
+// k (the index space gives the first cell of each column): the k face shared
+// by two consecutive cells is evaluated once and the upper cell's iterate is
+// loaded once and carried, which cuts the loads of a sweep by about a third.
+// Per cell the arithmetic and its order are those of k_jacobi.
+template <class T, bool EU, bool FIRST, int KC>
+__global__ void __launch_bounds__(kTile, 3) k_jacobi_col(
+    const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
+    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
+    const T* __restrict__ coefdiag, const T* __restrict__ d_in,
+    const T* __restrict__ df_in, T* __restrict__ d_out, T* __restrict__ df_out) {
+  int b, i, j, kc;
+  if (!space_elem(sp, threadIdx.x, b, i, j, kc)) return;
+  const Blk& B = blks[b];
+  const int k0 = 1 + (kc - 1) * KC;
+  const int k1 = min(k0 + KC - 1, B.nk - 1);
+  const long long K = B.nijd;
+  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
+  const T *sk0 = sn_ptr(sn, B, 2, 0), *sk1 = sn_ptr(sn, B, 2, 1), *sk2 = sn_ptr(sn, B, 2, 2);
+  const T* cek = coefe + 2 * ld;
+  long long n = cell_index(B, i, j, k0);
+  // lower k face of the first cell
+  T tnk[5];
+  jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - K, sk0[n], sk1[n], sk2[n], tnk);
+  T cek_lo = cek[n];
+  T dlo[5];  // iterate of the cell below
+#pragma unroll
+  for (int a = 0; a < 5; ++a) dlo[a] = FIRST ? T(0.) : d_in[a * ld + n - K];
+  for (int k = k0; k <= k1; ++k, n += K) {
+    T d2w[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
+    // i and j directions as in k_jacobi
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const long long inc = ninc_of(B, dir);
+      const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
+              *s2 = sn_ptr(sn, B, dir, 2);
+      const T* ce = coefe + (long long)dir * ld;
+      T tn[5];
+      jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - inc, s0[n], s1[n], s2[n], tn);
+      const T cel = ce[n], ceu = ce[n + inc];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        const T dl = FIRST ? T(0.) : d_in[a * ld + n - inc];
+        const T du = FIRST ? T(0.) : d_in[a * ld + n + inc];
+        d2w[a] = d2w[a] + tn[a] + cel * dl + ceu * du;
+      }
+      const long long nu = n + inc;
+      jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, s0[nu], s1[nu], s2[nu], tn);
+#pragma unroll
+      for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
+    }
+    // k direction: lower face carried, upper face evaluated once
+    const long long nu = n + K;
+    const T ceu = cek[nu];
+    T dup[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      dup[a] = FIRST ? T(0.) : d_in[a * ld + nu];
+      d2w[a] = d2w[a] + tnk[a] + cek_lo * dlo[a] + ceu * dup[a];
+    }
+    T tnu[5];
+    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, sk0[nu], sk1[nu], sk2[nu], tnu);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tnu[a];
+    // this cell's new iterate
+    const T cd = coefdiag[n];
+    T dn[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      dn[a] = d2w[a] / cd;
+      d_out[a * ld + n] = dn[a];
+    }
+    T f[9];
+    jacobi_df<T, EU>(dn, v[n], v[ld + n], v[2 * ld + n], v[3 * ld + n], v[4 * ld + n], ps[n],
+                     EU ? T(0.) : prim[n], EU ? T(0.) : prim[ld + n],
+                     EU ? T(0.) : prim[2 * ld + n], gam1, pinfl, qfix, f);
+#pragma unroll
+    for (int a = 0; a < 9; ++a) df_out[a * ld + n] = f[a];
+    // move up: the upper face becomes the next cell's lower face
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      tnk[a] = tnu[a];
+      dlo[a] = FIRST ? T(0.) : d_in[a * ld + n];
+    }
+    cek_lo = ceu;
+  }
+}
+
+// Reduced-precision sweep that stores no flux increments: each neighbour's
+// increment f(v+d) - f(v) is recomputed from its state and iterate (ghost
+// neighbours contribute zero, as their stored increments do in the reference
+// sweep).  A sweep then moves the iterate and the per-iteration constants
+// only.  Used by the mixed forms, where the sweeps only precondition the
+// pseudo-time step.
+//
+// The increment is evaluated in difference form: with q the velocity, rho'
+// = rho + d_rho, dq = (d_m - q d_rho) / rho' and dp = p' - p,
+//   rho' u'u' - rho u u = d_rho u u + rho' (2 u du + du du) (+ dp on the
+//   diagonal), u' (E' + p' - pinfl) - u (E + p - pinfl) = du H' + u (dE + dp),
+// the same quantities as implimf_3d.f90:430-463 / implimf_eu.f90:301-312 in
+// exact arithmetic, but exactly zero for d = 0.  The reference form cancels
+// O(1) fluxes, and in FP32 that leaves a rounding residue of ~1e-7 at d = 0
+// which would hold the iteration off the FP64 steady state.
+template <class T>
+__device__ __forceinline__ T rcpT(T a) {
+  return T(1.) / a;
+}
+template <>
+__device__ __forceinline__ float rcpT<float>(float a) {
+  return __fdividef(1.f, a);
+}
+
+template <class T, bool EU>
+__device__ __forceinline__ void df_of(const T* __restrict__ v, const T* __restrict__ prim,
+                                      const T* __restrict__ ps, const T* __restrict__ d,
+                                      long long ld, long long n, T gam1, T pinfl, int qfix,
+                                      T dd[5], T f[9]) {
+#pragma unroll
+  for (int a = 0; a < 5; ++a) dd[a] = d[a * ld + n];
+  const T E = v[4 * ld + n], p = ps[n];
+  const T qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
+  const T r1 = v[n] + dd[0];
+  const T ir1 = rcpT(r1);
+  const T du = (dd[1] - qu * dd[0]) * ir1;
+  const T dv = (dd[2] - qv * dd[0]) * ir1;
+  const T dw = (dd[3] - qw * dd[0]) * ir1;
+  const T dk = dd[0] * (qu * qu + qv * qv + qw * qw) +
+               r1 * (T(2.) * (qu * du + qv * dv + qw * dw) + du * du + dv * dv + dw * dw);
+  const T dp = gam1 * (dd[4] - T(0.5) * dk);
+  const T h0 = E + p - pinfl;
+  const T h1 = h0 + dd[4] + dp;
+  const T de = dd[4] + dp;
+  f[0] = dd[0] * qu * qu + r1 * (T(2.) * qu * du + du * du) + dp;
+  f[1] = dd[0] * qu * qv + r1 * (qu * dv + qv * du + du * dv);
+  f[2] = dd[0] * qu * qw + r1 * (qu * dw + qw * du + du * dw);
+  f[3] = du * h1 + qu * de;
+  f[4] = dd[0] * qv * qv + r1 * (T(2.) * qv * dv + dv * dv) + dp;
+  f[5] = dd[0] * qv * qw + r1 * (qv * dw + qw * dv + dv * dw);
+  f[6] = dv * h1 + qv * de;
+  f[7] = dd[0] * qw * qw + r1 * (T(2.) * qw * dw + dw * dw) + dp;
+  // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
+  // Euler form keeps it unless qfix (a flagged non-reference option) is set
+  f[8] = (EU && !qfix) ? h1 * ir1 - h0 * qw : dw * h1 + qw * de;
+}
+
+template <class T, bool EU>
+__device__ __forceinline__ void face_tn(const T du[5], const T dl[5], const T fu[9],
+                                        const T fl[9], T sx, T sy, T sz, T tn[5]) {
+  const T h = T(0.5);
+  const T a2 = du[1] + dl[1], a3 = du[2] + dl[2], a4 = du[3] + dl[3];
+  T s[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) s[q] = fu[q] + fl[q];
+  if (EU) {
+    tn[0] = h * (a2 * sx + a3 * sy + a4 * sz);
+    tn[1] = h * (s[0] * sx + s[1] * sy + s[2] * sz);
+    tn[2] = h * (s[1] * sx + s[4] * sy + s[5] * sz);
+    tn[3] = h * (s[2] * sx + s[5] * sy + s[7] * sz);
+    tn[4] = h * (s[3] * sx + s[6] * sy + s[8] * sz);
+  } else {
+    tn[0] = h * a2 * sx + h * a3 * sy + h * a4 * sz;
+    tn[1] = h * s[0] * sx + h * s[1] * sy + h * s[2] * sz;
+    tn[2] = h * s[1] * sx + h * s[4] * sy + h * s[5] * sz;
+    tn[3] = h * s[2] * sx + h * s[5] * sy + h * s[7] * sz;
+    tn[4] = h * s[3] * sx + h * s[6] * sy + h * s[8] * sz;
+  }
+}
+
+template <class T, bool EU, bool FIRST>
+__global__ void __launch_bounds__(kTile) k_jacobi_rc(
+    const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
+    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
+    const T* __restrict__ coefdiag, const T* __restrict__ d_in, T* __restrict__ d_out) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
+  T d0[5], f0[9];
+  if (FIRST) {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d0[a] = T(0.);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f0[q] = T(0.);
+  } else {
+    df_of<T, EU>(v, prim, ps, d_in, ld, n, gam1, pinfl, qfix, d0, f0);
+  }
+  T d2w[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long inc = ninc_of(B, dir);
+    const int nd = nd_of(B, dir);
+    const int p = dir == 0 ? i : (dir == 1 ? j : k);
+    const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
+            *s2 = sn_ptr(sn, B, dir, 2);
+    const T* ce = coefe + (long long)dir * ld;
+    T dl[5], fl[9], du[5], fu[9];
+    if (FIRST || p == 1) {
+#pragma unroll
+      for (int a = 0; a < 5; ++a) dl[a] = T(0.);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) fl[q] = T(0.);
+    } else {
+      df_of<T, EU>(v, prim, ps, d_in, ld, n - inc, gam1, pinfl, qfix, dl, fl);
+    }
+    if (FIRST || p == nd - 1) {
+#pragma unroll
+      for (int a = 0; a < 5; ++a) du[a] = T(0.);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) fu[q] = T(0.);
+    } else {
+      df_of<T, EU>(v, prim, ps, d_in, ld, n + inc, gam1, pinfl, qfix, du, fu);
+    }
+    T tn[5];
+    face_tn<T, EU>(d0, dl, f0, fl, s0[n], s1[n], s2[n], tn);
+    const T cel = ce[n], ceu = ce[n + inc];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] + tn[a] + cel * dl[a] + ceu * du[a];
+    const long long nu = n + inc;
+    face_tn<T, EU>(du, d0, fu, f0, s0[nu], s1[nu], s2[nu], tn);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
+  }
+  const T cd = coefdiag[n];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
+}
+
+// per-tile partial residual norms of (v_new - v_old)/dt (residu.f90:127-182)
+__device__ __forceinline__ void norm_tile_reduce(const double res[5], bool valid,
+                                                 double* out15) {
+  __shared__ double sh[kTile / 32][15];
+  double a1[5], a2[5], am[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    a1[a] = valid ? fabs(res[a]) : 0.;
+    a2[a] = valid ? res[a] * res[a] : 0.;
+    am[a] = a1[a];
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      a1[a] = a1[a] + __shfl_down_sync(0xffffffffu, a1[a], off);
+      a2[a] = a2[a] + __shfl_down_sync(0xffffffffu, a2[a], off);
+      am[a] = fmax(am[a], __shfl_down_sync(0xffffffffu, am[a], off));
+    }
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      sh[w][a] = a1[a];
+      sh[w][5 + a] = a2[a];
+      sh[w][10 + a] = am[a];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 15) {
+    const int q = threadIdx.x;
+    double s = sh[0][q];
+    for (int ww = 1; ww < kTile / 32; ++ww) s = (q >= 10) ? fmax(s, sh[ww][q]) : s + sh[ww][q];
+    out15[q] = s;
+  }
+}
+
+// v += d on the real cells (FP64 state update of implimf_*.f90), the residual
+// norm partials and, when requested, the final increment copied to d_out
+template <class T>
+__global__ void __launch_bounds__(kTile) k_update(const Blk* __restrict__ blks,
+                                                  Space sp, long long ld,
+                                                  const T* __restrict__ d,
+                                                  double* __restrict__ v,
+                                                  const double* __restrict__ dt,
+                                                  double* d_out, double* normpart) {
+  int b, i, j, k;
+  const bool valid = space_elem(sp, threadIdx.x, b, i, j, k);
+  double res[5] = {0., 0., 0., 0., 0.};
+  if (valid) {
+    const long long n = cell_index(blks[b], i, j, k);
+    const double t = dt[n];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      const double vo = v[a * ld + n], dd = (double)d[a * ld + n];
+      const double vn = vo + dd;
+      v[a * ld + n] = vn;
+      if (d_out) d_out[a * ld + n] = dd;
+      res[a] = (vn - vo) / t;
+    }
+  }
+  if (normpart) norm_tile_reduce(res, valid, normpart + (long long)(sp.tile0 + blockIdx.x) * 15);
+}
+
+}  // namespace
+}  // namespace cns

@@ -12,6 +12,7 @@ __device__ __forceinline__ double* sn_wptr(double* sn, const Blk& B, int dir,
 }
 
 constexpr int kTile = 128;  // elements per tile (= threads per CTA)
+constexpr int kJacCol = 4;  // cells per thread of a Jacobi sweep (a k column)
 
 struct HostLayout {
   std::vector<Blk> blks;
@@ -54,7 +55,16 @@ struct Work {
   double* dfpp[2] = {nullptr, nullptr};  // flux increments, [9][ld] each
   double* normpart = nullptr; // per tile partial norms [ntiles][15]
   double* norms = nullptr;    // [16]
+  double* blocksum = nullptr; // per block norm sums [nblk][15]
   int* status = nullptr;      // device status word
+  // mixed precision (allocated on first use)
+  bool mixed_ready = false;
+  float *v32 = nullptr, *prim32 = nullptr, *ps32 = nullptr, *tau32 = nullptr;
+  float *sn32 = nullptr, *G32 = nullptr, *R32 = nullptr, *u32 = nullptr;
+  float *coefe32 = nullptr, *coefdiag32 = nullptr;
+  float* d32pp[2] = {nullptr, nullptr};
+  float* df32pp[2] = {nullptr, nullptr};
+  double *corr = nullptr, *ur32 = nullptr;
 };
 
 cudaError_t launch_metric(const HostLayout& lay, const Blk* dblks, const Bnd& bd,
@@ -92,18 +102,95 @@ cudaError_t launch_grad(const Blk* blks, Space sp, Phys ph, const double* v,
                         const double* mut, double* tau, const double* sn,
                         const double* vol, const double* temp, cudaStream_t st);
 
-cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
-                         const double* v, const double* prim, long long ld,
-                         const double* ps, double* R, cudaStream_t st);
+// hot kernels templated on the real type T (double: cns_flow.cu, bit-exact;
+// float: cns_mixed.cu, the reduced-precision half of the mixed form)
+template <class T>
+cudaError_t launch_ratio_t(const Blk* blks, const SpaceBuf* lines, int l0, const T* v,
+                           const T* prim, long long ld, const T* ps, T* R,
+                           cudaStream_t st);
+template <class T>
+cudaError_t launch_face_flux_t(const Blk* blks, const SpaceBuf* faces, int l0, Phys ph,
+                               Scheme sc, const T* v, const T* prim, long long ld,
+                               const T* ps, const T* tau, const T* sn, const T* R, T* G,
+                               cudaStream_t st);
+// u = FP64 sum of the face fluxes (+ corr); u32 an optional float copy
+template <class T>
+cudaError_t launch_accumulate_t(const Blk* blks, Space sp, const T* G, long long ld,
+                                const double* corr, double* u, float* u32,
+                                cudaStream_t st);
+// lmx Jacobi sweeps over the real cells; the final iterate is in dpp[*cur_out]
+template <class T>
+cudaError_t launch_sweeps_t(const Blk* blks, Space cells, Phys ph, Scheme sc, int eu,
+                            int lmx, long long ld, const T* u, const T* v, const T* prim,
+                            const T* ps, const T* sn, const T* coefe, const T* coefdiag,
+                            T* const dpp[2], T* const dfpp[2], int* cur_out,
+                            cudaStream_t st);
+template <class T>
+cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T* d,
+                            double* v, const double* dt, double* d_out, double* normpart,
+                            cudaStream_t st);
 
-cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
-                             Phys ph, Scheme sc, const double* v,
-                             const double* prim, long long ld, const double* ps,
-                             const double* tau, const double* sn, const double* R,
-                             double* G, cudaStream_t st);
+// the two precisions are defined in cns_flow.cu (double) and cns_mixed.cu (float)
+#define CNS_DECLARE_HOT(T)                                                                  \
+  template <>                                                                               \
+  cudaError_t launch_ratio_t<T>(const Blk*, const SpaceBuf*, int, const T*, const T*,      \
+                                long long, const T*, T*, cudaStream_t);                     \
+  template <>                                                                               \
+  cudaError_t launch_face_flux_t<T>(const Blk*, const SpaceBuf*, int, Phys, Scheme,        \
+                                    const T*, const T*, long long, const T*, const T*,     \
+                                    const T*, const T*, T*, cudaStream_t);                  \
+  template <>                                                                               \
+  cudaError_t launch_accumulate_t<T>(const Blk*, Space, const T*, long long,               \
+                                     const double*, double*, float*, cudaStream_t);        \
+  template <>                                                                               \
+  cudaError_t launch_sweeps_t<T>(const Blk*, Space, Phys, Scheme, int, int, long long,     \
+                                 const T*, const T*, const T*, const T*, const T*,          \
+                                 const T*, const T*, T* const[2], T* const[2], int*,        \
+                                 cudaStream_t);                                             \
+  template <>                                                                               \
+  cudaError_t launch_update_t<T>(const Blk*, Space, long long, const T*, double*,          \
+                                 const double*, double*, double*, cudaStream_t);
+CNS_DECLARE_HOT(double)
+CNS_DECLARE_HOT(float)
+#undef CNS_DECLARE_HOT
 
-cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
-                              long long ld, double* u, cudaStream_t st);
+inline cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
+                                const double* v, const double* prim, long long ld,
+                                const double* ps, double* R, cudaStream_t st) {
+  return launch_ratio_t<double>(blks, lines, l0, v, prim, ld, ps, R, st);
+}
+inline cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
+                                    Phys ph, Scheme sc, const double* v,
+                                    const double* prim, long long ld, const double* ps,
+                                    const double* tau, const double* sn, const double* R,
+                                    double* G, cudaStream_t st) {
+  return launch_face_flux_t<double>(blks, faces, l0, ph, sc, v, prim, ld, ps, tau, sn, R, G,
+                                    st);
+}
+inline cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
+                                     long long ld, double* u, cudaStream_t st) {
+  return launch_accumulate_t<double>(blks, sp, G, ld, nullptr, u, nullptr, st);
+}
+
+// FP64 implicit coefficients with float copies for the mixed sweeps
+cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
+                                         const SpaceBuf* faces, int l0, Phys ph, int eu,
+                                         const double* dt, const double* v,
+                                         const double* prim, const double* mu,
+                                         const double* mut, const double* sn,
+                                         const double* vol, const double* cson, Work& w,
+                                         float* coefe32, float* coefdiag32,
+                                         cudaStream_t st);
+
+// primitive velocities over the flat range [0, ncells) together with the
+// single-precision copies of v, prim and ps the reduced-precision sweeps read
+cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
+                               const double* ps, float* v32, float* prim32, float* ps32,
+                               cudaStream_t st);
+cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t st);
+// corr = u64 - u_r32 on the real cells (defect correction)
+cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const double* u64,
+                          const double* ur32, double* corr, cudaStream_t st);
 
 // the implicit phase of implimf_eu (eu = 1) or implimf_3d (eu = 0) on the
 // cells of the space: coefficients, lmx Jacobi sweeps, v += d; d_out
@@ -124,6 +211,6 @@ cudaError_t launch_norm_partials(const Blk* blks, Space cells, long long ld,
 
 cudaError_t launch_norm_finalize(const Blk* blks, const int* blk_tile0_dev,
                                  int b0, int b1, const double* normpart,
-                                 double* norms, cudaStream_t st);
+                                 double* blocksum, double* norms, cudaStream_t st);
 
 }  // namespace cns

@@ -1,0 +1,153 @@
+// cns_mixed.cu -- the single-precision instantiations of the hot kernels and
+// the helpers of the mixed-precision iteration.
+//
+// Mixed form (precision 1): the explicit residual, the time steps, the
+// boundary conditions, the state update v += d and the norms stay FP64; the
+// point-Jacobi sweeps of the implicit phase run in FP32 on single-precision
+// copies of the state, velocities, pressure and face areas.  The sweeps only
+// shape the pseudo-time increment, so the fixed point is the FP64 steady
+// state: R64(W) = 0.
+//
+// Defect-correction form (precision 2): the face fluxes also run in FP32;
+// every kdefect iterations the FP64 residual R64(W) and the FP32 residual
+// R32(W) of the same state give corr = R64 - R32, and the iterations in
+// between use R32 + corr.  Its residual stalls at the FP32 rounding level of
+// the fluxes (no longer exact between refreshes), so it is a transient
+// accelerator, not a steady-state solver.
+//
+// Built with FMA contraction (the FP32 path is not a parity path).
+#include "cns_kernels.cuh"
+#include "cns_hot.cuh"
+
+namespace cns {
+
+namespace {
+
+inline int grid_of(const Space& s) { return s.ntiles; }
+
+__global__ void __launch_bounds__(256) k_to_float(const double* __restrict__ a,
+                                                 float* __restrict__ b, long long n) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) b[q] = (float)a[q];
+}
+
+__global__ void __launch_bounds__(kTile) k_defect(const Blk* __restrict__ blks, Space sp,
+                                                  long long ld,
+                                                  const double* __restrict__ u64,
+                                                  const double* __restrict__ ur32,
+                                                  double* __restrict__ corr) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) corr[a * ld + n] = u64[a * ld + n] - ur32[a * ld + n];
+}
+
+}  // namespace
+
+cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t st) {
+  if (n > 0) k_to_float<<<(int)((n + 255) / 256), 256, 0, st>>>(a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const double* u64,
+                          const double* ur32, double* corr, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_defect<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, u64, ur32, corr);
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_ratio_t<float>(const Blk* blks, const SpaceBuf* lines, int l0,
+                                  const float* v, const float* prim, long long ld,
+                                  const float* ps, float* R, cudaStream_t st) {
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = lines[dir].view(l0);
+    if (sp.ntiles > 0)
+      k_ratio<float><<<dim3(grid_of(sp), 5), kTile, 0, st>>>(blks, sp, dir, v, prim, ld, ps, R);
+  }
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_face_flux_t<float>(const Blk* blks, const SpaceBuf* faces, int l0,
+                                      Phys ph, Scheme sc, const float* v, const float* prim,
+                                      long long ld, const float* ps, const float* tau,
+                                      const float* sn, const float* R, float* G,
+                                      cudaStream_t st) {
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = faces[dir].view(l0);
+    if (sp.ntiles == 0) continue;
+    if (sc.ns)
+      k_face_flux<float, true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                              ld, ps, tau, sn, R, G);
+    else
+      k_face_flux<float, false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                               ld, ps, tau, sn, R, G);
+  }
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_accumulate_t<float>(const Blk* blks, Space sp, const float* G,
+                                       long long ld, const double* corr, double* u,
+                                       float* u32, cudaStream_t st) {
+  if (sp.ntiles > 0)
+    k_accumulate<float><<<grid_of(sp), kTile, 0, st>>>(blks, sp, G, ld, corr, u, u32);
+  return cudaGetLastError();
+}
+
+// the FP32 sweeps of the mixed form: the flux increments are recomputed,
+// not stored (dfpp unused), so a sweep moves d and the constants only
+template <>
+cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Phys ph, Scheme sc, int eu,
+                                   int lmx, long long ld, const float* u, const float* v,
+                                   const float* prim, const float* ps, const float* sn,
+                                   const float* coefe, const float* coefdiag,
+                                   float* const dpp[2], float* const dfpp[2], int* cur_out,
+                                   cudaStream_t st) {
+  (void)dfpp;
+  const int g = grid_of(cells);
+  int cur = 0;
+  if (lmx == 0) {
+    cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(float) * 5 * ld, st);
+    if (e0 != cudaSuccess) return e0;
+  }
+  const int q = eu ? sc.qfix_dfez : 0;
+  for (int ls = 1; ls <= lmx; ++ls) {
+    const int nxt = (ls == 1) ? 0 : 1 - cur;
+    const float* din = dpp[cur];
+    float* dout = dpp[nxt];
+    if (eu) {
+      if (ls == 1)
+        k_jacobi_rc<float, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                            ps, sn, coefe, coefdiag, din, dout);
+      else
+        k_jacobi_rc<float, true, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                             ps, sn, coefe, coefdiag, din, dout);
+    } else {
+      if (ls == 1)
+        k_jacobi_rc<float, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
+                                                             ps, sn, coefe, coefdiag, din, dout);
+      else
+        k_jacobi_rc<float, false, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                              prim, ps, sn, coefe, coefdiag, din,
+                                                              dout);
+    }
+    cur = nxt;
+  }
+  *cur_out = cur;
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_update_t<float>(const Blk* blks, Space cells, long long ld, const float* d,
+                                   double* v, const double* dt, double* d_out,
+                                   double* normpart, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_update<float><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, d, v, dt, d_out,
+                                                      normpart);
+  return cudaGetLastError();
+}
+
+}  // namespace cns

@@ -114,7 +114,8 @@ class CodeNS:
     def _scheme_t(s, qfix_dfez: int = 0):
         return abi.Scheme_t(int(s.ns), int(s.muscl), float(s.xk), int(s.ilim), float(s.eta),
                             int(s.kdtl), float(s.dt1min), int(s.lmax),
-                            int(getattr(s, "qfix_dfez", qfix_dfez)))
+                            int(getattr(s, "qfix_dfez", qfix_dfez)),
+                            int(getattr(s, "precision", 0)), int(getattr(s, "kdefect", 4)))
 
     def _check(self, rc: int, where: str):
         if rc:
@@ -143,6 +144,11 @@ class CodeNS:
     @property
     def scratch_bytes(self) -> int:
         return int(self.lib.cns_scratch_bytes(self.ctx))
+
+    @property
+    def kernels_launched(self) -> int:
+        """kernels launched so far by the fused-step graphs of this solver"""
+        return int(self.lib.cns_kernels_launched(self.ctx))
 
     # ---- set-up -------------------------------------------------------
     def metric(self):

@@ -84,6 +84,14 @@ typedef struct {
   int32_t lmax;          /* Jacobi sub-iterations */
   int32_t qfix_dfez;     /* non-reference option: restore the missing *wi of
                             implimf_eu.f90:312 (0 = reference behaviour) */
+  int32_t precision;     /* fused step: 0 = FP64 (bit-exact); 1 = mixed: FP64
+                            residual, boundary conditions, update and norms,
+                            FP32 Jacobi sweeps (same steady state as FP64);
+                            2 = defect correction: FP32 face fluxes too, the
+                            FP64 residual every kdefect iterations (stalls at
+                            the FP32 rounding level of the fluxes) */
+  int32_t kdefect;       /* precision 2: the FP64 residual and the correction
+                            R64 - R32 are refreshed every kdefect iterations */
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
@@ -120,6 +128,10 @@ int cns_set_stream(cns_ctx *ctx, void *cuda_stream);
 int cns_set_scheme(cns_ctx *ctx, const cns_scheme_t *scheme);
 const char *cns_last_error(cns_ctx *ctx);
 int64_t cns_scratch_bytes(cns_ctx *ctx);
+
+/* kernels launched by the fused-step graphs of this context so far (the
+ * kernel nodes of each captured iteration times its launches) */
+int64_t cns_kernels_launched(cns_ctx *ctx);
 
 /* ---- set-up ------------------------------------------------------------ */
 /* metric.f90 -> metrics.f90: ghost nodes (extmhg), sn (norm), vol (svol),

@@ -1,0 +1,114 @@
+"""Reduced-precision forms of the fused iteration.
+
+precision 1 (mixed): FP64 residual, boundary conditions, update and norms,
+FP32 point-Jacobi sweeps.  Its fixed point is the FP64 steady state, so the
+converged state must agree with the FP64 one to far below FP32 rounding.
+
+precision 2 (defect correction): FP32 face fluxes, the FP64 residual every
+kdefect iterations.  Its refresh iteration must use the exact FP64 residual.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+
+from ._helpers import SMALL, assert_equal_bits, max_rel_cols, real
+
+pytestmark = pytest.mark.gpu
+
+# state agreement of the converged mixed and FP64 iterations (component-
+# relative); FP32 sweeps alone would leave ~1e-7
+STEADY_TOL = 1e-8
+
+
+def _solver(case, precision, kdefect=4):
+    from codens_b200.solver import CodeNS
+    case.scheme.precision = precision
+    case.scheme.kdefect = kdefect
+    s = CodeNS(case)
+    s.metric()
+    return s
+
+
+def _state(s, case):
+    return s.v.cpu().numpy().reshape(5, case.layout.ld)[:, real(case)]
+
+
+def _residual(s, case):
+    return s.u.cpu().numpy().reshape(5, case.layout.ld)[:, real(case)]
+
+
+def _box_viscous():
+    return cases.box_case((8, 6, 5), seed=12, ns=True, ilim=0, reynz=100.0, skew=0.02)
+
+
+@pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu_qfix"])
+def test_mixed_uses_fp64_residual(cuda, name):
+    """the first mixed iteration evaluates the same FP64 residual as the FP64
+    iteration (bit for bit) and moves the state by an FP32-accurate step"""
+    case = SMALL[name]()
+    a = _solver(case, 0)
+    b = _solver(SMALL[name](), 1)
+    v0 = _state(a, case)
+    a.atsch_num(1)
+    b.atsch_num(1)
+    assert_equal_bits(_residual(b, case), _residual(a, case), "residual of the first step")
+    dv64 = _state(a, case) - v0
+    dv32 = _state(b, case) - v0
+    scale = np.maximum(np.abs(dv64).max(axis=1, keepdims=True), 1e-300)
+    assert float((np.abs(dv32 - dv64) / scale).max()) < 1e-4
+    a.close()
+    b.close()
+
+
+def test_defect_refresh_uses_fp64_residual(cuda):
+    case = SMALL["box_ns"]()
+    a = _solver(case, 0)
+    b = _solver(SMALL["box_ns"](), 2, kdefect=3)
+    a.atsch_num(1)
+    b.atsch_num(1)
+    assert_equal_bits(_residual(b, case), _residual(a, case), "refresh residual")
+    # the regular iterations run on R32 + corr: finite and close to FP64
+    b.atsch_num(2)
+    assert np.isfinite(_state(b, case)).all()
+    a.close()
+    b.close()
+
+
+def test_mixed_reaches_fp64_steady_state(cuda):
+    """2400 iterations on a viscous box: both forms converge (L2 of the
+    density increment below 1e-12), and the mixed converged state is a fixed
+    point of the FP64 iteration (one FP64 iteration from it moves the state by
+    FP64 rounding only).  The box's extrapolated i faces leave a family of
+    steady states, so the two states themselves may differ by the path."""
+    case = _box_viscous()
+    a = _solver(case, 0)
+    b = _solver(_box_viscous(), 1)
+    na = a.atsch_num(2400)
+    nb = b.atsch_num(2400)
+    assert na[1, 0] < 1e-12 and nb[1, 0] < 1e-12, (na[1, 0], nb[1, 0])
+    case_b = _box_viscous()
+    case_b.scheme.precision = 0
+    b.set_scheme(case_b.scheme)
+    n1 = b.atsch_num(1)
+    assert n1[1, 0] < 1e-14, n1[1, 0]
+    a.close()
+    b.close()
+
+
+def test_mixed_rejects_bad_precision(cuda):
+    from codens_b200 import abi
+    case = SMALL["box_ns"]()
+    s = _solver(case, 0)
+    case.scheme.precision = 3
+    with pytest.raises(abi.CnsError) as ei:
+        s.set_scheme(case.scheme)
+    assert ei.value.code == abi.CNS_EINVAL
+    case.scheme.precision = 2
+    case.scheme.kdefect = 0
+    with pytest.raises(abi.CnsError) as ei:
+        s.set_scheme(case.scheme)
+    assert ei.value.code == abi.CNS_EINVAL
+    s.close()
