@@ -58,7 +58,7 @@ EXPORTS = [
     "cns_sch_roe", "cns_zvisqc", "cns_implimf_eu", "cns_implimf_3d",
     "cns_rscpsv", "cns_bind_state", "cns_atsch_num_step",
     "cns_atsch_num_launch", "cns_last_norms", "cns_atsch_num_step_host",
-    "cns_sch_roe_euler_noalloc",
+    "cns_sch_roe_euler_noalloc", "cns_sweep_tiles", "cns_set_sweep_tiles",
 ]
 
 _lib = None
@@ -102,6 +102,8 @@ def load(build_if_missing: bool = True):
     L.cns_atsch_num_step.argtypes = [vp, C.c_int, P(c_f64)]
     L.cns_atsch_num_launch.argtypes = [vp, C.c_int]
     L.cns_last_norms.argtypes = [vp, P(c_f64)]
+    L.cns_sweep_tiles.argtypes = [vp, C.c_int, P(c_i32)]
+    L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,
                                             c_f64, vp, vp, vp, vp, vp]

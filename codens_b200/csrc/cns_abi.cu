@@ -21,7 +21,10 @@ struct cns_ctx {
   Blk* d_blks = nullptr;
   Phys ph{};
   Scheme sc{};
-  SpaceBuf cells, cols, faces[3], lines[3];
+  SpaceBuf cells, faces[3], lines[3];
+  TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
+  bool tuned64 = false, tuned32 = false;
+  float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
   int* d_cells_tile0 = nullptr;  // cells.blk_tile0 on the device
   // boundaries
   Bnd bd{};
@@ -80,6 +83,17 @@ cudaError_t dev_alloc(cns_ctx* c, T** p, size_t n, bool zero = true) {
 }
 
 template <typename T>
+void dev_free(cns_ctx* c, T* p) {
+  if (!p) return;
+  for (size_t q = 0; q < c->allocs.size(); ++q)
+    if (c->allocs[q] == (void*)p) {
+      c->allocs.erase(c->allocs.begin() + q);
+      break;
+    }
+  cudaFree(p);
+}
+
+template <typename T>
 cudaError_t upload(cns_ctx* c, T** p, const T* h, size_t n) {
   cudaError_t e = dev_alloc(c, p, n, false);
   if (e != cudaSuccess) return e;
@@ -112,6 +126,28 @@ cudaError_t build_space(cns_ctx* c, SpaceBuf& s, F ext_of) {
   if (e == cudaSuccess) e = upload(c, &s.d_tile_start, ts.data(), ts.size());
   if (e == cudaSuccess) e = upload(c, &s.d_ext, ext.data(), ext.size());
   return e;
+}
+
+// the 2.5D sweep tiles: patches of ti x tj columns, kc planes deep, block by
+// block
+cudaError_t build_tiles(cns_ctx* c, TileBuf& t, int ti, int tj, int kc) {
+  dev_free(c, t.d_tile);
+  t.d_tile = nullptr;
+  std::vector<int4> tl;
+  t.blk_tile0.assign(c->lay.blks.size() + 1, 0);
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    const Blk& B = c->lay.blks[b];
+    t.blk_tile0[b] = (int)tl.size();
+    for (int k0 = 1; k0 <= B.nk - 1; k0 += kc)
+      for (int j0 = 1; j0 <= B.nj - 1; j0 += tj)
+        for (int i0 = 1; i0 <= B.ni - 1; i0 += ti) tl.push_back(make_int4((int)b, i0, j0, k0));
+  }
+  t.blk_tile0.back() = (int)tl.size();
+  t.ntiles = (int)tl.size();
+  t.ti = ti;
+  t.tj = tj;
+  t.kc = kc;
+  return upload(c, &t.d_tile, tl.data(), tl.size());
 }
 
 bool bad_block(cns_ctx* c, int l) { return l < 0 || l > (int)c->lay.blks.size(); }
@@ -204,7 +240,8 @@ cudaError_t enqueue_step(cns_ctx* c) {
   }
   if (e == cudaSuccess) e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
   if (e == cudaSuccess)
-    e = launch_implicit(c->d_blks, all, c->faces, -1, c->ph, c->sc, !c->sc.ns,
+    e = launch_implicit(c->d_blks, all, c->tiles64.view(-1), c->faces, -1, c->ph, c->sc,
+                        !c->sc.ns,
                         c->sc.lmax, s.u, s.dt, s.v, nullptr, s.mu, s.mut, s.sn, s.vol,
                         s.pression, s.cson, c->w, 1, c->st);
   if (e == cudaSuccess)
@@ -230,7 +267,6 @@ cudaError_t ensure_mixed(cns_ctx* c) {
   if (e == cudaSuccess) e = dev_alloc(c, &w.coefdiag32, (size_t)ld);
   for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
     e = dev_alloc(c, &w.d32pp[q], (size_t)(5 * ld));
-    if (e == cudaSuccess) e = dev_alloc(c, &w.df32pp[q], (size_t)(9 * ld));
   }
   if (e == cudaSuccess) e = dev_alloc(c, &w.corr, (size_t)(5 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &w.ur32, (size_t)(5 * ld));
@@ -301,15 +337,80 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode) {
                                      w.coefe32, w.coefdiag32, c->st);
   int cur = 0;
   if (e == cudaSuccess)
-    e = launch_sweeps_t<float>(c->d_blks, all, c->ph, c->sc, !c->sc.ns, c->sc.lmax, ld, w.u32,
+    e = launch_sweeps_t<float>(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
+                               c->sc.lmax, ld, w.u32,
                                w.v32, w.prim32, w.ps32, w.sn32, w.coefe32, w.coefdiag32,
-                               w.d32pp, w.df32pp, &cur, c->st);
+                               w.d32pp, &cur, c->st);
   if (e == cudaSuccess)
     e = launch_update_t<float>(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, nullptr,
                                w.normpart, c->st);
   if (e == cudaSuccess)
     e = launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
                              w.normpart, w.blocksum, w.norms, c->st);
+  return e;
+}
+
+// The sweep autotuner: times one 2.5D sweep of every patch shape and plane
+// count on the current iteration's data (u, coefficients and iterate of the
+// step that just ran; the sweep only writes the scratch iterate) and keeps
+// the fastest tile list.  FP64 results do not depend on the tiling.
+constexpr int kTuneKc[] = {2, 4, 8, 16, 32};
+
+template <class T>
+cudaError_t time_sweep(cns_ctx* c, Tiles tl, const T* u, const T* v, const T* prim,
+                       const T* ps, const T* sn, const T* coefe, const T* coefdiag,
+                       const T* din, T* dout, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  const int q = c->sc.ns ? 0 : c->sc.qfix_dfez;
+  const long long ld = c->lay.ld;
+  cudaError_t e = launch_jacobi_25d_t<T>(c->d_blks, tl, c->ph, q, !c->sc.ns, ld, u, v, prim, ps,
+                                         sn, coefe, coefdiag, din, dout, c->st);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, c->st);
+  for (int r = 0; r < 3 && e == cudaSuccess; ++r)
+    e = launch_jacobi_25d_t<T>(c->d_blks, tl, c->ph, q, !c->sc.ns, ld, u, v, prim, ps, sn,
+                               coefe, coefdiag, din, dout, c->st);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, c->st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+  return e;
+}
+
+cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
+  const cns_state_t& s = c->state;
+  Work& w = c->w;
+  TileBuf& best = fp32 ? c->tiles32 : c->tiles64;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  int bti = best.ti, btj = best.tj, bkc = best.kc;
+  TileBuf cand;
+  for (int sh = 0; sh < kSweepShapes && e == cudaSuccess; ++sh)
+    for (int kc : kTuneKc) {
+      e = build_tiles(c, cand, kSweepShape[sh][0], kSweepShape[sh][1], kc);
+      if (e != cudaSuccess) break;
+      float ms = 0.f;
+      if (fp32)
+        e = time_sweep<float>(c, cand.view(-1), w.u32, w.v32, w.prim32, w.ps32, w.sn32,
+                              w.coefe32, w.coefdiag32, w.d32pp[0], w.d32pp[1], e0, e1, &ms);
+      else
+        e = time_sweep<double>(c, cand.view(-1), s.u, s.v, w.prim, s.pression, s.sn, w.coefe,
+                               w.coefdiag, w.dpp[0], w.dpp[1], e0, e1, &ms);
+      if (e != cudaSuccess) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        bti = cand.ti;
+        btj = cand.tj;
+        bkc = cand.kc;
+      }
+    }
+  dev_free(c, cand.d_tile);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = build_tiles(c, best, bti, btj, bkc);
+  if (e == cudaSuccess) {
+    (fp32 ? c->tuned32 : c->tuned64) = true;
+    (fp32 ? c->tune_ms32 : c->tune_ms64) = best_ms / 3.f;
+  }
   return e;
 }
 
@@ -413,9 +514,9 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   if (e != cudaSuccess) return cleanup_fail(e, "blocks");
   e = build_space(c, c->cells, [](const Blk& B, int x[3]) {
     x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = B.nk - 1; });
-  if (e == cudaSuccess)
-    e = build_space(c, c->cols, [](const Blk& B, int x[3]) {
-      x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = (B.nk - 1 + kJacCol - 1) / kJacCol; });
+  if (e == cudaSuccess) e = build_tiles(c, c->tiles64, 32, 8, 8);
+  if (e == cudaSuccess) e = build_tiles(c, c->tiles32, 32, 8, 8);
+  if (e == cudaSuccess) e = init_jacobi_25d();
   for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
     e = build_space(c, c->faces[dir], [dir](const Blk& B, int x[3]) {
       x[0] = dir == 0 ? B.ni : B.ni - 1;
@@ -521,7 +622,6 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.rv, (size_t)ld);
   for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
     e = dev_alloc(c, &c->w.dpp[q], (size_t)(5 * ld));
-    if (e == cudaSuccess) e = dev_alloc(c, &c->w.dfpp[q], (size_t)(9 * ld));
   }
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.normpart, (size_t)(15 * c->cells.ntiles));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.norms, 16);
@@ -699,7 +799,8 @@ static int implimf(cns_ctx* c, int l, int eu, const double* u, const double* dt,
   if (lmx < 0) return CNS_EINVAL;
   CK(zero_cols(c, d, 5, l));
   CK(prim_of(c, l, v));
-  CK(launch_implicit(c->d_blks, c->cells.view(l - 1), c->faces, l - 1, c->ph, c->sc, eu,
+  CK(launch_implicit(c->d_blks, c->cells.view(l - 1), c->tiles64.view(l - 1), c->faces, l - 1,
+                     c->ph, c->sc, eu,
                      lmx, u, dt, v, d, mu, mut, sn, vol, ps, cson, c->w, 0, c->st));
   return CNS_OK;
 }
@@ -751,21 +852,41 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
   if (c->sc.kdtl == 0)
     return fail(c, CNS_EINVAL, "the fused step runs with local time steps (kdtl != 0)");
-  if (c->sc.precision == 0) {
-    if (!c->gexec) CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c); }));
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
-    c->kernels_launched += (long long)nsteps * c->nk_gexec;
-    return CNS_OK;
-  }
-  if (!c->w.mixed_ready) {
+  if (nsteps == 0) return CNS_OK;
+  const int prec = c->sc.precision;
+  if (prec != 0 && !c->w.mixed_ready) {
     CK(ensure_mixed(c));
     CK(launch_to_float(c->state.sn, c->w.sn32, 9 * c->lay.ld, c->st));
   }
-  if (c->sc.precision == 1) {
+  // first iteration of a form whose sweeps are not tuned yet: run it eagerly
+  // (the launches the graph would hold), tune the sweep tiles on its data,
+  // then capture with the chosen tiles
+  bool eager = false;
+  if (prec == 0 && !c->tuned64) {
+    CK(enqueue_step(c));
+    CK(tune_sweeps(c, false));
+    drop_graphs(c);
+    eager = true;
+  } else if (prec != 0 && !c->tuned32) {
+    const bool refresh = prec == 2 && (c->mixed_iter % c->sc.kdefect) == 0;
+    CK(enqueue_step_mixed(c, prec == 1 ? kMixed : (refresh ? kDefectRefresh : kDefectRegular)));
+    if (prec == 2) ++c->mixed_iter;
+    CK(tune_sweeps(c, true));
+    drop_graphs(c);
+    eager = true;
+  }
+  if (eager) --nsteps;
+  if (prec == 0) {
+    if (!c->gexec) CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c); }));
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
+    c->kernels_launched += (long long)(nsteps + eager) * c->nk_gexec;
+    return CNS_OK;
+  }
+  if (prec == 1) {
     if (!c->gexec_mref)
       CK(capture(c, &c->gexec_mref, &c->nk_mref, [&] { return enqueue_step_mixed(c, kMixed); }));
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec_mref, c->st));
-    c->kernels_launched += (long long)nsteps * c->nk_mref;
+    c->kernels_launched += (long long)(nsteps + eager) * c->nk_mref;
     return CNS_OK;
   }
   if (!c->gexec_mref)
@@ -774,12 +895,36 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   if (!c->gexec_mreg)
     CK(capture(c, &c->gexec_mreg, &c->nk_mreg,
                [&] { return enqueue_step_mixed(c, kDefectRegular); }));
+  if (eager) c->kernels_launched += c->nk_mref;
   for (int s = 0; s < nsteps; ++s) {
     const bool refresh = (c->mixed_iter % c->sc.kdefect) == 0;
     CK(cudaGraphLaunch(refresh ? c->gexec_mref : c->gexec_mreg, c->st));
     c->kernels_launched += refresh ? c->nk_mref : c->nk_mreg;
     ++c->mixed_iter;
   }
+  return CNS_OK;
+}
+
+int cns_sweep_tiles(cns_ctx* c, int precision, int32_t* cfg) {
+  if (!c || !cfg || precision < 0 || precision > 2) return CNS_EINVAL;
+  const TileBuf& t = precision == 0 ? c->tiles64 : c->tiles32;
+  cfg[0] = t.ti;
+  cfg[1] = t.tj;
+  cfg[2] = t.kc;
+  cfg[3] = precision == 0 ? c->tuned64 : c->tuned32;
+  return CNS_OK;
+}
+
+int cns_set_sweep_tiles(cns_ctx* c, int precision, int ti, int tj, int kc) {
+  if (!c || precision < 0 || precision > 2 || kc < 1) return CNS_EINVAL;
+  bool ok = false;
+  for (int sh = 0; sh < kSweepShapes; ++sh)
+    ok = ok || (kSweepShape[sh][0] == ti && kSweepShape[sh][1] == tj);
+  if (!ok) return fail(c, CNS_EINVAL, "sweep patch shape not one of 32x4, 32x8, 16x8, 16x16");
+  CK(cudaStreamSynchronize(c->st));
+  CK(build_tiles(c, precision == 0 ? c->tiles64 : c->tiles32, ti, tj, kc));
+  (precision == 0 ? c->tuned64 : c->tuned32) = true;
+  drop_graphs(c);
   return CNS_OK;
 }
 

@@ -52,6 +52,17 @@ struct Scheme {
   double xk, eta, dt1min;
 };
 
+// 2.5D tiles of the implicit sweeps: tile t = (block, i0, j0, k0) covers
+// the cells i0..i0+TI-1, j0..j0+TJ-1, k0..k0+kc-1 of the block (clipped to
+// its real cells); the tiles of one block are contiguous
+struct Tiles {
+  const int4* tile;
+  int tile0;
+  int ntiles;
+  int kc;
+  int ti, tj;  // patch shape (selects the kernel instantiation)
+};
+
 // boundary tables (per boundary, then per list entry)
 struct Bnd {
   int nbnd;

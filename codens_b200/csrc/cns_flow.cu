@@ -724,12 +724,30 @@ cudaError_t launch_accumulate_t<double>(const Blk* blks, Space sp, const double*
 }
 
 template <>
-cudaError_t launch_sweeps_t<double>(const Blk* blks, Space cells, Phys ph, Scheme sc,
-                                    int eu, int lmx, long long ld, const double* u,
-                                    const double* v, const double* prim,
-                                    const double* ps, const double* sn,
-                                    const double* coefe, const double* coefdiag,
-                                    double* const dpp[2], double* const dfpp[2],
+cudaError_t launch_jacobi_25d_t<double>(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                                        long long ld, const double* u, const double* v,
+                                        const double* prim, const double* ps, const double* sn,
+                                        const double* coefe, const double* coefdiag,
+                                        const double* d_in, double* d_out, cudaStream_t st) {
+  return jacobi_25d_dispatch<double, 0>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, coefe,
+                                        coefdiag, d_in, d_out, st);
+}
+
+cudaError_t init_jacobi_25d() {
+  cudaError_t e = jacobi_25d_attr<double, 0>();
+  if (e == cudaSuccess) e = init_jacobi_25d_float();
+  return e;
+}
+
+// the FP64 sweeps: the first (zero previous iterate) per cell, the others
+// 2.5D-blocked with the increments evaluated by the reference expressions
+// (bit-identical to storing them, implimf_3d.f90:222-466)
+template <>
+cudaError_t launch_sweeps_t<double>(const Blk* blks, Space cells, Tiles tl, Phys ph,
+                                    Scheme sc, int eu, int lmx, long long ld, const double* u,
+                                    const double* v, const double* prim, const double* ps,
+                                    const double* sn, const double* coefe,
+                                    const double* coefdiag, double* const dpp[2],
                                     int* cur_out, cudaStream_t st) {
   const int g = grid_of(cells);
   int cur = 0;
@@ -737,31 +755,26 @@ cudaError_t launch_sweeps_t<double>(const Blk* blks, Space cells, Phys ph, Schem
     cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(double) * 5 * ld, st);
     if (e0 != cudaSuccess) return e0;
   }
+  const int q = eu ? sc.qfix_dfez : 0;
   for (int ls = 1; ls <= lmx; ++ls) {
     const int nxt = (ls == 1) ? 0 : 1 - cur;
     const double* din = dpp[cur];
-    const double* dfin = dfpp[cur];
     double* dout = dpp[nxt];
-    double* dfout = dfpp[nxt];
-    const int q = eu ? sc.qfix_dfez : 0;
-    if (eu) {
-      if (ls == 1)
-        k_jacobi<double, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                          ps, sn, coefe, coefdiag, din, dfin,
-                                                          dout, dfout);
-      else
-        k_jacobi<double, true, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                           ps, sn, coefe, coefdiag, din, dfin,
-                                                           dout, dfout);
+    if (ls == 1) {
+      if (g > 0) {
+        if (eu)
+          k_jacobi_rc<double, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                               prim, ps, sn, coefe, coefdiag,
+                                                               din, dout);
+        else
+          k_jacobi_rc<double, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                                prim, ps, sn, coefe, coefdiag,
+                                                                din, dout);
+      }
     } else {
-      if (ls == 1)
-        k_jacobi<double, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                           ps, sn, coefe, coefdiag, din, dfin,
-                                                           dout, dfout);
-      else
-        k_jacobi<double, false, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
-                                                            prim, ps, sn, coefe, coefdiag, din,
-                                                            dfin, dout, dfout);
+      cudaError_t e1 = launch_jacobi_25d_t<double>(blks, tl, ph, q, eu, ld, u, v, prim, ps, sn,
+                                                   coefe, coefdiag, din, dout, st);
+      if (e1 != cudaSuccess) return e1;
     }
     cur = nxt;
   }
@@ -816,7 +829,7 @@ cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
                                       sn, vol, cson, w, coefe32, coefdiag32, st);
 }
 
-cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
+cudaError_t launch_implicit(const Blk* blks, Space cells, Tiles tl, const SpaceBuf* faces,
                             int l0, Phys ph, Scheme sc, int eu, int lmx,
                             const double* u, const double* dt, double* v,
                             double* d_out, const double* mu, const double* mut,
@@ -830,8 +843,8 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
                                                 st);
   int cur = 0;
   if (e == cudaSuccess)
-    e = launch_sweeps_t<double>(blks, cells, ph, sc, eu, lmx, ld, u, v, w.prim, ps, sn,
-                                w.coefe, w.coefdiag, w.dpp, w.dfpp, &cur, st);
+    e = launch_sweeps_t<double>(blks, cells, tl, ph, sc, eu, lmx, ld, u, v, w.prim, ps, sn,
+                                w.coefe, w.coefdiag, w.dpp, &cur, st);
   if (e == cudaSuccess)
     e = launch_update_t<double>(blks, cells, ld, w.dpp[cur], v, dt, d_out,
                                 want_norms ? w.normpart : nullptr, st);

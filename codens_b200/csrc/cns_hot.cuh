@@ -3,14 +3,16 @@
 //   k_ratio       limiter slope-ratio recurrence (sch_roe.f90:146-194)
 //   k_face_flux   Roe-MUSCL face flux, Euler or Navier-Stokes (sch_roe*.f90)
 //   k_accumulate  face-owned residual accumulation, always summed in FP64
-//   k_jacobi      one point-Jacobi sweep (implimf_eu.f90, implimf_3d.f90)
+//   k_jacobi_rc   first point-Jacobi sweep, per cell (implimf_eu.f90,
+//                 implimf_3d.f90)
+//   k_jacobi_25d  the following sweeps, 2.5D-blocked through shared memory
 //   k_update      v += d in FP64 and the residual-norm partials
 //
 // The FP64 instantiations (cns_flow.cu, built with --fmad=false) evaluate the
 // reference expressions in the reference's order and are bit-identical to
 // the reference semantics.  The FP32 instantiations (cns_mixed.cu, built with
 // FMA contraction) are the reduced-precision half of the mixed-precision
-// form, where FP64 stays for metrics, the residual accumulation, the state
+// forms, where FP64 stays for metrics, the residual accumulation, the state
 // update and the norms.  Every literal is written T(...) so that the FP32
 // instantiation never promotes to double.
 //
@@ -451,151 +453,6 @@ __global__ void __launch_bounds__(kTile) k_accumulate(const Blk* __restrict__ bl
 
 // df index: 0 xx, 1 xy, 2 xz, 3 ex, 4 yy, 5 yz, 6 ey, 7 zz, 8 ez
 
-// flux-increment projections tn(1..5) on the face between cells nu (above)
-// and nl (below) (implimf_eu.f90:272-291, implimf_3d.f90:243-262)
-template <class T, bool EU, bool FIRST>
-__device__ __forceinline__ void jacobi_tn(const T* __restrict__ d,
-                                          const T* __restrict__ df, long long ld,
-                                          long long nu, long long nl, T sx, T sy,
-                                          T sz, T tn[5]) {
-  T a2, a3, a4, fxx, fxy, fxz, fex, fyy, fyz, fey, fzz, fez;
-  if (FIRST) {
-    a2 = a3 = a4 = T(0.) + T(0.);
-    fxx = fxy = fxz = fex = fyy = fyz = fey = fzz = fez = T(0.) + T(0.);
-  } else {
-    a2 = d[ld + nu] + d[ld + nl];
-    a3 = d[2 * ld + nu] + d[2 * ld + nl];
-    a4 = d[3 * ld + nu] + d[3 * ld + nl];
-    fxx = df[nu] + df[nl];
-    fxy = df[ld + nu] + df[ld + nl];
-    fxz = df[2 * ld + nu] + df[2 * ld + nl];
-    fex = df[3 * ld + nu] + df[3 * ld + nl];
-    fyy = df[4 * ld + nu] + df[4 * ld + nl];
-    fyz = df[5 * ld + nu] + df[5 * ld + nl];
-    fey = df[6 * ld + nu] + df[6 * ld + nl];
-    fzz = df[7 * ld + nu] + df[7 * ld + nl];
-    fez = df[8 * ld + nu] + df[8 * ld + nl];
-  }
-  const T h = T(0.5);
-  if (EU) {
-    tn[0] = h * (a2 * sx + a3 * sy + a4 * sz);
-    tn[1] = h * (fxx * sx + fxy * sy + fxz * sz);
-    tn[2] = h * (fxy * sx + fyy * sy + fyz * sz);
-    tn[3] = h * (fxz * sx + fyz * sy + fzz * sz);
-    tn[4] = h * (fex * sx + fey * sy + fez * sz);
-  } else {
-    tn[0] = h * a2 * sx + h * a3 * sy + h * a4 * sz;
-    tn[1] = h * fxx * sx + h * fxy * sy + h * fxz * sz;
-    tn[2] = h * fxy * sx + h * fyy * sy + h * fyz * sz;
-    tn[3] = h * fxz * sx + h * fyz * sy + h * fzz * sz;
-    tn[4] = h * fex * sx + h * fey * sy + h * fez * sz;
-  }
-}
-
-// one Jacobi sub-iteration on one real cell: d2w = -u + sum over the faces,
-// d = d2w / coefdiag, then the flux increments of v+d (implimf_eu.f90:
-// 176-323, implimf_3d.f90:222-466).  Reads the previous iterate (d_in,
-// df_in), writes the next one; FIRST: the previous iterate is zero.
-template <class T, bool EU, bool FIRST>
-__global__ void __launch_bounds__(kTile) k_jacobi(
-    const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
-    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
-    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
-    const T* __restrict__ coefdiag, const T* __restrict__ d_in,
-    const T* __restrict__ df_in, T* __restrict__ d_out, T* __restrict__ df_out) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
-  T d2w[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long inc = ninc_of(B, dir);
-    const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
-            *s2 = sn_ptr(sn, B, dir, 2);
-    const T* ce = coefe + (long long)dir * ld;
-    T tn[5];
-    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - inc, s0[n], s1[n], s2[n], tn);
-    const T cel = ce[n], ceu = ce[n + inc];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      const T dl = FIRST ? T(0.) : d_in[a * ld + n - inc];
-      const T du = FIRST ? T(0.) : d_in[a * ld + n + inc];
-      d2w[a] = d2w[a] + tn[a] + cel * dl + ceu * du;
-    }
-    const long long nu = n + inc;
-    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, s0[nu], s1[nu], s2[nu], tn);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
-  }
-  const T cd = coefdiag[n];
-  T dn[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-    dn[a] = d2w[a] / cd;
-    d_out[a * ld + n] = dn[a];
-  }
-  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl), h = T(0.5);
-  const T v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n],
-          v5 = v[4 * ld + n], p = ps[n];
-  T f[9];
-  if (EU) {
-    const T wi1 = T(1.) / (v1 + dn[0]);
-    const T ui = v2 + dn[1], vi = v3 + dn[2], wi = v4 + dn[3], wi5 = v5 + dn[4];
-    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
-    const T norm = T(1.) / v1;
-    const T fxx = v2 * (v2 * norm) + p;
-    const T fxy = v3 * (v2 * norm);
-    const T fxz = v4 * (v2 * norm);
-    const T fyy = v3 * (v3 * norm) + p;
-    const T fyz = v4 * (v3 * norm);
-    const T fzz = v4 * (v4 * norm) + p;
-    const T fex = (v5 + p - pinfl) * v2 * norm;
-    const T fey = (v5 + p - pinfl) * v3 * norm;
-    const T fez = (v5 + p - pinfl) * v4 * norm;
-    f[0] = wi1 * sqT(ui) + pres - fxx;
-    f[1] = wi1 * ui * vi - fxy;
-    f[2] = wi1 * ui * wi - fxz;
-    f[3] = wi1 * ui * (wi5 + pres - pinfl) - fex;
-    f[4] = wi1 * sqT(vi) + pres - fyy;
-    f[5] = wi1 * vi * wi - fyz;
-    f[6] = wi1 * vi * (wi5 + pres - pinfl) - fey;
-    f[7] = wi1 * sqT(wi) + pres - fzz;
-    // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
-    // parity path keeps it, qfix (a flagged non-reference option) restores it
-    f[8] = qfix ? wi1 * wi * (wi5 + pres - pinfl) - fez
-                : wi1 * (wi5 + pres - pinfl) - fez;
-  } else {
-    const T wi1 = v1 + dn[0];
-    const T ui = (v2 + dn[1]) / wi1, vi = (v3 + dn[2]) / wi1, wi = (v4 + dn[3]) / wi1;
-    const T wi5 = v5 + dn[4];
-    const T pres = gam1 * (wi5 - h * wi1 * (sqT(ui) + sqT(vi) + sqT(wi)) - pinfl);
-    const T qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
-    const T fxx = v2 * qu + p;
-    const T fxy = v3 * qu;
-    const T fxz = v4 * qu;
-    const T fyy = v3 * qv + p;
-    const T fyz = v4 * qv;
-    const T fzz = v4 * qw + p;
-    const T fex = (v5 + p - pinfl) * v2 / v1;
-    const T fey = (v5 + p - pinfl) * v3 / v1;
-    const T fez = (v5 + p - pinfl) * v4 / v1;
-    f[0] = wi1 * sqT(ui) + pres - fxx;
-    f[1] = wi1 * ui * vi - fxy;
-    f[2] = wi1 * ui * wi - fxz;
-    f[3] = ui * (wi5 + pres - pinfl) - fex;
-    f[4] = wi1 * sqT(vi) + pres - fyy;
-    f[5] = wi1 * vi * wi - fyz;
-    f[6] = vi * (wi5 + pres - pinfl) - fey;
-    f[7] = wi1 * sqT(wi) + pres - fzz;
-    f[8] = wi * (wi5 + pres - pinfl) - fez;
-  }
-#pragma unroll
-  for (int a = 0; a < 9; ++a) df_out[a * ld + n] = f[a];
-}
-
 // flux increments of v+d minus those of v (implimf_eu.f90:301-312,
 // implimf_3d.f90:430-463) for one cell
 template <class T, bool EU>
@@ -649,97 +506,6 @@ __device__ __forceinline__ void jacobi_df(const T dn[5], T v1, T v2, T v3, T v4,
     f[6] = vi * (wi5 + pres - pinfl) - fey;
     f[7] = wi1 * sqT(wi) + pres - fzz;
     f[8] = wi * (wi5 + pres - pinfl) - fez;
-  }
-}
-
-// The same sweep with each thread walking a column of up to KC cells along
-// k (the index space gives the first cell of each column): the k face shared
-// by two consecutive cells is evaluated once and the upper cell's iterate is
-// loaded once and carried, which cuts the loads of a sweep by about a third.
-// Per cell the arithmetic and its order are those of k_jacobi.
-template <class T, bool EU, bool FIRST, int KC>
-__global__ void __launch_bounds__(kTile, 3) k_jacobi_col(
-    const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
-    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
-    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
-    const T* __restrict__ coefdiag, const T* __restrict__ d_in,
-    const T* __restrict__ df_in, T* __restrict__ d_out, T* __restrict__ df_out) {
-  int b, i, j, kc;
-  if (!space_elem(sp, threadIdx.x, b, i, j, kc)) return;
-  const Blk& B = blks[b];
-  const int k0 = 1 + (kc - 1) * KC;
-  const int k1 = min(k0 + KC - 1, B.nk - 1);
-  const long long K = B.nijd;
-  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
-  const T *sk0 = sn_ptr(sn, B, 2, 0), *sk1 = sn_ptr(sn, B, 2, 1), *sk2 = sn_ptr(sn, B, 2, 2);
-  const T* cek = coefe + 2 * ld;
-  long long n = cell_index(B, i, j, k0);
-  // lower k face of the first cell
-  T tnk[5];
-  jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - K, sk0[n], sk1[n], sk2[n], tnk);
-  T cek_lo = cek[n];
-  T dlo[5];  // iterate of the cell below
-#pragma unroll
-  for (int a = 0; a < 5; ++a) dlo[a] = FIRST ? T(0.) : d_in[a * ld + n - K];
-  for (int k = k0; k <= k1; ++k, n += K) {
-    T d2w[5];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
-    // i and j directions as in k_jacobi
-#pragma unroll
-    for (int dir = 0; dir < 2; ++dir) {
-      const long long inc = ninc_of(B, dir);
-      const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
-              *s2 = sn_ptr(sn, B, dir, 2);
-      const T* ce = coefe + (long long)dir * ld;
-      T tn[5];
-      jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, n, n - inc, s0[n], s1[n], s2[n], tn);
-      const T cel = ce[n], ceu = ce[n + inc];
-#pragma unroll
-      for (int a = 0; a < 5; ++a) {
-        const T dl = FIRST ? T(0.) : d_in[a * ld + n - inc];
-        const T du = FIRST ? T(0.) : d_in[a * ld + n + inc];
-        d2w[a] = d2w[a] + tn[a] + cel * dl + ceu * du;
-      }
-      const long long nu = n + inc;
-      jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, s0[nu], s1[nu], s2[nu], tn);
-#pragma unroll
-      for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
-    }
-    // k direction: lower face carried, upper face evaluated once
-    const long long nu = n + K;
-    const T ceu = cek[nu];
-    T dup[5];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      dup[a] = FIRST ? T(0.) : d_in[a * ld + nu];
-      d2w[a] = d2w[a] + tnk[a] + cek_lo * dlo[a] + ceu * dup[a];
-    }
-    T tnu[5];
-    jacobi_tn<T, EU, FIRST>(d_in, df_in, ld, nu, n, sk0[nu], sk1[nu], sk2[nu], tnu);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tnu[a];
-    // this cell's new iterate
-    const T cd = coefdiag[n];
-    T dn[5];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      dn[a] = d2w[a] / cd;
-      d_out[a * ld + n] = dn[a];
-    }
-    T f[9];
-    jacobi_df<T, EU>(dn, v[n], v[ld + n], v[2 * ld + n], v[3 * ld + n], v[4 * ld + n], ps[n],
-                     EU ? T(0.) : prim[n], EU ? T(0.) : prim[ld + n],
-                     EU ? T(0.) : prim[2 * ld + n], gam1, pinfl, qfix, f);
-#pragma unroll
-    for (int a = 0; a < 9; ++a) df_out[a * ld + n] = f[a];
-    // move up: the upper face becomes the next cell's lower face
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-      tnk[a] = tnu[a];
-      dlo[a] = FIRST ? T(0.) : d_in[a * ld + n];
-    }
-    cek_lo = ceu;
   }
 }
 
@@ -884,6 +650,220 @@ __global__ void __launch_bounds__(kTile) k_jacobi_rc(
   const T cd = coefdiag[n];
 #pragma unroll
   for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
+}
+
+// ---------------------------------------------------------------------------
+// 2.5D-blocked point-Jacobi sweep (every sweep after the first).
+//
+// A CTA owns a TI x TJ patch of columns of one block and marches along k over
+// kc planes.  For each plane it evaluates the iterate d and the flux
+// increment f(v+d) - f(v) of every cell of the patch and of its one-cell
+// ring once, into shared memory (double-buffered: planes k and k+1); the
+// own column's plane k-1 stays in registers.  A cell then reads all six
+// neighbours' (d, f) on chip, so a sweep moves d, v, prim, ps, u, the
+// coefficients and the face areas once per cell from HBM, and evaluates each
+// increment ~1.3 times (ring) instead of seven times.
+//
+// FORM 0 evaluates the increment with the reference expressions
+// (jacobi_df: implimf_3d.f90:430-463, implimf_eu.f90:301-312), so the FP64
+// instantiation reproduces the stored-increment sweep bit for bit (the same
+// inputs through the same operations); FORM 1 uses the difference form of
+// df_of (reduced precision).  Neighbours outside the block's real cells
+// contribute zero, as the reference's never-written ghost increments do.
+// ---------------------------------------------------------------------------
+template <class T, bool EU, int FORM>
+__device__ __forceinline__ void cell_df(const T* __restrict__ v, const T* __restrict__ prim,
+                                        const T* __restrict__ ps, const T* __restrict__ d,
+                                        long long ld, long long m, T gam1, T pinfl, int qfix,
+                                        T dd[5], T f[9]) {
+  if (FORM == 1) {
+    df_of<T, EU>(v, prim, ps, d, ld, m, gam1, pinfl, qfix, dd, f);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) dd[a] = d[a * ld + m];
+    jacobi_df<T, EU>(dd, v[m], v[ld + m], v[2 * ld + m], v[3 * ld + m], v[4 * ld + m], ps[m],
+                     EU ? T(0.) : prim[m], EU ? T(0.) : prim[ld + m],
+                     EU ? T(0.) : prim[2 * ld + m], gam1, pinfl, qfix, f);
+  }
+}
+
+template <class T, bool EU, int FORM, int TI, int TJ>
+__global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
+    const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
+    const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
+    const T* __restrict__ coefdiag, const T* __restrict__ d_in, T* __restrict__ d_out) {
+  constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);  // [2 planes][14 values][NP]
+  const int4 t = tl.tile[tl.tile0 + blockIdx.x];
+  const Blk B = blks[t.x];
+  const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+  const int i = t.y + tx, j = t.z + ty;
+  const int kbeg = t.w, kend = min(t.w + tl.kc, B.nk);
+  const bool own = i <= B.ni - 1 && j <= B.nj - 1;
+  const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
+
+  // plane kk of the patch and its ring into buffer b (zero outside the block)
+  auto fill = [&](int kk, int b) {
+    T* s = sm + b * 14 * NP;
+    for (int q = threadIdx.x; q < NP; q += NT) {
+      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+      T dd[5], f[9];
+      if (ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
+          kk <= B.nk - 1) {
+        cell_df<T, EU, FORM>(v, prim, ps, d_in, ld, cell_index(B, ii, jj, kk), gam1, pinfl,
+                             qfix, dd, f);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 5; ++a) dd[a] = T(0.);
+#pragma unroll
+        for (int a = 0; a < 9; ++a) f[a] = T(0.);
+      }
+#pragma unroll
+      for (int a = 0; a < 5; ++a) s[a * NP + q] = dd[a];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) s[(5 + a) * NP + q] = f[a];
+    }
+  };
+
+  // the own column's plane kbeg-1 (registers)
+  T pd[5], pf[9];
+  if (own && kbeg >= 2) {
+    cell_df<T, EU, FORM>(v, prim, ps, d_in, ld, cell_index(B, i, j, kbeg - 1), gam1, pinfl,
+                         qfix, pd, pf);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) pd[a] = T(0.);
+#pragma unroll
+    for (int a = 0; a < 9; ++a) pf[a] = T(0.);
+  }
+  fill(kbeg, kbeg & 1);
+  const int q0 = (ty + 1) * NX + tx + 1;
+  for (int k = kbeg; k < kend; ++k) {
+    fill(k + 1, (k + 1) & 1);
+    __syncthreads();
+    if (own) {
+      const T* s = sm + (k & 1) * 14 * NP;
+      const T* su = sm + ((k + 1) & 1) * 14 * NP;
+      const long long n = cell_index(B, i, j, k);
+      T d0[5], f0[9];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) d0[a] = s[a * NP + q0];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) f0[a] = s[(5 + a) * NP + q0];
+      T d2w[5];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        const long long inc = ninc_of(B, dir);
+        const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
+                *s2 = sn_ptr(sn, B, dir, 2);
+        const T* ce = coefe + (long long)dir * ld;
+        T dl[5], fl[9], du[5], fu[9];
+        if (dir == 2) {
+#pragma unroll
+          for (int a = 0; a < 5; ++a) {
+            dl[a] = pd[a];
+            du[a] = su[a * NP + q0];
+          }
+#pragma unroll
+          for (int a = 0; a < 9; ++a) {
+            fl[a] = pf[a];
+            fu[a] = su[(5 + a) * NP + q0];
+          }
+        } else {
+          const int off = dir == 0 ? 1 : NX;
+#pragma unroll
+          for (int a = 0; a < 5; ++a) {
+            dl[a] = s[a * NP + q0 - off];
+            du[a] = s[a * NP + q0 + off];
+          }
+#pragma unroll
+          for (int a = 0; a < 9; ++a) {
+            fl[a] = s[(5 + a) * NP + q0 - off];
+            fu[a] = s[(5 + a) * NP + q0 + off];
+          }
+        }
+        T tn[5];
+        face_tn<T, EU>(d0, dl, f0, fl, s0[n], s1[n], s2[n], tn);
+        const T cel = ce[n], ceu = ce[n + inc];
+#pragma unroll
+        for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] + tn[a] + cel * dl[a] + ceu * du[a];
+        const long long nu = n + inc;
+        face_tn<T, EU>(du, d0, fu, f0, s0[nu], s1[nu], s2[nu], tn);
+#pragma unroll
+        for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
+      }
+      const T cd = coefdiag[n];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) pd[a] = d0[a];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) pf[a] = f0[a];
+    }
+    __syncthreads();
+  }
+}
+
+template <int TI, int TJ, class T>
+constexpr size_t jacobi_25d_smem() {
+  return sizeof(T) * 2 * 14 * (TI + 2) * (TJ + 2);
+}
+
+template <class T, int FORM, int TI, int TJ>
+cudaError_t jacobi_25d_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                             long long ld, const T* u, const T* v, const T* prim, const T* ps,
+                             const T* sn, const T* coefe, const T* coefdiag, const T* d_in,
+                             T* d_out, cudaStream_t st) {
+  const size_t sm = jacobi_25d_smem<TI, TJ, T>();
+  if (eu)
+    k_jacobi_25d<T, true, FORM, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+  else
+    k_jacobi_25d<T, false, FORM, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+  return cudaGetLastError();
+}
+
+template <class T, int FORM>
+cudaError_t jacobi_25d_dispatch(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                                long long ld, const T* u, const T* v, const T* prim,
+                                const T* ps, const T* sn, const T* coefe, const T* coefdiag,
+                                const T* d_in, T* d_out, cudaStream_t st) {
+  if (tl.ntiles == 0) return cudaSuccess;
+#define CNS_SHAPE(A, B)                                                                   \
+  if (tl.ti == A && tl.tj == B)                                                           \
+    return jacobi_25d_shape<T, FORM, A, B>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, \
+                                           coefe, coefdiag, d_in, d_out, st);
+  CNS_SHAPE(32, 4)
+  CNS_SHAPE(32, 8)
+  CNS_SHAPE(16, 8)
+  CNS_SHAPE(16, 16)
+#undef CNS_SHAPE
+  return cudaErrorInvalidValue;
+}
+
+template <class T, int FORM, int TI, int TJ>
+cudaError_t jacobi_25d_attr_shape() {
+  const int sm = (int)jacobi_25d_smem<TI, TJ, T>();
+  cudaError_t e = cudaFuncSetAttribute(k_jacobi_25d<T, true, FORM, TI, TJ>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_jacobi_25d<T, false, FORM, TI, TJ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
+
+template <class T, int FORM>
+cudaError_t jacobi_25d_attr() {
+  cudaError_t e = jacobi_25d_attr_shape<T, FORM, 32, 4>();
+  if (e == cudaSuccess) e = jacobi_25d_attr_shape<T, FORM, 32, 8>();
+  if (e == cudaSuccess) e = jacobi_25d_attr_shape<T, FORM, 16, 8>();
+  if (e == cudaSuccess) e = jacobi_25d_attr_shape<T, FORM, 16, 16>();
+  return e;
 }
 
 // per-tile partial residual norms of (v_new - v_old)/dt (residu.f90:127-182)

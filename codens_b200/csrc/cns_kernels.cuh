@@ -12,7 +12,10 @@ __device__ __forceinline__ double* sn_wptr(double* sn, const Blk& B, int dir,
 }
 
 constexpr int kTile = 128;  // elements per tile (= threads per CTA)
-constexpr int kJacCol = 4;  // cells per thread of a Jacobi sweep (a k column)
+// patch shapes (TI x TJ columns) of the 2.5D Jacobi sweep; the autotuner
+// picks one of them and the plane count kc per context
+constexpr int kSweepShapes = 4;
+constexpr int kSweepShape[kSweepShapes][2] = {{32, 4}, {32, 8}, {16, 8}, {16, 16}};
 
 struct HostLayout {
   std::vector<Blk> blks;
@@ -42,6 +45,28 @@ struct SpaceBuf {
   }
 };
 
+// the 2.5D tile list of one sweep configuration
+struct TileBuf {
+  int ti = 0, tj = 0, kc = 0, ntiles = 0;
+  std::vector<int> blk_tile0;  // first tile of each block, size nblk+1
+  int4* d_tile = nullptr;
+  Tiles view(int l0 = -1) const {
+    Tiles t;
+    t.tile = d_tile;
+    t.kc = kc;
+    t.ti = ti;
+    t.tj = tj;
+    if (l0 < 0) {
+      t.tile0 = 0;
+      t.ntiles = ntiles;
+    } else {
+      t.tile0 = blk_tile0[l0];
+      t.ntiles = blk_tile0[l0 + 1] - blk_tile0[l0];
+    }
+    return t;
+  }
+};
+
 // per-step scratch (device)
 struct Work {
   long long ld = 0;
@@ -52,7 +77,6 @@ struct Work {
   double* coefdiag = nullptr; // [ld]
   double* rv = nullptr;       // [ld]
   double* dpp[2] = {nullptr, nullptr};   // Jacobi iterates, [5][ld] each
-  double* dfpp[2] = {nullptr, nullptr};  // flux increments, [9][ld] each
   double* normpart = nullptr; // per tile partial norms [ntiles][15]
   double* norms = nullptr;    // [16]
   double* blocksum = nullptr; // per block norm sums [nblk][15]
@@ -63,7 +87,6 @@ struct Work {
   float *sn32 = nullptr, *G32 = nullptr, *R32 = nullptr, *u32 = nullptr;
   float *coefe32 = nullptr, *coefdiag32 = nullptr;
   float* d32pp[2] = {nullptr, nullptr};
-  float* df32pp[2] = {nullptr, nullptr};
   double *corr = nullptr, *ur32 = nullptr;
 };
 
@@ -120,10 +143,10 @@ cudaError_t launch_accumulate_t(const Blk* blks, Space sp, const T* G, long long
                                 cudaStream_t st);
 // lmx Jacobi sweeps over the real cells; the final iterate is in dpp[*cur_out]
 template <class T>
-cudaError_t launch_sweeps_t(const Blk* blks, Space cells, Phys ph, Scheme sc, int eu,
+cudaError_t launch_sweeps_t(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
                             int lmx, long long ld, const T* u, const T* v, const T* prim,
                             const T* ps, const T* sn, const T* coefe, const T* coefdiag,
-                            T* const dpp[2], T* const dfpp[2], int* cur_out,
+                            T* const dpp[2], int* cur_out,
                             cudaStream_t st);
 template <class T>
 cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T* d,
@@ -143,9 +166,9 @@ cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T*
   cudaError_t launch_accumulate_t<T>(const Blk*, Space, const T*, long long,               \
                                      const double*, double*, float*, cudaStream_t);        \
   template <>                                                                               \
-  cudaError_t launch_sweeps_t<T>(const Blk*, Space, Phys, Scheme, int, int, long long,     \
+  cudaError_t launch_sweeps_t<T>(const Blk*, Space, Tiles, Phys, Scheme, int, int, long long, \
                                  const T*, const T*, const T*, const T*, const T*,          \
-                                 const T*, const T*, T* const[2], T* const[2], int*,        \
+                                 const T*, const T*, T* const[2], int*,                     \
                                  cudaStream_t);                                             \
   template <>                                                                               \
   cudaError_t launch_update_t<T>(const Blk*, Space, long long, const T*, double*,          \
@@ -153,6 +176,28 @@ cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T*
 CNS_DECLARE_HOT(double)
 CNS_DECLARE_HOT(float)
 #undef CNS_DECLARE_HOT
+
+// one sweep of the 2.5D kernel over the tiles tl (d_in -> d_out); every
+// sweep but the first of launch_sweeps_t runs through it
+template <class T>
+cudaError_t launch_jacobi_25d_t(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                                long long ld, const T* u, const T* v, const T* prim,
+                                const T* ps, const T* sn, const T* coefe, const T* coefdiag,
+                                const T* d_in, T* d_out, cudaStream_t st);
+template <>
+cudaError_t launch_jacobi_25d_t<double>(const Blk*, Tiles, Phys, int, int, long long,
+                                        const double*, const double*, const double*,
+                                        const double*, const double*, const double*,
+                                        const double*, const double*, double*, cudaStream_t);
+template <>
+cudaError_t launch_jacobi_25d_t<float>(const Blk*, Tiles, Phys, int, int, long long,
+                                       const float*, const float*, const float*, const float*,
+                                       const float*, const float*, const float*, const float*,
+                                       float*, cudaStream_t);
+// raise the dynamic shared-memory limit of every 2.5D instantiation (once
+// per device, before the first launch)
+cudaError_t init_jacobi_25d();
+cudaError_t init_jacobi_25d_float();
 
 inline cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
                                 const double* v, const double* prim, long long ld,
@@ -196,7 +241,7 @@ cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const doub
 // cells of the space: coefficients, lmx Jacobi sweeps, v += d; d_out
 // (optional) receives the final increment, want_norms stores per-tile
 // residual partials in w.normpart
-cudaError_t launch_implicit(const Blk* blks, Space cells, const SpaceBuf* faces,
+cudaError_t launch_implicit(const Blk* blks, Space cells, Tiles tl, const SpaceBuf* faces,
                             int l0, Phys ph, Scheme sc, int eu, int lmx,
                             const double* u, const double* dt, double* v,
                             double* d_out, const double* mu, const double* mut,

@@ -97,16 +97,26 @@ cudaError_t launch_accumulate_t<float>(const Blk* blks, Space sp, const float* G
   return cudaGetLastError();
 }
 
-// the FP32 sweeps of the mixed form: the flux increments are recomputed,
-// not stored (dfpp unused), so a sweep moves d and the constants only
 template <>
-cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Phys ph, Scheme sc, int eu,
-                                   int lmx, long long ld, const float* u, const float* v,
-                                   const float* prim, const float* ps, const float* sn,
-                                   const float* coefe, const float* coefdiag,
-                                   float* const dpp[2], float* const dfpp[2], int* cur_out,
-                                   cudaStream_t st) {
-  (void)dfpp;
+cudaError_t launch_jacobi_25d_t<float>(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                                       long long ld, const float* u, const float* v,
+                                       const float* prim, const float* ps, const float* sn,
+                                       const float* coefe, const float* coefdiag,
+                                       const float* d_in, float* d_out, cudaStream_t st) {
+  return jacobi_25d_dispatch<float, 1>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, coefe,
+                                       coefdiag, d_in, d_out, st);
+}
+
+cudaError_t init_jacobi_25d_float() { return jacobi_25d_attr<float, 1>(); }
+
+// the FP32 sweeps of the mixed forms: the first per cell, the others
+// 2.5D-blocked with the increments in difference form (no stored increments)
+template <>
+cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc,
+                                   int eu, int lmx, long long ld, const float* u,
+                                   const float* v, const float* prim, const float* ps,
+                                   const float* sn, const float* coefe, const float* coefdiag,
+                                   float* const dpp[2], int* cur_out, cudaStream_t st) {
   const int g = grid_of(cells);
   int cur = 0;
   if (lmx == 0) {
@@ -118,21 +128,21 @@ cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Phys ph, Scheme
     const int nxt = (ls == 1) ? 0 : 1 - cur;
     const float* din = dpp[cur];
     float* dout = dpp[nxt];
-    if (eu) {
-      if (ls == 1)
-        k_jacobi_rc<float, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                            ps, sn, coefe, coefdiag, din, dout);
-      else
-        k_jacobi_rc<float, true, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                             ps, sn, coefe, coefdiag, din, dout);
+    if (ls == 1) {
+      if (g > 0) {
+        if (eu)
+          k_jacobi_rc<float, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                              prim, ps, sn, coefe, coefdiag,
+                                                              din, dout);
+        else
+          k_jacobi_rc<float, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
+                                                               prim, ps, sn, coefe, coefdiag,
+                                                               din, dout);
+      }
     } else {
-      if (ls == 1)
-        k_jacobi_rc<float, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v, prim,
-                                                             ps, sn, coefe, coefdiag, din, dout);
-      else
-        k_jacobi_rc<float, false, false><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
-                                                              prim, ps, sn, coefe, coefdiag, din,
-                                                              dout);
+      cudaError_t e1 = launch_jacobi_25d_t<float>(blks, tl, ph, q, eu, ld, u, v, prim, ps, sn,
+                                                  coefe, coefdiag, din, dout, st);
+      if (e1 != cudaSuccess) return e1;
     }
     cur = nxt;
   }

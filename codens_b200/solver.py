@@ -145,6 +145,16 @@ class CodeNS:
     def scratch_bytes(self) -> int:
         return int(self.lib.cns_scratch_bytes(self.ctx))
 
+    def sweep_tiles(self, precision: int = 0):
+        """(ti, tj, kc, tuned) of the Jacobi sweep tiling of a precision"""
+        cfg = (C.c_int32 * 4)()
+        self._check(self.lib.cns_sweep_tiles(self.ctx, precision, cfg), "cns_sweep_tiles")
+        return tuple(int(x) for x in cfg)
+
+    def set_sweep_tiles(self, precision: int, ti: int, tj: int, kc: int):
+        self._check(self.lib.cns_set_sweep_tiles(self.ctx, precision, ti, tj, kc),
+                    "cns_set_sweep_tiles")
+
     @property
     def kernels_launched(self) -> int:
         """kernels launched so far by the fused-step graphs of this solver"""

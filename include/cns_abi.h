@@ -193,6 +193,16 @@ int cns_atsch_num_step(cns_ctx *ctx, int nsteps, double *norms);
  * for the stream and checks the device status word */
 int cns_atsch_num_launch(cns_ctx *ctx, int nsteps);
 int cns_last_norms(cns_ctx *ctx, double *norms);
+
+/* Jacobi sweep tiling (no counterpart in the reference).  Every sweep after
+ * the first runs 2.5D-blocked over patches of ti x tj cell columns, kc
+ * planes deep.  The first fused iteration of each precision tunes the tiling
+ * on its own data (FP64 results do not depend on it).  cns_sweep_tiles
+ * returns {ti, tj, kc, tuned} of precision 0 (FP64) or 1/2 (FP32 sweeps);
+ * cns_set_sweep_tiles fixes a tiling (ti x tj one of 32x4, 32x8, 16x8,
+ * 16x16; kc >= 1) and marks it tuned. */
+int cns_sweep_tiles(cns_ctx *ctx, int precision, int32_t *cfg);
+int cns_set_sweep_tiles(cns_ctx *ctx, int precision, int ti, int tj, int kc);
 /* drop-in call with host arrays: copies the real+ghost state v (host, ld x 5)
  * in, runs nsteps iterations, copies v back and returns the last norms */
 int cns_atsch_num_step_host(cns_ctx *ctx, double *v_host, int nsteps,

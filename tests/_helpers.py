@@ -57,6 +57,19 @@ def max_rel_cols(a, b):
     return float((np.abs(a - b) / scale).max())
 
 
+def state_err(a, b):
+    """largest state difference relative to the reference state's scale:
+    density and energy by their largest magnitude, every momentum component
+    by the largest momentum magnitude (a flow along x leaves the y and z
+    momenta at rounding level, where a per-component scale means nothing)"""
+    a = np.asarray(a).reshape(5, -1)
+    b = np.asarray(b).reshape(5, -1)
+    mom = float(np.sqrt((b[1:4] ** 2).sum(axis=0)).max())
+    scale = np.array([np.abs(b[0]).max(), mom, mom, mom, np.abs(b[4]).max()])
+    scale = np.maximum(scale, 1e-300)[:, None]
+    return float((np.abs(a - b) / scale).max())
+
+
 def assert_equal_bits(a, b, what):
     a = np.asarray(a)
     b = np.asarray(b)

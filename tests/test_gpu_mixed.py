@@ -14,7 +14,7 @@ import pytest
 
 from codens_b200 import cases
 
-from ._helpers import SMALL, assert_equal_bits, max_rel_cols, real
+from ._helpers import SMALL, assert_equal_bits, real, state_err
 
 pytestmark = pytest.mark.gpu
 
@@ -42,6 +42,13 @@ def _residual(s, case):
 
 def _box_viscous():
     return cases.box_case((8, 6, 5), seed=12, ns=True, ilim=0, reynz=100.0, skew=0.02)
+
+
+def _duct():
+    # inlet (idd) and outlet (prd) only, j and k periodic: a unique steady
+    # state (the uniform flow the inlet and outlet values set)
+    return cases.channel_case([6, 8, 5], 6, 4, seed=5, reynz=100.0, ilim=0, bump=0.0,
+                              walls=False)
 
 
 @pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu_qfix"])
@@ -94,6 +101,21 @@ def test_mixed_reaches_fp64_steady_state(cuda):
     b.set_scheme(case_b.scheme)
     n1 = b.atsch_num(1)
     assert n1[1, 0] < 1e-14, n1[1, 0]
+    a.close()
+    b.close()
+
+
+def test_mixed_matches_fp64_converged_state(cuda):
+    """a case with a unique steady state: 4500 iterations converge both
+    forms to FP64 rounding, and the states agree within STEADY_TOL"""
+    case = _duct()
+    a = _solver(case, 0)
+    b = _solver(_duct(), 1)
+    na = a.atsch_num(4500)
+    nb = b.atsch_num(4500)
+    assert na[1, 0] < 1e-13 and nb[1, 0] < 1e-13, (na[1, 0], nb[1, 0])
+    err = state_err(_state(b, case), _state(a, case))
+    assert err <= STEADY_TOL, err
     a.close()
     b.close()
 
