@@ -52,6 +52,10 @@ DTYPE = {"fp64": "f64", "mixed": "f64 residual/update, f32 sweeps",
 SWEEP_KERNEL = {"fp64": "k_jacobi<double> (point-Jacobi sweep, stored flux increments)",
                 "mixed": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)",
                 "defect": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)"}
+# DRAM bytes per cell of one 2.5D sweep launch, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 1.18M-cell channel;
+# traffic grows with the cells processed, so a full launch is this x cells
+SWEEP_TRAFFIC_PER_CELL = {"fp64": 326.3, "mixed": 144.4, "defect": 144.4}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -72,6 +76,8 @@ def parse():
     p.add_argument("--no-fp64-arm", action="store_true",
                    help="skip timing the plain FP64 iteration beside the mixed one")
     p.add_argument("--no-steady-check", action="store_true")
+    p.add_argument("--tiles", default=None,
+                   help="TI,TJ,KC: fix the Jacobi sweep tiling instead of autotuning it")
     p.add_argument("--ilim", type=int, default=0,
                    help="0: plain kappa=-1 MUSCL (default: the reference's limiter "
                         "recurrence stalls this channel at L2 ~1e-3); 1: minmod limiter")
@@ -319,6 +325,11 @@ def run_ours(args):
     case = make_case(args)
     s = CodeNS(case, device=local)
     s.metric()
+    if args.tiles:
+        ti, tj, kc = (int(x) for x in args.tiles.split(","))
+        s.set_sweep_tiles(PRECISION[args.precision], ti, tj, kc)
+        if args.precision != "fp64":
+            s.set_sweep_tiles(0, ti, tj, kc)
     nreal = case.layout.nreal
     warm = max(args.warmup, 3)
     # warm-up (also instantiates the step graphs)
@@ -411,7 +422,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": SWEEP_KERNEL[args.precision],
                          "achieved": ach_sweep, "peak": hbm, "unit": "GB/s",
                          "frac": ach_sweep / hbm, "peak_source": hbm_kind,
-                         "traffic": None, "ms_per_launch": t_sweep,
+                         "traffic": SWEEP_TRAFFIC_PER_CELL[args.precision] * nreal,
+                         "traffic_source": "ncu DRAM bytes per cell on the 1.18M-cell channel "
+                                           "x cells", "ms_per_launch": t_sweep,
                          "bytes_per_launch": bj * nreal, "bytes_per_cell": bj},
             "roofline_residual": {"bound": "hbm", "kernels": "FP64 residual (all blocks)",
                                   "achieved": ach_res, "peak": hbm, "unit": "GB/s",

@@ -534,15 +534,9 @@ __device__ __forceinline__ float rcpT<float>(float a) {
 }
 
 template <class T, bool EU>
-__device__ __forceinline__ void df_of(const T* __restrict__ v, const T* __restrict__ prim,
-                                      const T* __restrict__ ps, const T* __restrict__ d,
-                                      long long ld, long long n, T gam1, T pinfl, int qfix,
-                                      T dd[5], T f[9]) {
-#pragma unroll
-  for (int a = 0; a < 5; ++a) dd[a] = d[a * ld + n];
-  const T E = v[4 * ld + n], p = ps[n];
-  const T qu = prim[n], qv = prim[ld + n], qw = prim[2 * ld + n];
-  const T r1 = v[n] + dd[0];
+__device__ __forceinline__ void df_diff(const T dd[5], T rho, T E, T p, T qu, T qv, T qw,
+                                        T gam1, T pinfl, int qfix, T f[9]) {
+  const T r1 = rho + dd[0];
   const T ir1 = rcpT(r1);
   const T du = (dd[1] - qu * dd[0]) * ir1;
   const T dv = (dd[2] - qv * dd[0]) * ir1;
@@ -564,6 +558,17 @@ __device__ __forceinline__ void df_of(const T* __restrict__ v, const T* __restri
   // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
   // Euler form keeps it unless qfix (a flagged non-reference option) is set
   f[8] = (EU && !qfix) ? h1 * ir1 - h0 * qw : dw * h1 + qw * de;
+}
+
+template <class T, bool EU>
+__device__ __forceinline__ void df_of(const T* __restrict__ v, const T* __restrict__ prim,
+                                      const T* __restrict__ ps, const T* __restrict__ d,
+                                      long long ld, long long n, T gam1, T pinfl, int qfix,
+                                      T dd[5], T f[9]) {
+#pragma unroll
+  for (int a = 0; a < 5; ++a) dd[a] = d[a * ld + n];
+  df_diff<T, EU>(dd, v[n], v[4 * ld + n], ps[n], prim[n], prim[ld + n], prim[2 * ld + n], gam1,
+                 pinfl, qfix, f);
 }
 
 template <class T, bool EU>
@@ -655,22 +660,48 @@ __global__ void __launch_bounds__(kTile) k_jacobi_rc(
 // ---------------------------------------------------------------------------
 // 2.5D-blocked point-Jacobi sweep (every sweep after the first).
 //
-// A CTA owns a TI x TJ patch of columns of one block and marches along k over
-// kc planes.  For each plane it evaluates the iterate d and the flux
-// increment f(v+d) - f(v) of every cell of the patch and of its one-cell
-// ring once, into shared memory (double-buffered: planes k and k+1); the
-// own column's plane k-1 stays in registers.  A cell then reads all six
-// neighbours' (d, f) on chip, so a sweep moves d, v, prim, ps, u, the
-// coefficients and the face areas once per cell from HBM, and evaluates each
-// increment ~1.3 times (ring) instead of seven times.
+// A CTA owns a TI x TJ patch of cell columns of one block and marches along k
+// over kc planes.  For each plane it evaluates the iterate d and the flux
+// increment f(v+d) - f(v) of every cell of the patch and of its one-cell ring
+// once, into shared memory; the own column's plane k-1 stays in registers.
+// A cell then reads its six neighbours' (d, f) on chip, so a sweep moves d,
+// v, prim, ps, u, the coefficients and the face areas about once per cell
+// from HBM and evaluates each increment ~1.3 times (ring) instead of seven.
+//
+// Pipeline: the inputs of the increments (d, v, prim, ps of the patch and
+// ring) of plane k+2 are copied into shared memory with cp.async while plane
+// k is computed, and each cell's own inputs (u, face areas, coefficients)
+// are loaded before the barrier that precedes its evaluation, so neither
+// waits on HBM latency in the critical path.
 //
 // FORM 0 evaluates the increment with the reference expressions
 // (jacobi_df: implimf_3d.f90:430-463, implimf_eu.f90:301-312), so the FP64
 // instantiation reproduces the stored-increment sweep bit for bit (the same
 // inputs through the same operations); FORM 1 uses the difference form of
-// df_of (reduced precision).  Neighbours outside the block's real cells
+// df_diff (reduced precision).  Neighbours outside the block's real cells
 // contribute zero, as the reference's never-written ghost increments do.
 // ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// the increment of one cell read straight from global memory
 template <class T, bool EU, int FORM>
 __device__ __forceinline__ void cell_df(const T* __restrict__ v, const T* __restrict__ prim,
                                         const T* __restrict__ ps, const T* __restrict__ d,
@@ -687,6 +718,14 @@ __device__ __forceinline__ void cell_df(const T* __restrict__ v, const T* __rest
   }
 }
 
+// staged inputs of one increment: 0-4 d, then rho, rho E, p and the
+// velocity (FORM 1), or v(1..5), p and the velocity (FORM 0, the reference
+// expressions; the Euler form reads no velocity)
+template <int FORM>
+__host__ __device__ constexpr int raw_count(bool eu) {
+  return FORM == 1 ? 11 : (eu ? 11 : 14);
+}
+
 template <class T, bool EU, int FORM, int TI, int TJ>
 __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
     const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
@@ -694,8 +733,10 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
     const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
     const T* __restrict__ coefdiag, const T* __restrict__ d_in, T* __restrict__ d_out) {
   constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ;
+  constexpr int NR = raw_count<FORM>(EU);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sm = reinterpret_cast<T*>(smem_raw);  // [2 planes][14 values][NP]
+  T* sdf = reinterpret_cast<T*>(smem_raw);  // [2 planes][14 values][NP]: d, f
+  T* sraw = sdf + 2 * 14 * NP;              // [2 planes][NR inputs][NP]
   const int4 t = tl.tile[tl.tile0 + blockIdx.x];
   const Blk B = blks[t.x];
   const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
@@ -704,19 +745,57 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
   const bool own = i <= B.ni - 1 && j <= B.nj - 1;
   const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
 
-  // plane kk of the patch and its ring into buffer b (zero outside the block)
-  auto fill = [&](int kk, int b) {
-    T* s = sm + b * 14 * NP;
+  // the increment inputs of plane kk (patch and ring) into raw buffer b;
+  // cells outside the block's real cells are zero-filled
+  auto stage = [&](int kk, int b) {
+    T* r = sraw + b * NR * NP;
     for (int q = threadIdx.x; q < NP; q += NT) {
       const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
-      T dd[5], f[9];
-      if (ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
-          kk <= B.nk - 1) {
-        cell_df<T, EU, FORM>(v, prim, ps, d_in, ld, cell_index(B, ii, jj, kk), gam1, pinfl,
-                             qfix, dd, f);
+      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
+                      kk <= B.nk - 1;
+      const long long m = in ? cell_index(B, ii, jj, kk) : 0;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) cp_async_elem(r + a * NP + q, d_in + a * ld + m, in);
+      if (FORM == 1) {
+        cp_async_elem(r + 5 * NP + q, v + m, in);
+        cp_async_elem(r + 6 * NP + q, v + 4 * ld + m, in);
+        cp_async_elem(r + 7 * NP + q, ps + m, in);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) cp_async_elem(r + (8 + a) * NP + q, prim + a * ld + m, in);
       } else {
 #pragma unroll
-        for (int a = 0; a < 5; ++a) dd[a] = T(0.);
+        for (int a = 0; a < 5; ++a) cp_async_elem(r + (5 + a) * NP + q, v + a * ld + m, in);
+        cp_async_elem(r + 10 * NP + q, ps + m, in);
+        if (!EU) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            cp_async_elem(r + (11 + a) * NP + q, prim + a * ld + m, in);
+        }
+      }
+    }
+  };
+  // increments of the staged plane in raw buffer b into (d, f) buffer b
+  // (zero where the raw inputs are zero: outside the block)
+  auto fill = [&](int kk, int b) {
+    const T* r = sraw + b * NR * NP;
+    T* s = sdf + b * 14 * NP;
+    for (int q = threadIdx.x; q < NP; q += NT) {
+      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
+                      kk <= B.nk - 1;
+      T dd[5], f[9];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) dd[a] = r[a * NP + q];
+      if (in) {
+        if (FORM == 1)
+          df_diff<T, EU>(dd, r[5 * NP + q], r[6 * NP + q], r[7 * NP + q], r[8 * NP + q],
+                         r[9 * NP + q], r[10 * NP + q], gam1, pinfl, qfix, f);
+        else
+          jacobi_df<T, EU>(dd, r[5 * NP + q], r[6 * NP + q], r[7 * NP + q], r[8 * NP + q],
+                           r[9 * NP + q], r[10 * NP + q], EU ? T(0.) : r[11 * NP + q],
+                           EU ? T(0.) : r[12 * NP + q], EU ? T(0.) : r[13 * NP + q], gam1,
+                           pinfl, qfix, f);
+      } else {
 #pragma unroll
         for (int a = 0; a < 9; ++a) f[a] = T(0.);
       }
@@ -738,79 +817,145 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
 #pragma unroll
     for (int a = 0; a < 9; ++a) pf[a] = T(0.);
   }
+  stage(kbeg, kbeg & 1);
+  cp_async_commit();
+  stage(kbeg + 1, (kbeg + 1) & 1);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
   fill(kbeg, kbeg & 1);
+  __syncthreads();
   const int q0 = (ty + 1) * NX + tx + 1;
+  // the lower k face of plane kbeg; later planes carry it from the plane
+  // below (the upper face of cell k is the lower face of cell k+1: the same
+  // operands in the same order, so the carried value is bit-identical)
+  T tkl[5];
+  {
+    const T* s = sdf + (kbeg & 1) * 14 * NP;
+    T d0[5], f0[9], sk[3];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d0[a] = s[a * NP + q0];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) f0[a] = s[(5 + a) * NP + q0];
+    const long long n = cell_index(B, own ? i : 1, own ? j : 1, kbeg);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sk[c] = own ? sn_ptr(sn, B, 2, c)[n] : T(0.);
+    face_tn<T, EU>(d0, pd, f0, pf, sk[0], sk[1], sk[2], tkl);
+  }
+  // rows of the patch are TI consecutive lanes (TI = 16 or 32)
+  const bool iface = i <= B.ni && j <= B.nj - 1;  // lower i face exists (incl. i = ni)
+  const bool iedge = tx == TI - 1;
   for (int k = kbeg; k < kend; ++k) {
-    fill(k + 1, (k + 1) & 1);
-    __syncthreads();
+    // this cell's own inputs, in flight across the barrier
+    const long long n = cell_index(B, iface ? i : 1, iface ? j : 1, k);
+    T uu[5], si[3], sj[3], sju[3], sku[3], siu[3], cel[3], ceu[3], cd;
+    if (iface) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) si[c] = sn_ptr(sn, B, 0, c)[n];
+    }
     if (own) {
-      const T* s = sm + (k & 1) * 14 * NP;
-      const T* su = sm + ((k + 1) & 1) * 14 * NP;
-      const long long n = cell_index(B, i, j, k);
-      T d0[5], f0[9];
 #pragma unroll
-      for (int a = 0; a < 5; ++a) d0[a] = s[a * NP + q0];
+      for (int a = 0; a < 5; ++a) uu[a] = u[a * ld + n];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) f0[a] = s[(5 + a) * NP + q0];
-      T d2w[5];
-#pragma unroll
-      for (int a = 0; a < 5; ++a) d2w[a] = -u[a * ld + n];
+      for (int c = 0; c < 3; ++c) {
+        sj[c] = sn_ptr(sn, B, 1, c)[n];
+        sju[c] = sn_ptr(sn, B, 1, c)[n + B.nid];
+        sku[c] = sn_ptr(sn, B, 2, c)[n + B.nijd];
+        if (iedge) siu[c] = sn_ptr(sn, B, 0, c)[n + 1];
+      }
 #pragma unroll
       for (int dir = 0; dir < 3; ++dir) {
-        const long long inc = ninc_of(B, dir);
-        const T *s0 = sn_ptr(sn, B, dir, 0), *s1 = sn_ptr(sn, B, dir, 1),
-                *s2 = sn_ptr(sn, B, dir, 2);
-        const T* ce = coefe + (long long)dir * ld;
-        T dl[5], fl[9], du[5], fu[9];
-        if (dir == 2) {
-#pragma unroll
-          for (int a = 0; a < 5; ++a) {
-            dl[a] = pd[a];
-            du[a] = su[a * NP + q0];
-          }
-#pragma unroll
-          for (int a = 0; a < 9; ++a) {
-            fl[a] = pf[a];
-            fu[a] = su[(5 + a) * NP + q0];
-          }
-        } else {
-          const int off = dir == 0 ? 1 : NX;
-#pragma unroll
-          for (int a = 0; a < 5; ++a) {
-            dl[a] = s[a * NP + q0 - off];
-            du[a] = s[a * NP + q0 + off];
-          }
-#pragma unroll
-          for (int a = 0; a < 9; ++a) {
-            fl[a] = s[(5 + a) * NP + q0 - off];
-            fu[a] = s[(5 + a) * NP + q0 + off];
-          }
-        }
-        T tn[5];
-        face_tn<T, EU>(d0, dl, f0, fl, s0[n], s1[n], s2[n], tn);
-        const T cel = ce[n], ceu = ce[n + inc];
-#pragma unroll
-        for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] + tn[a] + cel * dl[a] + ceu * du[a];
-        const long long nu = n + inc;
-        face_tn<T, EU>(du, d0, fu, f0, s0[nu], s1[nu], s2[nu], tn);
-#pragma unroll
-        for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
+        cel[dir] = coefe[(long long)dir * ld + n];
+        ceu[dir] = coefe[(long long)dir * ld + n + ninc_of(B, dir)];
       }
-      const T cd = coefdiag[n];
-#pragma unroll
-      for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
-#pragma unroll
-      for (int a = 0; a < 5; ++a) pd[a] = d0[a];
-#pragma unroll
-      for (int a = 0; a < 9; ++a) pf[a] = f0[a];
+      cd = coefdiag[n];
     }
+    cp_async_wait<0>();
     __syncthreads();
+    // plane k+2's inputs go into the raw buffer plane k's used
+    stage(k + 2, k & 1);
+    cp_async_commit();
+    fill(k + 1, (k + 1) & 1);
+    __syncthreads();
+    const T* s = sdf + (k & 1) * 14 * NP;
+    const T* su = sdf + ((k + 1) & 1) * 14 * NP;
+    T d0[5], f0[9], dl[5], fl[9], du[5], fu[9], tl[5], tu[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d0[a] = s[a * NP + q0];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) f0[a] = s[(5 + a) * NP + q0];
+    // i: the lower face by every lane, the upper one from the next lane
+    // (the row's last lane evaluates its own)
+#pragma unroll
+    for (int a = 0; a < 5; ++a) dl[a] = s[a * NP + q0 - 1];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) fl[a] = s[(5 + a) * NP + q0 - 1];
+    face_tn<T, EU>(d0, dl, f0, fl, si[0], si[1], si[2], tl);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      du[a] = s[a * NP + q0 + 1];
+      tu[a] = __shfl_down_sync(0xffffffffu, tl[a], 1, TI);
+    }
+    if (iedge) {
+#pragma unroll
+      for (int a = 0; a < 9; ++a) fu[a] = s[(5 + a) * NP + q0 + 1];
+      face_tn<T, EU>(du, d0, fu, f0, siu[0], siu[1], siu[2], tu);
+    }
+    T d2w[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      d2w[a] = -uu[a];
+      d2w[a] = d2w[a] + tl[a] + cel[0] * dl[a] + ceu[0] * du[a];
+      d2w[a] = d2w[a] - tu[a];
+    }
+    // j: both faces
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      dl[a] = s[a * NP + q0 - NX];
+      du[a] = s[a * NP + q0 + NX];
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      fl[a] = s[(5 + a) * NP + q0 - NX];
+      fu[a] = s[(5 + a) * NP + q0 + NX];
+    }
+    face_tn<T, EU>(d0, dl, f0, fl, sj[0], sj[1], sj[2], tl);
+    face_tn<T, EU>(du, d0, fu, f0, sju[0], sju[1], sju[2], tu);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      d2w[a] = d2w[a] + tl[a] + cel[1] * dl[a] + ceu[1] * du[a];
+      d2w[a] = d2w[a] - tu[a];
+    }
+    // k: the lower face carried, the upper one evaluated and carried on
+#pragma unroll
+    for (int a = 0; a < 5; ++a) du[a] = su[a * NP + q0];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) fu[a] = su[(5 + a) * NP + q0];
+    face_tn<T, EU>(du, d0, fu, f0, sku[0], sku[1], sku[2], tu);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      d2w[a] = d2w[a] + tkl[a] + cel[2] * pd[a] + ceu[2] * du[a];
+      d2w[a] = d2w[a] - tu[a];
+      tkl[a] = tu[a];
+      pd[a] = d0[a];
+    }
+    if (own) {
+      if (FORM == 1) {
+        const T rc = T(1.) / cd;
+#pragma unroll
+        for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] * rc;
+      } else {
+#pragma unroll
+        for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
+      }
+    }
   }
+  cp_async_wait<0>();
 }
 
-template <int TI, int TJ, class T>
+template <int TI, int TJ, class T, int FORM, bool EU>
 constexpr size_t jacobi_25d_smem() {
-  return sizeof(T) * 2 * 14 * (TI + 2) * (TJ + 2);
+  return sizeof(T) * 2 * (14 + raw_count<FORM>(EU)) * (TI + 2) * (TJ + 2);
 }
 
 template <class T, int FORM, int TI, int TJ>
@@ -818,13 +963,14 @@ cudaError_t jacobi_25d_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int e
                              long long ld, const T* u, const T* v, const T* prim, const T* ps,
                              const T* sn, const T* coefe, const T* coefdiag, const T* d_in,
                              T* d_out, cudaStream_t st) {
-  const size_t sm = jacobi_25d_smem<TI, TJ, T>();
   if (eu)
-    k_jacobi_25d<T, true, FORM, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
-        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+    k_jacobi_25d<T, true, FORM, TI, TJ>
+        <<<tl.ntiles, TI * TJ, jacobi_25d_smem<TI, TJ, T, FORM, true>(), st>>>(
+            blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
   else
-    k_jacobi_25d<T, false, FORM, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
-        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+    k_jacobi_25d<T, false, FORM, TI, TJ>
+        <<<tl.ntiles, TI * TJ, jacobi_25d_smem<TI, TJ, T, FORM, false>(), st>>>(
+            blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
   return cudaGetLastError();
 }
 
@@ -848,12 +994,13 @@ cudaError_t jacobi_25d_dispatch(const Blk* blks, Tiles tl, Phys ph, int qfix, in
 
 template <class T, int FORM, int TI, int TJ>
 cudaError_t jacobi_25d_attr_shape() {
-  const int sm = (int)jacobi_25d_smem<TI, TJ, T>();
   cudaError_t e = cudaFuncSetAttribute(k_jacobi_25d<T, true, FORM, TI, TJ>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)jacobi_25d_smem<TI, TJ, T, FORM, true>());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_jacobi_25d<T, false, FORM, TI, TJ>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)jacobi_25d_smem<TI, TJ, T, FORM, false>());
   return e;
 }
 
