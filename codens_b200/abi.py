@@ -34,7 +34,8 @@ class Phys_t(C.Structure):
 class Scheme_t(C.Structure):
     _fields_ = [("ns", c_i32), ("muscl", c_i32), ("xk", c_f64), ("ilim", c_i32),
                 ("eta", c_f64), ("kdtl", c_i32), ("dt1min", c_f64), ("lmax", c_i32),
-                ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32)]
+                ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32),
+                ("ischema", c_i32), ("ki2", c_f64), ("ki4", c_f64)]
 
 
 class Bnd_t(C.Structure):
@@ -59,6 +60,7 @@ EXPORTS = [
     "cns_rscpsv", "cns_bind_state", "cns_atsch_num_step",
     "cns_atsch_num_launch", "cns_last_norms", "cns_atsch_num_step_host",
     "cns_sch_roe_euler_noalloc", "cns_sweep_tiles", "cns_set_sweep_tiles",
+    "cns_rfve", "cns_rfvc", "cns_dissip_jameson", "cns_sch_jameson",
 ]
 
 _lib = None
@@ -103,6 +105,10 @@ def load(build_if_missing: bool = True):
     L.cns_atsch_num_launch.argtypes = [vp, C.c_int]
     L.cns_last_norms.argtypes = [vp, P(c_f64)]
     L.cns_sweep_tiles.argtypes = [vp, C.c_int, P(c_i32)]
+    L.cns_rfve.argtypes = [vp] * 5
+    L.cns_rfvc.argtypes = [vp] * 5
+    L.cns_dissip_jameson.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_sch_jameson.argtypes = [vp, C.c_int] + [vp] * 6
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,

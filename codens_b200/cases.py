@@ -73,6 +73,9 @@ class Scheme:
     qfix_dfez: int = 0   # non-reference: restore the *wi of implimf_eu.f90:312
     precision: int = 0   # fused step: 0 FP64, 1 mixed (FP32 sweeps), 2 defect correction
     kdefect: int = 4     # precision 2: FP64 residual / defect refresh period
+    ischema: int = 7     # 7 Roe (sch_roe*), 1 Jameson (dissip_jameson + sch_jameson)
+    ki2: float = 0.5     # Jameson 2nd-difference coefficient ki2(lm)
+    ki4: float = 1.0 / 32.0  # Jameson 4th-difference coefficient ki4(lm)
 
 
 @dataclass
@@ -243,12 +246,13 @@ def box_case(cells=(64, 32, 32), mach: float = 0.8, seed: int = 1,
              noise: float = 0.01, ns: bool = False, ilim: int = 0,
              skew: float = 0.0, lmax: int = 10, eta: float = 5.0,
              pinfl: float = 0.0, reynz: float = 1.0e12, alpha: float = 0.0,
-             qfix_dfez: int = 0, name: str = "box") -> Case:
+             qfix_dfez: int = 0, ischema: int = 7, name: str = "box") -> Case:
     """Single stretched box: extr on i faces, self-periodic j and k."""
     ni, nj, nk = (c + 1 for c in cells)
     lay = Layout.from_dims([(ni, nj, nk)])
     phys = Phys(pinfl=pinfl, reynz=reynz)
-    scheme = Scheme(ns=int(ns), ilim=ilim, lmax=lmax, eta=eta, qfix_dfez=qfix_dfez)
+    scheme = Scheme(ns=int(ns), ilim=ilim, lmax=lmax, eta=eta, qfix_dfez=qfix_dfez,
+                    ischema=ischema)
     x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
     idx, X, Y, Z = _box_coords(lay, 0, skew=skew)
     x[idx], y[idx], z[idx] = X, Y, Z
@@ -316,7 +320,7 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
                  reynz: float = 1.0e4, noise: float = 0.01, lmax: int = 10,
                  eta: float = 5.0, ilim: int = 1, bump: float = 0.1,
                  length: float = 8.0, span: float = 0.5, walls: bool = True,
-                 name: str = "channel") -> Case:
+                 ischema: int = 7, name: str = "channel") -> Case:
     """Bump channel: blocks along x joined by coincident faces.
 
     Lower wall y_w(x) = bump*exp(-((x-x_c)/0.25)^2) with x_c at mid-length,
@@ -334,7 +338,7 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     dims = [(int(n) + 1, nj_cells + 1, nk_cells + 1) for n in ni_cells]
     lay = Layout.from_dims(dims)
     phys = Phys(reynz=reynz)
-    scheme = Scheme(ns=1, ilim=ilim, lmax=lmax, eta=eta)
+    scheme = Scheme(ns=1, ilim=ilim, lmax=lmax, eta=eta, ischema=ischema)
     x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
     ntot = int(sum(ni_cells))
     xc = 0.5 * length

@@ -48,6 +48,7 @@ struct cns_ctx {
   int nk_gexec = 0, nk_mref = 0, nk_mreg = 0;  // kernel nodes of each graph
   long long kernels_launched = 0;        // kernels of every fused-step graph launched
   long long mixed_iter = 0;              // mixed iterations since the last reset
+  long long ncyc = 0;                    // fused iterations since the state was bound
   std::string err;
 };
 
@@ -218,9 +219,32 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
   return e;
 }
 
+cudaError_t ensure_dis(cns_ctx* c) {
+  if (c->w.dis) return cudaSuccess;
+  return dev_alloc(c, &c->w.dis, (size_t)(5 * c->lay.ld));
+}
+
+bool jameson(const cns_ctx* c) { return c->sc.ischema <= 4; }
+
+// the Jameson dissipation of the fused iteration: rfve on the first cycle,
+// rfvc, then dissip_jameson into w.dis (atsch_num.f90:448-508, before rbord)
+cudaError_t jameson_dissipation(cns_ctx* c, bool first) {
+  const cns_state_t& s = c->state;
+  const long long ld = c->lay.ld;
+  cudaError_t e = cudaSuccess;
+  if (first) e = launch_ghost_refresh(c->bd, 1, s.v, ld, s.pression, s.ztemp, s.cson, c->st);
+  if (e == cudaSuccess)
+    e = launch_ghost_refresh(c->bd, 2, s.v, ld, s.pression, s.ztemp, s.cson, c->st);
+  if (e == cudaSuccess)
+    e = launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(-1), -1, c->sc.ki2, c->sc.ki4,
+                              s.v, ld, s.pression, s.cson, s.sn, c->w.G, c->w.dis, c->st);
+  return e;
+}
+
 // one pseudo-time iteration on the bound state (atsch_num.f90:245-1134 for
-// ischema = 7, kmf = 1, steady, dt recomputed every iteration)
-cudaError_t enqueue_step(cns_ctx* c) {
+// ischema = 7, kmf = 1, steady, dt recomputed every iteration; ischema <= 4:
+// the Jameson dissipation before rbord, sch_jameson for the residual)
+cudaError_t enqueue_step(cns_ctx* c, bool first) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   const Space all = c->cells.view(-1);
@@ -229,6 +253,7 @@ cudaError_t enqueue_step(cns_ctx* c) {
   if (e == cudaSuccess)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
+  if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
@@ -238,7 +263,13 @@ cudaError_t enqueue_step(cns_ctx* c) {
                     s.vol, s.ztemp, c->st);
     if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
   }
-  if (e == cudaSuccess) e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
+  if (e == cudaSuccess) {
+    if (jameson(c))
+      e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
+                             s.pression, s.tau, s.sn, c->w.dis, c->w.G, s.u, nullptr, c->st);
+    else
+      e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
+  }
   if (e == cudaSuccess)
     e = launch_implicit(c->d_blks, all, c->tiles64.view(-1), c->faces, -1, c->ph, c->sc,
                         !c->sc.ns,
@@ -280,7 +311,7 @@ cudaError_t ensure_mixed(cns_ctx* c) {
 // advances with it and stores corr = R64 - R32 for the regular iterations.
 enum MixedMode { kMixed, kDefectRefresh, kDefectRegular };
 
-cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode) {
+cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
   const cns_state_t& s = c->state;
   Work& w = c->w;
   const long long ld = c->lay.ld;
@@ -291,6 +322,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode) {
   if (e == cudaSuccess)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
+  if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
@@ -320,13 +352,19 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode) {
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, nullptr, w.ur32, nullptr,
                                      c->st);
-    if (e == cudaSuccess && lim)
-      e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
-    if (e == cudaSuccess)
-      e = launch_face_flux(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld, s.pression,
-                           s.tau, s.sn, w.R, w.G, c->st);
-    if (e == cudaSuccess)
-      e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st);
+    if (jameson(c)) {
+      if (e == cudaSuccess)
+        e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
+                               s.pression, s.tau, s.sn, w.dis, w.G, s.u, w.u32, c->st);
+    } else {
+      if (e == cudaSuccess && lim)
+        e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
+      if (e == cudaSuccess)
+        e = launch_face_flux(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
+                             s.pression, s.tau, s.sn, w.R, w.G, c->st);
+      if (e == cudaSuccess)
+        e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st);
+    }
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
   }
@@ -662,10 +700,11 @@ int cns_set_stream(cns_ctx* c, void* stream) {
 int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (!c || !s) return CNS_EINVAL;
   if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
-      s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1))
+      s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1) ||
+      (s->ischema != 1 && s->ischema != 7) || (s->ischema == 1 && s->precision == 2))
     return fail(c, CNS_EINVAL,
                 "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
-                "kdefect >= 1");
+                "kdefect >= 1, ischema in {1,7} (defect correction: Roe only)");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
   c->sc.xk = s->xk;
@@ -677,6 +716,9 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.qfix_dfez = s->qfix_dfez;
   c->sc.precision = s->precision;
   c->sc.kdefect = s->kdefect;
+  c->sc.ischema = s->ischema;
+  c->sc.ki2 = s->ki2;
+  c->sc.ki4 = s->ki4;
   drop_graphs(c);
   return CNS_OK;
 }
@@ -696,6 +738,7 @@ int cns_metric(cns_ctx* c, double* x, double* y, double* z, double* sn,
   CK(cudaStreamSynchronize(c->st));
   c->metric_done = true;
   c->mixed_iter = 0;
+  c->ncyc = 0;
   return CNS_OK;
 }
 
@@ -781,6 +824,38 @@ int cns_sch_roe(cns_ctx* c, int l, double* u, const double* v, const double* tau
   return CNS_OK;
 }
 
+int cns_rfve(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
+  if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
+  CK(launch_ghost_refresh(c->bd, 1, v, c->lay.ld, ps, temp, cson, c->st));
+  return CNS_OK;
+}
+
+int cns_rfvc(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
+  if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
+  CK(launch_ghost_refresh(c->bd, 2, v, c->lay.ld, ps, temp, cson, c->st));
+  return CNS_OK;
+}
+
+int cns_dissip_jameson(cns_ctx* c, int l, const double* v, double* d, const double* sn,
+                       const double* ps, const double* cson) {
+  if (!c || bad_block(c, l) || !v || !d || !sn || !ps || !cson) return CNS_EINVAL;
+  CK(zero_cols(c, d, 5, l));
+  CK(launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, c->sc.ki2,
+                           c->sc.ki4, v, c->lay.ld, ps, cson, sn, c->w.G, d, c->st));
+  return CNS_OK;
+}
+
+int cns_sch_jameson(cns_ctx* c, int l, double* u, const double* v, const double* d,
+                    const double* tau, const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || !u || !v || !d || !sn || !ps || (c->sc.ns && !tau))
+    return CNS_EINVAL;
+  CK(zero_cols(c, u, 5, l));
+  CK(launch_sch_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, c->sc.ns,
+                        c->ph.pinfl, v, c->lay.ld, ps, tau, sn, d, c->w.G, u, nullptr,
+                        c->st));
+  return CNS_OK;
+}
+
 int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,
                double* tau, const double* sn, const double* vol,
                const double* temp) {
@@ -842,6 +917,7 @@ int cns_bind_state(cns_ctx* c, const cns_state_t* s) {
     return CNS_EINVAL;
   c->state = *s;
   c->bound = true;
+  c->ncyc = 0;
   drop_graphs(c);
   return CNS_OK;
 }
@@ -858,43 +934,52 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
     CK(ensure_mixed(c));
     CK(launch_to_float(c->state.sn, c->w.sn32, 9 * c->lay.ld, c->st));
   }
-  // first iteration of a form whose sweeps are not tuned yet: run it eagerly
-  // (the launches the graph would hold), tune the sweep tiles on its data,
-  // then capture with the chosen tiles
-  bool eager = false;
-  if (prec == 0 && !c->tuned64) {
-    CK(enqueue_step(c));
-    CK(tune_sweeps(c, false));
-    drop_graphs(c);
-    eager = true;
-  } else if (prec != 0 && !c->tuned32) {
-    const bool refresh = prec == 2 && (c->mixed_iter % c->sc.kdefect) == 0;
-    CK(enqueue_step_mixed(c, prec == 1 ? kMixed : (refresh ? kDefectRefresh : kDefectRegular)));
-    if (prec == 2) ++c->mixed_iter;
-    CK(tune_sweeps(c, true));
-    drop_graphs(c);
-    eager = true;
+  if (jameson(c)) CK(ensure_dis(c));
+  // first iteration of a form whose sweeps are not tuned yet, and the first
+  // Jameson cycle (rfve before the dissipation): run it eagerly (the
+  // launches the graph would hold), tune the sweep tiles on its data, then
+  // capture the steady-state iteration with the chosen tiles
+  const bool first = c->ncyc == 0;
+  const bool tuned = prec == 0 ? c->tuned64 : c->tuned32;
+  const bool eager = !tuned || (jameson(c) && first);
+  if (eager) {
+    if (prec == 0) {
+      CK(enqueue_step(c, first));
+    } else {
+      const bool refresh = prec == 2 && (c->mixed_iter % c->sc.kdefect) == 0;
+      CK(enqueue_step_mixed(c, prec == 1 ? kMixed : (refresh ? kDefectRefresh : kDefectRegular),
+                            first));
+      if (prec == 2) ++c->mixed_iter;
+    }
+    if (!tuned) {
+      CK(tune_sweeps(c, prec != 0));
+      drop_graphs(c);
+    }
+    ++c->ncyc;
+    --nsteps;
   }
-  if (eager) --nsteps;
+  c->ncyc += nsteps;
   if (prec == 0) {
-    if (!c->gexec) CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c); }));
+    if (!c->gexec)
+      CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c, false); }));
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
     c->kernels_launched += (long long)(nsteps + eager) * c->nk_gexec;
     return CNS_OK;
   }
   if (prec == 1) {
     if (!c->gexec_mref)
-      CK(capture(c, &c->gexec_mref, &c->nk_mref, [&] { return enqueue_step_mixed(c, kMixed); }));
+      CK(capture(c, &c->gexec_mref, &c->nk_mref,
+                 [&] { return enqueue_step_mixed(c, kMixed, false); }));
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec_mref, c->st));
     c->kernels_launched += (long long)(nsteps + eager) * c->nk_mref;
     return CNS_OK;
   }
   if (!c->gexec_mref)
     CK(capture(c, &c->gexec_mref, &c->nk_mref,
-               [&] { return enqueue_step_mixed(c, kDefectRefresh); }));
+               [&] { return enqueue_step_mixed(c, kDefectRefresh, false); }));
   if (!c->gexec_mreg)
     CK(capture(c, &c->gexec_mreg, &c->nk_mreg,
-               [&] { return enqueue_step_mixed(c, kDefectRegular); }));
+               [&] { return enqueue_step_mixed(c, kDefectRegular, false); }));
   if (eager) c->kernels_launched += c->nk_mref;
   for (int s = 0; s < nsteps; ++s) {
     const bool refresh = (c->mixed_iter % c->sc.kdefect) == 0;

@@ -50,6 +50,8 @@ struct Phys {
 struct Scheme {
   int ns, muscl, ilim, kdtl, lmax, qfix_dfez, precision, kdefect;
   double xk, eta, dt1min;
+  int ischema;      // 7 Roe, 1 Jameson
+  double ki2, ki4;  // Jameson dissipation coefficients
 };
 
 // 2.5D tiles of the implicit sweeps: tile t = (block, i0, j0, k0) covers

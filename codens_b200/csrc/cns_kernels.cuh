@@ -71,6 +71,7 @@ struct TileBuf {
 struct Work {
   long long ld = 0;
   double* prim = nullptr;     // primitive velocities u, v, w, [3][ld]
+  double* dis = nullptr;      // Jameson dissipation [5][ld] (allocated on first use)
   double* G = nullptr;        // face fluxes, [3][5][ld]
   double* R = nullptr;        // limiter ratios, [3][5][ld]
   double* coefe = nullptr;    // [3][ld]
@@ -194,6 +195,21 @@ cudaError_t launch_jacobi_25d_t<float>(const Blk*, Tiles, Phys, int, int, long l
                                        const float*, const float*, const float*, const float*,
                                        const float*, const float*, const float*, const float*,
                                        float*, cudaStream_t);
+// the Jameson scheme (cns_jameson.cu): mode 1 rfve, mode 2 rfvc
+cudaError_t launch_ghost_refresh(const Bnd& bd, int mode, double* v, long long ld, double* ps,
+                                 double* temp, double* cson, cudaStream_t st);
+// dissipation of the faces of block l0 (all: -1) into G, summed into d
+cudaError_t launch_dissip_jameson(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
+                                  double ck2, double ck4, const double* v, long long ld,
+                                  const double* ps, const double* cson, const double* sn,
+                                  double* G, double* d, cudaStream_t st);
+// centred fluxes into G, u = 0.5 sum - dis (u32: float copy when given)
+cudaError_t launch_sch_jameson(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
+                               int ns, double pinfl, const double* v, long long ld,
+                               const double* ps, const double* tau, const double* sn,
+                               const double* dis, double* G, double* u, float* u32,
+                               cudaStream_t st);
+
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();

@@ -115,7 +115,9 @@ class CodeNS:
         return abi.Scheme_t(int(s.ns), int(s.muscl), float(s.xk), int(s.ilim), float(s.eta),
                             int(s.kdtl), float(s.dt1min), int(s.lmax),
                             int(getattr(s, "qfix_dfez", qfix_dfez)),
-                            int(getattr(s, "precision", 0)), int(getattr(s, "kdefect", 4)))
+                            int(getattr(s, "precision", 0)), int(getattr(s, "kdefect", 4)),
+                            int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
+                            float(getattr(s, "ki4", 1.0 / 32.0)))
 
     def _check(self, rc: int, where: str):
         if rc:
@@ -198,6 +200,23 @@ class CodeNS:
     def sch_roe(self, l, u, v, tau, sn, ps):
         self._check(self.lib.cns_sch_roe(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
                                          _ptr(ps)), "cns_sch_roe")
+
+    # Jameson scheme (dissip_jameson.f90, sch_jameson.f90, rfve.f90, rfvc.f90)
+    def rfve(self, v, ps, ztemp, cson):
+        self._check(self.lib.cns_rfve(self.ctx, _ptr(v), _ptr(ps), _ptr(ztemp), _ptr(cson)),
+                    "cns_rfve")
+
+    def rfvc(self, v, ps, ztemp, cson):
+        self._check(self.lib.cns_rfvc(self.ctx, _ptr(v), _ptr(ps), _ptr(ztemp), _ptr(cson)),
+                    "cns_rfvc")
+
+    def dissip_jameson(self, l, v, d, sn, ps, cson):
+        self._check(self.lib.cns_dissip_jameson(self.ctx, l, _ptr(v), _ptr(d), _ptr(sn),
+                                                _ptr(ps), _ptr(cson)), "cns_dissip_jameson")
+
+    def sch_jameson(self, l, u, v, d, tau, sn, ps):
+        self._check(self.lib.cns_sch_jameson(self.ctx, l, _ptr(u), _ptr(v), _ptr(d), _ptr(tau),
+                                             _ptr(sn), _ptr(ps)), "cns_sch_jameson")
 
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),

@@ -92,6 +92,10 @@ typedef struct {
                             the FP32 rounding level of the fluxes) */
   int32_t kdefect;       /* precision 2: the FP64 residual and the correction
                             R64 - R32 are refreshed every kdefect iterations */
+  int32_t ischema;       /* 7: Roe (sch_roe, sch_roe_euler); 1: Jameson
+                            (dissip_jameson + sch_jameson, kprec = 0) */
+  double ki2, ki4;       /* Jameson 2nd/4th-difference coefficients (ki2(lm),
+                            ki4(lm); one value for every block) */
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
@@ -128,6 +132,19 @@ int cns_set_stream(cns_ctx *ctx, void *cuda_stream);
 int cns_set_scheme(cns_ctx *ctx, const cns_scheme_t *scheme);
 const char *cns_last_error(cns_ctx *ctx);
 int64_t cns_scratch_bytes(cns_ctx *ctx);
+
+/* Jameson scheme.  rfve.f90 (ghost = interior on every non-coincident
+ * boundary) and rfvc.f90 (coincident ghosts = partner cells) refresh the
+ * ghosts the dissipation reads; dissip_jameson.f90:4-431 zeroes d over the
+ * block(s) and accumulates the scalar dissipation; sch_jameson.f90:4-437
+ * zeroes u, accumulates the centred fluxes (tau used for NS) and finishes
+ * with u = 0.5 u - d on the real cells.  l = 0: every block. */
+int cns_rfve(cns_ctx *ctx, double *v, double *pression, double *ztemp, double *cson);
+int cns_rfvc(cns_ctx *ctx, double *v, double *pression, double *ztemp, double *cson);
+int cns_dissip_jameson(cns_ctx *ctx, int l, const double *v, double *d, const double *sn,
+                       const double *pression, const double *cson);
+int cns_sch_jameson(cns_ctx *ctx, int l, double *u, const double *v, const double *d,
+                    const double *tau, const double *sn, const double *pression);
 
 /* kernels launched by the fused-step graphs of this context so far (the
  * kernel nodes of each captured iteration times its launches) */

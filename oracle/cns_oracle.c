@@ -32,6 +32,8 @@ static struct {
   /* schemanum */
   int ns, muscl, ilim, kdtl, lmax, qfix_dfez;
   double xk, eta, dt1min;
+  int ischema;           /* 1: Jameson (central + scalar dissipation), 7: Roe */
+  double ki2, ki4;       /* Jameson dissipation coefficients ki2(lm), ki4(lm) */
   /* boundary */
   int nbnd;
   int32_t *btype, *bblk, *bface, *bmmb, *bpart;
@@ -121,6 +123,12 @@ void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
   G.kdtl = kdtl;
   G.dt1min = dt1min;
   G.lmax = lmax;
+}
+
+void orc_set_dissipation(int ischema, double ki2, double ki4) {
+  G.ischema = ischema;
+  G.ki2 = ki2;
+  G.ki4 = ki4;
 }
 
 #define DUP(dst, src, n, T)                                   \
@@ -758,6 +766,229 @@ void orc_rbord(double *v, double *ps, double *temp, double *cson) {
     }
   }
   rbvc(v, ps, temp, cson);
+}
+
+static void zero_u(const blk_t *b, double *u);
+
+/* rfve.f90:14-31: every non-coincident boundary, ghost = interior cell */
+void orc_rfve(double *v, double *ps, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] == ORC_BC_RC) continue;
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ni = G.ncin[mb];
+      for (int a = 0; a < 5; ++a) v[a * L + nd] = v[a * L + ni];
+      ps[nd] = ps[ni];
+      temp[nd] = temp[ni];
+      cson[nd] = cson[ni];
+    }
+  }
+}
+
+/* rfvc.f90 (same-process branch): every coincident ghost = the coincident
+ * interior cell of the partner, velocity rotated by the receiver's angle */
+void orc_rfvc(double *v, double *ps, double *temp, double *cson) {
+  const int64_t L = G.ld;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_RC) continue;
+    const int p = G.bpart[bb];
+    const double c = G.bcos[bb], s = G.bsin[bb];
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], nc = G.ncin[G.bmpb[p] + m];
+      v[nd] = v[nc];
+      v[L + nd] = v[L + nc];
+      v[2 * L + nd] = v[2 * L + nc] * c + v[3 * L + nc] * s;
+      v[3 * L + nd] = v[3 * L + nc] * c - v[2 * L + nc] * s;
+      v[4 * L + nd] = v[4 * L + nc];
+      ps[nd] = ps[nc];
+      temp[nd] = temp[nc];
+      cson[nd] = cson[nc];
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Jameson scheme                                                            */
+/* ------------------------------------------------------------------------ */
+
+/* one direction of dissip_jameson.f90:94-316 (i, j) and :318-431 (k) */
+static void jameson_dissip_dir(const blk_t *b, int dir, double *d, const double *v,
+                               const double *sn, const double *ps,
+                               const double *cson, double *snu) {
+  const int64_t L = G.ld, n0 = b->npc, ninc = NINC(b, dir);
+  const double ck2 = G.ki2, ck4 = G.ki4;
+  const int kdir = dir;  /* sn(m, kdir, c): 0-based here */
+  /* sensor on the real cells (:99-110) */
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        snu[m] = fabs(ps[n + ninc] - 2. * ps[n] + ps[n - ninc]) /
+                 (ps[n + ninc] + 2. * ps[n] + ps[n - ninc]);
+      }
+  /* face quantities shared by the three loops */
+#define JAM_FACE()                                                              \
+  double cnds = SN(sn, b, m, kdir, 0) * SN(sn, b, m, kdir, 0) +                  \
+                SN(sn, b, m, kdir, 1) * SN(sn, b, m, kdir, 1) +                  \
+                SN(sn, b, m, kdir, 2) * SN(sn, b, m, kdir, 2);                   \
+  double uu = 0.5 * (v[L + n] / v[n] + v[L + n - ninc] / v[n - ninc]);           \
+  double vv = 0.5 * (v[2 * L + n] / v[n] + v[2 * L + n - ninc] / v[n - ninc]);   \
+  double ww = 0.5 * (v[3 * L + n] / v[n] + v[3 * L + n - ninc] / v[n - ninc]);   \
+  double cc = 0.5 * (cson[n] + cson[n - ninc]);                                  \
+  double rl = fabs(uu * SN(sn, b, m, kdir, 0) + vv * SN(sn, b, m, kdir, 1) +     \
+                   ww * SN(sn, b, m, kdir, 2)) + sqrt(cnds) * cc;
+  const int nd = NDIR(b, dir);
+  int lo[3], hi[3];
+  /* interior faces (:112-150): face index 2..nd-1 along dir */
+  lo[0] = 1; hi[0] = b->ni - 1; lo[1] = 1; hi[1] = b->nj - 1; lo[2] = 1; hi[2] = b->nk - 1;
+  lo[dir] = 2; hi[dir] = nd - 1;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        int64_t n = IC(b, i, j, k), m = n - n0;
+        double eps2 = ck2 * fmax(snu[m - ninc], snu[m]);
+        double eps4 = fmax(0., ck4 - eps2);
+        JAM_FACE()
+        for (int a = 0; a < 5; ++a) {
+          const double *w = v + a * L;
+          double ds = eps2 * rl * (w[n] - w[n - ninc]) -
+                      eps4 * rl * (w[n + ninc] + 3. * (w[n - ninc] - w[n]) - w[n - 2 * ninc]);
+          d[a * L + n] = d[a * L + n] - ds;
+          d[a * L + n - ninc] = d[a * L + n - ninc] + ds;
+        }
+      }
+  /* lower boundary faces (:152-177), then upper ones (:179-204) */
+  for (int side = 0; side < 2; ++side) {
+    lo[0] = 1; hi[0] = b->ni - 1; lo[1] = 1; hi[1] = b->nj - 1; lo[2] = 1; hi[2] = b->nk - 1;
+    lo[dir] = hi[dir] = side == 0 ? 1 : nd;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          double eps2 = side == 0 ? ck2 * snu[m] : ck2 * snu[m - ninc];
+          JAM_FACE()
+          for (int a = 0; a < 5; ++a) {
+            const double *w = v + a * L;
+            double ds = eps2 * rl * (w[n] - w[n - ninc]);
+            if (side == 0)
+              d[a * L + n] = d[a * L + n] - ds;
+            else
+              d[a * L + n - ninc] = d[a * L + n - ninc] + ds;
+          }
+        }
+  }
+#undef JAM_FACE
+}
+
+/* dissip_jameson.f90:4-431 (3-D): d zeroed over the block, then the i, j, k
+ * dissipation fluxes */
+void orc_dissip_jameson(int l, const double *v, double *d, const double *sn,
+                        const double *ps, const double *cson) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, d);
+  double *snu = calloc((size_t)b->nnn, sizeof(double));
+  for (int dir = 0; dir < 3; ++dir) jameson_dissip_dir(b, dir, d, v, sn, ps, cson, snu);
+  free(snu);
+}
+
+/* sch_jameson.f90:85-124: centred cell fluxes (with the cell stresses for
+ * Navier-Stokes) over the whole block, ghosts included */
+static void jameson_cell_flux(const blk_t *b, int ns, const double *v, const double *tau,
+                              const double *ps, double *f) {
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  const double pinfl = G.pinfl;
+  for (int64_t m = 0; m < nnn; ++m) {
+    int64_t n = n0 + m;
+    const double v1 = v[n], v2 = v[L + n], v3 = v[2 * L + n], v4 = v[3 * L + n],
+                 v5 = v[4 * L + n], p = ps[n];
+    double *F = f + 9 * m;
+    if (ns) {
+      const double txx = tau[n], txy = tau[L + n], txz = tau[2 * L + n],
+                   tyy = tau[3 * L + n], tyz = tau[4 * L + n], tzz = tau[5 * L + n],
+                   qx = tau[6 * L + n], qy = tau[7 * L + n], qz = tau[8 * L + n];
+      F[0] = v2 * (v2 / v1) + p - pinfl - txx;
+      F[1] = v3 * (v2 / v1) - txy;
+      F[2] = v4 * (v2 / v1) - txz;
+      F[3] = v3 * (v3 / v1) + p - pinfl - tyy;
+      F[4] = v4 * (v3 / v1) - tyz;
+      F[5] = v4 * (v4 / v1) + p - pinfl - tzz;
+      F[6] = ((v5 + p - pinfl - txx) * v2 - txy * v3 - txz * v4) / v1 - qx;
+      F[7] = ((v5 + p - pinfl - tyy) * v3 - txy * v2 - tyz * v4) / v1 - qy;
+      F[8] = ((v5 + p - pinfl - tzz) * v4 - txz * v2 - tyz * v3) / v1 - qz;
+    } else {
+      F[0] = v2 * (v2 / v1) + p - pinfl;
+      F[1] = v3 * (v2 / v1);
+      F[2] = v4 * (v2 / v1);
+      F[3] = v3 * (v3 / v1) + p - pinfl;
+      F[4] = v4 * (v3 / v1);
+      F[5] = v4 * (v4 / v1) + p - pinfl;
+      F[6] = (v5 + p - pinfl) * v2 / v1;
+      F[7] = (v5 + p - pinfl) * v3 / v1;
+      F[8] = (v5 + p - pinfl) * v4 / v1;
+    }
+  }
+}
+
+/* the five projections of one face from the (summed or doubled) cell
+ * momenta and fluxes (sch_jameson.f90:141-155); F order: xx xy xz yy yz zz
+ * ex ey ez */
+static void jameson_proj(const double m3[3], const double F[9], double s1, double s2,
+                         double s3, double si[5]) {
+  si[0] = m3[0] * s1 + m3[1] * s2 + m3[2] * s3;
+  si[1] = F[0] * s1 + F[1] * s2 + F[2] * s3;
+  si[2] = F[1] * s1 + F[3] * s2 + F[4] * s3;
+  si[3] = F[2] * s1 + F[4] * s2 + F[5] * s3;
+  si[4] = F[6] * s1 + F[7] * s2 + F[8] * s3;
+}
+
+/* sch_jameson.f90:4-437 (ityprk = 0, 3-D) */
+void orc_sch_jameson(int l, double *u, const double *v, const double *d,
+                     const double *tau, const double *sn, const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  zero_u(b, u);
+  double *f = malloc(sizeof(double) * 9 * (size_t)b->nnn);
+  jameson_cell_flux(b, G.ns, v, tau, ps, f);
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    const int kdir = dir, nd = NDIR(b, dir);
+    int lo[3], hi[3];
+    /* interior faces (:135-168), lower (:170-196), upper (:198-224) */
+    for (int pass = 0; pass < 3; ++pass) {
+      lo[0] = 1; hi[0] = b->ni - 1; lo[1] = 1; hi[1] = b->nj - 1; lo[2] = 1; hi[2] = b->nk - 1;
+      if (pass == 0) { lo[dir] = 2; hi[dir] = nd - 1; }
+      else lo[dir] = hi[dir] = pass == 1 ? 1 : nd;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            int64_t n = IC(b, i, j, k), m = n - n0;
+            const double s1 = SN(sn, b, m, kdir, 0), s2 = SN(sn, b, m, kdir, 1),
+                         s3 = SN(sn, b, m, kdir, 2);
+            double m3[3], F[9], si[5];
+            if (pass == 0) {
+              for (int a = 0; a < 3; ++a) m3[a] = v[(a + 1) * L + n] + v[(a + 1) * L + n - ninc];
+              for (int q = 0; q < 9; ++q) F[q] = f[9 * m + q] + f[9 * (m - ninc) + q];
+            } else {
+              const int64_t c = pass == 1 ? n - ninc : n;  /* the ghost cell */
+              for (int a = 0; a < 3; ++a) m3[a] = 2 * v[(a + 1) * L + c];
+              for (int q = 0; q < 9; ++q) F[q] = 2 * f[9 * (c - n0) + q];
+            }
+            jameson_proj(m3, F, s1, s2, s3, si);
+            for (int a = 0; a < 5; ++a) {
+              if (pass != 2) u[a * L + n] = u[a * L + n] - si[a];
+              if (pass != 1) u[a * L + n - ninc] = u[a * L + n - ninc] + si[a];
+            }
+          }
+    }
+  }
+  free(f);
+  /* normalisation and artificial dissipation (:421-437) */
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        for (int a = 0; a < 5; ++a) u[a * L + n] = 0.5 * u[a * L + n] - d[a * L + n];
+      }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1604,6 +1835,34 @@ void orc_rscpsv(const double *u0, const double *v, const double *dt,
 /* ------------------------------------------------------------------------ */
 /* one iteration                                                             */
 /* ------------------------------------------------------------------------ */
+
+/* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
+ * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
+ * (before rbord: the physical ghosts are the previous iteration's), rbord,
+ * zvisqc, sch_jameson, the implicit phase.  dis holds the dissipation (the
+ * reference reuses d for it; implimf then overwrites d with the increment). */
+int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
+                     const double *sn, const double *vol, double *ps, double *temp,
+                     double *cson, double *mu, double *mut, double *tau, int first_cycle) {
+  for (int l = 1; l <= G.nblk; ++l) orc_zpres(l, v, ps, temp, cson);
+  if (G.ns)
+    for (int l = 1; l <= G.nblk; ++l) orc_zvismo(l, mu, temp);
+  for (int l = 1; l <= G.nblk; ++l) orc_chronos(l, mu, mut, v, dt, sn, vol, cson);
+  if (G.kdtl == 0) orc_chrono_global(dt);
+  if (first_cycle) orc_rfve(v, ps, temp, cson);
+  orc_rfvc(v, ps, temp, cson);
+  for (int l = 1; l <= G.nblk; ++l) orc_dissip_jameson(l, v, dis, sn, ps, cson);
+  orc_rbord(v, ps, temp, cson);
+  if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+  for (int l = 1; l <= G.nblk; ++l) orc_sch_jameson(l, u, v, dis, tau, sn, ps);
+  for (int l = 1; l <= G.nblk; ++l) {
+    if (G.ns)
+      orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
+    else
+      orc_implimf_eu(l, u, dt, v, d, sn, vol, ps, cson, G.lmax);
+  }
+  return 0;
+}
 
 /* atsch_num.f90:245-1134 for ischema=7 (Roe), kmf=1 (implicit), steady */
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,

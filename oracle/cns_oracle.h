@@ -101,6 +101,18 @@ void orc_rscpsv(const double *u0, const double *v, const double *dt,
 /* one pseudo-time iteration over all blocks (atsch_num.f90:245-1134 for the
  * ischema=7, kmf=1 Roe/implicit path); work holds ld*(9+5) doubles for
  * ps,temp,cson,mu,mut,dt,...; returns 0 */
+/* Jameson scheme: ischema 1, ki2/ki4 of every block (schemanum) */
+void orc_set_dissipation(int ischema, double ki2, double ki4);
+void orc_rfve(double *v, double *ps, double *temp, double *cson);
+void orc_rfvc(double *v, double *ps, double *temp, double *cson);
+void orc_dissip_jameson(int l, const double *v, double *d, const double *sn,
+                        const double *ps, const double *cson);
+void orc_sch_jameson(int l, double *u, const double *v, const double *d,
+                     const double *tau, const double *sn, const double *ps);
+int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
+                     const double *sn, const double *vol, double *ps, double *temp,
+                     double *cson, double *mu, double *mut, double *tau, int first_cycle);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

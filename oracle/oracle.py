@@ -55,6 +55,13 @@ def lib():
         L.orc_rscpsv.argtypes = [_d, _d, _d, _d]
         L.orc_step.argtypes = [_d] * 12 + [C.c_int]
         L.orc_step.restype = C.c_int
+        L.orc_set_dissipation.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_rfve.argtypes = [_d] * 4
+        L.orc_rfvc.argtypes = [_d] * 4
+        L.orc_dissip_jameson.argtypes = [C.c_int] + [_d] * 5
+        L.orc_sch_jameson.argtypes = [C.c_int] + [_d] * 6
+        L.orc_step_jameson.argtypes = [_d] * 13 + [C.c_int]
+        L.orc_step_jameson.restype = C.c_int
         _lib = L
     return _lib
 
@@ -73,6 +80,7 @@ class OracleState:
         self.v = np.ascontiguousarray(case.v0.reshape(-1)).copy()
         self.u = np.zeros(5 * ld)
         self.d = np.zeros(5 * ld)
+        self.dis = np.zeros(5 * ld)   # Jameson dissipation
         self.dt = np.zeros(ld)
         self.ps = np.zeros(ld)
         self.temp = np.zeros(ld)
@@ -108,6 +116,10 @@ class Oracle:
     def set_scheme(self, s):
         lib().orc_set_scheme(s.ns, s.muscl, s.xk, s.ilim, s.eta, s.kdtl,
                              s.dt1min, s.lmax, int(getattr(s, "qfix_dfez", 0)))
+        lib().orc_set_dissipation(int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
+                                  float(getattr(s, "ki4", 1.0 / 32.0)))
+        self.jameson = int(getattr(s, "ischema", 7)) <= 4
+        self.ncyc = 0
 
     def metric(self, st: OracleState):
         lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)
@@ -119,6 +131,13 @@ class Oracle:
         return [o[:n] for o in out]
 
     def step(self, st: OracleState, compute_dt: bool = True):
+        """one iteration: atsch_num's Roe or Jameson sequence by ischema
+        (the Jameson one extrapolates the physical ghosts on the first cycle)"""
+        self.ncyc += 1
+        if self.jameson:
+            return lib().orc_step_jameson(st.v, st.u, st.d, st.dis, st.dt, st.sn, st.vol,
+                                          st.ps, st.temp, st.cson, st.mu, st.mut, st.tau,
+                                          int(self.ncyc == 1))
         return lib().orc_step(st.v, st.u, st.d, st.dt, st.sn, st.vol, st.ps,
                               st.temp, st.cson, st.mu, st.mut, st.tau,
                               int(compute_dt))
