@@ -22,6 +22,8 @@ struct cns_ctx {
   Phys ph{};
   Scheme sc{};
   SpaceBuf cells, faces[3], lines[3];
+  SpaceBuf cells_ext;  // i 0..ni, j 0..nj, k 0..nk (met_roe2o's zeroed range)
+  double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
   bool tuned64 = false, tuned32 = false;
   float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
@@ -552,6 +554,9 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   if (e != cudaSuccess) return cleanup_fail(e, "blocks");
   e = build_space(c, c->cells, [](const Blk& B, int x[3]) {
     x[0] = B.ni - 1; x[1] = B.nj - 1; x[2] = B.nk - 1; });
+  if (e == cudaSuccess)
+    e = build_space(c, c->cells_ext, [](const Blk& B, int x[3]) {
+      x[0] = B.ni + 1; x[1] = B.nj + 1; x[2] = B.nk + 1; });
   if (e == cudaSuccess) e = build_tiles(c, c->tiles64, 32, 8, 8);
   if (e == cudaSuccess) e = build_tiles(c, c->tiles32, 32, 8, 8);
   if (e == cudaSuccess) e = init_jacobi_25d();
@@ -854,6 +859,69 @@ int cns_sch_jameson(cns_ctx* c, int l, double* u, const double* v, const double*
                         c->ph.pinfl, v, c->lay.ld, ps, tau, sn, d, c->w.G, u, nullptr,
                         c->st));
   return CNS_OK;
+}
+
+int cns_set_turbulence(cns_ctx* c, double alfak, double alfae, double sigma, double epsroe) {
+  if (!c || !(alfak != 0.) || !(alfae != 0.) || !(sigma != 0.)) return CNS_EINVAL;
+  c->alfak = alfak;
+  c->alfae = alfae;
+  c->sigma = sigma;
+  c->epsroe = epsroe;
+  return CNS_OK;
+}
+
+// the flat range indc(1,1,1)..indc(ni-1,nj-1,nk-1) of block l (the whole
+// span for l = 0 is the union: first block's start to last block's end)
+static void fludc_range(cns_ctx* c, int l, long long& n0, long long& n1) {
+  const Blk& F = c->lay.blks[l == 0 ? 0 : l - 1];
+  const Blk& L = c->lay.blks[l == 0 ? c->lay.blks.size() - 1 : l - 1];
+  n0 = F.npc + 1 + F.nid + F.nijd;
+  n1 = L.npc + (L.ni - 1) + (long long)(L.nj - 1) * L.nid + (long long)(L.nk - 1) * L.nijd;
+}
+
+int cns_met_fludc(cns_ctx* c, int l, const double* mu, const double* mut, double* fd5x,
+                  double* fd5y, double* fd5z, double* fd6x, double* fd6y, double* fd6z) {
+  if (!c || bad_block(c, l) || !mu || !mut || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y ||
+      !fd6z)
+    return CNS_EINVAL;
+  double* const fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  const int l0 = l == 0 ? 1 : l, l1 = l == 0 ? (int)c->lay.blks.size() : l;
+  for (int b = l0; b <= l1; ++b) {
+    long long n0, n1;
+    fludc_range(c, b, n0, n1);
+    CK(launch_fludc(n0, n1, mu, mut, fd, c->alfak, c->alfae, c->st));
+  }
+  return CNS_OK;
+}
+
+int cns_met_fludcsa(cns_ctx* c, int l, const double* s, const double* mu, double* fd5x,
+                    double* fd5y, double* fd5z, double* fd6x, double* fd6y, double* fd6z) {
+  if (!c || bad_block(c, l) || !s || !mu || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y || !fd6z)
+    return CNS_EINVAL;
+  double* const fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  const int l0 = l == 0 ? 1 : l, l1 = l == 0 ? (int)c->lay.blks.size() : l;
+  for (int b = l0; b <= l1; ++b) {
+    long long n0, n1;
+    fludc_range(c, b, n0, n1);
+    CK(launch_fludcsa(n0, n1, s + 5 * c->lay.ld, mu, fd, c->sigma, c->st));
+  }
+  return CNS_OK;
+}
+
+static int met_roe2o_common(cns_ctx* c, int l, const double* t, double* d, const double* sn,
+                            int harten) {
+  if (!c || bad_block(c, l) || !t || !d || !sn) return CNS_EINVAL;
+  CK(launch_roe2o(c->d_blks, c->faces, c->cells_ext.view(l - 1), l - 1, harten, c->epsroe,
+                  c->ph.gam, c->ph.gam1, t, c->lay.ld, sn, c->w.G, d, c->st));
+  return CNS_OK;
+}
+
+int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
+  return met_roe2o_common(c, l, t, d, sn, 0);
+}
+
+int cns_met_roe2oh(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
+  return met_roe2o_common(c, l, t, d, sn, 1);
 }
 
 int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,

@@ -210,6 +210,19 @@ cudaError_t launch_sch_jameson(const Blk* blks, const SpaceBuf* faces, Space cel
                                const double* dis, double* G, double* u, float* u32,
                                cudaStream_t st);
 
+// turbulence-transport terms (cns_turb.cu): met_fludc / met_fludcsa over the
+// flat range [n0, n1]; fd = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z}
+cudaError_t launch_fludc(long long n0, long long n1, const double* mu, const double* mut,
+                         double* const fd[6], double alfak, double alfae, cudaStream_t st);
+cudaError_t launch_fludcsa(long long n0, long long n1, const double* s6, const double* mu,
+                           double* const fd[6], double sigma, cudaStream_t st);
+// met_roe2o / met_roe2oh (harten) of block l0 (all: -1): t, d are (ld, 7);
+// cells_ext covers i 0..ni, j 0..nj, k 0..nk
+cudaError_t launch_roe2o(const Blk* blks, const SpaceBuf* faces, Space cells_ext, int l0,
+                         int harten, double epsroe, double gam, double gam1, const double* t,
+                         long long ld, const double* sn, double* G, double* d,
+                         cudaStream_t st);
+
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();

@@ -218,6 +218,24 @@ class CodeNS:
         self._check(self.lib.cns_sch_jameson(self.ctx, l, _ptr(u), _ptr(v), _ptr(d), _ptr(tau),
                                              _ptr(sn), _ptr(ps)), "cns_sch_jameson")
 
+    # turbulence-transport terms (met_fludc, met_fludcsa, met_roe2o, met_roe2oh)
+    def set_turbulence(self, alfak=1.0, alfae=1.3, sigma=2.0 / 3.0, epsroe=0.0):
+        self._check(self.lib.cns_set_turbulence(self.ctx, alfak, alfae, sigma, epsroe),
+                    "cns_set_turbulence")
+
+    def met_fludc(self, l, mu, mut, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
+        self._check(self.lib.cns_met_fludc(self.ctx, l, *(_ptr(a) for a in (
+            mu, mut, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z))), "cns_met_fludc")
+
+    def met_fludcsa(self, l, s, mu, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
+        self._check(self.lib.cns_met_fludcsa(self.ctx, l, *(_ptr(a) for a in (
+            s, mu, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z))), "cns_met_fludcsa")
+
+    def met_roe2o(self, l, t, d, sn, harten=False):
+        f = self.lib.cns_met_roe2oh if harten else self.lib.cns_met_roe2o
+        self._check(f(self.ctx, l, _ptr(t), _ptr(d), _ptr(sn)),
+                    "cns_met_roe2oh" if harten else "cns_met_roe2o")
+
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
                                         _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")

@@ -146,6 +146,24 @@ int cns_dissip_jameson(cns_ctx *ctx, int l, const double *v, double *d, const do
 int cns_sch_jameson(cns_ctx *ctx, int l, double *u, const double *v, const double *d,
                     const double *tau, const double *sn, const double *pression);
 
+/* Turbulence-transport terms on the mean-flow path.  cns_set_turbulence
+ * sets the modeleturb / schemanum constants these routines read (alfak,
+ * alfae: k-epsilon diffusion numbers; sigma: Spalart-Allmaras; epsroe:
+ * Harten's parameter; defaults 1, 1.3, 2/3, 0).  t, s and d are the
+ * reference's (ld, 7) arrays; fd* are per cell (ip12).
+ *   cns_met_fludc   met_fludc.f90:4-87   fd5* *= mu + mut/alfak, fd6* *= mu + mut/alfae
+ *   cns_met_fludcsa met_fludcsa.f90:4-106 fd5* *= (mu + s(:,6))/sigma, fd6* = 0
+ *   cns_met_roe2o   met_roe2o.f90:4-297  TVD Roe dissipation of t(:,6:7) -> d(:,6:7)
+ *   cns_met_roe2oh  met_roe2oh.f90        the same with Harten's entropy fix
+ * l = 0: every block. */
+int cns_set_turbulence(cns_ctx *ctx, double alfak, double alfae, double sigma, double epsroe);
+int cns_met_fludc(cns_ctx *ctx, int l, const double *mu, const double *mut, double *fd5x,
+                  double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
+int cns_met_fludcsa(cns_ctx *ctx, int l, const double *s, const double *mu, double *fd5x,
+                    double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
+int cns_met_roe2o(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
+int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
+
 /* kernels launched by the fused-step graphs of this context so far (the
  * kernel nodes of each captured iteration times its launches) */
 int64_t cns_kernels_launched(cns_ctx *ctx);

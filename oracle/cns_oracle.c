@@ -1836,6 +1836,148 @@ void orc_rscpsv(const double *u0, const double *v, const double *dt,
 /* one iteration                                                             */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* turbulence transport terms on the mean-flow path                          */
+/* ------------------------------------------------------------------------ */
+
+/* the flat range indc(i1,j1,k1)..indc(i2m1,j2m1,k2m1) the fludc routines
+ * sweep (ghost cells inside the range included) */
+static void flat_real_range(const blk_t *b, int64_t *n0, int64_t *n1) {
+  *n0 = IC(b, 1, 1, 1);
+  *n1 = IC(b, b->ni - 1, b->nj - 1, b->nk - 1);
+}
+
+/* met_fludc.f90:72-85 (alfak, alfae: modeleturb) */
+void orc_met_fludc(int l, const double *mu, const double *mut, double *fd5x, double *fd5y,
+                   double *fd5z, double *fd6x, double *fd6y, double *fd6z, double alfak,
+                   double alfae) {
+  const blk_t *b = &G.b[l - 1];
+  int64_t n0, n1;
+  flat_real_range(b, &n0, &n1);
+  for (int64_t n = n0; n <= n1; ++n) {
+    fd5x[n] = (mu[n] + mut[n] / alfak) * fd5x[n];
+    fd5y[n] = (mu[n] + mut[n] / alfak) * fd5y[n];
+    fd5z[n] = (mu[n] + mut[n] / alfak) * fd5z[n];
+  }
+  for (int64_t n = n0; n <= n1; ++n) {
+    fd6x[n] = (mu[n] + mut[n] / alfae) * fd6x[n];
+    fd6y[n] = (mu[n] + mut[n] / alfae) * fd6y[n];
+    fd6z[n] = (mu[n] + mut[n] / alfae) * fd6z[n];
+  }
+}
+
+/* met_fludcsa.f90:92-104 (sigma: modeleturb); s is (ld, 7) */
+void orc_met_fludcsa(int l, const double *s, const double *mu, double *fd5x, double *fd5y,
+                     double *fd5z, double *fd6x, double *fd6y, double *fd6z, double sigma) {
+  const blk_t *b = &G.b[l - 1];
+  int64_t n0, n1;
+  flat_real_range(b, &n0, &n1);
+  const double sigma1 = 1. / sigma;
+  for (int64_t n = n0; n <= n1; ++n) {
+    const double smutot = sigma1 * (mu[n] + s[5 * G.ld + n]);
+    fd5x[n] = smutot * fd5x[n];
+    fd5y[n] = smutot * fd5y[n];
+    fd5z[n] = smutot * fd5z[n];
+    fd6x[n] = 0.;
+    fd6y[n] = 0.;
+    fd6z[n] = 0.;
+  }
+}
+
+/* met_roe2o.f90:288-296: minmod-type limiter */
+static double amimd(double a, double b) {
+  const double s = copysign(1.0, a);
+  return s * fmax(0., fmin(fabs(a), b * s));
+}
+static double fi1(double x, double y, double z) { return amimd(x, amimd(y, z)); }
+/* met_roe2oh.f90:318-323: Harten's entropy-fixed |a| */
+static double psi_h(double aa, double eps) {
+  return 0.5 * (1. + copysign(1.0, fabs(aa) - eps)) * fabs(aa) +
+         0.25 * (1. - copysign(1.0, fabs(aa) - eps)) * (aa * aa + eps * eps) / eps;
+}
+
+/* met_roe2o.f90:26-286 / met_roe2oh.f90 (harten): TVD Roe dissipation of the
+ * two transport variables t(:,6:7) into d(:,6:7); directions k, j, i; every
+ * face of a direction (boundary faces included) in one ascending loop, the
+ * slope differences extended by one face past each end */
+void orc_met_roe2o(int l, const double *t, double *d, const double *sn, int harten,
+                   double epsroe) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  /* zero d(:,6:7) over i 0..ni, j 0..nj, k 0..nk (:53-62) */
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 0; j <= b->nj; ++j)
+      for (int i = 0; i <= b->ni; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        d[5 * L + n] = 0.;
+        d[6 * L + n] = 0.;
+      }
+  double *del6 = calloc((size_t)b->nnn, sizeof(double));
+  double *del7 = calloc((size_t)b->nnn, sizeof(double));
+  static const int order[3] = {2, 1, 0};
+  for (int o = 0; o < 3; ++o) {
+    const int dir = order[o];
+    const int64_t ninc = NINC(b, dir);
+    const int nd = NDIR(b, dir);
+    /* slope differences on the faces 1..nd (the i direction also fills the
+     * j = nj row, unused), then the extension at faces 0 and nd+1 */
+    int lo[3] = {1, 1, 1}, hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+    lo[dir] = 1;
+    hi[dir] = nd;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int64_t n = IC(b, i, j, k), m = n - n0;
+          del6[m] = t[5 * L + n] - t[5 * L + n - ninc];
+          del7[m] = t[6 * L + n] - t[6 * L + n - ninc];
+        }
+    for (int side = 0; side < 2; ++side) {
+      int lo2[3] = {1, 1, 1}, hi2[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+      lo2[dir] = hi2[dir] = side == 0 ? 0 : nd + 1;
+      const int64_t is = side == 0 ? 1 : -1;
+      for (int k = lo2[2]; k <= hi2[2]; ++k)
+        for (int j = lo2[1]; j <= hi2[1]; ++j)
+          for (int i = lo2[0]; i <= hi2[0]; ++i) {
+            const int64_t m = IC(b, i, j, k) - n0;
+            del6[m] = del6[m + is * ninc];
+            del7[m] = del7[m + is * ninc];
+          }
+    }
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int64_t n = IC(b, i, j, k), m = n - n0, m1 = m - ninc, m2 = m + ninc,
+                        n1 = n - ninc;
+          const double rro = 2 * t[n], rro1 = 2 * t[n1];
+          const double u = t[L + n] / rro + t[L + n1] / rro1;
+          const double v = t[2 * L + n] / rro + t[2 * L + n1] / rro1;
+          const double w = t[3 * L + n] / rro + t[3 * L + n1] / rro1;
+          const double s1 = SN(sn, b, m, dir, 0), s2 = SN(sn, b, m, dir, 1),
+                       s3 = SN(sn, b, m, dir, 2);
+          double coef;
+          if (harten) {
+            const double etot = t[4 * L + n] / rro + t[4 * L + n1] / rro1;
+            const double q2 = 0.5 * (u * u + v * v + w * w);
+            const double c = sqrt(G.gam * G.gam1 * (etot - q2));
+            const double cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+            const double rlam = (u * s1 + v * s2 + w * s3) / cnds;
+            coef = 0.5 * psi_h(rlam, epsroe * c) * cnds;
+          } else {
+            const double rlam = u * s1 + v * s2 + w * s3;
+            coef = 0.5 * fabs(rlam);
+          }
+          double dd = coef * (del6[m] - fi1(del6[m1], del6[m], del6[m2]));
+          d[5 * L + n] = d[5 * L + n] - dd;
+          d[5 * L + n1] = d[5 * L + n1] + dd;
+          dd = coef * (del7[m] - fi1(del7[m1], del7[m], del7[m2]));
+          d[6 * L + n] = d[6 * L + n] - dd;
+          d[6 * L + n1] = d[6 * L + n1] + dd;
+        }
+  }
+  free(del6);
+  free(del7);
+}
+
 /* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
  * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
  * (before rbord: the physical ghosts are the previous iteration's), rbord,

@@ -113,6 +113,16 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
                      const double *sn, const double *vol, double *ps, double *temp,
                      double *cson, double *mu, double *mut, double *tau, int first_cycle);
 
+/* turbulence transport terms: met_fludc, met_fludcsa, met_roe2o(h); t, s, d
+ * are (ld, 7) */
+void orc_met_fludc(int l, const double *mu, const double *mut, double *fd5x, double *fd5y,
+                   double *fd5z, double *fd6x, double *fd6y, double *fd6z, double alfak,
+                   double alfae);
+void orc_met_fludcsa(int l, const double *s, const double *mu, double *fd5x, double *fd5y,
+                     double *fd5z, double *fd6x, double *fd6y, double *fd6z, double sigma);
+void orc_met_roe2o(int l, const double *t, double *d, const double *sn, int harten,
+                   double epsroe);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

@@ -62,6 +62,9 @@ def lib():
         L.orc_sch_jameson.argtypes = [C.c_int] + [_d] * 6
         L.orc_step_jameson.argtypes = [_d] * 13 + [C.c_int]
         L.orc_step_jameson.restype = C.c_int
+        L.orc_met_fludc.argtypes = [C.c_int] + [_d] * 8 + [C.c_double] * 2
+        L.orc_met_fludcsa.argtypes = [C.c_int] + [_d] * 8 + [C.c_double]
+        L.orc_met_roe2o.argtypes = [C.c_int, _d, _d, _d, C.c_int, C.c_double]
         _lib = L
     return _lib
 

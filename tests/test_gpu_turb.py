@@ -1,0 +1,120 @@
+"""GPU parity of the turbulence-transport terms on the mean-flow path
+(met_fludc, met_fludcsa, met_roe2o, met_roe2oh) against the oracle, bit for
+bit, on every block at once and block by block."""
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+from oracle.oracle import lib as orc_lib
+
+from ._helpers import assert_equal_bits, oracle_prepared
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "box": lambda: cases.box_case((9, 6, 5), seed=8, noise=0.02, skew=0.02, ns=True),
+    "channel": lambda: cases.channel_case([9, 6, 7], 8, 5, seed=13, reynz=1.0e3),
+}
+ALFAK, ALFAE, SIGMA, EPSROE = 1.0, 1.3, 2.0 / 3.0, 0.1
+
+
+def _gpu(case):
+    from codens_b200.solver import CodeNS
+    s = CodeNS(case)
+    s.metric()
+    s.set_turbulence(ALFAK, ALFAE, SIGMA, EPSROE)
+    s.sync()
+    return s
+
+
+def _t(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+def _transport_state(case, st, seed=31):
+    """(ld, 7) state: the mean flow with its ghost cells filled by the
+    boundary conditions, and two seeded transport variables"""
+    ld = case.layout.ld
+    L = orc_lib()
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_zpres(l, st.v, st.ps, st.temp, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    t = np.zeros((7, ld))
+    t[:5] = st.v.reshape(5, ld)
+    r = cases.splitmix64_uniform(seed, 2 * ld).reshape(2, ld)
+    t[5] = t[0] * (1e-3 + 1e-3 * r[0])
+    t[6] = t[0] * (0.5 + r[1])
+    return t
+
+
+def _fields(case, seed):
+    ld = case.layout.ld
+    r = cases.splitmix64_uniform(seed, 8 * ld).reshape(8, ld)
+    mu = 1e-3 * (1.0 + r[0])
+    mut = 1e-2 * r[1]
+    fd = r[2:8] - 0.5
+    return mu, mut, fd
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_fludc_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    mu, mut, fd = _fields(case, 41)
+    L = orc_lib()
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        fo = fd.copy()
+        blocks = range(1, case.layout.nblk + 1) if l == 0 else [l]
+        for b in blocks:
+            L.orc_met_fludc(b, mu, mut, *[fo[q] for q in range(6)], ALFAK, ALFAE)
+        fg = [_t(torch, fd[q]) for q in range(6)]
+        s.met_fludc(l, _t(torch, mu), _t(torch, mut), *fg)
+        s.sync()
+        for q in range(6):
+            assert_equal_bits(fg[q].cpu().numpy(), fo[q], f"fd[{q}] (l={l})")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_fludcsa_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    mu, _, fd = _fields(case, 43)
+    t = _transport_state(case, st)
+    L = orc_lib()
+    fo = fd.copy()
+    for b in range(1, case.layout.nblk + 1):
+        L.orc_met_fludcsa(b, t.reshape(-1), mu, *[fo[q] for q in range(6)], SIGMA)
+    fg = [_t(torch, fd[q]) for q in range(6)]
+    s.met_fludcsa(0, _t(torch, t.reshape(-1)), _t(torch, mu), *fg)
+    s.sync()
+    for q in range(6):
+        assert_equal_bits(fg[q].cpu().numpy(), fo[q], f"fd[{q}]")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("harten", [False, True])
+def test_met_roe2o_parity(cuda, name, harten):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    ld = case.layout.ld
+    L = orc_lib()
+    tg = _t(torch, t.reshape(-1))
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        d_o = np.full((7, ld), 3.0)
+        blocks = range(1, case.layout.nblk + 1) if l == 0 else [l]
+        for b in blocks:
+            L.orc_met_roe2o(b, t.reshape(-1), d_o.reshape(-1), st.sn, int(harten), EPSROE)
+        dg = _t(torch, np.full(7 * ld, 3.0))
+        s.met_roe2o(l, tg, dg, s.sn, harten=harten)
+        s.sync()
+        assert_equal_bits(dg.cpu().numpy().reshape(7, ld), d_o, f"d (l={l})")
+    s.close()

@@ -189,3 +189,33 @@ def test_jameson_box_converges():
         l2.append(orc.norms(u0, st)[1, 0])
     assert np.all(np.isfinite(l2))
     assert l2[-1] < 0.5 * l2[0]
+
+
+def _transport_state(case, seed=31):
+    """(ld, 7) state: the case's mean flow and two seeded transport variables"""
+    ld = case.layout.ld
+    t = np.zeros((7, ld))
+    t[:5] = case.v0.reshape(5, ld)
+    r = cases.splitmix64_uniform(seed, 2 * ld).reshape(2, ld)
+    t[5] = t[0] * (1e-3 + 1e-3 * r[0])
+    t[6] = t[0] * (0.5 + r[1])
+    return t
+
+
+@pytest.mark.parametrize("harten", [0, 1])
+def test_roe2o_conservative_and_tvd(harten):
+    """every face adds -dd to one cell and +dd to the other (ghosts
+    included), so d(:,6:7) sums to zero; a uniform transport field gives no
+    dissipation"""
+    case = cases.box_case((9, 6, 5), seed=8, noise=0.02, skew=0.02, ns=True)
+    orc, st = oracle_prepared(case)
+    L = lib()
+    t = _transport_state(case)
+    d = np.zeros((7, case.layout.ld))
+    L.orc_met_roe2o(1, t.reshape(-1), d.reshape(-1), st.sn, harten, 0.1)
+    assert np.isfinite(d[5:]).all() and np.abs(d[5:]).max() > 0
+    assert np.abs(d[5:].sum(axis=1)).max() < 1e-13 * np.abs(d[5:]).max() * d.shape[1]
+    t[5] = 1e-3
+    t[6] = 0.7
+    L.orc_met_roe2o(1, t.reshape(-1), d.reshape(-1), st.sn, harten, 0.1)
+    assert np.abs(d[5:]).max() == 0.0
