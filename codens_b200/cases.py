@@ -299,6 +299,28 @@ def batch_case(ncase: int = 64, side=(16, 96), seed: int = 4,
                           alpha=alphas.tolist()))
 
 
+def batch_member(batch: Case, ib: int) -> Case:
+    """Case ib of a batch as a case of its own: the same block dimensions,
+    coordinates, state and boundary conditions in a one-block layout."""
+    import copy
+    b = batch.layout.blocks[ib]
+    lay = Layout.from_dims([(b.ni, b.nj, b.nk)])
+    sl = slice(b.npc, b.npc + b.nnn)
+    x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
+    x[:b.nnn], y[:b.nnn], z[:b.nnn] = batch.x[sl], batch.y[sl], batch.z[sl]
+    v0 = np.zeros((5, lay.ld))
+    v0[:, :b.nnn] = batch.v0[:, sl]
+    own = [q for q, bd in enumerate(batch.boundaries) if bd.block == ib]
+    remap = {q: r for r, q in enumerate(own)}
+    bnd = [Boundary(0, batch.boundaries[q].face, batch.boundaries[q].kind,
+                    partner=remap.get(batch.boundaries[q].partner, -1),
+                    tper=batch.boundaries[q].tper, values=batch.boundaries[q].values)
+           for q in own]
+    return Case(f"{batch.name}[{ib}]", lay, copy.deepcopy(batch.phys),
+                copy.deepcopy(batch.scheme), bnd, x, y, z, v0,
+                meta=dict(batch=batch.name, member=ib))
+
+
 def channel_dims(nblk: int = 8, seed: int = 2, lo: int = 48, hi: int = 128,
                  target=(3.5e6, 4.5e6)):
     """Block sizes of the bump channel: n_i per block and a shared n_j, n_k,

@@ -190,10 +190,12 @@ void drop_graphs(cns_ctx* c) {
 int check_status(cns_ctx* c) {
   CK(cudaMemcpyAsync(c->h_status, c->w.status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  if (*c->h_status & 1) {
+  const int bits = *c->h_status;
+  if (bits) {
     *c->h_status = 0;
     CK(cudaMemsetAsync(c->w.status, 0, sizeof(int), c->st));
-    return fail(c, CNS_ETEMP, "non-positive temperature (zvismo)");
+    if (bits & 1) return fail(c, CNS_ETEMP, "non-positive temperature (zvismo)");
+    return fail(c, CNS_EDT, "global time step below dt1min (chrono)");
   }
   return CNS_OK;
 }
@@ -228,6 +230,19 @@ cudaError_t ensure_dis(cns_ctx* c) {
 
 bool jameson(const cns_ctx* c) { return c->sc.ischema <= 4; }
 
+cudaError_t ensure_dtpart(cns_ctx* c) {
+  if (c->w.dtpart) return cudaSuccess;
+  return dev_alloc(c, &c->w.dtpart, (size_t)(c->cells.ntiles + 1));
+}
+
+// the global time step of kdtl = 0 after the local ones (chrono.f90:113-151)
+cudaError_t global_dt(cns_ctx* c) {
+  if (c->sc.kdtl != 0) return cudaSuccess;
+  return launch_dt_global(c->d_blks, c->cells.view(-1), c->lay.ncells, c->sc.dt1min,
+                          c->state.dt, c->w.dtpart, c->w.dtpart + c->cells.ntiles, c->w.status,
+                          c->st);
+}
+
 // the Jameson dissipation of the fused iteration: rfve on the first cycle,
 // rfvc, then dissip_jameson into w.dis (atsch_num.f90:448-508, before rbord)
 cudaError_t jameson_dissipation(cns_ctx* c, bool first) {
@@ -255,6 +270,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first) {
   if (e == cudaSuccess)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
+  if (e == cudaSuccess) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
@@ -324,6 +340,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
   if (e == cudaSuccess)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
+  if (e == cudaSuccess) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
@@ -777,6 +794,14 @@ int cns_zvismo(cns_ctx* c, int l, double* mu, const double* v, const double* tem
   return check_status(c);
 }
 
+int cns_chrono_global(cns_ctx* c, double* dt) {
+  if (!c || !dt) return CNS_EINVAL;
+  CK(ensure_dtpart(c));
+  CK(launch_dt_global(c->d_blks, c->cells.view(-1), c->lay.ncells, c->sc.dt1min, dt,
+                      c->w.dtpart, c->w.dtpart + c->cells.ntiles, c->w.status, c->st));
+  return check_status(c);
+}
+
 int cns_chronos(cns_ctx* c, int l, const double* mu, const double* mut,
                 const double* v, double* dt, const double* sn, const double* vol,
                 const double* cson) {
@@ -994,8 +1019,7 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return CNS_EINVAL;
   if (!c->bound || !c->metric_done)
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
-  if (c->sc.kdtl == 0)
-    return fail(c, CNS_EINVAL, "the fused step runs with local time steps (kdtl != 0)");
+  if (c->sc.kdtl == 0) CK(ensure_dtpart(c));
   if (nsteps == 0) return CNS_OK;
   const int prec = c->sc.precision;
   if (prec != 0 && !c->w.mixed_ready) {

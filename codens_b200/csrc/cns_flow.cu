@@ -11,6 +11,8 @@
 // order in which the reference's loops add them (interior faces in ascending
 // order, then the lower and the upper boundary face), which keeps the FP64
 // result bit-identical.
+#include <math_constants.h>
+
 #include "cns_kernels.cuh"
 #include "cns_hot.cuh"
 
@@ -639,6 +641,52 @@ cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, 
   return cudaGetLastError();
 }
 
+// chrono.f90:113-151 (kdtl = 0): the smallest local time step over the real
+// cells of every block, min(dt1min, it) everywhere, and the reference's stop
+// when it is below dt1min as status bit 2.  Min is exact in any order.
+__global__ void __launch_bounds__(kTile) k_dt_partials(const Blk* __restrict__ blks, Space sp,
+                                                       const double* __restrict__ dt,
+                                                       double* __restrict__ part) {
+  int b, i, j, k;
+  double x = CUDART_INF;
+  if (space_elem(sp, threadIdx.x, b, i, j, k)) x = dt[cell_index(blks[b], i, j, k)];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+  __shared__ double wm[kTile / 32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = wm[0];
+    for (int q = 1; q < kTile / 32; ++q) m = fmin(m, wm[q]);
+    part[blockIdx.x] = m;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dt_reduce(const double* __restrict__ part, int n,
+                                                  double dt1min, double* __restrict__ out,
+                                                  int* status) {
+  double x = CUDART_INF;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) x = fmin(x, part[q]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+  __shared__ double wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = wm[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) m = fmin(m, wm[q]);
+    const double dtmin = fmin(dt1min, m);
+    if (dtmin < dt1min) atomicOr(status, 2);
+    *out = dtmin;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dt_set(long long ncells, const double* __restrict__ v,
+                                               double* __restrict__ dt) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < ncells) dt[n] = *v;
+}
+
 cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
                            const double* mu, const double* mut, const double* v,
                            long long ld, double* dt, const double* sn,
@@ -646,6 +694,16 @@ cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
   if (sp.ntiles > 0)
     k_chronos<<<grid_of(sp), kTile, 0, st>>>(blks, sp, ph, sc, mu, mut, v, ld, dt,
                                              sn, vol, cson);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt_global(const Blk* blks, Space cells, long long ncells, double dt1min,
+                             double* dt, double* part, double* scalar, int* status,
+                             cudaStream_t st) {
+  if (cells.ntiles == 0) return cudaSuccess;
+  k_dt_partials<<<grid_of(cells), kTile, 0, st>>>(blks, cells, dt, part);
+  k_dt_reduce<<<1, 256, 0, st>>>(part, cells.ntiles, dt1min, scalar, status);
+  k_dt_set<<<(int)((ncells + 255) / 256), 256, 0, st>>>(ncells, scalar, dt);
   return cudaGetLastError();
 }
 

@@ -72,6 +72,7 @@ struct Work {
   long long ld = 0;
   double* prim = nullptr;     // primitive velocities u, v, w, [3][ld]
   double* dis = nullptr;      // Jameson dissipation [5][ld] (allocated on first use)
+  double* dtpart = nullptr;   // global time step: per-tile minima + the result
   double* G = nullptr;        // face fluxes, [3][5][ld]
   double* R = nullptr;        // limiter ratios, [3][5][ld]
   double* coefe = nullptr;    // [3][ld]
@@ -195,6 +196,12 @@ cudaError_t launch_jacobi_25d_t<float>(const Blk*, Tiles, Phys, int, int, long l
                                        const float*, const float*, const float*, const float*,
                                        const float*, const float*, const float*, const float*,
                                        float*, cudaStream_t);
+// chrono.f90:113-151 (kdtl = 0): dt = min(dt1min, min over real cells) on
+// [0, ncells); status bit 2 when below dt1min; part: one double per cell tile
+cudaError_t launch_dt_global(const Blk* blks, Space cells, long long ncells, double dt1min,
+                             double* dt, double* part, double* scalar, int* status,
+                             cudaStream_t st);
+
 // the Jameson scheme (cns_jameson.cu): mode 1 rfve, mode 2 rfvc
 cudaError_t launch_ghost_refresh(const Bnd& bd, int mode, double* v, long long ld, double* ps,
                                  double* temp, double* cson, cudaStream_t st);

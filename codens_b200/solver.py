@@ -40,7 +40,7 @@ def _ptr(t):
 
 
 class CodeNS:
-    def __init__(self, case: Case, device: int | None = None):
+    def __init__(self, case: Case, device: int | None = None, stream=None):
         import torch
 
         if not torch.cuda.is_available():
@@ -82,7 +82,9 @@ class CodeNS:
         if rc:
             raise abi.CnsError(rc, "cns_create")
         self.ctx = ctx
-        self.stream = torch.cuda.Stream()
+        # every call of this solver is ordered on one stream (its own unless
+        # the caller passes one, e.g. to serialise several solvers)
+        self.stream = stream if stream is not None else torch.cuda.Stream()
         self._check(self.lib.cns_set_stream(ctx, C.c_void_p(self.stream.cuda_stream)),
                     "cns_set_stream")
         f64 = dict(dtype=torch.float64, device=self.dev)
@@ -200,6 +202,10 @@ class CodeNS:
     def sch_roe(self, l, u, v, tau, sn, ps):
         self._check(self.lib.cns_sch_roe(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
                                          _ptr(ps)), "cns_sch_roe")
+
+    def chrono_global(self, dt):
+        """chrono.f90:113-151: the global time step (kdtl = 0)"""
+        self._check(self.lib.cns_chrono_global(self.ctx, _ptr(dt)), "cns_chrono_global")
 
     # Jameson scheme (dissip_jameson.f90, sch_jameson.f90, rfve.f90, rfvc.f90)
     def rfve(self, v, ps, ztemp, cson):

@@ -133,6 +133,12 @@ int cns_set_scheme(cns_ctx *ctx, const cns_scheme_t *scheme);
 const char *cns_last_error(cns_ctx *ctx);
 int64_t cns_scratch_bytes(cns_ctx *ctx);
 
+/* chrono.f90:113-151, the global time step (kdtl = 0) after the per-block
+ * cns_chronos calls: dt = min(dt1min, smallest real-cell dt) on every cell;
+ * CNS_EDT when that is below dt1min (the reference stops).  The fused step
+ * applies it itself when kdtl = 0. */
+int cns_chrono_global(cns_ctx *ctx, double *dt);
+
 /* Jameson scheme.  rfve.f90 (ghost = interior on every non-coincident
  * boundary) and rfvc.f90 (coincident ghosts = partner cells) refresh the
  * ghosts the dissipation reads; dissip_jameson.f90:4-431 zeroes d over the

@@ -219,3 +219,20 @@ def test_roe2o_conservative_and_tvd(harten):
     t[6] = 0.7
     L.orc_met_roe2o(1, t.reshape(-1), d.reshape(-1), st.sn, harten, 0.1)
     assert np.abs(d[5:]).max() == 0.0
+
+
+def test_batch_is_its_members():
+    """a batch of independent boxes steps exactly like each box alone (the
+    oracle's per-block routines), the property the batched launch keeps"""
+    bt = cases.batch_case(ncase=3, side=(3, 7), seed=14, qfix_dfez=1)
+    orc, st = oracle_prepared(bt)
+    for _ in range(3):
+        orc.step(st)
+    vb = st.v.reshape(5, -1)
+    for ib in range(3):
+        m = cases.batch_member(bt, ib)
+        om, sm = oracle_prepared(m)
+        for _ in range(3):
+            om.step(sm)
+        assert np.array_equal(vb[:, bt.layout.blocks[ib].real_cells()],
+                              sm.v.reshape(5, -1)[:, m.layout.blocks[0].real_cells()])
