@@ -61,7 +61,8 @@ EXPORTS = [
     "cns_atsch_num_launch", "cns_last_norms", "cns_atsch_num_step_host",
     "cns_sch_roe_euler_noalloc", "cns_sweep_tiles", "cns_set_sweep_tiles",
     "cns_rfve", "cns_rfvc", "cns_dissip_jameson", "cns_sch_jameson",
-    "cns_chrono_global", "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
+    "cns_chrono_global", "cns_adjoint_prepare", "cns_adjoint_rt", "cns_adjoint_lt",
+    "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
 ]
 
 _lib = None
@@ -112,6 +113,9 @@ def load(build_if_missing: bool = True):
     L.cns_sch_jameson.argtypes = [vp, C.c_int] + [vp] * 6
     L.cns_set_turbulence.argtypes = [vp] + [c_f64] * 4
     L.cns_chrono_global.argtypes = [vp, vp]
+    L.cns_adjoint_prepare.argtypes = [vp]
+    L.cns_adjoint_rt.argtypes = [vp] * 4
+    L.cns_adjoint_lt.argtypes = [vp] * 3
     L.cns_met_fludc.argtypes = [vp, C.c_int] + [vp] * 8
     L.cns_met_fludcsa.argtypes = [vp, C.c_int] + [vp] * 8
     L.cns_met_roe2o.argtypes = [vp, C.c_int] + [vp] * 3

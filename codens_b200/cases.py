@@ -342,7 +342,8 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
                  reynz: float = 1.0e4, noise: float = 0.01, lmax: int = 10,
                  eta: float = 5.0, ilim: int = 1, bump: float = 0.1,
                  length: float = 8.0, span: float = 0.5, walls: bool = True,
-                 ischema: int = 7, name: str = "channel") -> Case:
+                 ischema: int = 7, alpha: float = 0.0, wall=None,
+                 name: str = "channel") -> Case:
     """Bump channel: blocks along x joined by coincident faces.
 
     Lower wall y_w(x) = bump*exp(-((x-x_c)/0.25)^2) with x_c at mid-length,
@@ -353,6 +354,9 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     pressure), para on both walls, periodic k on every block.  walls=False
     makes j periodic too (a duct with inlet and outlet only; with bump=0 its
     steady state is the uniform flow set by the inlet and outlet values).
+    alpha: inlet flow angle in the x-y plane (degrees); wall: the lower-wall
+    height of every node column along x (sum(ni_cells) + 1 values) instead
+    of the bump formula.
     """
     if ni_cells is None:
         ni_cells, nj_cells, nk_cells, seed = channel_dims(seed=seed)
@@ -374,7 +378,10 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
         X = length * (i0 + I - 1) / ntot
         eta_ = (J - 1) / (b.nj - 1)
         s = 0.5 * (1.0 + np.tanh(beta * (2.0 * eta_ - 1.0)) / math.tanh(beta))
-        yw = bump * np.exp(-((X - xc) / 0.25) ** 2)
+        if wall is None:
+            yw = bump * np.exp(-((X - xc) / 0.25) ** 2)
+        else:
+            yw = np.asarray(wall, dtype=float)[i0 + I - 1]
         Y = yw + (1.0 - yw) * s
         Z = span * (K - 1) / (b.nk - 1)
         idx = b.ic(I, J, K).ravel()
@@ -392,7 +399,8 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
         bnd.append(Boundary(ib, "i2", BC_RC, partner=a + 1))
         bnd.append(Boundary(ib + 1, "i1", BC_RC, partner=a))
     p_inf = st[4]
-    bnd.append(Boundary(0, "i1", BC_IDD, values=(1.0, 1.0, 1.0, 0.0, 0.0)))
+    bnd.append(Boundary(0, "i1", BC_IDD, values=(1.0, 1.0, math.cos(math.radians(alpha)),
+                                                 math.sin(math.radians(alpha)), 0.0)))
     bnd.append(Boundary(nblk - 1, "i2", BC_PRD, values=(p_inf,)))
     for ib in range(nblk):
         if walls:
@@ -406,5 +414,6 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
         bnd.append(Boundary(ib, "k1", BC_RC, partner=a + 1))
         bnd.append(Boundary(ib, "k2", BC_RC, partner=a))
     return Case(name, lay, phys, scheme, bnd, x, y, z, v0,
-                meta=dict(mach=mach, seed=seed, reynz=reynz,
-                          ni=list(ni_cells), nj=nj_cells, nk=nk_cells))
+                meta=dict(mach=mach, seed=seed, reynz=reynz, alpha=alpha,
+                          ni=list(ni_cells), nj=nj_cells, nk=nk_cells, length=length,
+                          span=span, bump=bump, beta=beta))

@@ -24,6 +24,9 @@ struct cns_ctx {
   SpaceBuf cells, faces[3], lines[3];
   SpaceBuf cells_ext;  // i 0..ni, j 0..nj, k 0..nk (met_roe2o's zeroed range)
   double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
+  double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
+  double* adj_N = nullptr;   // adjoint: linearised sweep blocks [35][5][ld]
+  double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
   bool tuned64 = false, tuned32 = false;
   float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
@@ -947,6 +950,60 @@ int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* s
 
 int cns_met_roe2oh(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
   return met_roe2o_common(c, l, t, d, sn, 1);
+}
+
+int cns_adjoint_prepare(cns_ctx* c) {
+  if (!c) return CNS_EINVAL;
+  if (!c->bound || !c->metric_done)
+    return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
+  if (c->sc.ns || jameson(c) || c->sc.muscl < 0 || c->sc.muscl > 1 || c->sc.ilim != 0)
+    return fail(c, CNS_EINVAL, "the adjoint covers the Euler Roe scheme (ns = 0, ischema 7, "
+                               "first order or unlimited MUSCL)");
+  if (!c->sc.qfix_dfez)
+    return fail(c, CNS_EINVAL, "the adjoint needs qfix_dfez = 1 (the reference Euler implicit "
+                               "phase is not linear in the increment)");
+  const cns_state_t& s = c->state;
+  const long long ld = c->lay.ld;
+  if (!c->adj_J) CK(dev_alloc(c, &c->adj_J, (size_t)(3 * 27 * 5) * ld, false));
+  if (!c->adj_N) CK(dev_alloc(c, &c->adj_N, (size_t)(35 * 5) * ld, false));
+  if (!c->adj_z) CK(dev_alloc(c, &c->adj_z, (size_t)(2 * 5) * ld));
+  const Space all = c->cells.view(-1);
+  // the iteration's inputs at the bound (converged) state: thermodynamics,
+  // time steps, ghost cells, velocities, implicit coefficients
+  CK(launch_zpres(c->d_blks, all, c->ph, 0, s.v, ld, s.pression, s.ztemp, s.cson, s.mu,
+                  c->w.status, c->st));
+  CK(launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn, s.vol,
+                    s.cson, c->st));
+  CK(global_dt(c));
+  CK(launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
+                  c->d_idd_ents, c->d_idd_masks, c->st));
+  CK(launch_prim(0, c->lay.ncells, s.v, ld, c->w.prim, c->st));
+  CK(launch_implicit_coefficients(c->d_blks, all, c->faces, -1, c->ph, 1, s.dt, s.v, c->w.prim,
+                                  s.mu, s.mut, s.sn, s.vol, s.cson, c->w, nullptr, nullptr,
+                                  c->st));
+  CK(launch_face_jac(c->d_blks, c->faces, c->ph, c->sc, s.v, s.pression, ld, s.sn, c->adj_J,
+                     c->st));
+  CK(launch_sweep_jac(c->d_blks, all, c->ph, c->sc.qfix_dfez, ld, s.v, s.pression, s.sn,
+                      c->w.coefe, c->adj_N, c->st));
+  return check_status(c);
+}
+
+int cns_adjoint_rt(cns_ctx* c, const double* lam, double* wbar, double* sbar) {
+  if (!c || !lam || !wbar) return CNS_EINVAL;
+  if (!c->adj_J) return fail(c, CNS_ENOTREADY, "run cns_adjoint_prepare first");
+  CK(launch_adj_gather(c->d_blks, c->cells_ext.view(-1), c->adj_J, lam, c->lay.ld, wbar, sbar,
+                       c->st));
+  return CNS_OK;
+}
+
+int cns_adjoint_lt(cns_ctx* c, const double* y, double* out) {
+  if (!c || !y || !out) return CNS_EINVAL;
+  if (!c->adj_N) return fail(c, CNS_ENOTREADY, "run cns_adjoint_prepare first");
+  const long long ld = c->lay.ld;
+  CK(launch_precond_t(c->d_blks, c->cells.view(-1), ld, c->adj_N, c->w.coefdiag,
+                      c->sc.lmax > 0 ? c->sc.lmax : 1, y, c->adj_z, c->adj_z + 5 * ld, out,
+                      c->st));
+  return CNS_OK;
 }
 
 int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,

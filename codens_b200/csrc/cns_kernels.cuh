@@ -230,6 +230,26 @@ cudaError_t launch_roe2o(const Blk* blks, const SpaceBuf* faces, Space cells_ext
                          long long ld, const double* sn, double* G, double* d,
                          cudaStream_t st);
 
+// discrete adjoint of the FP64 Euler Roe iteration (cns_adjoint.cu)
+// face-flux Jacobians J[3 dirs][27 seeds][5][ld] (4 stencil cells x (W, p),
+// face normal) at the state v, ps
+cudaError_t launch_face_jac(const Blk* blks, const SpaceBuf* faces, Phys ph, Scheme sc,
+                            const double* v, const double* ps, long long ld, const double* sn,
+                            double* J, cudaStream_t st);
+// wbar[6][ld] = (A^T lambda) per cell of i 0..ni, j 0..nj, k 0..nk (W, p
+// parts), sbar[3][3][ld] = lambda^T du/dS per face
+cudaError_t launch_adj_gather(const Blk* blks, Space cells_ext, const double* J,
+                              const double* lam, long long ld, double* wbar, double* sbar,
+                              cudaStream_t st);
+// linearised Jacobi update blocks N[35 seeds][5][ld] (Euler, implimf_eu)
+cudaError_t launch_sweep_jac(const Blk* blks, Space cells, Phys ph, int qfix, long long ld,
+                             const double* v, const double* ps, const double* sn,
+                             const double* coefe, double* N, cudaStream_t st);
+// out = L^T y over lmax sweeps (z0, z1: scratch [5][ld])
+cudaError_t launch_precond_t(const Blk* blks, Space cells, long long ld, const double* N,
+                             const double* cd, int lmax, const double* y, double* z0,
+                             double* z1, double* out, cudaStream_t st);
+
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();

@@ -207,6 +207,18 @@ class CodeNS:
         """chrono.f90:113-151: the global time step (kdtl = 0)"""
         self._check(self.lib.cns_chrono_global(self.ctx, _ptr(dt)), "cns_chrono_global")
 
+    # discrete adjoint of the Euler Roe iteration (see codens_b200/adjoint.py)
+    def adjoint_prepare(self):
+        self._check(self.lib.cns_adjoint_prepare(self.ctx), "cns_adjoint_prepare")
+
+    def adjoint_rt(self, lam, wbar, sbar=None):
+        self._check(self.lib.cns_adjoint_rt(self.ctx, _ptr(lam), _ptr(wbar),
+                                            None if sbar is None else _ptr(sbar)),
+                    "cns_adjoint_rt")
+
+    def adjoint_lt(self, y, out):
+        self._check(self.lib.cns_adjoint_lt(self.ctx, _ptr(y), _ptr(out)), "cns_adjoint_lt")
+
     # Jameson scheme (dissip_jameson.f90, sch_jameson.f90, rfve.f90, rfvc.f90)
     def rfve(self, v, ps, ztemp, cson):
         self._check(self.lib.cns_rfve(self.ctx, _ptr(v), _ptr(ps), _ptr(ztemp), _ptr(cson)),

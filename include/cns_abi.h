@@ -170,6 +170,26 @@ int cns_met_fludcsa(cns_ctx *ctx, int l, const double *s, const double *mu, doub
 int cns_met_roe2o(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
 int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
 
+/* Discrete adjoint of the FP64 Euler Roe iteration (sch_roe_euler with
+ * unlimited MUSCL + implimf_eu with qfix_dfez = 1) at the bound state, for a
+ * caller that solves A^T lambda = dJ/dW (no counterpart in the reference).
+ *   cns_adjoint_prepare  recomputes the iteration's inputs at the state
+ *                        (zpres, chronos, rbord, coefficients) and stores
+ *                        the exact face-flux Jacobians and the linearised
+ *                        Jacobi-update blocks (forward-mode dual numbers);
+ *   cns_adjoint_rt       wbar (6 x ld) = A^T lam for every cell of i 0..ni,
+ *                        j 0..nj, k 0..nk, split into the conserved-variable
+ *                        part (rows 0-4) and the pressure part (row 5; the
+ *                        residual reads the pressure array), and, when sbar
+ *                        is given, sbar (3 dirs x 3 x ld) = lam^T du/dS per
+ *                        face (at the face's cell index); lam is zero on
+ *                        ghost cells;
+ *   cns_adjoint_lt       out = L^T y, L the primal's implicit phase
+ *                        linearised at d = 0 (lmax sweeps). */
+int cns_adjoint_prepare(cns_ctx *ctx);
+int cns_adjoint_rt(cns_ctx *ctx, const double *lam, double *wbar, double *sbar);
+int cns_adjoint_lt(cns_ctx *ctx, const double *y, double *out);
+
 /* kernels launched by the fused-step graphs of this context so far (the
  * kernel nodes of each captured iteration times its launches) */
 int64_t cns_kernels_launched(cns_ctx *ctx);
