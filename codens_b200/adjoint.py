@@ -469,32 +469,55 @@ class WallForceGradient:
         return float(J.detach()), keep, gwall, gm
 
     def solve_adjoint(self, g):
+        """lambda += L^T (g - A^T lambda) until the relative residual is below
+        adj_tol; one iteration (A^T lambda in the library, the boundary-map
+        chain in torch, L^T in the library) is captured into a CUDA graph on
+        the solver's stream and replayed"""
         torch = self.torch
         s = self.s
         ld = self.maps.ld
         lam = torch.zeros(5 * ld, dtype=torch.float64, device=s.dev)
         wbar = torch.zeros(6 * ld, dtype=torch.float64, device=s.dev)
-        y = torch.zeros(5 * ld, dtype=torch.float64, device=s.dev)
+        r = torch.zeros(5 * ld, dtype=torch.float64, device=s.dev)
         dl = torch.zeros(5 * ld, dtype=torch.float64, device=s.dev)
-        gflat = g.reshape(-1)
+        gflat = g.reshape(-1).contiguous()
         gn = float(gflat.norm())
+
+        def step():
+            s.adjoint_rt(lam, wbar)
+            r.copy_(gflat - self._chain(wbar).reshape(-1))
+            s.adjoint_lt(r, dl)
+            lam.add_(dl)
+
         hist = []
         it = 0
-        with torch.cuda.stream(s.stream):
-            while it < self.adj_max:
-                s.adjoint_rt(lam, wbar)
-                r = gflat - self._chain(wbar).reshape(-1)
-                y.copy_(r)
-                s.adjoint_lt(y, dl)
-                lam += dl
-                it += 1
-                if it % self.check == 0:
-                    rn = float(r.norm()) / max(gn, 1e-300)
-                    hist.append(rn)
-                    if not math.isfinite(rn):
-                        raise RuntimeError("adjoint iteration diverged")
-                    if rn < self.adj_tol:
-                        break
+        graph = None
+        if self.adj_max > 0:
+            with torch.cuda.stream(s.stream):
+                step()
+            it = 1
+            s.sync()
+            try:
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, stream=s.stream):
+                    step()  # recorded, not run
+            except Exception:
+                graph = None
+        while it < self.adj_max:
+            with torch.cuda.stream(s.stream):
+                if graph is not None:
+                    graph.replay()
+                else:
+                    step()
+            it += 1
+            if it % self.check == 0:
+                s.sync()
+                rn = float(r.norm()) / max(gn, 1e-300)
+                hist.append(rn)
+                if not math.isfinite(rn):
+                    raise RuntimeError("adjoint iteration diverged")
+                if rn < self.adj_tol:
+                    break
         s.sync()
         self.adj_iters = it
         self.adj_hist = hist
@@ -585,10 +608,13 @@ def make_function():
     class WallForce(torch.autograd.Function):
         @staticmethod
         def forward(ctx, mach, alpha, wall, design):
-            g = WallForceGradient(design, float(mach), float(alpha),
-                                  wall.detach().cpu().numpy())
-            J, gm, ga, gw = g.gradient()
-            g.close()
+            # the local maps are differentiated with autograd inside (forward
+            # runs with gradients disabled)
+            with torch.enable_grad():
+                g = WallForceGradient(design, float(mach), float(alpha),
+                                      wall.detach().cpu().numpy())
+                J, gm, ga, gw = g.gradient()
+                g.close()
             ctx.save_for_backward(torch.tensor([gm, ga], dtype=torch.float64), gw.cpu())
             return torch.tensor(J, dtype=torch.float64)
 

@@ -1,0 +1,101 @@
+"""The discrete adjoint of the steady Euler Roe solution (bump channel,
+first-order reconstruction): gradients of the wall pressure force with
+respect to the inflow Mach number, the inflow angle and lower-wall node
+heights against central finite differences of the converged primal, and the
+transposed residual product against a finite-difference directional
+derivative of the library's residual."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# gradients: finite differences with step 1e-6 of primal solves converged to
+# L2 < 1e-14 agree with the adjoint to ~1e-9 relative; the bound leaves room
+# for the finite-difference truncation on small components
+GRAD_TOL = 1e-6
+
+
+def _design():
+    from codens_b200 import adjoint
+    return adjoint.Design(ni=16, nj=8, nk=2, mach=0.5, alpha=1.0, bump=0.1)
+
+
+def test_transposed_residual_product(cuda):
+    """<A^T lam, dW> = <lam, (u(W + e dW) - u(W - e dW)) / 2e> on random
+    vectors, u the library's residual with its boundary conditions"""
+    torch = cuda
+    from codens_b200 import adjoint
+    d = _design()
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-10, adj_max=0)
+    s, M = g.s, g.maps
+    ld = M.ld
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    lam = torch.zeros(5, ld, dtype=torch.float64, device="cuda")
+    dW = torch.zeros(5, ld, dtype=torch.float64, device="cuda")
+    lam[:, M.real] = torch.rand(5, len(M.real), generator=gen, device="cuda",
+                                dtype=torch.float64) - 0.5
+    dW[:, M.real] = (torch.rand(5, len(M.real), generator=gen, device="cuda",
+                                dtype=torch.float64) - 0.5) * g.W[:, M.real].abs()
+    wbar = torch.zeros(6 * ld, dtype=torch.float64, device="cuda")
+    s.adjoint_rt(lam.reshape(-1), wbar)
+    s.sync()
+    lhs = float((g._chain(wbar) * dW).sum())
+
+    def residual(W):
+        s.v.copy_(W.reshape(-1))
+        s.zpres(0, s.v, s.pression, s.ztemp, s.cson)
+        s.rbord(s.v, s.pression, s.ztemp, s.cson)
+        s.sch_roe_euler(0, s.u, s.v, s.sn, s.pression)
+        s.sync()
+        return s.u.reshape(5, ld).clone()
+
+    eps = 1e-6
+    up = residual(g.W + eps * dW)
+    um = residual(g.W - eps * dW)
+    rhs = float((lam * (up - um)).sum()) / (2 * eps)
+    assert abs(lhs - rhs) <= 1e-6 * abs(rhs), (lhs, rhs)
+    g.close()
+
+
+def test_wall_force_gradient_matches_finite_differences(cuda):
+    from codens_b200 import adjoint
+    d = _design()
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-14, adj_tol=1e-12)
+    J, gm, ga, gw = g.gradient()
+    gw = gw.cpu().numpy()
+    g.close()
+
+    def Jat(mach=d.mach, alpha=d.alpha, wall=None):
+        return adjoint.wall_force(d, mach, alpha, d.wall() if wall is None else wall,
+                                  tol=1e-14)
+
+    eps = 1e-6
+    fd_m = (Jat(mach=d.mach + eps) - Jat(mach=d.mach - eps)) / (2 * eps)
+    assert abs(gm - fd_m) <= GRAD_TOL * abs(fd_m), (gm, fd_m)
+    fd_a = (Jat(alpha=d.alpha + eps) - Jat(alpha=d.alpha - eps)) / (2 * eps)
+    assert abs(ga - fd_a) <= 1e-3 * abs(fd_a) + 1e-9, (ga, fd_a)
+    w0 = d.wall()
+    for i in (7, 8, 9):
+        wp, wm = w0.copy(), w0.copy()
+        wp[i] += eps
+        wm[i] -= eps
+        fd = (Jat(wall=wp) - Jat(wall=wm)) / (2 * eps)
+        assert abs(gw[i] - fd) <= GRAD_TOL * max(abs(fd), 1e-3), (i, gw[i], fd)
+
+
+def test_autograd_function(cuda):
+    torch = cuda
+    from codens_b200 import adjoint
+    d = _design()
+    WallForce = adjoint.make_function()
+    mach = torch.tensor(d.mach, dtype=torch.float64, requires_grad=True)
+    alpha = torch.tensor(d.alpha, dtype=torch.float64, requires_grad=True)
+    wall = torch.tensor(d.wall(), dtype=torch.float64, requires_grad=True)
+    J = WallForce.apply(mach, alpha, wall, d)
+    J.backward()
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-13, adj_tol=1e-12)
+    J2, gm, ga, gw = g.gradient()
+    g.close()
+    assert abs(float(J) - J2) <= 1e-12 * abs(J2)
+    assert abs(float(mach.grad) - gm) <= 1e-8 * abs(gm)
+    np.testing.assert_allclose(wall.grad.numpy(), gw.cpu().numpy(), rtol=1e-8, atol=1e-12)
