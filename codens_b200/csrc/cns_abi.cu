@@ -944,6 +944,31 @@ static int met_roe2o_common(cns_ctx* c, int l, const double* t, double* d, const
   return CNS_OK;
 }
 
+int cns_met_samut(cns_ctx* c, int l, const double* v, const double* mu, double* mut) {
+  if (!c || bad_block(c, l) || !v || !mu || !mut) return CNS_EINVAL;
+  CK(launch_samut(c->d_blks, c->cells.view(l - 1), v + 5 * c->lay.ld, mu, mut, c->st));
+  return CNS_OK;
+}
+
+int cns_sch_turb(cns_ctx* c, int l, double* u, const double* v, const double* d,
+                 const double* fd5x, const double* fd5y, const double* fd5z,
+                 const double* fd6x, const double* fd6y, const double* fd6z, const double* ts6,
+                 const double* ts7, const double* sn, const double* vol) {
+  if (!c || bad_block(c, l) || !u || !v || !d || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y ||
+      !fd6z || !ts6 || !ts7 || !sn || !vol)
+    return CNS_EINVAL;
+  const long long ld = c->lay.ld;
+  // sch_turb.f90:59-66 zeroes u(:,6:7) over the block(s)
+  long long n0, n1;
+  block_range(c, l, n0, n1);
+  CK(cudaMemsetAsync(u + 5 * ld + n0, 0, sizeof(double) * (n1 - n0), c->st));
+  CK(cudaMemsetAsync(u + 6 * ld + n0, 0, sizeof(double) * (n1 - n0), c->st));
+  const double* fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  CK(launch_sch_turb(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, v, ld, fd, ts6, ts7, d,
+                     sn, vol, c->w.G, u, c->st));
+  return CNS_OK;
+}
+
 int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
   return met_roe2o_common(c, l, t, d, sn, 0);
 }

@@ -250,6 +250,15 @@ cudaError_t launch_precond_t(const Blk* blks, Space cells, long long ld, const d
                              const double* cd, int lmax, const double* y, double* z0,
                              double* z1, double* out, cudaStream_t st);
 
+// met_samut (real cells of block l0's space) and sch_turb (u, v, d: (ld, 7))
+cudaError_t launch_samut(const Blk* blks, Space cells, const double* v6, const double* mu,
+                         double* mut, cudaStream_t st);
+cudaError_t launch_sch_turb(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
+                            const double* v, long long ld, const double* const fd[6],
+                            const double* ts6, const double* ts7, const double* d,
+                            const double* sn, const double* vol, double* G, double* u,
+                            cudaStream_t st);
+
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();

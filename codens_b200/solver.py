@@ -254,6 +254,14 @@ class CodeNS:
         self._check(f(self.ctx, l, _ptr(t), _ptr(d), _ptr(sn)),
                     "cns_met_roe2oh" if harten else "cns_met_roe2o")
 
+    def met_samut(self, l, v, mu, mut):
+        self._check(self.lib.cns_met_samut(self.ctx, l, _ptr(v), _ptr(mu), _ptr(mut)),
+                    "cns_met_samut")
+
+    def sch_turb(self, l, u, v, d, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z, ts6, ts7, sn, vol):
+        self._check(self.lib.cns_sch_turb(self.ctx, l, *(_ptr(a) for a in (
+            u, v, d, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z, ts6, ts7, sn, vol))), "cns_sch_turb")
+
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
                                         _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")

@@ -169,6 +169,17 @@ int cns_met_fludcsa(cns_ctx *ctx, int l, const double *s, const double *mu, doub
                     double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
 int cns_met_roe2o(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
 int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
+/* Spalart-Allmaras (constants of atlecdon.f90:193-204):
+ *   cns_met_samut  met_samut.f90:4-58   mut = v(:,6) fv1 on the real cells
+ *   cns_sch_turb   sch_turb.f90:4-290   centred fluxes of v(:,6:7) with the
+ *                  diffusion densities fd5*, fd6*, then
+ *                  u6 = 0.5 u6 - vol ts6 - d6 (and 7); u(:,6:7) zeroed over
+ *                  the block(s) first; no wall-law branch (kparoi = 0) */
+int cns_met_samut(cns_ctx *ctx, int l, const double *v, const double *mu, double *mut);
+int cns_sch_turb(cns_ctx *ctx, int l, double *u, const double *v, const double *d,
+                 const double *fd5x, const double *fd5y, const double *fd5z,
+                 const double *fd6x, const double *fd6y, const double *fd6z,
+                 const double *ts6, const double *ts7, const double *sn, const double *vol);
 
 /* Discrete adjoint of the FP64 Euler Roe iteration (sch_roe_euler with
  * unlimited MUSCL + implimf_eu with qfix_dfez = 1) at the bound state, for a

@@ -1978,6 +1978,103 @@ void orc_met_roe2o(int l, const double *t, double *d, const double *sn, int hart
   free(del7);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Spalart-Allmaras                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* the model constants of atlecdon.f90:193-204 */
+#define SA_CB1 0.1355
+#define SA_SIGMA (2. / 3.)
+#define SA_CB2 0.622
+#define SA_KAPPA 0.41
+#define SA_CV1 7.1
+
+/* met_samut.f90:35-46: mut = v6 fv1 on the real cells (x**3 as x*x*x) */
+void orc_met_samut(int l, const double *v, const double *mu, double *mut) {
+  const blk_t *b = &G.b[l - 1];
+  const double cv13 = SA_CV1 * SA_CV1 * SA_CV1;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        const double xkhi = v[5 * G.ld + n] / mu[n];
+        const double xkhi3 = xkhi * xkhi * xkhi;
+        const double fv1 = xkhi3 / (xkhi3 + cv13);
+        mut[n] = v[5 * G.ld + n] * fv1;
+      }
+}
+
+/* sch_turb.f90:4-290 (3-D, no wall law): centred fluxes of the transport
+ * variables, v(:,6:7) (q - (fd5, fd6)), summed per cell like sch_jameson,
+ * then u6 = 0.5 u6 - vol ts6 - d6 (and 7) */
+void orc_sch_turb(int l, double *u, const double *v, const double *d, const double *fd5x,
+                  const double *fd5y, const double *fd5z, const double *fd6x,
+                  const double *fd6y, const double *fd6z, const double *ts6,
+                  const double *ts7, const double *sn, const double *vol) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  for (int64_t n = n0; n < n0 + b->nnn; ++n) {
+    u[5 * L + n] = 0.;
+    u[6 * L + n] = 0.;
+  }
+  double *f = malloc(sizeof(double) * 6 * (size_t)b->nnn);
+  for (int64_t m = 0; m < b->nnn; ++m) {
+    const int64_t n = n0 + m;
+    if (v[n] == 0.) { /* cells never set (outside the flat range) */
+      for (int q = 0; q < 6; ++q) f[6 * m + q] = 0.;
+      continue;
+    }
+    f[6 * m + 0] = v[5 * L + n] * (v[L + n] / v[n]) - fd5x[n];
+    f[6 * m + 1] = v[5 * L + n] * (v[2 * L + n] / v[n]) - fd5y[n];
+    f[6 * m + 2] = v[5 * L + n] * (v[3 * L + n] / v[n]) - fd5z[n];
+    f[6 * m + 3] = v[6 * L + n] * (v[L + n] / v[n]) - fd6x[n];
+    f[6 * m + 4] = v[6 * L + n] * (v[2 * L + n] / v[n]) - fd6y[n];
+    f[6 * m + 5] = v[6 * L + n] * (v[3 * L + n] / v[n]) - fd6z[n];
+  }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    const int nd = NDIR(b, dir);
+    int lo[3], hi[3];
+    for (int pass = 0; pass < 3; ++pass) {
+      lo[0] = 1; hi[0] = b->ni - 1; lo[1] = 1; hi[1] = b->nj - 1; lo[2] = 1; hi[2] = b->nk - 1;
+      if (pass == 0) { lo[dir] = 2; hi[dir] = nd - 1; }
+      else lo[dir] = hi[dir] = pass == 1 ? 1 : nd;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            const int64_t n = IC(b, i, j, k), m = n - n0;
+            const double s1 = SN(sn, b, m, dir, 0), s2 = SN(sn, b, m, dir, 1),
+                         s3 = SN(sn, b, m, dir, 2);
+            double F[6];
+            if (pass == 0) {
+              for (int q = 0; q < 6; ++q) F[q] = f[6 * m + q] + f[6 * (m - ninc) + q];
+            } else {
+              const int64_t cg = (pass == 1 ? m - ninc : m);
+              for (int q = 0; q < 6; ++q) F[q] = 2 * f[6 * cg + q];
+            }
+            const double si6 = F[0] * s1 + F[1] * s2 + F[2] * s3;
+            const double si7 = F[3] * s1 + F[4] * s2 + F[5] * s3;
+            if (pass != 2) {
+              u[5 * L + n] = u[5 * L + n] - si6;
+              u[6 * L + n] = u[6 * L + n] - si7;
+            }
+            if (pass != 1) {
+              u[5 * L + n - ninc] = u[5 * L + n - ninc] + si6;
+              u[6 * L + n - ninc] = u[6 * L + n - ninc] + si7;
+            }
+          }
+    }
+  }
+  free(f);
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        u[5 * L + n] = 0.5 * u[5 * L + n] - vol[n] * ts6[n] - d[5 * L + n];
+        u[6 * L + n] = 0.5 * u[6 * L + n] - vol[n] * ts7[n] - d[6 * L + n];
+      }
+}
+
 /* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
  * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
  * (before rbord: the physical ghosts are the previous iteration's), rbord,

@@ -123,6 +123,13 @@ void orc_met_fludcsa(int l, const double *s, const double *mu, double *fd5x, dou
 void orc_met_roe2o(int l, const double *t, double *d, const double *sn, int harten,
                    double epsroe);
 
+/* Spalart-Allmaras: met_samut, sch_turb (v, u, d are (ld, 7)) */
+void orc_met_samut(int l, const double *v, const double *mu, double *mut);
+void orc_sch_turb(int l, double *u, const double *v, const double *d, const double *fd5x,
+                  const double *fd5y, const double *fd5z, const double *fd6x,
+                  const double *fd6y, const double *fd6z, const double *ts6,
+                  const double *ts7, const double *sn, const double *vol);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

@@ -65,6 +65,8 @@ def lib():
         L.orc_met_fludc.argtypes = [C.c_int] + [_d] * 8 + [C.c_double] * 2
         L.orc_met_fludcsa.argtypes = [C.c_int] + [_d] * 8 + [C.c_double]
         L.orc_met_roe2o.argtypes = [C.c_int, _d, _d, _d, C.c_int, C.c_double]
+        L.orc_met_samut.argtypes = [C.c_int, _d, _d, _d]
+        L.orc_sch_turb.argtypes = [C.c_int] + [_d] * 13
         _lib = L
     return _lib
 

@@ -118,3 +118,57 @@ def test_met_roe2o_parity(cuda, name, harten):
         s.sync()
         assert_equal_bits(dg.cpu().numpy().reshape(7, ld), d_o, f"d (l={l})")
     s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_samut_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    mu, _, _ = _fields(case, 47)
+    L = orc_lib()
+    mut_o = np.full(case.layout.ld, 5.0)
+    for b in range(1, case.layout.nblk + 1):
+        L.orc_met_samut(b, t.reshape(-1), mu, mut_o)
+    mut_g = _t(torch, np.full(case.layout.ld, 5.0))
+    s.met_samut(0, _t(torch, t.reshape(-1)), _t(torch, mu), mut_g)
+    s.sync()
+    assert_equal_bits(mut_g.cpu().numpy(), mut_o, "mut")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_sch_turb_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    ld = case.layout.ld
+    mu, mut, fd = _fields(case, 53)
+    r = cases.splitmix64_uniform(59, 4 * ld).reshape(4, ld) - 0.5
+    ts6, ts7 = r[0] * 1e-3, r[1] * 1e-3
+    d = np.zeros((7, ld))
+    d[5], d[6] = r[2] * 1e-4, r[3] * 1e-4
+    L = orc_lib()
+    tg = _t(torch, t.reshape(-1))
+    fdg = [_t(torch, fd[q]) for q in range(6)]
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        u_o = np.full((7, ld), 9.0)
+        blocks = range(1, case.layout.nblk + 1) if l == 0 else [l]
+        for b in blocks:
+            L.orc_sch_turb(b, u_o.reshape(-1), t.reshape(-1), d.reshape(-1),
+                           *[fd[q] for q in range(6)], ts6, ts7, st.sn, st.vol)
+        ug = _t(torch, np.full(7 * ld, 9.0))
+        s.sch_turb(l, ug, tg, _t(torch, d.reshape(-1)), *fdg, _t(torch, ts6), _t(torch, ts7),
+                   s.sn, s.vol)
+        s.sync()
+        if l == 0:
+            sel = np.arange(case.layout.ncells)
+        else:
+            b = case.layout.blocks[l - 1]
+            sel = np.arange(b.npc, b.npc + b.nnn)
+        assert_equal_bits(ug.cpu().numpy().reshape(7, ld)[5:, sel], u_o[5:, sel], f"u67 (l={l})")
+    s.close()

@@ -236,3 +236,26 @@ def test_batch_is_its_members():
             om.step(sm)
         assert np.array_equal(vb[:, bt.layout.blocks[ib].real_cells()],
                               sm.v.reshape(5, -1)[:, m.layout.blocks[0].real_cells()])
+
+
+def test_sch_turb_uniform_transport_is_source_only():
+    """a uniform transport field in a uniform flow with no diffusion gives a
+    zero flux balance: u6 = -vol ts6 - d6 exactly up to the metric closure"""
+    case = cases.box_case((8, 6, 5), seed=3, noise=0.0, ns=True, skew=0.02)
+    orc, st = oracle_prepared(case)
+    L = lib()
+    L.orc_zpres(1, st.v, st.ps, st.temp, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    ld = case.layout.ld
+    t = np.zeros((7, ld))
+    t[:5] = st.v.reshape(5, ld)
+    t[5] = 1e-3 * t[0]
+    t[6] = 0.5 * t[0]
+    z = np.zeros(ld)
+    ts = np.full(ld, 0.25)
+    d = np.zeros((7, ld))
+    u = np.zeros((7, ld))
+    L.orc_sch_turb(1, u.reshape(-1), t.reshape(-1), d.reshape(-1), z, z, z, z, z, z, ts, ts,
+                   st.sn, st.vol)
+    rc = real(case)
+    np.testing.assert_allclose(u[5, rc], -st.vol[rc] * 0.25, rtol=0, atol=1e-13)
