@@ -24,6 +24,8 @@ struct cns_ctx {
   SpaceBuf cells, faces[3], lines[3];
   SpaceBuf cells_ext;  // i 0..ni, j 0..nj, k 0..nk (met_roe2o's zeroed range)
   double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
+  double* sa_G = nullptr;    // Spalart-Allmaras gradient face values [3][9][ld]
+  double* sa_gr = nullptr;   // gradients of rho nu~ and rho [6][ld]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
   double* adj_N = nullptr;   // adjoint: linearised sweep blocks [35][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
@@ -966,6 +968,43 @@ int cns_sch_turb(cns_ctx* c, int l, double* u, const double* v, const double* d,
   const double* fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
   CK(launch_sch_turb(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, v, ld, fd, ts6, ts7, d,
                      sn, vol, c->w.G, u, c->st));
+  return CNS_OK;
+}
+
+static cudaError_t ensure_sa(cns_ctx* c) {
+  cudaError_t e = cudaSuccess;
+  if (!c->sa_G) e = dev_alloc(c, &c->sa_G, (size_t)27 * c->lay.ld, false);
+  if (e == cudaSuccess && !c->sa_gr) e = dev_alloc(c, &c->sa_gr, (size_t)6 * c->lay.ld, false);
+  return e;
+}
+
+int cns_teq_gradv(cns_ctx* c, int l, const double* v, const double* sn, const double* vol,
+                  double* dv) {
+  if (!c || bad_block(c, l) || !v || !sn || !vol || !dv) return CNS_EINVAL;
+  CK(ensure_sa(c));
+  CK(launch_teq_grads(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, 0, 3, v, nullptr,
+                      c->lay.ld, sn, vol, c->sa_G, dv, c->st));
+  return CNS_OK;
+}
+
+int cns_met_smsa(cns_ctx* c, int l, const double* v, const double* mu, const double* dist,
+                 const double* sn, const double* vol, const double* dv, const double* fd5x,
+                 const double* fd5y, const double* fd5z, double* ts6, double* ts7,
+                 double* cfke) {
+  if (!c || bad_block(c, l) || !v || !mu || !dist || !sn || !vol || !dv || !fd5x || !fd5y ||
+      !fd5z || !ts6 || !ts7 || !cfke)
+    return CNS_EINVAL;
+  CK(ensure_sa(c));
+  const long long ld = c->lay.ld;
+  const Space cells = c->cells.view(l - 1);
+  // met_difsa: grad(rho nu~); met_smsa: grad(rho)
+  CK(launch_teq_grads(c->d_blks, c->faces, cells, l - 1, 1, 1, v, v + 5 * ld, ld, sn, vol,
+                      c->sa_G, c->sa_gr, c->st));
+  CK(launch_teq_grads(c->d_blks, c->faces, cells, l - 1, 1, 1, v, v, ld, sn, vol, c->sa_G,
+                      c->sa_gr + 3 * ld, c->st));
+  const double* fd5[3] = {fd5x, fd5y, fd5z};
+  CK(launch_smsa(c->d_blks, cells, ld, v, mu, dist, dv, c->sa_gr, c->sa_gr + 3 * ld, fd5, ts6,
+                 ts7, cfke, c->st));
   return CNS_OK;
 }
 

@@ -259,6 +259,18 @@ cudaError_t launch_sch_turb(const Blk* blks, const SpaceBuf* faces, Space cells,
                             const double* sn, const double* vol, double* G, double* u,
                             cudaStream_t st);
 
+// teq_grads over the faces of block l0 (-1: all) into out[3 nsc][ld]:
+// mode 0 = the velocity (nsc 3), mode 1 = the field f (nsc 1); G scratch
+// [3][3 nsc][ld].  met_smsa with its gradients of rho nu~ (grt) and rho (grr)
+cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
+                             int mode, int nsc, const double* v, const double* f,
+                             long long ld, const double* sn, const double* vol, double* G,
+                             double* out, cudaStream_t st);
+cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double* v,
+                        const double* mu, const double* dist, const double* dv,
+                        const double* grt, const double* grr, const double* const fd5[3],
+                        double* ts6, double* ts7, double* cfke, cudaStream_t st);
+
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();

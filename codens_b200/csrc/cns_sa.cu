@@ -1,0 +1,205 @@
+// cns_sa.cu -- the Spalart-Allmaras source of the reference: the Green-Gauss
+// cell gradients of teq_grads.f90 (velocity gradients for teq_gradv.f90,
+// the gradients of rho nu~ and rho inside met_difsa.f90 / met_smsa.f90) and
+// the source term met_smsa.f90 with its derivative bound.
+//
+// Gradient: one thread per face computes the face value S (s_upper +
+// s_lower) (interior) or (2 S) s_ghost (boundary) of every scalar into the
+// face buffer, then one thread per real cell sums its faces in the
+// reference's order -- directions k, j, i; within a direction the lower face
+// subtracted then the upper added, the first cell of a line (lower face on
+// the boundary) taking its upper face first -- and multiplies by 0.5 / vol.
+// FP64, --fmad=false: bit-identical gradients.  The source uses exp and a
+// real power, whose last bit may differ from the host libm's.
+#include "cns_kernels.cuh"
+
+namespace cns {
+
+namespace {
+
+inline int grid_of(const Space& s) { return s.ntiles; }
+
+// SA constants (atlecdon.f90:193-204)
+constexpr double kCb1 = 0.1355, kSigma = 2. / 3., kCb2 = 0.622, kKappa = 0.41;
+constexpr double kCv1 = 7.1, kCw2 = 0.3, kCw3 = 2., kCt3 = 1.1, kCt4 = 2.;
+
+__device__ __forceinline__ double pow6(double x) {  // gcc's x**6: x3 * x3
+  const double x3 = x * x * x;
+  return x3 * x3;
+}
+
+// scalar q of cell n: mode 0 = the velocity component q (teq_gradv.f90:
+// t(:,q+1) / max(t(:,1), 1e-20)), mode 1 = the field f
+__device__ __forceinline__ double scalar_of(int mode, const double* __restrict__ v,
+                                            const double* __restrict__ f, long long ld,
+                                            long long n, int q) {
+  return mode == 0 ? v[(q + 1) * ld + n] / fmax(v[n], 1.e-20) : f[n];
+}
+
+template <int NSC>
+__global__ void __launch_bounds__(kTile) k_teq_face(const Blk* __restrict__ blks, Space sp,
+                                                    int dir, int mode,
+                                                    const double* __restrict__ v,
+                                                    const double* __restrict__ f, long long ld,
+                                                    const double* __restrict__ sn,
+                                                    double* __restrict__ G) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  const long long inc = ninc_of(B, dir);
+  const int nd = nd_of(B, dir);
+  const int p = dir == 0 ? i : (dir == 1 ? j : k);
+  const double S[3] = {sn_ptr(sn, B, dir, 0)[n], sn_ptr(sn, B, dir, 1)[n],
+                       sn_ptr(sn, B, dir, 2)[n]};
+  double* Gd = G + (long long)dir * 3 * NSC * ld;
+#pragma unroll
+  for (int q = 0; q < NSC; ++q) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double val;
+      if (p >= 2 && p <= nd - 1)
+        val = S[c] * (scalar_of(mode, v, f, ld, n, q) + scalar_of(mode, v, f, ld, n - inc, q));
+      else
+        val = S[c] * 2 * scalar_of(mode, v, f, ld, p == 1 ? n - inc : n, q);
+      Gd[(q * 3 + c) * ld + n] = val;
+    }
+  }
+}
+
+template <int NSC>
+__global__ void __launch_bounds__(kTile) k_teq_acc(const Blk* __restrict__ blks, Space sp,
+                                                   const double* __restrict__ G, long long ld,
+                                                   const double* __restrict__ vol,
+                                                   double* __restrict__ out) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  double acc[NSC * 3];
+#pragma unroll
+  for (int a = 0; a < NSC * 3; ++a) acc[a] = 0.;
+#pragma unroll
+  for (int o = 0; o < 3; ++o) {
+    const int dir = 2 - o;
+    const long long inc = ninc_of(B, dir);
+    const int nd = nd_of(B, dir);
+    const int p = dir == 0 ? i : (dir == 1 ? j : k);
+    const bool upper_first = (p == 1) && nd >= 3;
+    const double* Gd = G + (long long)dir * 3 * NSC * ld;
+#pragma unroll
+    for (int a = 0; a < NSC * 3; ++a) {
+      const double gl = Gd[a * ld + n], gu = Gd[a * ld + n + inc];
+      if (upper_first) {
+        acc[a] = acc[a] + gu;
+        acc[a] = acc[a] - gl;
+      } else {
+        acc[a] = acc[a] - gl;
+        acc[a] = acc[a] + gu;
+      }
+    }
+  }
+  // teq_grads.f90:338-346
+  const double ts = copysign(0.5, -vol[n]);
+  const double vols = (0.5 + ts) * 0.000001 + (0.5 - ts) * vol[n];
+  const double c0 = 0.5 / (vols + 2.2250738585072014e-308);
+#pragma unroll
+  for (int a = 0; a < NSC * 3; ++a) out[a * ld + n] = acc[a] * c0;
+}
+
+// met_smsa.f90:102-176 on the real cells; dv (global index, 9 rows: xx xy
+// xz yx yy yz zx zy zz), grt / grr: the gradients of rho nu~ and of rho
+__global__ void __launch_bounds__(kTile) k_smsa(
+    const Blk* __restrict__ blks, Space sp, long long ld, const double* __restrict__ v,
+    const double* __restrict__ mu, const double* __restrict__ dist,
+    const double* __restrict__ dv, const double* __restrict__ grt,
+    const double* __restrict__ grr, const double* __restrict__ fd5x,
+    const double* __restrict__ fd5y, const double* __restrict__ fd5z,
+    double* __restrict__ ts6, double* __restrict__ ts7, double* __restrict__ cfke) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  const long long m = n - B.npc;  // met_smsa.f90:177 reads txxf5x.. at this index
+  const double cw1 = kCb1 / (kKappa * kKappa) + (1 + kCb2) / kSigma;
+  const double kappa2 = kKappa * kKappa, uns6 = 1. / 6., cv13 = kCv1 * kCv1 * kCv1;
+  const double cw36 = pow6(kCw3), cv133 = 3. * cv13, ct42 = 2. * kCt4, cb2sig = kCb2 / kSigma;
+  // met_difsa.f90:96-101
+  double sdif = grt[n] * fd5x[n] + grt[ld + n] * fd5y[n] + grt[2 * ld + n] * fd5z[n];
+  sdif = sdif * kCb2 / kSigma;
+  const double v6 = v[5 * ld + n], v1 = v[n];
+  const double a1 = dv[7 * ld + n] - dv[5 * ld + n];  // dvzy - dvyz
+  const double a2 = dv[2 * ld + n] - dv[6 * ld + n];  // dvxz - dvzx
+  const double a3 = dv[3 * ld + n] - dv[ld + n];      // dvyx - dvxy
+  const double vort = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+  const double xkhi = v6 / mu[n];
+  const double xkhi2 = xkhi * xkhi;
+  const double xkhi3 = xkhi2 * xkhi;
+  const double dist2 = dist[n] * dist[n];
+  const double nutilde = v6 / v1;
+  const double kapd2 = kappa2 * dist2;
+  const double fv1 = xkhi3 / (xkhi3 + cv13);
+  const double fv2 = 1. - (xkhi / (1 + xkhi * fv1));
+  const double stilde = vort + nutilde * fv2 / kapd2;
+  double rtilde = nutilde / (stilde * kapd2);
+  rtilde = fmin(rtilde, 1.);
+  const double rtil6 = pow6(rtilde);
+  const double ft2 = kCt3 * exp(-kCt4 * xkhi2);
+  const double sm1 = kCb1 * (1. - ft2) * stilde * v6;
+  const double xg = rtilde + kCw2 * (rtil6 - rtilde);
+  const double xg6 = pow6(xg);
+  const double fw = xg * pow((1. + cw36) / (xg6 + cw36), uns6);
+  const double sm2 = -(cw1 * fw - kCb1 * ft2 / kappa2) * v6 * nutilde / dist2;
+  ts6[n] = sm1 + sm2 + sdif;
+  ts7[n] = 0.;
+  const double xkhi4 = xkhi3 * xkhi;
+  const double dfv1 = cv133 * (fv1 * fv1) / (mu[n] * xkhi4);
+  const double t1 = 1. + xkhi * fv1;
+  const double dfv2 = (xkhi2 * dfv1 - 1. / mu[n]) / (t1 * t1);
+  const double dst = (fv2 / v1 + nutilde * dfv2) / kapd2;
+  const double dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
+  const double dxg = dpr * (1. + kCw2 * (6. * rtil6 / rtilde - 1.));
+  const double dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+  const double dft2 = -ct42 * xkhi * ft2;
+  const double dsm1 = kCb1 * ((1. - ft2) * (stilde + dst * v6) - stilde * v6 * dft2);
+  const double dsm2 = 2. * sm2 / v6 - (cw1 * dfw - kCb1 * dft2 / kappa2) * nutilde * v6 / dist2;
+  const double dsdif =
+      -cb2sig * (fd5x[m] * grr[n] + fd5y[m] * grr[ld + n] + fd5z[m] * grr[2 * ld + n]) /
+      (v1 * v1);
+  cfke[n] = fabs(dsm1 + dsm2 + dsdif);
+}
+
+}  // namespace
+
+cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
+                             int mode, int nsc, const double* v, const double* f,
+                             long long ld, const double* sn, const double* vol, double* G,
+                             double* out, cudaStream_t st) {
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = faces[dir].view(l0);
+    if (sp.ntiles == 0) continue;
+    if (nsc == 3)
+      k_teq_face<3><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
+    else
+      k_teq_face<1><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
+  }
+  if (cells.ntiles > 0) {
+    if (nsc == 3)
+      k_teq_acc<3><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+    else
+      k_teq_acc<1><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double* v,
+                        const double* mu, const double* dist, const double* dv,
+                        const double* grt, const double* grr, const double* const fd5[3],
+                        double* ts6, double* ts7, double* cfke, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_smsa<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, v, mu, dist, dv, grt, grr,
+                                             fd5[0], fd5[1], fd5[2], ts6, ts7, cfke);
+  return cudaGetLastError();
+}
+
+}  // namespace cns

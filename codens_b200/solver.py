@@ -262,6 +262,14 @@ class CodeNS:
         self._check(self.lib.cns_sch_turb(self.ctx, l, *(_ptr(a) for a in (
             u, v, d, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z, ts6, ts7, sn, vol))), "cns_sch_turb")
 
+    def teq_gradv(self, l, v, sn, vol, dv):
+        self._check(self.lib.cns_teq_gradv(self.ctx, l, _ptr(v), _ptr(sn), _ptr(vol), _ptr(dv)),
+                    "cns_teq_gradv")
+
+    def met_smsa(self, l, v, mu, dist, sn, vol, dv, fd5x, fd5y, fd5z, ts6, ts7, cfke):
+        self._check(self.lib.cns_met_smsa(self.ctx, l, *(_ptr(a) for a in (
+            v, mu, dist, sn, vol, dv, fd5x, fd5y, fd5z, ts6, ts7, cfke))), "cns_met_smsa")
+
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
                                         _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")

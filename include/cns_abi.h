@@ -176,6 +176,19 @@ int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double
  *                  u6 = 0.5 u6 - vol ts6 - d6 (and 7); u(:,6:7) zeroed over
  *                  the block(s) first; no wall-law branch (kparoi = 0) */
 int cns_met_samut(cns_ctx *ctx, int l, const double *v, const double *mu, double *mut);
+/*   cns_teq_gradv  teq_gradv.f90:4-170  dv (9 x ld: xx xy xz yx yy yz zx zy
+ *                  zz) = Green-Gauss gradients of u, v, w on the real cells
+ *                  (teq_grads.f90, unit weights)
+ *   cns_met_smsa   met_smsa.f90:4-186 with met_difsa.f90: ts6 (qcxts5) =
+ *                  the SA source, ts7 (qcyts6) = 0, cfke = |d source| on the
+ *                  real cells, from dv, the diffusion densities fd5* and the
+ *                  wall distance dist */
+int cns_teq_gradv(cns_ctx *ctx, int l, const double *v, const double *sn, const double *vol,
+                  double *dv);
+int cns_met_smsa(cns_ctx *ctx, int l, const double *v, const double *mu, const double *dist,
+                 const double *sn, const double *vol, const double *dv, const double *fd5x,
+                 const double *fd5y, const double *fd5z, double *ts6, double *ts7,
+                 double *cfke);
 int cns_sch_turb(cns_ctx *ctx, int l, double *u, const double *v, const double *d,
                  const double *fd5x, const double *fd5y, const double *fd5z,
                  const double *fd6x, const double *fd6y, const double *fd6z,

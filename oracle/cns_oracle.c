@@ -2075,6 +2075,188 @@ void orc_sch_turb(int l, double *u, const double *v, const double *d, const doub
       }
 }
 
+/* x**6 as gcc expands an integer power: x3 = (x*x)*x, x6 = x3*x3 */
+static inline double pow6(double x) {
+  const double x3 = x * x * x;
+  return x3 * x3;
+}
+
+/* teq_grads.f90:4-374 (unit weights, the two branches coincide): Green-Gauss
+ * gradient of the cell field s (block-local index m) over the directions k,
+ * j, i -- interior faces (the lower one subtracted in a first sweep of each
+ * row, the upper one added in a second), then the lower and the upper
+ * boundary faces with twice the ghost value -- times 0.5 / vol on the flat
+ * range of the real cells */
+static void teq_grads(const blk_t *b, const double *sn, const double *vol, const double *s,
+                      double *dsdx, double *dsdy, double *dsdz) {
+  const int64_t n0 = b->npc;
+  for (int64_t m = 0; m < b->nnn; ++m) dsdx[m] = dsdy[m] = dsdz[m] = 0.;
+  static const int order[3] = {2, 1, 0};
+  double *g[3] = {dsdx, dsdy, dsdz};
+  for (int o = 0; o < 3; ++o) {
+    const int dir = order[o];
+    const int64_t ninc = NINC(b, dir);
+    const int nd = NDIR(b, dir);
+    int lo[3] = {1, 1, 1}, hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+    lo[dir] = 2;
+    hi[dir] = nd - 1;
+    /* the subtracting and the adding sweeps touch different cells of a
+     * face, so running them face by face gives every cell the same order */
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int64_t m = IC(b, i, j, k) - n0;
+          for (int c = 0; c < 3; ++c) g[c][m] = g[c][m] - SN(sn, b, m, dir, c) * (s[m] + s[m - ninc]);
+        }
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int64_t m = IC(b, i, j, k) - n0;
+          for (int c = 0; c < 3; ++c)
+            g[c][m - ninc] = g[c][m - ninc] + SN(sn, b, m, dir, c) * (s[m] + s[m - ninc]);
+        }
+    for (int side = 0; side < 2; ++side) {
+      int lo2[3] = {1, 1, 1}, hi2[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+      lo2[dir] = hi2[dir] = side == 0 ? 1 : nd;
+      for (int k = lo2[2]; k <= hi2[2]; ++k)
+        for (int j = lo2[1]; j <= hi2[1]; ++j)
+          for (int i = lo2[0]; i <= hi2[0]; ++i) {
+            const int64_t m = IC(b, i, j, k) - n0;
+            for (int c = 0; c < 3; ++c) {
+              if (side == 0)
+                g[c][m] = g[c][m] - SN(sn, b, m, dir, c) * 2 * s[m - ninc];
+              else
+                g[c][m - ninc] = g[c][m - ninc] + SN(sn, b, m, dir, c) * 2 * s[m];
+            }
+          }
+    }
+  }
+  const int64_t n1 = IC(b, 1, 1, 1), n2 = IC(b, b->ni - 1, b->nj - 1, b->nk - 1);
+  for (int64_t n = n1; n <= n2; ++n) {
+    const int64_t m = n - n0;
+    const double ts = copysign(0.5, -vol[n]);
+    const double vols = (0.5 + ts) * 0.000001 + (0.5 - ts) * vol[n];
+    const double c0 = 0.5 / (vols + DBL_MIN);
+    dsdx[m] = dsdx[m] * c0;
+    dsdy[m] = dsdy[m] * c0;
+    dsdz[m] = dsdz[m] * c0;
+  }
+}
+
+/* teq_gradv.f90:4-170: gradients of u, v, w (v is (ld, 7); the density
+ * floor of 1e-20 is applied to the values read, not written back).  dv:
+ * [9][nnn] block-local, order xx xy xz yx yy yz zx zy zz */
+void orc_teq_gradv(int l, const double *sn, const double *vol, const double *v, double *dv) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  double *s = calloc((size_t)nnn, sizeof(double));
+  for (int c = 0; c < 3; ++c) {
+    for (int k = 0; k <= b->nk; ++k)
+      for (int j = 0; j <= b->nj; ++j)
+        for (int i = 0; i <= b->ni; ++i) {
+          const int64_t n = IC(b, i, j, k);
+          s[n - n0] = v[(c + 1) * L + n] / fmax(v[n], 1.e-20);
+        }
+    teq_grads(b, sn, vol, s, dv + (3 * c) * nnn, dv + (3 * c + 1) * nnn, dv + (3 * c + 2) * nnn);
+  }
+  free(s);
+}
+
+/* met_smsa.f90:4-186 with met_difsa.f90:4-104: the Spalart-Allmaras source
+ * ts6 (qcxts5), ts7 = 0 (qcyts6) and the source-derivative bound cfke on the
+ * real cells.  v is (ld, 7); dv from orc_teq_gradv (block-local); fd5x..z the
+ * diffusion densities (txxf5x..); dist the wall distance */
+void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
+                  const double *mu, const double *dist, const double *dv,
+                  const double *fd5x, const double *fd5y, const double *fd5z, double *ts6,
+                  double *ts7, double *cfke) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  const double cb1 = SA_CB1, sigma = SA_SIGMA, cb2 = SA_CB2, kappa = SA_KAPPA, cv1 = SA_CV1;
+  const double cw1 = cb1 / (kappa * kappa) + (1 + cb2) / sigma;
+  const double cw2 = 0.3, cw3 = 2., ct3 = 1.1, ct4 = 2.;
+  double *t = calloc((size_t)nnn, sizeof(double));
+  double *dx = calloc((size_t)nnn, sizeof(double)), *dy = calloc((size_t)nnn, sizeof(double)),
+         *dz = calloc((size_t)nnn, sizeof(double)), *sdif = calloc((size_t)nnn, sizeof(double));
+  /* met_difsa: gradient of rho nu~, sdif = grad . fd5 * cb2 / sigma */
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 0; j <= b->nj; ++j)
+      for (int i = 0; i <= b->ni; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        t[n - n0] = v[5 * L + n];
+      }
+  teq_grads(b, sn, vol, t, dx, dy, dz);
+  const int64_t n1 = IC(b, 1, 1, 1), n2 = IC(b, b->ni - 1, b->nj - 1, b->nk - 1);
+  for (int64_t n = n1; n <= n2; ++n) {
+    const int64_t m = n - n0;
+    sdif[m] = dx[m] * fd5x[n] + dy[m] * fd5y[n] + dz[m] * fd5z[n];
+    sdif[m] = sdif[m] * cb2 / sigma;
+  }
+  /* gradient of the density */
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 0; j <= b->nj; ++j)
+      for (int i = 0; i <= b->ni; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        t[n - n0] = v[n];
+      }
+  teq_grads(b, sn, vol, t, dx, dy, dz);
+  const double kappa2 = kappa * kappa, uns6 = 1. / 6., cv13 = cv1 * cv1 * cv1;
+  const double cw36 = pow6(cw3), cv133 = 3. * cv13, ct42 = 2. * ct4, cb2sig = cb2 / sigma;
+  const double *dvxx = dv, *dvxy = dv + nnn, *dvxz = dv + 2 * nnn, *dvyx = dv + 3 * nnn,
+               *dvyy = dv + 4 * nnn, *dvyz = dv + 5 * nnn, *dvzx = dv + 6 * nnn,
+               *dvzy = dv + 7 * nnn, *dvzz = dv + 8 * nnn;
+  (void)dvxx;
+  (void)dvyy;
+  (void)dvzz;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        const double v6 = v[5 * L + n], v1 = v[n];
+        const double vort = sqrt(sq(dvzy[m] - dvyz[m]) + sq(dvxz[m] - dvzx[m]) +
+                                 sq(dvyx[m] - dvxy[m]));
+        const double xkhi = v6 / mu[n];
+        const double xkhi2 = xkhi * xkhi;
+        const double xkhi3 = xkhi2 * xkhi;
+        const double dist2 = dist[n] * dist[n];
+        const double nutilde = v6 / v1;
+        const double kapd2 = kappa2 * dist2;
+        const double fv1 = xkhi3 / (xkhi3 + cv13);
+        const double fv2 = 1. - (xkhi / (1 + xkhi * fv1));
+        const double stilde = vort + nutilde * fv2 / kapd2;
+        double rtilde = nutilde / (stilde * kapd2);
+        rtilde = fmin(rtilde, 1.);
+        const double rtil6 = pow6(rtilde);
+        const double ft2 = ct3 * exp(-ct4 * xkhi2);
+        const double sm1 = cb1 * (1. - ft2) * stilde * v6;
+        const double xg = rtilde + cw2 * (rtil6 - rtilde);
+        const double xg6 = pow6(xg);
+        const double fw = xg * pow((1. + cw36) / (xg6 + cw36), uns6);
+        const double sm2 = -(cw1 * fw - cb1 * ft2 / kappa2) * v6 * nutilde / dist2;
+        ts6[n] = sm1 + sm2 + sdif[m];
+        ts7[n] = 0.;
+        const double xkhi4 = xkhi3 * xkhi;
+        const double dfv1 = cv133 * sq(fv1) / (mu[n] * xkhi4);
+        const double dfv2 = (xkhi2 * dfv1 - 1. / mu[n]) / sq(1. + xkhi * fv1);
+        const double dst = (fv2 / v1 + nutilde * dfv2) / kapd2;
+        const double dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
+        const double dxg = dpr * (1. + cw2 * (6. * rtil6 / rtilde - 1.));
+        const double dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+        const double dft2 = -ct42 * xkhi * ft2;
+        const double dsm1 = cb1 * ((1. - ft2) * (stilde + dst * v6) - stilde * v6 * dft2);
+        const double dsm2 = 2. * sm2 / v6 - (cw1 * dfw - cb1 * dft2 / kappa2) * nutilde * v6 / dist2;
+        /* met_smsa.f90:177 reads txxf5x.. at the block-local index m (the
+         * global cell for block 1 only); reproduced */
+        const double dsdif = -cb2sig * (fd5x[m] * dx[m] + fd5y[m] * dy[m] + fd5z[m] * dz[m]) / sq(v1);
+        cfke[n] = fabs(dsm1 + dsm2 + dsdif);
+      }
+  free(t);
+  free(dx);
+  free(dy);
+  free(dz);
+  free(sdif);
+}
+
 /* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
  * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
  * (before rbord: the physical ghosts are the previous iteration's), rbord,

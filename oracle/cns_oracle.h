@@ -130,6 +130,13 @@ void orc_sch_turb(int l, double *u, const double *v, const double *d, const doub
                   const double *fd6y, const double *fd6z, const double *ts6,
                   const double *ts7, const double *sn, const double *vol);
 
+/* teq_gradv (dv: [9][nnn] block-local) and met_smsa (+ met_difsa) */
+void orc_teq_gradv(int l, const double *sn, const double *vol, const double *v, double *dv);
+void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
+                  const double *mu, const double *dist, const double *dv,
+                  const double *fd5x, const double *fd5y, const double *fd5z, double *ts6,
+                  double *ts7, double *cfke);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

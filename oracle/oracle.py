@@ -67,6 +67,8 @@ def lib():
         L.orc_met_roe2o.argtypes = [C.c_int, _d, _d, _d, C.c_int, C.c_double]
         L.orc_met_samut.argtypes = [C.c_int, _d, _d, _d]
         L.orc_sch_turb.argtypes = [C.c_int] + [_d] * 13
+        L.orc_teq_gradv.argtypes = [C.c_int] + [_d] * 4
+        L.orc_met_smsa.argtypes = [C.c_int] + [_d] * 12
         _lib = L
     return _lib
 

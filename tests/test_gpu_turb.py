@@ -172,3 +172,61 @@ def test_sch_turb_parity(cuda, name):
             sel = np.arange(b.npc, b.npc + b.nnn)
         assert_equal_bits(ug.cpu().numpy().reshape(7, ld)[5:, sel], u_o[5:, sel], f"u67 (l={l})")
     s.close()
+
+
+def _dv_oracle(case, st, t):
+    """teq_gradv of the oracle, block by block, in the global [9][ld] layout"""
+    ld = case.layout.ld
+    L = orc_lib()
+    dv = np.zeros((9, ld))
+    for l, b in enumerate(case.layout.blocks, start=1):
+        loc = np.zeros(9 * b.nnn)
+        L.orc_teq_gradv(l, st.sn, st.vol, t.reshape(-1), loc)
+        dv[:, b.npc:b.npc + b.nnn] = loc.reshape(9, b.nnn)
+    return dv
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_teq_gradv_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    dv_o = _dv_oracle(case, st, t)
+    dv_g = _t(torch, np.zeros(9 * case.layout.ld))
+    s.teq_gradv(0, _t(torch, t.reshape(-1)), s.sn, s.vol, dv_g)
+    s.sync()
+    rc = case.layout.real_cells()
+    assert_equal_bits(dv_g.cpu().numpy().reshape(9, -1)[:, rc], dv_o[:, rc], "dv")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_smsa_parity(cuda, name):
+    """the SA source against the oracle: exp and the real power of
+    met_smsa.f90 may differ in the last bit from the host libm, so 1e-13"""
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    ld = case.layout.ld
+    mu, _, fd = _fields(case, 61)
+    dist = 0.01 + cases.splitmix64_uniform(67, ld)
+    dv = _dv_oracle(case, st, t)
+    L = orc_lib()
+    ts6_o, ts7_o, cf_o = np.full(ld, 4.0), np.full(ld, 4.0), np.full(ld, 4.0)
+    for l, b in enumerate(case.layout.blocks, start=1):
+        L.orc_met_smsa(l, st.sn, st.vol, t.reshape(-1), mu, dist,
+                       np.ascontiguousarray(dv[:, b.npc:b.npc + b.nnn]).reshape(-1),
+                       fd[0], fd[1], fd[2], ts6_o, ts7_o, cf_o)
+    g = [_t(torch, np.full(ld, 4.0)) for _ in range(3)]
+    s.met_smsa(0, _t(torch, t.reshape(-1)), _t(torch, mu), _t(torch, dist), s.sn, s.vol,
+               _t(torch, dv.reshape(-1)), _t(torch, fd[0]), _t(torch, fd[1]), _t(torch, fd[2]),
+               *g)
+    s.sync()
+    rc = case.layout.real_cells()
+    for a, b, w in zip(g, (ts6_o, ts7_o, cf_o), ("ts6", "ts7", "cfke")):
+        np.testing.assert_allclose(a.cpu().numpy()[rc], b[rc], rtol=1e-13, atol=0, err_msg=w)
+    s.close()
