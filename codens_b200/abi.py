@@ -63,7 +63,7 @@ EXPORTS = [
     "cns_rfve", "cns_rfvc", "cns_dissip_jameson", "cns_sch_jameson",
     "cns_chrono_global", "cns_adjoint_prepare", "cns_adjoint_rt", "cns_adjoint_lt",
     "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
-    "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa",
+    "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
 ]
 
 _lib = None
@@ -125,6 +125,7 @@ def load(build_if_missing: bool = True):
     L.cns_sch_turb.argtypes = [vp, C.c_int] + [vp] * 13
     L.cns_teq_gradv.argtypes = [vp, C.c_int] + [vp] * 4
     L.cns_met_smsa.argtypes = [vp, C.c_int] + [vp] * 12
+    L.cns_impli2_eqt_3d.argtypes = [vp, C.c_int] + [vp] * 8 + [c_f64]
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,

@@ -26,6 +26,7 @@ struct cns_ctx {
   double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
   double* sa_G = nullptr;    // Spalart-Allmaras gradient face values [3][9][ld]
   double* sa_gr = nullptr;   // gradients of rho nu~ and rho [6][ld]
+  double* sa_w = nullptr;    // impli2_eqt_3d scratch [15][ld]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
   double* adj_N = nullptr;   // adjoint: linearised sweep blocks [35][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
@@ -1005,6 +1006,18 @@ int cns_met_smsa(cns_ctx* c, int l, const double* v, const double* mu, const dou
   const double* fd5[3] = {fd5x, fd5y, fd5z};
   CK(launch_smsa(c->d_blks, cells, ld, v, mu, dist, dv, c->sa_gr, c->sa_gr + 3 * ld, fd5, ts6,
                  ts7, cfke, c->st));
+  return CNS_OK;
+}
+
+int cns_impli2_eqt_3d(cns_ctx* c, int l, const double* u, const double* dt, double* v,
+                      const double* mu, const double* mut, const double* cfke,
+                      const double* sn, const double* vol, double cmt) {
+  if (!c || bad_block(c, l) || !u || !dt || !v || !mu || !mut || !cfke || !sn || !vol ||
+      !(cmt != 0.))
+    return CNS_EINVAL;
+  if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)15 * c->lay.ld, false));
+  CK(launch_impli2(c->d_blks, c->faces, c->lines, c->cells.view(l - 1), l - 1, c->lay.ld, u, dt,
+                   v, mu, mut, cfke, sn, vol, cmt, c->sa_w, c->st));
   return CNS_OK;
 }
 

@@ -270,6 +270,12 @@ cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double
                         const double* mu, const double* dist, const double* dv,
                         const double* grt, const double* grr, const double* const fd5[3],
                         double* ts6, double* ts7, double* cfke, cudaStream_t st);
+// impli2_eqt_3d of block l0 (-1: all): u, v are (ld, 7); w: 15 ld scratch
+cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf* lines,
+                          Space cells, int l0, long long ld, const double* u, const double* dt,
+                          double* v, const double* mu, const double* mut, const double* cfke,
+                          const double* sn, const double* vol, double cmt, double* w,
+                          cudaStream_t st);
 
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)

@@ -169,6 +169,129 @@ __global__ void __launch_bounds__(kTile) k_smsa(
   cfke[n] = fabs(dsm1 + dsm2 + dsdif);
 }
 
+// impli2_eqt_3d.f90:93-103: rv and the time-step part of the diagonal
+__global__ void __launch_bounds__(kTile) k_i2_cell(const Blk* __restrict__ blks, Space sp,
+                                                   const double* __restrict__ v,
+                                                   const double* __restrict__ mu,
+                                                   const double* __restrict__ mut,
+                                                   const double* __restrict__ dt,
+                                                   const double* __restrict__ cfke,
+                                                   const double* __restrict__ vol, double cmt,
+                                                   double* __restrict__ rv,
+                                                   double* __restrict__ cd) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  rv[n] = (mu[n] + mut[n] / cmt) / v[n];
+  cd[n] = vol[n] / dt[n] + cfke[n] * vol[n];
+}
+
+// impli2_eqt_3d.f90:104-160: face velocity flux u_dir and coefficient of one
+// face (boundary faces included)
+__global__ void __launch_bounds__(kTile) k_i2_face(const Blk* __restrict__ blks, Space sp,
+                                                   int dir, const double* __restrict__ v,
+                                                   long long ld, const double* __restrict__ sn,
+                                                   const double* __restrict__ vol,
+                                                   const double* __restrict__ rv,
+                                                   double* __restrict__ uf,
+                                                   double* __restrict__ ce) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  const long long inc = ninc_of(B, dir), nl = n - inc;
+  const double s1 = sn_ptr(sn, B, dir, 0)[n], s2 = sn_ptr(sn, B, dir, 1)[n],
+               s3 = sn_ptr(sn, B, dir, 2)[n];
+  const double cnds = s1 * s1 + s2 * s2 + s3 * s3;
+  const double uu = 0.5 * (v[ld + n] / v[n] + v[ld + nl] / v[nl]);
+  const double vv = 0.5 * (v[2 * ld + n] / v[n] + v[2 * ld + nl] / v[nl]);
+  const double ww = 0.5 * (v[3 * ld + n] / v[n] + v[3 * ld + nl] / v[nl]);
+  const double u = 0.5 * (uu * s1 + vv * s2 + ww * s3);
+  uf[(long long)dir * ld + n] = u;
+  ce[(long long)dir * ld + n] = fabs(u) + (rv[n] + rv[nl]) * cnds / (vol[n] + vol[nl]);
+}
+
+// impli2_eqt_3d.f90:161-171
+__global__ void __launch_bounds__(kTile) k_i2_diag(const Blk* __restrict__ blks, Space sp,
+                                                   long long ld, const double* __restrict__ ce,
+                                                   double* __restrict__ cd) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long m = cell_index(B, i, j, k);
+  cd[m] = cd[m] + ce[m] + ce[m + 1] + ce[ld + m] + ce[ld + m + B.nid] + ce[2 * ld + m] +
+          ce[2 * ld + m + B.nijd];
+}
+
+// one alternating-line sweep of direction dir (impli2_eqt_3d.f90:172-291):
+// a thread per line solves the tridiagonal system along it (backward
+// recurrence into al/b6/b7, forward substitution into the new iterate); the
+// two other directions' neighbours come from the previous iterate
+__global__ void __launch_bounds__(kTile) k_i2_line(
+    const Blk* __restrict__ blks, Space sp, int dir, long long ld,
+    const double* __restrict__ u, const double* __restrict__ uf,
+    const double* __restrict__ ce, const double* __restrict__ cd,
+    const double* __restrict__ o6, const double* __restrict__ o7, double* __restrict__ n6,
+    double* __restrict__ n7, double* __restrict__ al, double* __restrict__ b6,
+    double* __restrict__ b7) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const int oa = dir == 0 ? 1 : 0, ob = dir == 2 ? 1 : 2;
+  const long long inc = ninc_of(B, dir), inca = ninc_of(B, oa), incb = ninc_of(B, ob);
+  const int nd = nd_of(B, dir);
+  const double *ua = uf + (long long)oa * ld, *ub = uf + (long long)ob * ld,
+               *ud = uf + (long long)dir * ld;
+  const double *ca = ce + (long long)oa * ld, *cb = ce + (long long)ob * ld,
+               *cdir = ce + (long long)dir * ld;
+  const long long m1 = cell_index(B, i, j, k);  // the line's first cell (p = 1)
+  // backward recurrence; the values at p + 1 carried (zero past the end, as
+  // the never-written ghost entries of the reference)
+  double aln = 0., b6n = 0., b7n = 0.;
+  for (int p = nd - 1; p >= 1; --p) {
+    const long long m = m1 + (long long)(p - 1) * inc;
+    const double td = -ua[m + inca] + ua[m] - ub[m + incb] + ub[m];
+    const double tpa = ca[m + inca] - ua[m + inca], tma = ca[m] + ua[m];
+    const double tpb = cb[m + incb] - ub[m + incb], tmb = cb[m] + ub[m];
+    const double di6 = -u[5 * ld + m] + td * o6[m] + tma * o6[m - inca] + tpa * o6[m + inca] +
+                       tmb * o6[m - incb] + tpb * o6[m + incb];
+    const double di7 = -u[6 * ld + m] + td * o7[m] + tma * o7[m - inca] + tpa * o7[m + inca] +
+                       tmb * o7[m - incb] + tpb * o7[m + incb];
+    const double ai = cdir[m] + ud[m];
+    const double bi = cd[m] + ud[m + inc] - ud[m];
+    const double cci = -cdir[m + inc] + ud[m + inc];
+    const double den = bi + cci * aln;
+    aln = ai / den;
+    b6n = (di6 - cci * b6n) / den;
+    b7n = (di7 - cci * b7n) / den;
+    al[m] = aln;
+    b6[m] = b6n;
+    b7[m] = b7n;
+  }
+  // forward substitution (the cell before the line's first is a ghost: 0)
+  double w6 = 0., w7 = 0.;
+  for (int p = 1; p <= nd - 1; ++p) {
+    const long long m = m1 + (long long)(p - 1) * inc;
+    w6 = al[m] * w6 + b6[m];
+    w7 = al[m] * w7 + b7[m];
+    n6[m] = w6;
+    n7[m] = w7;
+  }
+}
+
+// v(:,6:7) += dw on the real cells (impli2_eqt_3d.f90:321-329)
+__global__ void __launch_bounds__(kTile) k_i2_update(const Blk* __restrict__ blks, Space sp,
+                                                     long long ld,
+                                                     const double* __restrict__ w6,
+                                                     const double* __restrict__ w7,
+                                                     double* __restrict__ v) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  v[5 * ld + n] = v[5 * ld + n] + w6[n];
+  v[6 * ld + n] = v[6 * ld + n] + w7[n];
+}
+
 }  // namespace
 
 cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
@@ -189,6 +312,41 @@ cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells
     else
       k_teq_acc<1><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf* lines,
+                          Space cells, int l0, long long ld, const double* u, const double* dt,
+                          double* v, const double* mu, const double* mut, const double* cfke,
+                          const double* sn, const double* vol, double cmt, double* w,
+                          cudaStream_t st) {
+  // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7) = 15 ld
+  double *rv = w, *cd = w + ld, *uf = w + 2 * ld, *ce = w + 5 * ld, *al = w + 8 * ld,
+         *b6 = w + 9 * ld, *b7 = w + 10 * ld;
+  double* it[2][2] = {{w + 11 * ld, w + 12 * ld}, {w + 13 * ld, w + 14 * ld}};
+  cudaError_t e = cudaMemsetAsync(w, 0, sizeof(double) * 15 * ld, st);
+  if (e != cudaSuccess) return e;
+  if (cells.ntiles == 0) return cudaSuccess;
+  k_i2_cell<<<grid_of(cells), kTile, 0, st>>>(blks, cells, v, mu, mut, dt, cfke, vol, cmt, rv,
+                                              cd);
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = faces[dir].view(l0);
+    if (sp.ntiles > 0)
+      k_i2_face<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, v, ld, sn, vol, rv, uf, ce);
+  }
+  k_i2_diag<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, ce, cd);
+  int cur = 0;
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = lines[dir].view(l0);
+    for (int sw = 0; sw < 2; ++sw) {
+      if (sp.ntiles > 0)
+        k_i2_line<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ld, u, uf, ce, cd, it[cur][0],
+                                                 it[cur][1], it[1 - cur][0], it[1 - cur][1], al,
+                                                 b6, b7);
+      cur = 1 - cur;
+    }
+  }
+  k_i2_update<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, it[cur][0], it[cur][1], v);
   return cudaGetLastError();
 }
 

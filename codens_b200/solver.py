@@ -270,6 +270,10 @@ class CodeNS:
         self._check(self.lib.cns_met_smsa(self.ctx, l, *(_ptr(a) for a in (
             v, mu, dist, sn, vol, dv, fd5x, fd5y, fd5z, ts6, ts7, cfke))), "cns_met_smsa")
 
+    def impli2_eqt_3d(self, l, u, dt, v, mu, mut, cfke, sn, vol, cmt=1.0):
+        self._check(self.lib.cns_impli2_eqt_3d(self.ctx, l, *(_ptr(a) for a in (
+            u, dt, v, mu, mut, cfke, sn, vol)), float(cmt)), "cns_impli2_eqt_3d")
+
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
                                         _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")

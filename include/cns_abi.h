@@ -185,6 +185,13 @@ int cns_met_samut(cns_ctx *ctx, int l, const double *v, const double *mu, double
  *                  wall distance dist */
 int cns_teq_gradv(cns_ctx *ctx, int l, const double *v, const double *sn, const double *vol,
                   double *dv);
+/*   cns_impli2_eqt_3d  impli2_eqt_3d.f90:4-330 (no wall law): implicit phase
+ *                  of the transport equations, two alternating-line sweeps
+ *                  (tridiagonal solves) per direction i, j, k; v(:,6:7) += dw
+ *                  on the real cells; cmt = the model's constant (1 for 1SA) */
+int cns_impli2_eqt_3d(cns_ctx *ctx, int l, const double *u, const double *dt, double *v,
+                      const double *mu, const double *mut, const double *cfke,
+                      const double *sn, const double *vol, double cmt);
 int cns_met_smsa(cns_ctx *ctx, int l, const double *v, const double *mu, const double *dist,
                  const double *sn, const double *vol, const double *dv, const double *fd5x,
                  const double *fd5y, const double *fd5z, double *ts6, double *ts7,

@@ -2257,6 +2257,118 @@ void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
   free(sdif);
 }
 
+/* impli2_eqt_3d.f90:4-330 (no wall law): implicit phase of the two
+ * transport equations -- coefficients, then for the directions i, j, k two
+ * alternating-line sweeps each (a tridiagonal solve along every line of the
+ * direction, the other directions' neighbours taken from the previous
+ * iterate), then v(:,6:7) += dw on the real cells.  cmt: the model's
+ * diffusion constant (1 for 1SA) */
+void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, const double *mu,
+                       const double *mut, const double *cfke, const double *sn,
+                       const double *vol, double cmt) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  const int64_t nci = 1, ncj = b->nid, nck = b->nijd;
+  double *dw6 = calloc(nnn, sizeof(double)), *dw7 = calloc(nnn, sizeof(double));
+  double *ce = calloc(3 * nnn, sizeof(double)), *rv = calloc(nnn, sizeof(double));
+  double *uf = calloc(3 * nnn, sizeof(double)), *cd = calloc(nnn, sizeof(double));
+  double *al = calloc(nnn, sizeof(double)), *b6 = calloc(nnn, sizeof(double)),
+         *b7 = calloc(nnn, sizeof(double));
+  double *o6 = calloc(nnn, sizeof(double)), *o7 = calloc(nnn, sizeof(double));
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        rv[m] = (mu[n] + mut[n] / cmt) / v[n];
+        cd[m] = vol[n] / dt[n] + cfke[n] * vol[n];
+      }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    int lo[3] = {1, 1, 1}, hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+    hi[dir] = NDIR(b, dir);
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int64_t n = IC(b, i, j, k), m = n - n0;
+          const double s1 = SN(sn, b, m, dir, 0), s2 = SN(sn, b, m, dir, 1),
+                       s3 = SN(sn, b, m, dir, 2);
+          const double cnds = s1 * s1 + s2 * s2 + s3 * s3;
+          const double uu = 0.5 * (v[L + n] / v[n] + v[L + n - ninc] / v[n - ninc]);
+          const double vv = 0.5 * (v[2 * L + n] / v[n] + v[2 * L + n - ninc] / v[n - ninc]);
+          const double ww = 0.5 * (v[3 * L + n] / v[n] + v[3 * L + n - ninc] / v[n - ninc]);
+          uf[dir * nnn + m] = 0.5 * (uu * s1 + vv * s2 + ww * s3);
+          ce[dir * nnn + m] = fabs(uf[dir * nnn + m]) +
+                              (rv[m] + rv[m - ninc]) * cnds / (vol[n] + vol[n - ninc]);
+        }
+  }
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t m = IC(b, i, j, k) - n0;
+        cd[m] = cd[m] + ce[m] + ce[m + nci] + ce[nnn + m] + ce[nnn + m + ncj] + ce[2 * nnn + m] +
+                ce[2 * nnn + m + nck];
+      }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    const int d1 = (dir + 1) % 3, d2 = (dir + 2) % 3;
+    /* the two other directions in the reference's order (i: j, k; j: i, k;
+     * k: i, j) */
+    const int oa = d1 < d2 ? d1 : d2, ob = d1 < d2 ? d2 : d1;
+    const int64_t inca = NINC(b, oa), incb = NINC(b, ob);
+    const double *ua = uf + oa * nnn, *ub = uf + ob * nnn, *ud = uf + dir * nnn;
+    const double *ca = ce + oa * nnn, *cb = ce + ob * nnn, *cdir = ce + dir * nnn;
+    for (int64_t m = 0; m < nnn; ++m) al[m] = b6[m] = b7[m] = 0.;
+    for (int sw = 0; sw < 2; ++sw) {
+      /* backward recurrence on every line, from the previous iterate */
+      int lo[3] = {1, 1, 1}, hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+      const int nd = NDIR(b, dir);
+      for (int p = nd - 1; p >= 1; --p) {
+        lo[dir] = hi[dir] = p;
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+              const int64_t n = IC(b, i, j, k), m = n - n0;
+              const double td = -ua[m + inca] + ua[m] - ub[m + incb] + ub[m];
+              const double tpa = ca[m + inca] - ua[m + inca], tma = ca[m] + ua[m];
+              const double tpb = cb[m + incb] - ub[m + incb], tmb = cb[m] + ub[m];
+              const double di6 = -u[5 * L + n] + td * dw6[m] + tma * dw6[m - inca] +
+                                 tpa * dw6[m + inca] + tmb * dw6[m - incb] + tpb * dw6[m + incb];
+              const double di7 = -u[6 * L + n] + td * dw7[m] + tma * dw7[m - inca] +
+                                 tpa * dw7[m + inca] + tmb * dw7[m - incb] + tpb * dw7[m + incb];
+              const double ai = cdir[m] + ud[m];
+              const double bi = cd[m] + ud[m + ninc] - ud[m];
+              const double cci = -cdir[m + ninc] + ud[m + ninc];
+              al[m] = ai / (bi + cci * al[m + ninc]);
+              b6[m] = (di6 - cci * b6[m + ninc]) / (bi + cci * al[m + ninc]);
+              b7[m] = (di7 - cci * b7[m + ninc]) / (bi + cci * al[m + ninc]);
+            }
+      }
+      /* forward substitution */
+      memcpy(o6, dw6, nnn * sizeof(double));
+      memcpy(o7, dw7, nnn * sizeof(double));
+      for (int p = 1; p <= nd - 1; ++p) {
+        lo[dir] = hi[dir] = p;
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+              const int64_t m = IC(b, i, j, k) - n0;
+              dw6[m] = al[m] * dw6[m - ninc] + b6[m];
+              dw7[m] = al[m] * dw7[m - ninc] + b7[m];
+            }
+      }
+    }
+  }
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        v[5 * L + n] = v[5 * L + n] + dw6[m];
+        v[6 * L + n] = v[6 * L + n] + dw7[m];
+      }
+  free(dw6); free(dw7); free(ce); free(rv); free(uf); free(cd); free(al); free(b6); free(b7);
+  free(o6); free(o7);
+}
+
 /* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
  * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
  * (before rbord: the physical ghosts are the previous iteration's), rbord,

@@ -137,6 +137,10 @@ void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
                   const double *fd5x, const double *fd5y, const double *fd5z, double *ts6,
                   double *ts7, double *cfke);
 
+void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, const double *mu,
+                       const double *mut, const double *cfke, const double *sn,
+                       const double *vol, double cmt);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

@@ -69,6 +69,7 @@ def lib():
         L.orc_sch_turb.argtypes = [C.c_int] + [_d] * 13
         L.orc_teq_gradv.argtypes = [C.c_int] + [_d] * 4
         L.orc_met_smsa.argtypes = [C.c_int] + [_d] * 12
+        L.orc_impli2_eqt_3d.argtypes = [C.c_int] + [_d] * 8 + [C.c_double]
         _lib = L
     return _lib
 

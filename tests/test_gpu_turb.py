@@ -230,3 +230,32 @@ def test_met_smsa_parity(cuda, name):
     for a, b, w in zip(g, (ts6_o, ts7_o, cf_o), ("ts6", "ts7", "cfke")):
         np.testing.assert_allclose(a.cpu().numpy()[rc], b[rc], rtol=1e-13, atol=0, err_msg=w)
     s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_impli2_eqt_3d_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    t = _transport_state(case, st)
+    ld = case.layout.ld
+    mu, mut, _ = _fields(case, 71)
+    r = cases.splitmix64_uniform(73, 4 * ld).reshape(4, ld)
+    dt = 0.01 + 0.01 * r[0]
+    cfke = r[1]
+    u = np.zeros((7, ld))
+    u[5], u[6] = (r[2] - 0.5) * 1e-4, (r[3] - 0.5) * 1e-3
+    L = orc_lib()
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        to = t.copy()
+        blocks = range(1, case.layout.nblk + 1) if l == 0 else [l]
+        for b in blocks:
+            L.orc_impli2_eqt_3d(b, u.reshape(-1), dt, to.reshape(-1), mu, mut, cfke, st.sn,
+                                st.vol, 1.0)
+        tg = _t(torch, t.reshape(-1))
+        s.impli2_eqt_3d(l, _t(torch, u.reshape(-1)), _t(torch, dt), tg, _t(torch, mu),
+                        _t(torch, mut), _t(torch, cfke), s.sn, s.vol, 1.0)
+        s.sync()
+        assert_equal_bits(tg.cpu().numpy().reshape(7, ld), to, f"v (l={l})")
+    s.close()
