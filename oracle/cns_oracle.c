@@ -125,6 +125,16 @@ void orc_set_scheme(int ns, int muscl, double xk, int ilim, double eta,
   G.lmax = lmax;
 }
 
+/* threads of the per-block loops of an iteration (OpenMP) */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  extern void omp_set_num_threads(int);
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
+}
+
 void orc_set_dissipation(int ischema, double ki2, double ki4) {
   G.ischema = ischema;
   G.ki2 = ki2;
@@ -2401,15 +2411,16 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt) {
-  for (int l = 1; l <= G.nblk; ++l) orc_zpres(l, v, ps, temp, cson);
-  if (G.ns)
-    for (int l = 1; l <= G.nblk; ++l) orc_zvismo(l, mu, temp);
-  if (compute_dt) {
-    for (int l = 1; l <= G.nblk; ++l) orc_chronos(l, mu, mut, v, dt, sn, vol, cson);
-    if (G.kdtl == 0) orc_chrono_global(dt);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int l = 1; l <= G.nblk; ++l) {
+    orc_zpres(l, v, ps, temp, cson);
+    if (G.ns) orc_zvismo(l, mu, temp);
+    if (compute_dt) orc_chronos(l, mu, mut, v, dt, sn, vol, cson);
   }
+  if (compute_dt && G.kdtl == 0) orc_chrono_global(dt);
   orc_rbord(v, ps, temp, cson);
   if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int l = 1; l <= G.nblk; ++l) {
     if (G.ns) {
       orc_sch_roe(l, u, v, tau, sn, ps);

@@ -101,6 +101,9 @@ void orc_rscpsv(const double *u0, const double *v, const double *dt,
 /* one pseudo-time iteration over all blocks (atsch_num.f90:245-1134 for the
  * ischema=7, kmf=1 Roe/implicit path); work holds ld*(9+5) doubles for
  * ps,temp,cson,mu,mut,dt,...; returns 0 */
+/* threads of the per-block loops of an iteration (OpenMP) */
+void orc_set_threads(int n);
+
 /* Jameson scheme: ischema 1, ki2/ki4 of every block (schemanum) */
 void orc_set_dissipation(int ischema, double ki2, double ki4);
 void orc_rfve(double *v, double *ps, double *temp, double *cson);

@@ -56,6 +56,7 @@ def lib():
         L.orc_step.argtypes = [_d] * 12 + [C.c_int]
         L.orc_step.restype = C.c_int
         L.orc_set_dissipation.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_set_threads.argtypes = [C.c_int]
         L.orc_rfve.argtypes = [_d] * 4
         L.orc_rfvc.argtypes = [_d] * 4
         L.orc_dissip_jameson.argtypes = [C.c_int] + [_d] * 5
