@@ -275,7 +275,7 @@ __device__ __forceinline__ void load_prim(const T* __restrict__ v,
 // face 1, upper face nd).  Results go to G[dir][a][n], n the cell above the
 // face.
 template <class T, bool NS>
-__global__ void __launch_bounds__(kTile, 3) k_face_flux(
+__global__ void __launch_bounds__(kTile, 4) k_face_flux(
     const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
     const T* __restrict__ v, const T* __restrict__ prim, long long ld,
     const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
