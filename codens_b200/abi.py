@@ -46,6 +46,10 @@ class Bnd_t(C.Structure):
                 ("bceqt", P(c_f64))]
 
 
+class Sa_t(C.Structure):
+    _fields_ = [("dist", C.c_void_p), ("rokinf", c_f64), ("roeinf", c_f64), ("epsk", c_f64)]
+
+
 class State_t(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in
                 ("v", "u", "d", "dt", "sn", "vol", "pression", "ztemp", "cson",
@@ -64,6 +68,8 @@ EXPORTS = [
     "cns_chrono_global", "cns_adjoint_prepare", "cns_adjoint_rt", "cns_adjoint_lt",
     "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
     "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
+    "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
+    "cns_set_sa", "cns_met_num",
 ]
 
 _lib = None
@@ -126,6 +132,13 @@ def load(build_if_missing: bool = True):
     L.cns_teq_gradv.argtypes = [vp, C.c_int] + [vp] * 4
     L.cns_met_smsa.argtypes = [vp, C.c_int] + [vp] * 12
     L.cns_impli2_eqt_3d.argtypes = [vp, C.c_int] + [vp] * 8 + [c_f64]
+    L.cns_atcaldis3.argtypes = [vp] * 5
+    L.cns_met_bord.argtypes = [vp, vp, c_f64, c_f64]
+    L.cns_met_gradtr.argtypes = [vp, C.c_int] + [vp] * 9
+    L.cns_met_rbse.argtypes = [vp] * 7
+    L.cns_met_cutsa.argtypes = [vp, C.c_int, vp, c_f64]
+    L.cns_set_sa.argtypes = [vp, P(Sa_t)]
+    L.cns_met_num.argtypes = [vp]
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,

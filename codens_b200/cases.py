@@ -16,7 +16,11 @@ Workloads (sizes are cells):
   * ``channel_case``  -- blocks in a row forming a channel with a Gaussian
                          bump on the lower wall: injection / outlet pressure /
                          adiabatic walls / periodic k, coincident joins;
-  * ``batch_case``    -- many independent boxes of random sides and Mach.
+  * ``batch_case``    -- many independent boxes of random sides and Mach;
+  * ``flat_plate_case`` -- one wall-bounded block with geometric wall
+                         stretching and the two Spalart-Allmaras transport
+                         columns: injection / outlet / adiabatic plate /
+                         extrapolated top / periodic span.
 """
 from __future__ import annotations
 
@@ -417,3 +421,60 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
                 meta=dict(mach=mach, seed=seed, reynz=reynz, alpha=alpha,
                           ni=list(ni_cells), nj=nj_cells, nk=nk_cells, length=length,
                           span=span, bump=bump, beta=beta))
+
+
+def sutherland_mu(phys: Phys, temp: float) -> float:
+    """zvismo.f90:90-104 (air): mu = T^1.5 (1 + a) / (T + a) / Re"""
+    a = phys.suth_a
+    return (1.0 / phys.reynz) * temp * math.sqrt(temp) * (1.0 + a) / (temp + a)
+
+
+def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e6,
+                    dy1: float = 1.0e-5, ratio: float = 1.1, length: float = 1.0,
+                    span: float = 0.1, nut_ratio: float = 3.0, seed: int = 3,
+                    noise: float = 0.01, lmax: int = 10, eta: float = 5.0,
+                    name: str = "flat_plate") -> Case:
+    """RANS flat plate: one block of cells[0] x cells[1] x cells[2] cells.
+
+    x uniform over ``length`` (the plate spans the whole lower face, leading
+    edge at the inlet), y geometric from the wall (first spacing dy1, growth
+    ratio), z uniform over ``span``.  Boundaries: idd at i1 (freestream total
+    pressure / temperature along +x), prd at i2 (freestream static
+    pressure), para (adiabatic wall) at j1, extr at j2, periodic k.  The
+    state has 7 columns: the noisy freestream and the Spalart-Allmaras
+    variable rho nu~ = nut_ratio * mu_inf (v(:,7) = 0), as met_inisa.f90
+    leaves it for a uniform mut.  meta['rokinf'] is the freestream rho nu~
+    the injection ghosts take (met_bord.f90:60-63).
+    """
+    ni, nj, nk = (c + 1 for c in cells)
+    lay = Layout.from_dims([(ni, nj, nk)])
+    phys = Phys(reynz=reynz)
+    scheme = Scheme(ns=1, ilim=0, lmax=lmax, eta=eta)
+    x = np.zeros(lay.ld); y = np.zeros(lay.ld); z = np.zeros(lay.ld)
+    b = lay.blocks[0]
+    i = np.arange(1, ni + 1)
+    j = np.arange(1, nj + 1)
+    k = np.arange(1, nk + 1)
+    K, J, I = np.meshgrid(k, j, i, indexing="ij")
+    X = length * (I - 1) / (ni - 1)
+    Y = dy1 * (ratio ** (J - 1) - 1.0) / (ratio - 1.0)
+    Z = span * (K - 1) / (nk - 1)
+    idx = b.ic(I, J, K).ravel()
+    x[idx], y[idx], z[idx] = X.ravel(), Y.ravel(), Z.ravel()
+    st = freestream(phys, mach)
+    v5 = _fill_state(lay, [0], dict(gam=phys.gam, pinfl=0.0, state={0: st}), seed, noise)
+    t_inf = phys.gam * st[4] / st[0]
+    mu_inf = sutherland_mu(phys, t_inf)
+    rokinf = nut_ratio * mu_inf
+    v0 = np.zeros((7, lay.ld))
+    v0[:5] = v5
+    r = splitmix64_uniform(seed + 104729, b.nnn)
+    v0[5, b.npc:b.npc + b.nnn] = rokinf * (1.0 + noise * (2.0 * r - 1.0))
+    bnd = [Boundary(0, "i1", BC_IDD, values=(1.0, 1.0, 1.0, 0.0, 0.0)),
+           Boundary(0, "i2", BC_PRD, values=(st[4],)),
+           Boundary(0, "j1", BC_PARA), Boundary(0, "j2", BC_EXTR),
+           Boundary(0, "k1", BC_RC, partner=5), Boundary(0, "k2", BC_RC, partner=4)]
+    return Case(name, lay, phys, scheme, bnd, x, y, z, v0,
+                meta=dict(mach=mach, reynz=reynz, seed=seed, cells=tuple(cells), dy1=dy1,
+                          ratio=ratio, length=length, span=span, rokinf=rokinf,
+                          mu_inf=mu_inf, nut_ratio=nut_ratio))

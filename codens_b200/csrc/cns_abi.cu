@@ -27,6 +27,17 @@ struct cns_ctx {
   double* sa_G = nullptr;    // Spalart-Allmaras gradient face values [3][9][ld]
   double* sa_gr = nullptr;   // gradients of rho nu~ and rho [6][ld]
   double* sa_w = nullptr;    // impli2_eqt_3d scratch [15][ld]
+  // Spalart-Allmaras transport step of the fused iteration (cns_set_sa)
+  bool sa_on = false;
+  double sa_rokinf = 0., sa_roeinf = 0., sa_epsk = 1e-8;
+  const double* sa_dist = nullptr;  // the caller's wall distance (device)
+  double* sa_dv = nullptr;          // velocity gradients [9][ld]
+  double* sa_fd = nullptr;          // diffusion densities fd5x..fd6z [6][ld]
+  double* sa_ts = nullptr;          // sources ts6, ts7 [2][ld]
+  double* sa_cfke = nullptr;        // source-derivative bound [ld]
+  long long n_wall_ent = 0;
+  long long* d_wall_ents = nullptr;  // list entries of the wall boundaries
+  double* wall_par = nullptr;        // wall facet centres [3][n_wall_ent]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
   double* adj_N = nullptr;   // adjoint: linearised sweep blocks [35][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
@@ -264,6 +275,96 @@ cudaError_t jameson_dissipation(cns_ctx* c, bool first) {
   return e;
 }
 
+// the Spalart-Allmaras scratch, allocated on first use
+cudaError_t ensure_sa_step(cns_ctx* c) {
+  const size_t ld = (size_t)c->lay.ld;
+  cudaError_t e = cudaSuccess;
+  if (!c->sa_G) e = dev_alloc(c, &c->sa_G, 27 * ld, false);
+  if (e == cudaSuccess && !c->sa_gr) e = dev_alloc(c, &c->sa_gr, 6 * ld, false);
+  if (e == cudaSuccess && !c->sa_w) e = dev_alloc(c, &c->sa_w, 15 * ld, false);
+  if (e == cudaSuccess && !c->sa_dv) e = dev_alloc(c, &c->sa_dv, 9 * ld);
+  if (e == cudaSuccess && !c->sa_fd) e = dev_alloc(c, &c->sa_fd, 6 * ld);
+  if (e == cudaSuccess && !c->sa_ts) e = dev_alloc(c, &c->sa_ts, 2 * ld);
+  if (e == cudaSuccess && !c->sa_cfke) e = dev_alloc(c, &c->sa_cfke, ld);
+  return e;
+}
+
+// the flat range indc(1,1,1)..indc(ni-1,nj-1,nk-1) of block l (the whole
+// span for l = 0 is the union: first block's start to last block's end)
+void fludc_range(cns_ctx* c, int l, long long& n0, long long& n1) {
+  const Blk& F = c->lay.blks[l == 0 ? 0 : l - 1];
+  const Blk& L = c->lay.blks[l == 0 ? c->lay.blks.size() - 1 : l - 1];
+  n0 = F.npc + 1 + F.nid + F.nijd;
+  n1 = L.npc + (L.ni - 1) + (long long)(L.nj - 1) * L.nid + (long long)(L.nk - 1) * L.nijd;
+}
+
+// met_num.f90:145-790 for equat '1SA ' (kcutke 2, kfludis 2, ksecmb 2, kcmut
+// 2, kditur 2, klroe 2, kparoi 0) on the bound (ld, 7) state, after rbord:
+// turbulence ghosts; per block, in block order (met_smsa.f90:177 reads
+// txxf5x at the block-local index, so a later block sees block 1's scaled
+// densities), the velocity gradients, grad(s6/s1) and grad(s7/s1), the
+// source and the diffusion densities; their ghosts; then over every block
+// the Roe dissipation, the explicit balance, the implicit line Jacobi, the
+// clip and mut = v6 fv1.  dt is this iteration's mean-flow time step.
+// met_num.f90:628-641: met_roe2oh (Harten) when |epsroe| > tiny(1.)
+int sa_harten(const cns_ctx* c) { return fabs(c->epsroe) > 1.17549435082228751e-38 ? 1 : 0; }
+
+cudaError_t enqueue_met_num(cns_ctx* c) {
+  const cns_state_t& s = c->state;
+  const long long ld = c->lay.ld;
+  const int nb = (int)c->lay.blks.size();
+  double* fd = c->sa_fd;
+  double* const fdw[6] = {fd, fd + ld, fd + 2 * ld, fd + 3 * ld, fd + 4 * ld, fd + 5 * ld};
+  const double* const fdr[6] = {fdw[0], fdw[1], fdw[2], fdw[3], fdw[4], fdw[5]};
+  double* ts6 = c->sa_ts;
+  double* ts7 = c->sa_ts + ld;
+  cudaError_t e = launch_turb_bord(c->bd, s.v, ld, c->sa_rokinf, c->sa_roeinf, c->st);
+  for (int b = 0; b < nb && e == cudaSuccess; ++b) {
+    const Space cb = c->cells.view(b);
+    e = launch_teq_grads(c->d_blks, c->faces, cb, b, 0, 3, s.v, nullptr, ld, s.sn, s.vol,
+                         c->sa_G, c->sa_dv, c->st);
+    // met_gradtr.f90:97-104 writes the whole flat range of the real cells,
+    // zero on the ghost cells inside it (what the next block's met_smsa
+    // reads there through its block-local index)
+    long long n0, n1;
+    fludc_range(c, b + 1, n0, n1);
+    for (int q = 0; q < 6 && e == cudaSuccess; ++q)
+      e = cudaMemsetAsync(fdw[q] + n0, 0, sizeof(double) * (size_t)(n1 - n0 + 1), c->st);
+    if (e == cudaSuccess)
+      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 2, 2, s.v, nullptr, ld, s.sn, s.vol,
+                           c->sa_G, fd, c->st);
+    if (e == cudaSuccess)
+      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 1, 1, s.v, s.v + 5 * ld, ld, s.sn,
+                           s.vol, c->sa_G, c->sa_gr, c->st);
+    if (e == cudaSuccess)
+      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 1, 1, s.v, s.v, ld, s.sn, s.vol,
+                           c->sa_G, c->sa_gr + 3 * ld, c->st);
+    if (e == cudaSuccess)
+      e = launch_smsa(c->d_blks, cb, ld, s.v, s.mu, c->sa_dist, c->sa_dv, c->sa_gr,
+                      c->sa_gr + 3 * ld, fdr, ts6, ts7, c->sa_cfke, c->st);
+    if (e == cudaSuccess) e = launch_fludcsa(n0, n1, s.v + 5 * ld, s.mu, fdw, c->sigma, c->st);
+  }
+  if (e == cudaSuccess) e = launch_fd_ghosts(c->bd, fdw, c->st);
+  const Space all = c->cells.view(-1);
+  if (e == cudaSuccess)
+    e = launch_roe2o(c->d_blks, c->faces, c->cells_ext.view(-1), -1, sa_harten(c), c->epsroe,
+                     c->ph.gam, c->ph.gam1, s.v, ld, s.sn, c->w.G, s.d, c->st);
+  // sch_turb.f90:59-66 zeroes u(:,6:7) over every block
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(s.u + 5 * ld, 0, sizeof(double) * c->lay.ncells, c->st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(s.u + 6 * ld, 0, sizeof(double) * c->lay.ncells, c->st);
+  if (e == cudaSuccess)
+    e = launch_sch_turb(c->d_blks, c->faces, all, -1, s.v, ld, fdr, ts6, ts7, s.d, s.sn, s.vol,
+                        c->w.G, s.u, c->st);
+  if (e == cudaSuccess)
+    e = launch_impli2(c->d_blks, c->faces, c->lines, all, -1, ld, s.u, s.dt, s.v, s.mu, s.mut,
+                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->st);
+  if (e == cudaSuccess) e = launch_cutsa(c->d_blks, all, s.v, ld, c->sa_epsk, c->st);
+  if (e == cudaSuccess) e = launch_samut(c->d_blks, all, s.v + 5 * ld, s.mu, s.mut, c->st);
+  return e;
+}
+
 // one pseudo-time iteration on the bound state (atsch_num.f90:245-1134 for
 // ischema = 7, kmf = 1, steady, dt recomputed every iteration; ischema <= 4:
 // the Jameson dissipation before rbord, sch_jameson for the residual)
@@ -281,6 +382,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first) {
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
+  if (e == cudaSuccess && c->sa_on) e = enqueue_met_num(c);
   if (e == cudaSuccess) e = launch_prim(0, c->lay.ncells, s.v, ld, c->w.prim, c->st);
   if (e == cudaSuccess && c->sc.ns) {
     e = launch_grad(c->d_blks, all, c->ph, s.v, c->w.prim, ld, s.mu, s.mut, s.tau, s.sn,
@@ -329,8 +431,8 @@ cudaError_t ensure_mixed(cns_ctx* c) {
   return e;
 }
 
-// one reduced-precision iteration on the bound state.  kMixed: FP64 residual,
-// FP32 sweeps (precision 1).  kDefectRefresh / kDefectRegular (precision 2):
+// one reduced-precision iteration on the bound state.  kMixed: FP64 residual
+// (face fluxes with FMA contraction), FP32 sweeps (precision 1).  kDefectRefresh / kDefectRegular (precision 2):
 // FP32 face fluxes; the refresh iteration also evaluates the FP64 residual,
 // advances with it and stores corr = R64 - R32 for the regular iterations.
 enum MixedMode { kMixed, kDefectRefresh, kDefectRegular };
@@ -351,6 +453,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
+  if (e == cudaSuccess && c->sa_on) e = enqueue_met_num(c);
   if (e == cudaSuccess)
     e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression, w.v32, w.prim32,
                            w.ps32, c->st);
@@ -385,19 +488,19 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
       if (e == cudaSuccess && lim)
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
       if (e == cudaSuccess)
-        e = launch_face_flux(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
-                             s.pression, s.tau, s.sn, w.R, w.G, c->st);
+        e = launch_face_flux_fma(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
+                                 s.pression, s.tau, s.sn, w.R, w.G, c->st);
       if (e == cudaSuccess)
         e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st);
     }
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
   }
-  // single-precision implicit sweeps, FP64 update
+  // single-precision coefficients and implicit sweeps, FP64 update
   if (e == cudaSuccess)
-    e = launch_implicit_coefficients(c->d_blks, all, c->faces, -1, c->ph, !c->sc.ns, s.dt,
-                                     s.v, w.prim, s.mu, s.mut, s.sn, s.vol, s.cson, w,
-                                     w.coefe32, w.coefdiag32, c->st);
+    e = launch_coefficients32(c->d_blks, all, c->ph, !c->sc.ns, ld, s.dt, s.v, w.prim32,
+                              s.mu, s.mut, w.sn32, s.vol, s.cson, w.coefe32, w.coefdiag32,
+                              c->st);
   int cur = 0;
   if (e == cudaSuccess)
     e = launch_sweeps_t<float>(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
@@ -605,7 +708,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     return CNS_EINVAL;
   }
   std::vector<int> ent_bnd((size_t)nl), blk0(nb);
-  std::vector<long long> idd_ents;
+  std::vector<long long> idd_ents, wall_ents;
   for (int b = 0; b < nb; ++b) {
     const int t = bnd->type[b];
     if (t < CNS_BC_EXTR || t > CNS_BC_PRD) {
@@ -628,6 +731,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     for (int m = 0; m < bnd->mmb[b]; ++m) {
       ent_bnd[(size_t)(bnd->mpb[b] + m)] = b;
       if (t == CNS_BC_IDD) idd_ents.push_back(bnd->mpb[b] + m);
+      if (t == CNS_BC_PARA) wall_ents.push_back(bnd->mpb[b] + m);
     }
     c->h_btype.push_back(t);
   }
@@ -640,6 +744,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   c->bd.nbnd = nb;
   c->bd.nlist = nl;
   c->n_idd_ent = (long long)idd_ents.size();
+  c->n_wall_ent = (long long)wall_ents.size();
   {
     int *t_, *b_, *f_, *m_, *p_, *eb_;
     long long *mpb_, *ncbd_, *ncin_;
@@ -657,6 +762,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     if (e == cudaSuccess) e = upload(c, &ncin_, (const long long*)bnd->ncin, (size_t)nl);
     if (e == cudaSuccess) e = upload(c, &bc_, bnd->bceqt, (size_t)(5 * nl));
     if (e == cudaSuccess) e = upload(c, &c->d_idd_ents, idd_ents.data(), idd_ents.size());
+    if (e == cudaSuccess) e = upload(c, &c->d_wall_ents, wall_ents.data(), wall_ents.size());
     if (e == cudaSuccess) e = dev_alloc(c, &c->d_idd_masks, (size_t)nb);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nxn, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nyn, (size_t)nl);
@@ -901,14 +1007,6 @@ int cns_set_turbulence(cns_ctx* c, double alfak, double alfae, double sigma, dou
   return CNS_OK;
 }
 
-// the flat range indc(1,1,1)..indc(ni-1,nj-1,nk-1) of block l (the whole
-// span for l = 0 is the union: first block's start to last block's end)
-static void fludc_range(cns_ctx* c, int l, long long& n0, long long& n1) {
-  const Blk& F = c->lay.blks[l == 0 ? 0 : l - 1];
-  const Blk& L = c->lay.blks[l == 0 ? c->lay.blks.size() - 1 : l - 1];
-  n0 = F.npc + 1 + F.nid + F.nijd;
-  n1 = L.npc + (L.ni - 1) + (long long)(L.nj - 1) * L.nid + (long long)(L.nk - 1) * L.nijd;
-}
 
 int cns_met_fludc(cns_ctx* c, int l, const double* mu, const double* mut, double* fd5x,
                   double* fd5y, double* fd5z, double* fd6x, double* fd6y, double* fd6z) {
@@ -1027,6 +1125,91 @@ int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* s
 
 int cns_met_roe2oh(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
   return met_roe2o_common(c, l, t, d, sn, 1);
+}
+
+int cns_atcaldis3(cns_ctx* c, const double* x, const double* y, const double* z,
+                  double* dist) {
+  if (!c || !x || !y || !z || !dist) return CNS_EINVAL;
+  if (c->n_wall_ent == 0)
+    return fail(c, CNS_EBC, "no wall boundary to measure the distance to (atcaldis3 stops)");
+  if (!c->wall_par) CK(dev_alloc(c, &c->wall_par, (size_t)(3 * c->n_wall_ent), false));
+  CK(launch_wall_dist(c->bd, c->d_blks, c->cells.view(-1), c->d_wall_ents, c->n_wall_ent, x,
+                      y, z, c->wall_par, dist, c->st));
+  return CNS_OK;
+}
+
+int cns_met_bord(cns_ctx* c, double* v, double rokinf, double roeinf) {
+  if (!c || !v) return CNS_EINVAL;
+  CK(launch_turb_bord(c->bd, v, c->lay.ld, rokinf, roeinf, c->st));
+  return CNS_OK;
+}
+
+int cns_met_gradtr(cns_ctx* c, int l, const double* s, const double* sn, const double* vol,
+                   double* fd5x, double* fd5y, double* fd5z, double* fd6x, double* fd6y,
+                   double* fd6z) {
+  if (!c || bad_block(c, l) || !s || !sn || !vol || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y ||
+      !fd6z)
+    return CNS_EINVAL;
+  CK(ensure_sa_step(c));
+  const long long ld = c->lay.ld;
+  double* const out[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  const int b0 = l == 0 ? 0 : l - 1, b1 = l == 0 ? (int)c->lay.blks.size() : l;
+  for (int b = b0; b < b1; ++b) {
+    // met_gradtr.f90:97-104: the flat range of the real cells, ghost cells
+    // inside it included (zero there)
+    long long n0, n1;
+    fludc_range(c, b + 1, n0, n1);
+    const size_t cnt = (size_t)(n1 - n0 + 1);
+    for (int q = 0; q < 6; ++q)
+      CK(cudaMemsetAsync(c->sa_fd + q * ld + n0, 0, sizeof(double) * cnt, c->st));
+    CK(launch_teq_grads(c->d_blks, c->faces, c->cells.view(b), b, 2, 2, s, nullptr, ld, sn,
+                        vol, c->sa_G, c->sa_fd, c->st));
+    for (int q = 0; q < 6; ++q)
+      CK(cudaMemcpyAsync(out[q] + n0, c->sa_fd + q * ld + n0, sizeof(double) * cnt,
+                         cudaMemcpyDeviceToDevice, c->st));
+  }
+  return CNS_OK;
+}
+
+int cns_met_rbse(cns_ctx* c, double* fd5x, double* fd5y, double* fd5z, double* fd6x,
+                 double* fd6y, double* fd6z) {
+  if (!c || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y || !fd6z) return CNS_EINVAL;
+  double* const fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  CK(launch_fd_ghosts(c->bd, fd, c->st));
+  return CNS_OK;
+}
+
+int cns_met_cutsa(cns_ctx* c, int l, double* v, double epsk) {
+  if (!c || bad_block(c, l) || !v) return CNS_EINVAL;
+  CK(launch_cutsa(c->d_blks, c->cells.view(l - 1), v, c->lay.ld, epsk, c->st));
+  return CNS_OK;
+}
+
+int cns_set_sa(cns_ctx* c, const cns_sa_t* sa) {
+  if (!c) return CNS_EINVAL;
+  drop_graphs(c);
+  if (!sa) {
+    c->sa_on = false;
+    return CNS_OK;
+  }
+  if (!sa->dist) return CNS_EINVAL;
+  if (!c->sc.ns)
+    return fail(c, CNS_EINVAL, "the Spalart-Allmaras step needs the Navier-Stokes equations");
+  CK(ensure_sa_step(c));
+  c->sa_dist = sa->dist;
+  c->sa_rokinf = sa->rokinf;
+  c->sa_roeinf = sa->roeinf;
+  c->sa_epsk = sa->epsk;
+  c->sa_on = true;
+  return CNS_OK;
+}
+
+int cns_met_num(cns_ctx* c) {
+  if (!c) return CNS_EINVAL;
+  if (!c->bound || !c->sa_on)
+    return fail(c, CNS_ENOTREADY, "bind the state and enable the Spalart-Allmaras step first");
+  CK(enqueue_met_num(c));
+  return CNS_OK;
 }
 
 int cns_adjoint_prepare(cns_ctx* c) {
@@ -1261,7 +1444,8 @@ int cns_atsch_num_step(cns_ctx* c, int nsteps, double* norms) {
 int cns_atsch_num_step_host(cns_ctx* c, double* v_host, int nsteps, double* norms) {
   if (!c || !v_host) return CNS_EINVAL;
   if (!c->bound) return fail(c, CNS_ENOTREADY, "bind the state first");
-  const size_t bytes = sizeof(double) * 5 * (size_t)c->lay.ld;
+  // the (ld, 5) state, or (ld, 7) with the Spalart-Allmaras step
+  const size_t bytes = sizeof(double) * (c->sa_on ? 7 : 5) * (size_t)c->lay.ld;
   CK(cudaMemcpyAsync(c->state.v, v_host, bytes, cudaMemcpyHostToDevice, c->st));
   int rc = cns_atsch_num_step(c, nsteps, norms);
   if (rc) return rc;

@@ -260,8 +260,10 @@ cudaError_t launch_sch_turb(const Blk* blks, const SpaceBuf* faces, Space cells,
                             cudaStream_t st);
 
 // teq_grads over the faces of block l0 (-1: all) into out[3 nsc][ld]:
-// mode 0 = the velocity (nsc 3), mode 1 = the field f (nsc 1); G scratch
-// [3][3 nsc][ld].  met_smsa with its gradients of rho nu~ (grt) and rho (grr)
+// mode 0 = the velocity (nsc 3), mode 1 = the field f (nsc 1), mode 2 = the
+// transport variables per unit mass s6/s1, s7/s1 (nsc 2, met_gradtr); G
+// scratch [3][3 nsc][ld].  met_smsa with its gradients of rho nu~ (grt) and
+// rho (grr)
 cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
                              int mode, int nsc, const double* v, const double* f,
                              long long ld, const double* sn, const double* vol, double* G,
@@ -276,6 +278,20 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
                           double* v, const double* mu, const double* mut, const double* cfke,
                           const double* sn, const double* vol, double cmt, double* w,
                           cudaStream_t st);
+
+// wall distance of the real cells to the nearest facet centre of the nw wall
+// entries went (atcaldis3 / atdist_3); par: 3 nw scratch
+cudaError_t launch_wall_dist(const Bnd& bd, const Blk* blks, Space cells,
+                             const long long* went, long long nw, const double* x,
+                             const double* y, const double* z, double* par, double* dist,
+                             cudaStream_t st);
+// met_bord (kparoi 0) on v(:,6:7); met_rbse + met_rbsc on fd[6][ld];
+// met_cutsa on the real cells
+cudaError_t launch_turb_bord(const Bnd& bd, double* v, long long ld, double rokinf,
+                             double roeinf, cudaStream_t st);
+cudaError_t launch_fd_ghosts(const Bnd& bd, double* const fd[6], cudaStream_t st);
+cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, double epsk,
+                         cudaStream_t st);
 
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
@@ -319,6 +335,20 @@ cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t
 // corr = u64 - u_r32 on the real cells (defect correction)
 cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const double* u64,
                           const double* ur32, double* corr, cudaStream_t st);
+// the FP32 implicit coefficients (coefe32 per face, coefdiag32 per cell) of
+// the mixed sweeps in one pass over the real cells
+cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
+                                  const double* dt, const double* v, const float* prim32,
+                                  const double* mu, const double* mut, const float* sn32,
+                                  const double* vol, const double* cson, float* coefe32,
+                                  float* coefdiag32, cudaStream_t st);
+// FP64 face fluxes with FMA contraction (the mixed form's residual; agrees
+// with launch_face_flux_t<double> to FP64 rounding, not bit for bit)
+cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0, Phys ph,
+                                 Scheme sc, const double* v, const double* prim,
+                                 long long ld, const double* ps, const double* tau,
+                                 const double* sn, const double* R, double* G,
+                                 cudaStream_t st);
 
 // the implicit phase of implimf_eu (eu = 1) or implimf_3d (eu = 0) on the
 // cells of the space: coefficients, lmx Jacobi sweeps, v += d; d_out

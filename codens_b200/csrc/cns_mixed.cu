@@ -43,7 +43,88 @@ __global__ void __launch_bounds__(kTile) k_defect(const Blk* __restrict__ blks, 
   for (int a = 0; a < 5; ++a) corr[a * ld + n] = u64[a * ld + n] - ur32[a * ld + n];
 }
 
+// spectral radius of the face between cells nh (upper side) and nl; rvh, rvl
+// the viscous factors (zero off the real cells, as the reference's zeroed rv)
+template <bool EU>
+__device__ __forceinline__ float face_coef(const float* __restrict__ prim, long long ld,
+                                           const double* __restrict__ vol,
+                                           const double* __restrict__ cson, long long nh,
+                                           long long nl, float sx, float sy, float sz,
+                                           float rvh, float rvl) {
+  const float cnds = sx * sx + sy * sy + sz * sz;
+  const float cc = 0.5f * ((float)cson[nh] + (float)cson[nl]);
+  const float uu = 0.5f * (prim[nh] + prim[nl]);
+  const float vv = 0.5f * (prim[ld + nh] + prim[ld + nl]);
+  const float ww = 0.5f * (prim[2 * ld + nh] + prim[2 * ld + nl]);
+  const float vn = uu * sx + vv * sy + ww * sz;
+  if (EU) return 0.5f * fabsf(vn) + sqrtf(cnds) * cc;
+  return 0.5f * (fabsf(vn) + sqrtf(cnds) * cc) +
+         (rvh + rvl) * cnds / (float)(vol[nh] + vol[nl]);
+}
+
+// the implicit coefficients of the FP32 sweeps in one pass (the FP32 form of
+// implimf_3d.f90:111-203 / implimf_eu.f90:124-170): each real cell evaluates
+// the spectral radii of its six faces, stores the lower faces (and the upper
+// one at the end of each line) and sums the diagonal in the reference order.
+// Every interior face is evaluated by both its cells (cheaper than a second
+// pass over memory).
+template <bool EU>
+__global__ void __launch_bounds__(kTile) k_coef32(
+    const Blk* __restrict__ blks, Space sp, Phys ph, long long ld,
+    const double* __restrict__ dt, const double* __restrict__ v,
+    const float* __restrict__ prim, const double* __restrict__ mu,
+    const double* __restrict__ mut, const float* __restrict__ sn,
+    const double* __restrict__ vol, const double* __restrict__ cson,
+    float* __restrict__ coefe, float* __restrict__ coefdiag) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  const float gp = (float)(ph.gam / ph.pr), gpt = (float)(ph.gam / ph.prt);
+  auto rv_of = [&](long long m, bool real) -> float {
+    if (EU || !real) return 0.f;
+    return (gp * (float)mu[m] + gpt * (float)mut[m]) / (float)v[m];
+  };
+  const float rv0 = rv_of(n, true);
+  float cd = (float)(vol[n] / dt[n]);
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long inc = ninc_of(B, dir);
+    const int nd = nd_of(B, dir);
+    const int p = dir == 0 ? i : (dir == 1 ? j : k);
+    const float* s0 = sn_ptr(sn, B, dir, 0);
+    const float* s1 = sn_ptr(sn, B, dir, 1);
+    const float* s2 = sn_ptr(sn, B, dir, 2);
+    const long long nl = n - inc, nu = n + inc;
+    const float cel = face_coef<EU>(prim, ld, vol, cson, n, nl, s0[n], s1[n], s2[n], rv0,
+                                    rv_of(nl, p > 1));
+    const float ceu = face_coef<EU>(prim, ld, vol, cson, nu, n, s0[nu], s1[nu], s2[nu],
+                                    rv_of(nu, p < nd - 1), rv0);
+    coefe[(long long)dir * ld + n] = cel;
+    if (p == nd - 1) coefe[(long long)dir * ld + nu] = ceu;
+    cd = cd + cel + ceu;
+  }
+  coefdiag[n] = cd;
+}
+
 }  // namespace
+
+cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
+                                  const double* dt, const double* v, const float* prim32,
+                                  const double* mu, const double* mut, const float* sn32,
+                                  const double* vol, const double* cson, float* coefe32,
+                                  float* coefdiag32, cudaStream_t st) {
+  if (cells.ntiles == 0) return cudaSuccess;
+  if (eu)
+    k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dt, v, prim32, mu,
+                                                     mut, sn32, vol, cson, coefe32,
+                                                     coefdiag32);
+  else
+    k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dt, v, prim32, mu,
+                                                      mut, sn32, vol, cson, coefe32,
+                                                      coefdiag32);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t st) {
   if (n > 0) k_to_float<<<(int)((n + 255) / 256), 256, 0, st>>>(a, b, n);
@@ -84,6 +165,28 @@ cudaError_t launch_face_flux_t<float>(const Blk* blks, const SpaceBuf* faces, in
     else
       k_face_flux<float, false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
                                                                ld, ps, tau, sn, R, G);
+  }
+  return cudaGetLastError();
+}
+
+// the FP64 face fluxes of the mixed form: the parity kernel compiled in this
+// translation unit, i.e. with FMA contraction (each a*b+c rounded once).  The
+// result differs from the bit-exact residual by FP64 rounding only, and the
+// fused multiply-adds cut the FP64 instruction count of the Roe/viscous flux.
+cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0, Phys ph,
+                                 Scheme sc, const double* v, const double* prim,
+                                 long long ld, const double* ps, const double* tau,
+                                 const double* sn, const double* R, double* G,
+                                 cudaStream_t st) {
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = faces[dir].view(l0);
+    if (sp.ntiles == 0) continue;
+    if (sc.ns)
+      k_face_flux<double, true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                               prim, ld, ps, tau, sn, R, G);
+    else
+      k_face_flux<double, false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                                prim, ld, ps, tau, sn, R, G);
   }
   return cudaGetLastError();
 }

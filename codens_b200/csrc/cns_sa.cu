@@ -29,11 +29,14 @@ __device__ __forceinline__ double pow6(double x) {  // gcc's x**6: x3 * x3
 }
 
 // scalar q of cell n: mode 0 = the velocity component q (teq_gradv.f90:
-// t(:,q+1) / max(t(:,1), 1e-20)), mode 1 = the field f
+// t(:,q+1) / max(t(:,1), 1e-20)), mode 1 = the field f, mode 2 = the
+// transport variable q per unit mass (met_gradtr.f90:78-84: s(:,6+q) / s(:,1))
 __device__ __forceinline__ double scalar_of(int mode, const double* __restrict__ v,
                                             const double* __restrict__ f, long long ld,
                                             long long n, int q) {
-  return mode == 0 ? v[(q + 1) * ld + n] / fmax(v[n], 1.e-20) : f[n];
+  if (mode == 0) return v[(q + 1) * ld + n] / fmax(v[n], 1.e-20);
+  if (mode == 2) return v[(5 + q) * ld + n] / v[n];
+  return f[n];
 }
 
 template <int NSC>
@@ -292,7 +295,174 @@ __global__ void __launch_bounds__(kTile) k_i2_update(const Blk* __restrict__ blk
   v[6 * ld + n] = v[6 * ld + n] + w7[n];
 }
 
+// ---------------------------------------------------------------------------
+// wall distance (atcaldis3.f90 -> atdist_3.f90, every block attached to every
+// wall): facet centres of the adiabatic-wall boundaries (atccfp.f90:60-72) in
+// boundary list order, then per real cell the cell centre (atccc.f90:36-60)
+// and the smallest squared distance to a facet centre.  The facet centres are
+// staged through shared memory in chunks, every thread of the CTA scanning
+// the same chunk; the minimum of a set is order-free, so dist is bit-exact.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_wall_facets(Bnd bd, const Blk* __restrict__ blks,
+                                                    const long long* __restrict__ went,
+                                                    long long nw, const double* __restrict__ x,
+                                                    const double* __restrict__ y,
+                                                    const double* __restrict__ z,
+                                                    double* __restrict__ par) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nw) return;
+  const long long e = went[q];
+  const int bb = bd.ent_bnd[e];
+  const Blk& B = blks[bd.blk[bb]];
+  const int face = bd.face[bb], dir = face / 2;
+  const long long dm1 = dir == 0 ? (long long)B.nid : 1LL;
+  const long long dm2 = dir == 2 ? (long long)B.nid : B.nijd;
+  const long long nci = bd.ncin[e] + ((face & 1) ? ninc_of(B, dir) : 0LL);
+  par[q] = (x[nci] + x[nci + dm1] + x[nci + dm2] + x[nci + dm1 + dm2]) * .25;
+  par[nw + q] = (y[nci] + y[nci + dm1] + y[nci + dm2] + y[nci + dm1 + dm2]) * .25;
+  par[2 * nw + q] = (z[nci] + z[nci + dm1] + z[nci + dm2] + z[nci + dm1 + dm2]) * .25;
+}
+
+constexpr int kWallChunk = 1024;
+
+__global__ void __launch_bounds__(kTile) k_wall_dist(const Blk* __restrict__ blks, Space sp,
+                                                     const double* __restrict__ x,
+                                                     const double* __restrict__ y,
+                                                     const double* __restrict__ z,
+                                                     const double* __restrict__ par,
+                                                     long long nw, double* __restrict__ dist) {
+  __shared__ double sx[kWallChunk], sy[kWallChunk], sz[kWallChunk];
+  int b, i, j, k;
+  const bool live = space_elem(sp, threadIdx.x, b, i, j, k);
+  double xcc = 0., ycc = 0., zcc = 0.;
+  long long n = 0;
+  if (live) {
+    const Blk& B = blks[b];
+    n = cell_index(B, i, j, k);
+    const long long a = 1, bj = B.nid, n1 = n + B.nijd;
+    xcc = ((x[n] + x[n + a] + x[n + bj] + x[n + a + bj]) +
+           (x[n1] + x[n1 + a] + x[n1 + bj] + x[n1 + a + bj])) * 0.125;
+    ycc = ((y[n] + y[n + a] + y[n + bj] + y[n + a + bj]) +
+           (y[n1] + y[n1 + a] + y[n1 + bj] + y[n1 + a + bj])) * 0.125;
+    zcc = ((z[n] + z[n + a] + z[n + bj] + z[n + a + bj]) +
+           (z[n1] + z[n1 + a] + z[n1 + bj] + z[n1 + a + bj])) * 0.125;
+  }
+  double dmini = 1.e+20;
+  for (long long f0 = 0; f0 < nw; f0 += kWallChunk) {
+    const int cnt = (int)min((long long)kWallChunk, nw - f0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      sx[q] = par[f0 + q];
+      sy[q] = par[nw + f0 + q];
+      sz[q] = par[2 * nw + f0 + q];
+    }
+    __syncthreads();
+    for (int q = 0; q < cnt; ++q) {
+      const double d2 = (xcc - sx[q]) * (xcc - sx[q]) + (ycc - sy[q]) * (ycc - sy[q]) +
+                        (zcc - sz[q]) * (zcc - sz[q]);
+      dmini = d2 < dmini ? d2 : dmini;
+    }
+  }
+  if (live) dist[n] = sqrt(dmini);
+}
+
+// met_bord.f90:24-258 (kparoi = 0) on v(:,6:7): coincident ghosts average
+// with the partner's interior cell (met_rbvc.f90:53-62), idd ghosts take
+// (rokinf, roeinf), walls 0, extrapolation and outlet the interior cell
+__global__ void __launch_bounds__(256) k_turb_bord(Bnd bd, double* v, long long ld,
+                                                  double rokinf, double roeinf) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= bd.nlist) return;
+  const int bb = bd.ent_bnd[e];
+  const long long nd = bd.ncbd[e], ni = bd.ncin[e];
+  double* v6 = v + 5 * ld;
+  double* v7 = v + 6 * ld;
+  switch (bd.type[bb]) {
+    case BC_RC: {
+      const long long nc = bd.ncin[bd.mpb[bd.partner[bb]] + (e - bd.mpb[bb])];
+      v6[nd] = 0.5 * (v6[ni] + v6[nc]);
+      v7[nd] = 0.5 * (v7[ni] + v7[nc]);
+      break;
+    }
+    case BC_IDD:
+      v6[nd] = rokinf;
+      v7[nd] = roeinf;
+      break;
+    case BC_PARA:
+      v6[nd] = 0.;
+      v7[nd] = 0.;
+      break;
+    default:
+      v6[nd] = v6[ni];
+      v7[nd] = v7[ni];
+      break;
+  }
+}
+
+// met_rbse.f90:19-31 (non-coincident boundaries: ghost = interior) and
+// met_rbsc.f90:38-70 (coincident: average with the partner's interior cell)
+// on the six diffusion densities fd (6 rows of ld)
+struct Fd6 {
+  double* p[6];
+};
+
+__global__ void __launch_bounds__(256) k_fd_ghosts(Bnd bd, Fd6 fd) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= bd.nlist) return;
+  const int bb = bd.ent_bnd[e];
+  const long long nd = bd.ncbd[e], ndm = bd.ncin[e];
+  if (bd.type[bb] == BC_RC) {
+    const long long nc = bd.ncin[bd.mpb[bd.partner[bb]] + (e - bd.mpb[bb])];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) fd.p[q][nd] = 0.5 * (fd.p[q][ndm] + fd.p[q][nc]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) fd.p[q][nd] = fd.p[q][ndm];
+  }
+}
+
+// met_cutsa.f90:35-48 on the real cells
+__global__ void __launch_bounds__(kTile) k_cutsa(const Blk* __restrict__ blks, Space sp,
+                                                 double* v, long long ld, double epsk) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  if (v[5 * ld + n] < 0.) v[5 * ld + n] = epsk;
+  v[6 * ld + n] = 0.;
+}
+
 }  // namespace
+
+cudaError_t launch_wall_dist(const Bnd& bd, const Blk* blks, Space cells,
+                             const long long* went, long long nw, const double* x,
+                             const double* y, const double* z, double* par, double* dist,
+                             cudaStream_t st) {
+  if (nw <= 0) return cudaErrorInvalidValue;
+  k_wall_facets<<<(int)((nw + 255) / 256), 256, 0, st>>>(bd, blks, went, nw, x, y, z, par);
+  if (cells.ntiles > 0)
+    k_wall_dist<<<grid_of(cells), kTile, 0, st>>>(blks, cells, x, y, z, par, nw, dist);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_turb_bord(const Bnd& bd, double* v, long long ld, double rokinf,
+                             double roeinf, cudaStream_t st) {
+  if (bd.nlist > 0)
+    k_turb_bord<<<(int)((bd.nlist + 255) / 256), 256, 0, st>>>(bd, v, ld, rokinf, roeinf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_ghosts(const Bnd& bd, double* const fd[6], cudaStream_t st) {
+  Fd6 f;
+  for (int q = 0; q < 6; ++q) f.p[q] = fd[q];
+  if (bd.nlist > 0) k_fd_ghosts<<<(int)((bd.nlist + 255) / 256), 256, 0, st>>>(bd, f);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, double epsk,
+                         cudaStream_t st) {
+  if (cells.ntiles > 0) k_cutsa<<<grid_of(cells), kTile, 0, st>>>(blks, cells, v, ld, epsk);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
                              int mode, int nsc, const double* v, const double* f,
@@ -303,12 +473,16 @@ cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells
     if (sp.ntiles == 0) continue;
     if (nsc == 3)
       k_teq_face<3><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
+    else if (nsc == 2)
+      k_teq_face<2><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
     else
       k_teq_face<1><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
   }
   if (cells.ntiles > 0) {
     if (nsc == 3)
       k_teq_acc<3><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+    else if (nsc == 2)
+      k_teq_acc<2><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
     else
       k_teq_acc<1><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
   }

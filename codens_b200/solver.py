@@ -91,9 +91,11 @@ class CodeNS:
         self.x = torch.as_tensor(case.x, **f64).contiguous()
         self.y = torch.as_tensor(case.y, **f64).contiguous()
         self.z = torch.as_tensor(case.z, **f64).contiguous()
+        # (ld, 5) conserved state, or (ld, 7) with the two transport variables
+        self.ncol = ncol = int(case.v0.shape[0])
         self.v = torch.as_tensor(case.v0.reshape(-1), **f64).contiguous()
-        self.u = torch.zeros(5 * ld, **f64)
-        self.d = torch.zeros(5 * ld, **f64)
+        self.u = torch.zeros(ncol * ld, **f64)
+        self.d = torch.zeros(ncol * ld, **f64)
         self.dt = torch.zeros(ld, **f64)
         self.sn = torch.zeros(9 * ld, **f64)
         self.vol = torch.zeros(ld, **f64)
@@ -273,6 +275,46 @@ class CodeNS:
     def impli2_eqt_3d(self, l, u, dt, v, mu, mut, cfke, sn, vol, cmt=1.0):
         self._check(self.lib.cns_impli2_eqt_3d(self.ctx, l, *(_ptr(a) for a in (
             u, dt, v, mu, mut, cfke, sn, vol)), float(cmt)), "cns_impli2_eqt_3d")
+
+    # --- the rest of the Spalart-Allmaras step (met_num.f90, 1SA) ---------
+    def atcaldis3(self, dist=None):
+        """wall distance of the real cells from this case's nodes"""
+        if dist is None:
+            dist = self.torch.zeros(self.ld, dtype=self.torch.float64, device=self.dev)
+        self._check(self.lib.cns_atcaldis3(self.ctx, _ptr(self.x), _ptr(self.y), _ptr(self.z),
+                                           _ptr(dist)), "cns_atcaldis3")
+        return dist
+
+    def met_bord(self, v, rokinf, roeinf):
+        self._check(self.lib.cns_met_bord(self.ctx, _ptr(v), rokinf, roeinf), "cns_met_bord")
+
+    def met_gradtr(self, l, s, sn, vol, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
+        self._check(self.lib.cns_met_gradtr(self.ctx, l, *map(_ptr, (s, sn, vol, fd5x, fd5y, fd5z,
+                                                                   fd6x, fd6y, fd6z))),
+                    "cns_met_gradtr")
+
+    def met_rbse(self, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
+        self._check(self.lib.cns_met_rbse(self.ctx, *map(_ptr, (fd5x, fd5y, fd5z, fd6x, fd6y,
+                                                              fd6z))), "cns_met_rbse")
+
+    def met_cutsa(self, l, v, epsk):
+        self._check(self.lib.cns_met_cutsa(self.ctx, l, _ptr(v), epsk), "cns_met_cutsa")
+
+    def set_sa(self, dist=None, rokinf=0.0, roeinf=0.0, epsk=1e-8):
+        """enable the Spalart-Allmaras step in the fused iteration (dist: the
+        wall distance, device FP64; None disables it).  The state must have
+        7 columns."""
+        if dist is None:
+            self._check(self.lib.cns_set_sa(self.ctx, None), "cns_set_sa")
+            self._sa = None
+            return
+        if self.ncol != 7:
+            raise ValueError("the Spalart-Allmaras step needs a (ld, 7) state")
+        self._sa = (dist, abi.Sa_t(C.c_void_p(dist.data_ptr()), rokinf, roeinf, epsk))
+        self._check(self.lib.cns_set_sa(self.ctx, C.byref(self._sa[1])), "cns_set_sa")
+
+    def met_num(self):
+        self._check(self.lib.cns_met_num(self.ctx), "cns_met_num")
 
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),

@@ -201,6 +201,43 @@ int cns_sch_turb(cns_ctx *ctx, int l, double *u, const double *v, const double *
                  const double *fd6x, const double *fd6y, const double *fd6z,
                  const double *ts6, const double *ts7, const double *sn, const double *vol);
 
+/* The rest of the Spalart-Allmaras transport step (met_num.f90 for equat
+ * '1SA ': kcutke 2, kfludis 2, ksecmb 2, kcmut 2, kditur 2, klroe 2 with
+ * met_roe2oh when |epsroe| > tiny, kparoi 0), bit-exact in FP64:
+ *   cns_atcaldis3   atcaldis3.f90 with the default attachment of every block
+ *                   to every wall (atdist_3.f90:34-58): dist = the distance
+ *                   from each real cell centre (atccc.f90) to the nearest
+ *                   facet centre (atccfp.f90) of the adiabatic-wall ('para')
+ *                   boundaries; x, y, z are the node coordinates in the cell
+ *                   index space; CNS_EBC when there is no wall
+ *   cns_met_bord    met_bord.f90:24-258 on v(:,6:7): coincident ghosts =
+ *                   average with the partner cell (met_rbvc), injection =
+ *                   (rokinf, roeinf), wall = 0, others = interior cell
+ *   cns_met_gradtr  met_gradtr.f90:48-130: fd5* = grad(s6/s1), fd6* =
+ *                   grad(s7/s1) (teq_grads) over the flat real-cell range
+ *   cns_met_rbse    met_rbse.f90 + met_rbsc.f90: ghost diffusion densities
+ *   cns_met_cutsa   met_cutsa.f90:35-48: s6 < 0 -> epsk, s7 = 0
+ * cns_set_sa enables the whole step in the fused iteration (after rbord,
+ * before zvisqc, as atsch_num.f90:541-559 calls met_num; the bound v, u, d
+ * must then have 7 columns); cns_met_num runs it once on the bound state.
+ * NULL disables it. */
+typedef struct {
+  const double *dist;    /* wall distance of the real cells (device, ip12) */
+  double rokinf, roeinf; /* v(:,6), v(:,7) of the injection ghosts */
+  double epsk;           /* met_cutsa floor of v(:,6) */
+} cns_sa_t;
+int cns_atcaldis3(cns_ctx *ctx, const double *x, const double *y, const double *z,
+                  double *dist);
+int cns_met_bord(cns_ctx *ctx, double *v, double rokinf, double roeinf);
+int cns_met_gradtr(cns_ctx *ctx, int l, const double *s, const double *sn, const double *vol,
+                   double *fd5x, double *fd5y, double *fd5z, double *fd6x, double *fd6y,
+                   double *fd6z);
+int cns_met_rbse(cns_ctx *ctx, double *fd5x, double *fd5y, double *fd5z, double *fd6x,
+                 double *fd6y, double *fd6z);
+int cns_met_cutsa(cns_ctx *ctx, int l, double *v, double epsk);
+int cns_set_sa(cns_ctx *ctx, const cns_sa_t *sa);
+int cns_met_num(cns_ctx *ctx);
+
 /* Discrete adjoint of the FP64 Euler Roe iteration (sch_roe_euler with
  * unlimited MUSCL + implimf_eu with qfix_dfez = 1) at the bound state, for a
  * caller that solves A^T lambda = dJ/dW (no counterpart in the reference).

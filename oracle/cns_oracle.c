@@ -2379,6 +2379,222 @@ void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, cons
   free(o6); free(o7);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Spalart-Allmaras transport step (met_num.f90 for equat '1SA ': kcutke 2,  */
+/* kfludis 2, ksecmb 2, kcmut 2, kditur 2, klroe 2, kparoi 0)                */
+/* ------------------------------------------------------------------------ */
+
+/* the wall boundaries: cl 'pa..' (adiabatic wall) -- atcaldis3.f90:51-60 */
+static int is_wall(int bb) { return G.btype[bb] == ORC_BC_PARA; }
+
+/* atindnor.f90 + atccfp.f90:56-72: node increments of a wall facet (dm1,
+ * dm2 span the face, ndm3 moves from the interior cell's lower node to the
+ * face for the upper faces i2, j2, k2) */
+static void facet_incs(const blk_t *b, int face, int64_t *dm1, int64_t *dm2, int64_t *ndm3) {
+  const int dir = face / 2, upper = face % 2;
+  if (dir == 0) { *dm1 = b->nid; *dm2 = b->nijd; }
+  else if (dir == 1) { *dm1 = 1; *dm2 = b->nijd; }
+  else { *dm1 = 1; *dm2 = b->nid; }
+  *ndm3 = upper ? NINC(b, dir) : 0;
+}
+
+/* atcaldis3.f90 with the default attachment of every block to every wall
+ * (at_lecopt: idefaut = 1, igr = jgr = kgr = 1 -> atdist_3.f90:34-58): the
+ * distance from each real cell centre (atccc.f90:36-60) to the nearest wall
+ * facet centre (atccfp.f90:60-72), brute force over the facets in boundary
+ * list order; dist = sqrt(min d^2) on the real cells */
+int orc_atcaldis3(const double *x, const double *y, const double *z, double *dist) {
+  int64_t nw = 0;
+  for (int bb = 0; bb < G.nbnd; ++bb)
+    if (is_wall(bb)) nw += G.bmmb[bb];
+  if (nw == 0) return 1;
+  double *xp = malloc(sizeof(double) * nw), *yp = malloc(sizeof(double) * nw),
+         *zp = malloc(sizeof(double) * nw);
+  int64_t q = 0;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (!is_wall(bb)) continue;
+    const blk_t *b = &G.b[G.bblk[bb] - 1];
+    int64_t dm1, dm2, ndm3;
+    facet_incs(b, G.bface[bb], &dm1, &dm2, &ndm3);
+    for (int m = 0; m < G.bmmb[bb]; ++m, ++q) {
+      const int64_t nci = G.ncin[G.bmpb[bb] + m] + ndm3;
+      xp[q] = (x[nci] + x[nci + dm1] + x[nci + dm2] + x[nci + dm1 + dm2]) * .25;
+      yp[q] = (y[nci] + y[nci + dm1] + y[nci + dm2] + y[nci + dm1 + dm2]) * .25;
+      zp[q] = (z[nci] + z[nci + dm1] + z[nci + dm2] + z[nci + dm1 + dm2]) * .25;
+    }
+  }
+  for (int l = 1; l <= G.nblk; ++l) {
+    const blk_t *b = &G.b[l - 1];
+    const int64_t a = 1, bj = b->nid, ck = b->nijd;
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          const int64_t n = IC(b, i, j, k), n1 = n + ck;
+          const double xcc = ((x[n] + x[n + a] + x[n + bj] + x[n + a + bj]) +
+                              (x[n1] + x[n1 + a] + x[n1 + bj] + x[n1 + a + bj])) * 0.125;
+          const double ycc = ((y[n] + y[n + a] + y[n + bj] + y[n + a + bj]) +
+                              (y[n1] + y[n1 + a] + y[n1 + bj] + y[n1 + a + bj])) * 0.125;
+          const double zcc = ((z[n] + z[n + a] + z[n + bj] + z[n + a + bj]) +
+                              (z[n1] + z[n1 + a] + z[n1 + bj] + z[n1 + a + bj])) * 0.125;
+          double dmini = 1.e+20;
+          for (int64_t f = 0; f < nw; ++f) {
+            const double d2 = (xcc - xp[f]) * (xcc - xp[f]) + (ycc - yp[f]) * (ycc - yp[f]) +
+                              (zcc - zp[f]) * (zcc - zp[f]);
+            if (d2 < dmini) dmini = d2;
+          }
+          dist[n] = sqrt(dmini);
+        }
+  }
+  free(xp); free(yp); free(zp);
+  return 0;
+}
+
+/* met_bord.f90:24-258 with kparoi = 0 (met_rbvc before and after: every
+ * ghost depends on interior cells only, so one pass gives the same values):
+ * coincident ghosts = average with the partner's interior cell
+ * (met_rbvc.f90:53-62), idd = (rokinf, roeinf), para = 0, extr / prd =
+ * the interior cell (met_rbve) */
+void orc_met_bord(double *v, double rokinf, double roeinf) {
+  const int64_t L = G.ld;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      const int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ni = G.ncin[mb];
+      switch (G.btype[bb]) {
+        case ORC_BC_RC: {
+          const int64_t nc = G.ncin[G.bmpb[G.bpart[bb]] + m];
+          v[5 * L + nd] = 0.5 * (v[5 * L + ni] + v[5 * L + nc]);
+          v[6 * L + nd] = 0.5 * (v[6 * L + ni] + v[6 * L + nc]);
+          break;
+        }
+        case ORC_BC_IDD:
+          v[5 * L + nd] = rokinf;
+          v[6 * L + nd] = roeinf;
+          break;
+        case ORC_BC_PARA:
+          v[5 * L + nd] = 0.;
+          v[6 * L + nd] = 0.;
+          break;
+        default:
+          v[5 * L + nd] = v[5 * L + ni];
+          v[6 * L + nd] = v[6 * L + ni];
+          break;
+      }
+    }
+  }
+}
+
+/* met_gradtr.f90:48-130: fd5 = grad(s6 / s1), fd6 = grad(s7 / s1) by
+ * teq_grads over the flat range of the real cells (ghost cells inside the
+ * range receive the zero teq_grads leaves there) */
+void orc_met_gradtr(int l, const double *sn, const double *vol, const double *s, double *fd5x,
+                    double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  double *tt = calloc((size_t)nnn, sizeof(double));
+  double *g = calloc((size_t)(3 * nnn), sizeof(double));
+  double *out[2][3] = {{fd5x, fd5y, fd5z}, {fd6x, fd6y, fd6z}};
+  int64_t n1, n2;
+  flat_real_range(b, &n1, &n2);
+  for (int q = 0; q < 2; ++q) {
+    for (int k = 0; k <= b->nk; ++k)
+      for (int j = 0; j <= b->nj; ++j)
+        for (int i = 0; i <= b->ni; ++i) {
+          const int64_t n = IC(b, i, j, k);
+          tt[n - n0] = s[(5 + q) * L + n] / s[n];
+        }
+    teq_grads(b, sn, vol, tt, g, g + nnn, g + 2 * nnn);
+    for (int64_t n = n1; n <= n2; ++n)
+      for (int c = 0; c < 3; ++c) out[q][c][n] = g[c * nnn + n - n0];
+  }
+  free(tt); free(g);
+}
+
+/* met_rbse.f90:19-31 (every non-coincident boundary: ghost = interior) and
+ * met_rbsc.f90:38-70 (coincident: average with the partner's interior
+ * cell) on the six diffusion densities */
+void orc_met_rbse(double *fd5x, double *fd5y, double *fd5z, double *fd6x, double *fd6y,
+                  double *fd6z) {
+  double *f[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  for (int bb = 0; bb < G.nbnd; ++bb)
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      const int64_t mb = G.bmpb[bb] + m, nd = G.ncbd[mb], ndm = G.ncin[mb];
+      if (G.btype[bb] == ORC_BC_RC) {
+        const int64_t nc = G.ncin[G.bmpb[G.bpart[bb]] + m];
+        for (int q = 0; q < 6; ++q) f[q][nd] = 0.5 * (f[q][ndm] + f[q][nc]);
+      } else {
+        for (int q = 0; q < 6; ++q) f[q][nd] = f[q][ndm];
+      }
+    }
+}
+
+/* met_cutsa.f90:35-48: s6 < 0 -> epsk, s7 = 0 on the real cells */
+void orc_met_cutsa(int l, double *s, double epsk) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        if (s[5 * L + n] < 0.) s[5 * L + n] = epsk;
+        s[6 * L + n] = 0.;
+      }
+}
+
+static struct {
+  int on, harten;
+  const double *dist;
+  double rokinf, roeinf, epsk, epsroe, sigma;
+  double *fd, *ts, *cfke;  /* 6 ld, 2 ld, ld */
+} SA;
+
+void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double epsk,
+                int harten, double epsroe, double sigma, double *fd, double *ts,
+                double *cfke) {
+  SA.on = on;
+  SA.dist = dist;
+  SA.rokinf = rokinf;
+  SA.roeinf = roeinf;
+  SA.epsk = epsk;
+  SA.harten = harten;
+  SA.epsroe = epsroe;
+  SA.sigma = sigma;
+  SA.fd = fd;
+  SA.ts = ts;
+  SA.cfke = cfke;
+}
+
+/* met_num.f90:145-790 for 1SA, after rbord: turbulence ghosts; per block
+ * (in block order, which met_smsa.f90:177's block-local read of txxf5x
+ * depends on) velocity gradients, grad(nu~), source, diffusion densities;
+ * their ghosts; per block Roe dissipation, explicit balance, implicit line
+ * Jacobi and the clip; mut = v6 fv1.  v, u, d are (ld, 7). */
+void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
+                 double *mut, const double *sn, const double *vol) {
+  const int64_t L = G.ld;
+  double *fd = SA.fd, *ts6 = SA.ts, *ts7 = SA.ts + L;
+  double *f5x = fd, *f5y = fd + L, *f5z = fd + 2 * L, *f6x = fd + 3 * L, *f6y = fd + 4 * L,
+         *f6z = fd + 5 * L;
+  orc_met_bord(v, SA.rokinf, SA.roeinf);
+  for (int l = 1; l <= G.nblk; ++l) {
+    const blk_t *b = &G.b[l - 1];
+    double *dv = calloc((size_t)(9 * b->nnn), sizeof(double));
+    orc_teq_gradv(l, sn, vol, v, dv);
+    orc_met_gradtr(l, sn, vol, v, f5x, f5y, f5z, f6x, f6y, f6z);
+    orc_met_smsa(l, sn, vol, v, mu, SA.dist, dv, f5x, f5y, f5z, ts6, ts7, SA.cfke);
+    orc_met_fludcsa(l, v, mu, f5x, f5y, f5z, f6x, f6y, f6z, SA.sigma);
+    free(dv);
+  }
+  orc_met_rbse(f5x, f5y, f5z, f6x, f6y, f6z);
+  for (int l = 1; l <= G.nblk; ++l) {
+    orc_met_roe2o(l, v, d, sn, SA.harten, SA.epsroe);
+    orc_sch_turb(l, u, v, d, f5x, f5y, f5z, f6x, f6y, f6z, ts6, ts7, sn, vol);
+    orc_impli2_eqt_3d(l, u, dt, v, mu, mut, SA.cfke, sn, vol, 1.0);
+    orc_met_cutsa(l, v, SA.epsk);
+  }
+  for (int l = 1; l <= G.nblk; ++l) orc_met_samut(l, v, mu, mut);
+}
+
 /* atsch_num.f90:245-1134 for ischema<=4 (Jameson, kprec=0), kmf=1, steady:
  * zpres/zvismo, chrono, rfve (first cycle only) and rfvc, dissip_jameson
  * (before rbord: the physical ghosts are the previous iteration's), rbord,
@@ -2396,6 +2612,7 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
   orc_rfvc(v, ps, temp, cson);
   for (int l = 1; l <= G.nblk; ++l) orc_dissip_jameson(l, v, dis, sn, ps, cson);
   orc_rbord(v, ps, temp, cson);
+  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol);
   if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
   for (int l = 1; l <= G.nblk; ++l) orc_sch_jameson(l, u, v, dis, tau, sn, ps);
   for (int l = 1; l <= G.nblk; ++l) {
@@ -2419,6 +2636,7 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
   }
   if (compute_dt && G.kdtl == 0) orc_chrono_global(dt);
   orc_rbord(v, ps, temp, cson);
+  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol);
   if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int l = 1; l <= G.nblk; ++l) {

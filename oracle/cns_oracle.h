@@ -144,6 +144,25 @@ void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, cons
                        const double *mut, const double *cfke, const double *sn,
                        const double *vol, double cmt);
 
+/* Spalart-Allmaras transport step: wall distance (atcaldis3 / atdist_3),
+ * turbulence ghosts (met_bord, kparoi 0), grad(s6/s1), grad(s7/s1)
+ * (met_gradtr), diffusion-density ghosts (met_rbse + met_rbsc), the clip
+ * (met_cutsa) and the whole chain (met_num for 1SA).  orc_set_sa(on, ...)
+ * makes orc_step / orc_step_jameson run met_num after rbord; fd (6 ld), ts
+ * (2 ld) and cfke (ld) are the caller's scratch. */
+int orc_atcaldis3(const double *x, const double *y, const double *z, double *dist);
+void orc_met_bord(double *v, double rokinf, double roeinf);
+void orc_met_gradtr(int l, const double *sn, const double *vol, const double *s, double *fd5x,
+                    double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
+void orc_met_rbse(double *fd5x, double *fd5y, double *fd5z, double *fd6x, double *fd6y,
+                  double *fd6z);
+void orc_met_cutsa(int l, double *s, double epsk);
+void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double epsk,
+                int harten, double epsroe, double sigma, double *fd, double *ts,
+                double *cfke);
+void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
+                 double *mut, const double *sn, const double *vol);
+
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);

@@ -71,6 +71,16 @@ def lib():
         L.orc_teq_gradv.argtypes = [C.c_int] + [_d] * 4
         L.orc_met_smsa.argtypes = [C.c_int] + [_d] * 12
         L.orc_impli2_eqt_3d.argtypes = [C.c_int] + [_d] * 8 + [C.c_double]
+        L.orc_atcaldis3.argtypes = [_d] * 4
+        L.orc_atcaldis3.restype = C.c_int
+        L.orc_met_bord.argtypes = [_d, C.c_double, C.c_double]
+        L.orc_met_gradtr.argtypes = [C.c_int] + [_d] * 9
+        L.orc_met_rbse.argtypes = [_d] * 6
+        L.orc_met_cutsa.argtypes = [C.c_int, _d, C.c_double]
+        L.orc_set_sa.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                 C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+        L.orc_met_num.argtypes = [_d] * 8
         _lib = L
     return _lib
 
@@ -87,8 +97,9 @@ class OracleState:
         self.sn = np.zeros(9 * ld)
         self.vol = np.zeros(ld)
         self.v = np.ascontiguousarray(case.v0.reshape(-1)).copy()
-        self.u = np.zeros(5 * ld)
-        self.d = np.zeros(5 * ld)
+        ncol = int(case.v0.shape[0])   # 5, or 7 with the transport variables
+        self.u = np.zeros(ncol * ld)
+        self.d = np.zeros(ncol * ld)
         self.dis = np.zeros(5 * ld)   # Jameson dissipation
         self.dt = np.zeros(ld)
         self.ps = np.zeros(ld)
@@ -115,6 +126,7 @@ class Oracle:
         L.orc_set_phys(p.gam, p.pinfl, p.pr, p.prt, p.reynz, p.suth_a, p.pa1,
                        p.aa1, p.omg)
         self.set_scheme(case.scheme)
+        self.clear_sa()
         ba = case.boundary_arrays()
         self._ba = ba
         L.orc_set_boundaries(len(ba["type"]), ba["type"], ba["blk"], ba["face"],
@@ -129,6 +141,22 @@ class Oracle:
                                   float(getattr(s, "ki4", 1.0 / 32.0)))
         self.jameson = int(getattr(s, "ischema", 7)) <= 4
         self.ncyc = 0
+
+    def set_sa(self, st: OracleState, dist, rokinf: float, roeinf: float, epsk: float = 1e-8,
+               epsroe: float = 0.0, sigma: float = 2.0 / 3.0):
+        """run the Spalart-Allmaras step (met_num, 1SA) in every iteration
+        from now on; dist: the wall distance (kept referenced here)"""
+        ld = self.case.layout.ld
+        self._sa = dict(dist=np.ascontiguousarray(dist, dtype=np.float64),
+                        fd=np.zeros(6 * ld), ts=np.zeros(2 * ld), cfke=np.zeros(ld))
+        harten = int(abs(epsroe) > 1.17549435082228751e-38)
+        a = self._sa
+        lib().orc_set_sa(1, a["dist"].ctypes.data, rokinf, roeinf, epsk, harten, epsroe, sigma,
+                         a["fd"].ctypes.data, a["ts"].ctypes.data, a["cfke"].ctypes.data)
+
+    def clear_sa(self):
+        lib().orc_set_sa(0, None, 0.0, 0.0, 0.0, 0, 0.0, 1.0, None, None, None)
+        self._sa = None
 
     def metric(self, st: OracleState):
         lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)

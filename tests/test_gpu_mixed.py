@@ -1,11 +1,12 @@
 """Reduced-precision forms of the fused iteration.
 
-precision 1 (mixed): FP64 residual, boundary conditions, update and norms,
-FP32 point-Jacobi sweeps.  Its fixed point is the FP64 steady state, so the
-converged state must agree with the FP64 one to far below FP32 rounding.
+precision 1 (mixed): FP64 residual (face fluxes with FMA contraction),
+boundary conditions, update and norms, FP32 point-Jacobi sweeps.  Its fixed
+point is the FP64 steady state, so the converged state must agree with the
+FP64 one to far below FP32 rounding.
 
 precision 2 (defect correction): FP32 face fluxes, the FP64 residual every
-kdefect iterations.  Its refresh iteration must use the exact FP64 residual.
+kdefect iterations.  Its refresh iteration must use the FP64 residual.
 """
 from __future__ import annotations
 
@@ -14,7 +15,7 @@ import pytest
 
 from codens_b200 import cases
 
-from ._helpers import SMALL, assert_equal_bits, real, state_err
+from ._helpers import SMALL, real, state_err
 
 pytestmark = pytest.mark.gpu
 
@@ -51,17 +52,26 @@ def _duct():
                               walls=False)
 
 
+def _assert_fp64_close(got, want, what):
+    # FP64 residual with fused multiply-adds against the bit-exact one:
+    # rounding-level differences, relative to each component's scale
+    scale = np.maximum(np.abs(want).max(axis=1, keepdims=True), 1e-300)
+    err = float((np.abs(got - want) / scale).max())
+    assert err < 1e-12, (what, err)
+
+
 @pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu_qfix"])
 def test_mixed_uses_fp64_residual(cuda, name):
-    """the first mixed iteration evaluates the same FP64 residual as the FP64
-    iteration (bit for bit) and moves the state by an FP32-accurate step"""
+    """the first mixed iteration evaluates the FP64 residual (its face fluxes
+    compiled with FMA contraction: the FP64 iteration's residual to FP64
+    rounding) and moves the state by an FP32-accurate step"""
     case = SMALL[name]()
     a = _solver(case, 0)
     b = _solver(SMALL[name](), 1)
     v0 = _state(a, case)
     a.atsch_num(1)
     b.atsch_num(1)
-    assert_equal_bits(_residual(b, case), _residual(a, case), "residual of the first step")
+    _assert_fp64_close(_residual(b, case), _residual(a, case), "residual of the first step")
     dv64 = _state(a, case) - v0
     dv32 = _state(b, case) - v0
     scale = np.maximum(np.abs(dv64).max(axis=1, keepdims=True), 1e-300)
@@ -76,7 +86,7 @@ def test_defect_refresh_uses_fp64_residual(cuda):
     b = _solver(SMALL["box_ns"](), 2, kdefect=3)
     a.atsch_num(1)
     b.atsch_num(1)
-    assert_equal_bits(_residual(b, case), _residual(a, case), "refresh residual")
+    _assert_fp64_close(_residual(b, case), _residual(a, case), "refresh residual")
     # the regular iterations run on R32 + corr: finite and close to FP64
     b.atsch_num(2)
     assert np.isfinite(_state(b, case)).all()

@@ -1,0 +1,261 @@
+"""GPU parity of the Spalart-Allmaras transport step (met_num.f90 for
+1SA) against the oracle: the wall distance, the turbulence ghosts, the
+transport-variable gradients, the diffusion-density ghosts and the clip bit
+for bit; the whole step and fused RANS iterations (whose source term uses
+exp and a real power, last-bit libm differences) to 1e-12."""
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+from oracle.oracle import lib as orc_lib
+
+from ._helpers import assert_equal_bits, max_rel_cols, oracle_prepared
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "plate": lambda: cases.flat_plate_case((14, 10, 4), reynz=1.0e4, dy1=2e-3, ratio=1.2,
+                                           seed=5),
+    # three blocks: coincident joins, idd, prd and walls on both sides.
+    # Unlimited MUSCL: the minmod limiter's in-place ratio recurrence is
+    # discontinuous (a 1e-14 change of the state moves the next one by
+    # ~1e-5), which would turn the last-bit libm differences of the SA source
+    # (exp, real power) into O(1e-6) state differences within two iterations
+    "channel": lambda: cases.channel_case([9, 6, 7], 8, 5, seed=13, reynz=1.0e3, ilim=0),
+}
+
+
+def _seven(case, seed=71):
+    """the case's state with seeded transport columns when it has only 5"""
+    if case.v0.shape[0] == 7:
+        return case
+    ld = case.layout.ld
+    v = np.zeros((7, ld))
+    v[:5] = case.v0
+    r = cases.splitmix64_uniform(seed, 2 * ld).reshape(2, ld)
+    v[5] = v[0] * (1e-3 + 1e-3 * r[0])
+    v[6] = v[0] * (0.1 + r[1])
+    case.v0 = v
+    case.meta["rokinf"] = 2e-3
+    return case
+
+
+def _gpu(case):
+    from codens_b200.solver import CodeNS
+    s = CodeNS(case)
+    s.metric()
+    s.sync()
+    return s
+
+
+def _t(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_atcaldis3_parity(cuda, name):
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    d_o = np.full(case.layout.ld, -1.0)
+    assert orc_lib().orc_atcaldis3(st.x, st.y, st.z, d_o) == 0
+    d_g = s.atcaldis3()
+    s.sync()
+    rc = case.layout.real_cells()
+    assert_equal_bits(d_g.cpu().numpy()[rc], d_o[rc], "dist")
+    assert (d_o[rc] > 0).all()
+    s.close()
+
+
+def test_atcaldis3_needs_a_wall(cuda):
+    from codens_b200 import abi
+    s = _gpu(cases.box_case((6, 5, 4), ns=True))
+    with pytest.raises(abi.CnsError) as ei:
+        s.atcaldis3()
+    assert ei.value.code == abi.CNS_EBC
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_bord_parity(cuda, name):
+    torch = cuda
+    case = _seven(CASES[name]())
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    v_o = st.v.copy()
+    orc_lib().orc_met_bord(v_o, 1.25e-3, 0.5)
+    vg = _t(torch, case.v0.reshape(-1))
+    s.met_bord(vg, 1.25e-3, 0.5)
+    s.sync()
+    assert_equal_bits(vg.cpu().numpy(), v_o, "v after met_bord")
+    s.close()
+
+
+def _bordered(case, st):
+    """(ld, 7) state whose ghost cells hold the mean-flow and turbulence
+    boundary values (rbord then met_bord), as met_num sees it"""
+    L = orc_lib()
+    v = st.v.copy()
+    ld = case.layout.ld
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_zpres(l, v, st.ps, st.temp, st.cson)
+    L.orc_rbord(v, st.ps, st.temp, st.cson)
+    L.orc_met_bord(v, case.meta["rokinf"], 0.0)
+    return v.reshape(7, ld)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_gradtr_parity(cuda, name):
+    torch = cuda
+    case = _seven(CASES[name]())
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    v = _bordered(case, st)
+    ld = case.layout.ld
+    L = orc_lib()
+    vg = _t(torch, v.reshape(-1))
+    for l in [0] + list(range(1, case.layout.nblk + 1)):
+        fo = np.full((6, ld), 7.0)
+        blocks = range(1, case.layout.nblk + 1) if l == 0 else [l]
+        for b in blocks:
+            L.orc_met_gradtr(b, st.sn, st.vol, v.reshape(-1), *[fo[q] for q in range(6)])
+        fg = [_t(torch, np.full(ld, 7.0)) for _ in range(6)]
+        s.met_gradtr(l, vg, s.sn, s.vol, *fg)
+        s.sync()
+        for q in range(6):
+            assert_equal_bits(fg[q].cpu().numpy(), fo[q], f"fd[{q}] (l={l})")
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_rbse_parity(cuda, name):
+    torch = cuda
+    case = CASES[name]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    fd = cases.splitmix64_uniform(73, 6 * ld).reshape(6, ld) - 0.5
+    fo = fd.copy()
+    orc_lib().orc_met_rbse(*[fo[q] for q in range(6)])
+    fg = [_t(torch, fd[q]) for q in range(6)]
+    s.met_rbse(*fg)
+    s.sync()
+    for q in range(6):
+        assert_equal_bits(fg[q].cpu().numpy(), fo[q], f"fd[{q}]")
+    s.close()
+
+
+def test_met_cutsa_parity(cuda):
+    torch = cuda
+    case = CASES["channel"]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    v = np.zeros((7, ld))
+    v[:5] = case.v0
+    r = cases.splitmix64_uniform(79, 2 * ld).reshape(2, ld)
+    v[5] = r[0] - 0.3
+    v[6] = r[1]
+    vo = v.reshape(-1).copy()
+    for b in range(1, case.layout.nblk + 1):
+        orc_lib().orc_met_cutsa(b, vo, 1e-8)
+    vg = _t(torch, v.reshape(-1))
+    s.met_cutsa(0, vg, 1e-8)
+    s.sync()
+    assert_equal_bits(vg.cpu().numpy(), vo, "v after met_cutsa")
+    s.close()
+
+
+def _sa_pair(case):
+    """oracle and GPU solver with the SA step on, from the same state and the
+    oracle's wall distance"""
+    orc, st = oracle_prepared(case)
+    dist = np.zeros(case.layout.ld)
+    assert orc_lib().orc_atcaldis3(st.x, st.y, st.z, dist) == 0
+    rok = case.meta["rokinf"]
+    orc.set_sa(st, dist, rok, 0.0)
+    s = _gpu(case)
+    dg = _t(s.torch, dist)
+    s.set_sa(dg, rok, 0.0, 1e-8)
+    return orc, st, s
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_met_num_parity(cuda, name):
+    """one transport step (met_num for 1SA) on the state after the mean-flow
+    thermodynamics, time step and boundary conditions"""
+    case = _seven(CASES[name]())
+    orc, st, s = _sa_pair(case)
+    L = orc_lib()
+    ld = case.layout.ld
+    nb = case.layout.nblk
+    for l in range(1, nb + 1):
+        L.orc_zpres(l, st.v, st.ps, st.temp, st.cson)
+        L.orc_zvismo(l, st.mu, st.temp)
+        L.orc_chronos(l, st.mu, st.mut, st.v, st.dt, st.sn, st.vol, st.cson)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    # the GPU solver on the same inputs: state and the mean-flow arrays
+    for name_, a in (("v", st.v), ("dt", st.dt), ("mu", st.mu), ("mut", st.mut),
+                     ("pression", st.ps), ("ztemp", st.temp), ("cson", st.cson)):
+        getattr(s, name_).copy_(s.torch.as_tensor(a))
+    s.torch.cuda.synchronize()
+    s.sync()
+    L.orc_met_num(st.v, st.u, st.d, st.dt, st.mu, st.mut, st.sn, st.vol)
+    s.met_num()
+    s.sync()
+    rc = case.layout.real_cells()
+    v_g = s.v.cpu().numpy().reshape(7, ld)
+    v_o = st.v.reshape(7, ld)
+    assert max_rel_cols(v_g[5:6, rc], v_o[5:6, rc]) < 1e-12
+    assert_equal_bits(v_g[:5], v_o[:5], "mean-flow columns untouched")
+    np.testing.assert_allclose(s.mut.cpu().numpy()[rc], st.mut[rc], rtol=1e-11, atol=1e-300)
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fused_rans_iterations_parity(cuda, name):
+    """fused FP64 iterations with the SA step against the oracle's
+    atsch_num + met_num sequence"""
+    case = _seven(CASES[name]())
+    orc, st, s = _sa_pair(case)
+    for _ in range(3):
+        orc.step(st)
+    s.atsch_num(3)
+    s.sync()
+    ld = case.layout.ld
+    rc = case.layout.real_cells()
+    v_g = s.v.cpu().numpy().reshape(7, ld)[:, rc]
+    v_o = st.v.reshape(7, ld)[:, rc]
+    assert max_rel_cols(v_g[:6], v_o[:6]) < 1e-11
+    np.testing.assert_allclose(s.mut.cpu().numpy()[rc], st.mut[rc], rtol=1e-10, atol=1e-300)
+    s.close()
+
+
+def test_mixed_rans_iterations(cuda):
+    """the mixed form with the SA step (FP32 mean-flow sweeps, everything
+    else FP64) stays within FP32 reach of the FP64 iteration"""
+    case = CASES["plate"]()
+    orc, st, a = _sa_pair(case)
+    case_b = CASES["plate"]()
+    case_b.scheme.precision = 1
+    from codens_b200.solver import CodeNS
+    b = CodeNS(case_b)
+    b.metric()
+    b.set_sa(b.atcaldis3(), case.meta["rokinf"], 0.0, 1e-8)
+    a.atsch_num(20)
+    b.atsch_num(20)
+    ld = case.layout.ld
+    rc = case.layout.real_cells()
+    va = a.v.cpu().numpy().reshape(7, ld)[:, rc]
+    vb = b.v.cpu().numpy().reshape(7, ld)[:, rc]
+    assert np.isfinite(vb).all()
+    assert max_rel_cols(vb[:6], va[:6]) < 1e-3
+    a.close()
+    b.close()
+
+
+def test_set_sa_needs_seven_columns(cuda):
+    s = _gpu(CASES["channel"]())
+    with pytest.raises(ValueError):
+        s.set_sa(s.vol, 1e-3, 0.0)
+    s.close()

@@ -259,3 +259,74 @@ def test_sch_turb_uniform_transport_is_source_only():
                    st.sn, st.vol)
     rc = real(case)
     np.testing.assert_allclose(u[5, rc], -st.vol[rc] * 0.25, rtol=0, atol=1e-13)
+
+
+def test_wall_distance_is_the_nearest_facet_centre():
+    """atcaldis3 against a numpy brute force over the plate's facet centres;
+    on the flat plate the nearest facet lies straight below the cell centre,
+    so the distance is the centre's height up to the facet offset"""
+    case = cases.flat_plate_case((10, 8, 3), dy1=1e-3, ratio=1.3)
+    orc, st = oracle_prepared(case)
+    dist = np.zeros(case.layout.ld)
+    assert lib().orc_atcaldis3(st.x, st.y, st.z, dist) == 0
+    b = case.layout.blocks[0]
+    I, K = np.meshgrid(np.arange(1, b.ni), np.arange(1, b.nk), indexing="ij")
+    corners = [b.ic(I + di, 1, K + dk) for di, dk in ((0, 0), (1, 0), (0, 1), (1, 1))]
+    fc = np.stack([sum(c[n] for n in corners).ravel() * 0.25 for c in (st.x, st.y, st.z)], 1)
+    rc = real(case)
+    ijk = [(i, j, k) for k in range(1, b.nk) for j in range(1, b.nj) for i in range(1, b.ni)]
+    cc = np.array([[sum(c[b.ic(i + a, j + e, k + f)] for a in (0, 1) for e in (0, 1)
+                        for f in (0, 1)) / 8.0 for c in (st.x, st.y, st.z)]
+                   for (i, j, k) in ijk])
+    ref = np.sqrt(((cc[:, None, :] - fc[None, :, :]) ** 2).sum(-1).min(1))
+    np.testing.assert_allclose(dist[rc], ref, rtol=1e-14)
+    np.testing.assert_allclose(dist[rc], cc[:, 1], rtol=1e-12)
+
+
+def test_turbulence_ghosts_follow_the_boundary_kinds():
+    """met_bord: injection ghosts take the freestream pair, walls zero,
+    outlet / extrapolation the interior cell, periodic joins the average"""
+    case = cases.flat_plate_case((6, 5, 4))
+    orc, st = oracle_prepared(case)
+    ld = case.layout.ld
+    v = st.v.copy()
+    lib().orc_met_bord(v, 0.125, 0.25)
+    v = v.reshape(7, ld)
+    ba = case.boundary_arrays()
+    for q, bd in enumerate(case.boundaries):
+        sl = slice(ba["mpb"][q], ba["mpb"][q] + ba["mmb"][q])
+        g, inn = ba["ncbd"][sl], ba["ncin"][sl]
+        if bd.kind == cases.BC_IDD:
+            assert (v[5, g] == 0.125).all() and (v[6, g] == 0.25).all()
+        elif bd.kind == cases.BC_PARA:
+            assert (v[5:, g] == 0.0).all()
+        elif bd.kind == cases.BC_RC:
+            p = bd.partner
+            pin = ba["ncin"][ba["mpb"][p]:ba["mpb"][p] + ba["mmb"][p]]
+            assert np.array_equal(v[5, g], 0.5 * (v[5, inn] + v[5, pin]))
+        else:
+            assert np.array_equal(v[5:, g], v[5:, inn])
+
+
+def test_rans_plate_runs_and_clips():
+    """a short RANS run of the plate: finite, nu~ >= epsk on the real cells
+    (met_cutsa), mut >= 0 and v(:,7) = 0, the density residual falling"""
+    case = cases.flat_plate_case((16, 10, 3), reynz=1e4, dy1=1e-3, ratio=1.25)
+    orc, st = oracle_prepared(case)
+    dist = np.zeros(case.layout.ld)
+    assert lib().orc_atcaldis3(st.x, st.y, st.z, dist) == 0
+    orc.set_sa(st, dist, case.meta["rokinf"], 0.0, epsk=1e-8)
+    rc = real(case)
+    hist = []
+    try:
+        for it in range(60):
+            v0 = st.v.copy()
+            orc.step(st)
+            hist.append(orc.norms(v0, st)[1, 0])
+    finally:
+        orc.clear_sa()
+    v = st.v.reshape(7, -1)
+    assert np.isfinite(st.v).all()
+    assert (v[5, rc] >= 1e-8).all() and (v[6, rc] == 0).all()
+    assert (st.mut[rc] >= 0).all() and st.mut[rc].max() > 0
+    assert hist[-1] < 0.2 * hist[0]
