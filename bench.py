@@ -76,7 +76,10 @@ def parse():
     p.add_argument("--no-fp64-arm", action="store_true",
                    help="skip timing the plain FP64 iteration beside the mixed one")
     p.add_argument("--no-steady-check", action="store_true")
-    p.add_argument("--workload", default="channel", choices=["channel", "batch", "adjoint"],
+    p.add_argument("--rans-iters", type=int, default=3000,
+                   help="rans workload: iterations of the convergence history")
+    p.add_argument("--workload", default="channel",
+                   choices=["channel", "batch", "adjoint", "rans"],
                    help="channel: the 8-block NS channel; batch: 64 independent Euler boxes "
                         "in one launch against the same boxes one at a time")
     p.add_argument("--tiles", default=None,
@@ -617,6 +620,97 @@ def run_adjoint(args):
     return 0
 
 
+def run_rans(args):
+    """RANS Spalart-Allmaras flat plate (configuration 3 form): one block of
+    256x128x64 cells, wall spacing 1e-5 growing by 1.1, Mach 0.3, Re 1e6,
+    freestream nu~ = 3 nu, the SA transport step (met_num) in every fused
+    iteration; wall distance once in FP64 on the device.  Mixed (headline)
+    and FP64 iterations are timed; the mixed run then continues for
+    --rans-iters iterations to report the residual drop."""
+    import torch
+    from codens_b200 import cases
+    from codens_b200.solver import CodeNS
+
+    torch.cuda.set_device(0)
+    warm = max(args.warmup, 3)
+    steps = args.steps
+
+    def timed(s, k):
+        s.sync()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(s.stream)
+        s.atsch_num_launch(k)
+        e.record(s.stream)
+        e.synchronize()
+        return a.elapsed_time(e)
+
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        case = cases.flat_plate_case(lmax=args.lmax)
+        case.scheme.precision = prec
+        nreal = case.layout.nreal
+        s = CodeNS(case)
+        s.metric()
+        s.sync()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(s.stream)
+        dist = s.atcaldis3()
+        e.record(s.stream)
+        e.synchronize()
+        ms_dist = a.elapsed_time(e)
+        s.set_sa(dist, case.meta["rokinf"], 0.0, 1e-8)
+        first = s.atsch_num(1)[1, 0]
+        s.atsch_num(warm - 1)
+        ms = timed(s, steps)
+        # the transport step alone (met_num on the bound state)
+        s.sync()
+        a.record(s.stream)
+        for _ in range(5):
+            s.met_num()
+        e.record(s.stream)
+        e.synchronize()
+        ms_sa = a.elapsed_time(e) / 5
+        rec = {"value": nreal * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
+               "sa_step_ms": ms_sa, "wall_distance_ms": ms_dist,
+               "kernels_launched": s.kernels_launched}
+        if name == "mixed":
+            hist = []
+            n = args.rans_iters
+            chunk = max(1, n // 10)
+            done = 0
+            while done < n:
+                k = min(chunk, n - done)
+                hist.append((warm + steps + 5 + done + k, float(s.atsch_num(k)[1, 0])))
+                done += k
+            rec["l2_rho_first"] = float(first)
+            rec["l2_rho_history"] = hist
+            rec["l2_drop"] = hist[-1][1] / float(first) if hist else None
+            v = s.v.view(7, -1)
+            rc = torch.as_tensor(case.layout.real_cells(), device=s.dev)
+            rec["mut_over_mu_max"] = float((s.mut[rc] / s.mu[rc]).max())
+            rec["finite"] = bool(torch.isfinite(v).all())
+        out[name] = rec
+        s.close()
+    line = {
+        "metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": steps, "warmup": warm, "ms_per_step": out["mixed"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPE["mixed"], "data": "synthetic (uniform freestream start)",
+        "config": {"workload": "RANS Spalart-Allmaras flat plate, one block 256x128x64, "
+                               "wall spacing 1e-5 ratio 1.1, Mach 0.3, Re 1e6, nu~ = 3 nu, "
+                               f"Roe-MUSCL + viscous, lmax={args.lmax}, met_num every "
+                               "iteration",
+                   "cells": nreal, "eta": case.scheme.eta,
+                   "l2_flush": "inputs larger than L2 (~2 GB of state and scratch)"},
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -625,6 +719,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "rans":
+        return run_rans(args)
     return run_ours(args)
 
 

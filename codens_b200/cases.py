@@ -432,7 +432,7 @@ def sutherland_mu(phys: Phys, temp: float) -> float:
 def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e6,
                     dy1: float = 1.0e-5, ratio: float = 1.1, length: float = 1.0,
                     span: float = 0.1, nut_ratio: float = 3.0, seed: int = 3,
-                    noise: float = 0.01, lmax: int = 10, eta: float = 5.0,
+                    noise: float = 0.0, lmax: int = 10, eta: float = 5.0,
                     name: str = "flat_plate") -> Case:
     """RANS flat plate: one block of cells[0] x cells[1] x cells[2] cells.
 
@@ -441,10 +441,14 @@ def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e
     ratio), z uniform over ``span``.  Boundaries: idd at i1 (freestream total
     pressure / temperature along +x), prd at i2 (freestream static
     pressure), para (adiabatic wall) at j1, extr at j2, periodic k.  The
-    state has 7 columns: the noisy freestream and the Spalart-Allmaras
-    variable rho nu~ = nut_ratio * mu_inf (v(:,7) = 0), as met_inisa.f90
-    leaves it for a uniform mut.  meta['rokinf'] is the freestream rho nu~
-    the injection ghosts take (met_bord.f90:60-63).
+    state has 7 columns: the freestream (uniform unless ``noise`` > 0) and
+    the Spalart-Allmaras variable rho nu~ = nut_ratio * mu_inf (v(:,7) = 0),
+    as met_inisa.f90 leaves it for a uniform mut.  meta['rokinf'] is the
+    freestream rho nu~ the injection ghosts take (met_bord.f90:60-63).
+    A seeded +-1% noise on a 3-D plate (several cells across the span) makes
+    the SA iteration unstable at the wall cells (the density of single wall
+    cells grows until the state is not finite), in the oracle and on the
+    GPU alike; the uniform start converges.
     """
     ni, nj, nk = (c + 1 for c in cells)
     lay = Layout.from_dims([(ni, nj, nk)])

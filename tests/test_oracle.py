@@ -311,7 +311,7 @@ def test_turbulence_ghosts_follow_the_boundary_kinds():
 def test_rans_plate_runs_and_clips():
     """a short RANS run of the plate: finite, nu~ >= epsk on the real cells
     (met_cutsa), mut >= 0 and v(:,7) = 0, the density residual falling"""
-    case = cases.flat_plate_case((16, 10, 3), reynz=1e4, dy1=1e-3, ratio=1.25)
+    case = cases.flat_plate_case((16, 10, 3), reynz=1e4, dy1=1e-3, ratio=1.25, noise=0.01)
     orc, st = oracle_prepared(case)
     dist = np.zeros(case.layout.ld)
     assert lib().orc_atcaldis3(st.x, st.y, st.z, dist) == 0
