@@ -24,9 +24,8 @@ struct cns_ctx {
   SpaceBuf cells, faces[3], lines[3];
   SpaceBuf cells_ext;  // i 0..ni, j 0..nj, k 0..nk (met_roe2o's zeroed range)
   double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
-  double* sa_G = nullptr;    // Spalart-Allmaras gradient face values [3][9][ld]
   double* sa_gr = nullptr;   // gradients of rho nu~ and rho [6][ld]
-  double* sa_w = nullptr;    // impli2_eqt_3d scratch [15][ld]
+  double* sa_w = nullptr;    // impli2_eqt_3d scratch [17][ld]
   // Spalart-Allmaras transport step of the fused iteration (cns_set_sa)
   bool sa_on = false;
   double sa_rokinf = 0., sa_roeinf = 0., sa_epsk = 1e-8;
@@ -279,9 +278,8 @@ cudaError_t jameson_dissipation(cns_ctx* c, bool first) {
 cudaError_t ensure_sa_step(cns_ctx* c) {
   const size_t ld = (size_t)c->lay.ld;
   cudaError_t e = cudaSuccess;
-  if (!c->sa_G) e = dev_alloc(c, &c->sa_G, 27 * ld, false);
-  if (e == cudaSuccess && !c->sa_gr) e = dev_alloc(c, &c->sa_gr, 6 * ld, false);
-  if (e == cudaSuccess && !c->sa_w) e = dev_alloc(c, &c->sa_w, 15 * ld, false);
+  if (!c->sa_gr) e = dev_alloc(c, &c->sa_gr, 6 * ld, false);
+  if (e == cudaSuccess && !c->sa_w) e = dev_alloc(c, &c->sa_w, 17 * ld, false);
   if (e == cudaSuccess && !c->sa_dv) e = dev_alloc(c, &c->sa_dv, 9 * ld);
   if (e == cudaSuccess && !c->sa_fd) e = dev_alloc(c, &c->sa_fd, 6 * ld);
   if (e == cudaSuccess && !c->sa_ts) e = dev_alloc(c, &c->sa_ts, 2 * ld);
@@ -321,8 +319,7 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
   cudaError_t e = launch_turb_bord(c->bd, s.v, ld, c->sa_rokinf, c->sa_roeinf, c->st);
   for (int b = 0; b < nb && e == cudaSuccess; ++b) {
     const Space cb = c->cells.view(b);
-    e = launch_teq_grads(c->d_blks, c->faces, cb, b, 0, 3, s.v, nullptr, ld, s.sn, s.vol,
-                         c->sa_G, c->sa_dv, c->st);
+    e = launch_teq_grads(c->d_blks, cb, 0, 3, s.v, nullptr, ld, s.sn, s.vol, c->sa_dv, c->st);
     // met_gradtr.f90:97-104 writes the whole flat range of the real cells,
     // zero on the ghost cells inside it (what the next block's met_smsa
     // reads there through its block-local index)
@@ -331,14 +328,13 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
     for (int q = 0; q < 6 && e == cudaSuccess; ++q)
       e = cudaMemsetAsync(fdw[q] + n0, 0, sizeof(double) * (size_t)(n1 - n0 + 1), c->st);
     if (e == cudaSuccess)
-      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 2, 2, s.v, nullptr, ld, s.sn, s.vol,
-                           c->sa_G, fd, c->st);
+      e = launch_teq_grads(c->d_blks, cb, 2, 2, s.v, nullptr, ld, s.sn, s.vol, fd, c->st);
     if (e == cudaSuccess)
-      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 1, 1, s.v, s.v + 5 * ld, ld, s.sn,
-                           s.vol, c->sa_G, c->sa_gr, c->st);
+      e = launch_teq_grads(c->d_blks, cb, 1, 1, s.v, s.v + 5 * ld, ld, s.sn, s.vol, c->sa_gr,
+                           c->st);
     if (e == cudaSuccess)
-      e = launch_teq_grads(c->d_blks, c->faces, cb, b, 1, 1, s.v, s.v, ld, s.sn, s.vol,
-                           c->sa_G, c->sa_gr + 3 * ld, c->st);
+      e = launch_teq_grads(c->d_blks, cb, 1, 1, s.v, s.v, ld, s.sn, s.vol, c->sa_gr + 3 * ld,
+                           c->st);
     if (e == cudaSuccess)
       e = launch_smsa(c->d_blks, cb, ld, s.v, s.mu, c->sa_dist, c->sa_dv, c->sa_gr,
                       c->sa_gr + 3 * ld, fdr, ts6, ts7, c->sa_cfke, c->st);
@@ -1072,8 +1068,7 @@ int cns_sch_turb(cns_ctx* c, int l, double* u, const double* v, const double* d,
 
 static cudaError_t ensure_sa(cns_ctx* c) {
   cudaError_t e = cudaSuccess;
-  if (!c->sa_G) e = dev_alloc(c, &c->sa_G, (size_t)27 * c->lay.ld, false);
-  if (e == cudaSuccess && !c->sa_gr) e = dev_alloc(c, &c->sa_gr, (size_t)6 * c->lay.ld, false);
+  if (!c->sa_gr) e = dev_alloc(c, &c->sa_gr, (size_t)6 * c->lay.ld, false);
   return e;
 }
 
@@ -1081,8 +1076,8 @@ int cns_teq_gradv(cns_ctx* c, int l, const double* v, const double* sn, const do
                   double* dv) {
   if (!c || bad_block(c, l) || !v || !sn || !vol || !dv) return CNS_EINVAL;
   CK(ensure_sa(c));
-  CK(launch_teq_grads(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, 0, 3, v, nullptr,
-                      c->lay.ld, sn, vol, c->sa_G, dv, c->st));
+  CK(launch_teq_grads(c->d_blks, c->cells.view(l - 1), 0, 3, v, nullptr, c->lay.ld, sn, vol,
+                      dv, c->st));
   return CNS_OK;
 }
 
@@ -1097,10 +1092,8 @@ int cns_met_smsa(cns_ctx* c, int l, const double* v, const double* mu, const dou
   const long long ld = c->lay.ld;
   const Space cells = c->cells.view(l - 1);
   // met_difsa: grad(rho nu~); met_smsa: grad(rho)
-  CK(launch_teq_grads(c->d_blks, c->faces, cells, l - 1, 1, 1, v, v + 5 * ld, ld, sn, vol,
-                      c->sa_G, c->sa_gr, c->st));
-  CK(launch_teq_grads(c->d_blks, c->faces, cells, l - 1, 1, 1, v, v, ld, sn, vol, c->sa_G,
-                      c->sa_gr + 3 * ld, c->st));
+  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v + 5 * ld, ld, sn, vol, c->sa_gr, c->st));
+  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v, ld, sn, vol, c->sa_gr + 3 * ld, c->st));
   const double* fd5[3] = {fd5x, fd5y, fd5z};
   CK(launch_smsa(c->d_blks, cells, ld, v, mu, dist, dv, c->sa_gr, c->sa_gr + 3 * ld, fd5, ts6,
                  ts7, cfke, c->st));
@@ -1113,7 +1106,7 @@ int cns_impli2_eqt_3d(cns_ctx* c, int l, const double* u, const double* dt, doub
   if (!c || bad_block(c, l) || !u || !dt || !v || !mu || !mut || !cfke || !sn || !vol ||
       !(cmt != 0.))
     return CNS_EINVAL;
-  if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)15 * c->lay.ld, false));
+  if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)17 * c->lay.ld, false));
   CK(launch_impli2(c->d_blks, c->faces, c->lines, c->cells.view(l - 1), l - 1, c->lay.ld, u, dt,
                    v, mu, mut, cfke, sn, vol, cmt, c->sa_w, c->st));
   return CNS_OK;
@@ -1162,8 +1155,8 @@ int cns_met_gradtr(cns_ctx* c, int l, const double* s, const double* sn, const d
     const size_t cnt = (size_t)(n1 - n0 + 1);
     for (int q = 0; q < 6; ++q)
       CK(cudaMemsetAsync(c->sa_fd + q * ld + n0, 0, sizeof(double) * cnt, c->st));
-    CK(launch_teq_grads(c->d_blks, c->faces, c->cells.view(b), b, 2, 2, s, nullptr, ld, sn,
-                        vol, c->sa_G, c->sa_fd, c->st));
+    CK(launch_teq_grads(c->d_blks, c->cells.view(b), 2, 2, s, nullptr, ld, sn, vol, c->sa_fd,
+                        c->st));
     for (int q = 0; q < 6; ++q)
       CK(cudaMemcpyAsync(out[q] + n0, c->sa_fd + q * ld + n0, sizeof(double) * cnt,
                          cudaMemcpyDeviceToDevice, c->st));

@@ -3,12 +3,12 @@
 // the gradients of rho nu~ and rho inside met_difsa.f90 / met_smsa.f90) and
 // the source term met_smsa.f90 with its derivative bound.
 //
-// Gradient: one thread per face computes the face value S (s_upper +
-// s_lower) (interior) or (2 S) s_ghost (boundary) of every scalar into the
-// face buffer, then one thread per real cell sums its faces in the
-// reference's order -- directions k, j, i; within a direction the lower face
-// subtracted then the upper added, the first cell of a line (lower face on
-// the boundary) taking its upper face first -- and multiplies by 0.5 / vol.
+// Gradient: one thread per real cell evaluates the face values S (s_upper +
+// s_lower) (interior) or (2 S) s_ghost (boundary) of its six faces and sums
+// them in the reference's order -- directions k, j, i; within a direction
+// the lower face subtracted then the upper added, the first cell of a line
+// (lower face on the boundary) taking its upper face first -- and
+// multiplies by 0.5 / vol.
 // FP64, --fmad=false: bit-identical gradients.  The source uses exp and a
 // real power, whose last bit may differ from the host libm's.
 #include "cns_kernels.cuh"
@@ -39,46 +39,28 @@ __device__ __forceinline__ double scalar_of(int mode, const double* __restrict__
   return f[n];
 }
 
+// teq_grads.f90:38-346 per real cell: the Green-Gauss sum over the six faces
+// in the reference's order -- directions k, j, i; within a direction the
+// lower face subtracted then the upper one added, except that the first cell
+// of a line (lower face on the boundary) takes its upper face first -- then
+// times 0.5 / vol.  A face value is S (s_upper + s_lower) inside the block
+// and (S * 2) s_ghost on a boundary face; every cell evaluates its six face
+// values itself (the face's two cells compute the same operands in the same
+// order, so the value is the one a stored face buffer would hold).
 template <int NSC>
-__global__ void __launch_bounds__(kTile) k_teq_face(const Blk* __restrict__ blks, Space sp,
-                                                    int dir, int mode,
-                                                    const double* __restrict__ v,
+__global__ void __launch_bounds__(kTile) k_teq_cell(const Blk* __restrict__ blks, Space sp,
+                                                    int mode, const double* __restrict__ v,
                                                     const double* __restrict__ f, long long ld,
                                                     const double* __restrict__ sn,
-                                                    double* __restrict__ G) {
+                                                    const double* __restrict__ vol,
+                                                    double* __restrict__ out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const long long n = cell_index(B, i, j, k);
-  const long long inc = ninc_of(B, dir);
-  const int nd = nd_of(B, dir);
-  const int p = dir == 0 ? i : (dir == 1 ? j : k);
-  const double S[3] = {sn_ptr(sn, B, dir, 0)[n], sn_ptr(sn, B, dir, 1)[n],
-                       sn_ptr(sn, B, dir, 2)[n]};
-  double* Gd = G + (long long)dir * 3 * NSC * ld;
+  double s0[NSC];
 #pragma unroll
-  for (int q = 0; q < NSC; ++q) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double val;
-      if (p >= 2 && p <= nd - 1)
-        val = S[c] * (scalar_of(mode, v, f, ld, n, q) + scalar_of(mode, v, f, ld, n - inc, q));
-      else
-        val = S[c] * 2 * scalar_of(mode, v, f, ld, p == 1 ? n - inc : n, q);
-      Gd[(q * 3 + c) * ld + n] = val;
-    }
-  }
-}
-
-template <int NSC>
-__global__ void __launch_bounds__(kTile) k_teq_acc(const Blk* __restrict__ blks, Space sp,
-                                                   const double* __restrict__ G, long long ld,
-                                                   const double* __restrict__ vol,
-                                                   double* __restrict__ out) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
+  for (int q = 0; q < NSC; ++q) s0[q] = scalar_of(mode, v, f, ld, n, q);
   double acc[NSC * 3];
 #pragma unroll
   for (int a = 0; a < NSC * 3; ++a) acc[a] = 0.;
@@ -89,16 +71,27 @@ __global__ void __launch_bounds__(kTile) k_teq_acc(const Blk* __restrict__ blks,
     const int nd = nd_of(B, dir);
     const int p = dir == 0 ? i : (dir == 1 ? j : k);
     const bool upper_first = (p == 1) && nd >= 3;
-    const double* Gd = G + (long long)dir * 3 * NSC * ld;
+    const double* s0p = sn_ptr(sn, B, dir, 0);
+    const double* s1p = sn_ptr(sn, B, dir, 1);
+    const double* s2p = sn_ptr(sn, B, dir, 2);
+    const double Sl[3] = {s0p[n], s1p[n], s2p[n]};
+    const double Su[3] = {s0p[n + inc], s1p[n + inc], s2p[n + inc]};
 #pragma unroll
-    for (int a = 0; a < NSC * 3; ++a) {
-      const double gl = Gd[a * ld + n], gu = Gd[a * ld + n + inc];
-      if (upper_first) {
-        acc[a] = acc[a] + gu;
-        acc[a] = acc[a] - gl;
-      } else {
-        acc[a] = acc[a] - gl;
-        acc[a] = acc[a] + gu;
+    for (int q = 0; q < NSC; ++q) {
+      const double sl = scalar_of(mode, v, f, ld, n - inc, q);
+      const double su = scalar_of(mode, v, f, ld, n + inc, q);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double gl = p >= 2 ? Sl[c] * (s0[q] + sl) : Sl[c] * 2 * sl;
+        const double gu = p + 1 <= nd - 1 ? Su[c] * (su + s0[q]) : Su[c] * 2 * su;
+        double& x = acc[q * 3 + c];
+        if (upper_first) {
+          x = x + gu;
+          x = x - gl;
+        } else {
+          x = x - gl;
+          x = x + gu;
+        }
       }
     }
   }
@@ -226,59 +219,108 @@ __global__ void __launch_bounds__(kTile) k_i2_diag(const Blk* __restrict__ blks,
           ce[2 * ld + m + B.nijd];
 }
 
-// one alternating-line sweep of direction dir (impli2_eqt_3d.f90:172-291):
-// a thread per line solves the tridiagonal system along it (backward
-// recurrence into al/b6/b7, forward substitution into the new iterate); the
-// two other directions' neighbours come from the previous iterate
-__global__ void __launch_bounds__(kTile) k_i2_line(
+// one alternating-line sweep of direction dir (impli2_eqt_3d.f90:172-291),
+// in two kernels.  k_i2_rhs (a thread per real cell, fully parallel): the
+// tridiagonal coefficients ai, bi, cci of the cell and the right-hand sides
+// di6, di7, whose neighbours in the two other directions come from the
+// previous iterate.  k_i2_line (a thread per line): the backward recurrence
+// into al/b6/b7 (written over ai/bi/cci) and the forward substitution into
+// the new iterate -- the only sequential part, reading five values per cell.
+// The expressions and their order are the reference's, so the split is
+// bit-identical to evaluating everything inside the line loop.
+__global__ void __launch_bounds__(kTile) k_i2_rhs(
     const Blk* __restrict__ blks, Space sp, int dir, long long ld,
     const double* __restrict__ u, const double* __restrict__ uf,
     const double* __restrict__ ce, const double* __restrict__ cd,
-    const double* __restrict__ o6, const double* __restrict__ o7, double* __restrict__ n6,
-    double* __restrict__ n7, double* __restrict__ al, double* __restrict__ b6,
-    double* __restrict__ b7) {
+    const double* __restrict__ o6, const double* __restrict__ o7, double* __restrict__ ta,
+    double* __restrict__ tb, double* __restrict__ tc, double* __restrict__ d6,
+    double* __restrict__ d7) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const int oa = dir == 0 ? 1 : 0, ob = dir == 2 ? 1 : 2;
   const long long inc = ninc_of(B, dir), inca = ninc_of(B, oa), incb = ninc_of(B, ob);
-  const int nd = nd_of(B, dir);
   const double *ua = uf + (long long)oa * ld, *ub = uf + (long long)ob * ld,
                *ud = uf + (long long)dir * ld;
   const double *ca = ce + (long long)oa * ld, *cb = ce + (long long)ob * ld,
                *cdir = ce + (long long)dir * ld;
+  const long long m = cell_index(B, i, j, k);
+  const double td = -ua[m + inca] + ua[m] - ub[m + incb] + ub[m];
+  const double tpa = ca[m + inca] - ua[m + inca], tma = ca[m] + ua[m];
+  const double tpb = cb[m + incb] - ub[m + incb], tmb = cb[m] + ub[m];
+  d6[m] = -u[5 * ld + m] + td * o6[m] + tma * o6[m - inca] + tpa * o6[m + inca] +
+          tmb * o6[m - incb] + tpb * o6[m + incb];
+  d7[m] = -u[6 * ld + m] + td * o7[m] + tma * o7[m - inca] + tpa * o7[m + inca] +
+          tmb * o7[m - incb] + tpb * o7[m + incb];
+  ta[m] = cdir[m] + ud[m];
+  tb[m] = cd[m] + ud[m + inc] - ud[m];
+  tc[m] = -cdir[m + inc] + ud[m + inc];
+}
+
+__global__ void __launch_bounds__(kTile) k_i2_line(const Blk* __restrict__ blks, Space sp,
+                                                   int dir, double* __restrict__ al,
+                                                   double* __restrict__ b6,
+                                                   double* __restrict__ b7,
+                                                   const double* __restrict__ d6,
+                                                   const double* __restrict__ d7,
+                                                   double* __restrict__ n6,
+                                                   double* __restrict__ n7) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long inc = ninc_of(B, dir);
+  const int nd = nd_of(B, dir);
   const long long m1 = cell_index(B, i, j, k);  // the line's first cell (p = 1)
   // backward recurrence; the values at p + 1 carried (zero past the end, as
-  // the never-written ghost entries of the reference)
+  // the never-written ghost entries of the reference).  The next cell's
+  // inputs are loaded one step ahead, off the dependent chain.
   double aln = 0., b6n = 0., b7n = 0.;
+  long long m = m1 + (long long)(nd - 2) * inc;
+  double ai = al[m], bi = b6[m], cci = b7[m], e6 = d6[m], e7 = d7[m];
   for (int p = nd - 1; p >= 1; --p) {
-    const long long m = m1 + (long long)(p - 1) * inc;
-    const double td = -ua[m + inca] + ua[m] - ub[m + incb] + ub[m];
-    const double tpa = ca[m + inca] - ua[m + inca], tma = ca[m] + ua[m];
-    const double tpb = cb[m + incb] - ub[m + incb], tmb = cb[m] + ub[m];
-    const double di6 = -u[5 * ld + m] + td * o6[m] + tma * o6[m - inca] + tpa * o6[m + inca] +
-                       tmb * o6[m - incb] + tpb * o6[m + incb];
-    const double di7 = -u[6 * ld + m] + td * o7[m] + tma * o7[m - inca] + tpa * o7[m + inca] +
-                       tmb * o7[m - incb] + tpb * o7[m + incb];
-    const double ai = cdir[m] + ud[m];
-    const double bi = cd[m] + ud[m + inc] - ud[m];
-    const double cci = -cdir[m + inc] + ud[m + inc];
+    const long long mn = m - inc;
+    double ai2 = 0., bi2 = 0., cci2 = 0., e62 = 0., e72 = 0.;
+    if (p > 1) {
+      ai2 = al[mn];
+      bi2 = b6[mn];
+      cci2 = b7[mn];
+      e62 = d6[mn];
+      e72 = d7[mn];
+    }
     const double den = bi + cci * aln;
     aln = ai / den;
-    b6n = (di6 - cci * b6n) / den;
-    b7n = (di7 - cci * b7n) / den;
+    b6n = (e6 - cci * b6n) / den;
+    b7n = (e7 - cci * b7n) / den;
     al[m] = aln;
     b6[m] = b6n;
     b7[m] = b7n;
+    m = mn;
+    ai = ai2;
+    bi = bi2;
+    cci = cci2;
+    e6 = e62;
+    e7 = e72;
   }
   // forward substitution (the cell before the line's first is a ghost: 0)
   double w6 = 0., w7 = 0.;
+  m = m1;
+  double a0 = al[m], p6 = b6[m], p7 = b7[m];
   for (int p = 1; p <= nd - 1; ++p) {
-    const long long m = m1 + (long long)(p - 1) * inc;
-    w6 = al[m] * w6 + b6[m];
-    w7 = al[m] * w7 + b7[m];
+    const long long mn = m + inc;
+    double a1 = 0., q6 = 0., q7 = 0.;
+    if (p < nd - 1) {
+      a1 = al[mn];
+      q6 = b6[mn];
+      q7 = b7[mn];
+    }
+    w6 = a0 * w6 + p6;
+    w7 = a0 * w7 + p7;
     n6[m] = w6;
     n7[m] = w7;
+    m = mn;
+    a0 = a1;
+    p6 = q6;
+    p7 = q7;
   }
 }
 
@@ -464,27 +506,16 @@ cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_teq_grads(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
-                             int mode, int nsc, const double* v, const double* f,
-                             long long ld, const double* sn, const double* vol, double* G,
-                             double* out, cudaStream_t st) {
-  for (int dir = 0; dir < 3; ++dir) {
-    const Space sp = faces[dir].view(l0);
-    if (sp.ntiles == 0) continue;
-    if (nsc == 3)
-      k_teq_face<3><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
-    else if (nsc == 2)
-      k_teq_face<2><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
-    else
-      k_teq_face<1><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, mode, v, f, ld, sn, G);
-  }
+cudaError_t launch_teq_grads(const Blk* blks, Space cells, int mode, int nsc,
+                             const double* v, const double* f, long long ld, const double* sn,
+                             const double* vol, double* out, cudaStream_t st) {
   if (cells.ntiles > 0) {
     if (nsc == 3)
-      k_teq_acc<3><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+      k_teq_cell<3><<<grid_of(cells), kTile, 0, st>>>(blks, cells, mode, v, f, ld, sn, vol, out);
     else if (nsc == 2)
-      k_teq_acc<2><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+      k_teq_cell<2><<<grid_of(cells), kTile, 0, st>>>(blks, cells, mode, v, f, ld, sn, vol, out);
     else
-      k_teq_acc<1><<<grid_of(cells), kTile, 0, st>>>(blks, cells, G, ld, vol, out);
+      k_teq_cell<1><<<grid_of(cells), kTile, 0, st>>>(blks, cells, mode, v, f, ld, sn, vol, out);
   }
   return cudaGetLastError();
 }
@@ -494,10 +525,12 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
                           double* v, const double* mu, const double* mut, const double* cfke,
                           const double* sn, const double* vol, double cmt, double* w,
                           cudaStream_t st) {
-  // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7) = 15 ld
+  // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7),
+  // the right-hand sides d6, d7 = 17 ld
   double *rv = w, *cd = w + ld, *uf = w + 2 * ld, *ce = w + 5 * ld, *al = w + 8 * ld,
          *b6 = w + 9 * ld, *b7 = w + 10 * ld;
   double* it[2][2] = {{w + 11 * ld, w + 12 * ld}, {w + 13 * ld, w + 14 * ld}};
+  double *d6 = w + 15 * ld, *d7 = w + 16 * ld;
   cudaError_t e = cudaMemsetAsync(w, 0, sizeof(double) * 15 * ld, st);
   if (e != cudaSuccess) return e;
   if (cells.ntiles == 0) return cudaSuccess;
@@ -513,10 +546,11 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = lines[dir].view(l0);
     for (int sw = 0; sw < 2; ++sw) {
+      k_i2_rhs<<<grid_of(cells), kTile, 0, st>>>(blks, cells, dir, ld, u, uf, ce, cd,
+                                                 it[cur][0], it[cur][1], al, b6, b7, d6, d7);
       if (sp.ntiles > 0)
-        k_i2_line<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ld, u, uf, ce, cd, it[cur][0],
-                                                 it[cur][1], it[1 - cur][0], it[1 - cur][1], al,
-                                                 b6, b7);
+        k_i2_line<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, al, b6, b7, d6, d7,
+                                                 it[1 - cur][0], it[1 - cur][1]);
       cur = 1 - cur;
     }
   }
