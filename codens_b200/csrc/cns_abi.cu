@@ -25,7 +25,8 @@ struct cns_ctx {
   SpaceBuf cells_ext;  // i 0..ni, j 0..nj, k 0..nk (met_roe2o's zeroed range)
   double alfak = 1.0, alfae = 1.3, sigma = 2.0 / 3.0, epsroe = 0.0;  // modeleturb, schemanum
   double* sa_gr = nullptr;   // gradients of rho nu~ and rho [6][ld]
-  double* sa_w = nullptr;    // impli2_eqt_3d scratch [17][ld]
+  double* sa_sc = nullptr;   // gradient scalars (velocity, s6/s1, s7/s1) [3][ld]
+  double* sa_w = nullptr;    // impli2_eqt_3d scratch [20][ld]
   // Spalart-Allmaras transport step of the fused iteration (cns_set_sa)
   bool sa_on = false;
   double sa_rokinf = 0., sa_roeinf = 0., sa_epsk = 1e-8;
@@ -279,7 +280,8 @@ cudaError_t ensure_sa_step(cns_ctx* c) {
   const size_t ld = (size_t)c->lay.ld;
   cudaError_t e = cudaSuccess;
   if (!c->sa_gr) e = dev_alloc(c, &c->sa_gr, 6 * ld, false);
-  if (e == cudaSuccess && !c->sa_w) e = dev_alloc(c, &c->sa_w, 17 * ld, false);
+  if (e == cudaSuccess && !c->sa_sc) e = dev_alloc(c, &c->sa_sc, 3 * ld, false);
+  if (e == cudaSuccess && !c->sa_w) e = dev_alloc(c, &c->sa_w, 20 * ld, false);
   if (e == cudaSuccess && !c->sa_dv) e = dev_alloc(c, &c->sa_dv, 9 * ld);
   if (e == cudaSuccess && !c->sa_fd) e = dev_alloc(c, &c->sa_fd, 6 * ld);
   if (e == cudaSuccess && !c->sa_ts) e = dev_alloc(c, &c->sa_ts, 2 * ld);
@@ -303,7 +305,9 @@ void fludc_range(cns_ctx* c, int l, long long& n0, long long& n1) {
 // densities), the velocity gradients, grad(s6/s1) and grad(s7/s1), the
 // source and the diffusion densities; their ghosts; then over every block
 // the Roe dissipation, the explicit balance, the implicit line Jacobi, the
-// clip and mut = v6 fv1.  dt is this iteration's mean-flow time step.
+// clip and mut = v6 fv1.  dt is this iteration's mean-flow time step.  The
+// reduced-precision forms solve the line systems with one reciprocal per
+// step (same fixed point); precision 0 is the bit-exact FP64 step.
 // met_num.f90:628-641: met_roe2oh (Harten) when |epsroe| > tiny(1.)
 int sa_harten(const cns_ctx* c) { return fabs(c->epsroe) > 1.17549435082228751e-38 ? 1 : 0; }
 
@@ -319,7 +323,10 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
   cudaError_t e = launch_turb_bord(c->bd, s.v, ld, c->sa_rokinf, c->sa_roeinf, c->st);
   for (int b = 0; b < nb && e == cudaSuccess; ++b) {
     const Space cb = c->cells.view(b);
-    e = launch_teq_grads(c->d_blks, cb, 0, 3, s.v, nullptr, ld, s.sn, s.vol, c->sa_dv, c->st);
+    long long b0, b1;
+    block_range(c, b + 1, b0, b1);
+    e = launch_teq_grads(c->d_blks, cb, 0, 3, s.v, nullptr, ld, s.sn, s.vol, c->sa_dv, c->sa_sc,
+                         b0, b1, c->st);
     // met_gradtr.f90:97-104 writes the whole flat range of the real cells,
     // zero on the ghost cells inside it (what the next block's met_smsa
     // reads there through its block-local index)
@@ -328,13 +335,14 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
     for (int q = 0; q < 6 && e == cudaSuccess; ++q)
       e = cudaMemsetAsync(fdw[q] + n0, 0, sizeof(double) * (size_t)(n1 - n0 + 1), c->st);
     if (e == cudaSuccess)
-      e = launch_teq_grads(c->d_blks, cb, 2, 2, s.v, nullptr, ld, s.sn, s.vol, fd, c->st);
+      e = launch_teq_grads(c->d_blks, cb, 2, 2, s.v, nullptr, ld, s.sn, s.vol, fd, c->sa_sc, b0,
+                           b1, c->st);
     if (e == cudaSuccess)
       e = launch_teq_grads(c->d_blks, cb, 1, 1, s.v, s.v + 5 * ld, ld, s.sn, s.vol, c->sa_gr,
-                           c->st);
+                           nullptr, 0, 0, c->st);
     if (e == cudaSuccess)
       e = launch_teq_grads(c->d_blks, cb, 1, 1, s.v, s.v, ld, s.sn, s.vol, c->sa_gr + 3 * ld,
-                           c->st);
+                           nullptr, 0, 0, c->st);
     if (e == cudaSuccess)
       e = launch_smsa(c->d_blks, cb, ld, s.v, s.mu, c->sa_dist, c->sa_dv, c->sa_gr,
                       c->sa_gr + 3 * ld, fdr, ts6, ts7, c->sa_cfke, c->st);
@@ -355,7 +363,7 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
                         c->w.G, s.u, c->st);
   if (e == cudaSuccess)
     e = launch_impli2(c->d_blks, c->faces, c->lines, all, -1, ld, s.u, s.dt, s.v, s.mu, s.mut,
-                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->st);
+                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->sc.precision != 0, c->st);
   if (e == cudaSuccess) e = launch_cutsa(c->d_blks, all, s.v, ld, c->sa_epsk, c->st);
   if (e == cudaSuccess) e = launch_samut(c->d_blks, all, s.v + 5 * ld, s.mu, s.mut, c->st);
   return e;
@@ -1069,6 +1077,7 @@ int cns_sch_turb(cns_ctx* c, int l, double* u, const double* v, const double* d,
 static cudaError_t ensure_sa(cns_ctx* c) {
   cudaError_t e = cudaSuccess;
   if (!c->sa_gr) e = dev_alloc(c, &c->sa_gr, (size_t)6 * c->lay.ld, false);
+  if (e == cudaSuccess && !c->sa_sc) e = dev_alloc(c, &c->sa_sc, (size_t)3 * c->lay.ld, false);
   return e;
 }
 
@@ -1076,8 +1085,10 @@ int cns_teq_gradv(cns_ctx* c, int l, const double* v, const double* sn, const do
                   double* dv) {
   if (!c || bad_block(c, l) || !v || !sn || !vol || !dv) return CNS_EINVAL;
   CK(ensure_sa(c));
+  long long n0, n1;
+  block_range(c, l, n0, n1);
   CK(launch_teq_grads(c->d_blks, c->cells.view(l - 1), 0, 3, v, nullptr, c->lay.ld, sn, vol,
-                      dv, c->st));
+                      dv, c->sa_sc, n0, n1, c->st));
   return CNS_OK;
 }
 
@@ -1092,8 +1103,10 @@ int cns_met_smsa(cns_ctx* c, int l, const double* v, const double* mu, const dou
   const long long ld = c->lay.ld;
   const Space cells = c->cells.view(l - 1);
   // met_difsa: grad(rho nu~); met_smsa: grad(rho)
-  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v + 5 * ld, ld, sn, vol, c->sa_gr, c->st));
-  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v, ld, sn, vol, c->sa_gr + 3 * ld, c->st));
+  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v + 5 * ld, ld, sn, vol, c->sa_gr, nullptr, 0,
+                      0, c->st));
+  CK(launch_teq_grads(c->d_blks, cells, 1, 1, v, v, ld, sn, vol, c->sa_gr + 3 * ld, nullptr, 0,
+                      0, c->st));
   const double* fd5[3] = {fd5x, fd5y, fd5z};
   CK(launch_smsa(c->d_blks, cells, ld, v, mu, dist, dv, c->sa_gr, c->sa_gr + 3 * ld, fd5, ts6,
                  ts7, cfke, c->st));
@@ -1106,9 +1119,9 @@ int cns_impli2_eqt_3d(cns_ctx* c, int l, const double* u, const double* dt, doub
   if (!c || bad_block(c, l) || !u || !dt || !v || !mu || !mut || !cfke || !sn || !vol ||
       !(cmt != 0.))
     return CNS_EINVAL;
-  if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)17 * c->lay.ld, false));
+  if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)20 * c->lay.ld, false));
   CK(launch_impli2(c->d_blks, c->faces, c->lines, c->cells.view(l - 1), l - 1, c->lay.ld, u, dt,
-                   v, mu, mut, cfke, sn, vol, cmt, c->sa_w, c->st));
+                   v, mu, mut, cfke, sn, vol, cmt, c->sa_w, 0, c->st));
   return CNS_OK;
 }
 
@@ -1155,8 +1168,10 @@ int cns_met_gradtr(cns_ctx* c, int l, const double* s, const double* sn, const d
     const size_t cnt = (size_t)(n1 - n0 + 1);
     for (int q = 0; q < 6; ++q)
       CK(cudaMemsetAsync(c->sa_fd + q * ld + n0, 0, sizeof(double) * cnt, c->st));
+    long long b0, b1;
+    block_range(c, b + 1, b0, b1);
     CK(launch_teq_grads(c->d_blks, c->cells.view(b), 2, 2, s, nullptr, ld, sn, vol, c->sa_fd,
-                        c->st));
+                        c->sa_sc, b0, b1, c->st));
     for (int q = 0; q < 6; ++q)
       CK(cudaMemcpyAsync(out[q] + n0, c->sa_fd + q * ld + n0, sizeof(double) * cnt,
                          cudaMemcpyDeviceToDevice, c->st));

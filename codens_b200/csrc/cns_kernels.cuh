@@ -260,21 +260,26 @@ cudaError_t launch_sch_turb(const Blk* blks, const SpaceBuf* faces, Space cells,
                             cudaStream_t st);
 
 // teq_grads over the cells of the space into out[3 nsc][ld]: mode 0 = the
-// velocity (nsc 3), mode 1 = the field f (nsc 1), mode 2 = the transport
-// variables per unit mass s6/s1, s7/s1 (nsc 2, met_gradtr).  met_smsa with
-// its gradients of rho nu~ (grt) and rho (grr)
+// velocity (nsc 3), mode 1 = the fields f[q][ld], mode 2 = the transport
+// variables per unit mass s6/s1, s7/s1 (nsc 2, met_gradtr); modes 0 and 2
+// evaluate their scalars once into sc[nsc][ld] over the flat range [n0, n1)
+// covering the cells of the space and their ghosts.  met_smsa with its
+// gradients of rho nu~ (grt) and rho (grr)
 cudaError_t launch_teq_grads(const Blk* blks, Space cells, int mode, int nsc,
                              const double* v, const double* f, long long ld, const double* sn,
-                             const double* vol, double* out, cudaStream_t st);
+                             const double* vol, double* out, double* sc, long long n0,
+                             long long n1, cudaStream_t st);
 cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double* v,
                         const double* mu, const double* dist, const double* dv,
                         const double* grt, const double* grr, const double* const fd5[3],
                         double* ts6, double* ts7, double* cfke, cudaStream_t st);
-// impli2_eqt_3d of block l0 (-1: all): u, v are (ld, 7); w: 17 ld scratch
+// impli2_eqt_3d of block l0 (-1: all): u, v are (ld, 7); w: 20 ld scratch;
+// rcp = 1: one reciprocal per line step instead of three divisions (the
+// reduced-precision forms; not bit-exact)
 cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf* lines,
                           Space cells, int l0, long long ld, const double* u, const double* dt,
                           double* v, const double* mu, const double* mut, const double* cfke,
-                          const double* sn, const double* vol, double cmt, double* w,
+                          const double* sn, const double* vol, double cmt, double* w, int rcp,
                           cudaStream_t st);
 
 // wall distance of the real cells to the nearest facet centre of the nw wall

@@ -36,7 +36,19 @@ __device__ __forceinline__ double scalar_of(int mode, const double* __restrict__
                                             long long n, int q) {
   if (mode == 0) return v[(q + 1) * ld + n] / fmax(v[n], 1.e-20);
   if (mode == 2) return v[(5 + q) * ld + n] / v[n];
-  return f[n];
+  return f[q * ld + n];
+}
+
+// the scalars of modes 0 and 2 over the flat cell range [n0, n1) into
+// sc[q][ld], once per cell (the gradient kernel reads each six more times)
+template <int NSC>
+__global__ void __launch_bounds__(256) k_teq_scalars(int mode, const double* __restrict__ v,
+                                                    long long ld, long long n0, long long n1,
+                                                    double* __restrict__ sc) {
+  const long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= n1) return;
+#pragma unroll
+  for (int q = 0; q < NSC; ++q) sc[q * ld + n] = scalar_of(mode, v, nullptr, ld, n, q);
 }
 
 // teq_grads.f90:38-346 per real cell: the Green-Gauss sum over the six faces
@@ -257,70 +269,142 @@ __global__ void __launch_bounds__(kTile) k_i2_rhs(
   tc[m] = -cdir[m + inc] + ud[m + inc];
 }
 
-__global__ void __launch_bounds__(kTile) k_i2_line(const Blk* __restrict__ blks, Space sp,
-                                                   int dir, double* __restrict__ al,
-                                                   double* __restrict__ b6,
-                                                   double* __restrict__ b7,
-                                                   const double* __restrict__ d6,
-                                                   const double* __restrict__ d7,
-                                                   double* __restrict__ n6,
-                                                   double* __restrict__ n7) {
+// The recurrence reads the coefficients from arrays it does not write, so
+// the loads of the next kLineUnroll cells are issued while the current ones
+// are consumed (a thread walks its line alone: memory latency, not
+// bandwidth, bounds this kernel; a chunk of eight dependent division steps
+// covers an HBM round trip).  Few threads run it, so it may use up to 255
+// registers a thread for the two chunks in flight.
+constexpr int kLineUnroll = 8;
+
+// RCP: the reduced-precision forms' variant, one division per step (the
+// reciprocal of the pivot times each numerator).  The sweep only shapes the
+// pseudo-time increment, so the fixed point is unchanged; the dependent
+// chain per step shrinks from three divisions to one.
+template <bool RCP>
+__global__ void __launch_bounds__(kTile, 1) k_i2_line(const Blk* __restrict__ blks, Space sp,
+                                                      int dir, const double* __restrict__ ta,
+                                                      const double* __restrict__ tb,
+                                                      const double* __restrict__ tc,
+                                                      const double* __restrict__ d6,
+                                                      const double* __restrict__ d7,
+                                                      double* __restrict__ al,
+                                                      double* __restrict__ b6,
+                                                      double* __restrict__ b7,
+                                                      double* __restrict__ n6,
+                                                      double* __restrict__ n7) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const long long inc = ninc_of(B, dir);
-  const int nd = nd_of(B, dir);
+  const int nc = nd_of(B, dir) - 1;             // cells on the line
   const long long m1 = cell_index(B, i, j, k);  // the line's first cell (p = 1)
-  // backward recurrence; the values at p + 1 carried (zero past the end, as
-  // the never-written ghost entries of the reference).  The next cell's
-  // inputs are loaded one step ahead, off the dependent chain.
+  constexpr int U = kLineUnroll;
+  // backward recurrence over p = nc .. 1 (step q = nc - p); the values at
+  // p + 1 carried, zero past the end (the reference's never-written ghost
+  // entries)
   double aln = 0., b6n = 0., b7n = 0.;
-  long long m = m1 + (long long)(nd - 2) * inc;
-  double ai = al[m], bi = b6[m], cci = b7[m], e6 = d6[m], e7 = d7[m];
-  for (int p = nd - 1; p >= 1; --p) {
-    const long long mn = m - inc;
-    double ai2 = 0., bi2 = 0., cci2 = 0., e62 = 0., e72 = 0.;
-    if (p > 1) {
-      ai2 = al[mn];
-      bi2 = b6[mn];
-      cci2 = b7[mn];
-      e62 = d6[mn];
-      e72 = d7[mn];
+  double xa[U], xb[U], xc[U], x6[U], x7[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int p = nc - u;
+    if (p >= 1) {
+      const long long m = m1 + (long long)(p - 1) * inc;
+      xa[u] = ta[m];
+      xb[u] = tb[m];
+      xc[u] = tc[m];
+      x6[u] = d6[m];
+      x7[u] = d7[m];
     }
-    const double den = bi + cci * aln;
-    aln = ai / den;
-    b6n = (e6 - cci * b6n) / den;
-    b7n = (e7 - cci * b7n) / den;
-    al[m] = aln;
-    b6[m] = b6n;
-    b7[m] = b7n;
-    m = mn;
-    ai = ai2;
-    bi = bi2;
-    cci = cci2;
-    e6 = e62;
-    e7 = e72;
   }
-  // forward substitution (the cell before the line's first is a ghost: 0)
-  double w6 = 0., w7 = 0.;
-  m = m1;
-  double a0 = al[m], p6 = b6[m], p7 = b7[m];
-  for (int p = 1; p <= nd - 1; ++p) {
-    const long long mn = m + inc;
-    double a1 = 0., q6 = 0., q7 = 0.;
-    if (p < nd - 1) {
-      a1 = al[mn];
-      q6 = b6[mn];
-      q7 = b7[mn];
+  for (int q0 = 0; q0 < nc; q0 += U) {
+    double ya[U], yb[U], yc[U], y6[U], y7[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ya[u] = xa[u];
+      yb[u] = xb[u];
+      yc[u] = xc[u];
+      y6[u] = x6[u];
+      y7[u] = x7[u];
     }
-    w6 = a0 * w6 + p6;
-    w7 = a0 * w7 + p7;
-    n6[m] = w6;
-    n7[m] = w7;
-    m = mn;
-    a0 = a1;
-    p6 = q6;
-    p7 = q7;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int p = nc - (q0 + U + u);
+      if (p >= 1) {
+        const long long m = m1 + (long long)(p - 1) * inc;
+        xa[u] = ta[m];
+        xb[u] = tb[m];
+        xc[u] = tc[m];
+        x6[u] = d6[m];
+        x7[u] = d7[m];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int p = nc - (q0 + u);
+      if (p >= 1) {
+        const long long m = m1 + (long long)(p - 1) * inc;
+        const double den = yb[u] + yc[u] * aln;
+        if (RCP) {
+          const double r = 1. / den;
+          aln = ya[u] * r;
+          b6n = (y6[u] - yc[u] * b6n) * r;
+          b7n = (y7[u] - yc[u] * b7n) * r;
+        } else {
+          aln = ya[u] / den;
+          b6n = (y6[u] - yc[u] * b6n) / den;
+          b7n = (y7[u] - yc[u] * b7n) / den;
+        }
+        al[m] = aln;
+        b6[m] = b6n;
+        b7[m] = b7n;
+      }
+    }
+  }
+  // forward substitution over p = 1 .. nc (the cell before the line's first
+  // is a ghost: 0), the next chunk's al/b6/b7 (this thread's own stores of
+  // the backward pass) loaded ahead in the same way
+  double w6 = 0., w7 = 0.;
+  double fa[U], f6[U], f7[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int p = 1 + u;
+    if (p <= nc) {
+      const long long m = m1 + (long long)(p - 1) * inc;
+      fa[u] = al[m];
+      f6[u] = b6[m];
+      f7[u] = b7[m];
+    }
+  }
+  for (int p0 = 1; p0 <= nc; p0 += U) {
+    double ga[U], g6[U], g7[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ga[u] = fa[u];
+      g6[u] = f6[u];
+      g7[u] = f7[u];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int p = p0 + U + u;
+      if (p <= nc) {
+        const long long m = m1 + (long long)(p - 1) * inc;
+        fa[u] = al[m];
+        f6[u] = b6[m];
+        f7[u] = b7[m];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int p = p0 + u;
+      if (p <= nc) {
+        const long long m = m1 + (long long)(p - 1) * inc;
+        w6 = ga[u] * w6 + g6[u];
+        w7 = ga[u] * w7 + g7[u];
+        n6[m] = w6;
+        n7[m] = w7;
+      }
+    }
   }
 }
 
@@ -508,8 +592,21 @@ cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, 
 
 cudaError_t launch_teq_grads(const Blk* blks, Space cells, int mode, int nsc,
                              const double* v, const double* f, long long ld, const double* sn,
-                             const double* vol, double* out, cudaStream_t st) {
-  if (cells.ntiles > 0) {
+                             const double* vol, double* out, double* sc, long long n0,
+                             long long n1, cudaStream_t st) {
+  if (cells.ntiles == 0) return cudaSuccess;
+  if (mode != 1) {
+    const int g = (int)((n1 - n0 + 255) / 256);
+    if (nsc == 3)
+      k_teq_scalars<3><<<g, 256, 0, st>>>(mode, v, ld, n0, n1, sc);
+    else if (nsc == 2)
+      k_teq_scalars<2><<<g, 256, 0, st>>>(mode, v, ld, n0, n1, sc);
+    else
+      k_teq_scalars<1><<<g, 256, 0, st>>>(mode, v, ld, n0, n1, sc);
+    mode = 1;
+    f = sc;
+  }
+  {
     if (nsc == 3)
       k_teq_cell<3><<<grid_of(cells), kTile, 0, st>>>(blks, cells, mode, v, f, ld, sn, vol, out);
     else if (nsc == 2)
@@ -524,13 +621,15 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
                           Space cells, int l0, long long ld, const double* u, const double* dt,
                           double* v, const double* mu, const double* mut, const double* cfke,
                           const double* sn, const double* vol, double cmt, double* w,
-                          cudaStream_t st) {
+                          int rcp, cudaStream_t st) {
   // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7),
-  // the right-hand sides d6, d7 = 17 ld
+  // the tridiagonal coefficients ta, tb, tc and right-hand sides d6, d7 of
+  // a sweep = 20 ld
   double *rv = w, *cd = w + ld, *uf = w + 2 * ld, *ce = w + 5 * ld, *al = w + 8 * ld,
          *b6 = w + 9 * ld, *b7 = w + 10 * ld;
   double* it[2][2] = {{w + 11 * ld, w + 12 * ld}, {w + 13 * ld, w + 14 * ld}};
-  double *d6 = w + 15 * ld, *d7 = w + 16 * ld;
+  double *ta = w + 15 * ld, *tb = w + 16 * ld, *tc = w + 17 * ld, *d6 = w + 18 * ld,
+         *d7 = w + 19 * ld;
   cudaError_t e = cudaMemsetAsync(w, 0, sizeof(double) * 15 * ld, st);
   if (e != cudaSuccess) return e;
   if (cells.ntiles == 0) return cudaSuccess;
@@ -547,10 +646,13 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
     const Space sp = lines[dir].view(l0);
     for (int sw = 0; sw < 2; ++sw) {
       k_i2_rhs<<<grid_of(cells), kTile, 0, st>>>(blks, cells, dir, ld, u, uf, ce, cd,
-                                                 it[cur][0], it[cur][1], al, b6, b7, d6, d7);
-      if (sp.ntiles > 0)
-        k_i2_line<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, al, b6, b7, d6, d7,
-                                                 it[1 - cur][0], it[1 - cur][1]);
+                                                 it[cur][0], it[cur][1], ta, tb, tc, d6, d7);
+      if (sp.ntiles > 0 && rcp)
+        k_i2_line<true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al, b6,
+                                                       b7, it[1 - cur][0], it[1 - cur][1]);
+      else if (sp.ntiles > 0)
+        k_i2_line<false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al,
+                                                        b6, b7, it[1 - cur][0], it[1 - cur][1]);
       cur = 1 - cur;
     }
   }
