@@ -49,9 +49,9 @@ BYTES_JACOBI = {"fp64": 240, "mixed": 120, "defect": 120}
 PRECISION = {"fp64": 0, "mixed": 1, "defect": 2}
 DTYPE = {"fp64": "f64", "mixed": "f64 residual/update, f32 sweeps",
          "defect": "f32 fluxes/sweeps, f64 accumulate/update"}
-SWEEP_KERNEL = {"fp64": "k_jacobi<double> (point-Jacobi sweep, stored flux increments)",
-                "mixed": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)",
-                "defect": "k_jacobi_rc<float> (point-Jacobi sweep, recomputed increments)"}
+SWEEP_KERNEL = {"fp64": "k_jacobi_25d<double> (2.5D point-Jacobi sweep, recomputed increments)",
+                "mixed": "k_jacobi_25d<float> (2.5D point-Jacobi sweep, recomputed increments)",
+                "defect": "k_jacobi_25d<float> (2.5D point-Jacobi sweep, recomputed increments)"}
 # DRAM bytes per cell of one 2.5D sweep launch, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 1.18M-cell channel;
 # traffic grows with the cells processed, so a full launch is this x cells
