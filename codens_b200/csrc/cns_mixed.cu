@@ -200,17 +200,268 @@ cudaError_t launch_accumulate_t<float>(const Blk* blks, Space sp, const float* G
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// FP32 2.5D point-Jacobi sweep of the mixed forms (every sweep after the
+// first).  The tiling, the cp.async staging of plane k+2 and the one-cell
+// ring are those of k_jacobi_25d; two things differ from its FP64 form:
+//
+// * shared layout: the increment (d, f) of a staged cell is packed as four
+//   float4 quads [d0 d1 d2 d3] [d4 f0 f1 f2] [f3 f4 f5 f6] [f7 f8 - -] in
+//   quad-major arrays (quad g of point q at g * NP + q), so a cell reads a
+//   neighbour with four 128-bit loads and consecutive threads touch
+//   consecutive 16-byte words (no bank conflicts);
+// * arithmetic: the face term tn = 0.5 (Phi(U) + Phi(L)) . S is linear in
+//   the two cells' flux-increment tensors Phi (rows (d1 d2 d3), (f0 f1 f2),
+//   (f1 f4 f5), (f2 f5 f7), (f3 f6 f8)), so a cell sums Phi(nb) . (+-S/2)
+//   over its six neighbours plus Phi(self) . (S_lower - S_upper)/2 summed
+//   over the directions: 20 fused multiply-adds per neighbour instead of the
+//   two face evaluations.  The same sum in exact arithmetic (FP32 rounding
+//   differs; the sweep only shapes the increment).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Inc {
+  float d[5], f[9];
+};
+
+__device__ __forceinline__ void quad_load(const float4* __restrict__ s, int np, int q, Inc& x) {
+  const float4 a = s[q], b = s[np + q], c = s[2 * np + q], e = s[3 * np + q];
+  x.d[0] = a.x; x.d[1] = a.y; x.d[2] = a.z; x.d[3] = a.w;
+  x.d[4] = b.x; x.f[0] = b.y; x.f[1] = b.z; x.f[2] = b.w;
+  x.f[3] = c.x; x.f[4] = c.y; x.f[5] = c.z; x.f[6] = c.w;
+  x.f[7] = e.x; x.f[8] = e.y;
+}
+
+__device__ __forceinline__ void quad_store(float4* __restrict__ s, int np, int q,
+                                           const float d[5], const float f[9]) {
+  s[q] = make_float4(d[0], d[1], d[2], d[3]);
+  s[np + q] = make_float4(d[4], f[0], f[1], f[2]);
+  s[2 * np + q] = make_float4(f[3], f[4], f[5], f[6]);
+  s[3 * np + q] = make_float4(f[7], f[8], 0.f, 0.f);
+}
+
+// acc += Phi(x) . w + ce * d(x)
+__device__ __forceinline__ void phi_acc(const Inc& x, float w0, float w1, float w2, float ce,
+                                        float acc[5]) {
+  acc[0] = fmaf(x.d[1], w0, fmaf(x.d[2], w1, fmaf(x.d[3], w2, fmaf(ce, x.d[0], acc[0]))));
+  acc[1] = fmaf(x.f[0], w0, fmaf(x.f[1], w1, fmaf(x.f[2], w2, fmaf(ce, x.d[1], acc[1]))));
+  acc[2] = fmaf(x.f[1], w0, fmaf(x.f[4], w1, fmaf(x.f[5], w2, fmaf(ce, x.d[2], acc[2]))));
+  acc[3] = fmaf(x.f[2], w0, fmaf(x.f[5], w1, fmaf(x.f[7], w2, fmaf(ce, x.d[3], acc[3]))));
+  acc[4] = fmaf(x.f[3], w0, fmaf(x.f[6], w1, fmaf(x.f[8], w2, fmaf(ce, x.d[4], acc[4]))));
+}
+
+constexpr int kRawF32 = 11;  // staged inputs of one increment: d(5), rho, rho E, p, velocity
+
+template <int TI, int TJ>
+constexpr size_t sweep_f32_smem() {
+  return sizeof(float4) * 2 * 4 * (TI + 2) * (TJ + 2) +
+         sizeof(float) * 2 * kRawF32 * (TI + 2) * (TJ + 2);
+}
+
+template <bool EU, int TI, int TJ>
+__global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
+    const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
+    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ prim,
+    const float* __restrict__ ps, const float* __restrict__ sn, const float* __restrict__ coefe,
+    const float* __restrict__ coefdiag, const float* __restrict__ d_in,
+    float* __restrict__ d_out) {
+  constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ, NR = kRawF32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sq = reinterpret_cast<float4*>(smem_raw);    // [2 planes][4 quads][NP]
+  float* sraw = reinterpret_cast<float*>(sq + 2 * 4 * NP);  // [2 planes][NR][NP]
+  const int4 t = tl.tile[tl.tile0 + blockIdx.x];
+  const Blk B = blks[t.x];
+  const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+  const int i = t.y + tx, j = t.z + ty;
+  const int kbeg = t.w, kend = min(t.w + tl.kc, B.nk);
+  const bool own = i <= B.ni - 1 && j <= B.nj - 1;
+  const float gam1 = (float)ph64.gam1, pinfl = (float)ph64.pinfl;
+
+  // the increment inputs of plane kk (patch and ring) into raw buffer b;
+  // cells outside the block's real cells are zero-filled
+  auto stage = [&](int kk, int b) {
+    float* r = sraw + b * NR * NP;
+    for (int q = threadIdx.x; q < NP; q += NT) {
+      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
+                      kk <= B.nk - 1;
+      const long long m = in ? cell_index(B, ii, jj, kk) : 0;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) cp_async_elem(r + a * NP + q, d_in + a * ld + m, in);
+      cp_async_elem(r + 5 * NP + q, v + m, in);
+      cp_async_elem(r + 6 * NP + q, v + 4 * ld + m, in);
+      cp_async_elem(r + 7 * NP + q, ps + m, in);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) cp_async_elem(r + (8 + a) * NP + q, prim + a * ld + m, in);
+    }
+  };
+  // increments of the staged plane in raw buffer b into quad buffer b
+  auto fill = [&](int kk, int b) {
+    const float* r = sraw + b * NR * NP;
+    float4* s = sq + b * 4 * NP;
+    for (int q = threadIdx.x; q < NP; q += NT) {
+      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
+                      kk <= B.nk - 1;
+      float dd[5], f[9];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) dd[a] = r[a * NP + q];
+      if (in) {
+        df_diff<float, EU>(dd, r[5 * NP + q], r[6 * NP + q], r[7 * NP + q], r[8 * NP + q],
+                           r[9 * NP + q], r[10 * NP + q], gam1, pinfl, qfix, f);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 9; ++a) f[a] = 0.f;
+      }
+      quad_store(s, NP, q, dd, f);
+    }
+  };
+
+  // the own column's plane kbeg-1 (registers), and the lower k face area
+  Inc pk;
+  if (own && kbeg >= 2) {
+    cell_df<float, EU, 1>(v, prim, ps, d_in, ld, cell_index(B, i, j, kbeg - 1), gam1, pinfl,
+                          qfix, pk.d, pk.f);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) pk.d[a] = 0.f;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) pk.f[a] = 0.f;
+  }
+  float skl[3] = {0.f, 0.f, 0.f};
+  if (own) {
+    const long long n0 = cell_index(B, i, j, kbeg);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) skl[c] = sn_ptr(sn, B, 2, c)[n0];
+  }
+  stage(kbeg, kbeg & 1);
+  cp_async_commit();
+  stage(kbeg + 1, (kbeg + 1) & 1);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
+  fill(kbeg, kbeg & 1);
+  __syncthreads();
+  const int q0 = (ty + 1) * NX + tx + 1;
+  for (int k = kbeg; k < kend; ++k) {
+    // this cell's own inputs, in flight across the barrier
+    const long long n = cell_index(B, own ? i : 1, own ? j : 1, k);
+    float uu[5], si[3], siu[3], sj[3], sju[3], sku[3], cel[3], ceu[3], cd = 1.f;
+    if (own) {
+#pragma unroll
+      for (int a = 0; a < 5; ++a) uu[a] = u[a * ld + n];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        si[c] = sn_ptr(sn, B, 0, c)[n];
+        siu[c] = sn_ptr(sn, B, 0, c)[n + 1];
+        sj[c] = sn_ptr(sn, B, 1, c)[n];
+        sju[c] = sn_ptr(sn, B, 1, c)[n + B.nid];
+        sku[c] = sn_ptr(sn, B, 2, c)[n + B.nijd];
+      }
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        cel[dir] = coefe[(long long)dir * ld + n];
+        ceu[dir] = coefe[(long long)dir * ld + n + ninc_of(B, dir)];
+      }
+      cd = coefdiag[n];
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    // plane k+2's inputs go into the raw buffer plane k's used
+    stage(k + 2, k & 1);
+    cp_async_commit();
+    fill(k + 1, (k + 1) & 1);
+    __syncthreads();
+    const float4* s = sq + (k & 1) * 4 * NP;
+    const float4* su = sq + ((k + 1) & 1) * 4 * NP;
+    Inc c0, x;
+    quad_load(s, NP, q0, c0);
+    if (own) {
+      float acc[5];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) acc[a] = -uu[a];
+      const float h = 0.5f;
+      // the cell itself: Phi(c) . (sum of lower minus upper areas) / 2
+      phi_acc(c0, h * ((si[0] - siu[0]) + (sj[0] - sju[0]) + (skl[0] - sku[0])),
+              h * ((si[1] - siu[1]) + (sj[1] - sju[1]) + (skl[1] - sku[1])),
+              h * ((si[2] - siu[2]) + (sj[2] - sju[2]) + (skl[2] - sku[2])), 0.f, acc);
+      quad_load(s, NP, q0 - 1, x);
+      phi_acc(x, h * si[0], h * si[1], h * si[2], cel[0], acc);
+      quad_load(s, NP, q0 + 1, x);
+      phi_acc(x, -h * siu[0], -h * siu[1], -h * siu[2], ceu[0], acc);
+      quad_load(s, NP, q0 - NX, x);
+      phi_acc(x, h * sj[0], h * sj[1], h * sj[2], cel[1], acc);
+      quad_load(s, NP, q0 + NX, x);
+      phi_acc(x, -h * sju[0], -h * sju[1], -h * sju[2], ceu[1], acc);
+      phi_acc(pk, h * skl[0], h * skl[1], h * skl[2], cel[2], acc);
+      quad_load(su, NP, q0, x);
+      phi_acc(x, -h * sku[0], -h * sku[1], -h * sku[2], ceu[2], acc);
+      const float rc = 1.f / cd;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) d_out[a * ld + n] = acc[a] * rc;
+    }
+    pk = c0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) skl[c] = own ? sku[c] : 0.f;
+  }
+  cp_async_wait<0>();
+}
+
+template <int TI, int TJ>
+cudaError_t sweep_f32_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu, long long ld,
+                            const float* u, const float* v, const float* prim, const float* ps,
+                            const float* sn, const float* coefe, const float* coefdiag,
+                            const float* d_in, float* d_out, cudaStream_t st) {
+  constexpr size_t sm = sweep_f32_smem<TI, TJ>();
+  if (eu)
+    k_sweep_f32<true, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+  else
+    k_sweep_f32<false, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+  return cudaGetLastError();
+}
+
+template <int TI, int TJ>
+cudaError_t sweep_f32_attr() {
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_f32<true, TI, TJ>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sweep_f32_smem<TI, TJ>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_f32<false, TI, TJ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep_f32_smem<TI, TJ>());
+  return e;
+}
+
+}  // namespace
+
 template <>
 cudaError_t launch_jacobi_25d_t<float>(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
                                        long long ld, const float* u, const float* v,
                                        const float* prim, const float* ps, const float* sn,
                                        const float* coefe, const float* coefdiag,
                                        const float* d_in, float* d_out, cudaStream_t st) {
-  return jacobi_25d_dispatch<float, 1>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, coefe,
-                                       coefdiag, d_in, d_out, st);
+  if (tl.ntiles == 0) return cudaSuccess;
+#define CNS_SHAPE(A, B)                                                                   \
+  if (tl.ti == A && tl.tj == B)                                                           \
+    return sweep_f32_shape<A, B>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, coefe,   \
+                                 coefdiag, d_in, d_out, st);
+  CNS_SHAPE(32, 4)
+  CNS_SHAPE(32, 8)
+  CNS_SHAPE(16, 8)
+  CNS_SHAPE(16, 16)
+#undef CNS_SHAPE
+  return cudaErrorInvalidValue;
 }
 
-cudaError_t init_jacobi_25d_float() { return jacobi_25d_attr<float, 1>(); }
+cudaError_t init_jacobi_25d_float() {
+  cudaError_t e = sweep_f32_attr<32, 4>();
+  if (e == cudaSuccess) e = sweep_f32_attr<32, 8>();
+  if (e == cudaSuccess) e = sweep_f32_attr<16, 8>();
+  if (e == cudaSuccess) e = sweep_f32_attr<16, 16>();
+  return e;
+}
 
 // the FP32 sweeps of the mixed forms: the first per cell, the others
 // 2.5D-blocked with the increments in difference form (no stored increments)
