@@ -543,10 +543,12 @@ def run_batch(args):
 
 def run_adjoint(args):
     """adjoint / primal cost of the wall-force gradient (configuration 5
-    form): per-iteration cost at 512x256x4 cells, and the converged totals
-    (primal to L2 < 1e-12, adjoint to a 1e-10 relative residual) on a
-    128x64x4 channel, where the full size would not converge within a bench
-    run"""
+    form), in the FP64 and the mixed form (FP32 primal sweeps and FP32
+    transposed sweeps; FP64 residual and A^T lambda): per-iteration cost at
+    512x256x4 cells, and the converged totals (primal to L2 < 1e-12, adjoint
+    to a 1e-10 relative residual) on a 128x64x4 channel, where the full size
+    would not converge within a bench run"""
+    import dataclasses
     import torch
     from codens_b200 import adjoint
     from codens_b200.solver import CodeNS
@@ -554,67 +556,82 @@ def run_adjoint(args):
     torch.cuda.set_device(0)
     warm = max(args.warmup, 3)
     k = max(args.steps, 20)
-    d5 = adjoint.Design(ni=512, nj=256, nk=4)
-    case = d5.case()
-    nreal = case.layout.nreal
-    s = CodeNS(case)
-    s.metric()
-    s.atsch_num(warm)
-    s.sync()
-    a = torch.cuda.Event(enable_timing=True)
-    e = torch.cuda.Event(enable_timing=True)
-    a.record(s.stream)
-    s.atsch_num_launch(k)
-    e.record(s.stream)
-    e.synchronize()
-    ms_primal = a.elapsed_time(e) / k
-    s.close()
-    g = adjoint.WallForceGradient(d5, d5.mach, d5.alpha, d5.wall(), tol=1e30, max_iter=200,
-                                  adj_tol=0.0, adj_max=warm, check=10 ** 9)
-    t0 = time.perf_counter()
-    g.s.adjoint_prepare()
-    g.s.sync()
-    t_prep = time.perf_counter() - t0
-    _, gW, _, _ = g.value_and_partials()
-    g.solve_adjoint(gW)
-    g.adj_max = k
-    torch.cuda.synchronize()
-    a.record(g.s.stream)
-    g.solve_adjoint(gW)
-    e.record(g.s.stream)
-    e.synchronize()
-    ms_adj = a.elapsed_time(e) / k
-    g.close()
-    # converged totals on a reduced channel
-    dr = adjoint.Design(ni=128, nj=64, nk=4)
-    t0 = time.perf_counter()
-    gr = adjoint.WallForceGradient(dr, dr.mach, dr.alpha, dr.wall(), tol=1e-12,
-                                   max_iter=400000, adj_tol=1e-10, adj_max=400000, check=500)
-    torch.cuda.synchronize()
-    t_primal = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    J, gm, ga, gw = gr.gradient()
-    torch.cuda.synchronize()
-    t_adjoint = time.perf_counter() - t0
-    conv = {"cells": gr.case.layout.nreal, "primal_iters": gr.iters, "primal_l2": gr.l2,
-            "primal_s": t_primal, "adjoint_iters": gr.adj_iters,
-            "adjoint_residual": gr.adj_hist[-1] if gr.adj_hist else None,
-            "adjoint_s": t_adjoint, "adjoint_over_primal": t_adjoint / t_primal,
-            "J": J, "dJ_dmach": gm, "dJ_dalpha_deg": ga}
-    gr.close()
+    forms = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        d5 = adjoint.Design(ni=512, nj=256, nk=4, precision=prec)
+        case = d5.case()
+        nreal = case.layout.nreal
+        s = CodeNS(case)
+        s.metric()
+        s.atsch_num(warm)
+        s.sync()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(s.stream)
+        s.atsch_num_launch(k)
+        e.record(s.stream)
+        e.synchronize()
+        ms_primal = a.elapsed_time(e) / k
+        s.close()
+        g = adjoint.WallForceGradient(d5, d5.mach, d5.alpha, d5.wall(), tol=1e30, max_iter=200,
+                                      adj_tol=0.0, adj_max=warm, check=10 ** 9)
+        t0 = time.perf_counter()
+        g.s.adjoint_prepare()
+        g.s.sync()
+        t_prep = time.perf_counter() - t0
+        _, gW, _, _ = g.value_and_partials()
+        g.solve_adjoint(gW)
+        g.adj_max = k
+        torch.cuda.synchronize()
+        a.record(g.s.stream)
+        g.solve_adjoint(gW)
+        e.record(g.s.stream)
+        e.synchronize()
+        ms_adj = a.elapsed_time(e) / k
+        g.close()
+        # converged totals on a reduced channel
+        dr = adjoint.Design(ni=128, nj=64, nk=4, precision=prec)
+        t0 = time.perf_counter()
+        gr = adjoint.WallForceGradient(dr, dr.mach, dr.alpha, dr.wall(), tol=1e-12,
+                                       max_iter=400000, adj_tol=1e-10, adj_max=400000,
+                                       check=500)
+        torch.cuda.synchronize()
+        t_primal = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        J, gm, ga, gw = gr.gradient()
+        torch.cuda.synchronize()
+        t_adjoint = time.perf_counter() - t0
+        conv = {"cells": gr.case.layout.nreal, "primal_iters": gr.iters, "primal_l2": gr.l2,
+                "primal_s": t_primal, "adjoint_iters": gr.adj_iters,
+                "adjoint_residual": gr.adj_hist[-1] if gr.adj_hist else None,
+                "adjoint_s": t_adjoint, "adjoint_over_primal": t_adjoint / t_primal,
+                "J": J, "dJ_dmach": gm, "dJ_dalpha_deg": ga}
+        gr.close()
+        forms[name] = {"cells": nreal, "primal_ms_per_iter": ms_primal,
+                       "adjoint_ms_per_iter": ms_adj,
+                       "adjoint_over_primal_per_iter": ms_adj / ms_primal,
+                       "adjoint_prepare_s": t_prep, "converged_128x64x4": conv}
+    f64, mx = forms["fp64"], forms["mixed"]
     line = {
-        "metric": METRIC, "value": nreal / (ms_adj * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1,
-        "steps": k, "warmup": warm, "ms_per_step": ms_adj, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "metric": METRIC, "value": f64["cells"] / (f64["adjoint_ms_per_iter"] * 1e-3) / 1e6,
+        "unit": UNIT, "n_gpus": 1,
+        "steps": k, "warmup": warm, "ms_per_step": f64["adjoint_ms_per_iter"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
         "config": {"workload": "adjoint of the wall pressure force, Euler bump channel "
                                "512x256x4 cells (first-order Roe), one adjoint iteration "
                                "= A^T lambda + lmax transposed sweeps",
-                   "cells": nreal, "lmax": d5.lmax},
-        "primal_ms_per_iter": ms_primal,
-        "adjoint_ms_per_iter": ms_adj,
-        "adjoint_over_primal_per_iter": ms_adj / ms_primal,
-        "adjoint_prepare_s": t_prep,
-        "converged_128x64x4": conv,
+                   "cells": f64["cells"], "lmax": adjoint.Design().lmax},
+        "primal_ms_per_iter": f64["primal_ms_per_iter"],
+        "adjoint_ms_per_iter": f64["adjoint_ms_per_iter"],
+        "adjoint_over_primal_per_iter": f64["adjoint_over_primal_per_iter"],
+        "adjoint_prepare_s": f64["adjoint_prepare_s"],
+        "converged_128x64x4": f64["converged_128x64x4"],
+        "mixed": mx,
+        "mixed_gradient_vs_fp64": {
+            "dJ_dmach_rel": abs(mx["converged_128x64x4"]["dJ_dmach"] -
+                                f64["converged_128x64x4"]["dJ_dmach"]) /
+                            abs(f64["converged_128x64x4"]["dJ_dmach"])},
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -62,6 +62,8 @@ class Design:
     lmax: int = 10
     eta: float = 5.0
     muscl: int = 0           # 0: first-order reconstruction, 1: kappa = -1 MUSCL
+    precision: int = 0       # 0 FP64; 1 mixed: FP32 primal sweeps and FP32 transposed
+                             # sweeps of the adjoint (FP64 residual and A^T lambda)
 
     def wall(self) -> np.ndarray:
         """lower-wall height of every node column (ni + 1 values)"""
@@ -78,6 +80,7 @@ class Design:
         c.scheme.ns = 0
         c.scheme.qfix_dfez = 1
         c.scheme.muscl = self.muscl
+        c.scheme.precision = self.precision
         return c
 
 

@@ -39,8 +39,8 @@ struct cns_ctx {
   long long* d_wall_ents = nullptr;  // list entries of the wall boundaries
   double* wall_par = nullptr;        // wall facet centres [3][n_wall_ent]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
-  double* adj_N = nullptr;   // adjoint: linearised sweep blocks [35][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
+  bool adj_fp32 = false;     // L^T of the prepared adjoint in FP32 (precision != 0)
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
   bool tuned64 = false, tuned32 = false;
   float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
@@ -1233,7 +1233,6 @@ int cns_adjoint_prepare(cns_ctx* c) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   if (!c->adj_J) CK(dev_alloc(c, &c->adj_J, (size_t)(3 * 27 * 5) * ld, false));
-  if (!c->adj_N) CK(dev_alloc(c, &c->adj_N, (size_t)(35 * 5) * ld, false));
   if (!c->adj_z) CK(dev_alloc(c, &c->adj_z, (size_t)(2 * 5) * ld));
   const Space all = c->cells.view(-1);
   // the iteration's inputs at the bound (converged) state: thermodynamics,
@@ -1251,8 +1250,15 @@ int cns_adjoint_prepare(cns_ctx* c) {
                                   c->st));
   CK(launch_face_jac(c->d_blks, c->faces, c->ph, c->sc, s.v, s.pression, ld, s.sn, c->adj_J,
                      c->st));
-  CK(launch_sweep_jac(c->d_blks, all, c->ph, c->sc.qfix_dfez, ld, s.v, s.pression, s.sn,
-                      c->w.coefe, c->adj_N, c->st));
+  if (c->sc.precision != 0) {
+    // the reduced-precision form: L^T in FP32 (face areas and coefficients
+    // rounded once); A^T lambda stays FP64
+    CK(ensure_mixed(c));
+    CK(launch_to_float(s.sn, c->w.sn32, 9 * ld, c->st));
+    CK(launch_to_float(c->w.coefe, c->w.coefe32, 3 * ld, c->st));
+    CK(launch_to_float(c->w.coefdiag, c->w.coefdiag32, ld, c->st));
+  }
+  c->adj_fp32 = c->sc.precision != 0;
   return check_status(c);
 }
 
@@ -1266,11 +1272,20 @@ int cns_adjoint_rt(cns_ctx* c, const double* lam, double* wbar, double* sbar) {
 
 int cns_adjoint_lt(cns_ctx* c, const double* y, double* out) {
   if (!c || !y || !out) return CNS_EINVAL;
-  if (!c->adj_N) return fail(c, CNS_ENOTREADY, "run cns_adjoint_prepare first");
+  if (!c->adj_z) return fail(c, CNS_ENOTREADY, "run cns_adjoint_prepare first");
   const long long ld = c->lay.ld;
-  CK(launch_precond_t(c->d_blks, c->cells.view(-1), ld, c->adj_N, c->w.coefdiag,
-                      c->sc.lmax > 0 ? c->sc.lmax : 1, y, c->adj_z, c->adj_z + 5 * ld, out,
-                      c->st));
+  const int lmx = c->sc.lmax > 0 ? c->sc.lmax : 1;
+  const cns_state_t& s = c->state;
+  if (c->adj_fp32) {
+    float* z = reinterpret_cast<float*>(c->adj_z);
+    CK(launch_precond_ta<float>(c->d_blks, c->cells.view(-1), ld, s.v, s.pression, c->w.sn32,
+                                c->w.coefe32, c->w.coefdiag32, c->ph.gam1, c->ph.pinfl, lmx, y,
+                                z, z + 5 * ld, out, c->st));
+  } else {
+    CK(launch_precond_ta<double>(c->d_blks, c->cells.view(-1), ld, s.v, s.pression, s.sn,
+                                 c->w.coefe, c->w.coefdiag, c->ph.gam1, c->ph.pinfl, lmx, y,
+                                 c->adj_z, c->adj_z + 5 * ld, out, c->st));
+  }
   return CNS_OK;
 }
 

@@ -1,8 +1,8 @@
 // cns_adjoint.cu -- the discrete adjoint of the FP64 Euler Roe iteration
-// (sch_roe_euler + implimf_eu): exact Jacobian blocks of the face fluxes and
-// of the linearised point-Jacobi sweep, obtained by running the scheme's own
-// expressions in forward-mode dual numbers (one seed per launch row), and
-// the transposed products the adjoint iteration needs:
+// (sch_roe_euler + implimf_eu): exact Jacobian blocks of the face fluxes,
+// obtained by running the scheme's own expressions in forward-mode dual
+// numbers (one seed per launch row), and the transposed products the adjoint
+// iteration needs:
 //
 //   A^T lambda   the residual u(W) = sum of face fluxes, transposed, gathered
 //                per cell over the faces whose MUSCL stencil holds it (four
@@ -12,7 +12,8 @@
 //                transposed, so that the adjoint iteration
 //                lambda += L^T (dJ/dW - A^T lambda) contracts at the primal's
 //                asymptotic rate (the two iteration matrices are transposes
-//                up to similarity).
+//                up to similarity); its blocks are the cells' Euler flux
+//                Jacobians, evaluated on the fly.
 //
 // Stencil inputs per cell: the five conserved variables and the pressure
 // (the residual reads the pressure array; for real cells it is zpres of the
@@ -30,7 +31,6 @@ namespace {
 inline int grid_of(const Space& s) { return s.ntiles; }
 
 constexpr int kFaceSeeds = 27;  // 4 stencil cells x (W 5 + p) + the face normal (3)
-constexpr int kSweepSeeds = 35;  // 7 cells (own, i-, i+, j-, j+, k-, k+) x 5
 
 // The Euler face flux of sch_roe_euler.f90 (the arithmetic of
 // k_face_flux<T, false>) for one face from its stencil values:
@@ -214,131 +214,127 @@ __global__ void __launch_bounds__(kTile) k_adj_gather(const Blk* __restrict__ bl
   for (int c = 0; c < 6; ++c) wbar[c * ld + m] = acc[c];
 }
 
-// the linearised Jacobi update of one real cell (k_jacobi_rc's arithmetic
-// with jacobi_df, implimf_eu.f90:176-323) as a function of the iterate of
-// the cell and its six neighbours; seed blockIdx.y = 5 * cell + component.
-// N[((seed) * 5 + a) * ld + n] = d(d2w_a)/d(d_seed) at d = 0.
-__global__ void __launch_bounds__(kTile) k_sweep_jac(const Blk* __restrict__ blks, Space sp,
-                                                     Phys ph64, int qfix, long long ld,
-                                                     const double* __restrict__ v,
-                                                     const double* __restrict__ ps,
-                                                     const double* __restrict__ sn,
-                                                     const double* __restrict__ coefe,
-                                                     double* __restrict__ N) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const int seed = blockIdx.y;
-  const int cell = seed / 5, comp = seed % 5;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
-  const Dual gam1 = Dual(ph64.gam1), pinfl = Dual(ph64.pinfl);
-  auto df_at = [&](long long m, int which, Dual dd[5], Dual f[9]) {
-#pragma unroll
-    for (int a = 0; a < 5; ++a) dd[a] = Dual(0., (which == cell && a == comp) ? 1. : 0.);
-    jacobi_df<Dual, true>(dd, Dual(v[m]), Dual(v[ld + m]), Dual(v[2 * ld + m]),
-                          Dual(v[3 * ld + m]), Dual(v[4 * ld + m]), Dual(ps[m]), Dual(0.),
-                          Dual(0.), Dual(0.), gam1, pinfl, qfix, f);
-  };
-  Dual d0[5], f0[9];
-  df_at(n, 0, d0, f0);
-  Dual d2w[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) d2w[a] = Dual(0.);
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    const long long inc = ninc_of(B, dir);
-    const int nd = nd_of(B, dir);
-    const int p = dir == 0 ? i : (dir == 1 ? j : k);
-    Dual dl[5], fl[9], du[5], fu[9];
-    if (p == 1) {
-#pragma unroll
-      for (int a = 0; a < 5; ++a) dl[a] = Dual(0.);
-#pragma unroll
-      for (int a = 0; a < 9; ++a) fl[a] = Dual(0.);
-    } else {
-      df_at(n - inc, 1 + 2 * dir, dl, fl);
-    }
-    if (p == nd - 1) {
-#pragma unroll
-      for (int a = 0; a < 5; ++a) du[a] = Dual(0.);
-#pragma unroll
-      for (int a = 0; a < 9; ++a) fu[a] = Dual(0.);
-    } else {
-      df_at(n + inc, 2 + 2 * dir, du, fu);
-    }
-    const long long nu = n + inc;
-    Dual tn[5];
-    face_tn<Dual, true>(d0, dl, f0, fl, Dual(sn_ptr(sn, B, dir, 0)[n]),
-                        Dual(sn_ptr(sn, B, dir, 1)[n]), Dual(sn_ptr(sn, B, dir, 2)[n]), tn);
-    const Dual cel = Dual(coefe[(long long)dir * ld + n]);
-    const Dual ceu = Dual(coefe[(long long)dir * ld + nu]);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] + tn[a] + cel * dl[a] + ceu * du[a];
-    face_tn<Dual, true>(du, d0, fu, f0, Dual(sn_ptr(sn, B, dir, 0)[nu]),
-                        Dual(sn_ptr(sn, B, dir, 1)[nu]), Dual(sn_ptr(sn, B, dir, 2)[nu]), tn);
-#pragma unroll
-    for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
-  }
-#pragma unroll
-  for (int a = 0; a < 5; ++a) N[((long long)seed * 5 + a) * ld + n] = d2w[a].d;
-}
-
-// one transposed sweep: out(c) = y(c) + sum over the cells e whose update
-// reads c (c itself and its real neighbours) of N_e[c]^T (z(e) / cd(e))
-__global__ void __launch_bounds__(kTile) k_sweep_t(const Blk* __restrict__ blks, Space sp,
-                                                   long long ld, const double* __restrict__ N,
-                                                   const double* __restrict__ cd,
-                                                   const double* __restrict__ y,
-                                                   const double* __restrict__ z,
-                                                   double* __restrict__ out) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long c = cell_index(B, i, j, k);
-  double acc[5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) acc[a] = y[a * ld + c];
-  const int idx[3] = {i, j, k};
-  const int lim[3] = {B.ni, B.nj, B.nk};
-  // relation r of c seen from e: 0 own; e = c + inc sees c as its lower
-  // neighbour (cell index 1 + 2 dir); e = c - inc sees c as its upper one
-#pragma unroll
-  for (int r = 0; r < 7; ++r) {
-    long long e = c;
-    if (r > 0) {
-      const int dir = (r - 1) / 2;
-      const bool lower_of_e = ((r - 1) % 2) == 0;  // e is above c
-      const int q = idx[dir] + (lower_of_e ? 1 : -1);
-      if (q < 1 || q > lim[dir] - 1) continue;
-      e = c + (lower_of_e ? 1 : -1) * ninc_of(B, dir);
-    }
-    const double ie = 1. / cd[e];
-    double w[5];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) w[a] = z[a * ld + e] * ie;
-#pragma unroll
-    for (int comp = 0; comp < 5; ++comp) {
-      const long long seed = (long long)r * 5 + comp;
-      double t = 0.;
-#pragma unroll
-      for (int a = 0; a < 5; ++a) t += N[(seed * 5 + a) * ld + e] * w[a];
-      acc[comp] += t;
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 5; ++a) out[a * ld + c] = acc[a];
-}
-
+template <class T>
 __global__ void __launch_bounds__(kTile) k_scale_cd(const Blk* __restrict__ blks, Space sp,
-                                                    long long ld, const double* __restrict__ cd,
-                                                    const double* __restrict__ z,
+                                                    long long ld, const T* __restrict__ cd,
+                                                    const double* __restrict__ y,
+                                                    const T* __restrict__ z,
                                                     double* __restrict__ out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const long long c = cell_index(blks[b], i, j, k);
-  const double ic = 1. / cd[c];
+  const T ic = T(1.) / cd[c];
 #pragma unroll
-  for (int a = 0; a < 5; ++a) out[a * ld + c] = z[a * ld + c] * ic;
+  for (int a = 0; a < 5; ++a)
+    out[a * ld + c] = (double)((z ? z[a * ld + c] : (T)y[a * ld + c]) * ic);
+}
+
+// the linearised Jacobi update without stored blocks.  At d = 0 the
+// increment f(W + d) - f(W) of a cell differentiates to the Euler flux
+// Jacobians A_k(W) of that cell (jacobi_df with qfix: p = gam1 (E - |m|^2 /
+// (2 rho) - pinfl), H = (E + p - pinfl) / rho), so the block of e's update
+// with respect to its neighbour c across the face S is +-0.5 A(W_c) . S +
+// ce I, and the own block 0.5 A(W_e) . (sum over directions of S_lower -
+// S_upper).  Every block seen from c carries A(W_c): the transposed sweep
+// gathers V_k = sum of +-S_k w_e over the six neighbours and its own w, and
+// applies sum_k A_k(W_c)^T V_k once -- the transpose of the linearised
+// sweep (its blocks, differentiated with dual numbers, agree in exact
+// arithmetic).
+template <class T>
+__global__ void __launch_bounds__(kTile) k_sweep_ta(const Blk* __restrict__ blks, Space sp,
+                                                    long long ld, const double* __restrict__ v,
+                                                    const double* __restrict__ ps,
+                                                    const T* __restrict__ sn,
+                                                    const T* __restrict__ coefe,
+                                                    const T* __restrict__ cd,
+                                                    const double* __restrict__ y,
+                                                    const T* __restrict__ z,
+                                                    T* __restrict__ out, T gam1, T pinfl) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long c = cell_index(B, i, j, k);
+  auto wof = [&](long long e, T wv[5]) {
+    const T ie = T(1.) / cd[e];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) wv[a] = (z ? z[a * ld + e] : (T)y[a * ld + e]) * ie;
+  };
+  T acc[5], V[3][5], wc[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) acc[a] = (T)y[a * ld + c];
+  wof(c, wc);
+  const int idx[3] = {i, j, k};
+  const int lim[3] = {B.ni, B.nj, B.nk};
+  T Sc[3] = {T(0.), T(0.), T(0.)};
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long inc = ninc_of(B, dir);
+    T sl[3], su[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      sl[q] = sn_ptr(sn, B, dir, q)[c];
+      su[q] = sn_ptr(sn, B, dir, q)[c + inc];
+      Sc[q] += sl[q] - su[q];
+    }
+    if (dir == 0) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int a = 0; a < 5; ++a) V[q][a] = T(0.);
+    }
+    if (idx[dir] + 1 <= lim[dir] - 1) {  // e above: c is its lower neighbour
+      T we[5];
+      wof(c + inc, we);
+      const T ce = coefe[(long long)dir * ld + c + inc];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        acc[a] += ce * we[a];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) V[q][a] += su[q] * we[a];
+      }
+    }
+    if (idx[dir] - 1 >= 1) {  // e below: c is its upper neighbour
+      T we[5];
+      wof(c - inc, we);
+      const T ce = coefe[(long long)dir * ld + c];
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        acc[a] += ce * we[a];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) V[q][a] -= sl[q] * we[a];
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 5; ++a)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) V[q][a] += Sc[q] * wc[a];
+  // sum_k A_k^T V_k at W_c, times 0.5
+  const T rho = (T)v[c], ir = T(1.) / rho;
+  const T qv[3] = {(T)v[ld + c] * ir, (T)v[2 * ld + c] * ir, (T)v[3 * ld + c] * ir};
+  const T hq2 = T(0.5) * (qv[0] * qv[0] + qv[1] * qv[1] + qv[2] * qv[2]);
+  const T H = ((T)v[4 * ld + c] + (T)ps[c] - pinfl) * ir;
+  const T g = gam1;
+  T qVm[3], sumVkk = T(0.), sumqV4 = T(0.), r0 = T(0.);
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk) {
+    qVm[kk] = qv[0] * V[kk][1] + qv[1] * V[kk][2] + qv[2] * V[kk][3];
+    sumVkk += V[kk][1 + kk];
+    sumqV4 += qv[kk] * V[kk][4];
+    r0 += -qv[kk] * qVm[kk] + g * hq2 * V[kk][1 + kk] + (g * hq2 - H) * qv[kk] * V[kk][4];
+  }
+  T r[5];
+  r[0] = r0;
+#pragma unroll
+  for (int bb = 0; bb < 3; ++bb) {
+    T t = V[bb][0] + qVm[bb] + H * V[bb][4] - g * qv[bb] * sumVkk - g * qv[bb] * sumqV4;
+#pragma unroll
+    for (int kk = 0; kk < 3; ++kk) t += qv[kk] * V[kk][1 + bb];
+    r[1 + bb] = t;
+  }
+  r[4] = g * sumVkk + (g + T(1.)) * sumqV4;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) out[a * ld + c] = acc[a] + T(0.5) * r[a];
 }
 
 }  // namespace
@@ -363,28 +359,33 @@ cudaError_t launch_adj_gather(const Blk* blks, Space cells_ext, const double* J,
   return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_jac(const Blk* blks, Space cells, Phys ph, int qfix, long long ld,
-                             const double* v, const double* ps, const double* sn,
-                             const double* coefe, double* N, cudaStream_t st) {
-  if (cells.ntiles > 0)
-    k_sweep_jac<<<dim3(grid_of(cells), kSweepSeeds), kTile, 0, st>>>(blks, cells, ph, qfix, ld,
-                                                                     v, ps, sn, coefe, N);
-  return cudaGetLastError();
-}
+}  // namespace cns
 
-cudaError_t launch_precond_t(const Blk* blks, Space cells, long long ld, const double* N,
-                             const double* cd, int lmax, const double* y, double* z0,
-                             double* z1, double* out, cudaStream_t st) {
+namespace cns {
+template <class T>
+cudaError_t launch_precond_ta(const Blk* blks, Space cells, long long ld, const double* v,
+                              const double* ps, const T* sn, const T* coefe, const T* cd,
+                              double gam1, double pinfl, int lmax, const double* y, T* z0,
+                              T* z1, double* out, cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
-  const double* cur = y;
-  double* bufs[2] = {z0, z1};
+  const T* cur = nullptr;  // the first sweep's iterate: y
+  T* bufs[2] = {z0, z1};
   for (int l = 1; l < lmax; ++l) {
-    double* nxt = bufs[l & 1];
-    k_sweep_t<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, N, cd, y, cur, nxt);
+    T* nxt = bufs[l & 1];
+    k_sweep_ta<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, v, ps, sn, coefe, cd, y,
+                                                    cur, nxt, (T)gam1, (T)pinfl);
     cur = nxt;
   }
-  k_scale_cd<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, cd, cur, out);
+  k_scale_cd<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, cd, y, cur, out);
   return cudaGetLastError();
 }
-
+template cudaError_t launch_precond_ta<double>(const Blk*, Space, long long, const double*,
+                                               const double*, const double*, const double*,
+                                               const double*, double, double, int,
+                                               const double*, double*, double*, double*,
+                                               cudaStream_t);
+template cudaError_t launch_precond_ta<float>(const Blk*, Space, long long, const double*,
+                                              const double*, const float*, const float*,
+                                              const float*, double, double, int, const double*,
+                                              float*, float*, double*, cudaStream_t);
 }  // namespace cns

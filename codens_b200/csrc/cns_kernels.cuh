@@ -241,14 +241,15 @@ cudaError_t launch_face_jac(const Blk* blks, const SpaceBuf* faces, Phys ph, Sch
 cudaError_t launch_adj_gather(const Blk* blks, Space cells_ext, const double* J,
                               const double* lam, long long ld, double* wbar, double* sbar,
                               cudaStream_t st);
-// linearised Jacobi update blocks N[35 seeds][5][ld] (Euler, implimf_eu)
-cudaError_t launch_sweep_jac(const Blk* blks, Space cells, Phys ph, int qfix, long long ld,
-                             const double* v, const double* ps, const double* sn,
-                             const double* coefe, double* N, cudaStream_t st);
-// out = L^T y over lmax sweeps (z0, z1: scratch [5][ld])
-cudaError_t launch_precond_t(const Blk* blks, Space cells, long long ld, const double* N,
-                             const double* cd, int lmax, const double* y, double* z0,
-                             double* z1, double* out, cudaStream_t st);
+// out = L^T y over lmax transposed sweeps of the linearised Euler Jacobi
+// update (implimf_eu with qfix), from the flux Jacobians of each cell's state
+// (z0, z1: scratch [5][ld]); T = float: face areas, coefficients and the
+// sweep iterates in FP32 (the reduced-precision forms)
+template <class T>
+cudaError_t launch_precond_ta(const Blk* blks, Space cells, long long ld, const double* v,
+                              const double* ps, const T* sn, const T* coefe, const T* cd,
+                              double gam1, double pinfl, int lmax, const double* y, T* z0,
+                              T* z1, double* out, cudaStream_t st);
 
 // met_samut (real cells of block l0's space) and sch_turb (u, v, d: (ld, 7))
 cudaError_t launch_samut(const Blk* blks, Space cells, const double* v6, const double* mu,

@@ -99,3 +99,24 @@ def test_autograd_function(cuda):
     assert abs(float(J) - J2) <= 1e-12 * abs(J2)
     assert abs(float(mach.grad) - gm) <= 1e-8 * abs(gm)
     np.testing.assert_allclose(wall.grad.numpy(), gw.cpu().numpy(), rtol=1e-8, atol=1e-12)
+
+
+def test_mixed_form_gradient_matches_fp64(cuda):
+    """the mixed form (FP32 primal sweeps, FP32 transposed sweeps; FP64
+    residual and A^T lambda) converges to the same steady state and adjoint,
+    so its gradient equals the FP64 one to the convergence tolerances"""
+    from codens_b200 import adjoint
+    import dataclasses
+    d = _design()
+    dm = dataclasses.replace(d, precision=1)
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-14, adj_tol=1e-12)
+    J, gm, ga, gw = g.gradient()
+    g.close()
+    h = adjoint.WallForceGradient(dm, dm.mach, dm.alpha, dm.wall(), tol=1e-14, adj_tol=1e-12)
+    J2, gm2, ga2, gw2 = h.gradient()
+    h.close()
+    assert abs(J2 - J) <= 1e-12 * abs(J)
+    assert abs(gm2 - gm) <= 1e-8 * abs(gm), (gm2, gm)
+    assert abs(ga2 - ga) <= 1e-8 * abs(ga) + 1e-12, (ga2, ga)
+    np.testing.assert_allclose(gw2.cpu().numpy(), gw.cpu().numpy(), rtol=1e-7,
+                               atol=1e-9 * float(gw.abs().max()))
