@@ -745,15 +745,31 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
   const bool own = i <= B.ni - 1 && j <= B.nj - 1;
   const T gam1 = T(ph64.gam1), pinfl = T(ph64.pinfl);
 
+  // the patch-and-ring points this thread stages and fills (at most two for
+  // every shape: NP <= 2 NT): whether the column is inside the block's real
+  // cells, and its flat index at k = 0
+  constexpr int NQ = (NP + NT - 1) / NT;
+  static_assert(NQ <= 2, "a thread stages at most two ring points");
+  bool colin[NQ];
+  long long col0[NQ];
+#pragma unroll
+  for (int rr = 0; rr < NQ; ++rr) {
+    const int q = threadIdx.x + rr * NT;
+    const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+    colin[rr] = q < NP && ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1;
+    col0[rr] = colin[rr] ? cell_index(B, ii, jj, 0) : 0;
+  }
   // the increment inputs of plane kk (patch and ring) into raw buffer b;
   // cells outside the block's real cells are zero-filled
   auto stage = [&](int kk, int b) {
     T* r = sraw + b * NR * NP;
-    for (int q = threadIdx.x; q < NP; q += NT) {
-      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
-      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
-                      kk <= B.nk - 1;
-      const long long m = in ? cell_index(B, ii, jj, kk) : 0;
+    const bool kin = kk >= 1 && kk <= B.nk - 1;
+#pragma unroll
+    for (int rr = 0; rr < NQ; ++rr) {
+      const int q = threadIdx.x + rr * NT;
+      if (q >= NP) break;
+      const bool in = colin[rr] && kin;
+      const long long m = in ? col0[rr] + (long long)kk * B.nijd : 0;
 #pragma unroll
       for (int a = 0; a < 5; ++a) cp_async_elem(r + a * NP + q, d_in + a * ld + m, in);
       if (FORM == 1) {
@@ -779,10 +795,12 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
   auto fill = [&](int kk, int b) {
     const T* r = sraw + b * NR * NP;
     T* s = sdf + b * 14 * NP;
-    for (int q = threadIdx.x; q < NP; q += NT) {
-      const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
-      const bool in = ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1 && kk >= 1 &&
-                      kk <= B.nk - 1;
+    const bool kin = kk >= 1 && kk <= B.nk - 1;
+#pragma unroll
+    for (int rr = 0; rr < NQ; ++rr) {
+      const int q = threadIdx.x + rr * NT;
+      if (q >= NP) break;
+      const bool in = colin[rr] && kin;
       T dd[5], f[9];
 #pragma unroll
       for (int a = 0; a < 5; ++a) dd[a] = r[a * NP + q];
