@@ -677,7 +677,9 @@ def run_rans(args):
         e.record(s.stream)
         e.synchronize()
         ms_dist = a.elapsed_time(e)
-        s.set_sa(dist, case.meta["rokinf"], 0.0, 1e-8)
+        # the flagged source fix: the reference's S~ reaches zero in the
+        # freestream of this plate within ~80 iterations (cfke inf / NaN)
+        s.set_sa(dist, case.meta["rokinf"], 0.0, 1e-8, stilde_fix=1)
         first = s.atsch_num(1)[1, 0]
         s.atsch_num(warm - 1)
         ms = timed(s, steps)
@@ -720,6 +722,8 @@ def run_rans(args):
                                f"Roe-MUSCL + viscous, lmax={args.lmax}, met_num every "
                                "iteration",
                    "cells": nreal, "eta": case.scheme.eta,
+                   "sa_source": "modified vorticity (Allmaras, Johnson & Spalart 2012), "
+                                "non-reference flag stilde_fix=1",
                    "l2_flush": "inputs larger than L2 (~2 GB of state and scratch)"},
         "fp64": out["fp64"], "mixed": out["mixed"],
         "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],

@@ -47,7 +47,8 @@ class Bnd_t(C.Structure):
 
 
 class Sa_t(C.Structure):
-    _fields_ = [("dist", C.c_void_p), ("rokinf", c_f64), ("roeinf", c_f64), ("epsk", c_f64)]
+    _fields_ = [("dist", C.c_void_p), ("rokinf", c_f64), ("roeinf", c_f64), ("epsk", c_f64),
+                ("stilde_fix", c_i32)]
 
 
 class State_t(C.Structure):

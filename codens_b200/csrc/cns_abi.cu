@@ -30,6 +30,7 @@ struct cns_ctx {
   // Spalart-Allmaras transport step of the fused iteration (cns_set_sa)
   bool sa_on = false;
   double sa_rokinf = 0., sa_roeinf = 0., sa_epsk = 1e-8;
+  int sa_fix = 0;                   // flagged non-reference SA source fix (cns_sa_t)
   const double* sa_dist = nullptr;  // the caller's wall distance (device)
   double* sa_dv = nullptr;          // velocity gradients [9][ld]
   double* sa_fd = nullptr;          // diffusion densities fd5x..fd6z [6][ld]
@@ -345,7 +346,7 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
                            nullptr, 0, 0, c->st);
     if (e == cudaSuccess)
       e = launch_smsa(c->d_blks, cb, ld, s.v, s.mu, c->sa_dist, c->sa_dv, c->sa_gr,
-                      c->sa_gr + 3 * ld, fdr, ts6, ts7, c->sa_cfke, c->st);
+                      c->sa_gr + 3 * ld, fdr, ts6, ts7, c->sa_cfke, c->sa_fix, c->st);
     if (e == cudaSuccess) e = launch_fludcsa(n0, n1, s.v + 5 * ld, s.mu, fdw, c->sigma, c->st);
   }
   if (e == cudaSuccess) e = launch_fd_ghosts(c->bd, fdw, c->st);
@@ -1109,7 +1110,7 @@ int cns_met_smsa(cns_ctx* c, int l, const double* v, const double* mu, const dou
                       0, c->st));
   const double* fd5[3] = {fd5x, fd5y, fd5z};
   CK(launch_smsa(c->d_blks, cells, ld, v, mu, dist, dv, c->sa_gr, c->sa_gr + 3 * ld, fd5, ts6,
-                 ts7, cfke, c->st));
+                 ts7, cfke, c->sa_fix, c->st));
   return CNS_OK;
 }
 
@@ -1198,6 +1199,7 @@ int cns_set_sa(cns_ctx* c, const cns_sa_t* sa) {
   drop_graphs(c);
   if (!sa) {
     c->sa_on = false;
+    c->sa_fix = 0;
     return CNS_OK;
   }
   if (!sa->dist) return CNS_EINVAL;
@@ -1208,6 +1210,7 @@ int cns_set_sa(cns_ctx* c, const cns_sa_t* sa) {
   c->sa_rokinf = sa->rokinf;
   c->sa_roeinf = sa->roeinf;
   c->sa_epsk = sa->epsk;
+  c->sa_fix = sa->stilde_fix ? 1 : 0;
   c->sa_on = true;
   return CNS_OK;
 }

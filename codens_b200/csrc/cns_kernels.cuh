@@ -273,7 +273,7 @@ cudaError_t launch_teq_grads(const Blk* blks, Space cells, int mode, int nsc,
 cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double* v,
                         const double* mu, const double* dist, const double* dv,
                         const double* grt, const double* grr, const double* const fd5[3],
-                        double* ts6, double* ts7, double* cfke, cudaStream_t st);
+                        double* ts6, double* ts7, double* cfke, int fix, cudaStream_t st);
 // impli2_eqt_3d of block l0 (-1: all): u, v are (ld, 7); w: 20 ld scratch;
 // rcp = 1: one reciprocal per line step instead of three divisions (the
 // reduced-precision forms; not bit-exact)

@@ -22,6 +22,9 @@ inline int grid_of(const Space& s) { return s.ntiles; }
 // SA constants (atlecdon.f90:193-204)
 constexpr double kCb1 = 0.1355, kSigma = 2. / 3., kCb2 = 0.622, kKappa = 0.41;
 constexpr double kCv1 = 7.1, kCw2 = 0.3, kCw3 = 2., kCt3 = 1.1, kCt4 = 2.;
+// the modified vorticity of Allmaras, Johnson & Spalart (ICCFD7-1902, 2012,
+// eq. 12), used by the flagged non-reference source fix
+constexpr double kCv2 = 0.7, kCv3 = 0.9;
 
 __device__ __forceinline__ double pow6(double x) {  // gcc's x**6: x3 * x3
   const double x3 = x * x * x;
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(kTile) k_smsa(
     const double* __restrict__ dv, const double* __restrict__ grt,
     const double* __restrict__ grr, const double* __restrict__ fd5x,
     const double* __restrict__ fd5y, const double* __restrict__ fd5z,
-    double* __restrict__ ts6, double* __restrict__ ts7, double* __restrict__ cfke) {
+    double* __restrict__ ts6, double* __restrict__ ts7, double* __restrict__ cfke, int fix) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -148,9 +151,19 @@ __global__ void __launch_bounds__(kTile) k_smsa(
   const double kapd2 = kappa2 * dist2;
   const double fv1 = xkhi3 / (xkhi3 + cv13);
   const double fv2 = 1. - (xkhi / (1 + xkhi * fv1));
-  const double stilde = vort + nutilde * fv2 / kapd2;
-  double rtilde = nutilde / (stilde * kapd2);
-  rtilde = fmin(rtilde, 1.);
+  const double sbar = nutilde * fv2 / kapd2;
+  double stilde, rtilde;
+  if (!fix || sbar >= -kCv2 * vort) {
+    stilde = vort + sbar;
+  } else {
+    stilde = vort + vort * (kCv2 * kCv2 * vort + kCv3 * sbar) / ((kCv3 - 2. * kCv2) * vort - sbar);
+  }
+  if (fix && !(stilde > 0.)) {
+    rtilde = 1.;
+  } else {
+    rtilde = nutilde / (stilde * kapd2);
+    rtilde = fmin(rtilde, 1.);
+  }
   const double rtil6 = pow6(rtilde);
   const double ft2 = kCt3 * exp(-kCt4 * xkhi2);
   const double sm1 = kCb1 * (1. - ft2) * stilde * v6;
@@ -161,13 +174,25 @@ __global__ void __launch_bounds__(kTile) k_smsa(
   ts6[n] = sm1 + sm2 + sdif;
   ts7[n] = 0.;
   const double xkhi4 = xkhi3 * xkhi;
-  const double dfv1 = cv133 * (fv1 * fv1) / (mu[n] * xkhi4);
+  const double dfv1 =
+      (fix && !(xkhi4 > 0.)) ? 0. : cv133 * (fv1 * fv1) / (mu[n] * xkhi4);
   const double t1 = 1. + xkhi * fv1;
   const double dfv2 = (xkhi2 * dfv1 - 1. / mu[n]) / (t1 * t1);
   const double dst = (fv2 / v1 + nutilde * dfv2) / kapd2;
-  const double dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
-  const double dxg = dpr * (1. + kCw2 * (6. * rtil6 / rtilde - 1.));
-  const double dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+  double dpr, dxg, dfw;
+  if (!fix) {
+    dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
+    dxg = dpr * (1. + kCw2 * (6. * rtil6 / rtilde - 1.));
+    dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+  } else {
+    // r is constant where it is clipped; r^5 without r^6 / r; no division
+    // by xg = 0
+    dpr = (rtilde < 1. && stilde > 0.)
+              ? (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2) : 0.;
+    const double r2 = rtilde * rtilde;
+    dxg = dpr * (1. + kCw2 * (6. * (r2 * r2 * rtilde) - 1.));
+    dfw = xg != 0. ? (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg : 0.;
+  }
   const double dft2 = -ct42 * xkhi * ft2;
   const double dsm1 = kCb1 * ((1. - ft2) * (stilde + dst * v6) - stilde * v6 * dft2);
   const double dsm2 = 2. * sm2 / v6 - (cw1 * dfw - kCb1 * dft2 / kappa2) * nutilde * v6 / dist2;
@@ -663,10 +688,10 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
 cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double* v,
                         const double* mu, const double* dist, const double* dv,
                         const double* grt, const double* grr, const double* const fd5[3],
-                        double* ts6, double* ts7, double* cfke, cudaStream_t st) {
+                        double* ts6, double* ts7, double* cfke, int fix, cudaStream_t st) {
   if (cells.ntiles > 0)
     k_smsa<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, v, mu, dist, dv, grt, grr,
-                                             fd5[0], fd5[1], fd5[2], ts6, ts7, cfke);
+                                             fd5[0], fd5[1], fd5[2], ts6, ts7, cfke, fix);
   return cudaGetLastError();
 }
 

@@ -300,17 +300,19 @@ class CodeNS:
     def met_cutsa(self, l, v, epsk):
         self._check(self.lib.cns_met_cutsa(self.ctx, l, _ptr(v), epsk), "cns_met_cutsa")
 
-    def set_sa(self, dist=None, rokinf=0.0, roeinf=0.0, epsk=1e-8):
+    def set_sa(self, dist=None, rokinf=0.0, roeinf=0.0, epsk=1e-8, stilde_fix=0):
         """enable the Spalart-Allmaras step in the fused iteration (dist: the
         wall distance, device FP64; None disables it).  The state must have
-        7 columns."""
+        7 columns.  stilde_fix = 1: the non-reference source fix (modified
+        vorticity, guarded derivative; see cns_sa_t)."""
         if dist is None:
             self._check(self.lib.cns_set_sa(self.ctx, None), "cns_set_sa")
             self._sa = None
             return
         if self.ncol != 7:
             raise ValueError("the Spalart-Allmaras step needs a (ld, 7) state")
-        self._sa = (dist, abi.Sa_t(C.c_void_p(dist.data_ptr()), rokinf, roeinf, epsk))
+        self._sa = (dist, abi.Sa_t(C.c_void_p(dist.data_ptr()), rokinf, roeinf, epsk,
+                                   int(stilde_fix)))
         self._check(self.lib.cns_set_sa(self.ctx, C.byref(self._sa[1])), "cns_set_sa")
 
     def met_num(self):

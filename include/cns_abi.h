@@ -225,6 +225,12 @@ typedef struct {
   const double *dist;    /* wall distance of the real cells (device, ip12) */
   double rokinf, roeinf; /* v(:,6), v(:,7) of the injection ghosts */
   double epsk;           /* met_cutsa floor of v(:,6) */
+  int32_t stilde_fix;    /* non-reference option (0 = reference): met_smsa with the
+                            modified vorticity of Allmaras, Johnson & Spalart
+                            2012 (S~ >= 0.3 vort) and its derivative zero where
+                            r is clipped.  The reference's S~ can reach zero,
+                            where its source bound cfke becomes inf or NaN.
+                            cns_met_smsa follows it too while set */
 } cns_sa_t;
 int cns_atcaldis3(cns_ctx *ctx, const double *x, const double *y, const double *z,
                   double *dist);

@@ -1998,6 +1998,12 @@ void orc_met_roe2o(int l, const double *t, double *d, const double *sn, int hart
 #define SA_CB2 0.622
 #define SA_KAPPA 0.41
 #define SA_CV1 7.1
+/* the modified vorticity of Allmaras, Johnson & Spalart (ICCFD7-1902, 2012,
+ * eq. 12): the flagged non-reference source fix (orc_set_sa_fix) */
+#define SA_CV2 0.7
+#define SA_CV3 0.9
+static int SA_FIX = 0;
+void orc_set_sa_fix(int on) { SA_FIX = on ? 1 : 0; }
 
 /* met_samut.f90:35-46: mut = v6 fv1 on the real cells (x**3 as x*x*x) */
 void orc_met_samut(int l, const double *v, const double *mu, double *mut) {
@@ -2233,9 +2239,19 @@ void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
         const double kapd2 = kappa2 * dist2;
         const double fv1 = xkhi3 / (xkhi3 + cv13);
         const double fv2 = 1. - (xkhi / (1 + xkhi * fv1));
-        const double stilde = vort + nutilde * fv2 / kapd2;
-        double rtilde = nutilde / (stilde * kapd2);
-        rtilde = fmin(rtilde, 1.);
+        const double sbar = nutilde * fv2 / kapd2;
+        double stilde, rtilde;
+        if (!SA_FIX || sbar >= -SA_CV2 * vort)
+          stilde = vort + sbar;
+        else
+          stilde = vort + vort * (SA_CV2 * SA_CV2 * vort + SA_CV3 * sbar) /
+                              ((SA_CV3 - 2. * SA_CV2) * vort - sbar);
+        if (SA_FIX && !(stilde > 0.)) {
+          rtilde = 1.;
+        } else {
+          rtilde = nutilde / (stilde * kapd2);
+          rtilde = fmin(rtilde, 1.);
+        }
         const double rtil6 = pow6(rtilde);
         const double ft2 = ct3 * exp(-ct4 * xkhi2);
         const double sm1 = cb1 * (1. - ft2) * stilde * v6;
@@ -2246,12 +2262,24 @@ void orc_met_smsa(int l, const double *sn, const double *vol, const double *v,
         ts6[n] = sm1 + sm2 + sdif[m];
         ts7[n] = 0.;
         const double xkhi4 = xkhi3 * xkhi;
-        const double dfv1 = cv133 * sq(fv1) / (mu[n] * xkhi4);
+        const double dfv1 =
+            (SA_FIX && !(xkhi4 > 0.)) ? 0. : cv133 * sq(fv1) / (mu[n] * xkhi4);
         const double dfv2 = (xkhi2 * dfv1 - 1. / mu[n]) / sq(1. + xkhi * fv1);
         const double dst = (fv2 / v1 + nutilde * dfv2) / kapd2;
-        const double dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
-        const double dxg = dpr * (1. + cw2 * (6. * rtil6 / rtilde - 1.));
-        const double dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+        double dpr, dxg, dfw;
+        if (!SA_FIX) {
+          dpr = (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2);
+          dxg = dpr * (1. + cw2 * (6. * rtil6 / rtilde - 1.));
+          dfw = (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg;
+        } else {
+          /* r constant where clipped; r^5 without r^6 / r; no division by
+           * xg = 0 */
+          dpr = (rtilde < 1. && stilde > 0.)
+                    ? (1. / v1 - nutilde * dst / stilde) / (stilde * kapd2) : 0.;
+          const double r2 = rtilde * rtilde;
+          dxg = dpr * (1. + cw2 * (6. * (r2 * r2 * rtilde) - 1.));
+          dfw = xg != 0. ? (1. - xg6 / (xg6 + cw36)) * fw * dxg / xg : 0.;
+        }
         const double dft2 = -ct42 * xkhi * ft2;
         const double dsm1 = cb1 * ((1. - ft2) * (stilde + dst * v6) - stilde * v6 * dft2);
         const double dsm2 = 2. * sm2 / v6 - (cw1 * dfw - cb1 * dft2 / kappa2) * nutilde * v6 / dist2;

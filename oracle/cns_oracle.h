@@ -162,6 +162,10 @@ void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double
                 double *cfke);
 void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
                  double *mut, const double *sn, const double *vol);
+/* non-reference option of met_smsa: the modified vorticity of Allmaras,
+ * Johnson & Spalart 2012 and a derivative guarded where r is clipped
+ * (0 = reference) */
+void orc_set_sa_fix(int on);
 
 int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,

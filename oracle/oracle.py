@@ -81,6 +81,7 @@ def lib():
                                  C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 8
+        L.orc_set_sa_fix.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -143,7 +144,7 @@ class Oracle:
         self.ncyc = 0
 
     def set_sa(self, st: OracleState, dist, rokinf: float, roeinf: float, epsk: float = 1e-8,
-               epsroe: float = 0.0, sigma: float = 2.0 / 3.0):
+               epsroe: float = 0.0, sigma: float = 2.0 / 3.0, stilde_fix: int = 0):
         """run the Spalart-Allmaras step (met_num, 1SA) in every iteration
         from now on; dist: the wall distance (kept referenced here)"""
         ld = self.case.layout.ld
@@ -153,9 +154,11 @@ class Oracle:
         a = self._sa
         lib().orc_set_sa(1, a["dist"].ctypes.data, rokinf, roeinf, epsk, harten, epsroe, sigma,
                          a["fd"].ctypes.data, a["ts"].ctypes.data, a["cfke"].ctypes.data)
+        lib().orc_set_sa_fix(int(stilde_fix))
 
     def clear_sa(self):
         lib().orc_set_sa(0, None, 0.0, 0.0, 0.0, 0, 0.0, 1.0, None, None, None)
+        lib().orc_set_sa_fix(0)
         self._sa = None
 
     def metric(self, st: OracleState):

@@ -259,3 +259,79 @@ def test_set_sa_needs_seven_columns(cuda):
     with pytest.raises(ValueError):
         s.set_sa(s.vol, 1e-3, 0.0)
     s.close()
+
+
+def test_met_smsa_stilde_fix_parity(cuda):
+    """the flagged source fix (modified vorticity, guarded derivative) against
+    the oracle's, on a state where both branches of the modified vorticity
+    occur (chi = 2..6 makes fv2 < 0, so S_bar < -0.7 vort at the cells of
+    small vorticity); finite everywhere, and 1e-13 like the reference form"""
+    torch = cuda
+    case = CASES["plate"]()
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    t = _bordered(case, st).copy()
+    r = cases.splitmix64_uniform(83, 3 * ld).reshape(3, ld)
+    mu = 1e-3 * (1.0 + r[0])
+    t[5] = mu * (2.0 + 4.0 * r[1])              # chi in 2..6
+    dist = 0.01 + r[2]
+    L = orc_lib()
+    b = case.layout.blocks[0]
+    loc = np.zeros(9 * b.nnn)
+    L.orc_teq_gradv(1, st.sn, st.vol, t.reshape(-1), loc)
+    dv = np.zeros((9, ld))
+    dv[:, b.npc:b.npc + b.nnn] = loc.reshape(9, b.nnn)
+    fd = cases.splitmix64_uniform(89, 3 * ld).reshape(3, ld) - 0.5
+    rc = case.layout.real_cells()
+    # both branches of the modified vorticity are exercised
+    d = dv[:, rc]
+    vort = np.sqrt((d[7] - d[5]) ** 2 + (d[2] - d[6]) ** 2 + (d[3] - d[1]) ** 2)
+    chi = t[5, rc] / mu[rc]
+    fv1 = chi ** 3 / (chi ** 3 + 7.1 ** 3)
+    sbar = (t[5, rc] / t[0, rc]) * (1.0 - chi / (1.0 + chi * fv1)) / (0.41 ** 2 * dist[rc] ** 2)
+    low = sbar < -0.7 * vort
+    assert low.any() and (~low).any()
+    L.orc_set_sa_fix(1)
+    try:
+        out_o = [np.full(ld, 4.0) for _ in range(3)]
+        L.orc_met_smsa(1, st.sn, st.vol, t.reshape(-1), mu, dist, loc, fd[0], fd[1], fd[2],
+                       *out_o)
+    finally:
+        L.orc_set_sa_fix(0)
+    s.set_sa(_t(torch, dist), case.meta["rokinf"], 0.0, 1e-8, stilde_fix=1)
+    g = [_t(torch, np.full(ld, 4.0)) for _ in range(3)]
+    s.met_smsa(0, _t(torch, t.reshape(-1)), _t(torch, mu), _t(torch, dist), s.sn, s.vol,
+               _t(torch, dv.reshape(-1)), _t(torch, fd[0]), _t(torch, fd[1]), _t(torch, fd[2]),
+               *g)
+    s.sync()
+    for a, o, w in zip(g, out_o, ("ts6", "ts7", "cfke")):
+        ag = a.cpu().numpy()[rc]
+        assert np.isfinite(ag).all(), w
+        np.testing.assert_allclose(ag, o[rc], rtol=1e-13, atol=0, err_msg=w)
+    s.close()
+
+
+def test_fused_rans_iterations_stilde_fix_parity(cuda):
+    """fused FP64 iterations with the flagged source fix against the oracle"""
+    case = _seven(CASES["channel"]())
+    orc, st = oracle_prepared(case)
+    dist = np.zeros(case.layout.ld)
+    assert orc_lib().orc_atcaldis3(st.x, st.y, st.z, dist) == 0
+    rok = case.meta["rokinf"]
+    orc.set_sa(st, dist, rok, 0.0, stilde_fix=1)
+    s = _gpu(case)
+    s.set_sa(_t(s.torch, dist), rok, 0.0, 1e-8, stilde_fix=1)
+    try:
+        for _ in range(3):
+            orc.step(st)
+    finally:
+        orc.clear_sa()
+    s.atsch_num(3)
+    s.sync()
+    ld = case.layout.ld
+    rc = case.layout.real_cells()
+    v_g = s.v.cpu().numpy().reshape(7, ld)[:, rc]
+    v_o = st.v.reshape(7, ld)[:, rc]
+    assert max_rel_cols(v_g[:6], v_o[:6]) < 1e-11
+    s.close()
