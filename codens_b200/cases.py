@@ -445,10 +445,10 @@ def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e
     the Spalart-Allmaras variable rho nu~ = nut_ratio * mu_inf (v(:,7) = 0),
     as met_inisa.f90 leaves it for a uniform mut.  meta['rokinf'] is the
     freestream rho nu~ the injection ghosts take (met_bord.f90:60-63).
-    A seeded +-1% noise on a 3-D plate (several cells across the span) makes
-    the SA iteration unstable at the wall cells (the density of single wall
-    cells grows until the state is not finite), in the oracle and on the
-    GPU alike; the uniform start converges.
+    With the reference's Spalart-Allmaras source the iteration of the
+    full-size plate fails once S~ (negative in the freestream, where fv2 < 0)
+    crosses zero at some cell; run it with the flagged source fix
+    (CodeNS.set_sa(..., stilde_fix=1)).
     """
     ni, nj, nk = (c + 1 for c in cells)
     lay = Layout.from_dims([(ni, nj, nk)])
