@@ -574,7 +574,9 @@ class WallForceGradient:
 
 
 def wall_force(design: Design, mach: float, alpha: float, wall: np.ndarray, **kw) -> float:
-    """J at a design, from a converged primal (for finite differences)"""
+    """J at a design, from a converged primal (for finite differences).
+    state: a converged (5, ld) state computed elsewhere (e.g. by the CPU
+    restatement of the reference) to evaluate J at instead of solving"""
     g = WallForceGradient.__new__(WallForceGradient)
     import torch
     g.torch = torch
@@ -582,8 +584,16 @@ def wall_force(design: Design, mach: float, alpha: float, wall: np.ndarray, **kw
     g.mach, g.alpha = float(mach), float(alpha)
     g.wall = np.asarray(wall, dtype=float)
     g.case = design.case(mach, alpha, g.wall)
-    g.s, g.iters, g.l2 = solve_primal(g.case, tol=kw.get("tol", 1e-13),
-                                      max_iter=kw.get("max_iter", 40000))
+    if kw.get("state") is not None:
+        g.s = CodeNS(g.case)
+        g.s.metric()
+        g.s.v.copy_(torch.as_tensor(np.ascontiguousarray(kw["state"]).reshape(-1),
+                                    device=g.s.dev))
+        torch.cuda.synchronize()
+        g.iters, g.l2 = 0, float("nan")
+    else:
+        g.s, g.iters, g.l2 = solve_primal(g.case, tol=kw.get("tol", 1e-13),
+                                          max_iter=kw.get("max_iter", 40000))
     g.maps = _Maps(g.case, torch, g.s.dev)
     g.W = g.s.v.detach().reshape(5, g.maps.ld).clone()
     P0 = g.maps.nodes(torch.as_tensor(g.wall, device=g.s.dev))

@@ -120,3 +120,35 @@ def test_mixed_form_gradient_matches_fp64(cuda):
     assert abs(ga2 - ga) <= 1e-8 * abs(ga) + 1e-12, (ga2, ga)
     np.testing.assert_allclose(gw2.cpu().numpy(), gw.cpu().numpy(), rtol=1e-7,
                                atol=1e-9 * float(gw.abs().max()))
+
+
+def _oracle_state(d, mach, tol=1e-14, cap=200000):
+    """the converged primal of the CPU restatement of the reference"""
+    from oracle.oracle import Oracle, OracleState
+    case = d.case(mach, d.alpha, d.wall())
+    orc = Oracle(case)
+    st = OracleState(case)
+    orc.metric(st)
+    for it in range(cap):
+        v0 = st.v.copy()
+        orc.step(st)
+        if it % 50 == 49 and orc.norms(v0, st)[1, 0] < tol:
+            break
+    return st.v.copy()
+
+
+def test_gradient_matches_finite_differences_of_the_oracle(cuda):
+    """dJ/dMach of the adjoint against central differences of J evaluated on
+    primal states converged by the CPU restatement of the reference"""
+    from codens_b200 import adjoint
+    d = _design()
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-14, adj_tol=1e-12)
+    J, gm, _, _ = g.gradient()
+    g.close()
+    eps = 1e-6
+    Jp = adjoint.wall_force(d, d.mach + eps, d.alpha, d.wall(),
+                            state=_oracle_state(d, d.mach + eps))
+    Jm = adjoint.wall_force(d, d.mach - eps, d.alpha, d.wall(),
+                            state=_oracle_state(d, d.mach - eps))
+    fd = (Jp - Jm) / (2 * eps)
+    assert abs(gm - fd) <= GRAD_TOL * abs(fd), (gm, fd)
