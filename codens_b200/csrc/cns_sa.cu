@@ -649,13 +649,16 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
                           int rcp, cudaStream_t st) {
   // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7),
   // the tridiagonal coefficients ta, tb, tc and right-hand sides d6, d7 of
-  // a sweep = 20 ld
+  // a sweep = 20 ld.  rv and the iterates start at zero (their ghost
+  // entries are the reference's zeroed rv and never-written neighbours);
+  // every other entry read is written first.
   double *rv = w, *cd = w + ld, *uf = w + 2 * ld, *ce = w + 5 * ld, *al = w + 8 * ld,
          *b6 = w + 9 * ld, *b7 = w + 10 * ld;
   double* it[2][2] = {{w + 11 * ld, w + 12 * ld}, {w + 13 * ld, w + 14 * ld}};
   double *ta = w + 15 * ld, *tb = w + 16 * ld, *tc = w + 17 * ld, *d6 = w + 18 * ld,
          *d7 = w + 19 * ld;
-  cudaError_t e = cudaMemsetAsync(w, 0, sizeof(double) * 15 * ld, st);
+  cudaError_t e = cudaMemsetAsync(rv, 0, sizeof(double) * ld, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w + 11 * ld, 0, sizeof(double) * 4 * ld, st);
   if (e != cudaSuccess) return e;
   if (cells.ntiles == 0) return cudaSuccess;
   k_i2_cell<<<grid_of(cells), kTile, 0, st>>>(blks, cells, v, mu, mut, dt, cfke, vol, cmt, rv,
