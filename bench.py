@@ -314,23 +314,14 @@ def steady_state_check(iters=4500):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
+
+    from codens_b200.replicas import Replicas
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    if ws > 1:
-        dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=300))
-
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        if ws > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl")
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     from codens_b200.solver import CodeNS
 
@@ -455,8 +446,7 @@ def run_ours(args):
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
     s.close()
-    if ws > 1:
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
