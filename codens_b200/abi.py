@@ -16,10 +16,11 @@ P = C.POINTER
 ERRORS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-positive temperature",
     4: "time step below dt1min", 5: "unknown boundary condition",
-    6: "not ready", 7: "non-finite residual norm",
+    6: "not ready", 7: "non-finite residual norm", 8: "file error",
+    9: "file does not match the layout",
 }
 (CNS_OK, CNS_EINVAL, CNS_ECUDA, CNS_ETEMP, CNS_EDT, CNS_EBC, CNS_ENOTREADY,
- CNS_ENONFINITE) = range(8)
+ CNS_ENONFINITE, CNS_EIO, CNS_EFORMAT) = range(10)
 
 
 class Layout_t(C.Structure):
@@ -71,6 +72,7 @@ EXPORTS = [
     "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
     "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
     "cns_set_sa", "cns_met_num",
+    "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
 ]
 
 _lib = None
@@ -144,6 +146,12 @@ def load(build_if_missing: bool = True):
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,
                                             c_f64, vp, vp, vp, vp, vp]
+    cs = C.c_char_p
+    L.cns_set_subrecord_length.argtypes = [vp, c_i64]
+    L.cns_readdg.argtypes = [vp, cs, vp, vp, vp]
+    L.cns_writdg.argtypes = [vp, cs, cs, vp, vp, vp]
+    L.cns_readda.argtypes = [vp, cs, cs, C.c_int, vp, vp]
+    L.cns_writda.argtypes = [vp, cs, cs, cs, vp, vp]
     for f in EXPORTS:
         getattr(L, f).restype = getattr(L, f).restype or C.c_int
     L.cns_last_error.restype = C.c_char_p

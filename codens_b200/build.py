@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libcodens_b200.so")
 # written.  The FP32 half of the mixed-precision form (cns_mixed.cu) is not a
 # parity path and is built with contraction.
 SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_jameson.cu", "cns_turb.cu", "cns_sa.cu",
-           "cns_adjoint.cu", "cns_abi.cu", "cns_noalloc.cu"]
+           "cns_adjoint.cu", "cns_abi.cu", "cns_noalloc.cu", "cns_io.cu"]
 SOURCES_FMA = ["cns_mixed.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 OBJDIR = os.path.join(HERE, "_build")

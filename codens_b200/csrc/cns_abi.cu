@@ -69,6 +69,8 @@ struct cns_ctx {
   long long kernels_launched = 0;        // kernels of every fused-step graph launched
   long long mixed_iter = 0;              // mixed iterations since the last reset
   long long ncyc = 0;                    // fused iterations since the state was bound
+  long long io_maxsub = 2147483639;      // bytes per subrecord of the files written
+  IoStage io_stage;                      // pinned ring of the file readers and writers
   std::string err;
 };
 
@@ -617,6 +619,26 @@ cudaError_t capture(cns_ctx* c, cudaGraphExec_t* out, int* nkernels, F enqueue) 
   return e;
 }
 
+// the (i, j, k) box of a file record over block B: what 0 = the real nodes,
+// 1 = the real cells, 2 = the cells with the ghost layer (chdgcv.f90,
+// chdacc.f90: ii1..ii2, ii1..ii2-1, ii1-1..ii2)
+void io_box(const Blk& B, int what, int lo[3], int hi[3]) {
+  const int n[3] = {B.ni, B.nj, B.nk};
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = what == 2 ? 0 : 1;
+    hi[a] = what == 1 ? n[a] - 1 : n[a];
+  }
+}
+
+// equat(1:2) = 'ns' and equat(6:7) = 'ke' of the reference's 7-character
+// equation key (blank-padded)
+void equat_keys(const char* equat, bool& ns, bool& ke) {
+  char q[8] = "       ";
+  for (int a = 0; a < 7 && equat[a]; ++a) q[a] = equat[a];
+  ns = q[0] == 'n' && q[1] == 's';
+  ke = q[5] == 'k' && q[6] == 'e';
+}
+
 }  // namespace
 
 extern "C" {
@@ -821,6 +843,7 @@ int cns_destroy(cns_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_norms) cudaFreeHost(c->h_norms);
   if (c->h_status) cudaFreeHost(c->h_status);
+  io_stage_free(c->io_stage);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
   return CNS_OK;
@@ -1478,6 +1501,85 @@ int cns_atsch_num_step_host(cns_ctx* c, double* v_host, int nsteps, double* norm
   CK(cudaMemcpyAsync(v_host, c->state.v, bytes, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   return CNS_OK;
+}
+
+/* ---- reference grid and flow files ------------------------------------ */
+
+int cns_set_subrecord_length(cns_ctx* c, int64_t bytes) {
+  if (!c || bytes < 1 || bytes > 2147483639) return CNS_EINVAL;
+  c->io_maxsub = bytes;
+  return CNS_OK;
+}
+
+int cns_readdg(cns_ctx* c, const char* path, double* x, double* y, double* z) {
+  if (!c || !path || !x || !y || !z) return CNS_EINVAL;
+  cns::IoPlan p, none;
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    int lo[3], hi[3];
+    io_box(c->lay.blks[b], 0, lo, hi);
+    for (double* a : {x, y, z}) cns::io_add(p, (int)b, a, 0, lo, hi);
+  }
+  return cns::io_read(c->io_stage, p, none, c->d_blks, path, c->st, c->err);
+}
+
+int cns_writdg(cns_ctx* c, const char* path, const char* disc, const double* x,
+               const double* y, const double* z) {
+  if (!c || !path || !disc || !x || !y || !z) return CNS_EINVAL;
+  int what;
+  if (!std::strncmp(disc, "cvcv", 4)) what = 0;
+  else if (!std::strncmp(disc, "cvcc", 4)) what = 1;
+  else if (!std::strncmp(disc, "cvcf", 4)) what = 2;
+  else return fail(c, CNS_EINVAL, "disc must be cvcv, cvcc or cvcf");
+  cns::IoPlan p;
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    int lo[3], hi[3];
+    io_box(c->lay.blks[b], what, lo, hi);
+    for (const double* a : {x, y, z})
+      cns::io_add(p, (int)b, const_cast<double*>(a), what != 0, lo, hi);
+  }
+  return cns::io_write(c->io_stage, p, c->d_blks, path, c->io_maxsub, c->st, c->err);
+}
+
+int cns_readda(cns_ctx* c, const char* path, const char* equat, int keinit, double* v,
+               double* mut) {
+  if (!c || !path || !equat || !v) return CNS_EINVAL;
+  bool ns, ke;
+  equat_keys(equat, ns, ke);
+  if (ns && !mut) return fail(c, CNS_EINVAL, "equat 'ns': mut is read too");
+  const long long ld = c->lay.ld;
+  cns::IoPlan p, zero;
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    int lo[3], hi[3];
+    io_box(c->lay.blks[b], 1, lo, hi);
+    for (int a = 0; a < 5; ++a) cns::io_add(p, (int)b, v + a * ld, 0, lo, hi);
+    if (ns) cns::io_add(p, (int)b, mut, 0, lo, hi);
+    for (int a = 5; a < 7 && ke; ++a)
+      cns::io_add(keinit == 0 ? p : zero, (int)b, v + a * ld, 0, lo, hi);
+  }
+  return cns::io_read(c->io_stage, p, zero, c->d_blks, path, c->st, c->err);
+}
+
+int cns_writda(cns_ctx* c, const char* path, const char* disc, const char* equat,
+               const double* v, const double* mut) {
+  if (!c || !path || !disc || !equat || !v) return CNS_EINVAL;
+  int what;
+  if (!std::strncmp(disc, "cccc", 4)) what = 1;
+  else if (!std::strncmp(disc, "cccf", 4)) what = 2;
+  else return fail(c, CNS_EINVAL, "disc must be cccc or cccf");
+  bool ns, ke;
+  equat_keys(equat, ns, ke);
+  if (ns && !mut) return fail(c, CNS_EINVAL, "equat 'ns': mut is written too");
+  const long long ld = c->lay.ld;
+  double* w = const_cast<double*>(v);
+  cns::IoPlan p;
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    int lo[3], hi[3];
+    io_box(c->lay.blks[b], what, lo, hi);
+    for (int a = 0; a < 5; ++a) cns::io_add(p, (int)b, w + a * ld, 0, lo, hi);
+    if (ns) cns::io_add(p, (int)b, const_cast<double*>(mut), 0, lo, hi);
+    for (int a = 5; a < 7 && ke; ++a) cns::io_add(p, (int)b, w + a * ld, 0, lo, hi);
+  }
+  return cns::io_write(c->io_stage, p, c->d_blks, path, c->io_maxsub, c->st, c->err);
 }
 
 }  // extern "C"

@@ -1,5 +1,6 @@
 // cns_kernels.cuh -- host-side launchers of the CodeNS hot-path kernels.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "cns_common.cuh"
@@ -44,6 +45,36 @@ struct SpaceBuf {
     return s;
   }
 };
+
+// one record of a reference grid or flow file: nval values of the array arr
+// over the (i, j, k) box lo .. lo + ext - 1 of block blk, i fastest; img is
+// the record's first value in the file's data image (records back to back)
+struct IoRec {
+  long long img, nval;
+  double* arr;
+  int blk, centre;  // centre: the value is the centre of the cell's 8 nodes (writes)
+  int lo[3], ext[3];
+};
+struct IoPlan {
+  std::vector<IoRec> recs;
+  long long nval = 0;
+};
+// the pinned host ring the file readers and writers stream through
+struct IoStage {
+  static constexpr int kSlots = 4;
+  static constexpr size_t kSlotBytes = size_t(8) << 20;
+  char* ring = nullptr;
+  cudaEvent_t ev[kSlots] = {};
+};
+cudaError_t io_stage_init(IoStage& s);
+void io_stage_free(IoStage& s);
+void io_add(IoPlan& p, int b, double* arr, int centre, const int lo[3], const int hi[3]);
+// read the records of plan p from the file into the arrays, then zero the
+// boxes of plan zero; returns a CNS_* code and sets err
+int io_read(IoStage& stage, const IoPlan& p, const IoPlan& zero, const Blk* d_blks,
+            const char* path, cudaStream_t st, std::string& err);
+int io_write(IoStage& stage, const IoPlan& p, const Blk* d_blks, const char* path,
+             long long maxsub, cudaStream_t st, std::string& err);
 
 // the 2.5D tile list of one sweep configuration
 struct TileBuf {

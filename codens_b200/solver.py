@@ -16,6 +16,8 @@ the reference routine names and argument meaning:
     implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx)
     rscpsv(u0, v, dt) -> (3, 5) L1/L2/Linf         rscpsv.f90 + residu.f90
     atsch_num(nsteps) -> norms of the last step     atsch_num.f90 (fused, graph)
+    readdg(path) / writdg(path, disc)               readdg.f90 / svgr.f90 (fgv, fgc, fgcf)
+    readda(path, equat) / writda(path, equat, disc) readda.f90 / svfw.f90 (fac, facf)
 
 Block numbers are 1-based like the reference; ``l = 0`` runs every block in
 one launch.  Every array argument is a float64 CUDA tensor in the reference
@@ -24,6 +26,7 @@ layout (column-major (ld, ncol) flattened).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -37,6 +40,11 @@ def _ptr(t):
     if not (t.is_cuda and t.dtype.is_floating_point and t.is_contiguous()):
         raise ValueError("arrays must be contiguous float64 CUDA tensors")
     return C.c_void_p(t.data_ptr())
+
+
+def _check_ke(equat: str, v, ld: int):
+    if equat.ljust(7)[5:7] == "ke" and v.numel() < 7 * ld:
+        raise ValueError("equat 'ke' reads and writes v(:,6:7): v must be (ld, 7)")
 
 
 class CodeNS:
@@ -317,6 +325,43 @@ class CodeNS:
 
     def met_num(self):
         self._check(self.lib.cns_met_num(self.ctx), "cns_met_num")
+
+    # reference grid and flow files (Fortran unformatted sequential)
+    def set_subrecord_length(self, nbytes: int):
+        self._check(self.lib.cns_set_subrecord_length(self.ctx, int(nbytes)),
+                    "cns_set_subrecord_length")
+
+    def readdg(self, path, x=None, y=None, z=None):
+        """fgv: the real nodes of every block into x, y, z (default: this
+        context's node arrays)"""
+        x, y, z = (self.x if x is None else x, self.y if y is None else y,
+                   self.z if z is None else z)
+        self._check(self.lib.cns_readdg(self.ctx, os.fsencode(path), _ptr(x), _ptr(y), _ptr(z)),
+                    "cns_readdg")
+
+    def writdg(self, path, disc="cvcv", x=None, y=None, z=None):
+        """svgr: disc cvcv (fgv, nodes), cvcc (fgc, cell centres), cvcf (fgcf,
+        cell centres with the ghost layer)"""
+        x, y, z = (self.x if x is None else x, self.y if y is None else y,
+                   self.z if z is None else z)
+        self._check(self.lib.cns_writdg(self.ctx, os.fsencode(path), disc.encode(), _ptr(x),
+                                        _ptr(y), _ptr(z)), "cns_writdg")
+
+    def readda(self, path, equat, v=None, mut=None, keinit=0):
+        """fac: the real cells of v (and mut for 'ns', v(:,6:7) for 'ke')"""
+        v = self.v if v is None else v
+        mut = self.mut if mut is None else mut
+        _check_ke(equat, v, self.ld)
+        self._check(self.lib.cns_readda(self.ctx, os.fsencode(path), equat.encode(),
+                                        int(keinit), _ptr(v), _ptr(mut)), "cns_readda")
+
+    def writda(self, path, equat, disc="cccc", v=None, mut=None):
+        """svfw: disc cccc (fac, real cells) or cccf (facf, with the ghost layer)"""
+        v = self.v if v is None else v
+        mut = self.mut if mut is None else mut
+        _check_ke(equat, v, self.ld)
+        self._check(self.lib.cns_writda(self.ctx, os.fsencode(path), disc.encode(),
+                                        equat.encode(), _ptr(v), _ptr(mut)), "cns_writda")
 
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
         self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),

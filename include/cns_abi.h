@@ -49,7 +49,10 @@ enum {
   CNS_EDT = 4,         /* global time step below dt1min (chrono.f90:134-142) */
   CNS_EBC = 5,         /* unknown boundary condition (rbord.f90:417-421) */
   CNS_ENOTREADY = 6,   /* state arrays not bound / metric not computed */
-  CNS_ENONFINITE = 7   /* non-finite residual norm after a step */
+  CNS_ENONFINITE = 7,  /* non-finite residual norm after a step */
+  CNS_EIO = 8,         /* a file cannot be opened, read or written */
+  CNS_EFORMAT = 9      /* a file's records do not match the layout (the
+                          reference stops: readdg.f90:86-89) */
 };
 
 /* boundary kinds (rbord.f90:144-424) */
@@ -342,6 +345,41 @@ int cns_set_sweep_tiles(cns_ctx *ctx, int precision, int ti, int tj, int kc);
  * in, runs nsteps iterations, copies v back and returns the last norms */
 int cns_atsch_num_step_host(cns_ctx *ctx, double *v_host, int nsteps,
                             double *norms);
+
+/* ---- reference grid and flow files ------------------------------------ */
+/* The reference's Fortran unformatted sequential files (solve.f90:401-404),
+ * every block in block order, each record one array over a block's (i, j, k)
+ * box, i fastest, with gfortran's 4-byte record markers in the machine's
+ * byte order (a record longer than 2147483639 bytes split into subrecords
+ * with negated markers).  Arrays are device arrays in the layout above; the
+ * calls return when the file is complete.  A read modifies nothing unless the
+ * whole file matches the layout (else CNS_EFORMAT, or CNS_EIO when it cannot
+ * be opened), where the reference stops.
+ *
+ * cns_readdg: fgv, x, y, z at the real nodes of every block (ingr.f90:49 ->
+ *   readdg.f90:71-80).
+ * cns_writdg: svgr.f90 (chdgcv.f90 -> writdg.f90:46-48) for every block; disc
+ *   "cvcv" = the real nodes (fgv), "cvcc" = the real cell centres (fgc),
+ *   "cvcf" = the cell centres with the ghost layer (fgcf); a centre is .125
+ *   times the sum of the cell's 8 nodes (cvccg.f90), ghost nodes included.
+ * cns_readda: fac (infw.f90:64 -> readda.f90:88-128): v(:,1..5) at the real
+ *   cells, mut when equat(1:2) = 'ns', and with equat(6:7) = 'ke' v(:,6),
+ *   v(:,7) (v is (ld, 7)) when keinit = 0, else those two are zeroed.  The
+ *   utau records of kutau = 1 models and the dual-time copies of kfmg = 3 are
+ *   not handled.
+ * cns_writda: svfw.f90 (chdacc.f90 -> writda.f90:78-97) for every block; disc
+ *   "cccc" = the real cells (fac), "cccf" = the cells with the ghost layer
+ *   (facf); the node-averaged "cccv" is not handled.
+ * cns_set_subrecord_length: the largest subrecord the writers produce
+ *   (gfortran's -fmax-subrecord-length; default and maximum 2147483639). */
+int cns_set_subrecord_length(cns_ctx *ctx, int64_t bytes);
+int cns_readdg(cns_ctx *ctx, const char *path, double *x, double *y, double *z);
+int cns_writdg(cns_ctx *ctx, const char *path, const char *disc, const double *x,
+               const double *y, const double *z);
+int cns_readda(cns_ctx *ctx, const char *path, const char *equat, int keinit,
+               double *v, double *mut);
+int cns_writda(cns_ctx *ctx, const char *path, const char *disc, const char *equat,
+               const double *v, const double *mut);
 
 /* ---- no-allocation variant -------------------------------------------- */
 /* No counterpart in the reference.  The Euler Roe residual of ONE block

@@ -11,6 +11,7 @@
 #include "cns_oracle.h"
 #include <float.h>
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -2677,4 +2678,216 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
     }
   }
   return 0;
+}
+
+/* ---- reference grid and flow files ------------------------------------- */
+/* Fortran unformatted sequential files as gfortran writes them: a logical
+ * record is subrecords of at most maxsub data bytes, each framed by 4-byte
+ * byte counts; the leading count is negated when another subrecord follows,
+ * the trailing one when a subrecord precedes.  Return codes: 0, 8 (open,
+ * read or write failure), 9 (records do not match the layout). */
+enum { ORC_EIO = 8, ORC_EFORMAT = 9 };
+
+static int orc_put_record(FILE *f, const double *buf, int64_t n, int64_t maxsub) {
+  const unsigned char *p = (const unsigned char *)buf;
+  int64_t left = 8 * n;
+  int sub = 0;
+  do {
+    int64_t len = left > maxsub ? maxsub : left;
+    int32_t lead = (int32_t)(left > len ? -len : len);
+    int32_t trail = (int32_t)(sub > 0 ? -len : len);
+    if (fwrite(&lead, 4, 1, f) != 1) return ORC_EIO;
+    if (len > 0 && fwrite(p, 1, (size_t)len, f) != (size_t)len) return ORC_EIO;
+    if (fwrite(&trail, 4, 1, f) != 1) return ORC_EIO;
+    p += len;
+    left -= len;
+    ++sub;
+  } while (left > 0);
+  return 0;
+}
+
+/* the first n doubles of the next logical record (a Fortran READ of n items) */
+static int orc_get_record(FILE *f, double *buf, int64_t n) {
+  unsigned char *p = (unsigned char *)buf;
+  int64_t need = 8 * n;
+  int sub = 0;
+  for (;;) {
+    int32_t lead, trail;
+    if (fread(&lead, 4, 1, f) != 1) return ORC_EFORMAT;
+    int64_t len = lead < 0 ? -(int64_t)lead : lead;
+    for (int64_t b = 0; b < len; ++b) {
+      int ch = fgetc(f);
+      if (ch == EOF) return ORC_EFORMAT;
+      if (need > 0) {
+        *p++ = (unsigned char)ch;
+        --need;
+      }
+    }
+    if (fread(&trail, 4, 1, f) != 1) return ORC_EFORMAT;
+    if ((trail < 0 ? -(int64_t)trail : trail) != len) return ORC_EFORMAT;
+    if ((sub > 0) != (trail < 0)) return ORC_EFORMAT;
+    ++sub;
+    if (lead >= 0) break;
+  }
+  return need > 0 ? ORC_EFORMAT : 0;
+}
+
+/* (i, j, k) box of a record over block b: 0 real nodes, 1 real cells,
+ * 2 cells with the ghost layer (chdgcv.f90, chdacc.f90) */
+static void orc_box(const blk_t *b, int what, int lo[3], int hi[3]) {
+  int n[3] = {b->ni, b->nj, b->nk};
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = what == 2 ? 0 : 1;
+    hi[a] = what == 1 ? n[a] - 1 : n[a];
+  }
+}
+
+static int64_t orc_box_count(const int lo[3], const int hi[3]) {
+  return (int64_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+}
+
+/* writdg.f90:46-48 / writda.f90:78-97: the array over the box, i fastest;
+ * centre: cvccg.f90's .125*(sum of the 8 nodes of the cell) */
+static int orc_put_array(FILE *f, const blk_t *b, const double *x, int centre,
+                         const int lo[3], const int hi[3], int64_t maxsub, double *buf) {
+  int64_t m = 0;
+  int64_t inc1 = 1, inc2 = b->nid, inc3 = b->nijd;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        int64_t n = b->npc + i + (int64_t)j * b->nid + (int64_t)k * b->nijd;
+        if (!centre) {
+          buf[m++] = x[n];
+        } else {
+          buf[m++] = .125 * (x[n] + x[n + inc3] + x[n + inc1] + x[n + inc1 + inc3] +
+                             x[n + inc2] + x[n + inc2 + inc3] + x[n + inc1 + inc2] +
+                             x[n + inc1 + inc2 + inc3]);
+        }
+      }
+  return orc_put_record(f, buf, m, maxsub);
+}
+
+/* readdg.f90:71-80 / readda.f90:88-118: one record into the array's box */
+static int orc_get_array(FILE *f, const blk_t *b, double *x, const int lo[3], const int hi[3],
+                         double *buf) {
+  int rc = orc_get_record(f, buf, orc_box_count(lo, hi));
+  if (rc) return rc;
+  int64_t m = 0;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i)
+        x[b->npc + i + (int64_t)j * b->nid + (int64_t)k * b->nijd] = buf[m++];
+  return 0;
+}
+
+
+static void orc_equat(const char *equat, int *ns, int *ke) {
+  char q[8] = "       ";
+  for (int a = 0; a < 7 && equat[a]; ++a) q[a] = equat[a];
+  *ns = q[0] == 'n' && q[1] == 's';
+  *ke = q[5] == 'k' && q[6] == 'e';
+}
+
+static double *orc_block_buffer(void) {
+  int64_t mx = 1;
+  for (int l = 0; l < G.nblk; ++l)
+    if (G.b[l].nnn > mx) mx = G.b[l].nnn;
+  return (double *)malloc(sizeof(double) * (size_t)mx);
+}
+
+/* svgr.f90 for l = 1..nblk: disc cvcv (nodes, cvcvg), cvcc / cvcf (cell
+ * centres of the real cells / with the ghost layer, cvccg) */
+int orc_writdg(const char *path, const char *disc, const double *x, const double *y,
+               const double *z, int64_t maxsub) {
+  int what = !strncmp(disc, "cvcv", 4) ? 0 : !strncmp(disc, "cvcc", 4) ? 1
+             : !strncmp(disc, "cvcf", 4) ? 2 : -1;
+  if (what < 0) return 1;
+  FILE *f = fopen(path, "wb");
+  if (!f) return ORC_EIO;
+  double *buf = orc_block_buffer();
+  int rc = 0;
+  for (int l = 0; l < G.nblk && !rc; ++l) {
+    int lo[3], hi[3];
+    orc_box(&G.b[l], what, lo, hi);
+    const double *c[3] = {x, y, z};
+    for (int a = 0; a < 3 && !rc; ++a)
+      rc = orc_put_array(f, &G.b[l], c[a], what != 0, lo, hi, maxsub, buf);
+  }
+  free(buf);
+  if (fclose(f) && !rc) rc = ORC_EIO;
+  return rc;
+}
+
+/* ingr.f90:49 -> readdg.f90:71-80 for l = 1..nblk */
+int orc_readdg(const char *path, double *x, double *y, double *z) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return ORC_EIO;
+  double *buf = orc_block_buffer();
+  int rc = 0;
+  for (int l = 0; l < G.nblk && !rc; ++l) {
+    int lo[3], hi[3];
+    orc_box(&G.b[l], 0, lo, hi);
+    double *c[3] = {x, y, z};
+    for (int a = 0; a < 3 && !rc; ++a) rc = orc_get_array(f, &G.b[l], c[a], lo, hi, buf);
+  }
+  free(buf);
+  fclose(f);
+  return rc;
+}
+
+/* svfw.f90 for l = 1..nblk: chdacc.f90 (disc cccc = real cells, cccf = with
+ * the ghost layer) -> writda.f90:78-97: v1..v5, mut ('ns'), v6, v7 ('ke') */
+int orc_writda(const char *path, const char *disc, const char *equat, const double *v,
+               const double *mut, int64_t maxsub) {
+  int what = !strncmp(disc, "cccc", 4) ? 1 : !strncmp(disc, "cccf", 4) ? 2 : -1;
+  if (what < 0) return 1;
+  int ns, ke;
+  orc_equat(equat, &ns, &ke);
+  FILE *f = fopen(path, "wb");
+  if (!f) return ORC_EIO;
+  double *buf = orc_block_buffer();
+  int rc = 0;
+  for (int l = 0; l < G.nblk && !rc; ++l) {
+    const blk_t *b = &G.b[l];
+    int lo[3], hi[3];
+    orc_box(b, what, lo, hi);
+    for (int a = 0; a < 5 && !rc; ++a) rc = orc_put_array(f, b, v + a * G.ld, 0, lo, hi, maxsub, buf);
+    if (ns && !rc) rc = orc_put_array(f, b, mut, 0, lo, hi, maxsub, buf);
+    for (int a = 5; a < 7 && ke && !rc; ++a)
+      rc = orc_put_array(f, b, v + a * G.ld, 0, lo, hi, maxsub, buf);
+  }
+  free(buf);
+  if (fclose(f) && !rc) rc = ORC_EIO;
+  return rc;
+}
+
+/* infw.f90:64 -> readda.f90:88-131 for l = 1..nblk */
+int orc_readda(const char *path, const char *equat, int keinit, double *v, double *mut) {
+  int ns, ke;
+  orc_equat(equat, &ns, &ke);
+  FILE *f = fopen(path, "rb");
+  if (!f) return ORC_EIO;
+  double *buf = orc_block_buffer();
+  int rc = 0;
+  for (int l = 0; l < G.nblk && !rc; ++l) {
+    const blk_t *b = &G.b[l];
+    int lo[3], hi[3];
+    orc_box(b, 1, lo, hi);
+    for (int a = 0; a < 5 && !rc; ++a) rc = orc_get_array(f, b, v + a * G.ld, lo, hi, buf);
+    if (ns && !rc) rc = orc_get_array(f, b, mut, lo, hi, buf);
+    if (ke && keinit == 0) {
+      for (int a = 5; a < 7 && !rc; ++a) rc = orc_get_array(f, b, v + a * G.ld, lo, hi, buf);
+    } else if (ke) {
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            int64_t n = b->npc + i + (int64_t)j * b->nid + (int64_t)k * b->nijd;
+            v[5 * G.ld + n] = 0.;
+            v[6 * G.ld + n] = 0.;
+          }
+    }
+  }
+  free(buf);
+  fclose(f);
+  return rc;
 }

@@ -171,6 +171,18 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);
 
+/* reference grid and flow files (readdg.f90, svgr.f90 -> writdg.f90,
+ * readda.f90, svfw.f90 -> writda.f90), every block in order, gfortran's
+ * unformatted sequential records (4-byte markers, subrecords of at most
+ * maxsub bytes); returns 0, 1 (bad disc), 8 (file error) or 9 (records do
+ * not match the layout) */
+int orc_writdg(const char *path, const char *disc, const double *x, const double *y,
+               const double *z, int64_t maxsub);
+int orc_readdg(const char *path, double *x, double *y, double *z);
+int orc_writda(const char *path, const char *disc, const char *equat, const double *v,
+               const double *mut, int64_t maxsub);
+int orc_readda(const char *path, const char *equat, int keinit, double *v, double *mut);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,11 @@ def lib():
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 8
         L.orc_set_sa_fix.argtypes = [C.c_int]
+        cs = C.c_char_p
+        L.orc_writdg.argtypes = [cs, cs, _d, _d, _d, C.c_int64]
+        L.orc_readdg.argtypes = [cs, _d, _d, _d]
+        L.orc_writda.argtypes = [cs, cs, cs, _d, _d, C.c_int64]
+        L.orc_readda.argtypes = [cs, cs, C.c_int, _d, _d]
         _lib = L
     return _lib
 
@@ -163,6 +168,24 @@ class Oracle:
 
     def metric(self, st: OracleState):
         lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)
+
+    # reference grid and flow files; each returns the routine's code
+    # (0, 1 bad disc, 8 file error, 9 records do not match the layout)
+    @staticmethod
+    def writdg(path, disc, x, y, z, maxsub=2147483639) -> int:
+        return lib().orc_writdg(os.fsencode(path), disc.encode(), x, y, z, maxsub)
+
+    @staticmethod
+    def readdg(path, x, y, z) -> int:
+        return lib().orc_readdg(os.fsencode(path), x, y, z)
+
+    @staticmethod
+    def writda(path, disc, equat, v, mut, maxsub=2147483639) -> int:
+        return lib().orc_writda(os.fsencode(path), disc.encode(), equat.encode(), v, mut, maxsub)
+
+    @staticmethod
+    def readda(path, equat, v, mut, keinit=0) -> int:
+        return lib().orc_readda(os.fsencode(path), equat.encode(), int(keinit), v, mut)
 
     def boundary_geom(self):
         n = len(self._ba["ncbd"])
