@@ -80,6 +80,8 @@ class Scheme:
     ischema: int = 7     # 7 Roe (sch_roe*), 1 Jameson (dissip_jameson + sch_jameson)
     ki2: float = 0.5     # Jameson 2nd-difference coefficient ki2(lm)
     ki4: float = 1.0 / 32.0  # Jameson 4th-difference coefficient ki4(lm)
+    ncychro: int = 1     # time step recomputed when n mod ncychro = 1 or n < icychr0
+    icychr0: int = 0     # (atsch_num.f90:173-178, 436); ncychro <= 1: every iteration
 
 
 @dataclass

@@ -62,10 +62,11 @@ struct cns_ctx {
   cns_state_t state{};
   bool bound = false;
   bool metric_done = false;
-  cudaGraphExec_t gexec = nullptr;       // FP64 iteration
-  cudaGraphExec_t gexec_mref = nullptr;  // mixed, or defect iteration with refresh
-  cudaGraphExec_t gexec_mreg = nullptr;  // defect iteration without refresh
-  int nk_gexec = 0, nk_mref = 0, nk_mreg = 0;  // kernel nodes of each graph
+  // iteration graphs [form][time step recomputed]: form kGraph64 = FP64,
+  // kGraphRef = mixed or defect iteration with refresh, kGraphReg = defect
+  // iteration without refresh; and the kernel nodes of each
+  cudaGraphExec_t gexec[3][2] = {};
+  int nk_graph[3][2] = {};
   long long kernels_launched = 0;        // kernels of every fused-step graph launched
   long long mixed_iter = 0;              // mixed iterations since the last reset
   long long ncyc = 0;                    // fused iterations since the state was bound
@@ -198,13 +199,23 @@ cudaError_t zero_cols(cns_ctx* c, double* a, int ncol, int l) {
   return cudaSuccess;
 }
 
+enum { kGraph64 = 0, kGraphRef = 1, kGraphReg = 2 };
+
 void drop_graphs(cns_ctx* c) {
-  for (cudaGraphExec_t* g : {&c->gexec, &c->gexec_mref, &c->gexec_mreg})
-    if (*g) {
-      cudaGraphExecDestroy(*g);
-      *g = nullptr;
-    }
+  for (auto& form : c->gexec)
+    for (cudaGraphExec_t& g : form)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   c->mixed_iter = 0;
+}
+
+// atsch_num.f90:173-178, 436: whether iteration n (1-based since the state
+// was bound) recomputes the time step
+bool dt_due(const cns_ctx* c, long long n) {
+  const int nc = c->sc.ncychro;
+  return nc <= 1 || n % nc == 1 || n < c->sc.icychr0;
 }
 
 int check_status(cns_ctx* c) {
@@ -373,18 +384,19 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
 }
 
 // one pseudo-time iteration on the bound state (atsch_num.f90:245-1134 for
-// ischema = 7, kmf = 1, steady, dt recomputed every iteration; ischema <= 4:
-// the Jameson dissipation before rbord, sch_jameson for the residual)
-cudaError_t enqueue_step(cns_ctx* c, bool first) {
+// ischema = 7, kmf = 1, steady; dt_on: the time step is recomputed, else
+// the previous one is kept; ischema <= 4: the Jameson dissipation before
+// rbord, sch_jameson for the residual)
+cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   const Space all = c->cells.view(-1);
   cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
                                s.ztemp, s.cson, s.mu, c->w.status, c->st);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && dt_on)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
-  if (e == cudaSuccess) e = global_dt(c);
+  if (e == cudaSuccess && dt_on) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
@@ -444,7 +456,7 @@ cudaError_t ensure_mixed(cns_ctx* c) {
 // advances with it and stores corr = R64 - R32 for the regular iterations.
 enum MixedMode { kMixed, kDefectRefresh, kDefectRegular };
 
-cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
+cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_on) {
   const cns_state_t& s = c->state;
   Work& w = c->w;
   const long long ld = c->lay.ld;
@@ -452,10 +464,10 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first) {
   const bool lim = c->sc.ns && c->sc.ilim == 1;
   cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
                                s.ztemp, s.cson, s.mu, w.status, c->st);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && dt_on)
     e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
                        s.vol, s.cson, c->st);
-  if (e == cudaSuccess) e = global_dt(c);
+  if (e == cudaSuccess && dt_on) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
@@ -881,6 +893,8 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.ischema = s->ischema;
   c->sc.ki2 = s->ki2;
   c->sc.ki4 = s->ki4;
+  c->sc.ncychro = s->ncychro;
+  c->sc.icychr0 = s->icychr0;
   drop_graphs(c);
   return CNS_OK;
 }
@@ -1400,50 +1414,44 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   const bool first = c->ncyc == 0;
   const bool tuned = prec == 0 ? c->tuned64 : c->tuned32;
   const bool eager = !tuned || (jameson(c) && first);
+  auto enqueue = [&](int form, bool fst, bool on) {
+    if (form == kGraph64) return enqueue_step(c, fst, on);
+    return enqueue_step_mixed(c, prec == 1 ? kMixed : (form == kGraphRef ? kDefectRefresh
+                                                                          : kDefectRegular),
+                              fst, on);
+  };
+  // the form of the next iteration (defect correction refreshes every
+  // kdefect iterations), advancing the refresh counter
+  auto next_form = [&]() {
+    if (prec == 0) return (int)kGraph64;
+    if (prec == 1) return (int)kGraphRef;
+    return (c->mixed_iter++ % c->sc.kdefect) == 0 ? (int)kGraphRef : (int)kGraphReg;
+  };
+  std::vector<std::pair<int, bool>> plan;  // (form, time step recomputed) per iteration
   if (eager) {
-    if (prec == 0) {
-      CK(enqueue_step(c, first));
-    } else {
-      const bool refresh = prec == 2 && (c->mixed_iter % c->sc.kdefect) == 0;
-      CK(enqueue_step_mixed(c, prec == 1 ? kMixed : (refresh ? kDefectRefresh : kDefectRegular),
-                            first));
-      if (prec == 2) ++c->mixed_iter;
-    }
+    const int form = next_form();
+    const bool on = dt_due(c, ++c->ncyc);
+    CK(enqueue(form, first, on));
     if (!tuned) {
       CK(tune_sweeps(c, prec != 0));
       drop_graphs(c);
     }
-    ++c->ncyc;
     --nsteps;
+    plan.emplace_back(form, on);  // counted below with the launches of its graph
   }
-  c->ncyc += nsteps;
-  if (prec == 0) {
-    if (!c->gexec)
-      CK(capture(c, &c->gexec, &c->nk_gexec, [&] { return enqueue_step(c, false); }));
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
-    c->kernels_launched += (long long)(nsteps + eager) * c->nk_gexec;
-    return CNS_OK;
+  const size_t replay0 = plan.size();
+  for (int q = 0; q < nsteps; ++q) plan.emplace_back(next_form(), dt_due(c, ++c->ncyc));
+  // capture the graphs these iterations need, then replay them in order
+  for (const auto& fo : plan) {
+    cudaGraphExec_t& g = c->gexec[fo.first][fo.second];
+    if (!g)
+      CK(capture(c, &g, &c->nk_graph[fo.first][fo.second],
+                 [&] { return enqueue(fo.first, false, fo.second); }));
   }
-  if (prec == 1) {
-    if (!c->gexec_mref)
-      CK(capture(c, &c->gexec_mref, &c->nk_mref,
-                 [&] { return enqueue_step_mixed(c, kMixed, false); }));
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec_mref, c->st));
-    c->kernels_launched += (long long)(nsteps + eager) * c->nk_mref;
-    return CNS_OK;
-  }
-  if (!c->gexec_mref)
-    CK(capture(c, &c->gexec_mref, &c->nk_mref,
-               [&] { return enqueue_step_mixed(c, kDefectRefresh, false); }));
-  if (!c->gexec_mreg)
-    CK(capture(c, &c->gexec_mreg, &c->nk_mreg,
-               [&] { return enqueue_step_mixed(c, kDefectRegular, false); }));
-  if (eager) c->kernels_launched += c->nk_mref;
-  for (int s = 0; s < nsteps; ++s) {
-    const bool refresh = (c->mixed_iter % c->sc.kdefect) == 0;
-    CK(cudaGraphLaunch(refresh ? c->gexec_mref : c->gexec_mreg, c->st));
-    c->kernels_launched += refresh ? c->nk_mref : c->nk_mreg;
-    ++c->mixed_iter;
+  for (size_t q = 0; q < plan.size(); ++q) {
+    const auto& fo = plan[q];
+    if (q >= replay0) CK(cudaGraphLaunch(c->gexec[fo.first][fo.second], c->st));
+    c->kernels_launched += c->nk_graph[fo.first][fo.second];
   }
   return CNS_OK;
 }

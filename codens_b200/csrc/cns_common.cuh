@@ -52,6 +52,7 @@ struct Scheme {
   double xk, eta, dt1min;
   int ischema;      // 7 Roe, 1 Jameson
   double ki2, ki4;  // Jameson dissipation coefficients
+  int ncychro, icychr0;  // time-step update frequency of the fused iteration
 };
 
 // 2.5D tiles of the implicit sweeps: tile t = (block, i0, j0, k0) covers

@@ -129,7 +129,8 @@ class CodeNS:
                             int(getattr(s, "qfix_dfez", qfix_dfez)),
                             int(getattr(s, "precision", 0)), int(getattr(s, "kdefect", 4)),
                             int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
-                            float(getattr(s, "ki4", 1.0 / 32.0)))
+                            float(getattr(s, "ki4", 1.0 / 32.0)),
+                            int(getattr(s, "ncychro", 1)), int(getattr(s, "icychr0", 0)))
 
     def _check(self, rc: int, where: str):
         if rc:

@@ -99,6 +99,12 @@ typedef struct {
                             (dissip_jameson + sch_jameson, kprec = 0) */
   double ki2, ki4;       /* Jameson 2nd/4th-difference coefficients (ki2(lm),
                             ki4(lm); one value for every block) */
+  int32_t ncychro;       /* the fused iteration number n (1, 2, ... since the
+                            state was bound) recomputes the time step when
+                            n mod ncychro = 1 or n < icychr0, and otherwise keeps
+                            the previous one (atsch_num.f90:173-178, 436);
+                            ncychro <= 1: every iteration */
+  int32_t icychr0;
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
