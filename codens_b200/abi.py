@@ -37,7 +37,7 @@ class Scheme_t(C.Structure):
                 ("eta", c_f64), ("kdtl", c_i32), ("dt1min", c_f64), ("lmax", c_i32),
                 ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32),
                 ("ischema", c_i32), ("ki2", c_f64), ("ki4", c_f64), ("ncychro", c_i32),
-                ("icychr0", c_i32)]
+                ("icychr0", c_i32), ("kfmg", c_i32), ("kdualns", c_i32)]
 
 
 class Bnd_t(C.Structure):
@@ -56,7 +56,7 @@ class Sa_t(C.Structure):
 class State_t(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in
                 ("v", "u", "d", "dt", "sn", "vol", "pression", "ztemp", "cson",
-                 "mu", "mut", "tau")]
+                 "mu", "mut", "tau", "ptdual", "vdual", "vdual1", "vdual2")]
 
 
 EXPORTS = [
@@ -74,6 +74,7 @@ EXPORTS = [
     "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
     "cns_set_sa", "cns_met_num",
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
+    "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
 ]
 
 _lib = None
@@ -153,6 +154,11 @@ def load(build_if_missing: bool = True):
     L.cns_writdg.argtypes = [vp, cs, cs, vp, vp, vp]
     L.cns_readda.argtypes = [vp, cs, cs, C.c_int, vp, vp]
     L.cns_writda.argtypes = [vp, cs, cs, cs, vp, vp]
+    L.cns_set_cycle.argtypes = [vp, c_i64, c_i64]
+    L.cns_sch_duin.argtypes = [vp]
+    L.cns_sch_duup.argtypes = [vp]
+    L.cns_set_dual_cycle.argtypes = [vp, C.c_int]
+    L.cns_sch_dual.argtypes = [vp, C.c_int, vp, vp, C.c_int, vp, vp]
     for f in EXPORTS:
         getattr(L, f).restype = getattr(L, f).restype or C.c_int
     L.cns_last_error.restype = C.c_char_p

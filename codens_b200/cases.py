@@ -82,6 +82,8 @@ class Scheme:
     ki4: float = 1.0 / 32.0  # Jameson 4th-difference coefficient ki4(lm)
     ncychro: int = 1     # time step recomputed when n mod ncychro = 1 or n < icychr0
     icychr0: int = 0     # (atsch_num.f90:173-178, 436); ncychro <= 1: every iteration
+    kfmg: int = 0        # 3: dual time stepping, physical time step dt1min
+    kdualns: int = 0     # dual time order: 0, 1 second (BDF2), 2 third
 
 
 @dataclass

@@ -70,6 +70,8 @@ struct cns_ctx {
   long long kernels_launched = 0;        // kernels of every fused-step graph launched
   long long mixed_iter = 0;              // mixed iterations since the last reset
   long long ncyc = 0;                    // fused iterations since the state was bound
+  long long cyc_n = 0, cyc_i = 0;        // the reference's ncyc, icyc of the last iteration
+  int dual_icycle = 1;                   // physical step index of sch_dual (kfmg = 3)
   long long io_maxsub = 2147483639;      // bytes per subrecord of the files written
   IoStage io_stage;                      // pinned ring of the file readers and writers
   std::string err;
@@ -211,11 +213,24 @@ void drop_graphs(cns_ctx* c) {
   c->mixed_iter = 0;
 }
 
-// atsch_num.f90:173-178, 436: whether iteration n (1-based since the state
-// was bound) recomputes the time step
-bool dt_due(const cns_ctx* c, long long n) {
+// atsch_num.f90:173-178, 436: whether the iteration with counters ncyc = n,
+// icyc = i recomputes the time step
+bool dt_due(const cns_ctx* c, long long n, long long i) {
   const int nc = c->sc.ncychro;
-  return nc <= 1 || n % nc == 1 || n < c->sc.icychr0;
+  return nc <= 1 || n % nc == 1 || i < c->sc.icychr0;
+}
+
+// sch_dual.f90:18-19, sch_dual2.f90:18-19
+double dual_fact(const cns_ctx* c) {
+  if (c->dual_icycle <= 1) return 1.;
+  return c->sc.kdualns == 2 ? 11. / 6. : 1.5;
+}
+
+// the physical time term after the residual (atsch_num.f90:993-1003)
+cudaError_t enqueue_dual(cns_ctx* c, float* u32) {
+  const cns_state_t& s = c->state;
+  return launch_dual(c->d_blks, c->cells.view(-1), c->lay.ld, dual_fact(c), 1. / c->sc.dt1min,
+                     s.v, s.vol, s.ptdual, s.u, u32, c->st);
 }
 
 int check_status(cns_ctx* c) {
@@ -415,6 +430,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
     else
       e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
   }
+  if (e == cudaSuccess && c->sc.kfmg == 3) e = enqueue_dual(c, nullptr);
   if (e == cudaSuccess)
     e = launch_implicit(c->d_blks, all, c->tiles64.view(-1), c->faces, -1, c->ph, c->sc,
                         !c->sc.ns,
@@ -515,9 +531,11 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
   }
+  if (e == cudaSuccess && c->sc.kfmg == 3) e = enqueue_dual(c, w.u32);
   // single-precision coefficients and implicit sweeps, FP64 update
   if (e == cudaSuccess)
-    e = launch_coefficients32(c->d_blks, all, c->ph, !c->sc.ns, ld, s.dt, s.v, w.prim32,
+    e = launch_coefficients32(c->d_blks, all, c->ph, !c->sc.ns, ld,
+                              c->sc.kfmg == 3 ? c->sc.dt1min : 0., s.dt, s.v, w.prim32,
                               s.mu, s.mut, w.sn32, s.vol, s.cson, w.coefe32, w.coefdiag32,
                               c->st);
   int cur = 0;
@@ -875,10 +893,13 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (!c || !s) return CNS_EINVAL;
   if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
       s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1) ||
-      (s->ischema != 1 && s->ischema != 7) || (s->ischema == 1 && s->precision == 2))
+      (s->ischema != 1 && s->ischema != 7) || (s->ischema == 1 && s->precision == 2) ||
+      (s->kfmg != 0 && s->kfmg != 3) ||
+      (s->kfmg == 3 && (!(s->dt1min > 0.) || s->kdualns < 0 || s->kdualns > 2)))
     return fail(c, CNS_EINVAL,
                 "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
-                "kdefect >= 1, ischema in {1,7} (defect correction: Roe only)");
+                "kdefect >= 1, ischema in {1,7} (defect correction: Roe only), kfmg in "
+                "{0,3} (3: dt1min > 0, kdualns in {0,1,2})");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
   c->sc.xk = s->xk;
@@ -895,6 +916,8 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.ki4 = s->ki4;
   c->sc.ncychro = s->ncychro;
   c->sc.icychr0 = s->icychr0;
+  c->sc.kfmg = s->kfmg;
+  c->sc.kdualns = s->kdualns;
   drop_graphs(c);
   return CNS_OK;
 }
@@ -1264,9 +1287,10 @@ int cns_adjoint_prepare(cns_ctx* c) {
   if (!c) return CNS_EINVAL;
   if (!c->bound || !c->metric_done)
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
-  if (c->sc.ns || jameson(c) || c->sc.muscl < 0 || c->sc.muscl > 1 || c->sc.ilim != 0)
-    return fail(c, CNS_EINVAL, "the adjoint covers the Euler Roe scheme (ns = 0, ischema 7, "
-                               "first order or unlimited MUSCL)");
+  if (c->sc.ns || jameson(c) || c->sc.muscl < 0 || c->sc.muscl > 1 || c->sc.ilim != 0 ||
+      c->sc.kfmg == 3)
+    return fail(c, CNS_EINVAL, "the adjoint covers the steady Euler Roe scheme (ns = 0, "
+                               "ischema 7, kfmg 0, first order or unlimited MUSCL)");
   if (!c->sc.qfix_dfez)
     return fail(c, CNS_EINVAL, "the adjoint needs qfix_dfez = 1 (the reference Euler implicit "
                                "phase is not linear in the increment)");
@@ -1390,7 +1414,7 @@ int cns_bind_state(cns_ctx* c, const cns_state_t* s) {
     return CNS_EINVAL;
   c->state = *s;
   c->bound = true;
-  c->ncyc = 0;
+  c->ncyc = c->cyc_n = c->cyc_i = 0;
   drop_graphs(c);
   return CNS_OK;
 }
@@ -1399,6 +1423,12 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return CNS_EINVAL;
   if (!c->bound || !c->metric_done)
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
+  if (c->sc.kfmg == 3) {
+    const cns_state_t& s = c->state;
+    if (!s.ptdual || !s.vdual || !s.vdual1 || !s.vdual2)
+      return fail(c, CNS_ENOTREADY, "dual time stepping: bind ptdual, vdual, vdual1, vdual2");
+    if (c->sa_on) return fail(c, CNS_EINVAL, "dual time stepping with the SA step");
+  }
   if (c->sc.kdtl == 0) CK(ensure_dtpart(c));
   if (nsteps == 0) return CNS_OK;
   const int prec = c->sc.precision;
@@ -1411,7 +1441,7 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   // Jameson cycle (rfve before the dissipation): run it eagerly (the
   // launches the graph would hold), tune the sweep tiles on its data, then
   // capture the steady-state iteration with the chosen tiles
-  const bool first = c->ncyc == 0;
+  const bool first = c->cyc_n == 0;  // the next iteration is the reference's ncyc = 1
   const bool tuned = prec == 0 ? c->tuned64 : c->tuned32;
   const bool eager = !tuned || (jameson(c) && first);
   auto enqueue = [&](int form, bool fst, bool on) {
@@ -1430,7 +1460,8 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   std::vector<std::pair<int, bool>> plan;  // (form, time step recomputed) per iteration
   if (eager) {
     const int form = next_form();
-    const bool on = dt_due(c, ++c->ncyc);
+    ++c->ncyc;
+    const bool on = dt_due(c, ++c->cyc_n, ++c->cyc_i);
     CK(enqueue(form, first, on));
     if (!tuned) {
       CK(tune_sweeps(c, prec != 0));
@@ -1440,7 +1471,11 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
     plan.emplace_back(form, on);  // counted below with the launches of its graph
   }
   const size_t replay0 = plan.size();
-  for (int q = 0; q < nsteps; ++q) plan.emplace_back(next_form(), dt_due(c, ++c->ncyc));
+  c->ncyc += nsteps;
+  for (int q = 0; q < nsteps; ++q) {
+    const int form = next_form();
+    plan.emplace_back(form, dt_due(c, ++c->cyc_n, ++c->cyc_i));
+  }
   // capture the graphs these iterations need, then replay them in order
   for (const auto& fo : plan) {
     cudaGraphExec_t& g = c->gexec[fo.first][fo.second];
@@ -1588,6 +1623,54 @@ int cns_writda(cns_ctx* c, const char* path, const char* disc, const char* equat
     for (int a = 5; a < 7 && ke; ++a) cns::io_add(p, (int)b, w + a * ld, 0, lo, hi);
   }
   return cns::io_write(c->io_stage, p, c->d_blks, path, c->io_maxsub, c->st, c->err);
+}
+
+/* ---- iteration counters and dual time stepping -------------------------- */
+
+int cns_set_cycle(cns_ctx* c, int64_t ncyc, int64_t icyc) {
+  if (!c || ncyc < 0 || icyc < 0) return CNS_EINVAL;
+  c->cyc_n = ncyc;
+  c->cyc_i = icyc;
+  return CNS_OK;
+}
+
+int cns_set_dual_cycle(cns_ctx* c, int icycle) {
+  if (!c) return CNS_EINVAL;
+  const double before = dual_fact(c);
+  c->dual_icycle = icycle;
+  if (dual_fact(c) != before) drop_graphs(c);  // sch_dual's factor is a graph constant
+  return CNS_OK;
+}
+
+int cns_sch_duin(cns_ctx* c) {
+  if (!c) return CNS_EINVAL;
+  const cns_state_t& s = c->state;
+  if (!c->bound || !s.ptdual || !s.vdual || !s.vdual1 || !s.vdual2)
+    return fail(c, CNS_ENOTREADY, "bind the state with its dual time arrays first");
+  CK(launch_dual_update(c->d_blks, c->cells.view(-1), c->lay.ld, 0, s.v, s.ptdual, s.vdual,
+                        s.vdual1, s.vdual2, c->st));
+  return CNS_OK;
+}
+
+int cns_sch_duup(cns_ctx* c) {
+  if (!c) return CNS_EINVAL;
+  const cns_state_t& s = c->state;
+  if (!c->bound || !s.ptdual || !s.vdual || !s.vdual1 || !s.vdual2)
+    return fail(c, CNS_ENOTREADY, "bind the state with its dual time arrays first");
+  CK(launch_dual_update(c->d_blks, c->cells.view(-1), c->lay.ld, c->sc.kdualns == 2 ? 2 : 1,
+                        s.v, s.ptdual, s.vdual, s.vdual1, s.vdual2, c->st));
+  return CNS_OK;
+}
+
+int cns_sch_dual(cns_ctx* c, int l, double* u, const double* v, int icycle, const double* vol,
+                 const double* ptdual) {
+  if (!c || bad_block(c, l) || l == 0 || !u || !v || !vol || !ptdual) return CNS_EINVAL;
+  if (!(c->sc.dt1min > 0.)) return fail(c, CNS_EINVAL, "sch_dual needs dt1min > 0");
+  double fact = c->sc.kdualns == 2 ? 11. / 6. : 1.5;
+  if (icycle <= 1) fact = 1.;
+  CK(launch_dual(c->d_blks, c->cells.view(l - 1), c->lay.ld, fact, 1. / c->sc.dt1min, v, vol,
+                 ptdual, u, nullptr, c->st));
+  return CNS_OK;
 }
 
 }  // extern "C"

@@ -53,6 +53,7 @@ struct Scheme {
   int ischema;      // 7 Roe, 1 Jameson
   double ki2, ki4;  // Jameson dissipation coefficients
   int ncychro, icychr0;  // time-step update frequency of the fused iteration
+  int kfmg, kdualns;     // 3: dual time stepping (dt1min = physical step); its order
 };
 
 // 2.5D tiles of the implicit sweeps: tile t = (block, i0, j0, k0) covers

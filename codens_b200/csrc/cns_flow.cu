@@ -451,10 +451,11 @@ __global__ void __launch_bounds__(kTile) k_grad(const Blk* __restrict__ blks,
   tau[8 * ld + n] = kq * g[11];
 }
 
-// per real cell: coefdiag seed (vol/dt or vol*(0+1/dt)) and the viscous
-// spectral factor rv (implimf_3d.f90:95-105, implimf_eu.f90:124-134)
+// per real cell: coefdiag seed (vol/dt, or vol*(fact+1/dt) with fact = 0 or,
+// with dual time stepping, 1.5/dt1min) and the viscous spectral factor rv
+// (implimf_3d.f90:95-105, implimf_eu.f90:82-85, 124-134)
 __global__ void __launch_bounds__(kTile) k_impl_cell0(
-    const Blk* __restrict__ blks, Space sp, Phys ph, int eu,
+    const Blk* __restrict__ blks, Space sp, Phys ph, int eu, double fact,
     const double* __restrict__ v, const double* __restrict__ dt,
     const double* __restrict__ mu, const double* __restrict__ mut,
     const double* __restrict__ vol, double* coefdiag, double* rv) {
@@ -462,7 +463,6 @@ __global__ void __launch_bounds__(kTile) k_impl_cell0(
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const long long n = cell_index(blks[b], i, j, k);
   if (eu) {
-    const double fact = 0.;
     coefdiag[n] = vol[n] * (fact + 1. / dt[n]);
   } else {
     rv[n] = ph.gam * (mu[n] / ph.pr + mut[n] / ph.prt) / v[n];
@@ -507,11 +507,15 @@ __global__ void __launch_bounds__(kTile) k_impl_coefe(
 }
 
 // per real cell: coefdiag += coefe of the six faces (implimf_eu.f90:161-170,
-// implimf_3d.f90:192-203: the same left-to-right chain)
+// implimf_3d.f90:192-203: the same left-to-right chain); dtpas > 0: then
+// + 1.5*vol/dtpas, the physical time term of dual time stepping
+// (implimf_3d.f90:213-224)
 template <class TO>
 __global__ void __launch_bounds__(kTile) k_impl_diag(const Blk* __restrict__ blks,
                                                      Space sp, long long ld,
                                                      const double* __restrict__ coefe,
+                                                     const double* __restrict__ vol,
+                                                     double dtpas,
                                                      double* coefdiag, TO* coefdiag_out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
@@ -524,6 +528,7 @@ __global__ void __launch_bounds__(kTile) k_impl_diag(const Blk* __restrict__ blk
     c = c + coefe[(long long)dir * ld + n];
     c = c + coefe[(long long)dir * ld + n + inc];
   }
+  if (dtpas > 0.) c = c + 1.5 * vol[n] / dtpas;
   coefdiag[n] = c;
   if (coefdiag_out) coefdiag_out[n] = (TO)c;
 }
@@ -855,22 +860,25 @@ cudaError_t launch_update_t<double>(const Blk* blks, Space cells, long long ld,
 template <class TO>
 static cudaError_t implicit_coefficients(const Blk* blks, Space cells,
                                          const SpaceBuf* faces, int l0, Phys ph, int eu,
-                                         const double* dt, const double* v,
+                                         double dtpas, const double* dt, const double* v,
                                          const double* prim, const double* mu,
                                          const double* mut, const double* sn,
                                          const double* vol, const double* cson, Work& w,
                                          TO* coefe_out, TO* coefdiag_out, cudaStream_t st) {
   const long long ld = w.ld;
   const int g = grid_of(cells);
-  k_impl_cell0<<<g, kTile, 0, st>>>(blks, cells, ph, eu, v, dt, mu, mut, vol, w.coefdiag,
-                                    w.rv);
+  // dtpas > 0: dual time stepping with physical step dtpas
+  const double fact = dtpas > 0. ? 1.5 / dtpas : 0.;
+  k_impl_cell0<<<g, kTile, 0, st>>>(blks, cells, ph, eu, fact, v, dt, mu, mut, vol,
+                                    w.coefdiag, w.rv);
   for (int dir = 0; dir < 3; ++dir) {
     const Space fs = faces[dir].view(l0);
     if (fs.ntiles > 0)
       k_impl_coefe<TO><<<fs.ntiles, kTile, 0, st>>>(blks, fs, dir, eu, v, prim, ld, sn, vol,
                                                     cson, w.rv, w.coefe, coefe_out);
   }
-  k_impl_diag<TO><<<g, kTile, 0, st>>>(blks, cells, ld, w.coefe, w.coefdiag, coefdiag_out);
+  k_impl_diag<TO><<<g, kTile, 0, st>>>(blks, cells, ld, w.coefe, vol, eu ? 0. : dtpas,
+                                       w.coefdiag, coefdiag_out);
   return cudaGetLastError();
 }
 
@@ -883,7 +891,7 @@ cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
                                          float* coefe32, float* coefdiag32,
                                          cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
-  return implicit_coefficients<float>(blks, cells, faces, l0, ph, eu, dt, v, prim, mu, mut,
+  return implicit_coefficients<float>(blks, cells, faces, l0, ph, eu, 0., dt, v, prim, mu, mut,
                                       sn, vol, cson, w, coefe32, coefdiag32, st);
 }
 
@@ -896,7 +904,8 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, Tiles tl, const SpaceB
                             int want_norms, cudaStream_t st) {
   const long long ld = w.ld;
   if (cells.ntiles == 0) return cudaSuccess;
-  cudaError_t e = implicit_coefficients<double>(blks, cells, faces, l0, ph, eu, dt, v, w.prim,
+  cudaError_t e = implicit_coefficients<double>(blks, cells, faces, l0, ph, eu,
+                                                sc.kfmg == 3 ? sc.dt1min : 0., dt, v, w.prim,
                                                 mu, mut, sn, vol, cson, w, nullptr, nullptr,
                                                 st);
   int cur = 0;
@@ -907,6 +916,79 @@ cudaError_t launch_implicit(const Blk* blks, Space cells, Tiles tl, const SpaceB
     e = launch_update_t<double>(blks, cells, ld, w.dpp[cur], v, dt, d_out,
                                 want_norms ? w.normpart : nullptr, st);
   return e;
+}
+
+// sch_dual.f90:18-52 / sch_dual2.f90:18-52: u += vol*dti*(fact*v + ptdual)
+// on the real cells (the physical time term of dual time stepping); u32:
+// the single-precision copy of u the FP32 sweeps read, refreshed
+__global__ void __launch_bounds__(kTile) k_dual(const Blk* __restrict__ blks, Space sp,
+                                                long long ld, double fact, double dti,
+                                                const double* __restrict__ v,
+                                                const double* __restrict__ vol,
+                                                const double* __restrict__ ptdual,
+                                                double* __restrict__ u, float* __restrict__ u32) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  const double c0 = vol[n] * dti;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const double r = u[a * ld + n] + c0 * (fact * v[a * ld + n] + ptdual[a * ld + n]);
+    u[a * ld + n] = r;
+    if (u32) u32[a * ld + n] = (float)r;
+  }
+}
+
+// the physical-step arrays on the real cells: mode 0 = sch_duin.f90 after
+// utinia.f90:140-160 (vdual = vdual1 = vdual2 = v, ptdual = -vdual); mode 1
+// = sch_duup.f90 (vdual1 = vdual, vdual = v, ptdual = -2 vdual + 0.5 vdual1);
+// mode 2 = sch_duup2.f90 (vdual2 = vdual1, vdual1 = vdual, vdual = v,
+// ptdual = -3 vdual + 1.5 vdual1 - vdual2/3)
+__global__ void __launch_bounds__(kTile) k_dual_update(const Blk* __restrict__ blks, Space sp,
+                                                       long long ld, int mode,
+                                                       const double* __restrict__ v,
+                                                       double* ptdual, double* vdual,
+                                                       double* vdual1, double* vdual2) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  const double c13 = 1. / 3.;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const long long q = a * ld + n;
+    if (mode == 0) {
+      vdual[q] = v[q];
+      vdual1[q] = v[q];
+      vdual2[q] = v[q];
+      ptdual[q] = -vdual[q];
+    } else if (mode == 1) {
+      vdual1[q] = vdual[q];
+      vdual[q] = v[q];
+      ptdual[q] = -2. * vdual[q] + 0.5 * vdual1[q];
+    } else {
+      vdual2[q] = vdual1[q];
+      vdual1[q] = vdual[q];
+      vdual[q] = v[q];
+      ptdual[q] = -3. * vdual[q] + 1.5 * vdual1[q] - c13 * vdual2[q];
+    }
+  }
+}
+
+cudaError_t launch_dual(const Blk* blks, Space cells, long long ld, double fact, double dti,
+                        const double* v, const double* vol, const double* ptdual, double* u,
+                        float* u32, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_dual<<<cells.ntiles, kTile, 0, st>>>(blks, cells, ld, fact, dti, v, vol, ptdual, u, u32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dual_update(const Blk* blks, Space cells, long long ld, int mode,
+                               const double* v, double* ptdual, double* vdual, double* vdual1,
+                               double* vdual2, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_dual_update<<<cells.ntiles, kTile, 0, st>>>(blks, cells, ld, mode, v, ptdual, vdual,
+                                                  vdual1, vdual2);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_norm_partials(const Blk* blks, Space cells, long long ld,

@@ -76,6 +76,16 @@ int io_read(IoStage& stage, const IoPlan& p, const IoPlan& zero, const Blk* d_bl
 int io_write(IoStage& stage, const IoPlan& p, const Blk* d_blks, const char* path,
              long long maxsub, cudaStream_t st, std::string& err);
 
+// dual time stepping: sch_dual (u += vol*dti*(fact*v + ptdual), u32 refreshed
+// when given) and the physical-step arrays (mode 0 sch_duin, 1 sch_duup,
+// 2 sch_duup2)
+cudaError_t launch_dual(const Blk* blks, Space cells, long long ld, double fact, double dti,
+                        const double* v, const double* vol, const double* ptdual, double* u,
+                        float* u32, cudaStream_t st);
+cudaError_t launch_dual_update(const Blk* blks, Space cells, long long ld, int mode,
+                               const double* v, double* ptdual, double* vdual, double* vdual1,
+                               double* vdual2, cudaStream_t st);
+
 // the 2.5D tile list of one sweep configuration
 struct TileBuf {
   int ti = 0, tj = 0, kc = 0, ntiles = 0;
@@ -373,6 +383,7 @@ cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const doub
 // the FP32 implicit coefficients (coefe32 per face, coefdiag32 per cell) of
 // the mixed sweeps in one pass over the real cells
 cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
+                                  double dtpas,
                                   const double* dt, const double* v, const float* prim32,
                                   const double* mu, const double* mut, const float* sn32,
                                   const double* vol, const double* cson, float* coefe32,

@@ -70,7 +70,7 @@ __device__ __forceinline__ float face_coef(const float* __restrict__ prim, long 
 // pass over memory).
 template <bool EU>
 __global__ void __launch_bounds__(kTile) k_coef32(
-    const Blk* __restrict__ blks, Space sp, Phys ph, long long ld,
+    const Blk* __restrict__ blks, Space sp, Phys ph, long long ld, double dtpas,
     const double* __restrict__ dt, const double* __restrict__ v,
     const float* __restrict__ prim, const double* __restrict__ mu,
     const double* __restrict__ mut, const float* __restrict__ sn,
@@ -86,7 +86,8 @@ __global__ void __launch_bounds__(kTile) k_coef32(
     return (gp * (float)mu[m] + gpt * (float)mut[m]) / (float)v[m];
   };
   const float rv0 = rv_of(n, true);
-  float cd = (float)(vol[n] / dt[n]);
+  // dtpas > 0: dual time stepping (implimf_eu.f90:82-85, implimf_3d.f90:213-224)
+  float cd = (float)(EU && dtpas > 0. ? vol[n] * (1.5 / dtpas + 1. / dt[n]) : vol[n] / dt[n]);
 #pragma unroll
   for (int dir = 0; dir < 3; ++dir) {
     const long long inc = ninc_of(B, dir);
@@ -104,23 +105,25 @@ __global__ void __launch_bounds__(kTile) k_coef32(
     if (p == nd - 1) coefe[(long long)dir * ld + nu] = ceu;
     cd = cd + cel + ceu;
   }
+  if (!EU && dtpas > 0.) cd = cd + (float)(1.5 * vol[n] / dtpas);
   coefdiag[n] = cd;
 }
 
 }  // namespace
 
 cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
+                                  double dtpas,
                                   const double* dt, const double* v, const float* prim32,
                                   const double* mu, const double* mut, const float* sn32,
                                   const double* vol, const double* cson, float* coefe32,
                                   float* coefdiag32, cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
   if (eu)
-    k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dt, v, prim32, mu,
+    k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
                                                      mut, sn32, vol, cson, coefe32,
                                                      coefdiag32);
   else
-    k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dt, v, prim32, mu,
+    k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
                                                       mut, sn32, vol, cson, coefe32,
                                                       coefdiag32);
   return cudaGetLastError();

@@ -113,11 +113,17 @@ class CodeNS:
         self.mu = torch.zeros(ld, **f64)
         self.mut = torch.zeros(ld, **f64)
         self.tau = torch.zeros(9 * ld, **f64)
+        # dual time stepping: the physical-step arrays of smg_num.f90, (ld, 5)
+        if int(getattr(case.scheme, "kfmg", 0)) == 3:
+            self.ptdual, self.vdual, self.vdual1, self.vdual2 = (
+                torch.zeros(5 * ld, **f64) for _ in range(4))
+        else:
+            self.ptdual = self.vdual = self.vdual1 = self.vdual2 = None
         torch.cuda.synchronize()
-        st = abi.State_t(*[C.c_void_p(t.data_ptr()) for t in
+        st = abi.State_t(*[C.c_void_p(t.data_ptr()) if t is not None else None for t in
                            (self.v, self.u, self.d, self.dt, self.sn, self.vol,
                             self.pression, self.ztemp, self.cson, self.mu, self.mut,
-                            self.tau)])
+                            self.tau, self.ptdual, self.vdual, self.vdual1, self.vdual2)])
         self._check(self.lib.cns_bind_state(ctx, C.byref(st)), "cns_bind_state")
         self._metric_done = False
 
@@ -130,7 +136,8 @@ class CodeNS:
                             int(getattr(s, "precision", 0)), int(getattr(s, "kdefect", 4)),
                             int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
                             float(getattr(s, "ki4", 1.0 / 32.0)),
-                            int(getattr(s, "ncychro", 1)), int(getattr(s, "icychr0", 0)))
+                            int(getattr(s, "ncychro", 1)), int(getattr(s, "icychr0", 0)),
+                            int(getattr(s, "kfmg", 0)), int(getattr(s, "kdualns", 0)))
 
     def _check(self, rc: int, where: str):
         if rc:
@@ -326,6 +333,58 @@ class CodeNS:
 
     def met_num(self):
         self._check(self.lib.cns_met_num(self.ctx), "cns_met_num")
+
+    # iteration counters and dual time stepping
+    def set_cycle(self, ncyc: int, icyc: int):
+        """the reference's ncyc, icyc of the last iteration done"""
+        self._check(self.lib.cns_set_cycle(self.ctx, int(ncyc), int(icyc)), "cns_set_cycle")
+
+    def sch_duin(self):
+        self._check(self.lib.cns_sch_duin(self.ctx), "cns_sch_duin")
+
+    def sch_duup(self):
+        self._check(self.lib.cns_sch_duup(self.ctx), "cns_sch_duup")
+
+    def set_dual_cycle(self, icycle: int):
+        self._check(self.lib.cns_set_dual_cycle(self.ctx, int(icycle)), "cns_set_dual_cycle")
+
+    def sch_dual(self, l, u, v, icycle, vol, ptdual):
+        self._check(self.lib.cns_sch_dual(self.ctx, l, _ptr(u), _ptr(v), int(icycle), _ptr(vol),
+                                          _ptr(ptdual)), "cns_sch_dual")
+
+    def dual_time(self, ncycl: int, niter: int, tol: float, start: bool = True):
+        """the physical time loop of smg_num.f90:130-470 for kfmg = 3: ncycl
+        physical steps of at most niter pseudo-time iterations, each step
+        ending when the density residual relative to the first iteration's
+        falls to tol (dua_resro.f90; here from the fused step's L2 norm of
+        (v - u0)/dt, which differs from dua_resro's by the constant factor
+        1/sqrt(real cells), so only the last bits of the ratio can differ),
+        then sch_duup.  start: run sch_duin first (a fresh physical time
+        loop).  Returns the inner iteration count of each physical step."""
+        if self.ptdual is None:
+            raise ValueError("dual time stepping needs a case with scheme.kfmg = 3")
+        if not self._metric_done:
+            self.metric()
+        if start:
+            self.sch_duin()
+            self._resno1 = None
+        counts = []
+        for icycle in range(1, ncycl + 1):
+            self.set_dual_cycle(icycle)
+            # smg_num.f90:130-147: icyc restarts with each physical step and
+            # ncyc = icycle + iter - 1
+            self.set_cycle(icycle - 1, 0)
+            it = 0
+            for it in range(1, niter + 1):
+                norms = self.atsch_num(1)
+                r = float(norms[1, 0])
+                if self._resno1 is None:
+                    self._resno1 = r if abs(r) >= np.finfo(np.float64).tiny else 1.0
+                if r / self._resno1 <= tol:
+                    break
+            counts.append(it)
+            self.sch_duup()
+        return counts
 
     # reference grid and flow files (Fortran unformatted sequential)
     def set_subrecord_length(self, nbytes: int):

@@ -105,6 +105,10 @@ typedef struct {
                             the previous one (atsch_num.f90:173-178, 436);
                             ncychro <= 1: every iteration */
   int32_t icychr0;
+  int32_t kfmg;          /* 0: steady; 3: dual time stepping (smg_num.f90:110,
+                            atsch_num.f90:993-1003) with physical step dt1min */
+  int32_t kdualns;       /* dual time: 0 or 1 second order (sch_dual, sch_duup),
+                            2 third order (sch_dual2, sch_duup2) */
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
@@ -130,6 +134,9 @@ typedef struct {
 typedef struct {
   double *v, *u, *d, *dt, *sn, *vol;
   double *pression, *ztemp, *cson, *mu, *mut, *tau;
+  /* dual time stepping only (else NULL): (ld, 5) arrays ptdual, vdual,
+     vdual1, vdual2 of smg_num.f90 */
+  double *ptdual, *vdual, *vdual1, *vdual2;
 } cns_state_t;
 
 /* ---- context ---------------------------------------------------------- */
@@ -337,6 +344,28 @@ int cns_atsch_num_step(cns_ctx *ctx, int nsteps, double *norms);
  * for the stream and checks the device status word */
 int cns_atsch_num_launch(cns_ctx *ctx, int nsteps);
 int cns_last_norms(cns_ctx *ctx, double *norms);
+
+/* Iteration counters of the fused step: the reference's ncyc (global) and
+ * icyc (within the current run or physical step) of the LAST iteration done;
+ * each fused iteration advances both before use.  They select the time-step
+ * updates (ncychro, icychr0) and the Jameson first cycle (ncyc = 1).
+ * cns_bind_state sets both to 0. */
+int cns_set_cycle(cns_ctx *ctx, int64_t ncyc, int64_t icyc);
+
+/* Dual time stepping (kfmg = 3).  cns_sch_duin: the start of the physical
+ * time loop on the bound state (vdual = vdual1 = vdual2 = v as utinia.f90:
+ * 140-160 / readda.f90:150-176 set them, then sch_duin.f90: ptdual = -vdual);
+ * cns_set_dual_cycle: the physical step index icycle the fused step's
+ * sch_dual uses (fact = 1 for icycle <= 1); cns_sch_duup: the end of a
+ * physical step (sch_duup.f90 or sch_duup2.f90 by kdualns) on the bound
+ * state; cns_sch_dual: sch_dual.f90 / sch_dual2.f90 on block l with the
+ * caller's arrays.  The Spalart-Allmaras step and the adjoint do not run
+ * with dual time stepping (CNS_EINVAL). */
+int cns_sch_duin(cns_ctx *ctx);
+int cns_sch_duup(cns_ctx *ctx);
+int cns_set_dual_cycle(cns_ctx *ctx, int icycle);
+int cns_sch_dual(cns_ctx *ctx, int l, double *u, const double *v, int icycle,
+                 const double *vol, const double *ptdual);
 
 /* Jacobi sweep tiling (no counterpart in the reference).  Every sweep after
  * the first runs 2.5D-blocked over patches of ti x tj cell columns, kc

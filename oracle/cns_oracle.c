@@ -35,6 +35,9 @@ static struct {
   double xk, eta, dt1min;
   int ischema;           /* 1: Jameson (central + scalar dissipation), 7: Roe */
   double ki2, ki4;       /* Jameson dissipation coefficients ki2(lm), ki4(lm) */
+  /* dual time stepping (kfmg = 3): dt1min is the physical time step */
+  int kfmg, kdualns, icycle;
+  double *ptdual;
   /* boundary */
   int nbnd;
   int32_t *btype, *bblk, *bface, *bmmb, *bpart;
@@ -1605,13 +1608,14 @@ static void jacobi_faces(const blk_t *b, int eu, const double *d,
   }
 }
 
-/* implimf_eu.f90:79-330 (kfmg!=3, ityprk=0) */
+/* implimf_eu.f90:79-330 (ityprk=0; kfmg=3 adds the physical time term) */
 void orc_implimf_eu(int l, const double *u, const double *dt, double *v,
                     double *d, const double *sn, const double *vol,
                     const double *ps, const double *cson, int lmx) {
   const blk_t *b = &G.b[l - 1];
   const int64_t L = G.ld, n0 = b->npc;
-  const double gam1 = G.gam1, pinfl = G.pinfl, fact = 0.;
+  /* implimf_eu.f90:82-85: fact = 1.5/dt1min with dual time stepping */
+  const double gam1 = G.gam1, pinfl = G.pinfl, fact = G.kfmg == 3 ? 1.5 / G.dt1min : 0.;
   impl_work w;
   impl_alloc(b, &w);
   for (int a = 0; a < 5; ++a)
@@ -1702,7 +1706,7 @@ void orc_implimf_eu(int l, const double *u, const double *dt, double *v,
   impl_free(&w);
 }
 
-/* implimf_3d.f90:64-490 (kfmg!=3, ityprk=0) */
+/* implimf_3d.f90:64-490 (ityprk=0; kfmg=3 adds the physical time term) */
 void orc_implimf_3d(int l, const double *u, const double *dt, double *v,
                     double *d, const double *mu, const double *mut,
                     const double *sn, const double *vol, const double *ps,
@@ -1750,6 +1754,15 @@ void orc_implimf_3d(int l, const double *u, const double *dt, double *v,
                         w.coefe[1][m] + w.coefe[1][m + ncj] + w.coefe[2][m] +
                         w.coefe[2][m + nck];
       }
+  /* implimf_3d.f90:213-224: the physical time term of dual time stepping
+   * (fact = 1.5, dtpas = dt1min) */
+  if (G.kfmg == 3)
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          int64_t n = IC(b, i, j, k), m = n - n0;
+          w.coefdiag[m] = w.coefdiag[m] + 1.5 * vol[n] / G.dt1min;
+        }
   for (int ls = 1; ls <= lmx; ++ls) {
     for (int k = 1; k <= b->nk - 1; ++k)
       for (int j = 1; j <= b->nj - 1; ++j)
@@ -2644,6 +2657,8 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
   if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol);
   if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
   for (int l = 1; l <= G.nblk; ++l) orc_sch_jameson(l, u, v, dis, tau, sn, ps);
+  if (G.kfmg == 3)
+    for (int l = 1; l <= G.nblk; ++l) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
   for (int l = 1; l <= G.nblk; ++l) {
     if (G.ns)
       orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
@@ -2671,9 +2686,11 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
   for (int l = 1; l <= G.nblk; ++l) {
     if (G.ns) {
       orc_sch_roe(l, u, v, tau, sn, ps);
+      if (G.kfmg == 3) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
       orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
     } else {
       orc_sch_roe_euler(l, u, v, sn, ps);
+      if (G.kfmg == 3) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
       orc_implimf_eu(l, u, dt, v, d, sn, vol, ps, cson, G.lmax);
     }
   }
@@ -2891,3 +2908,77 @@ int orc_readda(const char *path, const char *equat, int keinit, double *v, doubl
   fclose(f);
   return rc;
 }
+
+/* ---- dual time stepping (kfmg = 3) -------------------------------------- */
+void orc_set_dual(int kfmg, int kdualns, int icycle, double *ptdual) {
+  G.kfmg = kfmg;
+  G.kdualns = kdualns;
+  G.icycle = icycle;
+  G.ptdual = ptdual;
+}
+
+/* sch_dual.f90:18-52 (kdualns 0, 1) and sch_dual2.f90:18-52 (kdualns 2):
+ * u += vol/dt1min * (fact*v + ptdual) on the real cells */
+void orc_sch_dual(int l, double *u, const double *v, int icycle, const double *vol,
+                  const double *ptdual) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld;
+  double fact = G.kdualns == 2 ? 11. / 6. : 1.5;
+  if (icycle <= 1) fact = 1.;
+  const double dti = 1. / G.dt1min;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        int64_t n = IC(b, i, j, k);
+        double c0 = vol[n] * dti;
+        for (int a = 0; a < 5; ++a) u[a * L + n] = u[a * L + n] + c0 * (fact * v[a * L + n] + ptdual[a * L + n]);
+      }
+}
+
+/* the real cells of every block, in block, k, j, i order */
+#define FOR_REAL_CELLS(n)                                 \
+  for (int l_ = 0; l_ < G.nblk; ++l_)                     \
+    for (int k_ = 1; k_ <= G.b[l_].nk - 1; ++k_)          \
+      for (int j_ = 1; j_ <= G.b[l_].nj - 1; ++j_)        \
+        for (int i_ = 1; i_ <= G.b[l_].ni - 1; ++i_)      \
+          for (int64_t n = IC(&G.b[l_], i_, j_, k_), once_ = 1; once_; once_ = 0)
+
+/* utinia.f90:140-160 / readda.f90:150-176 (vdual = vdual1 = vdual2 = v)
+ * then sch_duin.f90 (ptdual = -vdual) */
+void orc_sch_duin(const double *v, double *ptdual, double *vdual, double *vdual1,
+                  double *vdual2) {
+  const int64_t L = G.ld;
+  FOR_REAL_CELLS(n) {
+    for (int a = 0; a < 5; ++a) {
+      vdual[a * L + n] = v[a * L + n];
+      vdual1[a * L + n] = v[a * L + n];
+      vdual2[a * L + n] = v[a * L + n];
+      ptdual[a * L + n] = -vdual[a * L + n];
+    }
+  }
+}
+
+/* sch_duup.f90 (kdualns 0, 1): vdual1 = vdual, vdual = v,
+ * ptdual = -2 vdual + 0.5 vdual1; sch_duup2.f90 (kdualns 2): vdual2 =
+ * vdual1, vdual1 = vdual, vdual = v, ptdual = -3 vdual + 1.5 vdual1 - vdual2/3 */
+void orc_sch_duup(const double *v, double *ptdual, double *vdual, double *vdual1,
+                  double *vdual2) {
+  const int64_t L = G.ld;
+  const double c13 = 1. / 3.;
+  FOR_REAL_CELLS(n) {
+    for (int a = 0; a < 5; ++a) {
+      const int64_t q = a * L + n;
+      if (G.kdualns == 2) {
+        vdual2[q] = vdual1[q];
+        vdual1[q] = vdual[q];
+        vdual[q] = v[q];
+        ptdual[q] = -3. * vdual[q] + 1.5 * vdual1[q] - c13 * vdual2[q];
+      } else {
+        vdual1[q] = vdual[q];
+        vdual[q] = v[q];
+        ptdual[q] = -2. * vdual[q] + 0.5 * vdual1[q];
+      }
+    }
+  }
+}
+#undef FOR_REAL_CELLS

@@ -171,6 +171,17 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);
 
+/* dual time stepping (kfmg = 3; dt1min of orc_set_scheme is the physical
+ * time step): the fused step adds sch_dual after the residual with the
+ * physical step index icycle and the array ptdual given here */
+void orc_set_dual(int kfmg, int kdualns, int icycle, double *ptdual);
+void orc_sch_dual(int l, double *u, const double *v, int icycle, const double *vol,
+                  const double *ptdual);
+void orc_sch_duin(const double *v, double *ptdual, double *vdual, double *vdual1,
+                  double *vdual2);
+void orc_sch_duup(const double *v, double *ptdual, double *vdual, double *vdual1,
+                  double *vdual2);
+
 /* reference grid and flow files (readdg.f90, svgr.f90 -> writdg.f90,
  * readda.f90, svfw.f90 -> writda.f90), every block in order, gfortran's
  * unformatted sequential records (4-byte markers, subrecords of at most

@@ -82,6 +82,10 @@ def lib():
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 8
         L.orc_set_sa_fix.argtypes = [C.c_int]
+        L.orc_set_dual.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_sch_dual.argtypes = [C.c_int, _d, _d, C.c_int, _d, _d]
+        L.orc_sch_duin.argtypes = [_d] * 5
+        L.orc_sch_duup.argtypes = [_d] * 5
         cs = C.c_char_p
         L.orc_writdg.argtypes = [cs, cs, _d, _d, _d, C.c_int64]
         L.orc_readdg.argtypes = [cs, _d, _d, _d]
@@ -133,6 +137,8 @@ class Oracle:
                        p.aa1, p.omg)
         self.set_scheme(case.scheme)
         self.clear_sa()
+        L.orc_set_dual(0, 0, 0, None)
+        self._dual = None
         ba = case.boundary_arrays()
         self._ba = ba
         L.orc_set_boundaries(len(ba["type"]), ba["type"], ba["blk"], ba["face"],
@@ -160,6 +166,23 @@ class Oracle:
         lib().orc_set_sa(1, a["dist"].ctypes.data, rokinf, roeinf, epsk, harten, epsroe, sigma,
                          a["fd"].ctypes.data, a["ts"].ctypes.data, a["cfke"].ctypes.data)
         lib().orc_set_sa_fix(int(stilde_fix))
+
+    def set_dual(self, st: OracleState, kdualns: int = 0):
+        """dual time stepping (kfmg = 3; the scheme's dt1min is the physical
+        time step): allocates ptdual, vdual, vdual1, vdual2 on the state and
+        runs sch_duin on its v"""
+        ld = st.ld
+        st.ptdual, st.vdual, st.vdual1, st.vdual2 = (np.zeros(5 * ld) for _ in range(4))
+        self._dual = (kdualns, st.ptdual)
+        lib().orc_set_dual(3, kdualns, 1, st.ptdual.ctypes.data)
+        lib().orc_sch_duin(st.v[:5 * ld], st.ptdual, st.vdual, st.vdual1, st.vdual2)
+
+    def set_dual_cycle(self, icycle: int):
+        kdualns, pt = self._dual
+        lib().orc_set_dual(3, kdualns, int(icycle), pt.ctypes.data)
+
+    def sch_duup(self, st: OracleState):
+        lib().orc_sch_duup(st.v[:5 * st.ld], st.ptdual, st.vdual, st.vdual1, st.vdual2)
 
     def clear_sa(self):
         lib().orc_set_sa(0, None, 0.0, 0.0, 0.0, 0, 0.0, 1.0, None, None, None)
