@@ -79,7 +79,7 @@ def parse():
     p.add_argument("--rans-iters", type=int, default=3000,
                    help="rans workload: iterations of the convergence history")
     p.add_argument("--workload", default="channel",
-                   choices=["channel", "batch", "adjoint", "rans"],
+                   choices=["channel", "batch", "adjoint", "rans", "dual"],
                    help="channel: the 8-block NS channel; batch: 64 independent Euler boxes "
                         "in one launch against the same boxes one at a time")
     p.add_argument("--tiles", default=None,
@@ -722,6 +722,95 @@ def run_rans(args):
     return 0
 
 
+def run_dual(args):
+    """Dual time stepping (kfmg = 3) on the channel workload: the fused
+    pseudo-time iteration with sch_dual and the physical time term, FP64 and
+    mixed, against the steady iteration of the same case; the physical-step
+    update (sch_duup) and sch_dual alone; and one physical step run to an
+    inner tolerance through the host loop (a norm read per iteration)."""
+    import torch
+    from codens_b200.solver import CodeNS
+
+    torch.cuda.set_device(0)
+    warm = max(args.warmup, 3)
+    steps = args.steps
+    dt_phys = 0.05
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def timed(s, k):
+        s.sync()
+        a, e = ev(), ev()
+        a.record(s.stream)
+        s.atsch_num_launch(k)
+        e.record(s.stream)
+        e.synchronize()
+        return a.elapsed_time(e)
+
+    out = {}
+    for name in ("fp64", "mixed"):
+        case = make_case(args)
+        case.scheme.precision = PRECISION[name]
+        case.scheme.kfmg, case.scheme.dt1min = 3, dt_phys
+        nreal = case.layout.nreal
+        s = CodeNS(case)
+        s.metric()
+        s.sch_duin()
+        s.set_dual_cycle(2)          # the BDF2 form of every later physical step
+        s.atsch_num(warm)
+        ms = timed(s, steps)
+        s.sync()
+        a, e = ev(), ev()
+        a.record(s.stream)
+        for _ in range(5):
+            s.sch_duup()
+        e.record(s.stream)
+        e.synchronize()
+        ms_duup = a.elapsed_time(e) / 5
+        a.record(s.stream)
+        for _ in range(5):
+            for l in range(1, case.layout.nblk + 1):
+                s.sch_dual(l, s.u, s.v, 2, s.vol, s.ptdual)
+        e.record(s.stream)
+        e.synchronize()
+        ms_dual = a.elapsed_time(e) / 5
+        rec = {"value": nreal * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
+               "sch_duup_ms": ms_duup, "sch_dual_ms": ms_dual,
+               "kernels_launched": s.kernels_launched}
+        # one physical step to an inner tolerance of 1e-2 through the host loop
+        s.sync()
+        t0 = time.perf_counter()
+        counts = s.dual_time(1, 200, 1e-2, start=True)
+        s.sync()
+        rec["physical_step"] = {"inner_iterations": counts[0],
+                                "wall_ms": (time.perf_counter() - t0) * 1e3}
+        s.close()
+        # the steady iteration of the same case, for the cost of the dual terms
+        case.scheme.kfmg = 0
+        s = CodeNS(case)
+        s.metric()
+        s.atsch_num(warm)
+        ms0 = timed(s, steps)
+        rec["steady_ms_per_step"] = ms0 / steps
+        rec["dual_over_steady_time"] = (ms / steps) / (ms0 / steps)
+        s.close()
+        out[name] = rec
+    line = {
+        "metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": steps, "warmup": warm, "ms_per_step": out["mixed"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPE["mixed"], "data": "synthetic (seeded noisy freestream)",
+        "config": {**config_of(case, args, 1),
+                   "workload": "dual time stepping (kfmg 3, BDF2) on the laminar NS bump "
+                               f"channel, physical step {dt_phys}, lmax={args.lmax}",
+                   "dt1min": dt_phys},
+        "fp64": out["fp64"], "mixed": out["mixed"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -732,6 +821,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "rans":
         return run_rans(args)
+    if args.workload == "dual":
+        return run_dual(args)
     return run_ours(args)
 
 
