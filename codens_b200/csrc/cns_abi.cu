@@ -263,10 +263,17 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
     e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
   if (e == cudaSuccess)
     e = launch_face_flux(c->d_blks, c->faces, l0, c->ph, c->sc, v, c->w.prim, ld, ps, tau,
-                         sn, c->w.R, c->w.G, c->st);
+                         sn, c->w.R, c->w.G, c->st, c->w.V);
   if (e == cudaSuccess)
-    e = launch_accumulate(c->d_blks, c->cells.view(l0), c->w.G, ld, u, c->st);
+    e = launch_accumulate(c->d_blks, c->cells.view(l0), c->w.G, ld, u, c->st, c->w.V);
   return e;
+}
+
+// the HLLC viscous halves (sch_hllc with the stresses), allocated when the
+// scheme first asks for them (never inside a graph capture)
+cudaError_t ensure_hllc_v(cns_ctx* c) {
+  if (c->w.V || c->sc.ischema != 14 || !c->sc.ns) return cudaSuccess;
+  return dev_alloc(c, &c->w.V, (size_t)(12 * c->lay.ld));
 }
 
 cudaError_t ensure_dis(cns_ctx* c) {
@@ -505,16 +512,18 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
                                 c->st);
     if (e == cudaSuccess)
       e = launch_face_flux_t<float>(c->d_blks, c->faces, -1, c->ph, c->sc, w.v32, w.prim32,
-                                    ld, w.ps32, w.tau32, w.sn32, w.R32, w.G32, c->st);
+                                    ld, w.ps32, w.tau32, w.sn32, w.R32, w.G32, c->st,
+                                    nullptr);
   }
   if (mode == kDefectRegular) {
     if (e == cudaSuccess)
-      e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, w.corr, s.u, w.u32, c->st);
+      e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, w.corr, s.u, w.u32, c->st,
+                                     nullptr);
   } else {
     // the FP64 residual; the defect refresh also keeps R32 alone for corr
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_accumulate_t<float>(c->d_blks, all, w.G32, ld, nullptr, w.ur32, nullptr,
-                                     c->st);
+                                     c->st, nullptr);
     if (jameson(c)) {
       if (e == cudaSuccess)
         e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
@@ -524,9 +533,10 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
       if (e == cudaSuccess)
         e = launch_face_flux_fma(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
-                                 s.pression, s.tau, s.sn, w.R, w.G, c->st);
+                                 s.pression, s.tau, s.sn, w.R, w.G, c->st, w.V);
       if (e == cudaSuccess)
-        e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st);
+        e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st,
+                                        w.V);
     }
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
@@ -855,6 +865,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.normpart, (size_t)(15 * c->cells.ntiles));
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.norms, 16);
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.blocksum, (size_t)(15 * c->lay.blks.size()));
+  if (e == cudaSuccess) e = ensure_hllc_v(c);
   if (e == cudaSuccess) e = dev_alloc(c, &c->w.status, 1);
   if (e == cudaSuccess) e = cudaMallocHost(&c->h_norms, 16 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&c->h_status, sizeof(int));
@@ -893,12 +904,13 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (!c || !s) return CNS_EINVAL;
   if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
       s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1) ||
-      (s->ischema != 1 && s->ischema != 7) || (s->ischema == 1 && s->precision == 2) ||
+      (s->ischema != 1 && s->ischema != 7 && s->ischema != 9 && s->ischema != 14) ||
+      (s->ischema != 7 && s->precision == 2) ||
       (s->kfmg != 0 && s->kfmg != 3) ||
       (s->kfmg == 3 && (!(s->dt1min > 0.) || s->kdualns < 0 || s->kdualns > 2)))
     return fail(c, CNS_EINVAL,
                 "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
-                "kdefect >= 1, ischema in {1,7} (defect correction: Roe only), kfmg in "
+                "kdefect >= 1, ischema in {1,7,9,14} (defect correction: Roe only), kfmg in "
                 "{0,3} (3: dt1min > 0, kdualns in {0,1,2})");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
@@ -919,6 +931,7 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.kfmg = s->kfmg;
   c->sc.kdualns = s->kdualns;
   drop_graphs(c);
+  if (c->w.ld > 0) CK(ensure_hllc_v(c));
   return CNS_OK;
 }
 
@@ -1010,6 +1023,7 @@ int cns_sch_roe_euler(cns_ctx* c, int l, double* u, const double* v,
   if (!c || bad_block(c, l) || !u || !v || !sn || !ps) return CNS_EINVAL;
   const Scheme keep = c->sc;
   c->sc.ns = 0;
+  c->sc.ischema = 7;
   CK(zero_cols(c, u, 5, l));
   cudaError_t e = prim_of(c, l, v);
   if (e == cudaSuccess) e = residual(c, l - 1, u, v, nullptr, sn, ps);
@@ -1023,12 +1037,47 @@ int cns_sch_roe(cns_ctx* c, int l, double* u, const double* v, const double* tau
   if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
   const Scheme keep = c->sc;
   c->sc.ns = 1;
+  c->sc.ischema = 7;
   CK(zero_cols(c, u, 5, l));
   cudaError_t e = prim_of(c, l, v);
   if (e == cudaSuccess) e = residual(c, l - 1, u, v, tau, sn, ps);
   c->sc = keep;
   CK(e);
   return CNS_OK;
+}
+
+// one block's residual with the flux family ischema (ns: the equations'
+// form, Rusanov always with the stresses)
+static int other_family(cns_ctx* c, int l, int ischema, int ns, double* u, const double* v,
+                 const double* tau, const double* sn, const double* ps) {
+  const Scheme keep = c->sc;
+  c->sc.ns = ns;
+  c->sc.ischema = ischema;
+  cudaError_t e = ensure_hllc_v(c);
+  if (e == cudaSuccess) e = zero_cols(c, u, 5, l);
+  if (e == cudaSuccess) e = prim_of(c, l, v);
+  if (e == cudaSuccess) e = residual(c, l - 1, u, v, tau, sn, ps);
+  c->sc = keep;
+  CK(e);
+  return CNS_OK;
+}
+
+int cns_sch_hllc_euler(cns_ctx* c, int l, double* u, const double* v, const double* sn,
+                       const double* ps) {
+  if (!c || bad_block(c, l) || l == 0 || !u || !v || !sn || !ps) return CNS_EINVAL;
+  return other_family(c, l, 14, 0, u, v, nullptr, sn, ps);
+}
+
+int cns_sch_hllc(cns_ctx* c, int l, double* u, const double* v, const double* tau,
+                 const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || l == 0 || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  return other_family(c, l, 14, 1, u, v, tau, sn, ps);
+}
+
+int cns_sch_rusanov(cns_ctx* c, int l, double* u, const double* v, const double* tau,
+                    const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || l == 0 || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  return other_family(c, l, 9, c->sc.ns, u, v, tau, sn, ps);
 }
 
 int cns_rfve(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
@@ -1287,8 +1336,8 @@ int cns_adjoint_prepare(cns_ctx* c) {
   if (!c) return CNS_EINVAL;
   if (!c->bound || !c->metric_done)
     return fail(c, CNS_ENOTREADY, "bind the state and run cns_metric first");
-  if (c->sc.ns || jameson(c) || c->sc.muscl < 0 || c->sc.muscl > 1 || c->sc.ilim != 0 ||
-      c->sc.kfmg == 3)
+  if (c->sc.ns || c->sc.ischema != 7 || c->sc.muscl < 0 || c->sc.muscl > 1 ||
+      c->sc.ilim != 0 || c->sc.kfmg == 3)
     return fail(c, CNS_EINVAL, "the adjoint covers the steady Euler Roe scheme (ns = 0, "
                                "ischema 7, kfmg 0, first order or unlimited MUSCL)");
   if (!c->sc.qfix_dfez)

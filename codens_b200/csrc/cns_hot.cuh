@@ -257,6 +257,97 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   }
 }
 
+// flux families of the face kernel (atsch_num.f90:628-983 by ischema)
+enum { kFluxRoe = 0, kFluxHllc = 1, kFluxRusanov = 2 };
+
+// the HLLC flux (sch_hllc_euler.f90:135-221, sch_hllc.f90:270-357): the
+// left or right physical flux, or the star state's; absam: the sound speed
+// from |gam1 (hm - vitm2)| (sch_hllc.f90, i and j directions)
+template <class T>
+__device__ __forceinline__ void hllc_flux(const T WL[5], const T WR[5], T s1, T s2, T s3,
+                                          bool absam, const PhysT<T>& ph, T fc[5]) {
+  const T gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl;
+  const T one = T(1.), h = T(0.5), zero = T(0.);
+  const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const T cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const T nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
+  const T al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
+  const T hl = al * al / gam1 + h * q2l, hr = ar * ar / gam1 + h * q2r;
+  const T el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
+  const T er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
+  const T vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
+  const T gd = sqrt(rhor / rhol), gd1 = one / (one + gd), gd2 = gd * gd1;
+  const T um = gd1 * ul + gd2 * ur, vm = gd1 * vl + gd2 * vr, wm = gd1 * wl + gd2 * wr;
+  const T hm = gd1 * hl + gd2 * hr;
+  const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
+  const T am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
+  const T vnm = um * nx + vm * ny + wm * nz;
+  const T sl = vnm - am, sr = vnm + am;
+  const T sst = (rhor * vnr * (sr - vnr) - rhol * vnl * (sl - vnl) + pl - prr) /
+                (rhor * (sr - vnr) - rhol * (sl - vnl));
+  const T pst = rhol * (vnl - sl) * (vnl - sst) + pl;
+  if (sl > zero || sr < zero) {
+    const bool left = sl > zero;
+    const T rho = left ? rhol : rhor, u = left ? ul : ur, v = left ? vl : vr,
+            w = left ? wl : wr, p = left ? pl : prr, e = left ? el : er;
+    const T fxx = rho * sqT(u) + p - pinfl, fxy = rho * u * v, fxz = rho * u * w;
+    const T fyy = rho * sqT(v) + p - pinfl, fyz = rho * v * w, fzz = rho * sqT(w) + p - pinfl;
+    const T fex = (rho * e + p - pinfl) * u, fey = (rho * e + p - pinfl) * v,
+            fez = (rho * e + p - pinfl) * w;
+    fc[0] = rho * u * s1 + rho * v * s2 + rho * w * s3;
+    fc[1] = fxx * s1 + fxy * s2 + fxz * s3;
+    fc[2] = fxy * s1 + fyy * s2 + fyz * s3;
+    fc[3] = fxz * s1 + fyz * s2 + fzz * s3;
+    fc[4] = fex * s1 + fey * s2 + fez * s3;
+  } else if (sst >= zero || sst < zero) {
+    const bool left = sst >= zero;
+    const T rho = left ? rhol : rhor, u = left ? ul : ur, v = left ? vl : vr,
+            w = left ? wl : wr, p = left ? pl : prr, e = left ? el : er,
+            vn = left ? vnl : vnr, sk = left ? sl : sr;
+    const T ids = one / (sk - sst);
+    const T rhost = rho * (sk - vn);
+    const T rhoust = (rhost * u + (pst - p) * nx) * ids;
+    const T rhovst = (rhost * v + (pst - p) * ny) * ids;
+    const T rhowst = (rhost * w + (pst - p) * nz) * ids;
+    const T rhoest = (rho * e * (sk - vn) + (pst - pinfl) * sst - (p - pinfl) * vn) * ids;
+    fc[0] = rhost * ids * sst * cnds;
+    fc[1] = (rhoust * sst + (pst - pinfl) * nx) * cnds;
+    fc[2] = (rhovst * sst + (pst - pinfl) * ny) * cnds;
+    fc[3] = (rhowst * sst + (pst - pinfl) * nz) * cnds;
+    fc[4] = (rhoest + pst - pinfl) * sst * cnds;
+  } else {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) fc[a] = sst;  // NaN in, NaN out
+  }
+}
+
+// Rusanov dissipation rm (W_R - W_L), rm = |S| max(|vnl + al|, |vnr + ar|)
+// (sch_rusanov.f90:129-156), and the specific total energies el, er
+template <class T>
+__device__ __forceinline__ void rusanov_dissipation(const T WL[5], const T WR[5], T s1, T s2,
+                                                    T s3, const PhysT<T>& ph, T di[5], T& el,
+                                                    T& er) {
+  const T gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl, h = T(0.5);
+  const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const T cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const T nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
+  const T al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
+  el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
+  er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
+  const T vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
+  const T al1 = fabs(vnl + al), ar1 = fabs(vnr + ar);
+  const T rm = cnds * (al1 >= ar1 ? al1 : ar1);
+  di[0] = rm * (rhor - rhol);
+  di[1] = rm * (rhor * ur - rhol * ul);
+  di[2] = rm * (rhor * vr - rhol * vl);
+  di[3] = rm * (rhor * wr - rhol * wl);
+  di[4] = rm * (rhor * er - rhol * el);
+}
+
 // primitive (rho, u, v, w, p) of cell n
 template <class T>
 __device__ __forceinline__ void load_prim(const T* __restrict__ v,
@@ -271,15 +362,18 @@ __device__ __forceinline__ void load_prim(const T* __restrict__ v,
 }
 
 // one face per thread, direction dir: interior faces give 0.5*f (sch_roe*
-// interior loops), boundary faces give the ghost-cell physical flux s (lower
-// face 1, upper face nd).  Results go to G[dir][a][n], n the cell above the
-// face.
-template <class T, bool NS>
+// and sch_rusanov interior loops) or the HLLC flux fc (sch_hllc*), boundary
+// faces give the ghost-cell physical flux s (lower face 1, upper face nd).
+// Results go to G[dir][a][n], n the cell above the face; HLLC with the
+// stresses also writes the halves of its viscous flux 0.5*fv to
+// V[dir][a-1][n] (a = 1..4), which sch_hllc.f90 applies as a second term.
+// FL: kFluxRoe, kFluxHllc or kFluxRusanov (Rusanov with NS = true always).
+template <class T, bool NS, int FL = kFluxRoe>
 __global__ void __launch_bounds__(kTile, 4) k_face_flux(
     const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
     const T* __restrict__ v, const T* __restrict__ prim, long long ld,
     const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
-    const T* __restrict__ R, T* __restrict__ G) {
+    const T* __restrict__ R, T* __restrict__ G, T* __restrict__ V = nullptr) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const PhysT<T> ph(ph64);
@@ -297,6 +391,7 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
     // 438-513, sch_roe.f90:497-580); the Euler j/k lower faces divide the
     // energy flux by the interior density (sch_roe_euler.f90:630-632)
     const long long ng = (p == 1) ? n - inc : n;
+    // (the Euler forms of Roe and HLLC; Rusanov always has the NS form)
     const long long nrho = (!NS && p == 1 && dir > 0) ? n : ng;
     const T v1 = v[ng], v2 = v[ld + ng], v3 = v[2 * ld + ng], v4 = v[3 * ld + ng],
             v5 = v[4 * ld + ng], pg = ps[ng];
@@ -339,7 +434,7 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
     T WL[5], WR[5];
     const T c4 = T(0.25) * T(sc.muscl);
     const T xk = T(sc.xk);
-    if (NS && sc.ilim == 1 && p <= nd - 2) {
+    if (FL != kFluxRusanov && NS && sc.ilim == 1 && p <= nd - 2) {
       const T* Rd = R + (long long)dir * 5 * ld;
       T rm[5], rp[5];
 #pragma unroll
@@ -351,8 +446,40 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
     } else {
       muscl_plain(c, c4, xk, WL, WR);
     }
+    if (FL == kFluxHllc) {
+      hllc_flux(WL, WR, sx, sy, sz, NS && dir < 2, ph, out);
+      if (NS) {
+        // sch_hllc.f90:358-375
+        const long long nR = n, nL = n - inc;
+        const T ul = WL[1], vl = WL[2], wl = WL[3], ur = WR[1], vr = WR[2], wr = WR[3];
+        const T txxR = tau[nR], txyR = tau[ld + nR], txzR = tau[2 * ld + nR],
+                tyyR = tau[3 * ld + nR], tyzR = tau[4 * ld + nR], tzzR = tau[5 * ld + nR];
+        const T txxL = tau[nL], txyL = tau[ld + nL], txzL = tau[2 * ld + nL],
+                tyyL = tau[3 * ld + nL], tyzL = tau[4 * ld + nL], tzzL = tau[5 * ld + nL];
+        T fv[4];
+        fv[0] = (txxR + txxL) * sx + (txyR + txyL) * sy + (txzR + txzL) * sz;
+        fv[1] = (txyR + txyL) * sx + (tyyR + tyyL) * sy + (tyzR + tyzL) * sz;
+        fv[2] = (txzR + txzL) * sx + (tyzR + tyzL) * sy + (tzzR + tzzL) * sz;
+        fv[3] = (txxR * ur + txyR * vr + txzR * wr + txxL * ul + txyL * vl + txzL * wl +
+                 tau[6 * ld + nR] + tau[6 * ld + nL]) * sx +
+                (txyR * ur + tyyR * vr + tyzR * wr + txyL * ul + tyyL * vl + tyzL * wl +
+                 tau[7 * ld + nR] + tau[7 * ld + nL]) * sy +
+                (txzR * ur + tyzR * vr + tzzR * wr + txzL * ul + tyzL * vl + tzzL * wl +
+                 tau[8 * ld + nR] + tau[8 * ld + nL]) * sz;
+        T* Vd = V + (long long)dir * 4 * ld;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) Vd[a * ld + n] = T(0.5) * fv[a];
+      }
+      T* Gd = G + (long long)dir * 5 * ld;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
+      return;
+    }
     T di[5], el, er;
-    roe_dissipation(WL, WR, sx, sy, sz, (!NS) && dir > 0, ph, di, el, er);
+    if (FL == kFluxRusanov)
+      rusanov_dissipation(WL, WR, sx, sy, sz, ph, di, el, er);
+    else
+      roe_dissipation(WL, WR, sx, sy, sz, (!NS) && dir > 0, ph, di, el, er);
     const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
     const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
     T dfxx, dfxy, dfxz, dfyy, dfyz, dfzz, dfex, dfey, dfez;
@@ -405,16 +532,52 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
   for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
 }
 
+// the FP64 face kernels of one residual by flux family (atsch_num.f90:628-983):
+// ischema 14 HLLC (sch_hllc / sch_hllc_euler), 9 Rusanov (sch_rusanov, the
+// stresses always), else Roe; each translation unit instantiates it with its
+// own contraction flags
+static inline cudaError_t face_flux_dispatch(const Blk* blks, const SpaceBuf* faces, int l0,
+                                             Phys ph, Scheme sc, const double* v,
+                                             const double* prim, long long ld,
+                                             const double* ps, const double* tau,
+                                             const double* sn, const double* R, double* G,
+                                             double* V, cudaStream_t st) {
+  for (int dir = 0; dir < 3; ++dir) {
+    const Space sp = faces[dir].view(l0);
+    if (sp.ntiles == 0) continue;
+    const int g = sp.ntiles;
+    if (sc.ischema == 14 && sc.ns)
+      k_face_flux<double, true, kFluxHllc><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                               ld, ps, tau, sn, R, G, V);
+    else if (sc.ischema == 14)
+      k_face_flux<double, false, kFluxHllc><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                                prim, ld, ps, tau, sn, R, G);
+    else if (sc.ischema == 9)
+      k_face_flux<double, true, kFluxRusanov><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
+                                                                  prim, ld, ps, tau, sn, R, G);
+    else if (sc.ns)
+      k_face_flux<double, true><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim, ld, ps,
+                                                     tau, sn, R, G);
+    else
+      k_face_flux<double, false><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim, ld, ps,
+                                                      tau, sn, R, G);
+  }
+  return cudaGetLastError();
+}
+
 // u(n) from the six faces of the cell, summed in FP64 in the reference's
 // order; with corr (defect correction, FP64) u = that sum + corr; with u32 a
 // single-precision copy of u is written too
+// V (HLLC with the stresses): the halves 0.5*fv of the interior faces'
+// viscous flux, applied after each face's fc as sch_hllc.f90:376-385 does
 template <class T>
 __global__ void __launch_bounds__(kTile) k_accumulate(const Blk* __restrict__ blks,
                                                       Space sp, const T* __restrict__ G,
                                                       long long ld,
                                                       const double* __restrict__ corr,
                                                       double* __restrict__ u,
-                                                      float* __restrict__ u32) {
+                                                      float* __restrict__ u32,
+                                                      const T* __restrict__ V = nullptr) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -426,16 +589,21 @@ __global__ void __launch_bounds__(kTile) k_accumulate(const Blk* __restrict__ bl
     const int nd = nd_of(B, dir);
     const int p = dir == 0 ? i : (dir == 1 ? j : k);
     const bool upper_first = (p == 1) && nd >= 3;
+    const bool vlo = V && p >= 2, vup = V && p <= nd - 2;  // interior faces
     const T* Gd = G + (long long)dir * 5 * ld;
+    const T* Vd = V + (long long)dir * 4 * ld;
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
       const double gl = (double)Gd[a * ld + n], gu = (double)Gd[a * ld + n + inc];
       if (upper_first) {
         acc[a] = acc[a] + gu;
+        if (vup && a > 0) acc[a] = acc[a] - (double)Vd[(a - 1) * ld + n + inc];
         acc[a] = acc[a] - gl;
       } else {
         acc[a] = acc[a] - gl;
+        if (vlo && a > 0) acc[a] = acc[a] + (double)Vd[(a - 1) * ld + n];
         acc[a] = acc[a] + gu;
+        if (vup && a > 0) acc[a] = acc[a] - (double)Vd[(a - 1) * ld + n + inc];
       }
     }
   }

@@ -116,6 +116,7 @@ struct Work {
   double* dtpart = nullptr;   // global time step: per-tile minima + the result
   double* G = nullptr;        // face fluxes, [3][5][ld]
   double* R = nullptr;        // limiter ratios, [3][5][ld]
+  double* V = nullptr;        // HLLC viscous halves, [3][4][ld] (ischema 14 with ns)
   double* coefe = nullptr;    // [3][ld]
   double* coefdiag = nullptr; // [ld]
   double* rv = nullptr;       // [ld]
@@ -174,16 +175,19 @@ template <class T>
 cudaError_t launch_ratio_t(const Blk* blks, const SpaceBuf* lines, int l0, const T* v,
                            const T* prim, long long ld, const T* ps, T* R,
                            cudaStream_t st);
+// the face fluxes of the flux family sc.ischema selects (7 Roe, 14 HLLC,
+// 9 Rusanov); V: the HLLC viscous halves (ischema 14 with ns, [3][4][ld])
 template <class T>
 cudaError_t launch_face_flux_t(const Blk* blks, const SpaceBuf* faces, int l0, Phys ph,
                                Scheme sc, const T* v, const T* prim, long long ld,
                                const T* ps, const T* tau, const T* sn, const T* R, T* G,
-                               cudaStream_t st);
-// u = FP64 sum of the face fluxes (+ corr); u32 an optional float copy
+                               cudaStream_t st, T* V);
+// u = FP64 sum of the face fluxes (+ corr); u32 an optional float copy; V as
+// above or null
 template <class T>
 cudaError_t launch_accumulate_t(const Blk* blks, Space sp, const T* G, long long ld,
                                 const double* corr, double* u, float* u32,
-                                cudaStream_t st);
+                                cudaStream_t st, const T* V);
 // lmx Jacobi sweeps over the real cells; the final iterate is in dpp[*cur_out]
 template <class T>
 cudaError_t launch_sweeps_t(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
@@ -204,10 +208,11 @@ cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T*
   template <>                                                                               \
   cudaError_t launch_face_flux_t<T>(const Blk*, const SpaceBuf*, int, Phys, Scheme,        \
                                     const T*, const T*, long long, const T*, const T*,     \
-                                    const T*, const T*, T*, cudaStream_t);                  \
+                                    const T*, const T*, T*, cudaStream_t, T*);              \
   template <>                                                                               \
   cudaError_t launch_accumulate_t<T>(const Blk*, Space, const T*, long long,               \
-                                     const double*, double*, float*, cudaStream_t);        \
+                                     const double*, double*, float*, cudaStream_t,         \
+                                     const T*);                                             \
   template <>                                                                               \
   cudaError_t launch_sweeps_t<T>(const Blk*, Space, Tiles, Phys, Scheme, int, int, long long, \
                                  const T*, const T*, const T*, const T*, const T*,          \
@@ -352,13 +357,14 @@ inline cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int 
                                     Phys ph, Scheme sc, const double* v,
                                     const double* prim, long long ld, const double* ps,
                                     const double* tau, const double* sn, const double* R,
-                                    double* G, cudaStream_t st) {
+                                    double* G, cudaStream_t st, double* V = nullptr) {
   return launch_face_flux_t<double>(blks, faces, l0, ph, sc, v, prim, ld, ps, tau, sn, R, G,
-                                    st);
+                                    st, V);
 }
 inline cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
-                                     long long ld, double* u, cudaStream_t st) {
-  return launch_accumulate_t<double>(blks, sp, G, ld, nullptr, u, nullptr, st);
+                                     long long ld, double* u, cudaStream_t st,
+                                     const double* V = nullptr) {
+  return launch_accumulate_t<double>(blks, sp, G, ld, nullptr, u, nullptr, st, V);
 }
 
 // FP64 implicit coefficients with float copies for the mixed sweeps
@@ -394,7 +400,7 @@ cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0,
                                  Scheme sc, const double* v, const double* prim,
                                  long long ld, const double* ps, const double* tau,
                                  const double* sn, const double* R, double* G,
-                                 cudaStream_t st);
+                                 cudaStream_t st, double* V);
 
 // the implicit phase of implimf_eu (eu = 1) or implimf_3d (eu = 0) on the
 // cells of the space: coefficients, lmx Jacobi sweeps, v += d; d_out

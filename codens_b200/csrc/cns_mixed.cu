@@ -158,7 +158,8 @@ cudaError_t launch_face_flux_t<float>(const Blk* blks, const SpaceBuf* faces, in
                                       Phys ph, Scheme sc, const float* v, const float* prim,
                                       long long ld, const float* ps, const float* tau,
                                       const float* sn, const float* R, float* G,
-                                      cudaStream_t st) {
+                                      cudaStream_t st, float* V) {
+  (void)V;  // the single-precision fluxes are Roe only (defect correction)
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = faces[dir].view(l0);
     if (sp.ntiles == 0) continue;
@@ -180,26 +181,16 @@ cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0,
                                  Scheme sc, const double* v, const double* prim,
                                  long long ld, const double* ps, const double* tau,
                                  const double* sn, const double* R, double* G,
-                                 cudaStream_t st) {
-  for (int dir = 0; dir < 3; ++dir) {
-    const Space sp = faces[dir].view(l0);
-    if (sp.ntiles == 0) continue;
-    if (sc.ns)
-      k_face_flux<double, true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
-                                                               prim, ld, ps, tau, sn, R, G);
-    else
-      k_face_flux<double, false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
-                                                                prim, ld, ps, tau, sn, R, G);
-  }
-  return cudaGetLastError();
+                                 cudaStream_t st, double* V) {
+  return face_flux_dispatch(blks, faces, l0, ph, sc, v, prim, ld, ps, tau, sn, R, G, V, st);
 }
 
 template <>
 cudaError_t launch_accumulate_t<float>(const Blk* blks, Space sp, const float* G,
                                        long long ld, const double* corr, double* u,
-                                       float* u32, cudaStream_t st) {
+                                       float* u32, cudaStream_t st, const float* V) {
   if (sp.ntiles > 0)
-    k_accumulate<float><<<grid_of(sp), kTile, 0, st>>>(blks, sp, G, ld, corr, u, u32);
+    k_accumulate<float><<<grid_of(sp), kTile, 0, st>>>(blks, sp, G, ld, corr, u, u32, V);
   return cudaGetLastError();
 }
 

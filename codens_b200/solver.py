@@ -221,6 +221,18 @@ class CodeNS:
         self._check(self.lib.cns_sch_roe(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
                                          _ptr(ps)), "cns_sch_roe")
 
+    def sch_hllc_euler(self, l, u, v, sn, ps):
+        self._check(self.lib.cns_sch_hllc_euler(self.ctx, l, _ptr(u), _ptr(v), _ptr(sn),
+                                                _ptr(ps)), "cns_sch_hllc_euler")
+
+    def sch_hllc(self, l, u, v, tau, sn, ps):
+        self._check(self.lib.cns_sch_hllc(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
+                                          _ptr(ps)), "cns_sch_hllc")
+
+    def sch_rusanov(self, l, u, v, tau, sn, ps):
+        self._check(self.lib.cns_sch_rusanov(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau),
+                                             _ptr(sn), _ptr(ps)), "cns_sch_rusanov")
+
     def chrono_global(self, dt):
         """chrono.f90:113-151: the global time step (kdtl = 0)"""
         self._check(self.lib.cns_chrono_global(self.ctx, _ptr(dt)), "cns_chrono_global")

@@ -1370,6 +1370,248 @@ static void roe_direction(const blk_t *b, int dir, int ns, double *u,
   free(r);
 }
 
+/* ---- other flux families: HLLC (ischema 14), Rusanov (ischema 9) ------ */
+
+/* the HLLC flux through a face (sch_hllc_euler.f90:135-221,
+ * sch_hllc.f90:270-357): the left or right physical flux, or the star
+ * state's; absam: the sound speed from |gam1*(hm - vitm2)| (sch_hllc.f90 in
+ * the i and j directions) */
+static void hllc_core(const double WL[5], const double WR[5], double s1, double s2,
+                      double s3, int absam, double fc[5]) {
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const double cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const double nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
+  const double al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const double q2l = sq(ul) + sq(vl) + sq(wl), q2r = sq(ur) + sq(vr) + sq(wr);
+  const double hl = al * al / gam1 + 0.5 * q2l, hr = ar * ar / gam1 + 0.5 * q2r;
+  const double el = pl / (gam1 * rhol) + 0.5 * q2l + pinfl / rhol;
+  const double er = prr / (gam1 * rhor) + 0.5 * q2r + pinfl / rhor;
+  const double vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
+  const double gd = sqrt(rhor / rhol), gd1 = 1. / (1. + gd), gd2 = gd * gd1;
+  const double um = gd1 * ul + gd2 * ur, vm = gd1 * vl + gd2 * vr, wm = gd1 * wl + gd2 * wr;
+  const double hm = gd1 * hl + gd2 * hr;
+  const double vitm2 = 0.5 * (sq(um) + sq(vm) + sq(wm));
+  const double am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
+  const double vnm = um * nx + vm * ny + wm * nz;
+  const double sl = vnm - am, sr = vnm + am;
+  const double sst = (rhor * vnr * (sr - vnr) - rhol * vnl * (sl - vnl) + pl - prr) /
+                     (rhor * (sr - vnr) - rhol * (sl - vnl));
+  const double pst = rhol * (vnl - sl) * (vnl - sst) + pl;
+  if (sl > 0. || sr < 0.) {
+    const int left = sl > 0.;
+    const double rho = left ? rhol : rhor, u = left ? ul : ur, v = left ? vl : vr,
+                 w = left ? wl : wr, p = left ? pl : prr, e = left ? el : er;
+    const double fxx = rho * sq(u) + p - pinfl, fxy = rho * u * v, fxz = rho * u * w;
+    const double fyy = rho * sq(v) + p - pinfl, fyz = rho * v * w;
+    const double fzz = rho * sq(w) + p - pinfl;
+    const double fex = (rho * e + p - pinfl) * u, fey = (rho * e + p - pinfl) * v,
+                 fez = (rho * e + p - pinfl) * w;
+    fc[0] = rho * u * s1 + rho * v * s2 + rho * w * s3;
+    fc[1] = fxx * s1 + fxy * s2 + fxz * s3;
+    fc[2] = fxy * s1 + fyy * s2 + fyz * s3;
+    fc[3] = fxz * s1 + fyz * s2 + fzz * s3;
+    fc[4] = fex * s1 + fey * s2 + fez * s3;
+  } else if (sst >= 0. || sst < 0.) {
+    const int left = sst >= 0.;
+    const double rho = left ? rhol : rhor, u = left ? ul : ur, v = left ? vl : vr,
+                 w = left ? wl : wr, p = left ? pl : prr, e = left ? el : er,
+                 vn = left ? vnl : vnr, sk = left ? sl : sr;
+    const double ids = 1. / (sk - sst);
+    const double rhost = rho * (sk - vn);
+    const double rhoust = (rhost * u + (pst - p) * nx) * ids;
+    const double rhovst = (rhost * v + (pst - p) * ny) * ids;
+    const double rhowst = (rhost * w + (pst - p) * nz) * ids;
+    const double rhoest = (rho * e * (sk - vn) + (pst - pinfl) * sst - (p - pinfl) * vn) * ids;
+    fc[0] = rhost * ids * sst * cnds;
+    fc[1] = (rhoust * sst + (pst - pinfl) * nx) * cnds;
+    fc[2] = (rhovst * sst + (pst - pinfl) * ny) * cnds;
+    fc[3] = (rhowst * sst + (pst - pinfl) * nz) * cnds;
+    fc[4] = (rhoest + pst - pinfl) * sst * cnds;
+  } else {
+    for (int a = 0; a < 5; ++a) fc[a] = NAN;
+  }
+}
+
+/* the viscous part of sch_hllc.f90:358-375 (fv2..fv5) */
+static void hllc_viscous(const double WL[5], const double WR[5], double s1, double s2,
+                         double s3, const double *tau, int64_t L, int64_t nR, int64_t nL,
+                         double fv[5]) {
+  const double *txx = tau, *txy = tau + L, *txz = tau + 2 * L, *tyy = tau + 3 * L,
+               *tyz = tau + 4 * L, *tzz = tau + 5 * L, *qx = tau + 6 * L, *qy = tau + 7 * L,
+               *qz = tau + 8 * L;
+  const double ul = WL[1], vl = WL[2], wl = WL[3], ur = WR[1], vr = WR[2], wr = WR[3];
+  fv[0] = 0.;
+  fv[1] = (txx[nR] + txx[nL]) * s1 + (txy[nR] + txy[nL]) * s2 + (txz[nR] + txz[nL]) * s3;
+  fv[2] = (txy[nR] + txy[nL]) * s1 + (tyy[nR] + tyy[nL]) * s2 + (tyz[nR] + tyz[nL]) * s3;
+  fv[3] = (txz[nR] + txz[nL]) * s1 + (tyz[nR] + tyz[nL]) * s2 + (tzz[nR] + tzz[nL]) * s3;
+  fv[4] = (txx[nR] * ur + txy[nR] * vr + txz[nR] * wr + txx[nL] * ul + txy[nL] * vl +
+           txz[nL] * wl + qx[nR] + qx[nL]) * s1 +
+          (txy[nR] * ur + tyy[nR] * vr + tyz[nR] * wr + txy[nL] * ul + tyy[nL] * vl +
+           tyz[nL] * wl + qy[nR] + qy[nL]) * s2 +
+          (txz[nR] * ur + tyz[nR] * vr + tzz[nR] * wr + txz[nL] * ul + tyz[nL] * vl +
+           tzz[nL] * wl + qz[nR] + qz[nL]) * s3;
+}
+
+/* the Rusanov flux of sch_rusanov.f90:129-185: the centred flux (viscous
+ * stresses included) minus rm*(W_R - W_L), rm = |S| max(|vnl+al|, |vnr+ar|) */
+static void rusanov_flux(const double WL[5], const double WR[5], double s1, double s2,
+                         double s3, const double *tau, int64_t L, int64_t nR, int64_t nL,
+                         double f[5]) {
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const double cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const double nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
+  const double al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const double q2l = sq(ul) + sq(vl) + sq(wl), q2r = sq(ur) + sq(vr) + sq(wr);
+  const double el = pl / (gam1 * rhol) + 0.5 * q2l + pinfl / rhol;
+  const double er = prr / (gam1 * rhor) + 0.5 * q2r + pinfl / rhor;
+  const double vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
+  const double al1 = fabs(vnl + al), ar1 = fabs(vnr + ar);
+  const double rm = cnds * (al1 >= ar1 ? al1 : ar1);
+  double di[5];
+  di[0] = rm * (rhor - rhol);
+  di[1] = rm * (rhor * ur - rhol * ul);
+  di[2] = rm * (rhor * vr - rhol * vl);
+  di[3] = rm * (rhor * wr - rhol * wl);
+  di[4] = rm * (rhor * er - rhol * el);
+  const double *txx = tau, *txy = tau + L, *txz = tau + 2 * L, *tyy = tau + 3 * L,
+               *tyz = tau + 4 * L, *tzz = tau + 5 * L, *qx = tau + 6 * L, *qy = tau + 7 * L,
+               *qz = tau + 8 * L;
+  const double dfxx = rhor * sq(ur) + prr - pinfl - txx[nR] + rhol * sq(ul) + pl - pinfl - txx[nL];
+  const double dfxy = rhor * ur * vr - txy[nR] + rhol * ul * vl - txy[nL];
+  const double dfxz = rhor * ur * wr - txz[nR] + rhol * ul * wl - txz[nL];
+  const double dfyy = rhor * sq(vr) + prr - pinfl - tyy[nR] + rhol * sq(vl) + pl - pinfl - tyy[nL];
+  const double dfyz = rhor * vr * wr - tyz[nR] + rhol * vl * wl - tyz[nL];
+  const double dfzz = rhor * sq(wr) + prr - pinfl - tzz[nR] + rhol * sq(wl) + pl - pinfl - tzz[nL];
+  const double dfex = (rhor * er + prr - pinfl) * ur + (rhol * el + pl - pinfl) * ul -
+                      (txx[nR] * ur + txy[nR] * vr + txz[nR] * wr) -
+                      (txx[nL] * ul + txy[nL] * vl + txz[nL] * wl) - qx[nR] - qx[nL];
+  const double dfey = (rhor * er + prr - pinfl) * vr + (rhol * el + pl - pinfl) * vl -
+                      (txy[nR] * ur + tyy[nR] * vr + tyz[nR] * wr) -
+                      (txy[nL] * ul + tyy[nL] * vl + tyz[nL] * wl) - qy[nR] - qy[nL];
+  const double dfez = (rhor * er + prr - pinfl) * wr + (rhol * el + pl - pinfl) * wl -
+                      (txz[nR] * ur + tyz[nR] * vr + tzz[nR] * wr) -
+                      (txz[nL] * ul + tyz[nL] * vl + tzz[nL] * wl) - qz[nR] - qz[nL];
+  f[0] = (rhor * ur + rhol * ul) * s1 + (rhor * vr + rhol * vl) * s2 +
+         (rhor * wr + rhol * wl) * s3 - di[0];
+  f[1] = dfxx * s1 + dfxy * s2 + dfxz * s3 - di[1];
+  f[2] = dfxy * s1 + dfyy * s2 + dfyz * s3 - di[2];
+  f[3] = dfxz * s1 + dfyz * s2 + dfzz * s3 - di[3];
+  f[4] = dfex * s1 + dfey * s2 + dfez * s3 - di[4];
+}
+
+enum { ORC_FL_HLLC = 1, ORC_FL_RUSANOV = 2 };
+
+/* one direction of sch_hllc_euler (fl HLLC, ns 0), sch_hllc (fl HLLC, ns 1)
+ * or sch_rusanov (fl RUSANOV, always with the stresses): the same loop
+ * nests as roe_direction (interior faces, then lower and upper boundary
+ * faces); the minmod limiter only in sch_hllc */
+static void flux_direction(const blk_t *b, int dir, int fl, int ns, double *u,
+                           const double *v, const double *tau, const double *sn,
+                           const double *ps) {
+  const int64_t L = G.ld, n0 = b->npc, ninc = NINC(b, dir);
+  const int nd = NDIR(b, dir);
+  const int absam = fl == ORC_FL_HLLC && ns && dir < 2;
+  const int visc = ns || fl == ORC_FL_RUSANOV;
+  int lo[3], hi[3], idx[3];
+  double *r = NULL;
+  const int limited = fl == ORC_FL_HLLC && ns && G.ilim == 1;
+  if (limited) {
+    r = calloc((size_t)5 * b->nnn, sizeof(double));
+    dir_ranges(b, dir, 1, nd, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+          r[m] = v[n] - v[n - ninc];
+          r[b->nnn + m] = v[L + n] / v[n] - v[L + n - ninc] / v[n - ninc];
+          r[2 * b->nnn + m] = v[2 * L + n] / v[n] - v[2 * L + n - ninc] / v[n - ninc];
+          r[3 * b->nnn + m] = v[3 * L + n] / v[n] - v[3 * L + n - ninc] / v[n - ninc];
+          r[4 * b->nnn + m] = ps[n] - ps[n - ninc];
+        }
+    dir_ranges(b, dir, 2, nd - 1, lo, hi);
+    for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+      for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+        for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+          int64_t m = ML(b, idx[0], idx[1], idx[2]);
+          for (int a = 0; a < 5; ++a) {
+            double *ra = r + (int64_t)a * b->nnn;
+            if (fabs(ra[m - ninc] * ra[m] * ra[m + ninc]) <= DBL_MIN)
+              ra[m] = 1.;
+            else
+              ra[m] = ra[m] / ra[m - ninc];
+          }
+        }
+  }
+  dir_ranges(b, dir, 2, nd - 1, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double vv[4][5], pp[4], WL[5], WR[5], f[5];
+        gather_cells(v, ps, L, n, ninc, vv, pp);
+        if (limited && idx[dir] <= nd - 2) {
+          double rm[5], rp[5];
+          for (int a = 0; a < 5; ++a) {
+            rm[a] = r[(int64_t)a * b->nnn + m];
+            rp[a] = r[(int64_t)a * b->nnn + m + ninc];
+          }
+          muscl_limited(vv, pp, rm, rp, WL, WR);
+        } else {
+          muscl_plain(vv, pp, WL, WR);
+        }
+        const double s1 = SN(sn, b, m, dir, 0), s2 = SN(sn, b, m, dir, 1),
+                     s3 = SN(sn, b, m, dir, 2);
+        if (fl == ORC_FL_RUSANOV) {
+          rusanov_flux(WL, WR, s1, s2, s3, tau, L, n, n - ninc, f);
+          for (int a = 0; a < 5; ++a) {
+            u[a * L + n] = u[a * L + n] - 0.5 * f[a];
+            u[a * L + n - ninc] = u[a * L + n - ninc] + 0.5 * f[a];
+          }
+        } else if (!ns) {
+          hllc_core(WL, WR, s1, s2, s3, absam, f);
+          for (int a = 0; a < 5; ++a) {
+            u[a * L + n] = u[a * L + n] - f[a];
+            u[a * L + n - ninc] = u[a * L + n - ninc] + f[a];
+          }
+        } else {
+          double fv[5];
+          hllc_core(WL, WR, s1, s2, s3, absam, f);
+          hllc_viscous(WL, WR, s1, s2, s3, tau, L, n, n - ninc, fv);
+          u[n] = u[n] - f[0];
+          for (int a = 1; a < 5; ++a) u[a * L + n] = u[a * L + n] - f[a] + 0.5 * fv[a];
+          u[n - ninc] = u[n - ninc] + f[0];
+          for (int a = 1; a < 5; ++a)
+            u[a * L + n - ninc] = u[a * L + n - ninc] + f[a] - 0.5 * fv[a];
+        }
+      }
+  dir_ranges(b, dir, 1, 1, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double sb[5];
+        int64_t nrho = (!visc && dir > 0) ? n : n - ninc;
+        bnd_flux(v, ps, visc ? tau : NULL, L, n - ninc, nrho, SN(sn, b, m, dir, 0),
+                 SN(sn, b, m, dir, 1), SN(sn, b, m, dir, 2), sb);
+        for (int a = 0; a < 5; ++a) u[a * L + n] = u[a * L + n] - sb[a];
+      }
+  dir_ranges(b, dir, nd, nd, lo, hi);
+  for (idx[2] = lo[2]; idx[2] <= hi[2]; ++idx[2])
+    for (idx[1] = lo[1]; idx[1] <= hi[1]; ++idx[1])
+      for (idx[0] = lo[0]; idx[0] <= hi[0]; ++idx[0]) {
+        int64_t n = IC(b, idx[0], idx[1], idx[2]), m = n - n0;
+        double sb[5];
+        bnd_flux(v, ps, visc ? tau : NULL, L, n, n, SN(sn, b, m, dir, 0),
+                 SN(sn, b, m, dir, 1), SN(sn, b, m, dir, 2), sb);
+        for (int a = 0; a < 5; ++a) u[a * L + n - ninc] = u[a * L + n - ninc] + sb[a];
+      }
+  free(r);
+}
+
 static void zero_u(const blk_t *b, double *u) {
   for (int a = 0; a < 5; ++a)
     for (int64_t n = b->npc; n < b->npc + b->nnn; ++n) u[a * G.ld + n] = 0.;
@@ -1389,6 +1631,32 @@ void orc_sch_roe(int l, double *u, const double *v, const double *tau,
   const blk_t *b = &G.b[l - 1];
   zero_u(b, u);
   for (int dir = 0; dir < 3; ++dir) roe_direction(b, dir, 1, u, v, tau, sn, ps);
+}
+
+/* sch_hllc_euler.f90:4-891 (ityprk=0, 3-D) */
+void orc_sch_hllc_euler(int l, double *u, const double *v, const double *sn,
+                        const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) flux_direction(b, dir, ORC_FL_HLLC, 0, u, v, NULL, sn, ps);
+}
+
+/* sch_hllc.f90:4-1403 (ityprk=0, 3-D) */
+void orc_sch_hllc(int l, double *u, const double *v, const double *tau, const double *sn,
+                  const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) flux_direction(b, dir, ORC_FL_HLLC, 1, u, v, tau, sn, ps);
+}
+
+/* sch_rusanov.f90:4-791 (ityprk=0, 3-D; the stresses enter whatever the
+ * equations, zero for Euler) */
+void orc_sch_rusanov(int l, double *u, const double *v, const double *tau, const double *sn,
+                     const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir)
+    flux_direction(b, dir, ORC_FL_RUSANOV, G.ns, u, v, tau, sn, ps);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -2684,15 +2952,22 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
   if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int l = 1; l <= G.nblk; ++l) {
-    if (G.ns) {
+    /* atsch_num.f90:628-983: the flux family by ischema */
+    if (G.ischema == 9)
+      orc_sch_rusanov(l, u, v, tau, sn, ps);
+    else if (G.ischema == 14 && G.ns)
+      orc_sch_hllc(l, u, v, tau, sn, ps);
+    else if (G.ischema == 14)
+      orc_sch_hllc_euler(l, u, v, sn, ps);
+    else if (G.ns)
       orc_sch_roe(l, u, v, tau, sn, ps);
-      if (G.kfmg == 3) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
-      orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
-    } else {
+    else
       orc_sch_roe_euler(l, u, v, sn, ps);
-      if (G.kfmg == 3) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
+    if (G.kfmg == 3) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
+    if (G.ns)
+      orc_implimf_3d(l, u, dt, v, d, mu, mut, sn, vol, ps, cson, G.lmax);
+    else
       orc_implimf_eu(l, u, dt, v, d, sn, vol, ps, cson, G.lmax);
-    }
   }
   return 0;
 }

@@ -171,6 +171,17 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);
 
+/* other flux families (atsch_num.f90:628-983): ischema 14 HLLC
+ * (sch_hllc_euler, sch_hllc), ischema 9 Rusanov (sch_rusanov, with the
+ * stresses tau whatever the equations: zero for Euler); orc_step selects by
+ * the ischema of orc_set_dissipation */
+void orc_sch_hllc_euler(int l, double *u, const double *v, const double *sn,
+                        const double *ps);
+void orc_sch_hllc(int l, double *u, const double *v, const double *tau, const double *sn,
+                  const double *ps);
+void orc_sch_rusanov(int l, double *u, const double *v, const double *tau, const double *sn,
+                     const double *ps);
+
 /* dual time stepping (kfmg = 3; dt1min of orc_set_scheme is the physical
  * time step): the fused step adds sch_dual after the residual with the
  * physical step index icycle and the array ptdual given here */

@@ -82,6 +82,9 @@ def lib():
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 8
         L.orc_set_sa_fix.argtypes = [C.c_int]
+        L.orc_sch_hllc_euler.argtypes = [C.c_int, _d, _d, _d, _d]
+        L.orc_sch_hllc.argtypes = [C.c_int, _d, _d, _d, _d, _d]
+        L.orc_sch_rusanov.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_set_dual.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_sch_dual.argtypes = [C.c_int, _d, _d, C.c_int, _d, _d]
         L.orc_sch_duin.argtypes = [_d] * 5
