@@ -84,10 +84,18 @@ def parse():
                         "in one launch against the same boxes one at a time")
     p.add_argument("--tiles", default=None,
                    help="TI,TJ,KC: fix the Jacobi sweep tiling instead of autotuning it")
+    p.add_argument("--eta", type=float, default=5.0,
+                   help="CFL number of the local time step (AUSM+ needs 2 on the channel)")
+    p.add_argument("--flux", default="roe", choices=["roe", "hllc", "rusanov", "ausm"],
+                   help="flux family of the channel workload (ischema 7, 14, 9, 5)")
     p.add_argument("--ilim", type=int, default=0,
                    help="0: plain kappa=-1 MUSCL (default: the reference's limiter "
                         "recurrence stalls this channel at L2 ~1e-3); 1: minmod limiter")
     return p.parse_args()
+
+
+FLUX = {"roe": 7, "hllc": 14, "rusanov": 9, "ausm": 5}
+FLUX_NAME = {"roe": "Roe", "hllc": "HLLC", "rusanov": "Rusanov", "ausm": "AUSM+"}
 
 
 def make_case(args):
@@ -98,6 +106,8 @@ def make_case(args):
         case = cases.channel_case(seed=2)
     case.scheme.lmax = args.lmax
     case.scheme.ilim = args.ilim
+    case.scheme.ischema = FLUX[args.flux]
+    case.scheme.eta = args.eta
     case.scheme.precision = PRECISION[args.precision]
     case.scheme.kdefect = args.kdefect
     return case
@@ -106,7 +116,7 @@ def make_case(args):
 def config_of(case, args, n):
     m = case.meta
     return {
-        "workload": "laminar NS bump channel, 8 uneven blocks, Roe-MUSCL"
+        "workload": f"laminar NS bump channel, 8 uneven blocks, {FLUX_NAME[args.flux]}-MUSCL"
                     f"{' minmod' if args.ilim else ''} + viscous, "
                     f"implicit point-Jacobi lmax={args.lmax}, {args.precision}"
         if not args.small else "laminar NS bump channel, 3 blocks of 64x64x96 cells",
@@ -116,6 +126,8 @@ def config_of(case, args, n):
         "mach": m.get("mach"), "reynolds": m.get("reynz"), "seed": m.get("seed"),
         "precision": args.precision,
         "ilim": args.ilim,
+        "flux": args.flux,
+        "eta": args.eta,
         "l2_flush": "inputs larger than L2 (state and scratch ~GBs)",
         "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
     }
@@ -267,13 +279,23 @@ def _sweep_ms(s, torch, scheme, lmax, steps):
 
 
 def _residual_ms(s, torch, reps=5):
-    """the FP64 residual of every block (sch_roe / sch_roe_euler), ms"""
+    """the FP64 residual of every block with the case's flux family
+    (sch_roe / sch_roe_euler, sch_hllc / sch_hllc_euler, sch_rusanov), ms"""
     s.sync()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
+    ischema = s.case.scheme.ischema
     a.record(s.stream)
     for _ in range(reps):
-        if s.case.scheme.ns:
+        if ischema == 9:
+            s.sch_rusanov(0, s.u, s.v, s.tau, s.sn, s.pression)
+        elif ischema == 5:
+            s.sch_ausmp(0, s.u, s.v, s.tau, s.sn, s.pression)
+        elif ischema == 14 and s.case.scheme.ns:
+            s.sch_hllc(0, s.u, s.v, s.tau, s.sn, s.pression)
+        elif ischema == 14:
+            s.sch_hllc_euler(0, s.u, s.v, s.sn, s.pression)
+        elif s.case.scheme.ns:
             s.sch_roe(0, s.u, s.v, s.tau, s.sn, s.pression)
         else:
             s.sch_roe_euler(0, s.u, s.v, s.sn, s.pression)

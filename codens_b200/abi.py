@@ -75,7 +75,7 @@ EXPORTS = [
     "cns_set_sa", "cns_met_num",
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
     "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
-    "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov",
+    "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov", "cns_sch_ausmp",
 ]
 
 _lib = None
@@ -158,6 +158,7 @@ def load(build_if_missing: bool = True):
     L.cns_sch_hllc_euler.argtypes = [vp, C.c_int] + [vp] * 4
     L.cns_sch_hllc.argtypes = [vp, C.c_int] + [vp] * 5
     L.cns_sch_rusanov.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_sch_ausmp.argtypes = [vp, C.c_int] + [vp] * 5
     L.cns_set_cycle.argtypes = [vp, c_i64, c_i64]
     L.cns_sch_duin.argtypes = [vp]
     L.cns_sch_duup.argtypes = [vp]

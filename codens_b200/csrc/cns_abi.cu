@@ -904,13 +904,15 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (!c || !s) return CNS_EINVAL;
   if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
       s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1) ||
-      (s->ischema != 1 && s->ischema != 7 && s->ischema != 9 && s->ischema != 14) ||
+      (s->ischema != 1 && s->ischema != 7 && s->ischema != 9 && s->ischema != 14 &&
+       s->ischema != 5) ||
+      (s->ischema == 5 && !s->ns) ||
       (s->ischema != 7 && s->precision == 2) ||
       (s->kfmg != 0 && s->kfmg != 3) ||
       (s->kfmg == 3 && (!(s->dt1min > 0.) || s->kdualns < 0 || s->kdualns > 2)))
     return fail(c, CNS_EINVAL,
                 "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
-                "kdefect >= 1, ischema in {1,7,9,14} (defect correction: Roe only), kfmg in "
+                "kdefect >= 1, ischema in {1,5,7,9,14} (5: ns only; defect correction: Roe only), kfmg in "
                 "{0,3} (3: dt1min > 0, kdualns in {0,1,2})");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
@@ -1064,19 +1066,25 @@ static int other_family(cns_ctx* c, int l, int ischema, int ns, double* u, const
 
 int cns_sch_hllc_euler(cns_ctx* c, int l, double* u, const double* v, const double* sn,
                        const double* ps) {
-  if (!c || bad_block(c, l) || l == 0 || !u || !v || !sn || !ps) return CNS_EINVAL;
+  if (!c || bad_block(c, l) || !u || !v || !sn || !ps) return CNS_EINVAL;
   return other_family(c, l, 14, 0, u, v, nullptr, sn, ps);
 }
 
 int cns_sch_hllc(cns_ctx* c, int l, double* u, const double* v, const double* tau,
                  const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || l == 0 || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
   return other_family(c, l, 14, 1, u, v, tau, sn, ps);
+}
+
+int cns_sch_ausmp(cns_ctx* c, int l, double* u, const double* v, const double* tau,
+                  const double* sn, const double* ps) {
+  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  return other_family(c, l, 5, 1, u, v, tau, sn, ps);
 }
 
 int cns_sch_rusanov(cns_ctx* c, int l, double* u, const double* v, const double* tau,
                     const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || l == 0 || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
+  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
   return other_family(c, l, 9, c->sc.ns, u, v, tau, sn, ps);
 }
 

@@ -258,7 +258,85 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
 }
 
 // flux families of the face kernel (atsch_num.f90:628-983 by ischema)
-enum { kFluxRoe = 0, kFluxHllc = 1, kFluxRusanov = 2 };
+enum { kFluxRoe = 0, kFluxHllc = 1, kFluxRusanov = 2, kFluxAusm = 3 };
+
+// the AUSM+ splittings of sch_ausmp.f90:1010-1033 (sign(1, x) = +-1 by the
+// sign bit of x)
+template <class T>
+__device__ __forceinline__ T sgn1(T x) { return copysign(T(1.), x); }
+template <class T>
+__device__ __forceinline__ T ausm_fmp(T aa) {
+  const T s = sgn1(fabs(aa) - T(1.));
+  return T(0.25) * (T(1.) + s) * (aa + fabs(aa)) + T(0.125) * (T(1.) - s) * sqT(aa + T(1.));
+}
+template <class T>
+__device__ __forceinline__ T ausm_fmm(T xa) {
+  const T s = sgn1(fabs(xa) - T(1.));
+  return T(0.25) * (T(1.) + s) * (xa - fabs(xa)) - T(0.125) * (T(1.) - s) * sqT(xa - T(1.));
+}
+template <class T>
+__device__ __forceinline__ T ausm_fpp(T ta) {
+  const T s = sgn1(fabs(ta) - T(1.));
+  return T(0.25) * (T(1.) + s) * (T(1.) + sgn1(fabs(ta))) +
+         T(0.125) * (T(1.) - s) * sqT(ta + T(1.)) *
+             (T(2.) - ta + T(0.75) * ta * sqT(ta - T(1.)));
+}
+template <class T>
+__device__ __forceinline__ T ausm_fpm(T ra) {
+  const T s = sgn1(fabs(ra) - T(1.));
+  return T(0.25) * (T(1.) + s) * (T(1.) - sgn1(fabs(ra))) +
+         T(0.125) * (T(1.) - s) * sqT(ra - T(1.)) *
+             (T(2.) + ra - T(0.75) * ra * sqT(ra + T(1.)));
+}
+
+// the work and heat-flux terms sch_ausmp.f90:81-83 stores in d(n, 1:3)
+template <class T>
+__device__ __forceinline__ void ausm_dterm(const T* __restrict__ v, const T* __restrict__ tau,
+                                           long long ld, long long n, T dd[3]) {
+  const T v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n];
+  const T txx = tau[n], txy = tau[ld + n], txz = tau[2 * ld + n], tyy = tau[3 * ld + n],
+          tyz = tau[4 * ld + n], tzz = tau[5 * ld + n];
+  dd[0] = (txx * v2 + txy * v3 + txz * v4) / v1 + tau[6 * ld + n];
+  dd[1] = (tyy * v3 + txy * v2 + tyz * v4) / v1 + tau[7 * ld + n];
+  dd[2] = (tzz * v4 + txz * v2 + tyz * v3) / v1 + tau[8 * ld + n];
+}
+
+// the AUSM+ flux hi1..hi5 of sch_ausmp.f90:255-298
+template <class T>
+__device__ __forceinline__ void ausm_flux(const T WL[5], const T WR[5], T s1, T s2, T s3,
+                                          const T* __restrict__ v, const T* __restrict__ tau,
+                                          long long ld, long long nR, long long nL,
+                                          const PhysT<T>& ph, T hi[5]) {
+  const T gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl, h = T(0.5), two = T(2.);
+  const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const T cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const T al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const T hl = al * al / gam1 + h * (sqT(ul) + sqT(vl) + sqT(wl));
+  const T hr = ar * ar / gam1 + h * (sqT(ur) + sqT(vr) + sqT(wr));
+  const T ai = sqrt(al * ar);
+  const T cml = (ul * s1 + vl * s2 + wl * s3) / (al * cnds);
+  const T cmr = (ur * s1 + vr * s2 + wr * s3) / (ar * cnds);
+  const T psi = two * (pl * ausm_fpp(cml) + prr * ausm_fpm(cmr)) - two * pinfl;
+  const T cmi = ausm_fmp(cml) + ausm_fmm(cmr);
+  const T dm = h * ai * (cmi * (rhol + rhor) - fabs(cmi) * (rhor - rhol)) * cnds;
+  const T txxR = tau[nR], txyR = tau[ld + nR], txzR = tau[2 * ld + nR], tyyR = tau[3 * ld + nR],
+          tyzR = tau[4 * ld + nR], tzzR = tau[5 * ld + nR];
+  const T txxL = tau[nL], txyL = tau[ld + nL], txzL = tau[2 * ld + nL], tyyL = tau[3 * ld + nL],
+          tyzL = tau[4 * ld + nL], tzzL = tau[5 * ld + nL];
+  T dR[3], dL[3];
+  ausm_dterm(v, tau, ld, nR, dR);
+  ausm_dterm(v, tau, ld, nL, dL);
+  hi[0] = dm;
+  hi[1] = dm * (ul + ur) - fabs(dm) * (ur - ul) + psi * s1 - (txxR + txxL) * s1 -
+          (txyR + txyL) * s2 - (txzR + txzL) * s3;
+  hi[2] = dm * (vl + vr) - fabs(dm) * (vr - vl) + psi * s2 - (txyR + txyL) * s1 -
+          (tyyR + tyyL) * s2 - (tyzR + tyzL) * s3;
+  hi[3] = dm * (wl + wr) - fabs(dm) * (wr - wl) + psi * s3 - (txzR + txzL) * s1 -
+          (tyzR + tyzL) * s2 - (tzzR + tzzL) * s3;
+  hi[4] = dm * (hl + hr) - fabs(dm) * (hr - hl) - (dR[0] + dL[0]) * s1 - (dR[1] + dL[1]) * s2 -
+          (dR[2] + dL[2]) * s3;
+}
 
 // the HLLC flux (sch_hllc_euler.f90:135-221, sch_hllc.f90:270-357): the
 // left or right physical flux, or the star state's; absam: the sound speed
@@ -446,6 +524,15 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
     } else {
       muscl_plain(c, c4, xk, WL, WR);
     }
+    if (FL == kFluxAusm) {
+      // sch_ausmp.f90:289-298: hi1 whole, the others halved
+      ausm_flux(WL, WR, sx, sy, sz, v, tau, ld, n, n - inc, ph, out);
+      T* Gd = G + (long long)dir * 5 * ld;
+      Gd[n] = out[0];
+#pragma unroll
+      for (int a = 1; a < 5; ++a) Gd[a * ld + n] = T(0.5) * out[a];
+      return;
+    }
     if (FL == kFluxHllc) {
       hllc_flux(WL, WR, sx, sy, sz, NS && dir < 2, ph, out);
       if (NS) {
@@ -534,7 +621,7 @@ __global__ void __launch_bounds__(kTile, 4) k_face_flux(
 
 // the FP64 face kernels of one residual by flux family (atsch_num.f90:628-983):
 // ischema 14 HLLC (sch_hllc / sch_hllc_euler), 9 Rusanov (sch_rusanov, the
-// stresses always), else Roe; each translation unit instantiates it with its
+// stresses always), 5 AUSM+ (sch_ausmp, Navier-Stokes), else Roe; each translation unit instantiates it with its
 // own contraction flags
 static inline cudaError_t face_flux_dispatch(const Blk* blks, const SpaceBuf* faces, int l0,
                                              Phys ph, Scheme sc, const double* v,
@@ -555,6 +642,9 @@ static inline cudaError_t face_flux_dispatch(const Blk* blks, const SpaceBuf* fa
     else if (sc.ischema == 9)
       k_face_flux<double, true, kFluxRusanov><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v,
                                                                   prim, ld, ps, tau, sn, R, G);
+    else if (sc.ischema == 5)
+      k_face_flux<double, true, kFluxAusm><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim,
+                                                               ld, ps, tau, sn, R, G);
     else if (sc.ns)
       k_face_flux<double, true><<<g, kTile, 0, st>>>(blks, sp, dir, ph, sc, v, prim, ld, ps,
                                                      tau, sn, R, G);

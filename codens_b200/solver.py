@@ -233,6 +233,10 @@ class CodeNS:
         self._check(self.lib.cns_sch_rusanov(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau),
                                              _ptr(sn), _ptr(ps)), "cns_sch_rusanov")
 
+    def sch_ausmp(self, l, u, v, tau, sn, ps):
+        self._check(self.lib.cns_sch_ausmp(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
+                                           _ptr(ps)), "cns_sch_ausmp")
+
     def chrono_global(self, dt):
         """chrono.f90:113-151: the global time step (kdtl = 0)"""
         self._check(self.lib.cns_chrono_global(self.ctx, _ptr(dt)), "cns_chrono_global")

@@ -95,7 +95,7 @@ typedef struct {
                             the FP32 rounding level of the fluxes) */
   int32_t kdefect;       /* precision 2: the FP64 residual and the correction
                             R64 - R32 are refreshed every kdefect iterations */
-  int32_t ischema;       /* 7: Roe (sch_roe, sch_roe_euler); 14: HLLC; 9: Rusanov; 1: Jameson
+  int32_t ischema;       /* 7: Roe (sch_roe, sch_roe_euler); 14: HLLC; 9: Rusanov; 5: AUSM+; 1: Jameson
                             (dissip_jameson + sch_jameson, kprec = 0) */
   double ki2, ki4;       /* Jameson 2nd/4th-difference coefficients (ki2(lm),
                             ki4(lm); one value for every block) */
@@ -321,13 +321,18 @@ int cns_sch_roe(cns_ctx *ctx, int l, double *u, const double *v,
  * sch_hllc.f90:4-1403, with the minmod limiter of ilim = 1 in the NS form),
  * 9 = Rusanov (sch_rusanov.f90:4-791: plain MUSCL, the stresses tau enter
  * whatever the equations -- zero for Euler); same arguments as
- * cns_sch_roe_euler / cns_sch_roe (block l >= 1) */
+ * cns_sch_roe_euler / cns_sch_roe (l = 0: every block in one launch) */
 int cns_sch_hllc_euler(cns_ctx *ctx, int l, double *u, const double *v,
                        const double *sn, const double *ps);
 int cns_sch_hllc(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
                  const double *sn, const double *ps);
 int cns_sch_rusanov(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
                     const double *sn, const double *ps);
+/* ischema 5 = AUSM+ (sch_ausmp.f90:4-1157; the reference runs it for the
+ * Navier-Stokes equations only: with the minmod limiter of ilim = 1, the
+ * work and heat-flux terms of sch_ausmp.f90:81-83 from tau on the fly) */
+int cns_sch_ausmp(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
+                  const double *sn, const double *ps);
 int cns_zvisqc(cns_ctx *ctx, const double *v, const double *mu,
                const double *mut, double *tau, const double *sn,
                const double *vol, const double *ztemp);

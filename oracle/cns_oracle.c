@@ -1503,7 +1503,70 @@ static void rusanov_flux(const double WL[5], const double WR[5], double s1, doub
   f[4] = dfex * s1 + dfey * s2 + dfez * s3 - di[4];
 }
 
-enum { ORC_FL_HLLC = 1, ORC_FL_RUSANOV = 2 };
+/* the AUSM+ splittings of sch_ausmp.f90:1010-1033 (sign(1,x) = +-1 by the
+ * sign bit of x) */
+static double sgn1(double x) { return copysign(1., x); }
+static double ausm_fmp(double aa) {
+  return 0.25 * (1. + sgn1(fabs(aa) - 1.)) * (aa + fabs(aa)) +
+         0.125 * (1. - sgn1(fabs(aa) - 1.)) * sq(aa + 1.);
+}
+static double ausm_fmm(double xa) {
+  return 0.25 * (1. + sgn1(fabs(xa) - 1.)) * (xa - fabs(xa)) -
+         0.125 * (1. - sgn1(fabs(xa) - 1.)) * sq(xa - 1.);
+}
+static double ausm_fpp(double ta) {
+  return 0.25 * (1. + sgn1(fabs(ta) - 1.)) * (1. + sgn1(fabs(ta))) +
+         0.125 * (1. - sgn1(fabs(ta) - 1.)) * sq(ta + 1.) * (2. - ta + 0.75 * ta * sq(ta - 1.));
+}
+static double ausm_fpm(double ra) {
+  return 0.25 * (1. + sgn1(fabs(ra) - 1.)) * (1. - sgn1(fabs(ra))) +
+         0.125 * (1. - sgn1(fabs(ra) - 1.)) * sq(ra - 1.) * (2. + ra - 0.75 * ra * sq(ra + 1.));
+}
+
+/* the work and heat-flux terms sch_ausmp.f90:81-83 stores in d(n,1:3) */
+static void ausm_dterm(const double *v, const double *tau, int64_t L, int64_t n, double dd[3]) {
+  const double v1 = v[n], v2 = v[L + n], v3 = v[2 * L + n], v4 = v[3 * L + n];
+  const double txx = tau[n], txy = tau[L + n], txz = tau[2 * L + n], tyy = tau[3 * L + n],
+               tyz = tau[4 * L + n], tzz = tau[5 * L + n];
+  dd[0] = (txx * v2 + txy * v3 + txz * v4) / v1 + tau[6 * L + n];
+  dd[1] = (tyy * v3 + txy * v2 + tyz * v4) / v1 + tau[7 * L + n];
+  dd[2] = (tzz * v4 + txz * v2 + tyz * v3) / v1 + tau[8 * L + n];
+}
+
+/* the AUSM+ flux of sch_ausmp.f90:255-298 (hi1..hi5) */
+static void ausm_flux(const double WL[5], const double WR[5], double s1, double s2, double s3,
+                      const double *v, const double *tau, int64_t L, int64_t nR, int64_t nL,
+                      double hi[5]) {
+  const double gam = G.gam, gam1 = G.gam1, pinfl = G.pinfl;
+  const double rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
+  const double rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
+  const double cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const double al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
+  const double hl = al * al / gam1 + 0.5 * (sq(ul) + sq(vl) + sq(wl));
+  const double hr = ar * ar / gam1 + 0.5 * (sq(ur) + sq(vr) + sq(wr));
+  const double ai = sqrt(al * ar);
+  const double cml = (ul * s1 + vl * s2 + wl * s3) / (al * cnds);
+  const double cmr = (ur * s1 + vr * s2 + wr * s3) / (ar * cnds);
+  const double psi = 2. * (pl * ausm_fpp(cml) + prr * ausm_fpm(cmr)) - 2. * pinfl;
+  const double cmi = ausm_fmp(cml) + ausm_fmm(cmr);
+  const double dm = 0.5 * ai * (cmi * (rhol + rhor) - fabs(cmi) * (rhor - rhol)) * cnds;
+  const double *txx = tau, *txy = tau + L, *txz = tau + 2 * L, *tyy = tau + 3 * L,
+               *tyz = tau + 4 * L, *tzz = tau + 5 * L;
+  double dR[3], dL[3];
+  ausm_dterm(v, tau, L, nR, dR);
+  ausm_dterm(v, tau, L, nL, dL);
+  hi[0] = dm;
+  hi[1] = dm * (ul + ur) - fabs(dm) * (ur - ul) + psi * s1 - (txx[nR] + txx[nL]) * s1 -
+          (txy[nR] + txy[nL]) * s2 - (txz[nR] + txz[nL]) * s3;
+  hi[2] = dm * (vl + vr) - fabs(dm) * (vr - vl) + psi * s2 - (txy[nR] + txy[nL]) * s1 -
+          (tyy[nR] + tyy[nL]) * s2 - (tyz[nR] + tyz[nL]) * s3;
+  hi[3] = dm * (wl + wr) - fabs(dm) * (wr - wl) + psi * s3 - (txz[nR] + txz[nL]) * s1 -
+          (tyz[nR] + tyz[nL]) * s2 - (tzz[nR] + tzz[nL]) * s3;
+  hi[4] = dm * (hl + hr) - fabs(dm) * (hr - hl) - (dR[0] + dL[0]) * s1 -
+          (dR[1] + dL[1]) * s2 - (dR[2] + dL[2]) * s3;
+}
+
+enum { ORC_FL_HLLC = 1, ORC_FL_RUSANOV = 2, ORC_FL_AUSM = 3 };
 
 /* one direction of sch_hllc_euler (fl HLLC, ns 0), sch_hllc (fl HLLC, ns 1)
  * or sch_rusanov (fl RUSANOV, always with the stresses): the same loop
@@ -1518,7 +1581,7 @@ static void flux_direction(const blk_t *b, int dir, int fl, int ns, double *u,
   const int visc = ns || fl == ORC_FL_RUSANOV;
   int lo[3], hi[3], idx[3];
   double *r = NULL;
-  const int limited = fl == ORC_FL_HLLC && ns && G.ilim == 1;
+  const int limited = (fl == ORC_FL_HLLC || fl == ORC_FL_AUSM) && ns && G.ilim == 1;
   if (limited) {
     r = calloc((size_t)5 * b->nnn, sizeof(double));
     dir_ranges(b, dir, 1, nd, lo, hi);
@@ -1565,7 +1628,13 @@ static void flux_direction(const blk_t *b, int dir, int fl, int ns, double *u,
         }
         const double s1 = SN(sn, b, m, dir, 0), s2 = SN(sn, b, m, dir, 1),
                      s3 = SN(sn, b, m, dir, 2);
-        if (fl == ORC_FL_RUSANOV) {
+        if (fl == ORC_FL_AUSM) {
+          ausm_flux(WL, WR, s1, s2, s3, v, tau, L, n, n - ninc, f);
+          u[n] = u[n] - f[0];
+          for (int a = 1; a < 5; ++a) u[a * L + n] = u[a * L + n] - 0.5 * f[a];
+          u[n - ninc] = u[n - ninc] + f[0];
+          for (int a = 1; a < 5; ++a) u[a * L + n - ninc] = u[a * L + n - ninc] + 0.5 * f[a];
+        } else if (fl == ORC_FL_RUSANOV) {
           rusanov_flux(WL, WR, s1, s2, s3, tau, L, n, n - ninc, f);
           for (int a = 0; a < 5; ++a) {
             u[a * L + n] = u[a * L + n] - 0.5 * f[a];
@@ -1647,6 +1716,15 @@ void orc_sch_hllc(int l, double *u, const double *v, const double *tau, const do
   const blk_t *b = &G.b[l - 1];
   zero_u(b, u);
   for (int dir = 0; dir < 3; ++dir) flux_direction(b, dir, ORC_FL_HLLC, 1, u, v, tau, sn, ps);
+}
+
+/* sch_ausmp.f90:4-1157 (ityprk=0, 3-D; Navier-Stokes only, as the
+ * reference calls it) */
+void orc_sch_ausmp(int l, double *u, const double *v, const double *tau, const double *sn,
+                   const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) flux_direction(b, dir, ORC_FL_AUSM, 1, u, v, tau, sn, ps);
 }
 
 /* sch_rusanov.f90:4-791 (ityprk=0, 3-D; the stresses enter whatever the
@@ -2955,6 +3033,8 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
     /* atsch_num.f90:628-983: the flux family by ischema */
     if (G.ischema == 9)
       orc_sch_rusanov(l, u, v, tau, sn, ps);
+    else if (G.ischema == 5)
+      orc_sch_ausmp(l, u, v, tau, sn, ps);
     else if (G.ischema == 14 && G.ns)
       orc_sch_hllc(l, u, v, tau, sn, ps);
     else if (G.ischema == 14)

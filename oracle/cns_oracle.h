@@ -181,6 +181,9 @@ void orc_sch_hllc(int l, double *u, const double *v, const double *tau, const do
                   const double *ps);
 void orc_sch_rusanov(int l, double *u, const double *v, const double *tau, const double *sn,
                      const double *ps);
+/* ischema 5, AUSM+ (sch_ausmp.f90; Navier-Stokes only) */
+void orc_sch_ausmp(int l, double *u, const double *v, const double *tau, const double *sn,
+                   const double *ps);
 
 /* dual time stepping (kfmg = 3; dt1min of orc_set_scheme is the physical
  * time step): the fused step adds sch_dual after the residual with the

@@ -85,6 +85,7 @@ def lib():
         L.orc_sch_hllc_euler.argtypes = [C.c_int, _d, _d, _d, _d]
         L.orc_sch_hllc.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_sch_rusanov.argtypes = [C.c_int, _d, _d, _d, _d, _d]
+        L.orc_sch_ausmp.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_set_dual.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_sch_dual.argtypes = [C.c_int, _d, _d, C.c_int, _d, _d]
         L.orc_sch_duin.argtypes = [_d] * 5

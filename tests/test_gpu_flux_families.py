@@ -1,6 +1,6 @@
 """GPU tests of the other flux families (HLLC, ischema 14; Rusanov,
-ischema 9): each block's residual against the oracle's restatement of
-sch_hllc_euler / sch_hllc / sch_rusanov bit for bit, and the fused
+ischema 9; AUSM+, ischema 5): each block's residual against the oracle's
+restatement of sch_hllc_euler / sch_hllc / sch_rusanov / sch_ausmp bit for bit, and the fused
 iterations with each family against the oracle's atsch_num sequence."""
 from __future__ import annotations
 
@@ -14,7 +14,7 @@ from tests.test_gpu_parity import _gpu, _load_state, _n, _prepared_flow
 
 pytestmark = pytest.mark.gpu
 
-FAMILIES = {"hllc": 14, "rusanov": 9}
+FAMILIES = {"hllc": 14, "rusanov": 9, "ausm": 5}
 
 
 def with_family(case, ischema):
@@ -26,6 +26,8 @@ def with_family(case, ischema):
 @pytest.mark.parametrize("name", ["box_eu", "box_ns", "channel", "box_pinfl"])
 def test_block_residual_parity(cuda, family, name):
     torch = cuda
+    if family == "ausm" and name == "box_eu":
+        pytest.skip("the reference runs AUSM+ for the Navier-Stokes equations only")
     case = with_family(SMALL[name](), FAMILIES[family])
     orc, st = _prepared_flow(case)
     s = _gpu(case)
@@ -36,6 +38,8 @@ def test_block_residual_parity(cuda, family, name):
     for l in range(1, case.layout.nblk + 1):
         if family == "rusanov":
             L.orc_sch_rusanov(l, u_o, st.v, st.tau, st.sn, st.ps)
+        elif family == "ausm":
+            L.orc_sch_ausmp(l, u_o, st.v, st.tau, st.sn, st.ps)
         elif ns:
             L.orc_sch_hllc(l, u_o, st.v, st.tau, st.sn, st.ps)
         else:
@@ -46,6 +50,8 @@ def test_block_residual_parity(cuda, family, name):
         torch.cuda.synchronize()
         if family == "rusanov":
             s.sch_rusanov(l, s.u, s.v, s.tau, s.sn, s.pression)
+        elif family == "ausm":
+            s.sch_ausmp(l, s.u, s.v, s.tau, s.sn, s.pression)
         elif ns:
             s.sch_hllc(l, s.u, s.v, s.tau, s.sn, s.pression)
         else:
@@ -61,6 +67,8 @@ def test_block_residual_parity(cuda, family, name):
 @pytest.mark.parametrize("family", sorted(FAMILIES))
 @pytest.mark.parametrize("name,nsteps", [("box_ns", 5), ("channel", 5), ("box_eu_qfix", 5)])
 def test_fused_steps_parity(cuda, family, name, nsteps):
+    if family == "ausm" and name == "box_eu_qfix":
+        pytest.skip("the reference runs AUSM+ for the Navier-Stokes equations only")
     case = with_family(SMALL[name](), FAMILIES[family])
     orc, st = oracle_prepared(case)
     s = _gpu(case)
@@ -93,7 +101,10 @@ def test_mixed_form_matches_the_fp64_converged_state(cuda, family):
     b = _solver(with_family(_duct(), FAMILIES[family]), 1)
     na = a.atsch_num(4500)
     nb = b.atsch_num(4500)
-    assert na[1, 0] < 1e-12 and nb[1, 0] < 1e-12, (na[1, 0], nb[1, 0])
+    # AUSM+ settles near 1e-9 on this duct (FP64 and mixed alike: its
+    # splitting polynomials switch at |M| = 1); the others reach rounding
+    tol = 1e-8 if family == "ausm" else 1e-12
+    assert na[1, 0] < tol and nb[1, 0] < tol, (na[1, 0], nb[1, 0])
     case = a.case
     ld = case.layout.ld
     rc = case.layout.real_cells()
@@ -101,3 +112,16 @@ def test_mixed_form_matches_the_fp64_converged_state(cuda, family):
     assert err <= STEADY_TOL, err
     a.close()
     b.close()
+
+
+def test_ausm_needs_the_navier_stokes_equations(cuda):
+    from codens_b200 import abi
+    from codens_b200.solver import CodeNS
+    case = SMALL["box_eu"]()
+    s = CodeNS(case)
+    sc = case.scheme
+    sc.ischema = 5
+    with pytest.raises(abi.CnsError) as e:
+        s.set_scheme(sc)
+    assert e.value.code == abi.CNS_EINVAL
+    s.close()
