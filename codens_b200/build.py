@@ -18,7 +18,10 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcodens_b200.so")
 # FP64 parity sources: no FMA contraction, every product and sum rounded as
 # written.  The FP32 half of the mixed-precision form (cns_mixed.cu) is not a
-# parity path and is built with contraction.
+# parity path: it is built with contraction and with the approximate
+# single-precision division and square root (-prec-div/-prec-sqrt affect FP32
+# only; its FP64 residual keeps IEEE division), which the mixed form's FP64
+# fixed point does not depend on.
 SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_jameson.cu", "cns_turb.cu", "cns_sa.cu",
            "cns_adjoint.cu", "cns_abi.cu", "cns_noalloc.cu", "cns_io.cu"]
 SOURCES_FMA = ["cns_mixed.cu"]
@@ -31,7 +34,7 @@ COMMON = [
     "-I" + os.path.join(ROOT, "include"),
 ]
 FLAGS = COMMON + ["--fmad=false"]
-FLAGS_FMA = COMMON + ["--fmad=true"]
+FLAGS_FMA = COMMON + ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
 
 
 def sources():
