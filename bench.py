@@ -560,7 +560,6 @@ def run_adjoint(args):
     512x256x4 cells, and the converged totals (primal to L2 < 1e-12, adjoint
     to a 1e-10 relative residual) on a 128x64x4 channel, where the full size
     would not converge within a bench run"""
-    import dataclasses
     import torch
     from codens_b200 import adjoint
     from codens_b200.solver import CodeNS

@@ -8,7 +8,6 @@ import numpy as np
 import pytest
 
 from codens_b200 import cases
-from oracle.oracle import Oracle, OracleState
 from tests._helpers import oracle_prepared
 
 pytestmark = pytest.mark.gpu
