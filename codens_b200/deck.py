@@ -17,7 +17,9 @@ defdffw.f90, defsecpfw.f90):
     define physics  [iflu i] [gammal g] [rgazl r] [pinfl p] [ql q]
                     [prandtll pr] [prandtlt prt] [reyref re]   tcmd_dfph.f90
     define numerics [nfi n] [fmg kfmg lgx kcg] [schema s] [muscl m xk ilim]
-                    [prcd kprec cte kvisq] [dual ...]           tcmd_dfnm.f90
+                    [prcd kprec cte kvisq] [dual kdualns tol niter tolke nitur]
+                                                  tcmd_dfnm.f90 (fmg 3: dual time stepping,
+                                                  compute flow = smg_num's physical time loop)
     define state n [ktype t] [roi r] [ai a] [ti t] [long l] [mach m]
                    [alpha a] [beta b]                          tcmd_dfst.f90
     define normaliz n                             tcmd_dfnzst.f90, dfnzst.f90, c_nzst.f90
@@ -46,7 +48,7 @@ What the subset does not handle raises ``DeckError`` naming the command:
 boundary kinds other than extr, para, idd, prd and coincident joins;
 boundaries that do not cover a whole block face; coincident joins whose
 index directions are not the identity; turbulence models (equat(6:7) =
-'ke'), multigrid and dual time (kfmg /= 0), preconditioning (kprec /= 0),
+'ke'), multigrid (kfmg 1, 2), preconditioning (kprec /= 0),
 explicit stepping (kmf = 0), rotating frames, and per-domain values of eta,
 lmax, ki2 or ki4 that differ between domains.  Files are the reference's
 names in the deck's directory (fgv, fgc, fgcf, fac, facf, finia1).
@@ -141,6 +143,8 @@ class DeckRun:
     solver: object
     norms: List[np.ndarray] = field(default_factory=list)   # after each compute flow
     files: List[str] = field(default_factory=list)          # files written
+    inner: List[List[int]] = field(default_factory=list)    # dual time: inner iterations
+    dual_started: bool = False
 
 
 class Deck:
@@ -162,6 +166,7 @@ class Deck:
         self.omg = 0.0
         # numerics (defdfnm.f90, defdfpm*.f90)
         self.nfi, self.kfmg, self.lgx = 1, 0, 1
+        self.kdualns, self.dual_tol, self.dual_niter = 0, 0.0, 1
         self.ischema, self.muscl, self.xk, self.ilim, self.kprec = 1, 0, 0.0, 0, 0
         self.eta: Dict[int, float] = {}
         self.lmax: Dict[int, int] = {}
@@ -279,7 +284,11 @@ class Deck:
                 return 3
 
             def dual(cc, k):
-                raise DeckError(f"{cc}: dual time stepping not handled")
+                # kdualns tol niter tolke nitur (tolke, nitur: the transport
+                # equations' inner loop, not handled here)
+                self.kdualns, self.dual_tol = _int(cc, k), _real(cc, k + 1)
+                self.dual_niter = _int(cc, k + 2)
+                return 5
 
             self._keywords(c, {"nfi": setattr_("nfi", _int), "fmg": fmg,
                                "schema": setattr_("ischema", _int), "muscl": muscl,
@@ -458,8 +467,10 @@ class Deck:
             raise DeckError(f"equat {self.equat!r}: only 3-D equations are handled")
         if self.equat[5:7] == "ke":
             raise DeckError("turbulence models (equat 'ke') not handled")
-        if self.nfi != 1 or self.kfmg != 0 or self.lgx != 1:
-            raise DeckError("nfi 1, kfmg 0 and one grid level only")
+        if self.nfi != 1 or self.kfmg not in (0, 3) or self.lgx != 1:
+            raise DeckError("nfi 1, kfmg 0 or 3 (dual time) and one grid level only")
+        if self.kfmg == 3 and self.dt1min == REELMX:
+            raise DeckError("dual time stepping needs the physical step (pm_dtg dt1min)")
         if self.kprec != 0:
             raise DeckError("preconditioning (kprec) not handled")
         if self.ischema not in (1, 7):
@@ -473,7 +484,7 @@ class Deck:
                       lmax=self._uniform("lmax", self.lmax, 10), ischema=self.ischema,
                       ki2=self._uniform("ki2", self.ki2, 0.0),
                       ki4=self._uniform("ki4", self.ki4, 0.032), ncychro=self.ncychro,
-                      icychr0=self.icychr0)
+                      icychr0=self.icychr0, kfmg=self.kfmg, kdualns=self.kdualns)
 
     def phys(self) -> Phys:
         if self.tnz is None and self.equat[:2] == "ns":
@@ -607,7 +618,15 @@ class Deck:
             elif kind == "cpfw":
                 if self.ncycle == INTMX:
                     raise DeckError(f"{cmd}: set env_cpfw ... ncycle n first")
-                out.norms.append(s.atsch_num(self.ncycle))
+                if self.kfmg == 3:
+                    # smg_num.f90:130-470: ncycle physical steps of at most
+                    # niter inner iterations
+                    out.inner.append(s.dual_time(self.ncycle, self.dual_niter, self.dual_tol,
+                                                 start=not out.dual_started))
+                    out.dual_started = True
+                    out.norms.append(s.last_norms())
+                else:
+                    out.norms.append(s.atsch_num(self.ncycle))
             elif kind in ("svgr", "svfw"):
                 disc = act[1]
                 if disc not in files:

@@ -124,7 +124,7 @@ init boundary basic 3 para 1
     ("init boundary basic 1 nrd 1", "boundary kind"),
     ("create boundary st 2 1 1 1 1 1 3 1 3 i1\ninit boundary basic 2 extr 1",
      "whole block faces"),
-    ("define numerics dual 1 1.e-3 10 1.e-3 10", "dual time"),
+    ("define numerics fmg 1 1 0", "kfmg 0 or 3"),
     ("define pm_turbn icytur0 1", "turbulence"),
     ("frobnicate", "not handled"),
 ])
@@ -147,3 +147,18 @@ def test_per_domain_values_must_agree(tmp_path):
             "define pm_dtd ldom 1 lgr * eta 2.\nend\n")
     with pytest.raises(DeckError, match="eta differs"):
         Deck(write_deck(tmp_path, text)).scheme()
+
+
+def test_dual_time_deck(tmp_path):
+    text = BOX_DECK.replace("define numerics schema 7 muscl 1 -1. 1",
+                            "define numerics schema 7 muscl 1 -1. 1 fmg 3 1 0 "
+                            "dual 0 1.e-2 6 1.e-3 10")
+    text = text.replace("define pm_dtg kdtl 1 icychr0 3 ncychro 2",
+                        "define pm_dtg kdtl 1 icychr0 3 ncychro 2 dt1min 0.02")
+    deck = Deck(write_deck(tmp_path, text))
+    sc = deck.scheme()
+    assert (sc.kfmg, sc.kdualns, sc.dt1min) == (3, 0, 0.02)
+    assert (deck.dual_tol, deck.dual_niter) == (1.0e-2, 6)
+    bad = text.replace(" dt1min 0.02", "")
+    with pytest.raises(DeckError, match="physical step"):
+        Deck(write_deck(tmp_path, bad, "flec2")).scheme()

@@ -88,3 +88,32 @@ def test_time_step_frequency_in_the_mixed_form(cuda):
     assert np.all(np.isfinite(n))
     assert s.kernels_launched > 0
     s.close()
+
+
+def test_dual_time_deck_runs_the_physical_time_loop(cuda, tmp_path):
+    """a deck with fmg 3 / dual runs smg_num's physical time loop: the same
+    as CodeNS.dual_time from the deck's saved initial state, bit for bit"""
+    from codens_b200.solver import CodeNS
+    box = cases.box_case((10, 8, 5), ns=True, ilim=1, skew=0.02, alpha=-3.0)
+    lay = box.layout
+    assert orc_lib().orc_setup(lay.nblk, lay.dims_array(), lay.ld) == 0
+    assert Oracle.writdg(str(tmp_path / "fgv"), "cvcv", box.x, box.y, box.z) == 0
+    (tmp_path / "finia1").write_text("0.8 -3. 0.\n")
+    text = BOX_DECK.replace("define numerics schema 7 muscl 1 -1. 1",
+                            "define numerics schema 7 muscl 1 -1. 1 fmg 3 1 0 "
+                            "dual 0 1.e-2 6 1.e-3 10")
+    text = text.replace("define pm_dtg kdtl 1 icychr0 3 ncychro 2",
+                        "define pm_dtg kdtl 1 icychr0 3 ncychro 2 dt1min 0.02")
+    (tmp_path / "flec").write_text(text)
+    deck = Deck(str(tmp_path / "flec"))
+    run = deck.run()
+    s2 = CodeNS(deck.case())
+    s2.readdg(str(tmp_path / "fgv"))
+    s2.readda(str(tmp_path / "fac"), "ns3d   ")
+    counts = s2.dual_time(deck.ncycle, deck.dual_niter, deck.dual_tol)
+    assert run.inner == [counts]
+    rc = lay.real_cells()
+    assert np.array_equal(_n(run.solver.v).reshape(5, lay.ld)[:, rc],
+                          _n(s2.v).reshape(5, lay.ld)[:, rc])
+    run.solver.close()
+    s2.close()
