@@ -473,8 +473,11 @@ class Deck:
             raise DeckError("dual time stepping needs the physical step (pm_dtg dt1min)")
         if self.kprec != 0:
             raise DeckError("preconditioning (kprec) not handled")
-        if self.ischema not in (1, 7):
-            raise DeckError(f"schema {self.ischema} not handled (1 Jameson, 7 Roe)")
+        if self.ischema not in (1, 5, 7, 9, 14):
+            raise DeckError(f"schema {self.ischema} not handled (1 Jameson, 5 AUSM+, 7 Roe, "
+                            "9 Rusanov, 14 HLLC)")
+        if self.ischema == 5 and self.equat[:2] != "ns":
+            raise DeckError("schema 5 (AUSM+) runs with the Navier-Stokes equations only")
         if self._uniform("kmf", self.kmf, 1) != 1:
             raise DeckError("explicit stepping (kmf 0) not handled")
         return Scheme(ns=1 if self.equat[:2] == "ns" else 0, muscl=self.muscl, xk=self.xk,

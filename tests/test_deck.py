@@ -162,3 +162,13 @@ def test_dual_time_deck(tmp_path):
     bad = text.replace(" dt1min 0.02", "")
     with pytest.raises(DeckError, match="physical step"):
         Deck(write_deck(tmp_path, bad, "flec2")).scheme()
+
+
+@pytest.mark.parametrize("schema", [5, 9, 14])
+def test_other_flux_families_from_the_deck(tmp_path, schema):
+    text = BOX_DECK.replace("define numerics schema 7", f"define numerics schema {schema}")
+    assert Deck(write_deck(tmp_path, text)).scheme().ischema == schema
+    if schema == 5:
+        eu = text.replace("define flow equat ns3d", "define flow equat eu3d")
+        with pytest.raises(DeckError, match="AUSM"):
+            Deck(write_deck(tmp_path, eu, "flec2")).scheme()
