@@ -445,9 +445,12 @@ __device__ __forceinline__ void load_prim(const T* __restrict__ v,
 // Results go to G[dir][a][n], n the cell above the face; HLLC with the
 // stresses also writes the halves of its viscous flux 0.5*fv to
 // V[dir][a-1][n] (a = 1..4), which sch_hllc.f90 applies as a second term.
-// FL: kFluxRoe, kFluxHllc or kFluxRusanov (Rusanov with NS = true always).
+// FL: kFluxRoe, kFluxHllc, kFluxRusanov (with NS = true always) or kFluxAusm.
+// Occupancy: 4 CTAs per SM for Roe (128 registers; 2, 3, 5, 6 measured
+// slower), 5 for the lighter families (HLLC residual 1.59 -> 1.42 ms,
+// Rusanov 1.27 -> 1.18 ms against 4 on the 4.4M-cell channel).
 template <class T, bool NS, int FL = kFluxRoe>
-__global__ void __launch_bounds__(kTile, 4) k_face_flux(
+__global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
     const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
     const T* __restrict__ v, const T* __restrict__ prim, long long ld,
     const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
