@@ -37,7 +37,8 @@ class Scheme_t(C.Structure):
                 ("eta", c_f64), ("kdtl", c_i32), ("dt1min", c_f64), ("lmax", c_i32),
                 ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32),
                 ("ischema", c_i32), ("ki2", c_f64), ("ki4", c_f64), ("ncychro", c_i32),
-                ("icychr0", c_i32), ("kfmg", c_i32), ("kdualns", c_i32)]
+                ("icychr0", c_i32), ("kfmg", c_i32), ("kdualns", c_i32),
+                ("eta_l", P(c_f64)), ("ki2_l", P(c_f64)), ("ki4_l", P(c_f64))]
 
 
 class Bnd_t(C.Structure):

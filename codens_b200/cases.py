@@ -84,6 +84,9 @@ class Scheme:
     icychr0: int = 0     # (atsch_num.f90:173-178, 436); ncychro <= 1: every iteration
     kfmg: int = 0        # 3: dual time stepping, physical time step dt1min
     kdualns: int = 0     # dual time order: 0, 1 second (BDF2), 2 third
+    eta_l: Optional[Sequence[float]] = None   # per block eta(lm) (else eta for all)
+    ki2_l: Optional[Sequence[float]] = None   # per block ki2(lm)
+    ki4_l: Optional[Sequence[float]] = None   # per block ki4(lm)
 
 
 @dataclass

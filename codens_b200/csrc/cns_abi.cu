@@ -306,7 +306,7 @@ cudaError_t jameson_dissipation(cns_ctx* c, bool first) {
   if (e == cudaSuccess)
     e = launch_ghost_refresh(c->bd, 2, s.v, ld, s.pression, s.ztemp, s.cson, c->st);
   if (e == cudaSuccess)
-    e = launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(-1), -1, c->sc.ki2, c->sc.ki4,
+    e = launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(-1), -1,
                               s.v, ld, s.pression, s.cson, s.sn, c->w.G, c->w.dis, c->st);
   return e;
 }
@@ -932,6 +932,16 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.icychr0 = s->icychr0;
   c->sc.kfmg = s->kfmg;
   c->sc.kdualns = s->kdualns;
+  // eta(lm), ki2(lm), ki4(lm): per block when given, else the scalars
+  for (size_t b = 0; b < c->lay.blks.size(); ++b) {
+    Blk& B = c->lay.blks[b];
+    B.eta = s->eta_l ? s->eta_l[b] : s->eta;
+    B.ki2 = s->ki2_l ? s->ki2_l[b] : s->ki2;
+    B.ki4 = s->ki4_l ? s->ki4_l[b] : s->ki4;
+  }
+  if (c->d_blks)
+    CK(cudaMemcpy(c->d_blks, c->lay.blks.data(), sizeof(Blk) * c->lay.blks.size(),
+                  cudaMemcpyHostToDevice));
   drop_graphs(c);
   if (c->w.ld > 0) CK(ensure_hllc_v(c));
   return CNS_OK;
@@ -1104,8 +1114,8 @@ int cns_dissip_jameson(cns_ctx* c, int l, const double* v, double* d, const doub
                        const double* ps, const double* cson) {
   if (!c || bad_block(c, l) || !v || !d || !sn || !ps || !cson) return CNS_EINVAL;
   CK(zero_cols(c, d, 5, l));
-  CK(launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, c->sc.ki2,
-                           c->sc.ki4, v, c->lay.ld, ps, cson, sn, c->w.G, d, c->st));
+  CK(launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, v, c->lay.ld,
+                           ps, cson, sn, c->w.G, d, c->st));
   return CNS_OK;
 }
 

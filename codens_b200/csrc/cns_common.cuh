@@ -31,6 +31,7 @@ struct Blk {
   int nid, njd, nkd;        // with the ghost layer
   long long npc;            // flat offset of the block
   long long nijd, nnn;
+  double eta, ki2, ki4;     // the block's eta(lm), ki2(lm), ki4(lm) (schemanum)
 };
 
 // index space over all blocks: element e of block b has extents ext[3b..3b+2]

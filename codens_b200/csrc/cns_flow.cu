@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kTile) k_chronos(
   const double qq = (sq(t[ld + nc]) + sq(t[2 * ld + nc]) + sq(t[3 * ld + nc])) / sq(ro);
   const double q = sqrt(qq);
   const double dte = dism / (q + cson[nc]);
-  double d = sc.eta * dte;
+  double d = B.eta * dte;
   if (sc.ns) {
     const double rv1 = ph.gam * (mu[nc] / ph.pr + mut[nc] / ph.prt) / t[nc];
     const double rv = fmax(rv1, 4. / 3. * (mu[nc] + mut[nc]) / t[nc]);
-    const double dtv = sc.eta * 0.25 * sq(dism) / rv;
+    const double dtv = B.eta * 0.25 * sq(dism) / rv;
     d = fmin(d, dtv);
   }
   dt[nc] = d;

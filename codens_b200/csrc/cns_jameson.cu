@@ -62,7 +62,7 @@ __device__ __forceinline__ double sensor(const double* __restrict__ ps, long lon
 // twins): interior faces blend 2nd and 4th differences, boundary faces use
 // the 2nd difference with the sensor of their real cell
 __global__ void __launch_bounds__(kTile) k_dissip_face(const Blk* __restrict__ blks, Space sp,
-                                                       int dir, double ck2, double ck4,
+                                                       int dir,
                                                        const double* __restrict__ v,
                                                        long long ld,
                                                        const double* __restrict__ ps,
@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(kTile) k_dissip_face(const Blk* __restrict__ b
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
+  const double ck2 = B.ki2, ck4 = B.ki4;  // ki2(lm), ki4(lm)
   const long long n = cell_index(B, i, j, k);
   const long long inc = ninc_of(B, dir);
   const int nd = nd_of(B, dir);
@@ -238,13 +239,13 @@ cudaError_t launch_ghost_refresh(const Bnd& bd, int mode, double* v, long long l
 }
 
 cudaError_t launch_dissip_jameson(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
-                                  double ck2, double ck4, const double* v, long long ld,
+                                  const double* v, long long ld,
                                   const double* ps, const double* cson, const double* sn,
                                   double* G, double* d, cudaStream_t st) {
   for (int dir = 0; dir < 3; ++dir) {
     const Space sp = faces[dir].view(l0);
     if (sp.ntiles > 0)
-      k_dissip_face<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ck2, ck4, v, ld, ps, cson,
+      k_dissip_face<<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, v, ld, ps, cson,
                                                    sn, G);
   }
   if (cells.ntiles > 0)

@@ -253,7 +253,7 @@ cudaError_t launch_ghost_refresh(const Bnd& bd, int mode, double* v, long long l
                                  double* temp, double* cson, cudaStream_t st);
 // dissipation of the faces of block l0 (all: -1) into G, summed into d
 cudaError_t launch_dissip_jameson(const Blk* blks, const SpaceBuf* faces, Space cells, int l0,
-                                  double ck2, double ck4, const double* v, long long ld,
+                                  const double* v, long long ld,
                                   const double* ps, const double* cson, const double* sn,
                                   double* G, double* d, cudaStream_t st);
 // centred fluxes into G, u = 0.5 sum - dis (u32: float copy when given)

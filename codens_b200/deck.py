@@ -49,8 +49,8 @@ boundary kinds other than extr, para, idd, prd and coincident joins;
 boundaries that do not cover a whole block face; coincident joins whose
 index directions are not the identity; turbulence models (equat(6:7) =
 'ke'), multigrid (kfmg 1, 2), preconditioning (kprec /= 0),
-explicit stepping (kmf = 0), rotating frames, and per-domain values of eta,
-lmax, ki2 or ki4 that differ between domains.  Files are the reference's
+explicit stepping (kmf = 0), rotating frames, and values of lmax that differ
+between domains (eta, ki2 and ki4 may differ).  Files are the reference's
 names in the deck's directory (fgv, fgc, fgcf, fac, facf, finia1).
 """
 from __future__ import annotations
@@ -480,13 +480,19 @@ class Deck:
             raise DeckError("schema 5 (AUSM+) runs with the Navier-Stokes equations only")
         if self._uniform("kmf", self.kmf, 1) != 1:
             raise DeckError("explicit stepping (kmf 0) not handled")
+        ls = sorted(self.domains)
+        per = {n: [getattr(self, n).get(l, dflt) for l in ls]
+               for n, dflt in (("eta", 1.0), ("ki2", 0.0), ("ki4", 0.032))}
         return Scheme(ns=1 if self.equat[:2] == "ns" else 0, muscl=self.muscl, xk=self.xk,
-                      ilim=self.ilim, eta=self._uniform("eta", self.eta, 1.0),
+                      ilim=self.ilim, eta=per["eta"][0] if ls else 1.0,
+                      eta_l=per["eta"] if len(set(per["eta"])) > 1 else None,
+                      ki2_l=per["ki2"] if len(set(per["ki2"])) > 1 else None,
+                      ki4_l=per["ki4"] if len(set(per["ki4"])) > 1 else None,
                       kdtl=0 if self.kdtl == 0 else 1,
                       dt1min=self.dt1min if self.dt1min != REELMX else 0.0,
                       lmax=self._uniform("lmax", self.lmax, 10), ischema=self.ischema,
-                      ki2=self._uniform("ki2", self.ki2, 0.0),
-                      ki4=self._uniform("ki4", self.ki4, 0.032), ncychro=self.ncychro,
+                      ki2=per["ki2"][0] if ls else 0.0,
+                      ki4=per["ki4"][0] if ls else 0.032, ncychro=self.ncychro,
                       icychr0=self.icychr0, kfmg=self.kfmg, kdualns=self.kdualns)
 
     def phys(self) -> Phys:

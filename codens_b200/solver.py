@@ -130,6 +130,17 @@ class CodeNS:
     # ------------------------------------------------------------------
     @staticmethod
     def _scheme_t(s, qfix_dfez: int = 0):
+        # per-block eta(lm), ki2(lm), ki4(lm): ctypes arrays kept on the struct
+        keep = {}
+        for name in ("eta_l", "ki2_l", "ki4_l"):
+            vals = getattr(s, name, None)
+            keep[name] = (C.c_double * len(vals))(*map(float, vals)) if vals is not None else None
+        st = CodeNS._scheme_fields(s, qfix_dfez, keep)
+        st._keep = keep
+        return st
+
+    @staticmethod
+    def _scheme_fields(s, qfix_dfez, keep):
         return abi.Scheme_t(int(s.ns), int(s.muscl), float(s.xk), int(s.ilim), float(s.eta),
                             int(s.kdtl), float(s.dt1min), int(s.lmax),
                             int(getattr(s, "qfix_dfez", qfix_dfez)),
@@ -137,7 +148,9 @@ class CodeNS:
                             int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
                             float(getattr(s, "ki4", 1.0 / 32.0)),
                             int(getattr(s, "ncychro", 1)), int(getattr(s, "icychr0", 0)),
-                            int(getattr(s, "kfmg", 0)), int(getattr(s, "kdualns", 0)))
+                            int(getattr(s, "kfmg", 0)), int(getattr(s, "kdualns", 0)),
+                            *(C.cast(keep[n], C.POINTER(C.c_double)) if keep[n] is not None
+                              else None for n in ("eta_l", "ki2_l", "ki4_l")))
 
     def _check(self, rc: int, where: str):
         if rc:

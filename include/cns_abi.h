@@ -109,6 +109,9 @@ typedef struct {
                             atsch_num.f90:993-1003) with physical step dt1min */
   int32_t kdualns;       /* dual time: 0 or 1 second order (sch_dual, sch_duup),
                             2 third order (sch_dual2, sch_duup2) */
+  const double *eta_l;   /* [nblk] eta(lm) of each block, or NULL: eta for all */
+  const double *ki2_l;   /* [nblk] ki2(lm), or NULL: ki2 for all */
+  const double *ki4_l;   /* [nblk] ki4(lm), or NULL: ki4 for all */
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */

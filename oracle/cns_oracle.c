@@ -35,6 +35,8 @@ static struct {
   double xk, eta, dt1min;
   int ischema;           /* 1: Jameson (central + scalar dissipation), 7: Roe */
   double ki2, ki4;       /* Jameson dissipation coefficients ki2(lm), ki4(lm) */
+  /* eta(lm), ki2(lm), ki4(lm) per block (NULL: the scalars for all) */
+  double *eta_l, *ki2_l, *ki4_l;
   /* dual time stepping (kfmg = 3): dt1min is the physical time step */
   int kfmg, kdualns, icycle;
   double *ptdual;
@@ -137,6 +139,23 @@ void orc_set_threads(int n) {
 #else
   (void)n;
 #endif
+}
+
+static void set_block_array(double **dst, const double *src) {
+  free(*dst);
+  *dst = NULL;
+  if (!src) return;
+  *dst = (double *)malloc(sizeof(double) * (size_t)G.nblk);
+  memcpy(*dst, src, sizeof(double) * (size_t)G.nblk);
+}
+
+/* eta(lm), ki2(lm), ki4(lm) of each block (tcmd_dfpmdtd.f90,
+ * tcmd_dfpmdsd.f90); NULL keeps the scalar of orc_set_scheme /
+ * orc_set_dissipation for every block */
+void orc_set_block_scheme(const double *eta_l, const double *ki2_l, const double *ki4_l) {
+  set_block_array(&G.eta_l, eta_l);
+  set_block_array(&G.ki2_l, ki2_l);
+  set_block_array(&G.ki4_l, ki4_l);
 }
 
 void orc_set_dissipation(int ischema, double ki2, double ki4) {
@@ -519,7 +538,7 @@ void orc_chronos(int l, const double *mu, const double *mut, const double *t,
         double smoy = sqrt(simax + sjmax + skmax);
         dism[mn] = vol[nc] / smoy;
       }
-  const double etal = G.eta;
+  const double etal = G.eta_l ? G.eta_l[l - 1] : G.eta;
   for (int k = k1; k <= k2 - 1; ++k)
     for (int j = j1; j <= j2 - 1; ++j)
       for (int i = i1; i <= i2 - 1; ++i) {
@@ -830,7 +849,8 @@ static void jameson_dissip_dir(const blk_t *b, int dir, double *d, const double 
                                const double *sn, const double *ps,
                                const double *cson, double *snu) {
   const int64_t L = G.ld, n0 = b->npc, ninc = NINC(b, dir);
-  const double ck2 = G.ki2, ck4 = G.ki4;
+  const int lb = (int)(b - G.b);
+  const double ck2 = G.ki2_l ? G.ki2_l[lb] : G.ki2, ck4 = G.ki4_l ? G.ki4_l[lb] : G.ki4;
   const int kdir = dir;  /* sn(m, kdir, c): 0-based here */
   /* sensor on the real cells (:99-110) */
   for (int k = 1; k <= b->nk - 1; ++k)

@@ -171,6 +171,9 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
              const double *vol, double *ps, double *temp, double *cson,
              double *mu, double *mut, double *tau, int compute_dt);
 
+/* per-block eta(lm), ki2(lm), ki4(lm) (NULL: the scalar for every block) */
+void orc_set_block_scheme(const double *eta_l, const double *ki2_l, const double *ki4_l);
+
 /* other flux families (atsch_num.f90:628-983): ischema 14 HLLC
  * (sch_hllc_euler, sch_hllc), ischema 9 Rusanov (sch_rusanov, with the
  * stresses tau whatever the equations: zero for Euler); orc_step selects by

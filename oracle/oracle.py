@@ -82,6 +82,7 @@ def lib():
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 8
         L.orc_set_sa_fix.argtypes = [C.c_int]
+        L.orc_set_block_scheme.argtypes = [C.c_void_p] * 3
         L.orc_sch_hllc_euler.argtypes = [C.c_int, _d, _d, _d, _d]
         L.orc_sch_hllc.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_sch_rusanov.argtypes = [C.c_int, _d, _d, _d, _d, _d]
@@ -156,6 +157,10 @@ class Oracle:
         lib().orc_set_dissipation(int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
                                   float(getattr(s, "ki4", 1.0 / 32.0)))
         self.jameson = int(getattr(s, "ischema", 7)) <= 4
+        self._block = [None if getattr(s, n, None) is None
+                       else np.ascontiguousarray(getattr(s, n), dtype=np.float64)
+                       for n in ("eta_l", "ki2_l", "ki4_l")]
+        lib().orc_set_block_scheme(*[None if a is None else a.ctypes.data for a in self._block])
         self.ncyc = 0
 
     def set_sa(self, st: OracleState, dist, rokinf: float, roeinf: float, epsk: float = 1e-8,

@@ -142,11 +142,15 @@ def test_coincident_join_needs_identity_directions(tmp_path):
         Deck(write_deck(tmp_path, text))
 
 
-def test_per_domain_values_must_agree(tmp_path):
+def test_per_domain_values(tmp_path):
     text = ("create dom st 1 3 3 3\ncreate dom st 2 3 3 3\n"
-            "define pm_dtd ldom 1 lgr * eta 2.\nend\n")
-    with pytest.raises(DeckError, match="eta differs"):
-        Deck(write_deck(tmp_path, text)).scheme()
+            "define pm_dtd ldom 1 lgr * eta 2.\ndefine pm_numd ldom 2 lgr * ki4 0.05\nend\n")
+    sc = Deck(write_deck(tmp_path, text)).scheme()
+    assert sc.eta_l == [2.0, 1.0] and sc.ki4_l == [0.032, 0.05] and sc.ki2_l is None
+    lm = ("create dom st 1 3 3 3\ncreate dom st 2 3 3 3\n"
+          "define pm_numi ldom 1 lgr * lmax 4\nend\n")
+    with pytest.raises(DeckError, match="lmax differs"):
+        Deck(write_deck(tmp_path, lm, "flec2")).scheme()
 
 
 def test_dual_time_deck(tmp_path):
