@@ -76,6 +76,10 @@ def parse():
     p.add_argument("--no-fp64-arm", action="store_true",
                    help="skip timing the plain FP64 iteration beside the mixed one")
     p.add_argument("--no-steady-check", action="store_true")
+    p.add_argument("--no-minmod", action="store_true",
+                   help="skip timing the minmod-limited (ilim 1) iteration beside the headline")
+    p.add_argument("--no-c1", action="store_true",
+                   help="skip the 64x32x32 box sub-runs 1a/1b/1c")
     p.add_argument("--rans-iters", type=int, default=3000,
                    help="rans workload: iterations of the convergence history")
     p.add_argument("--workload", default="channel",
@@ -227,8 +231,6 @@ def run_reference(args):
     case = make_case(args)
     # each timed step is a bounded sample: one iteration of the full case
     steps = max(1, min(args.steps, 2))
-    for _ in range(min(args.warmup, 0)):
-        pass
     rate, t, cores = cpu_reference_rate(case, steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
@@ -334,6 +336,44 @@ def steady_state_check(iters=4500):
     return out
 
 
+def c1_runs(torch, steps=100, warm=3):
+    """the 64x32x32-cell box (65,536 cells) as its three reference-path
+    sub-runs, FP64 and mixed, `steps` graph-launched iterations each on the
+    device (the box's state fits in L2: latency- and launch-bound, not an HBM
+    case).  1a and 1b run the flagged implimf_eu fix (qfix_dfez = 1): the
+    reference form turns non-finite within a few iterations."""
+    from codens_b200 import cases
+    from codens_b200.solver import CodeNS
+
+    out = {}
+    for sub in cases.C1_SUBRUNS:
+        rec = {}
+        for name, prec in (("fp64", 0), ("mixed", 1)):
+            case = cases.c1_case(sub, qfix_dfez=0 if sub == "1c" else 1)
+            case.scheme.precision = prec
+            s = CodeNS(case)
+            s.metric()
+            s.atsch_num(warm)
+            s.sync()
+            k0 = s.kernels_launched
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(s.stream)
+            s.atsch_num_launch(steps)
+            b.record(s.stream)
+            b.synchronize()
+            ms = a.elapsed_time(b)
+            n = s.last_norms()
+            rec[name] = {"value": case.layout.nreal * steps / (ms * 1e-3) / 1e6,
+                         "ms_per_step": ms / steps,
+                         "kernels_per_step": (s.kernels_launched - k0) / steps,
+                         "l2_rho": float(n[1, 0])}
+            s.close()
+        rec["qfix_dfez"] = 0 if sub == "1c" else 1
+        out[sub] = rec
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -425,13 +465,48 @@ def run_ours(args):
     if rank == 0 and args.precision == "mixed" and not args.no_steady_check:
         steady = steady_state_check()
 
+    # the minmod limiter (ilim = 1: the reference's in-place ratio recurrence,
+    # three line-recurrence launches more per iteration), same form and steps
+    minmod = None
+    if not args.ilim and not args.no_minmod:
+        sch = case.scheme
+        sch.ilim = 1
+        minmod = {}
+        for name, prec in ((args.precision, PRECISION[args.precision]), ("fp64", 0)):
+            if name in minmod:
+                continue
+            keep = sch.precision
+            sch.precision = prec
+            s.set_scheme(sch)
+            s.v.copy_(v_keep)
+            s.atsch_num(warm)
+            barrier()
+            msm, _ = _timed_steps(s, torch, args.steps)
+            msm = max_over_ranks(msm)
+            minmod[name] = {"value": ws * nreal * args.steps / (msm * 1e-3) / 1e6,
+                            "ms_per_step": msm / args.steps}
+            sch.precision = keep
+        sch.ilim = 0
+        s.set_scheme(sch)
+        s.v.copy_(v_keep)
+        torch.cuda.synchronize()
+
+    c1 = None
+    if rank == 0 and not args.no_c1:
+        c1 = c1_runs(torch, steps=100, warm=warm)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         rate, tc, cores = cpu_reference_rate(case, args.cpu_steps)
+        rate1, tc1, _ = cpu_reference_rate(case, 1, threads=1)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{args.cpu_steps} iteration(s) of the full case, the C "
                          f"restatement of the reference, per-block routines on {cores} host "
-                         f"threads ({tc:.1f} s)"}
+                         f"threads ({tc:.1f} s)",
+               "single_core": {"value": rate1, "unit": UNIT, "cores": 1,
+                               "sample": f"1 iteration of the full case on one thread "
+                                         f"({tc1:.1f} s)"},
+               "host_cores": os.cpu_count()}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
@@ -462,6 +537,10 @@ def run_ours(args):
         if fp64:
             line["fp64"] = fp64
             line["mixed_over_fp64"] = value / fp64["value"]
+        if minmod:
+            line["minmod_ilim1"] = minmod
+        if c1:
+            line["c1_box_64x32x32"] = c1
         if steady:
             line["steady_state"] = steady
         if cpu:

@@ -277,6 +277,32 @@ def box_case(cells=(64, 32, 32), mach: float = 0.8, seed: int = 1,
                 meta=dict(mach=mach, seed=seed, cells=tuple(cells)))
 
 
+C1_SUBRUNS = ("1a", "1b", "1c")
+
+
+def c1_case(sub: str, qfix_dfez: int = 0, seed: int = 1, lmax: int = 10) -> Case:
+    """The 64x32x32-cell stretched box at Mach 0.8 (extr i faces, periodic j
+    and k, 1% noise, CFL 5) as one of its three reference-path sub-runs:
+    1a Euler Roe with the unlimited kappa = -1 MUSCL (sch_roe_euler +
+    implimf_eu), 1b Euler Jameson with ki2 = 0.5, ki4 = 1/32 (dissip_jameson +
+    sch_jameson + implimf_eu), 1c the Navier-Stokes path at Re 1e12 with the
+    minmod limiter (sch_roe + implimf_3d).  qfix_dfez = 1 restores the factor
+    implimf_eu.f90:312 lacks (non-reference; the reference form of 1a and 1b
+    turns non-finite within a few iterations)."""
+    if sub == "1a":
+        return box_case((64, 32, 32), mach=0.8, seed=seed, lmax=lmax, qfix_dfez=qfix_dfez,
+                        name="c1a")
+    if sub == "1b":
+        c = box_case((64, 32, 32), mach=0.8, seed=seed, lmax=lmax, qfix_dfez=qfix_dfez,
+                     ischema=1, name="c1b")
+        c.scheme.ki2, c.scheme.ki4 = 0.5, 1.0 / 32.0
+        return c
+    if sub == "1c":
+        return box_case((64, 32, 32), mach=0.8, seed=seed, lmax=lmax, ns=True, ilim=1,
+                        reynz=1.0e12, name="c1c")
+    raise ValueError(f"unknown sub-run {sub!r}")
+
+
 def batch_case(ncase: int = 64, side=(16, 96), seed: int = 4,
                noise: float = 0.01, lmax: int = 10, eta: float = 5.0,
                mach_range=(0.3, 2.0), alpha_range=(-5.0, 5.0),

@@ -210,7 +210,8 @@ void drop_graphs(cns_ctx* c) {
         cudaGraphExecDestroy(g);
         g = nullptr;
       }
-  c->mixed_iter = 0;
+  // the defect-correction refresh schedule (mixed_iter) is not touched: new
+  // tiles, a new stream or recaptured graphs change no iteration's form
 }
 
 // atsch_num.f90:173-178, 436: whether the iteration with counters ncyc = n,
@@ -943,6 +944,7 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
     CK(cudaMemcpy(c->d_blks, c->lay.blks.data(), sizeof(Blk) * c->lay.blks.size(),
                   cudaMemcpyHostToDevice));
   drop_graphs(c);
+  c->mixed_iter = 0;  // a new scheme restarts the defect refresh schedule
   if (c->w.ld > 0) CK(ensure_hllc_v(c));
   return CNS_OK;
 }
@@ -1482,6 +1484,7 @@ int cns_bind_state(cns_ctx* c, const cns_state_t* s) {
   c->state = *s;
   c->bound = true;
   c->ncyc = c->cyc_n = c->cyc_i = 0;
+  c->mixed_iter = 0;
   drop_graphs(c);
   return CNS_OK;
 }

@@ -20,6 +20,7 @@
 // an anonymous namespace.
 #pragma once
 #include <cfloat>
+#include <type_traits>
 
 #include "cns_kernels.cuh"
 
@@ -794,9 +795,56 @@ __device__ __forceinline__ float rcpT<float>(float a) {
   return __fdividef(1.f, a);
 }
 
+// FP32 form of df_diff with every operation spelled out as a rounding
+// intrinsic (never contracted or reordered by the compiler).  A sweep
+// evaluates the same cell's increment at different places of the kernel --
+// a tile's first plane from global memory, a ring or patch cell staged in
+// shared memory -- and which place a cell takes depends on the tiling; with
+// explicit roundings every place gives the same bits, so the FP32 sweeps are
+// independent of the tiling the autotuner picks.
+template <bool EU>
+__device__ __forceinline__ void df_diff_f32(const float dd[5], float rho, float E, float p,
+                                            float qu, float qv, float qw, float gam1,
+                                            float pinfl, int qfix, float f[9]) {
+  const float r1 = __fadd_rn(rho, dd[0]);
+  const float ir1 = __fdividef(1.f, r1);
+  const float du = __fmul_rn(__fmaf_rn(-qu, dd[0], dd[1]), ir1);
+  const float dv = __fmul_rn(__fmaf_rn(-qv, dd[0], dd[2]), ir1);
+  const float dw = __fmul_rn(__fmaf_rn(-qw, dd[0], dd[3]), ir1);
+  const float q2 = __fmaf_rn(qu, qu, __fmaf_rn(qv, qv, __fmul_rn(qw, qw)));
+  const float qd = __fmaf_rn(qu, du, __fmaf_rn(qv, dv, __fmul_rn(qw, dw)));
+  const float d2 = __fmaf_rn(du, du, __fmaf_rn(dv, dv, __fmul_rn(dw, dw)));
+  const float dk = __fmaf_rn(dd[0], q2, __fmul_rn(r1, __fmaf_rn(2.f, qd, d2)));
+  const float dp = __fmul_rn(gam1, __fmaf_rn(-0.5f, dk, dd[4]));
+  const float h0 = __fsub_rn(__fadd_rn(E, p), pinfl);
+  const float de = __fadd_rn(dd[4], dp);
+  const float h1 = __fadd_rn(h0, de);
+  const float d0u = __fmul_rn(dd[0], qu), d0v = __fmul_rn(dd[0], qv),
+              d0w = __fmul_rn(dd[0], qw);
+  f[0] = __fmaf_rn(d0u, qu, __fmaf_rn(r1, __fmaf_rn(__fmul_rn(2.f, qu), du, __fmul_rn(du, du)),
+                                      dp));
+  f[1] = __fmaf_rn(d0u, qv, __fmul_rn(r1, __fmaf_rn(qu, dv, __fmaf_rn(qv, du, __fmul_rn(du, dv)))));
+  f[2] = __fmaf_rn(d0u, qw, __fmul_rn(r1, __fmaf_rn(qu, dw, __fmaf_rn(qw, du, __fmul_rn(du, dw)))));
+  f[3] = __fmaf_rn(du, h1, __fmul_rn(qu, de));
+  f[4] = __fmaf_rn(d0v, qv, __fmaf_rn(r1, __fmaf_rn(__fmul_rn(2.f, qv), dv, __fmul_rn(dv, dv)),
+                                      dp));
+  f[5] = __fmaf_rn(d0v, qw, __fmul_rn(r1, __fmaf_rn(qv, dw, __fmaf_rn(qw, dv, __fmul_rn(dv, dw)))));
+  f[6] = __fmaf_rn(dv, h1, __fmul_rn(qv, de));
+  f[7] = __fmaf_rn(d0w, qw, __fmaf_rn(r1, __fmaf_rn(__fmul_rn(2.f, qw), dw, __fmul_rn(dw, dw)),
+                                      dp));
+  // implimf_eu.f90:312 lacks the *wi factor of the z energy increment; the
+  // Euler form keeps it unless qfix (a flagged non-reference option) is set
+  f[8] = (EU && !qfix) ? __fmaf_rn(h1, ir1, -__fmul_rn(h0, qw))
+                       : __fmaf_rn(dw, h1, __fmul_rn(qw, de));
+}
+
 template <class T, bool EU>
 __device__ __forceinline__ void df_diff(const T dd[5], T rho, T E, T p, T qu, T qv, T qw,
                                         T gam1, T pinfl, int qfix, T f[9]) {
+  if constexpr (std::is_same<T, float>::value) {
+    df_diff_f32<EU>(dd, rho, E, p, qu, qv, qw, gam1, pinfl, qfix, f);
+    return;
+  }
   const T r1 = rho + dd[0];
   const T ir1 = rcpT(r1);
   const T du = (dd[1] - qu * dd[0]) * ir1;

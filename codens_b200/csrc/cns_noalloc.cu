@@ -25,7 +25,10 @@
 //
 // The first call on a device looks up the device address of the array
 // (cudaGetSymbolAddress) with that device current and remembers it; make
-// that first call before any stream capture.
+// that first call before any stream capture.  The remembered address belongs
+// to the device's current context: after cudaDeviceReset on that device it
+// is stale, so a process that resets a device must not call this entry point
+// on it again.
 #include <cstdint>
 #include <mutex>
 
@@ -87,6 +90,11 @@ extern "C" int cns_sch_roe_euler_noalloc(int32_t ni, int32_t nj, int32_t nk,
                                          const double* ps, void* stream) {
   if (ni < 2 || nj < 2 || nk < 2 || !u || !v || !sn || !ps || muscl < 0)
     return CNS_EINVAL;
+  // each ghosted side (n + 2) must fit the static array on its own before
+  // the block's extents are formed, so no product below can overflow
+  if ((long long)ni + 2 > kNoallocMaxLd || (long long)nj + 2 > kNoallocMaxLd ||
+      (long long)nk + 2 > kNoallocMaxLd)
+    return CNS_EINVAL;
   Blk B{};
   B.ni = ni;
   B.nj = nj;
@@ -98,7 +106,8 @@ extern "C" int cns_sch_roe_euler_noalloc(int32_t ni, int32_t nj, int32_t nk,
   B.nnn = B.nijd * B.nkd;
   B.npc = 0;
   // the block's cells must fit the caller's arrays and the static scratch
-  if (ld < B.nnn || ld > kNoallocMaxLd) return CNS_EINVAL;
+  if (B.nnn <= 0 || B.nnn > kNoallocMaxLd || ld < B.nnn || ld > kNoallocMaxLd)
+    return CNS_EINVAL;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices)
     return CNS_ECUDA;

@@ -1,0 +1,92 @@
+"""Parity at the sizes of the benchmark configurations, against the oracle.
+
+* The 64x32x32-cell stretched box (Mach 0.8, 1% noise, CFL 5, 100 implicit
+  iterations) as its three reference-path sub-runs: 1a Euler Roe
+  (sch_roe_euler + implimf_eu), 1b Euler Jameson (dissip_jameson +
+  sch_jameson + implimf_eu), 1c Navier-Stokes Roe with the minmod limiter
+  (sch_roe + implimf_3d).  The state after every iteration is compared bit
+  for bit and the L2 history at 1e-12 (the norms' tree sum).  With the
+  reference's implimf_eu (implimf_eu.f90:312, the missing *wi) 1a and 1b turn
+  non-finite after a few iterations in the oracle; the fused iteration must
+  agree bit for bit up to that iteration and then report the non-finite norm
+  on the same one.  With the flagged fix they run the 100 iterations.
+* The 8-block, 4.43M-cell laminar channel with the minmod limiter: three
+  fused iterations against the oracle (atsch_num.f90:245-1134) at 1e-12 (the
+  injection boundary's libm power), norms at 1e-12.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from codens_b200 import cases
+from oracle.oracle import lib as orc_lib
+
+from ._helpers import assert_equal_bits, max_rel_cols, oracle_prepared, real
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(case):
+    from codens_b200.solver import CodeNS
+    s = CodeNS(case)
+    s.metric()
+    return s
+
+
+@pytest.mark.parametrize("sub,qfix", [("1a", 0), ("1b", 0), ("1a", 1), ("1b", 1), ("1c", 0)])
+def test_c1_subrun_parity_100_iterations(cuda, sub, qfix):
+    from codens_b200 import abi
+    case = cases.c1_case(sub, qfix_dfez=qfix)
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    rc = real(case)
+    ran = 0
+    for it in range(100):
+        u0 = st.v.copy()
+        orc.step(st)
+        no = orc.norms(u0, st)
+        if not np.isfinite(no).all():
+            # the reference form turned non-finite: the fused iteration
+            # reports it on the same iteration
+            with pytest.raises(abi.CnsError) as ei:
+                s.atsch_num(1)
+            assert ei.value.code in (abi.CNS_ENONFINITE, abi.CNS_ETEMP), ei.value
+            assert qfix == 0 and sub in ("1a", "1b"), f"{sub} non-finite at {it}"
+            break
+        ng = s.atsch_num(1)
+        assert_equal_bits(s.v.cpu().numpy().reshape(5, ld)[:, rc], st.v.reshape(5, ld)[:, rc],
+                          f"{sub} v after iteration {it}")
+        np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0,
+                                   err_msg=f"{sub} L2 history at iteration {it}")
+        ran += 1
+    if qfix or sub == "1c":
+        assert ran == 100
+    else:
+        assert 1 <= ran < 100
+    s.close()
+
+
+def test_c2_channel_three_iterations(cuda):
+    """the full 8-block channel (seeded sides in 48..128, 4.43M cells),
+    minmod limiter, three fused FP64 iterations"""
+    orc_lib().orc_set_threads(os.cpu_count() or 1)
+    case = cases.channel_case(seed=2)
+    case.scheme.ilim = 1
+    assert case.layout.nblk == 8 and 3.5e6 <= case.layout.nreal <= 4.5e6
+    orc, st = oracle_prepared(case)
+    s = _gpu(case)
+    ld = case.layout.ld
+    rc = real(case)
+    for it in range(3):
+        u0 = st.v.copy()
+        orc.step(st)
+        no = orc.norms(u0, st)
+        ng = s.atsch_num(1)
+        err = max_rel_cols(s.v.cpu().numpy().reshape(5, ld)[:, rc], st.v.reshape(5, ld)[:, rc])
+        assert err <= 1e-12, (it, err)
+        np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0, err_msg=f"norms {it}")
+    s.close()

@@ -39,10 +39,17 @@ def _call(s, case, u, ld=None):
         C.c_void_p(s.stream.cuda_stream))
 
 
-@pytest.mark.parametrize("cells,pinfl", [((12, 7, 6), 0.0), ((30, 20, 16), 0.25)])
-def test_noalloc_matches_regular_entry_point(cuda, cells, pinfl):
+@pytest.mark.parametrize("cells,pinfl,muscl,xk", [((12, 7, 6), 0.0, 1, -1.0),
+                                                   ((30, 20, 16), 0.25, 1, -1.0),
+                                                   ((12, 7, 6), 0.0, 0, -1.0),
+                                                   ((10, 9, 7), 0.1, 1, 1.0 / 3.0)])
+def test_noalloc_matches_regular_entry_point(cuda, cells, pinfl, muscl, xk):
+    """first-order (muscl 0) and two kappa values of the MUSCL scheme, each
+    against the regular entry point run with the same scheme"""
     torch = cuda
     case = cases.box_case(cells, seed=31, skew=0.02, alpha=3.0, pinfl=pinfl)
+    case.scheme.muscl = muscl
+    case.scheme.xk = xk
     s = _inputs(case)
     ref = s.u.clone()
     rc = case.layout.real_cells()
@@ -61,6 +68,31 @@ def test_noalloc_matches_regular_entry_point(cuda, cells, pinfl):
     s.close()
 
 
+def test_noalloc_allocates_nothing(cuda):
+    """after a first call (which loads the module and looks up the static
+    array's address), further calls leave the device's free memory as it was"""
+    torch = cuda
+    case = cases.box_case((20, 14, 10), seed=33, skew=0.02, alpha=1.0)
+    s = _inputs(case)
+    u = torch.zeros_like(s.u)
+    assert _call(s, case, u) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert _call(s, case, u) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    s.close()
+
+
+def _call_dims(s, u, ni, nj, nk, ld):
+    return s.lib.cns_sch_roe_euler_noalloc(
+        ni, nj, nk, ld, 1.4, 0.0, 1, -1.0, C.c_void_p(u.data_ptr()),
+        C.c_void_p(s.v.data_ptr()), C.c_void_p(s.sn.data_ptr()),
+        C.c_void_p(s.pression.data_ptr()), C.c_void_p(s.stream.cuda_stream))
+
+
 def test_noalloc_rejects_oversize(cuda):
     torch = cuda
     case = cases.box_case((8, 6, 5), seed=32)
@@ -68,4 +100,10 @@ def test_noalloc_rejects_oversize(cuda):
     u = torch.zeros_like(s.u)
     assert _call(s, case, u, ld=131072 + 1) == 1          # beyond the static array
     assert _call(s, case, u, ld=case.layout.blocks[0].nnn - 1) == 1  # arrays too short
+    # sides whose ghosted size overflows 32-bit arithmetic or the array alone
+    big = 2**31 - 1
+    for dims in ((big, 4, 4), (4, big, 4), (4, 4, big), (131071, 3, 3), (60, 60, 60)):
+        assert _call_dims(s, u, *dims, 131072) == 1, dims
+    s.sync()
+    assert bool((u == 0).all())  # nothing was launched
     s.close()
