@@ -108,13 +108,19 @@ def load(build_if_missing: bool = True):
     L.cns_boundary_geom.argtypes = [vp] + [P(c_f64)] * 5
     L.cns_zpres.argtypes = [vp, C.c_int] + [vp] * 4
     L.cns_zvismo.argtypes = [vp, C.c_int] + [vp] * 3
-    L.cns_chronos.argtypes = [vp, C.c_int] + [vp] * 7
+    cs, i64 = C.c_char_p, c_i64
+    # the reference's argument lists (include/cns_abi.h); work arrays as vp
+    L.cns_chronos.argtypes = ([vp, C.c_int, c_f64] + [vp] * 3 + [vp, cs, vp, i64, vp] + [vp] * 4
+                              + [vp])
     L.cns_rbord.argtypes = [vp] * 5
-    L.cns_sch_roe_euler.argtypes = [vp, C.c_int] + [vp] * 4
-    L.cns_sch_roe.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_sch_roe_euler.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, cs, vp, i64] + [vp] * 11
+    L.cns_sch_roe.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp] + [vp] * 9 + [cs, vp, i64] + \
+        [vp] * 11
     L.cns_zvisqc.argtypes = [vp] * 8
-    L.cns_implimf_eu.argtypes = [vp, C.c_int] + [vp] * 8 + [C.c_int]
-    L.cns_implimf_3d.argtypes = [vp, C.c_int] + [vp] * 10 + [C.c_int]
+    L.cns_implimf_eu.argtypes = ([vp, C.c_int] + [vp] * 5 + [cs, C.c_int, vp, i64, vp, c_f64,
+                                                             C.c_int] + [vp] * 10 + [vp] * 2)
+    L.cns_implimf_3d.argtypes = ([vp, C.c_int] + [vp] * 7 + [cs, C.c_int, vp, i64, vp, c_f64,
+                                                             C.c_int] + [vp] * 10 + [vp] * 2)
     L.cns_rscpsv.argtypes = [vp] * 4 + [P(c_f64)]
     L.cns_bind_state.argtypes = [vp, P(State_t)]
     L.cns_atsch_num_step.argtypes = [vp, C.c_int, P(c_f64)]
@@ -123,17 +129,18 @@ def load(build_if_missing: bool = True):
     L.cns_sweep_tiles.argtypes = [vp, C.c_int, P(c_i32)]
     L.cns_rfve.argtypes = [vp] * 5
     L.cns_rfvc.argtypes = [vp] * 5
-    L.cns_dissip_jameson.argtypes = [vp, C.c_int] + [vp] * 5
-    L.cns_sch_jameson.argtypes = [vp, C.c_int] + [vp] * 6
+    L.cns_dissip_jameson.argtypes = [vp, C.c_int, vp, vp, cs, vp, i64, vp, vp, vp]
+    L.cns_sch_jameson.argtypes = ([vp, C.c_int, C.c_int] + [vp] * 4 + [vp] * 9 + [cs, vp, i64]
+                                  + [vp] * 9 + [vp])
     L.cns_set_turbulence.argtypes = [vp] + [c_f64] * 4
     L.cns_chrono_global.argtypes = [vp, vp]
     L.cns_adjoint_prepare.argtypes = [vp]
     L.cns_adjoint_rt.argtypes = [vp] * 4
     L.cns_adjoint_lt.argtypes = [vp] * 3
-    L.cns_met_fludc.argtypes = [vp, C.c_int] + [vp] * 8
+    L.cns_met_fludc.argtypes = [vp, C.c_int] + [vp] * 13
     L.cns_met_fludcsa.argtypes = [vp, C.c_int] + [vp] * 8
-    L.cns_met_roe2o.argtypes = [vp, C.c_int] + [vp] * 3
-    L.cns_met_roe2oh.argtypes = [vp, C.c_int] + [vp] * 3
+    L.cns_met_roe2o.argtypes = [vp, C.c_int, vp, vp, vp, i64, vp, vp, vp]
+    L.cns_met_roe2oh.argtypes = [vp, C.c_int, vp, vp, vp, i64, vp, vp, vp]
     L.cns_met_samut.argtypes = [vp, C.c_int] + [vp] * 3
     L.cns_sch_turb.argtypes = [vp, C.c_int] + [vp] * 13
     L.cns_teq_gradv.argtypes = [vp, C.c_int] + [vp] * 4
@@ -150,16 +157,16 @@ def load(build_if_missing: bool = True):
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,
                                             c_f64, vp, vp, vp, vp, vp]
-    cs = C.c_char_p
     L.cns_set_subrecord_length.argtypes = [vp, c_i64]
     L.cns_readdg.argtypes = [vp, cs, vp, vp, vp]
     L.cns_writdg.argtypes = [vp, cs, cs, vp, vp, vp]
     L.cns_readda.argtypes = [vp, cs, cs, C.c_int, vp, vp]
     L.cns_writda.argtypes = [vp, cs, cs, cs, vp, vp]
-    L.cns_sch_hllc_euler.argtypes = [vp, C.c_int] + [vp] * 4
-    L.cns_sch_hllc.argtypes = [vp, C.c_int] + [vp] * 5
-    L.cns_sch_rusanov.argtypes = [vp, C.c_int] + [vp] * 5
-    L.cns_sch_ausmp.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_sch_hllc_euler.argtypes = L.cns_sch_roe_euler.argtypes
+    L.cns_sch_hllc.argtypes = L.cns_sch_roe.argtypes
+    L.cns_sch_rusanov.argtypes = L.cns_sch_roe.argtypes
+    L.cns_sch_ausmp.argtypes = ([vp, C.c_int, C.c_int, vp, vp, vp, vp] + [vp] * 9 +
+                                [cs, vp, i64] + [vp] * 11)
     L.cns_set_cycle.argtypes = [vp, c_i64, c_i64]
     L.cns_sch_duin.argtypes = [vp]
     L.cns_sch_duup.argtypes = [vp]

@@ -41,6 +41,8 @@ struct cns_ctx {
   double* wall_par = nullptr;        // wall facet centres [3][n_wall_ent]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
+  double* tau_pack = nullptr;  // nine separate stress arrays packed as (ld, 9)
+  double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
   bool adj_fp32 = false;     // L^T of the prepared adjoint in FP32 (precision != 0)
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
   bool tuned64 = false, tuned32 = false;
@@ -268,6 +270,161 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
   if (e == cudaSuccess)
     e = launch_accumulate(c->d_blks, c->cells.view(l0), c->w.G, ld, u, c->st, c->w.V);
   return e;
+}
+
+// ---------------------------------------------------------------------------
+// The reference call surface of the per-routine entry points.
+//
+// Arrays may be host or device pointers.  A host array (the reference's own
+// Fortran arrays, passed as they are) is copied into a device buffer before
+// the routine and, when the routine writes it, back after it, and the call
+// returns when the copies are done: the copy-in/out parity mode.  Device
+// arrays pass through and the call only enqueues work on the context stream.
+// ---------------------------------------------------------------------------
+bool host_pointer(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // a pageable pointer the runtime does not know
+    return true;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
+}
+
+struct Staging {
+  explicit Staging(cns_ctx* ctx) : c(ctx) {}
+  ~Staging() {
+    for (void* b : bufs) cudaFree(b);
+  }
+  // n elements at p, read (in) and/or written (out) by the routine
+  template <class T>
+  T* map(T* p, size_t n, bool in, bool out) {
+    if (!p || err != cudaSuccess || !host_pointer(p)) return p;
+    void* q = nullptr;
+    err = cudaMalloc(&q, sizeof(T) * (n > 0 ? n : 1));
+    if (err != cudaSuccess) return p;
+    bufs.push_back(q);
+    if (in) err = cudaMemcpyAsync(q, p, sizeof(T) * n, cudaMemcpyHostToDevice, c->st);
+    else err = cudaMemsetAsync(q, 0, sizeof(T) * n, c->st);
+    if (out) outs.push_back({(void*)p, q, sizeof(T) * n});
+    staged = true;
+    return static_cast<T*>(q);
+  }
+  template <class T>
+  T* in(T* p, size_t n) { return map(p, n, true, false); }
+  template <class T>
+  T* inout(T* p, size_t n) { return map(p, n, true, true); }
+  // copy the outputs back; wait for the stream when anything was staged
+  cudaError_t finish() {
+    for (const Out& o : outs)
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, c->st);
+    if (err == cudaSuccess && staged) err = cudaStreamSynchronize(c->st);
+    return err;
+  }
+  struct Out {
+    void* host;
+    void* dev;
+    size_t bytes;
+  };
+  cns_ctx* c;
+  std::vector<void*> bufs;
+  std::vector<Out> outs;
+  bool staged = false;
+  cudaError_t err = cudaSuccess;
+};
+
+// equat (the reference's character*7, not NUL-terminated): the equations
+// (1:2) 'eu' or 'ns' and the three-dimensional form (3:4) '3d'; the
+// two-dimensional variants ('2dk', ...) are not provided
+bool equat_ok(const char* e) {
+  if (!e) return false;
+  const bool eq = (e[0] == 'e' && e[1] == 'u') || (e[0] == 'n' && e[1] == 's');
+  return eq && e[2] == '3' && e[3] == 'd';
+}
+
+// the reference passes sn(npsn), the block's slice (sequence association,
+// atsch_num.f90:470-479), with lgsnlt = nnn(lm); l = 0 (every block) takes
+// the whole array.  Elements of the slice, and the array base the kernels
+// index from.
+bool sn_slice_ok(cns_ctx* c, int l, long long lgsnlt) {
+  return l == 0 ? lgsnlt == c->lay.ld : lgsnlt == c->lay.blks[l - 1].nnn;
+}
+size_t sn_elems(cns_ctx* c, int l) {
+  return 9 * (size_t)(l == 0 ? c->lay.ld : c->lay.blks[l - 1].nnn);
+}
+const double* sn_base(cns_ctx* c, int l, const double* sn) {
+  return l == 0 ? sn : sn - 9 * c->lay.blks[l - 1].npc;
+}
+
+// the reference's nine stress / heat-flux arrays toxx, toxy, toxz, toyy,
+// toyz, tozz, qcx, qcy, qcz as one (ld, 9) array: used in place when they
+// are the columns of one such array, else gathered into context scratch
+cudaError_t tau_view(cns_ctx* c, Staging& sg, const double* const t[9], const double** out) {
+  const long long ld = c->lay.ld;
+  const double* d[9];
+  for (int a = 0; a < 9; ++a) {
+    d[a] = sg.in(t[a], (size_t)ld);
+    if (sg.err != cudaSuccess) return sg.err;
+  }
+  bool packed = true;
+  for (int a = 1; a < 9; ++a) packed = packed && d[a] == d[0] + a * ld;
+  if (packed) {
+    *out = d[0];
+    return cudaSuccess;
+  }
+  if (!c->tau_pack) {
+    cudaError_t e = dev_alloc(c, &c->tau_pack, (size_t)(9 * ld));
+    if (e != cudaSuccess) return e;
+  }
+  for (int a = 0; a < 9; ++a) {
+    cudaError_t e = cudaMemcpyAsync(c->tau_pack + a * ld, d[a], sizeof(double) * ld,
+                                    cudaMemcpyDeviceToDevice, c->st);
+    if (e != cudaSuccess) return e;
+  }
+  *out = c->tau_pack;
+  return cudaSuccess;
+}
+
+// ityprk != 0 (multigrid forcing, sch_roe.f90:1466-1481 and the other flux
+// routines): ff(n, 1:5) -= u(n, 1:5) on the real cells of block l
+__global__ void __launch_bounds__(kTile) k_forcing_sub(const Blk* __restrict__ blks, Space sp,
+                                                       long long ld,
+                                                       const double* __restrict__ u,
+                                                       double* __restrict__ ff) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) ff[a * ld + n] = ff[a * ld + n] - u[a * ld + n];
+}
+
+// ityprk != 0 in implimf_3d.f90:249-264 / implimf_eu: the right-hand side
+// -u - ff; out = u + ff on the real cells (-(u + ff) = -u - ff exactly)
+__global__ void __launch_bounds__(kTile) k_forcing_add(const Blk* __restrict__ blks, Space sp,
+                                                       long long ld,
+                                                       const double* __restrict__ u,
+                                                       const double* __restrict__ ff,
+                                                       double* __restrict__ out) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) out[a * ld + n] = u[a * ld + n] + ff[a * ld + n];
+}
+
+cudaError_t forcing_sub(cns_ctx* c, int l, const double* u, double* ff) {
+  const Space sp = c->cells.view(l - 1);
+  if (sp.ntiles > 0)
+    k_forcing_sub<<<sp.ntiles, kTile, 0, c->st>>>(c->d_blks, sp, c->lay.ld, u, ff);
+  return cudaGetLastError();
+}
+
+cudaError_t forcing_add(cns_ctx* c, int l, const double* u, const double* ff, double* out) {
+  const Space sp = c->cells.view(l - 1);
+  if (sp.ntiles > 0)
+    k_forcing_add<<<sp.ntiles, kTile, 0, c->st>>>(c->d_blks, sp, c->lay.ld, u, ff, out);
+  return cudaGetLastError();
 }
 
 // the HLLC viscous halves (sch_hllc with the stresses), allocated when the
@@ -986,15 +1143,29 @@ int cns_boundary_geom(cns_ctx* c, double* nxn, double* nyn, double* nzn,
 int cns_zpres(cns_ctx* c, int l, const double* v, double* ps, double* temp,
               double* cson) {
   if (!c || bad_block(c, l) || !v || !ps || !temp || !cson) return CNS_EINVAL;
-  CK(launch_zpres(c->d_blks, c->cells.view(l - 1), c->ph, 0, v, c->lay.ld, ps, temp,
-                  cson, nullptr, c->w.status, c->st));
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dv = sg.in(v, 5 * ld);
+  double* dps = sg.inout(ps, ld);
+  double* dtemp = sg.inout(temp, ld);
+  double* dcson = sg.inout(cson, ld);
+  CK(sg.err);
+  CK(launch_zpres(c->d_blks, c->cells.view(l - 1), c->ph, 0, dv, ld, dps, dtemp, dcson,
+                  nullptr, c->w.status, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
 int cns_zvismo(cns_ctx* c, int l, double* mu, const double* v, const double* temp) {
   (void)v;
   if (!c || bad_block(c, l) || !mu || !temp) return CNS_EINVAL;
-  CK(launch_zvismo(c->d_blks, c->cells.view(l - 1), c->ph, mu, temp, c->w.status, c->st));
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  double* dmu = sg.inout(mu, ld);
+  const double* dtemp = sg.in(temp, ld);
+  CK(sg.err);
+  CK(launch_zvismo(c->d_blks, c->cells.view(l - 1), c->ph, dmu, dtemp, c->w.status, c->st));
+  CK(sg.finish());
   return check_status(c);
 }
 
@@ -1006,99 +1177,188 @@ int cns_chrono_global(cns_ctx* c, double* dt) {
   return check_status(c);
 }
 
-int cns_chronos(cns_ctx* c, int l, const double* mu, const double* mut,
-                const double* v, double* dt, const double* sn, const double* vol,
-                const double* cson) {
-  if (!c || bad_block(c, l) || !v || !dt || !sn || !vol || !cson) return CNS_EINVAL;
-  if (c->sc.ns && (!mu || !mut)) return CNS_EINVAL;
+int cns_chronos(cns_ctx* c, int l, double etal, const double* mu, const double* mut,
+                const double* t, double* dt, const char* equat, const double* sn,
+                int64_t lgsnlt, const double* vol, double* sfsi, double* sfsj, double* sfsk,
+                double* dism, const double* cson) {
+  (void)sfsi;
+  (void)sfsj;
+  (void)sfsk;
+  (void)dism;
+  if (!c || bad_block(c, l) || !t || !dt || !sn || !vol || !cson) return CNS_EINVAL;
+  if (!equat_ok(equat)) return fail(c, CNS_EINVAL, "equat: only 'eu3d' / 'ns3d' forms");
+  if (!sn_slice_ok(c, l, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(l)");
+  const int ns = equat[0] == 'n';
+  if (ns && (!mu || !mut)) return CNS_EINVAL;
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dmu = sg.in(mu, ld);
+  const double* dmut = sg.in(mut, ld);
+  const double* dv = sg.in(t, 5 * ld);
+  double* ddt = sg.inout(dt, ld);
+  const double* dsn = sg.in(sn, sn_elems(c, l));
+  const double* dvol = sg.in(vol, ld);
+  const double* dcson = sg.in(cson, ld);
+  CK(sg.err);
   // chronos.f90:138-141 zeroes dt from cell (1,1,1) to cell (ni,nj,nk)
   const int b0 = l == 0 ? 0 : l - 1, b1 = l == 0 ? (int)c->lay.blks.size() : l;
+  bool same_eta = true;
   for (int b = b0; b < b1; ++b) {
     const Blk& B = c->lay.blks[b];
     const long long n1 = B.npc + 1 + B.nid + B.nijd;
     const long long n2 = B.npc + B.ni + (long long)B.nj * B.nid + (long long)B.nk * B.nijd;
-    CK(cudaMemsetAsync(dt + n1, 0, sizeof(double) * (n2 - n1 + 1), c->st));
+    CK(cudaMemsetAsync(ddt + n1, 0, sizeof(double) * (n2 - n1 + 1), c->st));
+    same_eta = same_eta && B.eta == etal;
   }
-  CK(launch_chronos(c->d_blks, c->cells.view(l - 1), c->ph, c->sc, mu, mut, v,
-                    c->lay.ld, dt, sn, vol, cson, c->st));
+  // the kernels read eta(lm) from the block table: the call's etal for this
+  // launch, the context's values again after it
+  std::vector<Blk> tmp;
+  if (!same_eta) {
+    tmp = c->lay.blks;
+    for (int b = b0; b < b1; ++b) tmp[b].eta = etal;
+    CK(cudaMemcpyAsync(c->d_blks, tmp.data(), sizeof(Blk) * tmp.size(),
+                       cudaMemcpyHostToDevice, c->st));
+  }
+  Scheme sc = c->sc;
+  sc.ns = ns;
+  cudaError_t e = launch_chronos(c->d_blks, c->cells.view(l - 1), c->ph, sc, dmu, dmut, dv, ld,
+                                 ddt, sn_base(c, l, dsn), dvol, dcson, c->st);
+  if (!same_eta) {
+    const cudaError_t e2 = cudaMemcpyAsync(c->d_blks, c->lay.blks.data(),
+                                           sizeof(Blk) * c->lay.blks.size(),
+                                           cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);  // tmp stays alive until then
+  }
+  CK(e);
+  CK(sg.finish());
   return CNS_OK;
 }
 
 int cns_rbord(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
   if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
   if (!c->metric_done) return fail(c, CNS_ENOTREADY, "cns_metric has not run");
-  CK(launch_rbord(c->bd, c->ph, v, c->lay.ld, ps, temp, cson, c->n_idd_ent, c->d_idd_ents,
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  double* dv = sg.inout(v, 5 * ld);
+  double* dps = sg.inout(ps, ld);
+  double* dtemp = sg.inout(temp, ld);
+  double* dcson = sg.inout(cson, ld);
+  CK(sg.err);
+  CK(launch_rbord(c->bd, c->ph, dv, ld, dps, dtemp, dcson, c->n_idd_ent, c->d_idd_ents,
                   c->d_idd_masks, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
-int cns_sch_roe_euler(cns_ctx* c, int l, double* u, const double* v,
-                      const double* sn, const double* ps) {
+// the flux routines (sch_roe.f90, sch_roe_euler.f90, sch_hllc*.f90,
+// sch_rusanov.f90, sch_ausmp.f90): u zeroed over the block(s), the residual
+// of the family ischema accumulated; ityprk != 0 then forms the forcing
+// function ff -= u on the real cells (sch_roe.f90:1466-1481).  tau9: the
+// nine stress and heat-flux arrays, or NULL for the Euler routines.
+static int flux_entry(cns_ctx* c, int l, int ityprk, int ischema, int ns, double* u,
+                      const double* v, double* ff, const double* const* tau9,
+                      const char* equat, const double* sn, int64_t lgsnlt, const double* ps) {
   if (!c || bad_block(c, l) || !u || !v || !sn || !ps) return CNS_EINVAL;
-  const Scheme keep = c->sc;
-  c->sc.ns = 0;
-  c->sc.ischema = 7;
-  CK(zero_cols(c, u, 5, l));
-  cudaError_t e = prim_of(c, l, v);
-  if (e == cudaSuccess) e = residual(c, l - 1, u, v, nullptr, sn, ps);
-  c->sc = keep;
-  CK(e);
-  return CNS_OK;
-}
-
-int cns_sch_roe(cns_ctx* c, int l, double* u, const double* v, const double* tau,
-                const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
-  const Scheme keep = c->sc;
-  c->sc.ns = 1;
-  c->sc.ischema = 7;
-  CK(zero_cols(c, u, 5, l));
-  cudaError_t e = prim_of(c, l, v);
-  if (e == cudaSuccess) e = residual(c, l - 1, u, v, tau, sn, ps);
-  c->sc = keep;
-  CK(e);
-  return CNS_OK;
-}
-
-// one block's residual with the flux family ischema (ns: the equations'
-// form, Rusanov always with the stresses)
-static int other_family(cns_ctx* c, int l, int ischema, int ns, double* u, const double* v,
-                 const double* tau, const double* sn, const double* ps) {
+  if (!equat_ok(equat)) return fail(c, CNS_EINVAL, "equat: only 'eu3d' / 'ns3d' forms");
+  if (!sn_slice_ok(c, l, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(lm)");
+  if (ityprk != 0 && !ff) return fail(c, CNS_EINVAL, "ityprk != 0 needs ff");
+  if (tau9)
+    for (int a = 0; a < 9; ++a)
+      if (!tau9[a]) return CNS_EINVAL;
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  double* du = sg.inout(u, 5 * ld);
+  const double* dv = sg.in(v, 5 * ld);
+  double* dff = ityprk ? sg.inout(ff, 5 * ld) : nullptr;
+  const double* dsn = sg.in(sn, sn_elems(c, l));
+  const double* dps = sg.in(ps, ld);
+  CK(sg.err);
+  const double* dtau = nullptr;
+  if (tau9) CK(tau_view(c, sg, tau9, &dtau));
   const Scheme keep = c->sc;
   c->sc.ns = ns;
   c->sc.ischema = ischema;
   cudaError_t e = ensure_hllc_v(c);
-  if (e == cudaSuccess) e = zero_cols(c, u, 5, l);
-  if (e == cudaSuccess) e = prim_of(c, l, v);
-  if (e == cudaSuccess) e = residual(c, l - 1, u, v, tau, sn, ps);
+  if (e == cudaSuccess) e = zero_cols(c, du, 5, l);
+  if (e == cudaSuccess) e = prim_of(c, l, dv);
+  if (e == cudaSuccess) e = residual(c, l - 1, du, dv, dtau, sn_base(c, l, dsn), dps);
+  if (e == cudaSuccess && ityprk != 0) e = forcing_sub(c, l, du, dff);
   c->sc = keep;
   CK(e);
+  CK(sg.finish());
   return CNS_OK;
 }
 
-int cns_sch_hllc_euler(cns_ctx* c, int l, double* u, const double* v, const double* sn,
+#define CNS_TAU9 toxx, toxy, toxz, toyy, toyz, tozz, qcx, qcy, qcz
+#define CNS_TAU9_ARGS                                                                     \
+  const double *toxx, const double *toxy, const double *toxz, const double *toyy,         \
+      const double *toyz, const double *tozz, const double *qcx, const double *qcy,       \
+      const double *qcz
+#define CNS_MUSCL_WORK                                                                    \
+  double *rhol, double *ul, double *vl, double *wl, double *pl, double *rhor, double *ur,  \
+      double *vr, double *wr, double *prr
+
+int cns_sch_roe_euler(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                      const char* equat, const double* sn, int64_t lgsnlt, CNS_MUSCL_WORK,
+                      const double* ps) {
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  return flux_entry(c, lm, ityprk, 7, 0, u, v, ff, nullptr, equat, sn, lgsnlt, ps);
+}
+
+int cns_sch_roe(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                CNS_TAU9_ARGS, const char* equat, const double* sn, int64_t lgsnlt,
+                CNS_MUSCL_WORK, const double* ps) {
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  const double* t9[9] = {CNS_TAU9};
+  return flux_entry(c, lm, ityprk, 7, 1, u, v, ff, t9, equat, sn, lgsnlt, ps);
+}
+
+int cns_sch_hllc_euler(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                       const char* equat, const double* sn, int64_t lgsnlt, CNS_MUSCL_WORK,
                        const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !sn || !ps) return CNS_EINVAL;
-  return other_family(c, l, 14, 0, u, v, nullptr, sn, ps);
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  return flux_entry(c, lm, ityprk, 14, 0, u, v, ff, nullptr, equat, sn, lgsnlt, ps);
 }
 
-int cns_sch_hllc(cns_ctx* c, int l, double* u, const double* v, const double* tau,
-                 const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
-  return other_family(c, l, 14, 1, u, v, tau, sn, ps);
+int cns_sch_hllc(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                 CNS_TAU9_ARGS, const char* equat, const double* sn, int64_t lgsnlt,
+                 CNS_MUSCL_WORK, const double* ps) {
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  const double* t9[9] = {CNS_TAU9};
+  return flux_entry(c, lm, ityprk, 14, 1, u, v, ff, t9, equat, sn, lgsnlt, ps);
 }
 
-int cns_sch_ausmp(cns_ctx* c, int l, double* u, const double* v, const double* tau,
-                  const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
-  return other_family(c, l, 5, 1, u, v, tau, sn, ps);
+int cns_sch_rusanov(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                    CNS_TAU9_ARGS, const char* equat, const double* sn, int64_t lgsnlt,
+                    CNS_MUSCL_WORK, const double* ps) {
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  // sch_rusanov.f90 reads the stresses whatever the equations (zero for Euler)
+  const double* t9[9] = {CNS_TAU9};
+  return flux_entry(c, lm, ityprk, 9, equat && equat[0] == 'n', u, v, ff, t9, equat, sn,
+                    lgsnlt, ps);
 }
 
-int cns_sch_rusanov(cns_ctx* c, int l, double* u, const double* v, const double* tau,
-                    const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !tau || !sn || !ps) return CNS_EINVAL;
-  return other_family(c, l, 9, c->sc.ns, u, v, tau, sn, ps);
+int cns_sch_ausmp(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* d,
+                  double* ff, CNS_TAU9_ARGS, const char* equat, const double* sn,
+                  int64_t lgsnlt, CNS_MUSCL_WORK, const double* ps) {
+  (void)d;  // in the argument list of sch_ausmp.f90:4-11; not read by the flux
+  (void)rhol, (void)ul, (void)vl, (void)wl, (void)pl, (void)rhor, (void)ur, (void)vr, (void)wr,
+      (void)prr;
+  const double* t9[9] = {CNS_TAU9};
+  return flux_entry(c, lm, ityprk, 5, 1, u, v, ff, t9, equat, sn, lgsnlt, ps);
 }
+
+
+
+
+
+
 
 int cns_rfve(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
   if (!c || !v || !ps || !temp || !cson) return CNS_EINVAL;
@@ -1112,23 +1372,62 @@ int cns_rfvc(cns_ctx* c, double* v, double* ps, double* temp, double* cson) {
   return CNS_OK;
 }
 
-int cns_dissip_jameson(cns_ctx* c, int l, const double* v, double* d, const double* sn,
-                       const double* ps, const double* cson) {
-  if (!c || bad_block(c, l) || !v || !d || !sn || !ps || !cson) return CNS_EINVAL;
-  CK(zero_cols(c, d, 5, l));
-  CK(launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, v, c->lay.ld,
-                           ps, cson, sn, c->w.G, d, c->st));
+int cns_dissip_jameson(cns_ctx* c, int lm, const double* v, double* d, const char* equat,
+                       const double* sn, int64_t lgsnlt, double* snu, const double* ps,
+                       const double* cson) {
+  (void)snu;  // the sensor is evaluated inline from the pressures along the line
+  if (!c || bad_block(c, lm) || !v || !d || !sn || !ps || !cson) return CNS_EINVAL;
+  if (!equat_ok(equat)) return fail(c, CNS_EINVAL, "equat: only 'eu3d' / 'ns3d' forms");
+  if (!sn_slice_ok(c, lm, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(lm)");
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dv = sg.in(v, 5 * ld);
+  double* dd = sg.inout(d, 5 * ld);
+  const double* dsn = sg.in(sn, sn_elems(c, lm));
+  const double* dps = sg.in(ps, ld);
+  const double* dcson = sg.in(cson, ld);
+  CK(sg.err);
+  CK(zero_cols(c, dd, 5, lm));
+  CK(launch_dissip_jameson(c->d_blks, c->faces, c->cells.view(lm - 1), lm - 1, dv, ld, dps,
+                           dcson, sn_base(c, lm, dsn), c->w.G, dd, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
-int cns_sch_jameson(cns_ctx* c, int l, double* u, const double* v, const double* d,
-                    const double* tau, const double* sn, const double* ps) {
-  if (!c || bad_block(c, l) || !u || !v || !d || !sn || !ps || (c->sc.ns && !tau))
-    return CNS_EINVAL;
-  CK(zero_cols(c, u, 5, l));
-  CK(launch_sch_jameson(c->d_blks, c->faces, c->cells.view(l - 1), l - 1, c->sc.ns,
-                        c->ph.pinfl, v, c->lay.ld, ps, tau, sn, d, c->w.G, u, nullptr,
+int cns_sch_jameson(cns_ctx* c, int lm, int ityprk, double* u, const double* v,
+                    const double* d, double* ff, CNS_TAU9_ARGS, const char* equat,
+                    const double* sn, int64_t lgsnlt, double* fxx, double* fyy, double* fzz,
+                    double* fxy, double* fxz, double* fyz, double* fex, double* fey,
+                    double* fez, const double* ps) {
+  (void)fxx, (void)fyy, (void)fzz, (void)fxy, (void)fxz, (void)fyz, (void)fex, (void)fey,
+      (void)fez;  // the reference's flux-density work arrays: fluxes are formed per face
+  if (!c || bad_block(c, lm) || !u || !v || !d || !sn || !ps) return CNS_EINVAL;
+  if (!equat_ok(equat)) return fail(c, CNS_EINVAL, "equat: only 'eu3d' / 'ns3d' forms");
+  if (!sn_slice_ok(c, lm, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(lm)");
+  if (ityprk != 0 && !ff) return fail(c, CNS_EINVAL, "ityprk != 0 needs ff");
+  const int ns = equat[0] == 'n';  // sch_jameson.f90:85
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  double* du = sg.inout(u, 5 * ld);
+  const double* dv = sg.in(v, 5 * ld);
+  const double* dd = sg.in(d, 5 * ld);
+  double* dff = ityprk ? sg.inout(ff, 5 * ld) : nullptr;
+  const double* dsn = sg.in(sn, sn_elems(c, lm));
+  const double* dps = sg.in(ps, ld);
+  CK(sg.err);
+  const double* dtau = nullptr;
+  if (ns) {
+    const double* t9[9] = {CNS_TAU9};
+    for (int a = 0; a < 9; ++a)
+      if (!t9[a]) return CNS_EINVAL;
+    CK(tau_view(c, sg, t9, &dtau));
+  }
+  CK(zero_cols(c, du, 5, lm));
+  CK(launch_sch_jameson(c->d_blks, c->faces, c->cells.view(lm - 1), lm - 1, ns, c->ph.pinfl,
+                        dv, ld, dps, dtau, sn_base(c, lm, dsn), dd, c->w.G, du, nullptr,
                         c->st));
+  if (ityprk != 0) CK(forcing_sub(c, lm, du, dff));
+  CK(sg.finish());
   return CNS_OK;
 }
 
@@ -1142,18 +1441,30 @@ int cns_set_turbulence(cns_ctx* c, double alfak, double alfae, double sigma, dou
 }
 
 
-int cns_met_fludc(cns_ctx* c, int l, const double* mu, const double* mut, double* fd5x,
-                  double* fd5y, double* fd5z, double* fd6x, double* fd6y, double* fd6z) {
+int cns_met_fludc(cns_ctx* c, int l, const double* s, const double* mu, const double* mut,
+                  const double* t, const double* dtdx, const double* dtdy, const double* dtdz,
+                  double* fd5x, double* fd5y, double* fd5z, double* fd6x, double* fd6y,
+                  double* fd6z) {
+  // s, t and the temperature gradients are in the argument list of
+  // met_fludc.f90:4-8; the routine only scales the diffusion densities
+  (void)s, (void)t, (void)dtdx, (void)dtdy, (void)dtdz;
   if (!c || bad_block(c, l) || !mu || !mut || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y ||
       !fd6z)
     return CNS_EINVAL;
-  double* const fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dmu = sg.in(mu, ld);
+  const double* dmut = sg.in(mut, ld);
+  double* const fd[6] = {sg.inout(fd5x, ld), sg.inout(fd5y, ld), sg.inout(fd5z, ld),
+                         sg.inout(fd6x, ld), sg.inout(fd6y, ld), sg.inout(fd6z, ld)};
+  CK(sg.err);
   const int l0 = l == 0 ? 1 : l, l1 = l == 0 ? (int)c->lay.blks.size() : l;
   for (int b = l0; b <= l1; ++b) {
     long long n0, n1;
     fludc_range(c, b, n0, n1);
-    CK(launch_fludc(n0, n1, mu, mut, fd, c->alfak, c->alfae, c->st));
+    CK(launch_fludc(n0, n1, dmu, dmut, fd, c->alfak, c->alfae, c->st));
   }
+  CK(sg.finish());
   return CNS_OK;
 }
 
@@ -1161,27 +1472,49 @@ int cns_met_fludcsa(cns_ctx* c, int l, const double* s, const double* mu, double
                     double* fd5y, double* fd5z, double* fd6x, double* fd6y, double* fd6z) {
   if (!c || bad_block(c, l) || !s || !mu || !fd5x || !fd5y || !fd5z || !fd6x || !fd6y || !fd6z)
     return CNS_EINVAL;
-  double* const fd[6] = {fd5x, fd5y, fd5z, fd6x, fd6y, fd6z};
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* ds = sg.in(s, 7 * ld);
+  const double* dmu = sg.in(mu, ld);
+  double* const fd[6] = {sg.inout(fd5x, ld), sg.inout(fd5y, ld), sg.inout(fd5z, ld),
+                         sg.inout(fd6x, ld), sg.inout(fd6y, ld), sg.inout(fd6z, ld)};
+  CK(sg.err);
   const int l0 = l == 0 ? 1 : l, l1 = l == 0 ? (int)c->lay.blks.size() : l;
   for (int b = l0; b <= l1; ++b) {
     long long n0, n1;
     fludc_range(c, b, n0, n1);
-    CK(launch_fludcsa(n0, n1, s + 5 * c->lay.ld, mu, fd, c->sigma, c->st));
+    CK(launch_fludcsa(n0, n1, ds + 5 * ld, dmu, fd, c->sigma, c->st));
   }
+  CK(sg.finish());
   return CNS_OK;
 }
 
 static int met_roe2o_common(cns_ctx* c, int l, const double* t, double* d, const double* sn,
-                            int harten) {
+                            int64_t lgsnlt, int harten) {
   if (!c || bad_block(c, l) || !t || !d || !sn) return CNS_EINVAL;
+  if (!sn_slice_ok(c, l, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(l)");
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dt7 = sg.in(t, 7 * ld);
+  double* dd = sg.inout(d, 7 * ld);
+  const double* dsn = sg.in(sn, sn_elems(c, l));
+  CK(sg.err);
   CK(launch_roe2o(c->d_blks, c->faces, c->cells_ext.view(l - 1), l - 1, harten, c->epsroe,
-                  c->ph.gam, c->ph.gam1, t, c->lay.ld, sn, c->w.G, d, c->st));
+                  c->ph.gam, c->ph.gam1, dt7, ld, sn_base(c, l, dsn), c->w.G, dd, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
 int cns_met_samut(cns_ctx* c, int l, const double* v, const double* mu, double* mut) {
   if (!c || bad_block(c, l) || !v || !mu || !mut) return CNS_EINVAL;
-  CK(launch_samut(c->d_blks, c->cells.view(l - 1), v + 5 * c->lay.ld, mu, mut, c->st));
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dv = sg.in(v, 7 * ld);
+  const double* dmu = sg.in(mu, ld);
+  double* dmut = sg.inout(mut, ld);
+  CK(sg.err);
+  CK(launch_samut(c->d_blks, c->cells.view(l - 1), dv + 5 * ld, dmu, dmut, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
@@ -1255,12 +1588,16 @@ int cns_impli2_eqt_3d(cns_ctx* c, int l, const double* u, const double* dt, doub
   return CNS_OK;
 }
 
-int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
-  return met_roe2o_common(c, l, t, d, sn, 0);
+int cns_met_roe2o(cns_ctx* c, int l, const double* t, double* d, const double* sn,
+                  int64_t lgsnlt, const double* vol, double* del6, double* del7) {
+  (void)vol, (void)del6, (void)del7;  // met_roe2o.f90:4-7's volume and slope work arrays
+  return met_roe2o_common(c, l, t, d, sn, lgsnlt, 0);
 }
 
-int cns_met_roe2oh(cns_ctx* c, int l, const double* t, double* d, const double* sn) {
-  return met_roe2o_common(c, l, t, d, sn, 1);
+int cns_met_roe2oh(cns_ctx* c, int l, const double* t, double* d, const double* sn,
+                   int64_t lgsnlt, const double* vol, double* del6, double* del7) {
+  (void)vol, (void)del6, (void)del7;
+  return met_roe2o_common(c, l, t, d, sn, lgsnlt, 1);
 }
 
 int cns_atcaldis3(cns_ctx* c, const double* x, const double* y, const double* z,
@@ -1426,48 +1763,107 @@ int cns_zvisqc(cns_ctx* c, const double* v, const double* mu, const double* mut,
                double* tau, const double* sn, const double* vol,
                const double* temp) {
   if (!c || !v || !mu || !mut || !tau || !sn || !vol || !temp) return CNS_EINVAL;
-  CK(prim_of(c, 0, v));
-  CK(launch_grad(c->d_blks, c->cells.view(-1), c->ph, v, c->w.prim, c->lay.ld, mu, mut, tau,
-                 sn, vol, temp, c->st));
-  CK(launch_tau_ghosts(c->bd, tau, c->lay.ld, c->st));
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* dv = sg.in(v, 5 * ld);
+  const double* dmu = sg.in(mu, ld);
+  const double* dmut = sg.in(mut, ld);
+  double* dtau = sg.inout(tau, 9 * ld);
+  const double* dsn = sg.in(sn, 9 * ld);
+  const double* dvol = sg.in(vol, ld);
+  const double* dtemp = sg.in(temp, ld);
+  CK(sg.err);
+  CK(prim_of(c, 0, dv));
+  CK(launch_grad(c->d_blks, c->cells.view(-1), c->ph, dv, c->w.prim, ld, dmu, dmut, dtau, dsn,
+                 dvol, dtemp, c->st));
+  CK(launch_tau_ghosts(c->bd, dtau, ld, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
-static int implimf(cns_ctx* c, int l, int eu, const double* u, const double* dt,
-                   double* v, double* d, const double* mu, const double* mut,
-                   const double* sn, const double* vol, const double* ps,
-                   const double* cson, int lmx) {
-  if (lmx < 0) return CNS_EINVAL;
-  CK(zero_cols(c, d, 5, l));
-  CK(prim_of(c, l, v));
+// implimf_3d.f90 / implimf_eu.f90 on block(s) l: d zeroed, lmax point-Jacobi
+// sweeps, v += d.  ityprk != 0: right-hand side -u - ff; dtpas: the
+// physical step of the dual-time diagonal term when kfmg = 3.
+static int implimf(cns_ctx* c, int l, int eu, const double* u, const double* dt, double* v,
+                   double* d, const double* ff, const double* mu, const double* mut,
+                   const char* equat, int lmx, const double* sn, int64_t lgsnlt,
+                   const double* vol, double dtpas, int ityprk, const double* ps,
+                   const double* cson) {
+  if (!c || bad_block(c, l) || !u || !dt || !v || !d || !sn || !vol || !ps || !cson ||
+      lmx < 0)
+    return CNS_EINVAL;
+  if (!eu && (!mu || !mut)) return CNS_EINVAL;
+  if (!equat_ok(equat)) return fail(c, CNS_EINVAL, "equat: only 'eu3d' / 'ns3d' forms");
+  if (!sn_slice_ok(c, l, lgsnlt)) return fail(c, CNS_EINVAL, "lgsnlt must be nnn(lm)");
+  if (ityprk != 0 && !ff) return fail(c, CNS_EINVAL, "ityprk != 0 needs ff");
+  if (c->sc.kfmg == 3 && !(dtpas > 0.)) return fail(c, CNS_EINVAL, "kfmg = 3 needs dtpas > 0");
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* du = sg.in(u, 5 * ld);
+  const double* ddt = sg.in(dt, ld);
+  double* dv = sg.inout(v, 5 * ld);
+  double* dd = sg.inout(d, 5 * ld);
+  const double* dff = ityprk ? sg.in(ff, 5 * ld) : nullptr;
+  const double* dmu = eu ? nullptr : sg.in(mu, ld);
+  const double* dmut = eu ? nullptr : sg.in(mut, ld);
+  const double* dsn = sg.in(sn, sn_elems(c, l));
+  const double* dvol = sg.in(vol, ld);
+  const double* dps = sg.in(ps, ld);
+  const double* dcson = sg.in(cson, ld);
+  CK(sg.err);
+  if (ityprk != 0) {
+    if (!c->u_forced) CK(dev_alloc(c, &c->u_forced, (size_t)(5 * ld)));
+    CK(forcing_add(c, l, du, dff, c->u_forced));
+    du = c->u_forced;
+  }
+  CK(zero_cols(c, dd, 5, l));
+  CK(prim_of(c, l, dv));
+  Scheme sc = c->sc;
+  if (sc.kfmg == 3) sc.dt1min = dtpas;
   CK(launch_implicit(c->d_blks, c->cells.view(l - 1), c->tiles64.view(l - 1), c->faces, l - 1,
-                     c->ph, c->sc, eu,
-                     lmx, u, dt, v, d, mu, mut, sn, vol, ps, cson, c->w, 0, c->st));
+                     c->ph, sc, eu, lmx, du, ddt, dv, dd, dmu, dmut, sn_base(c, l, dsn), dvol,
+                     dps, dcson, c->w, 0, c->st));
+  CK(sg.finish());
   return CNS_OK;
 }
 
-int cns_implimf_eu(cns_ctx* c, int l, const double* u, const double* dt, double* v,
-                   double* d, const double* sn, const double* vol, const double* ps,
-                   const double* cson, int lmx) {
-  if (!c || bad_block(c, l) || !u || !dt || !v || !d || !sn || !vol || !ps || !cson)
-    return CNS_EINVAL;
-  return implimf(c, l, 1, u, dt, v, d, nullptr, nullptr, sn, vol, ps, cson, lmx);
+#define CNS_DF9                                                                           \
+  double *dfxx, double *dfyy, double *dfzz, double *dfxy, double *dfxz, double *dfyz,     \
+      double *dfex, double *dfey, double *dfez
+int cns_implimf_eu(cns_ctx* c, int lm, const double* u, const double* dt, double* v,
+                   double* d, const double* ff, const char* equat, int lmx, const double* sn,
+                   int64_t lgsnlt, const double* vol, double dtpas, int ityprk, CNS_DF9,
+                   double* coefdiag, const double* ps, const double* cson) {
+  // the stored flux increments and the diagonal are recomputed on the device
+  (void)dfxx, (void)dfyy, (void)dfzz, (void)dfxy, (void)dfxz, (void)dfyz, (void)dfex,
+      (void)dfey, (void)dfez, (void)coefdiag;
+  return implimf(c, lm, 1, u, dt, v, d, ff, nullptr, nullptr, equat, lmx, sn, lgsnlt, vol,
+                 dtpas, ityprk, ps, cson);
 }
 
-int cns_implimf_3d(cns_ctx* c, int l, const double* u, const double* dt, double* v,
-                   double* d, const double* mu, const double* mut, const double* sn,
-                   const double* vol, const double* ps, const double* cson, int lmx) {
-  if (!c || bad_block(c, l) || !u || !dt || !v || !d || !mu || !mut || !sn || !vol ||
-      !ps || !cson)
-    return CNS_EINVAL;
-  return implimf(c, l, 0, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx);
+int cns_implimf_3d(cns_ctx* c, int lm, const double* u, const double* dt, double* v,
+                   double* d, const double* ff, const double* mu, const double* mut,
+                   const char* equat, int lmx, const double* sn, int64_t lgsnlt,
+                   const double* vol, double dtpas, int ityprk, CNS_DF9, double* rv,
+                   const double* ps, const double* cson) {
+  (void)dfxx, (void)dfyy, (void)dfzz, (void)dfxy, (void)dfxz, (void)dfyz, (void)dfex,
+      (void)dfey, (void)dfez, (void)rv;
+  return implimf(c, lm, 0, u, dt, v, d, ff, mu, mut, equat, lmx, sn, lgsnlt, vol, dtpas,
+                 ityprk, ps, cson);
 }
+
+
 
 int cns_rscpsv(cns_ctx* c, const double* u0, const double* v, const double* dt,
                double* norms) {
   if (!c || !u0 || !v || !dt || !norms) return CNS_EINVAL;
-  CK(launch_norm_partials(c->d_blks, c->cells.view(-1), c->lay.ld, u0, v, dt,
-                          c->w.normpart, c->st));
+  const long long ld = c->lay.ld;
+  Staging sg(c);
+  const double* du0 = sg.in(u0, 5 * ld);
+  const double* dv = sg.in(v, 5 * ld);
+  const double* ddt = sg.in(dt, ld);
+  CK(sg.err);
+  CK(launch_norm_partials(c->d_blks, c->cells.view(-1), ld, du0, dv, ddt, c->w.normpart, c->st));
   CK(launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
                           c->w.normpart, c->w.blocksum, c->w.norms, c->st));
   CK(cudaMemcpyAsync(c->h_norms, c->w.norms, 15 * sizeof(double), cudaMemcpyDeviceToHost,

@@ -14,6 +14,7 @@
 #include <math_constants.h>
 
 #include "cns_kernels.cuh"
+#include "cns_pmath.h"
 #include "cns_hot.cuh"
 
 namespace cns {
@@ -264,7 +265,7 @@ __device__ __forceinline__ double idd_sweep(const Phys& ph, IddCell& c) {
   const double gamt = ph.gam / sq(ph.aa1);
   const double gam2t = 0.5 * ph.gam1 / sq(ph.aa1);
   const double b = 1. / (1. + gam2t / c.rti * c.usdn2 * sq(c.qn + c.un));
-  const double p = ph.pa1 * c.rpi * pow(b, gam6);
+  const double p = ph.pa1 * c.rpi * cns_pow(b, gam6);
   const double ro = gamt * p / (b * c.rti);
   const double f = p + c.roc0 * c.qn - c.am0;
   const double df = c.roc0 - ro * (c.qn + c.un) * c.usdn2;
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(256) k_clidd_apply(Bnd bd, Phys ph, const long
                d0z = bd.bceqt[4 * nl + e];
   const double ym = bd.ym[e], zm = bd.zm[e];
   const double b = 1. / (1. + gam2t / c.rti * c.usdn2 * sq(c.qn + c.un));
-  const double p = ph.pa1 * c.rpi * pow(b, gam6);
+  const double p = ph.pa1 * c.rpi * cns_pow(b, gam6);
   const double ro = gamt * p / (b * c.rti);
   const double wn = c.qn + c.un;
   const double w = wn * c.usdn;

@@ -12,6 +12,7 @@
 // FP64, --fmad=false: bit-identical gradients.  The source uses exp and a
 // real power, whose last bit may differ from the host libm's.
 #include "cns_kernels.cuh"
+#include "cns_pmath.h"
 
 namespace cns {
 
@@ -165,11 +166,11 @@ __global__ void __launch_bounds__(kTile) k_smsa(
     rtilde = fmin(rtilde, 1.);
   }
   const double rtil6 = pow6(rtilde);
-  const double ft2 = kCt3 * exp(-kCt4 * xkhi2);
+  const double ft2 = kCt3 * cns_exp(-kCt4 * xkhi2);
   const double sm1 = kCb1 * (1. - ft2) * stilde * v6;
   const double xg = rtilde + kCw2 * (rtil6 - rtilde);
   const double xg6 = pow6(xg);
-  const double fw = xg * pow((1. + cw36) / (xg6 + cw36), uns6);
+  const double fw = xg * cns_pow((1. + cw36) / (xg6 + cw36), uns6);
   const double sm2 = -(cw1 * fw - kCb1 * ft2 / kappa2) * v6 * nutilde / dist2;
   ts6[n] = sm1 + sm2 + sdif;
   ts7[n] = 0.;

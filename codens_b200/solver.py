@@ -42,6 +42,22 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+def _arr(a):
+    """a device tensor or a host numpy array (the copy-in/out parity mode of
+    the per-routine entry points) as a pointer"""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("host arrays must be contiguous float64")
+        return C.c_void_p(a.ctypes.data)
+    return _ptr(a)
+
+
+def _offset(p, elems: int):
+    return None if p is None else C.c_void_p(p.value + 8 * elems)
+
+
 def _check_ke(equat: str, v, ld: int):
     if equat.ljust(7)[5:7] == "ke" and v.numel() < 7 * ld:
         raise ValueError("equat 'ke' reads and writes v(:,6:7): v must be (ld, 7)")
@@ -210,45 +226,83 @@ class CodeNS:
         return [o[: self.nlist] for o in out]
 
     # ---- reference call surface ----------------------------------------
+    # The C entry points take the reference routines' argument lists:
+    # equat, the block's sn slice with lgsnlt = nnn(lm), the nine stress
+    # arrays toxx..qcz, ityprk and ff, work arrays (passed as NULL here).
+    def _equat(self, ns=None) -> bytes:
+        ns = self.case.scheme.ns if ns is None else ns
+        return b"ns3d   " if ns else b"eu3d   "
+
+    def _sn(self, l, sn):
+        """sn(npsn): the block's slice (lm >= 1) or the whole array (lm = 0),
+        and lgsnlt"""
+        if l == 0:
+            return _arr(sn), self.ld
+        b = self.case.layout.blocks[l - 1]
+        return _offset(_arr(sn), 9 * b.npc), b.nnn
+
+    def _tau9(self, tau):
+        base = _arr(tau)
+        if base is None:
+            return [None] * 9
+        return [_offset(base, a * self.ld) for a in range(9)]
+
     def zpres(self, l, v, pression, ztemp, cson):
-        self._check(self.lib.cns_zpres(self.ctx, l, _ptr(v), _ptr(pression), _ptr(ztemp),
-                                       _ptr(cson)), "cns_zpres")
+        self._check(self.lib.cns_zpres(self.ctx, l, _arr(v), _arr(pression), _arr(ztemp),
+                                       _arr(cson)), "cns_zpres")
 
     def zvismo(self, l, mu, v, ztemp):
-        self._check(self.lib.cns_zvismo(self.ctx, l, _ptr(mu), _ptr(v), _ptr(ztemp)),
+        self._check(self.lib.cns_zvismo(self.ctx, l, _arr(mu), _arr(v), _arr(ztemp)),
                     "cns_zvismo")
 
-    def chronos(self, l, mu, mut, v, dt, sn, vol, cson):
-        self._check(self.lib.cns_chronos(self.ctx, l, _ptr(mu), _ptr(mut), _ptr(v), _ptr(dt),
-                                         _ptr(sn), _ptr(vol), _ptr(cson)), "cns_chronos")
+    def chronos(self, l, mu, mut, v, dt, sn, vol, cson, etal=None):
+        """chronos.f90 with the CFL etal (default: the block's eta)"""
+        if etal is None:
+            sc = self.case.scheme
+            etal = sc.eta_l[l - 1] if (sc.eta_l is not None and l >= 1) else sc.eta
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_chronos(self.ctx, l, float(etal), _arr(mu), _arr(mut), _arr(v),
+                                         _arr(dt), self._equat(), snp, lg, _arr(vol), None,
+                                         None, None, None, _arr(cson)), "cns_chronos")
 
     def rbord(self, v, pression, ztemp, cson):
-        self._check(self.lib.cns_rbord(self.ctx, _ptr(v), _ptr(pression), _ptr(ztemp),
-                                       _ptr(cson)), "cns_rbord")
+        self._check(self.lib.cns_rbord(self.ctx, _arr(v), _arr(pression), _arr(ztemp),
+                                       _arr(cson)), "cns_rbord")
 
-    def sch_roe_euler(self, l, u, v, sn, ps):
-        self._check(self.lib.cns_sch_roe_euler(self.ctx, l, _ptr(u), _ptr(v), _ptr(sn),
-                                               _ptr(ps)), "cns_sch_roe_euler")
+    def _flux_euler(self, fn, name, l, u, v, sn, ps, ityprk, ff, equat):
+        snp, lg = self._sn(l, sn)
+        self._check(fn(self.ctx, l, ityprk, _arr(u), _arr(v), _arr(ff), equat or b"eu3d   ",
+                       snp, lg, *([None] * 10), _arr(ps)), name)
 
-    def sch_roe(self, l, u, v, tau, sn, ps):
-        self._check(self.lib.cns_sch_roe(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
-                                         _ptr(ps)), "cns_sch_roe")
+    def _flux_ns(self, fn, name, l, u, v, tau, sn, ps, ityprk, ff, equat, d=()):
+        snp, lg = self._sn(l, sn)
+        dd = [_arr(d[0])] if d else []
+        self._check(fn(self.ctx, l, ityprk, _arr(u), _arr(v), *dd, _arr(ff), *self._tau9(tau),
+                       equat or b"ns3d   ", snp, lg, *([None] * 10), _arr(ps)), name)
 
-    def sch_hllc_euler(self, l, u, v, sn, ps):
-        self._check(self.lib.cns_sch_hllc_euler(self.ctx, l, _ptr(u), _ptr(v), _ptr(sn),
-                                                _ptr(ps)), "cns_sch_hllc_euler")
+    def sch_roe_euler(self, l, u, v, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_euler(self.lib.cns_sch_roe_euler, "cns_sch_roe_euler", l, u, v, sn, ps,
+                         ityprk, ff, equat)
 
-    def sch_hllc(self, l, u, v, tau, sn, ps):
-        self._check(self.lib.cns_sch_hllc(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
-                                          _ptr(ps)), "cns_sch_hllc")
+    def sch_roe(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_ns(self.lib.cns_sch_roe, "cns_sch_roe", l, u, v, tau, sn, ps, ityprk, ff,
+                      equat)
 
-    def sch_rusanov(self, l, u, v, tau, sn, ps):
-        self._check(self.lib.cns_sch_rusanov(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau),
-                                             _ptr(sn), _ptr(ps)), "cns_sch_rusanov")
+    def sch_hllc_euler(self, l, u, v, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_euler(self.lib.cns_sch_hllc_euler, "cns_sch_hllc_euler", l, u, v, sn, ps,
+                         ityprk, ff, equat)
 
-    def sch_ausmp(self, l, u, v, tau, sn, ps):
-        self._check(self.lib.cns_sch_ausmp(self.ctx, l, _ptr(u), _ptr(v), _ptr(tau), _ptr(sn),
-                                           _ptr(ps)), "cns_sch_ausmp")
+    def sch_hllc(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_ns(self.lib.cns_sch_hllc, "cns_sch_hllc", l, u, v, tau, sn, ps, ityprk, ff,
+                      equat)
+
+    def sch_rusanov(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_ns(self.lib.cns_sch_rusanov, "cns_sch_rusanov", l, u, v, tau, sn, ps, ityprk,
+                      ff, equat or self._equat())
+
+    def sch_ausmp(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
+        self._flux_ns(self.lib.cns_sch_ausmp, "cns_sch_ausmp", l, u, v, tau, sn, ps, ityprk, ff,
+                      equat, d=(None,))
 
     def chrono_global(self, dt):
         """chrono.f90:113-151: the global time step (kdtl = 0)"""
@@ -276,12 +330,16 @@ class CodeNS:
                     "cns_rfvc")
 
     def dissip_jameson(self, l, v, d, sn, ps, cson):
-        self._check(self.lib.cns_dissip_jameson(self.ctx, l, _ptr(v), _ptr(d), _ptr(sn),
-                                                _ptr(ps), _ptr(cson)), "cns_dissip_jameson")
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_dissip_jameson(self.ctx, l, _arr(v), _arr(d), self._equat(),
+                                                snp, lg, None, _arr(ps), _arr(cson)),
+                    "cns_dissip_jameson")
 
-    def sch_jameson(self, l, u, v, d, tau, sn, ps):
-        self._check(self.lib.cns_sch_jameson(self.ctx, l, _ptr(u), _ptr(v), _ptr(d), _ptr(tau),
-                                             _ptr(sn), _ptr(ps)), "cns_sch_jameson")
+    def sch_jameson(self, l, u, v, d, tau, sn, ps, ityprk=0, ff=None):
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_sch_jameson(self.ctx, l, ityprk, _arr(u), _arr(v), _arr(d),
+                                             _arr(ff), *self._tau9(tau), self._equat(), snp,
+                                             lg, *([None] * 9), _arr(ps)), "cns_sch_jameson")
 
     # turbulence-transport terms (met_fludc, met_fludcsa, met_roe2o, met_roe2oh)
     def set_turbulence(self, alfak=1.0, alfae=1.3, sigma=2.0 / 3.0, epsroe=0.0):
@@ -289,8 +347,10 @@ class CodeNS:
                     "cns_set_turbulence")
 
     def met_fludc(self, l, mu, mut, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
-        self._check(self.lib.cns_met_fludc(self.ctx, l, *(_ptr(a) for a in (
-            mu, mut, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z))), "cns_met_fludc")
+        self._check(self.lib.cns_met_fludc(self.ctx, l, None, _arr(mu), _arr(mut), None, None,
+                                           None, None, *(_arr(a) for a in (
+                                               fd5x, fd5y, fd5z, fd6x, fd6y, fd6z))),
+                    "cns_met_fludc")
 
     def met_fludcsa(self, l, s, mu, fd5x, fd5y, fd5z, fd6x, fd6y, fd6z):
         self._check(self.lib.cns_met_fludcsa(self.ctx, l, *(_ptr(a) for a in (
@@ -298,7 +358,8 @@ class CodeNS:
 
     def met_roe2o(self, l, t, d, sn, harten=False):
         f = self.lib.cns_met_roe2oh if harten else self.lib.cns_met_roe2o
-        self._check(f(self.ctx, l, _ptr(t), _ptr(d), _ptr(sn)),
+        snp, lg = self._sn(l, sn)
+        self._check(f(self.ctx, l, _arr(t), _arr(d), snp, lg, None, None, None),
                     "cns_met_roe2oh" if harten else "cns_met_roe2o")
 
     def met_samut(self, l, v, mu, mut):
@@ -453,22 +514,32 @@ class CodeNS:
                                         equat.encode(), _ptr(v), _ptr(mut)), "cns_writda")
 
     def zvisqc(self, v, mu, mut, tau, sn, vol, ztemp):
-        self._check(self.lib.cns_zvisqc(self.ctx, _ptr(v), _ptr(mu), _ptr(mut), _ptr(tau),
-                                        _ptr(sn), _ptr(vol), _ptr(ztemp)), "cns_zvisqc")
+        self._check(self.lib.cns_zvisqc(self.ctx, _arr(v), _arr(mu), _arr(mut), _arr(tau),
+                                        _arr(sn), _arr(vol), _arr(ztemp)), "cns_zvisqc")
 
-    def implimf_eu(self, l, u, dt, v, d, sn, vol, ps, cson, lmx):
-        self._check(self.lib.cns_implimf_eu(self.ctx, l, _ptr(u), _ptr(dt), _ptr(v), _ptr(d),
-                                            _ptr(sn), _ptr(vol), _ptr(ps), _ptr(cson), lmx),
-                    "cns_implimf_eu")
+    def _dtpas(self, dtpas):
+        return float(self.case.scheme.dt1min if dtpas is None else dtpas)
 
-    def implimf_3d(self, l, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx):
-        self._check(self.lib.cns_implimf_3d(self.ctx, l, _ptr(u), _ptr(dt), _ptr(v), _ptr(d),
-                                            _ptr(mu), _ptr(mut), _ptr(sn), _ptr(vol), _ptr(ps),
-                                            _ptr(cson), lmx), "cns_implimf_3d")
+    def implimf_eu(self, l, u, dt, v, d, sn, vol, ps, cson, lmx, ityprk=0, ff=None,
+                   dtpas=None):
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_implimf_eu(self.ctx, l, _arr(u), _arr(dt), _arr(v), _arr(d),
+                                            _arr(ff), b"eu3d   ", lmx, snp, lg, _arr(vol),
+                                            self._dtpas(dtpas), ityprk, *([None] * 10),
+                                            _arr(ps), _arr(cson)), "cns_implimf_eu")
+
+    def implimf_3d(self, l, u, dt, v, d, mu, mut, sn, vol, ps, cson, lmx, ityprk=0, ff=None,
+                   dtpas=None):
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_implimf_3d(self.ctx, l, _arr(u), _arr(dt), _arr(v), _arr(d),
+                                            _arr(ff), _arr(mu), _arr(mut), b"ns3d   ", lmx, snp,
+                                            lg, _arr(vol), self._dtpas(dtpas), ityprk,
+                                            *([None] * 10), _arr(ps), _arr(cson)),
+                    "cns_implimf_3d")
 
     def rscpsv(self, u0, v, dt) -> np.ndarray:
         out = (C.c_double * 15)()
-        self._check(self.lib.cns_rscpsv(self.ctx, _ptr(u0), _ptr(v), _ptr(dt), out),
+        self._check(self.lib.cns_rscpsv(self.ctx, _arr(u0), _arr(v), _arr(dt), out),
                     "cns_rscpsv")
         return np.array(out).reshape(3, 5)
 

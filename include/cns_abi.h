@@ -21,8 +21,28 @@
  *     3 components), the area vector of the lower face of each cell oriented
  *     towards increasing index (norm.f90);
  *   - tau is (ld, 9): toxx, toxy, toxz, toyy, toyz, tozz, qcx, qcy, qcz.
- * All array pointers given to kernel entry points are DEVICE pointers on the
- * context's device; the *_host entry points take host pointers.
+ * Per-routine entry points (zpres ... implimf_3d below) take the reference
+ * routine's argument list in its order after the context handle: its
+ * switches (ityprk, equat, lmx, dtpas, etal), its arrays, and its work
+ * arrays (accepted for the drop-in and not used: the device recomputes what
+ * the reference stores in them; they may be NULL).  As in the reference,
+ * sn is the block's slice sn(npsn) with lgsnlt = nnn(lm) (sequence
+ * association, atsch_num.f90:470-479); lm = 0 (every block in one launch, an
+ * extension) takes the whole array with lgsnlt = ld.  equat is the
+ * reference's character*7 (no terminating NUL): the equations 'eu' or 'ns'
+ * in (1:2) and the three-dimensional form '3d' in (3:4); the
+ * two-dimensional forms return CNS_EINVAL.  ityprk != 0 (multigrid forcing)
+ * is honoured as in the reference: the flux routines subtract u from ff on
+ * the real cells, the implicit routines solve with -u - ff.
+ *
+ * Array arguments of the per-routine entry points may be DEVICE pointers on
+ * the context's device (the call only enqueues work on the context stream)
+ * or HOST pointers, the reference's own arrays passed as they are: a host
+ * array is copied to the device before the routine, copied back after it
+ * when the routine writes it, and the call returns when the copies are done
+ * (the copy-in/out parity mode; one call may mix both kinds).  The fast path
+ * (cns_bind_state, cns_atsch_num_step) takes device arrays; the *_host
+ * entry point host arrays.
  *
  * Errors: every function returns 0 on success or a CNS_E* code.  The
  * reference prints and stops instead (zvismo.f90:123-127, chrono.f90:134-142,
@@ -166,10 +186,19 @@ int cns_chrono_global(cns_ctx *ctx, double *dt);
  * with u = 0.5 u - d on the real cells.  l = 0: every block. */
 int cns_rfve(cns_ctx *ctx, double *v, double *pression, double *ztemp, double *cson);
 int cns_rfvc(cns_ctx *ctx, double *v, double *pression, double *ztemp, double *cson);
-int cns_dissip_jameson(cns_ctx *ctx, int l, const double *v, double *d, const double *sn,
-                       const double *pression, const double *cson);
-int cns_sch_jameson(cns_ctx *ctx, int l, double *u, const double *v, const double *d,
-                    const double *tau, const double *sn, const double *pression);
+/* dissip_jameson.f90:4-8 (snu: the sensor work array, not used) */
+int cns_dissip_jameson(cns_ctx *ctx, int lm, const double *v, double *d, const char *equat,
+                       const double *sn, int64_t lgsnlt, double *snu, const double *ps,
+                       const double *cson);
+/* sch_jameson.f90:4-11 (fxx..fez: the flux-density work arrays, not used;
+ * toxx..qcz read when equat(1:2) = 'ns') */
+int cns_sch_jameson(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v,
+                    const double *d, double *ff, const double *toxx, const double *toxy,
+                    const double *toxz, const double *toyy, const double *toyz,
+                    const double *tozz, const double *qcx, const double *qcy,
+                    const double *qcz, const char *equat, const double *sn, int64_t lgsnlt,
+                    double *fxx, double *fyy, double *fzz, double *fxy, double *fxz,
+                    double *fyz, double *fex, double *fey, double *fez, const double *ps);
 
 /* Turbulence-transport terms on the mean-flow path.  cns_set_turbulence
  * sets the modeleturb / schemanum constants these routines read (alfak,
@@ -182,12 +211,19 @@ int cns_sch_jameson(cns_ctx *ctx, int l, double *u, const double *v, const doubl
  *   cns_met_roe2oh  met_roe2oh.f90        the same with Harten's entropy fix
  * l = 0: every block. */
 int cns_set_turbulence(cns_ctx *ctx, double alfak, double alfae, double sigma, double epsroe);
-int cns_met_fludc(cns_ctx *ctx, int l, const double *mu, const double *mut, double *fd5x,
-                  double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
+/* met_fludc.f90:4-8 (s, t, dtdx, dtdy, dtdz: in its argument list, not read) */
+int cns_met_fludc(cns_ctx *ctx, int l, const double *s, const double *mu, const double *mut,
+                  const double *t, const double *dtdx, const double *dtdy,
+                  const double *dtdz, double *fd5x, double *fd5y, double *fd5z,
+                  double *fd6x, double *fd6y, double *fd6z);
+/* met_fludcsa.f90:4-7 */
 int cns_met_fludcsa(cns_ctx *ctx, int l, const double *s, const double *mu, double *fd5x,
                     double *fd5y, double *fd5z, double *fd6x, double *fd6y, double *fd6z);
-int cns_met_roe2o(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
-int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double *sn);
+/* met_roe2o.f90:4-7, met_roe2oh.f90:4-7 (vol, del6, del7: work, not used) */
+int cns_met_roe2o(cns_ctx *ctx, int l, const double *t, double *d, const double *sn,
+                  int64_t lgsnlt, const double *vol, double *del6, double *del7);
+int cns_met_roe2oh(cns_ctx *ctx, int l, const double *t, double *d, const double *sn,
+                   int64_t lgsnlt, const double *vol, double *del6, double *del7);
 /* Spalart-Allmaras (constants of atlecdon.f90:193-204):
  *   cns_met_samut  met_samut.f90:4-58   mut = v(:,6) fv1 on the real cells
  *   cns_sch_turb   sch_turb.f90:4-290   centred fluxes of v(:,6:7) with the
@@ -305,49 +341,91 @@ int cns_zpres(cns_ctx *ctx, int l, const double *v, double *pression,
 /* zvismo.f90:4-136 (iflu = 1) */
 int cns_zvismo(cns_ctx *ctx, int l, double *mu, const double *v,
                const double *ztemp);
-/* chronos.f90:4-213 (kprec = 0) with the scheme's eta */
-int cns_chronos(cns_ctx *ctx, int l, const double *mu, const double *mut,
-                const double *v, double *dt, const double *sn,
-                const double *vol, const double *cson);
+/* chronos.f90:4-11 (kprec = 0): local time step of block l with the CFL
+ * number etal; the viscous limit when equat(1:2) = 'ns'; sfsi, sfsj, sfsk,
+ * dism: work arrays, not used */
+int cns_chronos(cns_ctx *ctx, int l, double etal, const double *mu, const double *mut,
+                const double *t, double *dt, const char *equat, const double *sn,
+                int64_t lgsnlt, const double *vol, double *sfsi, double *sfsj,
+                double *sfsk, double *dism, const double *cson);
 /* rbord.f90:4-433 restricted to extr, rc, para, idd, prd */
 int cns_rbord(cns_ctx *ctx, double *v, double *pression, double *ztemp,
               double *cson);
-/* sch_roe_euler.f90:106-1009 (ityprk = 0) */
-int cns_sch_roe_euler(cns_ctx *ctx, int l, double *u, const double *v,
-                      const double *sn, const double *ps);
-/* sch_roe.f90:4-1505 (ityprk = 0) */
-int cns_sch_roe(cns_ctx *ctx, int l, double *u, const double *v,
-                const double *tau, const double *sn, const double *ps);
+/* sch_roe_euler.f90:4-10 (rhol..prr: the reconstructed-state work arrays,
+ * not used) */
+int cns_sch_roe_euler(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v,
+                      double *ff, const char *equat, const double *sn, int64_t lgsnlt,
+                      double *rhol, double *ul, double *vl, double *wl, double *pl,
+                      double *rhor, double *ur, double *vr, double *wr, double *prr,
+                      const double *ps);
+/* sch_roe.f90:4-11 (toxx..qcz: the stresses and heat fluxes of zvisqc, nine
+ * arrays of ip12; used in place when they are the columns of one (ld, 9)
+ * array) */
+int cns_sch_roe(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v, double *ff,
+                const double *toxx, const double *toxy, const double *toxz,
+                const double *toyy, const double *toyz, const double *tozz,
+                const double *qcx, const double *qcy, const double *qcz, const char *equat,
+                const double *sn, int64_t lgsnlt, double *rhol, double *ul, double *vl,
+                double *wl, double *pl, double *rhor, double *ur, double *vr, double *wr,
+                double *prr, const double *ps);
 /* zvisqc.f90:4-210: zgrad2 + zfluto on every block, then rbte/rbtc */
 /* other flux families (atsch_num.f90:628-983), selected in the fused
  * iteration by cns_scheme_t.ischema: 14 = HLLC (sch_hllc_euler.f90:4-891,
  * sch_hllc.f90:4-1403, with the minmod limiter of ilim = 1 in the NS form),
  * 9 = Rusanov (sch_rusanov.f90:4-791: plain MUSCL, the stresses tau enter
- * whatever the equations -- zero for Euler); same arguments as
- * cns_sch_roe_euler / cns_sch_roe (l = 0: every block in one launch) */
-int cns_sch_hllc_euler(cns_ctx *ctx, int l, double *u, const double *v,
-                       const double *sn, const double *ps);
-int cns_sch_hllc(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
-                 const double *sn, const double *ps);
-int cns_sch_rusanov(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
-                    const double *sn, const double *ps);
-/* ischema 5 = AUSM+ (sch_ausmp.f90:4-1157; the reference runs it for the
+ * whatever the equations -- zero for Euler); the argument lists of
+ * sch_hllc_euler.f90:4-10, sch_hllc.f90:4-11, sch_rusanov.f90:4-11 */
+int cns_sch_hllc_euler(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v,
+                       double *ff, const char *equat, const double *sn, int64_t lgsnlt,
+                       double *rhol, double *ul, double *vl, double *wl, double *pl,
+                       double *rhor, double *ur, double *vr, double *wr, double *prr,
+                       const double *ps);
+int cns_sch_hllc(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v, double *ff,
+                 const double *toxx, const double *toxy, const double *toxz,
+                 const double *toyy, const double *toyz, const double *tozz,
+                 const double *qcx, const double *qcy, const double *qcz, const char *equat,
+                 const double *sn, int64_t lgsnlt, double *rhol, double *ul, double *vl,
+                 double *wl, double *pl, double *rhor, double *ur, double *vr, double *wr,
+                 double *prr, const double *ps);
+int cns_sch_rusanov(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v,
+                    double *ff, const double *toxx, const double *toxy, const double *toxz,
+                    const double *toyy, const double *toyz, const double *tozz,
+                    const double *qcx, const double *qcy, const double *qcz,
+                    const char *equat, const double *sn, int64_t lgsnlt, double *rhol,
+                    double *ul, double *vl, double *wl, double *pl, double *rhor, double *ur,
+                    double *vr, double *wr, double *prr, const double *ps);
+/* ischema 5 = AUSM+ (sch_ausmp.f90:4-11; the reference runs it for the
  * Navier-Stokes equations only: with the minmod limiter of ilim = 1, the
- * work and heat-flux terms of sch_ausmp.f90:81-83 from tau on the fly) */
-int cns_sch_ausmp(cns_ctx *ctx, int l, double *u, const double *v, const double *tau,
-                  const double *sn, const double *ps);
+ * work and heat-flux terms of sch_ausmp.f90:81-83 from tau on the fly; d is
+ * in its argument list and not read) */
+int cns_sch_ausmp(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v, double *d,
+                  double *ff, const double *toxx, const double *toxy, const double *toxz,
+                  const double *toyy, const double *toyz, const double *tozz,
+                  const double *qcx, const double *qcy, const double *qcz,
+                  const char *equat, const double *sn, int64_t lgsnlt, double *rhol,
+                  double *ul, double *vl, double *wl, double *pl, double *rhor, double *ur,
+                  double *vr, double *wr, double *prr, const double *ps);
 int cns_zvisqc(cns_ctx *ctx, const double *v, const double *mu,
                const double *mut, double *tau, const double *sn,
                const double *vol, const double *ztemp);
-/* implimf_eu.f90:6-347 (kfmg != 3, ityprk = 0) */
-int cns_implimf_eu(cns_ctx *ctx, int l, const double *u, const double *dt,
-                   double *v, double *d, const double *sn, const double *vol,
-                   const double *ps, const double *cson, int lmx);
-/* implimf_3d.f90:4-502 (kfmg != 3, ityprk = 0) */
-int cns_implimf_3d(cns_ctx *ctx, int l, const double *u, const double *dt,
-                   double *v, double *d, const double *mu, const double *mut,
-                   const double *sn, const double *vol, const double *ps,
-                   const double *cson, int lmx);
+/* implimf_eu.f90:6-12: lmx point-Jacobi sweeps and v += d on block lm;
+ * dtpas: the physical step of the dual-time diagonal (used when the
+ * scheme's kfmg = 3); dfxx..dfez, coefdiag: work arrays, not used (the
+ * increments are recomputed in the sweeps) */
+int cns_implimf_eu(cns_ctx *ctx, int lm, const double *u, const double *dt, double *v,
+                   double *d, const double *ff, const char *equat, int lmx,
+                   const double *sn, int64_t lgsnlt, const double *vol, double dtpas,
+                   int ityprk, double *dfxx, double *dfyy, double *dfzz, double *dfxy,
+                   double *dfxz, double *dfyz, double *dfex, double *dfey, double *dfez,
+                   double *coefdiag, const double *ps, const double *cson);
+/* implimf_3d.f90:4-11 (dfxx..dfez, rv: work arrays, not used) */
+int cns_implimf_3d(cns_ctx *ctx, int lm, const double *u, const double *dt, double *v,
+                   double *d, const double *ff, const double *mu, const double *mut,
+                   const char *equat, int lmx, const double *sn, int64_t lgsnlt,
+                   const double *vol, double dtpas, int ityprk, double *dfxx,
+                   double *dfyy, double *dfzz, double *dfxy, double *dfxz, double *dfyz,
+                   double *dfex, double *dfey, double *dfez, double *rv, const double *ps,
+                   const double *cson);
 /* rscpsv.f90 + residu.f90: L1, L2, Linf of (v-u0)/dt over all blocks;
  * norms: host array of 15 doubles (L1[5], L2[5], Linf[5]) */
 int cns_rscpsv(cns_ctx *ctx, const double *u0, const double *v,

@@ -211,6 +211,11 @@ int orc_writda(const char *path, const char *disc, const char *equat, const doub
                const double *mut, int64_t maxsub);
 int orc_readda(const char *path, const char *equat, int keinit, double *v, double *mut);
 
+/* cns_pmath.h's exp and pow (the injection condition's b**gam6 and the SA
+   source), exported for the libm comparison tests */
+double orc_pow(double x, double y);
+double orc_exp(double t);
+
 #ifdef __cplusplus
 }
 #endif

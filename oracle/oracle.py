@@ -33,6 +33,10 @@ def lib():
             build()
         L = C.CDLL(_LIB)
         L.orc_setup.argtypes = [C.c_int, _i32, C.c_int64]
+        L.orc_pow.argtypes = [C.c_double, C.c_double]
+        L.orc_pow.restype = C.c_double
+        L.orc_exp.argtypes = [C.c_double]
+        L.orc_exp.restype = C.c_double
         L.orc_setup.restype = C.c_int
         L.orc_set_phys.argtypes = [C.c_double] * 9
         L.orc_set_scheme.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int,

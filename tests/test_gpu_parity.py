@@ -2,8 +2,8 @@
 
 FP64 results are compared bit for bit (the kernels evaluate the reference
 expressions in the reference's order with separately rounded multiplies and
-adds), except where a libm power is involved (the injection condition,
-clidd.f90:128 b**gam6): there the tolerance is 1e-13 relative per routine.
+adds; the injection condition's real power, clidd.f90:128 b**gam6, is one
+portable implementation on both sides).
 """
 import numpy as np
 import pytest
@@ -82,13 +82,12 @@ def test_zpres_zvismo_chronos_rbord(cuda, name):
     has_idd = any(b.kind == cases.BC_IDD for b in case.boundaries)
     v_g = _n(s.v).reshape(5, -1)[:, g]
     v_o = st.v.reshape(5, -1)[:, g]
-    if has_idd:
-        assert max_rel_cols(v_g, v_o) <= 1e-13
-        assert max_rel(_n(s.pression)[g], st.ps[g]) <= 1e-13
-    else:
-        assert_equal_bits(v_g, v_o, "ghost v")
-        assert_equal_bits(_n(s.pression)[g], st.ps[g], "ghost p")
-        assert_equal_bits(_n(s.cson)[g], st.cson[g], "ghost c")
+    # the injection condition's real power is the portable cns_pow on both
+    # sides, so every boundary kind is compared bit for bit
+    assert has_idd in (True, False)
+    assert_equal_bits(v_g, v_o, "ghost v")
+    assert_equal_bits(_n(s.pression)[g], st.ps[g], "ghost p")
+    assert_equal_bits(_n(s.cson)[g], st.cson[g], "ghost c")
     s.close()
 
 
@@ -223,10 +222,7 @@ def test_fused_steps_parity(cuda, name, nsteps):
         ng = s.atsch_num(1)
         v_g = _n(s.v).reshape(5, ld)[:, rc]
         v_o = st.v.reshape(5, ld)[:, rc]
-        if has_idd:
-            assert max_rel_cols(v_g, v_o) <= 1e-12, f"step {it}"
-        else:
-            assert_equal_bits(v_g, v_o, f"v after step {it}")
+        assert_equal_bits(v_g, v_o, f"v after step {it} (injection: {has_idd})")
         np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0, err_msg=f"norms step {it}")
     s.close()
 

@@ -205,7 +205,8 @@ def test_teq_gradv_parity(cuda, name):
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_met_smsa_parity(cuda, name):
     """the SA source against the oracle: exp and the real power of
-    met_smsa.f90 may differ in the last bit from the host libm, so 1e-13"""
+    met_smsa.f90 are one portable implementation on both sides, so bit for
+    bit"""
     torch = cuda
     case = CASES[name]()
     orc, st = oracle_prepared(case)
@@ -228,7 +229,7 @@ def test_met_smsa_parity(cuda, name):
     s.sync()
     rc = case.layout.real_cells()
     for a, b, w in zip(g, (ts6_o, ts7_o, cf_o), ("ts6", "ts7", "cfke")):
-        np.testing.assert_allclose(a.cpu().numpy()[rc], b[rc], rtol=1e-13, atol=0, err_msg=w)
+        assert_equal_bits(a.cpu().numpy()[rc], b[rc], w)
     s.close()
 
 

@@ -1,5 +1,8 @@
 """CPU tests of the oracle: the analytic invariants that pin the restatement
 of the reference (no reference outputs exist to pin it against)."""
+import math
+import struct
+
 import numpy as np
 import pytest
 
@@ -330,3 +333,31 @@ def test_rans_plate_runs_and_clips():
     assert (v[5, rc] >= 1e-8).all() and (v[6, rc] == 0).all()
     assert (st.mut[rc] >= 0).all() and st.mut[rc].max() > 0
     assert hist[-1] < 0.2 * hist[0]
+
+
+def _ulps(a: float, b: float) -> int:
+    ia = struct.unpack("<q", struct.pack("<d", a))[0]
+    ib = struct.unpack("<q", struct.pack("<d", b))[0]
+    return abs(ia - ib)
+
+
+def test_portable_pow_and_exp_against_libm():
+    """the one exp and real power the kernels and the oracle share
+    (codens_b200/csrc/cns_pmath.h) stay within a few ulp of the host libm on
+    the arguments of the injection condition (b**gam6, b in (0, 1]) and the
+    SA source (exp of -ct4 chi^2, a sixth root)"""
+    L = lib()
+    rng = np.random.default_rng(3)
+    worst = {"pow_idd": 0, "exp": 0, "root6": 0, "pow": 0}
+    for b in rng.uniform(1e-3, 1.0, 20000):
+        worst["pow_idd"] = max(worst["pow_idd"], _ulps(L.orc_pow(b, 3.5), math.pow(b, 3.5)))
+    for t in rng.uniform(-40.0, 5.0, 20000):
+        worst["exp"] = max(worst["exp"], _ulps(L.orc_exp(t), math.exp(t)))
+    for r in rng.uniform(1e-3, 60.0, 20000):
+        worst["root6"] = max(worst["root6"], _ulps(L.orc_pow(r, 1 / 6), math.pow(r, 1 / 6)))
+    for x, y in zip(np.exp(rng.uniform(-10, 10, 20000)), rng.uniform(-4, 4, 20000)):
+        worst["pow"] = max(worst["pow"], _ulps(L.orc_pow(x, y), math.pow(x, y)))
+    assert worst["pow_idd"] <= 4 and worst["exp"] <= 2 and worst["root6"] <= 2, worst
+    assert worst["pow"] <= 8, worst
+    assert L.orc_pow(0.0, 3.5) == 0.0 and L.orc_pow(2.0, 0.0) == 1.0
+    assert math.isnan(L.orc_pow(-1.0, 0.5)) and L.orc_exp(-800.0) == 0.0
