@@ -45,6 +45,7 @@ struct cns_ctx {
   double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
   bool adj_fp32 = false;     // L^T of the prepared adjoint in FP32 (precision != 0)
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
+  TileBuf tiles_res;          // 2.5D tiles of the fused residual (kResTI x kResTJ x kResKC)
   bool tuned64 = false, tuned32 = false;
   float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
   int* d_cells_tile0 = nullptr;  // cells.blk_tile0 on the device
@@ -264,6 +265,9 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
   cudaError_t e = cudaSuccess;
   if (c->sc.ns && c->sc.ilim == 1)
     e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
+  if (e == cudaSuccess && residual_fused_ok(c->sc))
+    return launch_residual_fused(c->d_blks, c->tiles_res.view(l0), c->ph, c->sc, v, c->w.prim,
+                                 ld, ps, tau, sn, c->w.R, u, nullptr, c->st);
   if (e == cudaSuccess)
     e = launch_face_flux(c->d_blks, c->faces, l0, c->ph, c->sc, v, c->w.prim, ld, ps, tau,
                          sn, c->w.R, c->w.G, c->st, c->w.V);
@@ -689,12 +693,19 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     } else {
       if (e == cudaSuccess && lim)
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
-      if (e == cudaSuccess)
-        e = launch_face_flux_fma(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
-                                 s.pression, s.tau, s.sn, w.R, w.G, c->st, w.V);
-      if (e == cudaSuccess)
-        e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st,
-                                        w.V);
+      if (residual_fused_ok(c->sc)) {
+        if (e == cudaSuccess)
+          e = launch_residual_fused_fma(c->d_blks, c->tiles_res.view(-1), c->ph, c->sc, s.v,
+                                        w.prim, ld, s.pression, s.tau, s.sn, w.R, s.u, w.u32,
+                                        c->st);
+      } else {
+        if (e == cudaSuccess)
+          e = launch_face_flux_fma(c->d_blks, c->faces, -1, c->ph, c->sc, s.v, w.prim, ld,
+                                   s.pression, s.tau, s.sn, w.R, w.G, c->st, w.V);
+        if (e == cudaSuccess)
+          e = launch_accumulate_t<double>(c->d_blks, all, w.G, ld, nullptr, s.u, w.u32, c->st,
+                                          w.V);
+      }
     }
     if (e == cudaSuccess && mode == kDefectRefresh)
       e = launch_defect(c->d_blks, all, ld, s.u, w.ur32, w.corr, c->st);
@@ -910,6 +921,7 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
       x[0] = B.ni + 1; x[1] = B.nj + 1; x[2] = B.nk + 1; });
   if (e == cudaSuccess) e = build_tiles(c, c->tiles64, 32, 8, 8);
   if (e == cudaSuccess) e = build_tiles(c, c->tiles32, 32, 8, 8);
+  if (e == cudaSuccess) e = build_tiles(c, c->tiles_res, kResTI, kResTJ, kResKC);
   if (e == cudaSuccess) e = init_jacobi_25d();
   for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
     e = build_space(c, c->faces[dir], [dir](const Blk& B, int x[3]) {

@@ -758,6 +758,14 @@ cudaError_t launch_ratio_t<double>(const Blk* blks, const SpaceBuf* lines, int l
   return cudaGetLastError();
 }
 
+cudaError_t launch_residual_fused(const Blk* blks, Tiles tl, Phys ph, Scheme sc, const double* v,
+                                  const double* prim, long long ld, const double* ps,
+                                  const double* tau, const double* sn, const double* R,
+                                  double* u, float* u32, cudaStream_t st) {
+  return residual_fused_dispatch<double>(blks, tl, ph, sc, v, prim, ld, ps, tau, sn, R, u, u32,
+                                         st);
+}
+
 template <>
 cudaError_t launch_face_flux_t<double>(const Blk* blks, const SpaceBuf* faces, int l0,
                                        Phys ph, Scheme sc, const double* v,

@@ -450,24 +450,25 @@ __device__ __forceinline__ void load_prim(const T* __restrict__ v,
 // Occupancy: 4 CTAs per SM for Roe (128 registers; 2, 3, 5, 6 measured
 // slower), 5 for the lighter families (HLLC residual 1.59 -> 1.42 ms,
 // Rusanov 1.27 -> 1.18 ms against 4 on the 4.4M-cell channel).
-template <class T, bool NS, int FL = kFluxRoe>
-__global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
-    const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
-    const T* __restrict__ v, const T* __restrict__ prim, long long ld,
-    const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
-    const T* __restrict__ R, T* __restrict__ G, T* __restrict__ V = nullptr) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const PhysT<T> ph(ph64);
-  const Blk& B = blks[b];
+// The value a face contributes to the face buffer (the expressions of the
+// face kernel below, shared with the fused residual kernel): face p of
+// direction dir, n the cell above it.  HLLC with the stresses also writes the
+// viscous halves to V (when V is given).
+template <class T, bool NS, int FL>
+__device__ __forceinline__ void face_flux_eval(const Blk& B, int dir, int p, long long n,
+                                               const PhysT<T>& ph, const Scheme& sc,
+                                               const T* __restrict__ v,
+                                               const T* __restrict__ prim, long long ld,
+                                               const T* __restrict__ ps,
+                                               const T* __restrict__ tau,
+                                               const T* __restrict__ sn,
+                                               const T* __restrict__ R, T out[5],
+                                               T* __restrict__ V) {
   const long long inc = ninc_of(B, dir);
   const int nd = nd_of(B, dir);
-  const int p = dir == 0 ? i : (dir == 1 ? j : k);
-  const long long n = cell_index(B, i, j, k);
   const T sx = sn_ptr(sn, B, dir, 0)[n], sy = sn_ptr(sn, B, dir, 1)[n],
           sz = sn_ptr(sn, B, dir, 2)[n];
   const T pinfl = ph.pinfl;
-  T out[5];
   if (p == 1 || p == nd) {
     // boundary face: physical flux of the ghost cell (sch_roe_euler.f90:
     // 438-513, sch_roe.f90:497-580); the Euler j/k lower faces divide the
@@ -531,10 +532,8 @@ __global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
     if (FL == kFluxAusm) {
       // sch_ausmp.f90:289-298: hi1 whole, the others halved
       ausm_flux(WL, WR, sx, sy, sz, v, tau, ld, n, n - inc, ph, out);
-      T* Gd = G + (long long)dir * 5 * ld;
-      Gd[n] = out[0];
 #pragma unroll
-      for (int a = 1; a < 5; ++a) Gd[a * ld + n] = T(0.5) * out[a];
+      for (int a = 1; a < 5; ++a) out[a] = T(0.5) * out[a];
       return;
     }
     if (FL == kFluxHllc) {
@@ -557,13 +556,12 @@ __global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
                  tau[7 * ld + nR] + tau[7 * ld + nL]) * sy +
                 (txzR * ur + tyzR * vr + tzzR * wr + txzL * ul + tyzL * vl + tzzL * wl +
                  tau[8 * ld + nR] + tau[8 * ld + nL]) * sz;
-        T* Vd = V + (long long)dir * 4 * ld;
+        if (V) {
+          T* Vd = V + (long long)dir * 4 * ld;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) Vd[a * ld + n] = T(0.5) * fv[a];
+          for (int a = 0; a < 4; ++a) Vd[a * ld + n] = T(0.5) * fv[a];
+        }
       }
-      T* Gd = G + (long long)dir * 5 * ld;
-#pragma unroll
-      for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
       return;
     }
     T di[5], el, er;
@@ -618,9 +616,180 @@ __global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
     out[3] = T(0.5) * f4;
     out[4] = T(0.5) * f5;
   }
+}
+
+template <class T, bool NS, int FL = kFluxRoe>
+__global__ void __launch_bounds__(kTile, FL == kFluxRoe ? 4 : 5) k_face_flux(
+    const Blk* __restrict__ blks, Space sp, int dir, Phys ph64, Scheme sc,
+    const T* __restrict__ v, const T* __restrict__ prim, long long ld,
+    const T* __restrict__ ps, const T* __restrict__ tau, const T* __restrict__ sn,
+    const T* __restrict__ R, T* __restrict__ G, T* __restrict__ V = nullptr) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const PhysT<T> ph(ph64);
+  const Blk& B = blks[b];
+  const int p = dir == 0 ? i : (dir == 1 ? j : k);
+  const long long n = cell_index(B, i, j, k);
+  T out[5];
+  face_flux_eval<T, NS, FL>(B, dir, p, n, ph, sc, v, prim, ld, ps, tau, sn, R, out, V);
   T* Gd = G + (long long)dir * 5 * ld;
 #pragma unroll
   for (int a = 0; a < 5; ++a) Gd[a * ld + n] = out[a];
+}
+
+// ---------------------------------------------------------------------------
+// Fused residual: the three face directions and the accumulation in one
+// launch.  A CTA owns a TI x TJ patch of cell columns of one block and
+// marches along k over kc planes (the 2.5D tiles of the sweeps).  Per plane
+// it evaluates, once, every face its patch's cells touch -- the i faces
+// i0..i0+TI of each row, the j faces j0..j0+TJ of each column and the upper
+// k face of each column; the lower k face is the previous plane's upper one,
+// kept in shared memory -- with face_flux_eval (the face kernel's
+// expressions), then each real cell sums its six faces from shared memory in
+// the order of k_accumulate.  Same bits as the face kernels + k_accumulate,
+// without the face buffer's write and re-read in HBM and without the
+// accumulation launch.  Per plane a CTA evaluates (TI+1)TJ + TI(TJ+1) + TI TJ
+// faces for TI TJ cells: the patch-edge faces are evaluated by both
+// neighbouring CTAs (1/TI + 1/TJ of the faces).
+// ---------------------------------------------------------------------------
+template <int TI, int TJ>
+constexpr size_t residual_smem_faces() {
+  return (size_t)(TI + 1) * TJ + (size_t)TI * (TJ + 1) + 2 * (size_t)TI * TJ;
+}
+
+template <class T, bool NS, int FL, int TI, int TJ, int MINB>
+__global__ void __launch_bounds__(TI * TJ, MINB) k_residual_25d(
+    const Blk* __restrict__ blks, Tiles tl, Phys ph64, Scheme sc, const T* __restrict__ v,
+    const T* __restrict__ prim, long long ld, const T* __restrict__ ps,
+    const T* __restrict__ tau, const T* __restrict__ sn, const T* __restrict__ R,
+    double* __restrict__ u, float* __restrict__ u32) {
+  constexpr int NT = TI * TJ, NFI = (TI + 1) * TJ, NFJ = TI * (TJ + 1);
+  constexpr int NF = NFI + NFJ + 2 * NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // face values [5][NF]: i faces (x, y) at y (TI+1) + x (face i0 + x), then
+  // j faces (x, y) at NFI + y TI + x (face j0 + y), then two slots of k faces
+  T* sf = reinterpret_cast<T*>(smem_raw);
+  const int4 t = tl.tile[tl.tile0 + blockIdx.x];
+  const Blk B = blks[t.x];
+  const PhysT<T> ph(ph64);
+  const int i0 = t.y, j0 = t.z, kbeg = t.w, kend = min(t.w + tl.kc, B.nk);
+  const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = i <= B.ni - 1 && j <= B.nj - 1;
+  // one work loop per plane over the faces it needs (a single evaluation
+  // site keeps the register allocation of the face kernel): the i faces, the
+  // j faces, the upper k faces of the columns, and on the first plane the
+  // lower k faces too
+  for (int k = kbeg; k < kend; ++k) {
+    const int nitems = NFI + NFJ + NT + (k == kbeg ? NT : 0);
+    for (int q = threadIdx.x; q < nitems; q += NT) {
+      int dir, fi, fj, fk, slot;
+      bool ok;
+      if (q < NFI) {
+        dir = 0;
+        fi = i0 + q % (TI + 1);
+        fj = j0 + q / (TI + 1);
+        fk = k;
+        slot = q;
+        ok = fi <= B.ni && fj <= B.nj - 1;
+      } else if (q < NFI + NFJ) {
+        const int r = q - NFI;
+        dir = 1;
+        fi = i0 + r % TI;
+        fj = j0 + r / TI;
+        fk = k;
+        slot = q;
+        ok = fi <= B.ni - 1 && fj <= B.nj;
+      } else {
+        const int r = (q - NFI - NFJ) % NT;
+        const bool upper = q < NFI + NFJ + NT;  // else the first plane's lower faces
+        dir = 2;
+        fi = i0 + r % TI;
+        fj = j0 + r / TI;
+        fk = upper ? k + 1 : k;
+        slot = NFI + NFJ + (fk & 1) * NT + r;
+        ok = fi <= B.ni - 1 && fj <= B.nj - 1;
+      }
+      if (ok) {
+        const int p = dir == 0 ? fi : (dir == 1 ? fj : fk);
+        T out[5];
+        face_flux_eval<T, NS, FL>(B, dir, p, cell_index(B, fi, fj, fk), ph, sc, v, prim, ld, ps,
+                                  tau, sn, R, out, nullptr);
+#pragma unroll
+        for (int a = 0; a < 5; ++a) sf[a * NF + slot] = out[a];
+      }
+    }
+    __syncthreads();
+    if (own) {
+      // k_accumulate's order: directions i, j, k; lower face then upper,
+      // except the upper face first for the first cell of a line (nd >= 3)
+      const int slo[3] = {ty * (TI + 1) + tx, NFI + ty * TI + tx,
+                          NFI + NFJ + (k & 1) * NT + threadIdx.x};
+      const int sup[3] = {slo[0] + 1, slo[1] + TI, NFI + NFJ + ((k + 1) & 1) * NT + threadIdx.x};
+      const int pos[3] = {i, j, k};
+      double acc[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        const bool upper_first = pos[dir] == 1 && nd_of(B, dir) >= 3;
+#pragma unroll
+        for (int a = 0; a < 5; ++a) {
+          const double gl = (double)sf[a * NF + slo[dir]], gu = (double)sf[a * NF + sup[dir]];
+          if (upper_first) {
+            acc[a] = acc[a] + gu;
+            acc[a] = acc[a] - gl;
+          } else {
+            acc[a] = acc[a] - gl;
+            acc[a] = acc[a] + gu;
+          }
+        }
+      }
+      const long long n = cell_index(B, i, j, k);
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        if (u) u[a * ld + n] = acc[a];
+        if (u32) u32[a * ld + n] = (float)acc[a];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class T, bool NS, int FL, int TI, int TJ, int MINB>
+cudaError_t residual_fused_shape(const Blk* blks, Tiles tl, Phys ph, Scheme sc, const T* v,
+                                 const T* prim, long long ld, const T* ps, const T* tau,
+                                 const T* sn, const T* R, double* u, float* u32,
+                                 cudaStream_t st) {
+  constexpr size_t sm = sizeof(T) * 5 * residual_smem_faces<TI, TJ>();
+  k_residual_25d<T, NS, FL, TI, TJ, MINB><<<tl.ntiles, TI * TJ, sm, st>>>(
+      blks, tl, ph, sc, v, prim, ld, ps, tau, sn, R, u, u32);
+  return cudaGetLastError();
+}
+
+// the fused residual of the flux families that keep one value per face (all
+// but HLLC with the stresses, whose viscous halves go through the face
+// buffer path); tl: the residual's 2.5D tiles (patch 32 x 4)
+template <class T>
+cudaError_t residual_fused_dispatch(const Blk* blks, Tiles tl, Phys ph, Scheme sc, const T* v,
+                                    const T* prim, long long ld, const T* ps, const T* tau,
+                                    const T* sn, const T* R, double* u, float* u32,
+                                    cudaStream_t st) {
+  if (tl.ntiles == 0) return cudaSuccess;
+  if (tl.ti != 32 || tl.tj != 4) return cudaErrorInvalidValue;
+  if (sc.ischema == 14 && sc.ns) return cudaErrorInvalidValue;
+  if (sc.ischema == 14)
+    return residual_fused_shape<T, false, kFluxHllc, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
+                                                               tau, sn, R, u, u32, st);
+  if (sc.ischema == 9)
+    return residual_fused_shape<T, true, kFluxRusanov, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld,
+                                                                 ps, tau, sn, R, u, u32, st);
+  if (sc.ischema == 5)
+    return residual_fused_shape<T, true, kFluxAusm, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
+                                                              tau, sn, R, u, u32, st);
+  if (sc.ns)
+    return residual_fused_shape<T, true, kFluxRoe, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
+                                                             tau, sn, R, u, u32, st);
+  return residual_fused_shape<T, false, kFluxRoe, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
+                                                            tau, sn, R, u, u32, st);
 }
 
 // the FP64 face kernels of one residual by flux family (atsch_num.f90:628-983):

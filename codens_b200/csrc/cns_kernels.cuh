@@ -353,6 +353,27 @@ inline cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
                                 const double* ps, double* R, cudaStream_t st) {
   return launch_ratio_t<double>(blks, lines, l0, v, prim, ld, ps, R, st);
 }
+// The fused residual (the face fluxes of the three directions and their
+// accumulation into u, and u32 when given, in one launch over the 32 x 4
+// residual tiles) for every flux family that keeps one value per face: all
+// but HLLC with the stresses (ischema 14 with ns) and the Jameson scheme.
+// launch_residual_fused: FP64 without contraction (the bit-exact path);
+// launch_residual_fused_fma: the same kernel compiled with contraction (the
+// FP64 residual of the mixed form).
+inline bool residual_fused_ok(const Scheme& sc) {
+  return (sc.ischema == 7 || sc.ischema == 9 || sc.ischema == 5 || sc.ischema == 14) &&
+         !(sc.ischema == 14 && sc.ns);
+}
+constexpr int kResTI = 32, kResTJ = 4, kResKC = 16;
+cudaError_t launch_residual_fused(const Blk* blks, Tiles tl, Phys ph, Scheme sc, const double* v,
+                                  const double* prim, long long ld, const double* ps,
+                                  const double* tau, const double* sn, const double* R,
+                                  double* u, float* u32, cudaStream_t st);
+cudaError_t launch_residual_fused_fma(const Blk* blks, Tiles tl, Phys ph, Scheme sc,
+                                      const double* v, const double* prim, long long ld,
+                                      const double* ps, const double* tau, const double* sn,
+                                      const double* R, double* u, float* u32, cudaStream_t st);
+
 inline cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int l0,
                                     Phys ph, Scheme sc, const double* v,
                                     const double* prim, long long ld, const double* ps,

@@ -185,6 +185,16 @@ cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0,
   return face_flux_dispatch(blks, faces, l0, ph, sc, v, prim, ld, ps, tau, sn, R, G, V, st);
 }
 
+// the fused residual compiled with contraction (the mixed form's FP64
+// residual: FP64 rounding from the bit-exact one, as the face kernels above)
+cudaError_t launch_residual_fused_fma(const Blk* blks, Tiles tl, Phys ph, Scheme sc,
+                                      const double* v, const double* prim, long long ld,
+                                      const double* ps, const double* tau, const double* sn,
+                                      const double* R, double* u, float* u32, cudaStream_t st) {
+  return residual_fused_dispatch<double>(blks, tl, ph, sc, v, prim, ld, ps, tau, sn, R, u, u32,
+                                         st);
+}
+
 template <>
 cudaError_t launch_accumulate_t<float>(const Blk* blks, Space sp, const float* G,
                                        long long ld, const double* corr, double* u,
