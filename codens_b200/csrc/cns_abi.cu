@@ -45,7 +45,8 @@ struct cns_ctx {
   double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
   bool adj_fp32 = false;     // L^T of the prepared adjoint in FP32 (precision != 0)
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
-  TileBuf tiles_res;          // 2.5D tiles of the fused residual (kResTI x kResTJ x kResKC)
+  TileBuf tiles_res;          // 2.5D tiles of the fused residual
+  bool res_fused = false;     // residual: fused kernel (tiles_res) or face kernels + accumulate
   bool tuned64 = false, tuned32 = false;
   float tune_ms64 = 0.f, tune_ms32 = 0.f;  // the chosen configuration's sweep time
   int* d_cells_tile0 = nullptr;  // cells.blk_tile0 on the device
@@ -265,7 +266,7 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
   cudaError_t e = cudaSuccess;
   if (c->sc.ns && c->sc.ilim == 1)
     e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
-  if (e == cudaSuccess && residual_fused_ok(c->sc))
+  if (e == cudaSuccess && c->res_fused && residual_fused_ok(c->sc))
     return launch_residual_fused(c->d_blks, c->tiles_res.view(l0), c->ph, c->sc, v, c->w.prim,
                                  ld, ps, tau, sn, c->w.R, u, nullptr, c->st);
   if (e == cudaSuccess)
@@ -693,7 +694,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     } else {
       if (e == cudaSuccess && lim)
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
-      if (residual_fused_ok(c->sc)) {
+      if (c->res_fused && residual_fused_ok(c->sc)) {
         if (e == cudaSuccess)
           e = launch_residual_fused_fma(c->d_blks, c->tiles_res.view(-1), c->ph, c->sc, s.v,
                                         w.prim, ld, s.pression, s.tau, s.sn, w.R, s.u, w.u32,
@@ -1989,6 +1990,34 @@ int cns_set_sweep_tiles(cns_ctx* c, int precision, int ti, int tj, int kc) {
   CK(build_tiles(c, precision == 0 ? c->tiles64 : c->tiles32, ti, tj, kc));
   (precision == 0 ? c->tuned64 : c->tuned32) = true;
   drop_graphs(c);
+  return CNS_OK;
+}
+
+int cns_set_residual_tiles(cns_ctx* c, int ti, int tj, int kc) {
+  if (!c || ti < 0 || tj < 0 || kc < 0) return CNS_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  if (ti == 0) {
+    c->res_fused = false;
+    drop_graphs(c);
+    return CNS_OK;
+  }
+  bool ok = kc >= 1;
+  bool shape = false;
+  for (int sh = 0; sh < kResShapes; ++sh)
+    shape = shape || (kResShape[sh][0] == ti && kResShape[sh][1] == tj);
+  if (!ok || !shape)
+    return fail(c, CNS_EINVAL, "residual patch shape not one of 32x4, 16x8, or kc < 1");
+  CK(build_tiles(c, c->tiles_res, ti, tj, kc));
+  c->res_fused = true;
+  drop_graphs(c);
+  return CNS_OK;
+}
+
+int cns_residual_tiles(cns_ctx* c, int32_t* cfg) {
+  if (!c || !cfg) return CNS_EINVAL;
+  cfg[0] = c->res_fused ? c->tiles_res.ti : 0;
+  cfg[1] = c->res_fused ? c->tiles_res.tj : 0;
+  cfg[2] = c->res_fused ? c->tiles_res.kc : 0;
   return CNS_OK;
 }
 

@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(TI * TJ, MINB) k_residual_25d(
   // j faces (x, y) at NFI + y TI + x (face j0 + y), then two slots of k faces
   T* sf = reinterpret_cast<T*>(smem_raw);
   const int4 t = tl.tile[tl.tile0 + blockIdx.x];
-  const Blk B = blks[t.x];
+  const Blk& B = blks[t.x];  // fields read where used (not held in registers)
   const PhysT<T> ph(ph64);
   const int i0 = t.y, j0 = t.z, kbeg = t.w, kend = min(t.w + tl.kc, B.nk);
   const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
@@ -774,22 +774,29 @@ cudaError_t residual_fused_dispatch(const Blk* blks, Tiles tl, Phys ph, Scheme s
                                     const T* sn, const T* R, double* u, float* u32,
                                     cudaStream_t st) {
   if (tl.ntiles == 0) return cudaSuccess;
-  if (tl.ti != 32 || tl.tj != 4) return cudaErrorInvalidValue;
   if (sc.ischema == 14 && sc.ns) return cudaErrorInvalidValue;
-  if (sc.ischema == 14)
-    return residual_fused_shape<T, false, kFluxHllc, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
-                                                               tau, sn, R, u, u32, st);
-  if (sc.ischema == 9)
-    return residual_fused_shape<T, true, kFluxRusanov, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld,
-                                                                 ps, tau, sn, R, u, u32, st);
-  if (sc.ischema == 5)
-    return residual_fused_shape<T, true, kFluxAusm, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
-                                                              tau, sn, R, u, u32, st);
-  if (sc.ns)
-    return residual_fused_shape<T, true, kFluxRoe, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
-                                                             tau, sn, R, u, u32, st);
-  return residual_fused_shape<T, false, kFluxRoe, 32, 4, 4>(blks, tl, ph, sc, v, prim, ld, ps,
-                                                            tau, sn, R, u, u32, st);
+#define CNS_RES_SHAPE(A, B_)                                                              \
+  if (tl.ti == A && tl.tj == B_) {                                                        \
+    if (sc.ischema == 14)                                                                 \
+      return residual_fused_shape<T, false, kFluxHllc, A, B_, 4>(blks, tl, ph, sc, v, prim, \
+                                                                 ld, ps, tau, sn, R, u, u32, \
+                                                                 st);                      \
+    if (sc.ischema == 9)                                                                  \
+      return residual_fused_shape<T, true, kFluxRusanov, A, B_, 4>(                       \
+          blks, tl, ph, sc, v, prim, ld, ps, tau, sn, R, u, u32, st);                     \
+    if (sc.ischema == 5)                                                                  \
+      return residual_fused_shape<T, true, kFluxAusm, A, B_, 4>(blks, tl, ph, sc, v, prim, \
+                                                                ld, ps, tau, sn, R, u, u32, st); \
+    if (sc.ns)                                                                            \
+      return residual_fused_shape<T, true, kFluxRoe, A, B_, 4>(blks, tl, ph, sc, v, prim, ld, \
+                                                               ps, tau, sn, R, u, u32, st); \
+    return residual_fused_shape<T, false, kFluxRoe, A, B_, 4>(blks, tl, ph, sc, v, prim, ld, \
+                                                              ps, tau, sn, R, u, u32, st);  \
+  }
+  CNS_RES_SHAPE(32, 4)
+  CNS_RES_SHAPE(16, 8)
+#undef CNS_RES_SHAPE
+  return cudaErrorInvalidValue;
 }
 
 // the FP64 face kernels of one residual by flux family (atsch_num.f90:628-983):

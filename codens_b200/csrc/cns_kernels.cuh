@@ -364,7 +364,10 @@ inline bool residual_fused_ok(const Scheme& sc) {
   return (sc.ischema == 7 || sc.ischema == 9 || sc.ischema == 5 || sc.ischema == 14) &&
          !(sc.ischema == 14 && sc.ns);
 }
-constexpr int kResTI = 32, kResTJ = 4, kResKC = 16;
+constexpr int kResTI = 32, kResTJ = 4, kResKC = 16;  // default fused tiles
+// the patch shapes the fused residual is instantiated for
+constexpr int kResShapes = 2;
+constexpr int kResShape[kResShapes][2] = {{32, 4}, {16, 8}};
 cudaError_t launch_residual_fused(const Blk* blks, Tiles tl, Phys ph, Scheme sc, const double* v,
                                   const double* prim, long long ld, const double* ps,
                                   const double* tau, const double* sn, const double* R,

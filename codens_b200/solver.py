@@ -206,6 +206,17 @@ class CodeNS:
         self._check(self.lib.cns_set_sweep_tiles(self.ctx, precision, ti, tj, kc),
                     "cns_set_sweep_tiles")
 
+    def residual_tiles(self):
+        """(ti, tj, kc) of the fused residual, or zeros for the face kernels"""
+        cfg = (C.c_int32 * 3)()
+        self._check(self.lib.cns_residual_tiles(self.ctx, cfg), "cns_residual_tiles")
+        return tuple(int(x) for x in cfg)
+
+    def set_residual_tiles(self, ti: int, tj: int = 0, kc: int = 0):
+        """ti = 0: the face kernels + accumulation; else the fused kernel"""
+        self._check(self.lib.cns_set_residual_tiles(self.ctx, ti, tj, kc),
+                    "cns_set_residual_tiles")
+
     @property
     def kernels_launched(self) -> int:
         """kernels launched so far by the fused-step graphs of this solver"""

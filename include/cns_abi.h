@@ -474,6 +474,14 @@ int cns_sch_dual(cns_ctx *ctx, int l, double *u, const double *v, int icycle,
  * 16x16; kc >= 1) and marks it tuned. */
 int cns_sweep_tiles(cns_ctx *ctx, int precision, int32_t *cfg);
 int cns_set_sweep_tiles(cns_ctx *ctx, int precision, int ti, int tj, int kc);
+/* Residual kernel variant (no counterpart in the reference): ti = 0 selects
+ * the face kernels (one launch per direction into a face buffer, then the
+ * per-cell accumulation); ti x tj = 32 x 4 or 16 x 8 selects the fused kernel
+ * (all three directions and the accumulation in one launch over 2.5D tiles
+ * of kc planes).  Both give the same bits in FP64.  cns_residual_tiles
+ * returns {ti, tj, kc} (zeros for the face kernels). */
+int cns_set_residual_tiles(cns_ctx *ctx, int ti, int tj, int kc);
+int cns_residual_tiles(cns_ctx *ctx, int32_t *cfg);
 /* drop-in call with host arrays: copies the real+ghost state v (host, ld x 5)
  * in, runs nsteps iterations, copies v back and returns the last norms */
 int cns_atsch_num_step_host(cns_ctx *ctx, double *v_host, int nsteps,

@@ -64,3 +64,25 @@ def test_rejects_unknown_shape(cuda):
     with pytest.raises(abi.CnsError):
         s.set_sweep_tiles(0, 32, 8, 0)
     s.close()
+
+
+@pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu", "box_pinfl"])
+def test_fused_residual_variant_gives_the_same_bits(cuda, name):
+    """the fused residual kernel (three face directions and the accumulation
+    in one 2.5D launch) against the face kernels + accumulation: the same
+    FP64 iteration bit for bit, for both patch shapes and several plane
+    counts"""
+    from codens_b200.solver import CodeNS
+    ref, _ = _run(name, 0, (32, 8, 8))
+    for ti, tj in ((32, 4), (16, 8)):
+        for kc in (1, 3, 16):
+            case = SMALL[name]()
+            s = CodeNS(case)
+            s.metric()
+            s.set_residual_tiles(ti, tj, kc)
+            assert s.residual_tiles() == (ti, tj, kc)
+            s.set_sweep_tiles(0, 32, 8, 8)
+            s.atsch_num(3)
+            v = s.v.cpu().numpy().reshape(5, case.layout.ld)[:, real(case)]
+            s.close()
+            assert_equal_bits(v, ref, f"fused residual {ti}x{tj}x{kc}")
