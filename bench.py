@@ -86,6 +86,8 @@ def parse():
                    choices=["channel", "batch", "adjoint", "rans", "dual"],
                    help="channel: the 8-block NS channel; batch: 64 independent Euler boxes "
                         "in one launch against the same boxes one at a time")
+    p.add_argument("--tune-cache", default=None,
+                   help="sweep-tiling cache file: a tiling found there is used without timing")
     p.add_argument("--tiles", default=None,
                    help="TI,TJ,KC: fix the Jacobi sweep tiling instead of autotuning it")
     p.add_argument("--eta", type=float, default=5.0,
@@ -390,6 +392,8 @@ def run_ours(args):
     case = make_case(args)
     s = CodeNS(case, device=local)
     s.metric()
+    if args.tune_cache:
+        s.set_tune_cache(args.tune_cache)
     if args.tiles:
         ti, tj, kc = (int(x) for x in args.tiles.split(","))
         s.set_sweep_tiles(PRECISION[args.precision], ti, tj, kc)
@@ -516,7 +520,8 @@ def run_ours(args):
             "data": "synthetic (seeded)",
             "config": dict(config_of(case, args, ws),
                            sweep_tiles={"ti": tiles[0], "tj": tiles[1], "kc": tiles[2],
-                                        "autotuned": bool(tiles[3])}),
+                                        "source": {0: "set", 1: "timed on the data",
+                                                   2: "tuning cache"}[tiles[3]]}),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_v,
                     "d2h_bytes_per_step": bytes_v + 15 * 8},
             "gpu_launches": kernels,

@@ -378,12 +378,6 @@ class WallForceGradient:
         torch = self.torch
         s, M = self.s, self.maps
         dev = s.dev
-        ld = M.ld
-        # the iteration's inputs at the converged state
-        s.adjoint_prepare()
-        s.sync()
-        W = s.v.detach().reshape(5, ld).clone()
-        self.W = W
         # orientation of the face areas (norm.f90's psk/psj/psi) from the
         # library's metric
         P0 = M.nodes(torch.as_tensor(self.wall, device=dev))
@@ -401,12 +395,25 @@ class WallForceGradient:
                 raise RuntimeError(f"torch face areas differ from the metric ({err:.2e})")
             self.sgn.append(sg)
         nrm = M.boundary_normals(P0, self.sgn)
+        self.nrm = nrm
         self.sgn_nx = torch.sign(nrm[0, M.wall_ent]).detach()
-        # interior pressure derivative (zpres) and boundary-map Jacobians
+        self._linearise()
+
+    def _linearise(self):
+        """the iteration's inputs and Jacobians at the solver's current state:
+        the library's face-flux Jacobians and implicit coefficients
+        (cns_adjoint_prepare), the interior pressure derivative (zpres) and
+        the boundary-map Jacobians"""
+        torch = self.torch
+        s, M = self.s, self.maps
+        s.adjoint_prepare()
+        s.sync()
+        W = s.v.detach().reshape(5, M.ld).clone()
+        self.W = W
         Wr = W.clone().requires_grad_(True)
         self.dp_dW = torch.autograd.functional.jacobian(
             lambda w: M.pressure(w).sum(), Wr)       # (5, ld)
-        self._bc_jac(W, nrm)
+        self._bc_jac(W, self.nrm)
 
     def _bc_inputs(self, W):
         M = self.maps
@@ -539,7 +546,20 @@ class WallForceGradient:
         sbar = torch.zeros(9 * ld, dtype=torch.float64, device=dev)
         s.adjoint_rt(lam, wbar, sbar)
         s.sync()
-        # lambda^T du/dtheta through the face areas and the boundary maps
+        gwall_u, gm_u, ga_u = self._lin_grads(wbar, sbar)
+        gwall = gwall_J - gwall_u
+        gm = gm_J - gm_u
+        ga = -ga_u
+        return J, float(gm), float(ga), gwall.detach()
+
+    def _lin_grads(self, wbar, sbar):
+        """d(lambda^T u)/d(wall heights, Mach, angle) at the linearisation
+        state self.W, from the library's per-cell wbar and per-face sbar of
+        lambda: through the face areas and the boundary maps"""
+        torch = self.torch
+        M = self.maps
+        dev = self.s.dev
+        ld = M.ld
         wall = torch.as_tensor(self.wall, device=dev).requires_grad_(True)
         mach = torch.tensor(self.mach, dtype=torch.float64, device=dev, requires_grad=True)
         alpha = torch.tensor(self.alpha, dtype=torch.float64, device=dev, requires_grad=True)
@@ -567,9 +587,111 @@ class WallForceGradient:
         zero = torch.zeros((), dtype=torch.float64, device=dev)
         gm_u = zero if gm_u is None else gm_u
         ga_u = zero if ga_u is None else ga_u
-        gwall = gwall_J - gwall_u
-        gm = gm_J - gm_u
-        ga = -ga_u
+        return gwall_u.detach(), gm_u.detach(), ga_u.detach()
+
+
+class CheckpointedGradient(WallForceGradient):
+    """Reverse accumulation of J(W_N) through N pseudo-time iterations of the
+    primal, W_{n+1} = W_n + d(W_n) with d the implicit phase's increment,
+    with pseudo-time checkpointing: the forward run keeps the state every
+    `every` iterations; the reverse sweep takes the segments from the last to
+    the first, recomputes each segment's states from its checkpoint, and
+    steps back through them -- at most N/every + every states in memory
+    instead of N.  Each reverse step linearises the iteration at its state
+    W_n (library face-flux Jacobians and implicit coefficients, torch
+    boundary maps):
+
+        mu_n   = L_n^T wbar_{n+1}
+        wbar_n = wbar_{n+1} - A_n^T mu_n
+        dJ/dtheta -= d(mu_n^T u)/dtheta at W_n,
+
+    from wbar_N = dJ/dW at W_N; L_n is the implicit phase linearised at
+    d = 0, whose own dependence on the state is not differentiated (it
+    multiplies the residual, zero at a steady state).  Over a converged
+    history the sum of the mu_n after N reverse steps is the steady adjoint's
+    lambda after N of its iterations, so the gradient tends to
+    WallForceGradient's; for a history that has not converged it is the
+    derivative of the truncated iteration with the implicit phase frozen.
+    The start state is held fixed.  The result does not depend on `every`
+    (the recomputed states are the forward run's, bit for bit)."""
+
+    def __init__(self, design: Design, mach: float, alpha: float, wall: np.ndarray,
+                 n_iter: int, every: int, start=None):
+        import torch
+        if n_iter < 1 or every < 1:
+            raise ValueError("n_iter and every must be positive")
+        self.torch = torch
+        self.design = design
+        self.mach, self.alpha = float(mach), float(alpha)
+        self.wall = np.asarray(wall, dtype=float)
+        self.case = design.case(mach, alpha, self.wall)
+        self.n_iter, self.every = int(n_iter), int(every)
+        s = CodeNS(self.case)
+        s.metric()
+        if start is not None:
+            s.v.copy_(torch.as_tensor(np.ascontiguousarray(start).reshape(-1), device=s.dev))
+            torch.cuda.synchronize()
+        self.s = s
+        self.maps = _Maps(self.case, torch, s.dev)
+        # forward: checkpoints at n = 0, every, 2 every, ...
+        self.ckpt = {}
+        n = 0
+        while n < self.n_iter:
+            s.sync()
+            self.ckpt[n] = s.v.detach().clone()
+            k = min(self.every, self.n_iter - n)
+            self.l2 = float(s.atsch_num(k)[1, 0])
+            n += k
+        s.sync()
+        self.iters = self.n_iter
+        self.max_states = 0  # the most states held at once in the reverse sweep
+        self._setup()        # orientation and the linearisation at W_N
+
+    def _set_state(self, W):
+        self.s.sync()
+        self.s.v.copy_(W)
+        self.s.sync()
+
+    def gradient(self):
+        """(J(W_N), dJ/dM, dJ/dalpha [per degree], dJ/dwall) by reverse
+        accumulation over the checkpointed history"""
+        torch = self.torch
+        M = self.maps
+        s = self.s
+        dev = s.dev
+        ld = M.ld
+        J, gW, gwall, gm = self.value_and_partials()      # at W_N (the last _setup)
+        gwall = gwall.detach().clone()
+        gm = gm.detach().clone()
+        ga = torch.zeros((), dtype=torch.float64, device=dev)
+        wb_state = gW.reshape(-1).contiguous()
+        mu = torch.zeros(5 * ld, dtype=torch.float64, device=dev)
+        wbar = torch.zeros(6 * ld, dtype=torch.float64, device=dev)
+        sbar = torch.zeros(9 * ld, dtype=torch.float64, device=dev)
+        self.mu_sum = torch.zeros(5 * ld, dtype=torch.float64, device=dev)
+        for n0 in sorted(self.ckpt, reverse=True):
+            k = min(self.every, self.n_iter - n0)
+            # recompute the segment's states W_n0 .. W_{n0+k-1}
+            states = [self.ckpt[n0]]
+            self._set_state(self.ckpt[n0])
+            for _ in range(k - 1):
+                s.atsch_num(1)
+                s.sync()
+                states.append(s.v.detach().clone())
+            self.max_states = max(self.max_states, len(states) + len(self.ckpt))
+            for W_n in reversed(states):
+                self._set_state(W_n)
+                self._linearise()
+                s.adjoint_lt(wb_state, mu)
+                s.adjoint_rt(mu, wbar, sbar)
+                s.sync()
+                a = self._chain(wbar).reshape(-1)
+                wb_state = (wb_state - a).contiguous()
+                self.mu_sum += mu
+                gw_u, gm_u, ga_u = self._lin_grads(wbar, sbar)
+                gwall -= gw_u
+                gm -= gm_u
+                ga -= ga_u
         return J, float(gm), float(ga), gwall.detach()
 
 

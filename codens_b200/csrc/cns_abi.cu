@@ -43,6 +43,10 @@ struct cns_ctx {
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
   double* tau_pack = nullptr;  // nine separate stress arrays packed as (ld, 9)
   double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
+  int* sched32 = nullptr;      // tile counter pair of the persistent FP32 sweep
+  std::string tune_cache;      // sweep-tiling cache file ("" = none)
+  int tune_src64 = 0, tune_src32 = 0;  // tiling source: 0 default or set, 1 timed, 2 cache
+  int nsm = 0;                 // streaming multiprocessors of the device
   bool adj_fp32 = false;     // L^T of the prepared adjoint in FP32 (precision != 0)
   TileBuf tiles64, tiles32;   // 2.5D tiles of the FP64 and the FP32 Jacobi sweeps
   TileBuf tiles_res;          // 2.5D tiles of the fused residual
@@ -178,6 +182,14 @@ cudaError_t build_tiles(cns_ctx* c, TileBuf& t, int ti, int tj, int kc) {
   t.tj = tj;
   t.kc = kc;
   return upload(c, &t.d_tile, tl.data(), tl.size());
+}
+
+// the FP32 sweep tiles run as a persistent launch: one CTA per resident slot
+// of the GPU (every SM times the kernel's CTAs per SM), taking tiles in turn
+void persistent_sweep32(cns_ctx* c) {
+  const int per_sm = sweep_f32_blocks_per_sm(c->tiles32.ti, c->tiles32.tj, !c->sc.ns);
+  c->tiles32.sched = (c->sched32 && per_sm > 0 && c->nsm > 0) ? c->sched32 : nullptr;
+  c->tiles32.grid = per_sm * c->nsm;
 }
 
 bool bad_block(cns_ctx* c, int l) { return l < 0 || l > (int)c->lay.blks.size(); }
@@ -757,10 +769,77 @@ cudaError_t time_sweep(cns_ctx* c, Tiles tl, const T* u, const T* v, const T* pr
   return e;
 }
 
+// The tuning cache (cns_set_tune_cache): one line per tuned configuration,
+//   <key> <ti> <tj> <kc>
+// key = GPU name (blanks as '_') | SM count | sweep precision (f64 / f32) |
+// equations (eu / ns) | floor(log2(real cells)) | floor(log2(blocks)) |
+// floor(log2(cells of the smallest block)).  A key found in the file is used
+// as it is, without timing, so a given cache file always gives the same
+// tiling; a missing key is tuned on the data and appended.
+std::string tune_key(cns_ctx* c, bool fp32) {
+  cudaDeviceProp pr{};
+  if (cudaGetDeviceProperties(&pr, c->device) != cudaSuccess) return "";
+  std::string name(pr.name);
+  for (char& ch : name)
+    if (ch == ' ' || ch == '|') ch = '_';
+  auto lg = [](long long x) {
+    int r = 0;
+    while (x > 1) {
+      x >>= 1;
+      ++r;
+    }
+    return r;
+  };
+  long long smallest = -1;
+  for (const Blk& B : c->lay.blks) {
+    const long long n = (long long)(B.ni - 1) * (B.nj - 1) * (B.nk - 1);
+    if (smallest < 0 || n < smallest) smallest = n;
+  }
+  char buf[512];
+  std::snprintf(buf, sizeof buf, "%s|%d|%s|%s|%d|%d|%d", name.c_str(), pr.multiProcessorCount,
+                fp32 ? "f32" : "f64", c->sc.ns ? "ns" : "eu", lg(c->lay.nreal),
+                lg((long long)c->lay.blks.size()), lg(smallest));
+  return buf;
+}
+
+bool tune_cache_lookup(cns_ctx* c, const std::string& key, int* ti, int* tj, int* kc) {
+  FILE* f = std::fopen(c->tune_cache.c_str(), "r");
+  if (!f) return false;
+  char k[512];
+  int a, b, d;
+  bool found = false;
+  while (std::fscanf(f, "%511s %d %d %d", k, &a, &b, &d) == 4) {
+    if (key == k) {  // the last entry of a key wins
+      *ti = a;
+      *tj = b;
+      *kc = d;
+      found = true;
+    }
+  }
+  std::fclose(f);
+  if (!found) return false;
+  for (int sh = 0; sh < kSweepShapes; ++sh)
+    if (kSweepShape[sh][0] == *ti && kSweepShape[sh][1] == *tj && *kc >= 1) return true;
+  return false;  // an entry this build has no kernel for: tune again
+}
+
 cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
   const cns_state_t& s = c->state;
   Work& w = c->w;
   TileBuf& best = fp32 ? c->tiles32 : c->tiles64;
+  const std::string key = c->tune_cache.empty() ? std::string() : tune_key(c, fp32);
+  {
+    int cti, ctj, ckc;
+    if (!key.empty() && tune_cache_lookup(c, key, &cti, &ctj, &ckc)) {
+      cudaError_t e = build_tiles(c, best, cti, ctj, ckc);
+      if (e == cudaSuccess && fp32) persistent_sweep32(c);
+      if (e == cudaSuccess) {
+        (fp32 ? c->tuned32 : c->tuned64) = true;
+        (fp32 ? c->tune_src32 : c->tune_src64) = 2;
+      }
+      return e;
+    }
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -771,6 +850,11 @@ cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
     for (int kc : kTuneKc) {
       e = build_tiles(c, cand, kSweepShape[sh][0], kSweepShape[sh][1], kc);
       if (e != cudaSuccess) break;
+      if (fp32) {  // timed as it runs: the persistent launch
+        const int per_sm = sweep_f32_blocks_per_sm(cand.ti, cand.tj, !c->sc.ns);
+        cand.sched = per_sm > 0 && c->nsm > 0 ? c->sched32 : nullptr;
+        cand.grid = per_sm * c->nsm;
+      }
       float ms = 0.f;
       if (fp32)
         e = time_sweep<float>(c, cand.view(-1), w.u32, w.v32, w.prim32, w.ps32, w.sn32,
@@ -790,9 +874,18 @@ cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (e == cudaSuccess) e = build_tiles(c, best, bti, btj, bkc);
+  if (e == cudaSuccess && fp32) persistent_sweep32(c);
   if (e == cudaSuccess) {
     (fp32 ? c->tuned32 : c->tuned64) = true;
     (fp32 ? c->tune_ms32 : c->tune_ms64) = best_ms / 3.f;
+    (fp32 ? c->tune_src32 : c->tune_src64) = 1;
+    if (!key.empty()) {
+      FILE* f = std::fopen(c->tune_cache.c_str(), "a");
+      if (f) {
+        std::fprintf(f, "%s %d %d %d\n", key.c_str(), bti, btj, bkc);
+        std::fclose(f);
+      }
+    }
   }
   return e;
 }
@@ -922,6 +1015,9 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
       x[0] = B.ni + 1; x[1] = B.nj + 1; x[2] = B.nk + 1; });
   if (e == cudaSuccess) e = build_tiles(c, c->tiles64, 32, 8, 8);
   if (e == cudaSuccess) e = build_tiles(c, c->tiles32, 32, 8, 8);
+  if (e == cudaSuccess) e = dev_alloc(c, &c->sched32, 2);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
+  if (e == cudaSuccess) persistent_sweep32(c);
   if (e == cudaSuccess) e = build_tiles(c, c->tiles_res, kResTI, kResTJ, kResKC);
   if (e == cudaSuccess) e = init_jacobi_25d();
   for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
@@ -1114,6 +1210,7 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
     CK(cudaMemcpy(c->d_blks, c->lay.blks.data(), sizeof(Blk) * c->lay.blks.size(),
                   cudaMemcpyHostToDevice));
   drop_graphs(c);
+  persistent_sweep32(c);  // the Euler and Navier-Stokes instantiations differ
   c->mixed_iter = 0;  // a new scheme restarts the defect refresh schedule
   if (c->w.ld > 0) CK(ensure_hllc_v(c));
   return CNS_OK;
@@ -1976,7 +2073,13 @@ int cns_sweep_tiles(cns_ctx* c, int precision, int32_t* cfg) {
   cfg[0] = t.ti;
   cfg[1] = t.tj;
   cfg[2] = t.kc;
-  cfg[3] = precision == 0 ? c->tuned64 : c->tuned32;
+  cfg[3] = precision == 0 ? c->tune_src64 : c->tune_src32;
+  return CNS_OK;
+}
+
+int cns_set_tune_cache(cns_ctx* c, const char* path) {
+  if (!c) return CNS_EINVAL;
+  c->tune_cache = path ? path : "";
   return CNS_OK;
 }
 
@@ -1988,7 +2091,9 @@ int cns_set_sweep_tiles(cns_ctx* c, int precision, int ti, int tj, int kc) {
   if (!ok) return fail(c, CNS_EINVAL, "sweep patch shape not one of 32x4, 32x8, 16x8, 16x16");
   CK(cudaStreamSynchronize(c->st));
   CK(build_tiles(c, precision == 0 ? c->tiles64 : c->tiles32, ti, tj, kc));
+  if (precision != 0) persistent_sweep32(c);
   (precision == 0 ? c->tuned64 : c->tuned32) = true;
+  (precision == 0 ? c->tune_src64 : c->tune_src32) = 0;
   drop_graphs(c);
   return CNS_OK;
 }

@@ -66,6 +66,11 @@ struct Tiles {
   int ntiles;
   int kc;
   int ti, tj;  // patch shape (selects the kernel instantiation)
+  // persistent launch (kernels that support it): when sched is set, grid
+  // CTAs (at most ntiles) pull tiles from the work list through the counter
+  // pair sched[0..1], which the last CTA to finish resets to zero
+  int* sched;
+  int grid;
 };
 
 // boundary tables (per boundary, then per list entry)

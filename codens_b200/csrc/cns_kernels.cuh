@@ -91,12 +91,16 @@ struct TileBuf {
   int ti = 0, tj = 0, kc = 0, ntiles = 0;
   std::vector<int> blk_tile0;  // first tile of each block, size nblk+1
   int4* d_tile = nullptr;
+  int* sched = nullptr;  // persistent launch: tile counter pair (device), else null
+  int grid = 0;          // persistent launch: resident CTAs of the whole GPU
   Tiles view(int l0 = -1) const {
     Tiles t;
     t.tile = d_tile;
     t.kc = kc;
     t.ti = ti;
     t.tj = tj;
+    t.sched = sched;
+    t.grid = grid;
     if (l0 < 0) {
       t.tile0 = 0;
       t.ntiles = ntiles;
@@ -346,6 +350,8 @@ cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, 
 // raise the dynamic shared-memory limit of every 2.5D instantiation (once
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();
+// resident CTAs per SM of the FP32 sweep kernel of patch ti x tj (persistent launch size)
+int sweep_f32_blocks_per_sm(int ti, int tj, int eu);
 cudaError_t init_jacobi_25d_float();
 
 inline cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,

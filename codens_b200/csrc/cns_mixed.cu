@@ -262,18 +262,17 @@ constexpr size_t sweep_f32_smem() {
          sizeof(float) * 2 * kRawF32 * (TI + 2) * (TJ + 2);
 }
 
+// one tile (patch t of a block, kc planes) of the sweep
 template <bool EU, int TI, int TJ>
-__global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
-    const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
-    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ prim,
-    const float* __restrict__ ps, const float* __restrict__ sn, const float* __restrict__ coefe,
-    const float* __restrict__ coefdiag, const float* __restrict__ d_in,
-    float* __restrict__ d_out) {
+__device__ __forceinline__ void sweep_f32_tile(
+    const int4 t, const Blk* __restrict__ blks, const Tiles& tl, Phys ph64, int qfix,
+    long long ld, const float* __restrict__ u, const float* __restrict__ v,
+    const float* __restrict__ prim, const float* __restrict__ ps, const float* __restrict__ sn,
+    const float* __restrict__ coefe, const float* __restrict__ coefdiag,
+    const float* __restrict__ d_in, float* __restrict__ d_out, unsigned char* smem_raw) {
   constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ, NR = kRawF32;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sq = reinterpret_cast<float4*>(smem_raw);    // [2 planes][4 quads][NP]
   float* sraw = reinterpret_cast<float*>(sq + 2 * 4 * NP);  // [2 planes][NR][NP]
-  const int4 t = tl.tile[tl.tile0 + blockIdx.x];
   const Blk B = blks[t.x];
   const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
   const int i = t.y + tx, j = t.z + ty;
@@ -429,17 +428,58 @@ __global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
   cp_async_wait<0>();
 }
 
+// The sweep over the tile list.  With tl.sched set it is a persistent
+// launch: tl.grid CTAs take tiles in turn from the counter sched[0] (each
+// tile's result does not depend on the CTA that runs it), and the last CTA
+// to finish resets the counter pair for the next launch on the stream.
+// Without it, one CTA per tile.
+template <bool EU, int TI, int TJ>
+__global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
+    const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
+    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ prim,
+    const float* __restrict__ ps, const float* __restrict__ sn, const float* __restrict__ coefe,
+    const float* __restrict__ coefdiag, const float* __restrict__ d_in,
+    float* __restrict__ d_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (!tl.sched) {
+    sweep_f32_tile<EU, TI, TJ>(tl.tile[tl.tile0 + blockIdx.x], blks, tl, ph64, qfix, ld, u, v,
+                               prim, ps, sn, coefe, coefdiag, d_in, d_out, smem_raw);
+    return;
+  }
+  __shared__ int s_next;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(&tl.sched[0], 1);
+    __syncthreads();
+    const int tt = s_next;
+    __syncthreads();  // every thread has read s_next before it is taken again
+    if (tt >= tl.ntiles) break;
+    sweep_f32_tile<EU, TI, TJ>(tl.tile[tl.tile0 + tt], blks, tl, ph64, qfix, ld, u, v, prim,
+                               ps, sn, coefe, coefdiag, d_in, d_out, smem_raw);
+    __syncthreads();  // the shared buffers are free for the next tile
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    // every other CTA has taken its last tile before counting itself out
+    if (atomicAdd(&tl.sched[1], 1) == (int)gridDim.x - 1) {
+      atomicExch(&tl.sched[0], 0);
+      atomicExch(&tl.sched[1], 0);
+    }
+  }
+}
+
 template <int TI, int TJ>
 cudaError_t sweep_f32_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu, long long ld,
                             const float* u, const float* v, const float* prim, const float* ps,
                             const float* sn, const float* coefe, const float* coefdiag,
                             const float* d_in, float* d_out, cudaStream_t st) {
   constexpr size_t sm = sweep_f32_smem<TI, TJ>();
+  const int grid = tl.sched ? min(tl.grid, tl.ntiles) : tl.ntiles;
+  if (grid <= 0) return cudaErrorInvalidValue;
   if (eu)
-    k_sweep_f32<true, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+    k_sweep_f32<true, TI, TJ><<<grid, TI * TJ, sm, st>>>(
         blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
   else
-    k_sweep_f32<false, TI, TJ><<<tl.ntiles, TI * TJ, sm, st>>>(
+    k_sweep_f32<false, TI, TJ><<<grid, TI * TJ, sm, st>>>(
         blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
   return cudaGetLastError();
 }
@@ -475,6 +515,27 @@ cudaError_t launch_jacobi_25d_t<float>(const Blk* blks, Tiles tl, Phys ph, int q
   CNS_SHAPE(16, 16)
 #undef CNS_SHAPE
   return cudaErrorInvalidValue;
+}
+
+// resident CTAs per SM of the FP32 sweep with patch ti x tj (0: unknown shape)
+int sweep_f32_blocks_per_sm(int ti, int tj, int eu) {
+  int n = 0;
+#define CNS_OCC(A, B)                                                                      \
+  if (ti == A && tj == B) {                                                                \
+    if (eu)                                                                                \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_f32<true, A, B>, A * B,   \
+                                                    sweep_f32_smem<A, B>());               \
+    else                                                                                   \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_f32<false, A, B>, A * B,  \
+                                                    sweep_f32_smem<A, B>());               \
+    return n;                                                                              \
+  }
+  CNS_OCC(32, 4)
+  CNS_OCC(32, 8)
+  CNS_OCC(16, 8)
+  CNS_OCC(16, 16)
+#undef CNS_OCC
+  return 0;
 }
 
 cudaError_t init_jacobi_25d_float() {

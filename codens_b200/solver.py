@@ -206,6 +206,13 @@ class CodeNS:
         self._check(self.lib.cns_set_sweep_tiles(self.ctx, precision, ti, tj, kc),
                     "cns_set_sweep_tiles")
 
+    def set_tune_cache(self, path):
+        """the sweep-tiling cache file (None: off); a configuration found there
+        is used without timing"""
+        self._check(self.lib.cns_set_tune_cache(self.ctx, None if path is None
+                                                else str(path).encode()),
+                    "cns_set_tune_cache")
+
     def residual_tiles(self):
         """(ti, tj, kc) of the fused residual, or zeros for the face kernels"""
         cfg = (C.c_int32 * 3)()

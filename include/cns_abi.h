@@ -468,12 +468,20 @@ int cns_sch_dual(cns_ctx *ctx, int l, double *u, const double *v, int icycle,
 /* Jacobi sweep tiling (no counterpart in the reference).  Every sweep after
  * the first runs 2.5D-blocked over patches of ti x tj cell columns, kc
  * planes deep.  The first fused iteration of each precision tunes the tiling
- * on its own data (FP64 results do not depend on it).  cns_sweep_tiles
- * returns {ti, tj, kc, tuned} of precision 0 (FP64) or 1/2 (FP32 sweeps);
- * cns_set_sweep_tiles fixes a tiling (ti x tj one of 32x4, 32x8, 16x8,
- * 16x16; kc >= 1) and marks it tuned. */
+ * on its own data (no result depends on it: the FP32 sweeps round every
+ * operation explicitly).  cns_sweep_tiles returns {ti, tj, kc, source} of
+ * precision 0 (FP64) or 1/2 (FP32 sweeps), source 0 = the default or a tiling
+ * set by cns_set_sweep_tiles, 1 = timed on the data, 2 = read from the tuning
+ * cache; cns_set_sweep_tiles fixes a tiling (ti x tj one of 32x4, 32x8, 16x8,
+ * 16x16; kc >= 1).  cns_set_tune_cache names a text file of tuned tilings,
+ * one line "key ti tj kc" per (GPU name, SM count, sweep precision,
+ * equations, log2 real cells, log2 blocks, log2 cells of the smallest block):
+ * a configuration found there is used without timing (the same tiling on
+ * every run with that file), a new one is timed and appended; NULL or ""
+ * turns the cache off. */
 int cns_sweep_tiles(cns_ctx *ctx, int precision, int32_t *cfg);
 int cns_set_sweep_tiles(cns_ctx *ctx, int precision, int ti, int tj, int kc);
+int cns_set_tune_cache(cns_ctx *ctx, const char *path);
 /* Residual kernel variant (no counterpart in the reference): ti = 0 selects
  * the face kernels (one launch per direction into a face buffer, then the
  * per-cell accumulation); ti x tj = 32 x 4 or 16 x 8 selects the fused kernel

@@ -66,7 +66,7 @@ def test_rejects_unknown_shape(cuda):
     s.close()
 
 
-@pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu", "box_pinfl"])
+@pytest.mark.parametrize("name", ["box_ns", "channel", "box_eu_qfix", "box_pinfl"])
 def test_fused_residual_variant_gives_the_same_bits(cuda, name):
     """the fused residual kernel (three face directions and the accumulation
     in one 2.5D launch) against the face kernels + accumulation: the same
@@ -86,3 +86,37 @@ def test_fused_residual_variant_gives_the_same_bits(cuda, name):
             v = s.v.cpu().numpy().reshape(5, case.layout.ld)[:, real(case)]
             s.close()
             assert_equal_bits(v, ref, f"fused residual {ti}x{tj}x{kc}")
+
+
+def test_tuning_cache(cuda, tmp_path):
+    """the first context times the sweep tilings and appends its pick to the
+    cache file; a second context of the same configuration reads it (no
+    timing) and runs the same tiling; an entry this build has no kernel for
+    is ignored"""
+    from codens_b200.solver import CodeNS
+    path = tmp_path / "tune.txt"
+    picks = []
+    for run in range(2):
+        case = SMALL["channel"]()
+        case.scheme.precision = 1
+        s = CodeNS(case)
+        s.metric()
+        s.set_tune_cache(path)
+        s.atsch_num(2)
+        cfg32 = s.sweep_tiles(1)
+        assert cfg32[3] == (1 if run == 0 else 2), (run, cfg32)
+        picks.append(cfg32[:3])
+        s.close()
+    assert picks[0] == picks[1]
+    lines = path.read_text().split()
+    assert len(lines) == 4 and lines[0].count("|") == 6 and "f32" in lines[0]
+    # an unusable entry (shape without a kernel) for the same key: timed again
+    path.write_text(f"{lines[0]} 8 8 4\n")
+    case = SMALL["channel"]()
+    case.scheme.precision = 1
+    s = CodeNS(case)
+    s.metric()
+    s.set_tune_cache(path)
+    s.atsch_num(1)
+    assert s.sweep_tiles(1)[3] == 1
+    s.close()
