@@ -147,6 +147,11 @@ class _Maps:
                 m0, mm = ba["mpb"][q], ba["mmb"][q]
                 part_in[m0:m0 + mm] = ba["ncin"][ba["mpb"][p]:ba["mpb"][p] + mm]
         self.part_in = L(part_in)
+        # list-entry ranges of the boundaries: within one boundary the
+        # interior cells (and the partner's) are distinct, so a scatter-add
+        # per boundary has no colliding indices and a fixed summation order
+        self.bnd_ranges = [(int(ba["mpb"][q]), int(ba["mpb"][q] + ba["mmb"][q]),
+                            bool(ba["type"][q] == cases.BC_RC)) for q in range(nb)]
         self.face = ba["face"][ent_b]
         self.sel = {k: L(np.flatnonzero(self.kind == k)) for k in
                     (cases.BC_RC, cases.BC_PARA, cases.BC_IDD, cases.BC_PRD, cases.BC_EXTR)}
@@ -454,8 +459,12 @@ class WallForceGradient:
         out = wb[:5] + wb[5:6] * self.dp_dW
         g = torch.cat([wb[:5, M.ncbd], wb[5:6, M.ncbd]], 0)           # (6, nl)
         back = torch.einsum("eoi,oe->ie", self.bcJ, g)                # (10, nl)
-        out = out.index_add(1, M.ncin, back[:5])
-        out = out.index_add(1, M.part_in, back[5:])
+        # boundary by boundary (an atomic scatter over all entries would sum
+        # the two contributions of a block-corner cell in a varying order)
+        for m0, m1, rc in M.bnd_ranges:
+            out = out.index_add(1, M.ncin[m0:m1], back[:5, m0:m1])
+            if rc:
+                out = out.index_add(1, M.part_in[m0:m1], back[5:, m0:m1])
         res = torch.zeros_like(out)
         res[:, M.real] = out[:, M.real]
         return res
@@ -612,8 +621,10 @@ class CheckpointedGradient(WallForceGradient):
     lambda after N of its iterations, so the gradient tends to
     WallForceGradient's; for a history that has not converged it is the
     derivative of the truncated iteration with the implicit phase frozen.
-    The start state is held fixed.  The result does not depend on `every`
-    (the recomputed states are the forward run's, bit for bit)."""
+    The start state is held fixed.  The adjoint states do not depend on
+    `every` (the recomputed states are the forward run's, bit for bit); the
+    parameter gradients agree to rounding (torch's scatter-adds into the wall
+    nodes sum in a varying order)."""
 
     def __init__(self, design: Design, mach: float, alpha: float, wall: np.ndarray,
                  n_iter: int, every: int, start=None):

@@ -156,7 +156,7 @@ def test_gradient_matches_finite_differences_of_the_oracle(cuda):
 
 def test_checkpointed_reverse_accumulation_independent_of_interval(cuda):
     """pseudo-time checkpointing: the reverse sweep over 12 iterations from
-    the initial state gives the same gradient bit for bit whether every
+    the initial state gives the same adjoint states bit for bit whether every
     state, every fifth or only the first is kept (the recomputed states are
     the forward run's), with at most N/every + every states held"""
     from codens_b200 import adjoint
@@ -165,12 +165,19 @@ def test_checkpointed_reverse_accumulation_independent_of_interval(cuda):
     for every in (1, 5, 12):
         g = adjoint.CheckpointedGradient(d, d.mach, d.alpha, d.wall(), n_iter=12, every=every)
         J, gm, ga, gw = g.gradient()
-        out.append((J, gm, ga, gw.cpu().numpy()))
+        out.append((J, gm, ga, gw.cpu().numpy(), g.mu_sum.cpu().numpy()))
         assert g.max_states <= (12 + every - 1) // every + every, (every, g.max_states)
         g.close()
-    for J, gm, ga, gw in out[1:]:
-        assert (J, gm, ga) == out[0][:3]
-        assert np.array_equal(gw, out[0][3])
+    for J, gm, ga, gw, mu in out[1:]:
+        # the state part of the reverse sweep (library kernels and the
+        # boundary chain) is the same bits; the parameter parts go through
+        # torch autograd, whose scatter-adds into the wall nodes sum in a
+        # varying order, so they agree to rounding
+        assert J == out[0][0]
+        assert np.array_equal(mu, out[0][4])
+        assert abs(gm - out[0][1]) <= 1e-13 * abs(out[0][1])
+        assert abs(ga - out[0][2]) <= 1e-12 * max(abs(out[0][2]), 1e-3 * abs(out[0][1]))
+        assert np.abs(gw - out[0][3]).max() <= 1e-13 * np.abs(out[0][3]).max()
     assert np.isfinite(out[0][1]) and np.isfinite(out[0][3]).all()
 
 
