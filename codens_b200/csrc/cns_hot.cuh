@@ -1211,8 +1211,10 @@ __host__ __device__ constexpr int raw_count(bool eu) {
   return FORM == 1 ? 11 : (eu ? 11 : 14);
 }
 
+// 128-thread patches fit three CTAs per SM (shared memory ~60-67 KB each):
+// registers capped to match
 template <class T, bool EU, int FORM, int TI, int TJ>
-__global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
+__global__ void __launch_bounds__(TI * TJ, TI * TJ <= 128 ? 3 : 1) k_jacobi_25d(
     const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
     const T* __restrict__ ps, const T* __restrict__ sn, const T* __restrict__ coefe,
@@ -1221,7 +1223,7 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
   constexpr int NR = raw_count<FORM>(EU);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sdf = reinterpret_cast<T*>(smem_raw);  // [2 planes][14 values][NP]: d, f
-  T* sraw = sdf + 2 * 14 * NP;              // [2 planes][NR inputs][NP]
+  T* sraw = sdf + 2 * 14 * NP;              // [NR inputs][NP]: one staged plane
   const int4 t = tl.tile[tl.tile0 + blockIdx.x];
   const Blk B = blks[t.x];
   const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
@@ -1244,10 +1246,10 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
     colin[rr] = q < NP && ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1;
     col0[rr] = colin[rr] ? cell_index(B, ii, jj, 0) : 0;
   }
-  // the increment inputs of plane kk (patch and ring) into raw buffer b;
+  // the increment inputs of plane kk (patch and ring) into the raw buffer;
   // cells outside the block's real cells are zero-filled
-  auto stage = [&](int kk, int b) {
-    T* r = sraw + b * NR * NP;
+  auto stage = [&](int kk) {
+    T* r = sraw;
     const bool kin = kk >= 1 && kk <= B.nk - 1;
 #pragma unroll
     for (int rr = 0; rr < NQ; ++rr) {
@@ -1275,10 +1277,10 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
       }
     }
   };
-  // increments of the staged plane in raw buffer b into (d, f) buffer b
-  // (zero where the raw inputs are zero: outside the block)
+  // increments of the staged plane kk into (d, f) buffer b (zero where the
+  // raw inputs are zero: outside the block)
   auto fill = [&](int kk, int b) {
-    const T* r = sraw + b * NR * NP;
+    const T* r = sraw;
     T* s = sdf + b * 14 * NP;
     const bool kin = kk >= 1 && kk <= B.nk - 1;
 #pragma unroll
@@ -1320,14 +1322,16 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
 #pragma unroll
     for (int a = 0; a < 9; ++a) pf[a] = T(0.);
   }
-  stage(kbeg, kbeg & 1);
+  // one raw buffer: plane kk+1's inputs are copied in while plane kk-1 is
+  // computed, after plane kk's increments have been filled from it
+  stage(kbeg);
   cp_async_commit();
-  stage(kbeg + 1, (kbeg + 1) & 1);
-  cp_async_commit();
-  cp_async_wait<1>();
+  cp_async_wait<0>();
   __syncthreads();
   fill(kbeg, kbeg & 1);
   __syncthreads();
+  stage(kbeg + 1);
+  cp_async_commit();
   const int q0 = (ty + 1) * NX + tx + 1;
   // the lower k face of plane kbeg; later planes carry it from the plane
   // below (the upper face of cell k is the lower face of cell k+1: the same
@@ -1375,11 +1379,11 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
     }
     cp_async_wait<0>();
     __syncthreads();
-    // plane k+2's inputs go into the raw buffer plane k's used
-    stage(k + 2, k & 1);
-    cp_async_commit();
     fill(k + 1, (k + 1) & 1);
     __syncthreads();
+    // plane k+2's inputs, in flight while plane k is computed
+    stage(k + 2);
+    cp_async_commit();
     const T* s = sdf + (k & 1) * 14 * NP;
     const T* su = sdf + ((k + 1) & 1) * 14 * NP;
     T d0[5], f0[9], dl[5], fl[9], du[5], fu[9], tl[5], tu[5];
@@ -1458,7 +1462,8 @@ __global__ void __launch_bounds__(TI * TJ) k_jacobi_25d(
 
 template <int TI, int TJ, class T, int FORM, bool EU>
 constexpr size_t jacobi_25d_smem() {
-  return sizeof(T) * 2 * (14 + raw_count<FORM>(EU)) * (TI + 2) * (TJ + 2);
+  // two planes of increments (d, f) and one staged plane of raw inputs
+  return sizeof(T) * (2 * 14 + raw_count<FORM>(EU)) * (TI + 2) * (TJ + 2);
 }
 
 template <class T, int FORM, int TI, int TJ>
