@@ -86,6 +86,9 @@ def parse():
                    choices=["channel", "batch", "adjoint", "rans", "dual"],
                    help="channel: the 8-block NS channel; batch: 64 independent Euler boxes "
                         "in one launch against the same boxes one at a time")
+    p.add_argument("--residual-tiles", default=None,
+                   help="TI,TJ,KC: the fused residual kernel with these 2.5D tiles (32,4 or "
+                        "16,8) instead of the face kernels + accumulation")
     p.add_argument("--tune-cache", default=None,
                    help="sweep-tiling cache file: a tiling found there is used without timing")
     p.add_argument("--tiles", default=None,
@@ -132,6 +135,8 @@ def config_of(case, args, n):
         "mach": m.get("mach"), "reynolds": m.get("reynz"), "seed": m.get("seed"),
         "precision": args.precision,
         "ilim": args.ilim,
+        "residual": (f"fused kernel, tiles {args.residual_tiles}" if args.residual_tiles
+                     else "face kernels + accumulation"),
         "flux": args.flux,
         "eta": args.eta,
         "l2_flush": "inputs larger than L2 (state and scratch ~GBs)",
@@ -394,6 +399,8 @@ def run_ours(args):
     s.metric()
     if args.tune_cache:
         s.set_tune_cache(args.tune_cache)
+    if args.residual_tiles:
+        s.set_residual_tiles(*(int(x) for x in args.residual_tiles.split(",")))
     if args.tiles:
         ti, tj, kc = (int(x) for x in args.tiles.split(","))
         s.set_sweep_tiles(PRECISION[args.precision], ti, tj, kc)

@@ -205,3 +205,33 @@ def test_checkpointed_gradient_equals_the_steady_adjoint_truncation(cuda):
     assert abs(gac - gas) <= 1e-8 * max(abs(gas), 1e-3 * abs(gms)), (gac, gas)
     scale = float(torch.as_tensor(gws).abs().max())
     assert float((gwc - gws).abs().max()) <= 1e-8 * scale
+
+
+def test_muscl_gradient_matches_finite_differences(cuda):
+    """the configuration-5 scheme, kappa = -1 MUSCL (sch_roe_euler.f90:137-174),
+    on a channel small enough for its primal to converge (on 128x64x4 and
+    larger the MUSCL iteration settles into a limit cycle at CFL 5): the
+    adjoint linearises the four-cell stencil of every face"""
+    from codens_b200 import adjoint
+    d = adjoint.Design(ni=16, nj=8, nk=2, mach=0.5, alpha=1.0, bump=0.1, muscl=1)
+    g = adjoint.WallForceGradient(d, d.mach, d.alpha, d.wall(), tol=1e-14, max_iter=80000,
+                                  adj_tol=1e-12, adj_max=80000)
+    assert g.l2 < 1e-13, g.l2
+    J, gm, ga, gw = g.gradient()
+    gw = gw.cpu().numpy()
+    g.close()
+
+    def Jat(mach=d.mach, alpha=d.alpha, wall=None):
+        return adjoint.wall_force(d, mach, alpha, d.wall() if wall is None else wall,
+                                  tol=1e-14, max_iter=80000)
+
+    eps = 1e-6
+    fd_m = (Jat(mach=d.mach + eps) - Jat(mach=d.mach - eps)) / (2 * eps)
+    assert abs(gm - fd_m) <= GRAD_TOL * abs(fd_m), (gm, fd_m)
+    w0 = d.wall()
+    for i in (7, 9):
+        wp, wm = w0.copy(), w0.copy()
+        wp[i] += eps
+        wm[i] -= eps
+        fd = (Jat(wall=wp) - Jat(wall=wm)) / (2 * eps)
+        assert abs(gw[i] - fd) <= GRAD_TOL * max(abs(fd), 1e-3), (i, gw[i], fd)
