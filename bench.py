@@ -50,12 +50,12 @@ PRECISION = {"fp64": 0, "mixed": 1, "defect": 2}
 DTYPE = {"fp64": "f64", "mixed": "f64 residual/update, f32 sweeps",
          "defect": "f32 fluxes/sweeps, f64 accumulate/update"}
 SWEEP_KERNEL = {"fp64": "k_jacobi_25d<double> (2.5D point-Jacobi sweep, recomputed increments)",
-                "mixed": "k_jacobi_25d<float> (2.5D point-Jacobi sweep, recomputed increments)",
-                "defect": "k_jacobi_25d<float> (2.5D point-Jacobi sweep, recomputed increments)"}
+                "mixed": "k_sweep_f32 (persistent 2.5D point-Jacobi sweep, FP32 increments)",
+                "defect": "k_sweep_f32 (persistent 2.5D point-Jacobi sweep, FP32 increments)"}
 # DRAM bytes per cell of one 2.5D sweep launch, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 1.18M-cell channel;
 # traffic grows with the cells processed, so a full launch is this x cells
-SWEEP_TRAFFIC_PER_CELL = {"fp64": 326.3, "mixed": 144.4, "defect": 144.4}
+SWEEP_TRAFFIC_PER_CELL = {"fp64": 326.4, "mixed": 146.6, "defect": 146.6}
 FALLBACK_HBM_GBS = 6650.0
 
 
