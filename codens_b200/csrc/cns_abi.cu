@@ -190,6 +190,7 @@ void persistent_sweep32(cns_ctx* c) {
   const int per_sm = sweep_f32_blocks_per_sm(c->tiles32.ti, c->tiles32.tj, !c->sc.ns);
   c->tiles32.sched = (c->sched32 && per_sm > 0 && c->nsm > 0) ? c->sched32 : nullptr;
   c->tiles32.grid = per_sm * c->nsm;
+  c->tiles32.faces = c->w.snc32;
 }
 
 bool bad_block(cns_ctx* c, int l) { return l < 0 || l > (int)c->lay.blks.size(); }
@@ -644,7 +645,20 @@ cudaError_t ensure_mixed(cns_ctx* c) {
   }
   if (e == cudaSuccess) e = dev_alloc(c, &w.corr, (size_t)(5 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &w.ur32, (size_t)(5 * ld));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.snc32, (size_t)(3 * ld));
   if (e == cudaSuccess) w.mixed_ready = true;
+  c->tiles32.faces = w.snc32;
+  return e;
+}
+
+// the FP32 face areas of the bound state's sn and the face lanes of the FP32
+// sweep's pack
+cudaError_t refresh_sn32(cns_ctx* c, const double* sn) {
+  cudaError_t e = launch_to_float(sn, c->w.sn32, 9 * c->lay.ld, c->st);
+  if (e == cudaSuccess)
+    e = launch_pack_faces32(c->d_blks, (int)c->lay.blks.size(), c->lay.ncells, c->w.sn32,
+                            c->w.snc32, c->st);
+  c->tiles32.faces = c->w.snc32;
   return e;
 }
 
@@ -729,7 +743,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     e = launch_coefficients32(c->d_blks, all, c->ph, !c->sc.ns, ld,
                               c->sc.kfmg == 3 ? c->sc.dt1min : 0., s.dt, s.v, w.prim32,
                               s.mu, s.mut, w.sn32, s.vol, s.cson, w.coefe32, w.coefdiag32,
-                              c->st);
+                              w.snc32, c->st);
   int cur = 0;
   if (e == cudaSuccess)
     e = launch_sweeps_t<float>(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
@@ -854,6 +868,7 @@ cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
         const int per_sm = sweep_f32_blocks_per_sm(cand.ti, cand.tj, !c->sc.ns);
         cand.sched = per_sm > 0 && c->nsm > 0 ? c->sched32 : nullptr;
         cand.grid = per_sm * c->nsm;
+        cand.faces = w.snc32;
       }
       float ms = 0.f;
       if (fp32)
@@ -1227,7 +1242,7 @@ int cns_metric(cns_ctx* c, double* x, double* y, double* z, double* sn,
   if (!c || !x || !y || !z || !sn || !vol) return CNS_EINVAL;
   CK(launch_metric(c->lay, c->d_blks, c->bd, x, y, z, sn, vol, c->st));
   if (c->w.mixed_ready && c->bound && c->state.sn == sn)
-    CK(launch_to_float(sn, c->w.sn32, 9 * c->lay.ld, c->st));
+    CK(refresh_sn32(c, sn));
   CK(cudaStreamSynchronize(c->st));
   c->metric_done = true;
   c->mixed_iter = 0;
@@ -1834,7 +1849,7 @@ int cns_adjoint_prepare(cns_ctx* c) {
     // the reduced-precision form: L^T in FP32 (face areas and coefficients
     // rounded once); A^T lambda stays FP64
     CK(ensure_mixed(c));
-    CK(launch_to_float(s.sn, c->w.sn32, 9 * ld, c->st));
+    CK(refresh_sn32(c, s.sn));
     CK(launch_to_float(c->w.coefe, c->w.coefe32, 3 * ld, c->st));
     CK(launch_to_float(c->w.coefdiag, c->w.coefdiag32, ld, c->st));
   }
@@ -2010,7 +2025,7 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
   const int prec = c->sc.precision;
   if (prec != 0 && !c->w.mixed_ready) {
     CK(ensure_mixed(c));
-    CK(launch_to_float(c->state.sn, c->w.sn32, 9 * c->lay.ld, c->st));
+    CK(refresh_sn32(c, c->state.sn));
   }
   if (jameson(c)) CK(ensure_dis(c));
   // first iteration of a form whose sweeps are not tuned yet, and the first

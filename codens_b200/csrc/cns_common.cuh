@@ -71,6 +71,10 @@ struct Tiles {
   // pair sched[0..1], which the last CTA to finish resets to zero
   int* sched;
   int grid;
+  // the FP32 sweep's per-cell pack (3 float4 per cell: half the area vector
+  // of the cell's lower face of each direction, and that face's implicit
+  // coefficient), or null
+  const float4* faces;
 };
 
 // boundary tables (per boundary, then per list entry)

@@ -93,6 +93,7 @@ struct TileBuf {
   int4* d_tile = nullptr;
   int* sched = nullptr;  // persistent launch: tile counter pair (device), else null
   int grid = 0;          // persistent launch: resident CTAs of the whole GPU
+  const float4* faces = nullptr;  // FP32 sweep face/coefficient pack (Tiles::faces)
   Tiles view(int l0 = -1) const {
     Tiles t;
     t.tile = d_tile;
@@ -101,6 +102,7 @@ struct TileBuf {
     t.tj = tj;
     t.sched = sched;
     t.grid = grid;
+    t.faces = faces;
     if (l0 < 0) {
       t.tile0 = 0;
       t.ntiles = ntiles;
@@ -136,6 +138,7 @@ struct Work {
   float *coefe32 = nullptr, *coefdiag32 = nullptr;
   float* d32pp[2] = {nullptr, nullptr};
   double *corr = nullptr, *ur32 = nullptr;
+  float4* snc32 = nullptr;  // [ld][3]: half lower-face areas and their coefficients
 };
 
 cudaError_t launch_metric(const HostLayout& lay, const Blk* dblks, const Bnd& bd,
@@ -423,7 +426,11 @@ cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu,
                                   const double* dt, const double* v, const float* prim32,
                                   const double* mu, const double* mut, const float* sn32,
                                   const double* vol, const double* cson, float* coefe32,
-                                  float* coefdiag32, cudaStream_t st);
+                                  float* coefdiag32, float4* snc32, cudaStream_t st);
+// the face lanes of the FP32 sweep's pack: snc[3n + dir].xyz = S/2 of cell n's
+// lower face in dir (exact halves of sn32), .w = 0 until k_coef32 writes it
+cudaError_t launch_pack_faces32(const Blk* blks, int nblk, long long ncells, const float* sn32,
+                                float4* snc32, cudaStream_t st);
 // FP64 face fluxes with FMA contraction (the mixed form's residual; agrees
 // with launch_face_flux_t<double> to FP64 rounding, not bit for bit)
 cudaError_t launch_face_flux_fma(const Blk* blks, const SpaceBuf* faces, int l0, Phys ph,

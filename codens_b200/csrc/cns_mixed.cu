@@ -75,11 +75,13 @@ __global__ void __launch_bounds__(kTile) k_coef32(
     const float* __restrict__ prim, const double* __restrict__ mu,
     const double* __restrict__ mut, const float* __restrict__ sn,
     const double* __restrict__ vol, const double* __restrict__ cson,
-    float* __restrict__ coefe, float* __restrict__ coefdiag) {
+    float* __restrict__ coefe, float* __restrict__ coefdiag, float4* __restrict__ snc) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const long long n = cell_index(B, i, j, k);
+  // the coefficient lane of the sweep's face pack: float 4 (3 m + dir) + 3
+  float* const sncw = reinterpret_cast<float*>(snc);
   const float gp = (float)(ph.gam / ph.pr), gpt = (float)(ph.gam / ph.prt);
   auto rv_of = [&](long long m, bool real) -> float {
     if (EU || !real) return 0.f;
@@ -103,6 +105,10 @@ __global__ void __launch_bounds__(kTile) k_coef32(
                                     rv_of(nu, p < nd - 1), rv0);
     coefe[(long long)dir * ld + n] = cel;
     if (p == nd - 1) coefe[(long long)dir * ld + nu] = ceu;
+    if (snc) {
+      sncw[4 * (3 * n + dir) + 3] = cel;
+      if (p == nd - 1) sncw[4 * (3 * nu + dir) + 3] = ceu;
+    }
     cd = cd + cel + ceu;
   }
   if (!EU && dtpas > 0.) cd = cd + (float)(1.5 * vol[n] / dtpas);
@@ -116,16 +122,42 @@ cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu,
                                   const double* dt, const double* v, const float* prim32,
                                   const double* mu, const double* mut, const float* sn32,
                                   const double* vol, const double* cson, float* coefe32,
-                                  float* coefdiag32, cudaStream_t st) {
+                                  float* coefdiag32, float4* snc32, cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
   if (eu)
     k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
                                                      mut, sn32, vol, cson, coefe32,
-                                                     coefdiag32);
+                                                     coefdiag32, snc32);
   else
     k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
                                                       mut, sn32, vol, cson, coefe32,
-                                                      coefdiag32);
+                                                      coefdiag32, snc32);
+  return cudaGetLastError();
+}
+
+namespace {
+// the face lanes of the sweep's pack for every cell of every block
+__global__ void __launch_bounds__(256) k_pack_faces32(const Blk* __restrict__ blks, int nblk,
+                                                     long long ncells,
+                                                     const float* __restrict__ sn,
+                                                     float4* __restrict__ snc) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ncells) return;
+  int b = 0;
+  while (b + 1 < nblk && q >= blks[b + 1].npc) ++b;
+  const Blk& B = blks[b];
+  if (q >= B.npc + B.nnn) return;
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir)
+    snc[3 * q + dir] = make_float4(0.5f * sn_ptr(sn, B, dir, 0)[q], 0.5f * sn_ptr(sn, B, dir, 1)[q],
+                                   0.5f * sn_ptr(sn, B, dir, 2)[q], 0.f);
+}
+}  // namespace
+
+cudaError_t launch_pack_faces32(const Blk* blks, int nblk, long long ncells, const float* sn32,
+                                float4* snc32, cudaStream_t st) {
+  if (ncells > 0)
+    k_pack_faces32<<<(int)((ncells + 255) / 256), 256, 0, st>>>(blks, nblk, ncells, sn32, snc32);
   return cudaGetLastError();
 }
 
@@ -349,12 +381,6 @@ __device__ __forceinline__ void sweep_f32_tile(
 #pragma unroll
     for (int a = 0; a < 9; ++a) pk.f[a] = 0.f;
   }
-  float skl[3] = {0.f, 0.f, 0.f};
-  if (own) {
-    const long long n0 = cell_index(B, i, j, kbeg);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) skl[c] = sn_ptr(sn, B, 2, c)[n0];
-  }
   stage(kbeg, kbeg & 1);
   cp_async_commit();
   stage(kbeg + 1, (kbeg + 1) & 1);
@@ -367,23 +393,22 @@ __device__ __forceinline__ void sweep_f32_tile(
   for (int k = kbeg; k < kend; ++k) {
     // this cell's own inputs, in flight across the barrier
     const long long n = cell_index(B, own ? i : 1, own ? j : 1, k);
-    float uu[5], si[3], siu[3], sj[3], sju[3], sku[3], cel[3], ceu[3], cd = 1.f;
+    // half face areas and face coefficients from the pack (tl.faces): the
+    // cell's three lower faces and the lower faces of its i+1, j+1, k+1
+    // neighbours (its upper faces); 0.5 S is exact, so the sums below equal
+    // the unpacked form's bit for bit
+    float uu[5], cd = 1.f;
+    float4 fi, fj, fk, fiu, fju, fku;
+    fi = fj = fk = fiu = fju = fku = make_float4(0.f, 0.f, 0.f, 0.f);
     if (own) {
 #pragma unroll
       for (int a = 0; a < 5; ++a) uu[a] = u[a * ld + n];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        si[c] = sn_ptr(sn, B, 0, c)[n];
-        siu[c] = sn_ptr(sn, B, 0, c)[n + 1];
-        sj[c] = sn_ptr(sn, B, 1, c)[n];
-        sju[c] = sn_ptr(sn, B, 1, c)[n + B.nid];
-        sku[c] = sn_ptr(sn, B, 2, c)[n + B.nijd];
-      }
-#pragma unroll
-      for (int dir = 0; dir < 3; ++dir) {
-        cel[dir] = coefe[(long long)dir * ld + n];
-        ceu[dir] = coefe[(long long)dir * ld + n + ninc_of(B, dir)];
-      }
+      fi = tl.faces[3 * n];
+      fj = tl.faces[3 * n + 1];
+      fk = tl.faces[3 * n + 2];
+      fiu = tl.faces[3 * (n + 1)];
+      fju = tl.faces[3 * (n + B.nid) + 1];
+      fku = tl.faces[3 * (n + B.nijd) + 2];
       cd = coefdiag[n];
     }
     cp_async_wait<0>();
@@ -401,29 +426,26 @@ __device__ __forceinline__ void sweep_f32_tile(
       float acc[5];
 #pragma unroll
       for (int a = 0; a < 5; ++a) acc[a] = -uu[a];
-      const float h = 0.5f;
       // the cell itself: Phi(c) . (sum of lower minus upper areas) / 2
-      phi_acc(c0, h * ((si[0] - siu[0]) + (sj[0] - sju[0]) + (skl[0] - sku[0])),
-              h * ((si[1] - siu[1]) + (sj[1] - sju[1]) + (skl[1] - sku[1])),
-              h * ((si[2] - siu[2]) + (sj[2] - sju[2]) + (skl[2] - sku[2])), 0.f, acc);
+      phi_acc(c0, (fi.x - fiu.x) + (fj.x - fju.x) + (fk.x - fku.x),
+              (fi.y - fiu.y) + (fj.y - fju.y) + (fk.y - fku.y),
+              (fi.z - fiu.z) + (fj.z - fju.z) + (fk.z - fku.z), 0.f, acc);
       quad_load(s, NP, q0 - 1, x);
-      phi_acc(x, h * si[0], h * si[1], h * si[2], cel[0], acc);
+      phi_acc(x, fi.x, fi.y, fi.z, fi.w, acc);
       quad_load(s, NP, q0 + 1, x);
-      phi_acc(x, -h * siu[0], -h * siu[1], -h * siu[2], ceu[0], acc);
+      phi_acc(x, -fiu.x, -fiu.y, -fiu.z, fiu.w, acc);
       quad_load(s, NP, q0 - NX, x);
-      phi_acc(x, h * sj[0], h * sj[1], h * sj[2], cel[1], acc);
+      phi_acc(x, fj.x, fj.y, fj.z, fj.w, acc);
       quad_load(s, NP, q0 + NX, x);
-      phi_acc(x, -h * sju[0], -h * sju[1], -h * sju[2], ceu[1], acc);
-      phi_acc(pk, h * skl[0], h * skl[1], h * skl[2], cel[2], acc);
+      phi_acc(x, -fju.x, -fju.y, -fju.z, fju.w, acc);
+      phi_acc(pk, fk.x, fk.y, fk.z, fk.w, acc);
       quad_load(su, NP, q0, x);
-      phi_acc(x, -h * sku[0], -h * sku[1], -h * sku[2], ceu[2], acc);
+      phi_acc(x, -fku.x, -fku.y, -fku.z, fku.w, acc);
       const float rc = 1.f / cd;
 #pragma unroll
       for (int a = 0; a < 5; ++a) d_out[a * ld + n] = acc[a] * rc;
     }
     pk = c0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) skl[c] = own ? sku[c] : 0.f;
   }
   cp_async_wait<0>();
 }
@@ -474,7 +496,7 @@ cudaError_t sweep_f32_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu
                             const float* d_in, float* d_out, cudaStream_t st) {
   constexpr size_t sm = sweep_f32_smem<TI, TJ>();
   const int grid = tl.sched ? min(tl.grid, tl.ntiles) : tl.ntiles;
-  if (grid <= 0) return cudaErrorInvalidValue;
+  if (grid <= 0 || !tl.faces) return cudaErrorInvalidValue;
   if (eu)
     k_sweep_f32<true, TI, TJ><<<grid, TI * TJ, sm, st>>>(
         blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
