@@ -599,31 +599,34 @@ def run_batch(args):
         out[name] = {"value": nreal * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
                      "kernels_per_step": None}
         s.close()
-    # one at a time, FP64: every box in its own context, all on one stream so
-    # that the boxes run one after the other, each its own graph-launched
-    # iteration; timed on that stream from the first launch to the last
-    members = [cases.batch_member(bt, ib) for ib in range(bt.layout.nblk)]
-    one_stream = torch.cuda.Stream()
-    solvers = []
-    for m in members:
-        m.scheme.precision = 0
-        sm = CodeNS(m, stream=one_stream)
-        sm.metric()
-        sm.atsch_num(warm)
-        solvers.append(sm)
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(one_stream)
-    for _ in range(steps):
+    def one_at_a_time(prec):
+        # every box in its own context, all on one stream so that the boxes
+        # run one after the other, each its own graph-launched iteration
+        members = [cases.batch_member(bt, ib) for ib in range(bt.layout.nblk)]
+        one_stream = torch.cuda.Stream()
+        solvers = []
+        for m in members:
+            m.scheme.precision = prec
+            sm = CodeNS(m, stream=one_stream)
+            sm.metric()
+            sm.atsch_num(warm)
+            solvers.append(sm)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(one_stream)
+        for _ in range(steps):
+            for sm in solvers:
+                sm.atsch_num_launch(1)
+        t1.record(one_stream)
+        t1.synchronize()
+        ms1 = t0.elapsed_time(t1)
         for sm in solvers:
-            sm.atsch_num_launch(1)
-    t1.record(one_stream)
-    t1.synchronize()
-    ms1 = t0.elapsed_time(t1)
-    for sm in solvers:
-        sm.close()
-    one = {"value": nreal * steps / (ms1 * 1e-3) / 1e6, "ms_per_step": ms1 / steps}
+            sm.close()
+        return {"value": nreal * steps / (ms1 * 1e-3) / 1e6, "ms_per_step": ms1 / steps}
+
+    one = one_at_a_time(0)
+    one_mixed = one_at_a_time(1)
     line = {
         "metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1,
         "steps": steps, "warmup": warm, "ms_per_step": out["mixed"]["ms_per_step"],
@@ -637,7 +640,9 @@ def run_batch(args):
                    "l2_flush": "inputs larger than L2 (~17M cells)"},
         "batched_fp64": out["fp64"], "batched_mixed": out["mixed"],
         "one_at_a_time_fp64": one,
+        "one_at_a_time_mixed": one_mixed,
         "batched_over_one_at_a_time": out["fp64"]["value"] / one["value"],
+        "batched_over_one_at_a_time_mixed": out["mixed"]["value"] / one_mixed["value"],
         "mixed_batched_over_one_at_a_time_fp64": out["mixed"]["value"] / one["value"],
     }
     print(json.dumps(line), flush=True)
