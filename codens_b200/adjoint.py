@@ -147,11 +147,24 @@ class _Maps:
                 m0, mm = ba["mpb"][q], ba["mmb"][q]
                 part_in[m0:m0 + mm] = ba["ncin"][ba["mpb"][p]:ba["mpb"][p] + mm]
         self.part_in = L(part_in)
-        # list-entry ranges of the boundaries: within one boundary the
-        # interior cells (and the partner's) are distinct, so a scatter-add
-        # per boundary has no colliding indices and a fixed summation order
-        self.bnd_ranges = [(int(ba["mpb"][q]), int(ba["mpb"][q] + ba["mmb"][q]),
-                            bool(ba["type"][q] == cases.BC_RC)) for q in range(nb)]
+        # the boundary entries' scatter targets in layers with distinct cells
+        # (a cell's first entry in list order in layer 0, its second in
+        # layer 1, ...; only block corners and edges have more than one), so
+        # every layer is a scatter-add without colliding indices and the
+        # layers add in a fixed order: deterministic sums
+        def layers(dest, use):
+            seen = {}
+            lay_of = np.full(len(dest), -1)
+            for e in np.flatnonzero(use):
+                c = int(dest[e])
+                lay_of[e] = seen.get(c, 0)
+                seen[c] = lay_of[e] + 1
+            return [L(np.flatnonzero(lay_of == q)) for q in range(int(lay_of.max()) + 1)]
+        self.in_layers = layers(ba["ncin"], np.ones(len(ent_b), bool))
+        self.part_layers = layers(part_in, ba["type"][ent_b] == cases.BC_RC)
+        ghost = np.ones(self.ld, bool)
+        ghost[lay.real_cells()] = False
+        self.not_real = L(ghost)
         self.face = ba["face"][ent_b]
         self.sel = {k: L(np.flatnonzero(self.kind == k)) for k in
                     (cases.BC_RC, cases.BC_PARA, cases.BC_IDD, cases.BC_PRD, cases.BC_EXTR)}
@@ -459,15 +472,13 @@ class WallForceGradient:
         out = wb[:5] + wb[5:6] * self.dp_dW
         g = torch.cat([wb[:5, M.ncbd], wb[5:6, M.ncbd]], 0)           # (6, nl)
         back = torch.einsum("eoi,oe->ie", self.bcJ, g)                # (10, nl)
-        # boundary by boundary (an atomic scatter over all entries would sum
-        # the two contributions of a block-corner cell in a varying order)
-        for m0, m1, rc in M.bnd_ranges:
-            out = out.index_add(1, M.ncin[m0:m1], back[:5, m0:m1])
-            if rc:
-                out = out.index_add(1, M.part_in[m0:m1], back[5:, m0:m1])
-        res = torch.zeros_like(out)
-        res[:, M.real] = out[:, M.real]
-        return res
+        # layer by layer (one atomic scatter over all entries would sum the
+        # two contributions of a block-corner cell in a varying order)
+        for e in M.in_layers:
+            out = out.index_add(1, M.ncin[e], back[:5, e])
+        for e in M.part_layers:
+            out = out.index_add(1, M.part_in[e], back[5:, e])
+        return out.masked_fill(M.not_real, 0.0)
 
     def value_and_partials(self):
         """J and its explicit derivatives (state at real cells, wall nodes,
