@@ -74,7 +74,7 @@ EXPORTS = [
     "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
     "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
     "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
-    "cns_set_sa", "cns_met_num",
+    "cns_set_sa", "cns_met_num", "cns_lpsa", "cns_cllparoi1",
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
     "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
     "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov", "cns_sch_ausmp",
@@ -154,6 +154,8 @@ def load(build_if_missing: bool = True):
     L.cns_met_cutsa.argtypes = [vp, C.c_int, vp, c_f64]
     L.cns_set_sa.argtypes = [vp, P(Sa_t)]
     L.cns_met_num.argtypes = [vp]
+    L.cns_lpsa.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_cllparoi1.argtypes = [vp] * 7
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_set_residual_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     L.cns_set_tune_cache.argtypes = [vp, C.c_char_p]

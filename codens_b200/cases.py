@@ -35,6 +35,7 @@ from .layout import Layout
 # boundary kinds (rbord.f90:144-424): extr, rc (coincident join), para
 # (adiabatic wall), idd (injection), prd (imposed pressure)
 BC_EXTR, BC_RC, BC_PARA, BC_IDD, BC_PRD = 1, 2, 3, 4, 5
+BC_LP2 = 6  # adiabatic wall with the wall law ('lp2': rbord.f90:374-388)
 FACES = {"i1": 0, "i2": 1, "j1": 2, "j2": 3, "k1": 4, "k2": 5}
 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
@@ -380,7 +381,7 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
                  eta: float = 5.0, ilim: int = 1, bump: float = 0.1,
                  length: float = 8.0, span: float = 0.5, walls: bool = True,
                  ischema: int = 7, alpha: float = 0.0, wall=None,
-                 name: str = "channel") -> Case:
+                 wall_kind: int = BC_PARA, name: str = "channel") -> Case:
     """Bump channel: blocks along x joined by coincident faces.
 
     Lower wall y_w(x) = bump*exp(-((x-x_c)/0.25)^2) with x_c at mid-length,
@@ -393,7 +394,7 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     steady state is the uniform flow set by the inlet and outlet values).
     alpha: inlet flow angle in the x-y plane (degrees); wall: the lower-wall
     height of every node column along x (sum(ni_cells) + 1 values) instead
-    of the bump formula.
+    of the bump formula; wall_kind: BC_LP2 gives both walls the wall law.
     """
     if ni_cells is None:
         ni_cells, nj_cells, nk_cells, seed = channel_dims(seed=seed)
@@ -441,8 +442,8 @@ def channel_case(ni_cells: Optional[Sequence[int]] = None, nj_cells: int = 0,
     bnd.append(Boundary(nblk - 1, "i2", BC_PRD, values=(p_inf,)))
     for ib in range(nblk):
         if walls:
-            bnd.append(Boundary(ib, "j1", BC_PARA))
-            bnd.append(Boundary(ib, "j2", BC_PARA))
+            bnd.append(Boundary(ib, "j1", wall_kind))
+            bnd.append(Boundary(ib, "j2", wall_kind))
         else:
             a = len(bnd)
             bnd.append(Boundary(ib, "j1", BC_RC, partner=a + 1))
@@ -466,6 +467,7 @@ def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e
                     dy1: float = 1.0e-5, ratio: float = 1.1, length: float = 1.0,
                     span: float = 0.1, nut_ratio: float = 3.0, seed: int = 3,
                     noise: float = 0.0, lmax: int = 10, eta: float = 5.0,
+                    wall_kind: int = BC_PARA, side_walls: bool = False,
                     name: str = "flat_plate") -> Case:
     """RANS flat plate: one block of cells[0] x cells[1] x cells[2] cells.
 
@@ -481,7 +483,9 @@ def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e
     With the reference's Spalart-Allmaras source the iteration of the
     full-size plate fails once S~ (negative in the freestream, where fv2 < 0)
     crosses zero at some cell; run it with the flagged source fix
-    (CodeNS.set_sa(..., stilde_fix=1)).
+    (CodeNS.set_sa(..., stilde_fix=1)).  wall_kind: BC_LP2 puts the wall law
+    on the plate; side_walls: the k faces are walls of that kind too instead
+    of periodic (cells along the corners then have two walls).
     """
     ni, nj, nk = (c + 1 for c in cells)
     lay = Layout.from_dims([(ni, nj, nk)])
@@ -509,8 +513,11 @@ def flat_plate_case(cells=(256, 128, 64), mach: float = 0.3, reynz: float = 1.0e
     v0[5, b.npc:b.npc + b.nnn] = rokinf * (1.0 + noise * (2.0 * r - 1.0))
     bnd = [Boundary(0, "i1", BC_IDD, values=(1.0, 1.0, 1.0, 0.0, 0.0)),
            Boundary(0, "i2", BC_PRD, values=(st[4],)),
-           Boundary(0, "j1", BC_PARA), Boundary(0, "j2", BC_EXTR),
-           Boundary(0, "k1", BC_RC, partner=5), Boundary(0, "k2", BC_RC, partner=4)]
+           Boundary(0, "j1", wall_kind), Boundary(0, "j2", BC_EXTR)]
+    if side_walls:
+        bnd += [Boundary(0, "k1", wall_kind), Boundary(0, "k2", wall_kind)]
+    else:
+        bnd += [Boundary(0, "k1", BC_RC, partner=5), Boundary(0, "k2", BC_RC, partner=4)]
     return Case(name, lay, phys, scheme, bnd, x, y, z, v0,
                 meta=dict(mach=mach, reynz=reynz, seed=seed, cells=tuple(cells), dy1=dy1,
                           ratio=ratio, length=length, span=span, rokinf=rokinf,

@@ -38,6 +38,14 @@ struct cns_ctx {
   double* sa_cfke = nullptr;        // source-derivative bound [ld]
   long long n_wall_ent = 0;
   long long* d_wall_ents = nullptr;  // list entries of the wall boundaries
+  // the wall-law walls 'lp2' in list order: first list entry, count, block
+  struct Lp2 {
+    long long e0;
+    int cnt, blk;
+  };
+  std::vector<Lp2> lp2;
+  long long* d_lp2_ni = nullptr;  // their first cells (no SA increment there)
+  long long n_lp2_ni = 0;
   double* wall_par = nullptr;        // wall facet centres [3][n_wall_ent]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
   double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
@@ -523,6 +531,34 @@ void fludc_range(cns_ctx* c, int l, long long& n0, long long& n1) {
 // met_num.f90:628-641: met_roe2oh (Harten) when |epsroe| > tiny(1.)
 int sa_harten(const cns_ctx* c) { return fabs(c->epsroe) > 1.17549435082228751e-38 ? 1 : 0; }
 
+// the wall-law constants (rbord.f90:377-379) with the SA cv1
+// (atlecdon.f90:193-204) and the nu~ floor of the step
+WallLaw wall_law(const cns_ctx* c) { return WallLaw{0.41, 5.25, 11.13, 7.1, c->sa_epsk}; }
+
+// lpsa.f90:70-100 for block b (0-based): lpsa1 on its 'lp2' walls in
+// boundary order
+cudaError_t enqueue_lpsa(cns_ctx* c, int b, double* v, const double* mu, double* mut,
+                         const double* dist, const double* temp) {
+  cudaError_t e = cudaSuccess;
+  for (const auto& w : c->lp2)
+    if (w.blk == b && e == cudaSuccess)
+      e = launch_lpsa1(c->bd, w.e0, w.cnt, c->ph, wall_law(c), c->lay.ld, v, mu, mut, dist,
+                       temp, c->st);
+  return e;
+}
+
+// cllparoi1.f90:89-124 (atsch_num.f90:579-604, after zvisqc): lparoi1 on
+// every 'lp2' wall in boundary order
+cudaError_t enqueue_cllparoi1(cns_ctx* c, const double* v, const double* mu, const double* mut,
+                              const double* dist, const double* temp, double* tau) {
+  cudaError_t e = cudaSuccess;
+  for (const auto& w : c->lp2)
+    if (e == cudaSuccess)
+      e = launch_lparoi1(c->bd, w.e0, w.cnt, c->ph, wall_law(c), c->lay.ld, v, mu, mut, dist,
+                         temp, tau, c->st);
+  return e;
+}
+
 cudaError_t enqueue_met_num(cns_ctx* c) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
@@ -539,6 +575,9 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
     block_range(c, b + 1, b0, b1);
     e = launch_teq_grads(c->d_blks, cb, 0, 3, s.v, nullptr, ld, s.sn, s.vol, c->sa_dv, c->sa_sc,
                          b0, b1, c->st);
+    // met_num.f90:193-279: the wall law of the block's 'lp2' walls after
+    // teq_gradv and met_prod, before met_gradtr reads rho nu~
+    if (e == cudaSuccess) e = enqueue_lpsa(c, b, s.v, s.mu, s.mut, c->sa_dist, s.ztemp);
     // met_gradtr.f90:97-104 writes the whole flat range of the real cells,
     // zero on the ghost cells inside it (what the next block's met_smsa
     // reads there through its block-local index)
@@ -575,7 +614,8 @@ cudaError_t enqueue_met_num(cns_ctx* c) {
                         c->w.G, s.u, c->st);
   if (e == cudaSuccess)
     e = launch_impli2(c->d_blks, c->faces, c->lines, all, -1, ld, s.u, s.dt, s.v, s.mu, s.mut,
-                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->sc.precision != 0, c->st);
+                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->sc.precision != 0,
+                      c->d_lp2_ni, c->n_lp2_ni, c->st);
   if (e == cudaSuccess) e = launch_cutsa(c->d_blks, all, s.v, ld, c->sa_epsk, c->st);
   if (e == cudaSuccess) e = launch_samut(c->d_blks, all, s.v + 5 * ld, s.mu, s.mut, c->st);
   return e;
@@ -605,6 +645,8 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
     e = launch_grad(c->d_blks, all, c->ph, s.v, c->w.prim, ld, s.mu, s.mut, s.tau, s.sn,
                     s.vol, s.ztemp, c->st);
     if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
+    if (e == cudaSuccess)
+      e = enqueue_cllparoi1(c, s.v, s.mu, s.mut, c->sa_dist, s.ztemp, s.tau);
   }
   if (e == cudaSuccess) {
     if (jameson(c))
@@ -692,6 +734,8 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     e = launch_grad(c->d_blks, all, c->ph, s.v, w.prim, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
                     s.ztemp, c->st);
     if (e == cudaSuccess) e = launch_tau_ghosts(c->bd, s.tau, ld, c->st);
+    if (e == cudaSuccess)
+      e = enqueue_cllparoi1(c, s.v, s.mu, s.mut, c->sa_dist, s.ztemp, s.tau);
   }
   if (mode != kMixed) {
     // single-precision face fluxes
@@ -1057,10 +1101,10 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     return CNS_EINVAL;
   }
   std::vector<int> ent_bnd((size_t)nl), blk0(nb);
-  std::vector<long long> idd_ents, wall_ents;
+  std::vector<long long> idd_ents, wall_ents, lp2_ni;
   for (int b = 0; b < nb; ++b) {
     const int t = bnd->type[b];
-    if (t < CNS_BC_EXTR || t > CNS_BC_PRD) {
+    if (t < CNS_BC_EXTR || t > CNS_BC_LP2) {
       cns_destroy(c);
       return CNS_EBC;
     }
@@ -1080,8 +1124,12 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     for (int m = 0; m < bnd->mmb[b]; ++m) {
       ent_bnd[(size_t)(bnd->mpb[b] + m)] = b;
       if (t == CNS_BC_IDD) idd_ents.push_back(bnd->mpb[b] + m);
-      if (t == CNS_BC_PARA) wall_ents.push_back(bnd->mpb[b] + m);
+      // atcaldis3.f90:171: 'pa' and 'lp' boundaries are walls
+      if (t == CNS_BC_PARA || t == CNS_BC_LP2) wall_ents.push_back(bnd->mpb[b] + m);
+      if (t == CNS_BC_LP2) lp2_ni.push_back(bnd->ncin[bnd->mpb[b] + m]);
     }
+    if (t == CNS_BC_LP2 && bnd->mmb[b] > 0)
+      c->lp2.push_back({(long long)bnd->mpb[b], bnd->mmb[b], bnd->blk[b] - 1});
     c->h_btype.push_back(t);
   }
   for (long long q = 0; q < nl; ++q) {
@@ -1112,6 +1160,8 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     if (e == cudaSuccess) e = upload(c, &bc_, bnd->bceqt, (size_t)(5 * nl));
     if (e == cudaSuccess) e = upload(c, &c->d_idd_ents, idd_ents.data(), idd_ents.size());
     if (e == cudaSuccess) e = upload(c, &c->d_wall_ents, wall_ents.data(), wall_ents.size());
+    if (e == cudaSuccess) e = upload(c, &c->d_lp2_ni, lp2_ni.data(), lp2_ni.size());
+    c->n_lp2_ni = (long long)lp2_ni.size();
     if (e == cudaSuccess) e = dev_alloc(c, &c->d_idd_masks, (size_t)nb);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nxn, (size_t)nl);
     if (e == cudaSuccess) e = dev_alloc(c, &c->bd.nyn, (size_t)nl);
@@ -1709,7 +1759,8 @@ int cns_impli2_eqt_3d(cns_ctx* c, int l, const double* u, const double* dt, doub
     return CNS_EINVAL;
   if (!c->sa_w) CK(dev_alloc(c, &c->sa_w, (size_t)20 * c->lay.ld, false));
   CK(launch_impli2(c->d_blks, c->faces, c->lines, c->cells.view(l - 1), l - 1, c->lay.ld, u, dt,
-                   v, mu, mut, cfke, sn, vol, cmt, c->sa_w, 0, c->st));
+                   v, mu, mut, cfke, sn, vol, cmt, c->sa_w, 0, c->d_lp2_ni, c->n_lp2_ni,
+                   c->st));
   return CNS_OK;
 }
 
@@ -1785,12 +1836,27 @@ int cns_met_cutsa(cns_ctx* c, int l, double* v, double epsk) {
   return CNS_OK;
 }
 
+int cns_lpsa(cns_ctx* c, int l, double* v, const double* mu, double* mut, const double* dist,
+             const double* ztemp) {
+  if (!c || bad_block(c, l) || !v || !mu || !mut || !dist || !ztemp) return CNS_EINVAL;
+  CK(enqueue_lpsa(c, l - 1, v, mu, mut, dist, ztemp));
+  return CNS_OK;
+}
+
+int cns_cllparoi1(cns_ctx* c, const double* v, const double* dist, const double* mu,
+                  const double* mut, double* tau, const double* ztemp) {
+  if (!c || !v || !dist || !mu || !mut || !tau || !ztemp) return CNS_EINVAL;
+  CK(enqueue_cllparoi1(c, v, mu, mut, dist, ztemp, tau));
+  return CNS_OK;
+}
+
 int cns_set_sa(cns_ctx* c, const cns_sa_t* sa) {
   if (!c) return CNS_EINVAL;
   drop_graphs(c);
   if (!sa) {
     c->sa_on = false;
     c->sa_fix = 0;
+    c->sa_dist = nullptr;
     return CNS_OK;
   }
   if (!sa->dist) return CNS_EINVAL;
@@ -2020,6 +2086,9 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
       return fail(c, CNS_ENOTREADY, "dual time stepping: bind ptdual, vdual, vdual1, vdual2");
     if (c->sa_on) return fail(c, CNS_EINVAL, "dual time stepping with the SA step");
   }
+  if (c->sc.ns && !c->lp2.empty() && !c->sa_dist)
+    return fail(c, CNS_ENOTREADY, "the wall law of the 'lp2' walls needs the wall distance "
+                                  "(cns_set_sa)");
   if (c->sc.kdtl == 0) CK(ensure_dtpart(c));
   if (nsteps == 0) return CNS_OK;
   const int prec = c->sc.precision;

@@ -100,7 +100,8 @@ struct Bnd {
   double* zm;
 };
 
-enum BcKind { BC_EXTR = 1, BC_RC = 2, BC_PARA = 3, BC_IDD = 4, BC_PRD = 5 };
+// BC_LP2: the adiabatic wall-law wall 'lp2', whose ghosts are those of 'para'
+enum BcKind { BC_EXTR = 1, BC_RC = 2, BC_PARA = 3, BC_IDD = 4, BC_PRD = 5, BC_LP2 = 6 };
 
 __device__ __forceinline__ double sq(double a) { return a * a; }
 

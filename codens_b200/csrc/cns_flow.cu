@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(256) k_rbord(Bnd bd, Phys ph, double* v,
     ps[nd] = ps[ni];
     temp[nd] = temp[ni];
     cson[nd] = cson[ni];
-  } else if (kind == BC_PARA) {  // clpara.f90:24-40
+  } else if (kind == BC_PARA || kind == BC_LP2) {  // clpara.f90:24-40 (rbord.f90:374-388)
     const double v1 = v[ni], v2 = v[ld + ni], v3 = v[2 * ld + ni], v4 = v[3 * ld + ni];
     const double rhoe1 = v[4 * ld + ni] - 0.5 * (sq(v2) + sq(v3) + sq(v4)) / v1;
     v[nd] = v1;

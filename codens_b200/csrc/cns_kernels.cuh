@@ -330,11 +330,28 @@ cudaError_t launch_smsa(const Blk* blks, Space cells, long long ld, const double
 // impli2_eqt_3d of block l0 (-1: all): u, v are (ld, 7); w: 20 ld scratch;
 // rcp = 1: one reciprocal per line step instead of three divisions (the
 // reduced-precision forms; not bit-exact)
+// wall_ni: the first cells of the wall-law walls (nwall of them), whose
+// increments are zeroed before the update (impli2_eqt_3d.f90:384-405)
 cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf* lines,
                           Space cells, int l0, long long ld, const double* u, const double* dt,
                           double* v, const double* mu, const double* mut, const double* cfke,
                           const double* sn, const double* vol, double cmt, double* w, int rcp,
-                          cudaStream_t st);
+                          const long long* wall_ni, long long nwall, cudaStream_t st);
+
+// wall laws of the adiabatic wall-law walls 'lp2' (rbord.f90:377-379: vkar,
+// cllog, yp0; the SA cv1 and the nu~ floor epsk) on the cnt list entries
+// from e0 of one boundary: lpsa1 (first cell's mut and rho nu~, ghost rho
+// nu~ = 0; v is (ld, 7)) and lparoi1 (wall stresses and heat flux in tau)
+struct WallLaw {
+  double vkar, cllog, yp0, cv1, epsk;
+};
+cudaError_t launch_lpsa1(const Bnd& bd, long long e0, int cnt, Phys ph, WallLaw wl,
+                         long long ld, double* v, const double* mu, double* mut,
+                         const double* dist, const double* temp, cudaStream_t st);
+cudaError_t launch_lparoi1(const Bnd& bd, long long e0, int cnt, Phys ph, WallLaw wl,
+                           long long ld, const double* v, const double* mu, const double* mut,
+                           const double* dist, const double* temp, double* tau,
+                           cudaStream_t st);
 
 // wall distance of the real cells to the nearest facet centre of the nw wall
 // entries went (atcaldis3 / atdist_3); par: 3 nw scratch

@@ -20,6 +20,8 @@
  *                  (|s| <= 0.1716: 12 terms), plus e ln2, as a double-double.
  *   cns_pow(x, y): exp(y log x) for x > 0, y log x formed in double-double
  *                  (Dekker's product); 0 or inf for x = 0; NaN for x < 0.
+ *   cns_asin(x):   the Taylor series of asin for |x| <= 1/2, the half-angle
+ *                  identity above (the wall laws' Van Driest transform).
  */
 #ifndef CNS_PMATH_H
 #define CNS_PMATH_H
@@ -139,6 +141,41 @@ CNS_PM_FN double cns_pow(double x, double y) {
   cns_log_dd(x, &lh, &ll);
   cns_two_prod(y, lh, &th, &te);
   return cns_exp_dd(th, CNS_PM_ADD(te, CNS_PM_MUL(y, ll)));
+}
+
+/* pi/2 = 1.5707963267948966192313216916397514...: the nearest double and
+ * the rest */
+#define CNS_PM_PIO2_HI 0x1.921fb54442d18p+0
+#define CNS_PM_PIO2_LO 0x1.1a62633145c07p-54
+
+/* asin(x) for |x| <= 1/2 by its Taylor series
+ *   asin(x) = x (1 + r1 z (1 + r2 z (1 + ... (1 + r29 z)))),  z = x^2,
+ *   r_n = (2n - 1)^2 / ((2n) (2n + 1))   (the ratio of consecutive terms),
+ * whose tail after 29 terms is below 2^-58 relative for z <= 1/4 */
+CNS_PM_FN double cns_asin_small(double x) {
+  const double z = CNS_PM_MUL(x, x);
+  double p = 1.0;
+  CNS_PM_UNROLL
+  for (int n = 29; n >= 1; --n)
+    p = CNS_PM_ADD(1.0, CNS_PM_MUL(CNS_PM_MUL(CNS_PM_DIV((double)((2 * n - 1) * (2 * n - 1)),
+                                                         (double)((2 * n) * (2 * n + 1))),
+                                              z),
+                                   p));
+  return CNS_PM_MUL(x, p);
+}
+
+/* asin(x): the series for |x| <= 1/2; above, asin(|x|) = pi/2 - 2 asin(s)
+ * with s = sqrt((1 - |x|)/2) <= 1/2 (1 - |x| and the halving are exact);
+ * NaN outside [-1, 1] */
+CNS_PM_FN double cns_asin(double x) {
+  if (x != x) return x;
+  const double a = fabs(x);
+  if (a > 1.0) return NAN;
+  if (a <= 0.5) return cns_asin_small(x);
+  const double s = sqrt(CNS_PM_MUL(CNS_PM_SUB(1.0, a), 0.5));
+  const double r =
+      CNS_PM_ADD(CNS_PM_SUB(CNS_PM_PIO2_HI, CNS_PM_MUL(2.0, cns_asin_small(s))), CNS_PM_PIO2_LO);
+  return x < 0.0 ? -r : r;
 }
 
 #endif /* CNS_PMATH_H */

@@ -541,6 +541,7 @@ __global__ void __launch_bounds__(256) k_turb_bord(Bnd bd, double* v, long long 
       v7[nd] = roeinf;
       break;
     case BC_PARA:
+    case BC_LP2:  // met_bord.f90:296-305 with kparoi = 0
       v6[nd] = 0.;
       v7[nd] = 0.;
       break;
@@ -549,6 +550,148 @@ __global__ void __launch_bounds__(256) k_turb_bord(Bnd bd, double* v, long long 
       v7[nd] = v7[ni];
       break;
   }
+}
+
+// ---------------------------------------------------------------------------
+// wall laws of the adiabatic wall-law walls 'lp2' (lparoi = 1; constants of
+// rbord.f90:377-379; air, iflu = 1; no transition, ktransi = 0).  lpsa1.f90
+// and lparoi1.f90 share the friction law: the unit tangent t of the first
+// cell's velocity, the Crocco wall temperature, the wall viscosity
+// (Sutherland) and density, Van Driest's compressible velocity, and the wall
+// stress top of the linear law (u+ y+ <= yp0^2) or of ten fixed-point passes
+// of the log law.  One launch per boundary in list order: a corner cell next
+// to two such walls sees the writes of the earlier boundary first, as in the
+// reference's boundary loop.
+struct WallFriction {
+  double t1, t2, t3, n1, n2, n3, top, dudy, rop, mup;
+};
+
+__device__ __forceinline__ WallFriction wall_friction(const Bnd& bd, long long e, Phys ph,
+                                                      WallLaw wl, long long ld,
+                                                      const double* v, const double* mu,
+                                                      const double* mut, const double* dist,
+                                                      const double* temp) {
+  const long long ni = bd.ncin[e];
+  WallFriction f;
+  const double v1x = v[ld + ni] / v[ni], v1y = v[2 * ld + ni] / v[ni],
+               v1z = v[3 * ld + ni] / v[ni];
+  f.n1 = bd.nxn[e];
+  f.n2 = bd.nyn[e];
+  f.n3 = bd.nzn[e];
+  const double tn = v1x * f.n1 + v1y * f.n2 + v1z * f.n3;
+  double t1 = v1x - tn * f.n1, t2 = v1y - tn * f.n2, t3 = v1z - tn * f.n3;
+  const double tt = sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+  t1 = t1 / tt;
+  t2 = t2 / tt;
+  t3 = t3 / tt;
+  f.t1 = t1;
+  f.t2 = t2;
+  f.t3 = t3;
+  double v1t = v1x * t1 + v1y * t2 + v1z * t3;
+  const double temp1 = temp[ni];
+  const double pka = ph.cp * (mu[ni] / ph.pr + mut[ni] / ph.prt);
+  const double pkb = mu[ni] + mut[ni];
+  const double tparoi = temp1 + 0.5 * pkb * (v1t * v1t) / pka;
+  const double sv = ph.suth_a;
+  const double mup = mu[ni] * sqrt(tparoi / temp1) * (1. + sv / temp1) / (1. + sv / tparoi);
+  const double rop = v[ni] * temp1 / tparoi;
+  f.rop = rop;
+  f.mup = mup;
+  const double co = sqrt(2. * pka * tparoi / pkb);
+  v1t = co * cns_asin(v1t / co);
+  const double d = dist[ni];
+  const double upyp1 = rop * v1t * d / mup;
+  double top = mup * v1t / d;
+  if (upyp1 <= wl.yp0 * wl.yp0) {
+    f.dudy = top / mup;
+  } else {
+    for (int it = 0; it < 10; ++it) {
+      const double q = cns_log(d * sqrt(rop * top) / mup) / wl.vkar + wl.cllog;
+      top = rop * (v1t * v1t) / (q * q);
+    }
+    f.dudy = sqrt(top / rop) / (wl.vkar * d);
+  }
+  f.top = top;
+  return f;
+}
+
+// lpsa1.f90:70-236: mut and rho nu~ of the first cell from the wall law
+// (mut = rho (kappa d)^2 du/dy (1 - exp(-y+/26))^2, then nu~ from the
+// closed-form root of mut = rho nu~ fv1), the wall ghost's rho nu~ = 0
+__global__ void __launch_bounds__(128) k_lpsa1(Bnd bd, long long e0, int cnt, Phys ph,
+                                              WallLaw wl, long long ld, double* v,
+                                              const double* __restrict__ mu, double* mut,
+                                              const double* __restrict__ dist,
+                                              const double* __restrict__ temp) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= cnt) return;
+  const long long e = e0 + m, ni = bd.ncin[e], nc = bd.ncbd[e];
+  const WallFriction f = wall_friction(bd, e, ph, wl, ld, v, mu, mut, dist, temp);
+  const double d = dist[ni];
+  const double yplus1 = d * sqrt(f.top * f.rop) / f.mup;
+  const double ex = 1. - cns_exp(-yplus1 / 26.);
+  const double mt = v[ni] * (wl.vkar * wl.vkar) * (d * d) * f.dudy * (ex * ex);
+  mut[ni] = mt;
+  const double c13 = 1. / 3., c18 = 1. / 18.;
+  const double ca = mt;
+  const double mu1 = mu[ni];
+  const double cb = mu1 * mu1 * mu1 * mt * (wl.cv1 * wl.cv1 * wl.cv1);
+  const double ca2 = ca * ca;
+  const double c1 = cb * sqrt(3.) * sqrt(256. * cb + 27. * (ca2 * ca2));
+  const double c2 = 0.5 * cb * ca2 + c18 * c1;
+  const double c3 = -(0.5 * cb * ca2) + c18 * c1;
+  const double p3 = cns_pow(c3, c13), p2 = cns_pow(c2, c13);
+  const double c4 = 4. * fabs(p3 - p2);
+  const double rc4 = sqrt(ca2 + c4);
+  const double rnut = 0.25 * (ca + rc4) +
+                      0.25 * sqrt(2.) *
+                          sqrt(ca2 * rc4 - 2. * p3 * rc4 + 2. * p2 * rc4 + ca2 * ca) /
+                          cns_pow(rc4, 0.5);
+  v[5 * ld + ni] = fmax(rnut, wl.epsk);
+  v[5 * ld + nc] = 0.;
+}
+
+// lparoi1.f90:77-229: the wall stress tensor top (t n + n t) in the wall
+// ghost and the first cell, the first cell's heat flux -n top (u . t) and
+// none in the ghost
+__global__ void __launch_bounds__(128) k_lparoi1(Bnd bd, long long e0, int cnt, Phys ph,
+                                                WallLaw wl, long long ld,
+                                                const double* __restrict__ v,
+                                                const double* __restrict__ mu,
+                                                const double* __restrict__ mut,
+                                                const double* __restrict__ dist,
+                                                const double* __restrict__ temp, double* tau) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= cnt) return;
+  const long long e = e0 + m, ni = bd.ncin[e], nc = bd.ncbd[e];
+  const WallFriction f = wall_friction(bd, e, ph, wl, ld, v, mu, mut, dist, temp);
+  const double top = f.top;
+  const double t[6] = {2. * f.t1 * f.n1 * top,           (f.t2 * f.n1 + f.t1 * f.n2) * top,
+                       (f.t1 * f.n3 + f.t3 * f.n1) * top, 2. * f.t2 * f.n2 * top,
+                       (f.t2 * f.n3 + f.t3 * f.n2) * top, 2. * f.t3 * f.n3 * top};
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    tau[a * ld + nc] = t[a];
+    tau[a * ld + ni] = t[a];
+  }
+  const double qc1 =
+      top * ((v[ld + ni] * f.t1 + v[2 * ld + ni] * f.t2 + v[3 * ld + ni] * f.t3) / v[ni]);
+  tau[6 * ld + ni] = -f.n1 * qc1;
+  tau[7 * ld + ni] = -f.n2 * qc1;
+  tau[8 * ld + ni] = -f.n3 * qc1;
+  tau[6 * ld + nc] = 0.;
+  tau[7 * ld + nc] = 0.;
+  tau[8 * ld + nc] = 0.;
+}
+
+// impli2_eqt_3d.f90:384-405: the increments of rho nu~ and of the second
+// variable vanish in the first cell of every wall-law wall
+__global__ void __launch_bounds__(256) k_i2_wall_freeze(const long long* __restrict__ ni,
+                                                       long long cnt, double* w6, double* w7) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cnt) return;
+  w6[ni[q]] = 0.;
+  w7[ni[q]] = 0.;
 }
 
 // met_rbse.f90:19-31 (non-coincident boundaries: ghost = interior) and
@@ -647,7 +790,8 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
                           Space cells, int l0, long long ld, const double* u, const double* dt,
                           double* v, const double* mu, const double* mut, const double* cfke,
                           const double* sn, const double* vol, double cmt, double* w,
-                          int rcp, cudaStream_t st) {
+                          int rcp, const long long* wall_ni, long long nwall,
+                          cudaStream_t st) {
   // scratch w: rv, cd, uf[3], ce[3], al, b6, b7, two iterates x (6, 7),
   // the tridiagonal coefficients ta, tb, tc and right-hand sides d6, d7 of
   // a sweep = 20 ld.  rv and the iterates start at zero (their ghost
@@ -685,7 +829,28 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
       cur = 1 - cur;
     }
   }
+  if (nwall > 0)
+    k_i2_wall_freeze<<<(unsigned)((nwall + 255) / 256), 256, 0, st>>>(wall_ni, nwall,
+                                                                     it[cur][0], it[cur][1]);
   k_i2_update<<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, it[cur][0], it[cur][1], v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lpsa1(const Bnd& bd, long long e0, int cnt, Phys ph, WallLaw wl,
+                         long long ld, double* v, const double* mu, double* mut,
+                         const double* dist, const double* temp, cudaStream_t st) {
+  if (cnt > 0)
+    k_lpsa1<<<(cnt + 127) / 128, 128, 0, st>>>(bd, e0, cnt, ph, wl, ld, v, mu, mut, dist, temp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lparoi1(const Bnd& bd, long long e0, int cnt, Phys ph, WallLaw wl,
+                           long long ld, const double* v, const double* mu, const double* mut,
+                           const double* dist, const double* temp, double* tau,
+                           cudaStream_t st) {
+  if (cnt > 0)
+    k_lparoi1<<<(cnt + 127) / 128, 128, 0, st>>>(bd, e0, cnt, ph, wl, ld, v, mu, mut, dist,
+                                                 temp, tau);
   return cudaGetLastError();
 }
 

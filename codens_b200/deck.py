@@ -62,7 +62,7 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
-from .cases import (BC_EXTR, BC_IDD, BC_PARA, BC_PRD, BC_RC, Boundary, Case, Phys,
+from .cases import (BC_EXTR, BC_IDD, BC_LP2, BC_PARA, BC_PRD, BC_RC, Boundary, Case, Phys,
                     Scheme)
 from .layout import Layout
 
@@ -419,7 +419,7 @@ class Deck:
                 raise DeckError(f"{c}: prd needs a pressure")
             pdim = 1.0 if ibddim == 0 else self._pt_ref(c)[0]
             return [vals[0] / pdim * (1.0 / self.gam)]   # pa1 = roa1 ta1 / gam
-        if clmf in ("extr", "para"):
+        if clmf in ("extr", "para", "lp2 "):
             return []
         raise DeckError(f"{c}: boundary kind {clmf.strip()!r} not handled")
 
@@ -513,7 +513,7 @@ class Deck:
 
     def boundaries(self) -> List[Boundary]:
         kinds = {"extr": BC_EXTR, "para": BC_PARA, "idd ": BC_IDD, "prd ": BC_PRD,
-                 "rc  ": BC_RC}
+                 "rc  ": BC_RC, "lp2 ": BC_LP2}
         order = list(self.bnds)
         pos = {m: q for q, m in enumerate(order)}
         out = []

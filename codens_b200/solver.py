@@ -442,6 +442,18 @@ class CodeNS:
     def met_num(self):
         self._check(self.lib.cns_met_num(self.ctx), "cns_met_num")
 
+    def lpsa(self, l, v, mu, mut, dist, ztemp):
+        """the wall law's rho nu~ and mut of block l's 'lp2' first cells
+        (lpsa.f90; the floor is set_sa's epsk)"""
+        self._check(self.lib.cns_lpsa(self.ctx, l, _ptr(v), _ptr(mu), _ptr(mut), _ptr(dist),
+                                      _ptr(ztemp)), "cns_lpsa")
+
+    def cllparoi1(self, v, dist, mu, mut, tau, ztemp):
+        """the wall law's stresses and heat flux at every 'lp2' wall
+        (cllparoi1.f90)"""
+        self._check(self.lib.cns_cllparoi1(self.ctx, _ptr(v), _ptr(dist), _ptr(mu), _ptr(mut),
+                                           _ptr(tau), _ptr(ztemp)), "cns_cllparoi1")
+
     # iteration counters and dual time stepping
     def set_cycle(self, ncyc: int, icyc: int):
         """the reference's ncyc, icyc of the last iteration done"""

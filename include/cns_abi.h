@@ -75,9 +75,14 @@ enum {
                           reference stops: readdg.f90:86-89) */
 };
 
-/* boundary kinds (rbord.f90:144-424) */
+/* boundary kinds (rbord.f90:144-424); CNS_BC_LP2: the adiabatic wall with
+ * the wall law ('lp2', rbord.f90:374-388): the ghosts of 'para', and with
+ * the Navier-Stokes equations the wall stresses of lparoi1.f90 after zvisqc
+ * (cllparoi1.f90, atsch_num.f90:579-604), with the Spalart-Allmaras step the
+ * first cell's nu~ of lpsa1.f90 and no implicit increment there
+ * (impli2_eqt_3d.f90:384-405); it needs the wall distance of cns_set_sa */
 enum { CNS_BC_EXTR = 1, CNS_BC_RC = 2, CNS_BC_PARA = 3, CNS_BC_IDD = 4,
-       CNS_BC_PRD = 5 };
+       CNS_BC_PRD = 5, CNS_BC_LP2 = 6 };
 
 typedef struct cns_ctx cns_ctx;
 
@@ -296,6 +301,25 @@ int cns_met_gradtr(cns_ctx *ctx, int l, const double *s, const double *sn, const
 int cns_met_rbse(cns_ctx *ctx, double *fd5x, double *fd5y, double *fd5z, double *fd6x,
                  double *fd6y, double *fd6z);
 int cns_met_cutsa(cns_ctx *ctx, int l, double *v, double epsk);
+/* Wall law of the adiabatic wall-law walls (CNS_BC_LP2; air, no transition;
+ * vkar 0.41, cllog 5.25, yp0 11.13 as rbord.f90:377-379 sets them).  Both
+ * take the friction law of lpsa1.f90:111-160 / lparoi1.f90:111-160: the
+ * first cell's tangential velocity, the Crocco wall temperature, Sutherland's
+ * wall viscosity, Van Driest's transform, and the wall stress of the linear
+ * law (rho u y / mu <= yp0^2) or ten passes of the log law.  Device arrays.
+ *   cns_lpsa       lpsa.f90 -> lpsa1.f90 on the 'lp2' walls of block l in
+ *                  boundary order: mut of the first cell from the mixing
+ *                  length, rho nu~ there from mut = rho nu~ fv1 (floored at
+ *                  the context's epsk, cns_sa_t), rho nu~ = 0 in the ghost;
+ *                  v is (ld, 7)
+ *   cns_cllparoi1  cllparoi1.f90 -> lparoi1.f90 on every 'lp2' wall: the
+ *                  wall stress tensor in the ghost and the first cell, the
+ *                  first cell's heat flux, none in the ghost; tau (ld, 9) as
+ *                  cns_zvisqc writes it */
+int cns_lpsa(cns_ctx *ctx, int l, double *v, const double *mu, double *mut, const double *dist,
+             const double *ztemp);
+int cns_cllparoi1(cns_ctx *ctx, const double *v, const double *dist, const double *mu,
+                  const double *mut, double *tau, const double *ztemp);
 int cns_set_sa(cns_ctx *ctx, const cns_sa_t *sa);
 int cns_met_num(cns_ctx *ctx);
 

@@ -791,7 +791,10 @@ void orc_rbord(double *v, double *ps, double *temp, double *cson) {
   for (int bb = 0; bb < G.nbnd; ++bb) {
     switch (G.btype[bb]) {
       case ORC_BC_EXTR: clextr(bb, v, ps, temp, cson); break;
-      case ORC_BC_PARA: clpara(bb, v, ps, temp, cson); break;
+      case ORC_BC_PARA:
+      case ORC_BC_LP2: /* rbord.f90:374-388: 'lp2' walls take clpara */
+        clpara(bb, v, ps, temp, cson);
+        break;
       case ORC_BC_IDD:
         rbve(bb, v);
         clidd(bb, v, ps, temp, cson);
@@ -2781,6 +2784,15 @@ void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, cons
       }
     }
   }
+  /* impli2_eqt_3d.f90:384-405 (lparoi 1): no increment in the first cell
+   * of the block's wall-law walls */
+  for (int bb = 0; bb < G.nbnd; ++bb)
+    if (G.btype[bb] == ORC_BC_LP2 && G.bblk[bb] == l)
+      for (int m = 0; m < G.bmmb[bb]; ++m) {
+        const int64_t ni = G.ncin[G.bmpb[bb] + m] - n0;
+        dw6[ni] = 0.;
+        dw7[ni] = 0.;
+      }
   for (int k = 1; k <= b->nk - 1; ++k)
     for (int j = 1; j <= b->nj - 1; ++j)
       for (int i = 1; i <= b->ni - 1; ++i) {
@@ -2797,8 +2809,9 @@ void orc_impli2_eqt_3d(int l, const double *u, const double *dt, double *v, cons
 /* kfludis 2, ksecmb 2, kcmut 2, kditur 2, klroe 2, kparoi 0)                */
 /* ------------------------------------------------------------------------ */
 
-/* the wall boundaries: cl 'pa..' (adiabatic wall) -- atcaldis3.f90:51-60 */
-static int is_wall(int bb) { return G.btype[bb] == ORC_BC_PARA; }
+/* the wall boundaries: cl 'pa..' (adiabatic wall) and 'lp..' (wall-law
+ * wall) -- atcaldis3.f90:171 */
+static int is_wall(int bb) { return G.btype[bb] == ORC_BC_PARA || G.btype[bb] == ORC_BC_LP2; }
 
 /* atindnor.f90 + atccfp.f90:56-72: node increments of a wall facet (dm1,
  * dm2 span the face, ndm3 moves from the interior cell's lower node to the
@@ -2885,6 +2898,7 @@ void orc_met_bord(double *v, double rokinf, double roeinf) {
           v[6 * L + nd] = roeinf;
           break;
         case ORC_BC_PARA:
+        case ORC_BC_LP2: /* met_bord.f90:296-305, kparoi = 0 */
           v[5 * L + nd] = 0.;
           v[6 * L + nd] = 0.;
           break;
@@ -2977,13 +2991,144 @@ void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double
   SA.cfke = cfke;
 }
 
+/* ------------------------------------------------------------------------ */
+/* wall laws of the adiabatic wall-law walls 'lp2' (lparoi = 1; air,          */
+/* iflu = 1; no transition, ktransi = 0)                                    */
+/* ------------------------------------------------------------------------ */
+
+/* rbord.f90:377-379 */
+#define WL_VKAR 0.41
+#define WL_CLLOG 5.25
+#define WL_YP0 11.13
+
+static int has_lp2(void) {
+  for (int bb = 0; bb < G.nbnd; ++bb)
+    if (G.btype[bb] == ORC_BC_LP2) return 1;
+  return 0;
+}
+
+typedef struct {
+  double t1, t2, t3, n1, n2, n3, top, dudy, rop, mup;
+} wall_fr;
+
+/* the friction law of lpsa1.f90:111-160 and lparoi1.f90:111-160 for list
+ * entry mb: unit tangent of the first cell's velocity, Crocco wall
+ * temperature, Sutherland wall viscosity, wall density, Van Driest's
+ * velocity v1t = co asin(v1t / co), then the wall stress of the linear law
+ * or ten fixed-point passes of the log law */
+static wall_fr wall_friction(int64_t mb, const double *v, const double *mu, const double *mut,
+                             const double *dist, const double *temp) {
+  const int64_t L = G.ld, ni = G.ncin[mb];
+  wall_fr f;
+  const double v1x = v[L + ni] / v[ni], v1y = v[2 * L + ni] / v[ni], v1z = v[3 * L + ni] / v[ni];
+  f.n1 = G.nxn[mb];
+  f.n2 = G.nyn[mb];
+  f.n3 = G.nzn[mb];
+  const double tn = v1x * f.n1 + v1y * f.n2 + v1z * f.n3;
+  double t1 = v1x - tn * f.n1, t2 = v1y - tn * f.n2, t3 = v1z - tn * f.n3;
+  const double tt = sqrt(sq(t1) + sq(t2) + sq(t3));
+  f.t1 = t1 = t1 / tt;
+  f.t2 = t2 = t2 / tt;
+  f.t3 = t3 = t3 / tt;
+  double v1t = v1x * t1 + v1y * t2 + v1z * t3;
+  const double temp1 = temp[ni];
+  const double pka = G.cp * (mu[ni] / G.pr + mut[ni] / G.prt);
+  const double pkb = mu[ni] + mut[ni];
+  const double tparoi = temp1 + 0.5 * pkb * sq(v1t) / pka;
+  const double sv = G.suth_a; /* 110.4 / tnz */
+  f.mup = mu[ni] * sqrt(tparoi / temp1) * (1. + sv / temp1) / (1. + sv / tparoi);
+  f.rop = v[ni] * temp1 / tparoi;
+  const double co = sqrt(2. * pka * tparoi / pkb);
+  v1t = co * cns_asin(v1t / co);
+  const double d = dist[ni];
+  const double upyp1 = f.rop * v1t * d / f.mup;
+  double top = f.mup * v1t / d;
+  if (upyp1 <= WL_YP0 * WL_YP0) {
+    f.dudy = top / f.mup;
+  } else {
+    for (int it = 1; it <= 10; ++it)
+      top = f.rop * sq(v1t) / sq(cns_log(d * sqrt(f.rop * top) / f.mup) / WL_VKAR + WL_CLLOG);
+    f.dudy = sqrt(top / f.rop) / (WL_VKAR * d);
+  }
+  f.top = top;
+  return f;
+}
+
+/* lpsa.f90:70-100 -> lpsa1.f90:111-236 on the 'lp2' walls of block l in
+ * boundary order: mut of the first cell from the mixing length with van
+ * Driest's damping, rho nu~ there from the closed-form root of
+ * mut = rho nu~ fv1 (floored at epsk), rho nu~ = 0 in the ghost */
+void orc_lpsa(int l, double *v, const double *mu, double *mut, const double *dist,
+              const double *temp, double epsk) {
+  const int64_t L = G.ld;
+  const double c13 = 1. / 3., c18 = 1. / 18., cv1 = SA_CV1;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_LP2 || G.bblk[bb] != l) continue;
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      const int64_t mb = G.bmpb[bb] + m, ni = G.ncin[mb], nc = G.ncbd[mb];
+      const wall_fr f = wall_friction(mb, v, mu, mut, dist, temp);
+      const double d = dist[ni];
+      const double yplus1 = d * sqrt(f.top * f.rop) / f.mup;
+      mut[ni] = v[ni] * sq(WL_VKAR) * sq(d) * f.dudy * sq(1. - cns_exp(-yplus1 / 26.));
+      const double ca = mut[ni];
+      const double cb = mu[ni] * mu[ni] * mu[ni] * mut[ni] * (cv1 * cv1 * cv1);
+      const double c1 = cb * sqrt(3.) * sqrt(256. * cb + 27. * (sq(ca) * sq(ca)));
+      const double c2 = 0.5 * cb * sq(ca) + c18 * c1;
+      const double c3 = -(0.5 * cb * sq(ca)) + c18 * c1;
+      const double c4 = 4. * fabs(cns_pow(c3, c13) - cns_pow(c2, c13));
+      const double rc4 = sqrt(sq(ca) + c4);
+      const double rnutilde =
+          0.25 * (ca + rc4) + 0.25 * sqrt(2.) *
+                                  sqrt(sq(ca) * rc4 - 2. * cns_pow(c3, c13) * rc4 +
+                                       2. * cns_pow(c2, c13) * rc4 + sq(ca) * ca) /
+                                  cns_pow(rc4, 0.5);
+      v[5 * L + ni] = fmax(rnutilde, epsk);
+      v[5 * L + nc] = 0.;
+    }
+  }
+}
+
+/* cllparoi1.f90:89-124 -> lparoi1.f90:111-229 on every 'lp2' wall in
+ * boundary order: the wall stress tensor top (t n + n t) in the ghost and
+ * the first cell, the first cell's heat flux -n top (u . t), none in the
+ * ghost; tau (ld, 9): txx txy txz tyy tyz tzz qcx qcy qcz */
+void orc_cllparoi1(const double *v, const double *dist, const double *mu, const double *mut,
+                   double *tau, const double *temp) {
+  const int64_t L = G.ld;
+  for (int bb = 0; bb < G.nbnd; ++bb) {
+    if (G.btype[bb] != ORC_BC_LP2) continue;
+    for (int m = 0; m < G.bmmb[bb]; ++m) {
+      const int64_t mb = G.bmpb[bb] + m, ni = G.ncin[mb], nc = G.ncbd[mb];
+      const wall_fr f = wall_friction(mb, v, mu, mut, dist, temp);
+      const double top = f.top;
+      tau[nc] = 2. * f.t1 * f.n1 * top;
+      tau[3 * L + nc] = 2. * f.t2 * f.n2 * top;
+      tau[5 * L + nc] = 2. * f.t3 * f.n3 * top;
+      tau[L + nc] = (f.t2 * f.n1 + f.t1 * f.n2) * top;
+      tau[2 * L + nc] = (f.t1 * f.n3 + f.t3 * f.n1) * top;
+      tau[4 * L + nc] = (f.t2 * f.n3 + f.t3 * f.n2) * top;
+      for (int a = 0; a < 6; ++a) tau[a * L + ni] = tau[a * L + nc];
+      const double qc1 = top * ((v[L + ni] * f.t1 + v[2 * L + ni] * f.t2 + v[3 * L + ni] * f.t3) /
+                                v[ni]);
+      tau[6 * L + ni] = -f.n1 * qc1;
+      tau[7 * L + ni] = -f.n2 * qc1;
+      tau[8 * L + ni] = -f.n3 * qc1;
+      tau[6 * L + nc] = 0.;
+      tau[7 * L + nc] = 0.;
+      tau[8 * L + nc] = 0.;
+    }
+  }
+}
+
+double orc_asin(double x) { return cns_asin(x); }
+
 /* met_num.f90:145-790 for 1SA, after rbord: turbulence ghosts; per block
  * (in block order, which met_smsa.f90:177's block-local read of txxf5x
  * depends on) velocity gradients, grad(nu~), source, diffusion densities;
  * their ghosts; per block Roe dissipation, explicit balance, implicit line
  * Jacobi and the clip; mut = v6 fv1.  v, u, d are (ld, 7). */
 void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
-                 double *mut, const double *sn, const double *vol) {
+                 double *mut, const double *sn, const double *vol, const double *temp) {
   const int64_t L = G.ld;
   double *fd = SA.fd, *ts6 = SA.ts, *ts7 = SA.ts + L;
   double *f5x = fd, *f5y = fd + L, *f5z = fd + 2 * L, *f6x = fd + 3 * L, *f6y = fd + 4 * L,
@@ -2993,6 +3138,8 @@ void orc_met_num(double *v, double *u, double *d, const double *dt, const double
     const blk_t *b = &G.b[l - 1];
     double *dv = calloc((size_t)(9 * b->nnn), sizeof(double));
     orc_teq_gradv(l, sn, vol, v, dv);
+    /* met_num.f90:193-279: the wall law after teq_gradv and met_prod */
+    orc_lpsa(l, v, mu, mut, SA.dist, temp, SA.epsk);
     orc_met_gradtr(l, sn, vol, v, f5x, f5y, f5z, f6x, f6y, f6z);
     orc_met_smsa(l, sn, vol, v, mu, SA.dist, dv, f5x, f5y, f5z, ts6, ts7, SA.cfke);
     orc_met_fludcsa(l, v, mu, f5x, f5y, f5z, f6x, f6y, f6z, SA.sigma);
@@ -3025,8 +3172,12 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
   orc_rfvc(v, ps, temp, cson);
   for (int l = 1; l <= G.nblk; ++l) orc_dissip_jameson(l, v, dis, sn, ps, cson);
   orc_rbord(v, ps, temp, cson);
-  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol);
-  if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol, temp);
+  if (G.ns) {
+    orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+    /* atsch_num.f90:579-604: the wall law of the 'lp2' walls */
+    if (has_lp2()) orc_cllparoi1(v, SA.dist, mu, mut, tau, temp);
+  }
   for (int l = 1; l <= G.nblk; ++l) orc_sch_jameson(l, u, v, dis, tau, sn, ps);
   if (G.kfmg == 3)
     for (int l = 1; l <= G.nblk; ++l) orc_sch_dual(l, u, v, G.icycle, vol, G.ptdual);
@@ -3051,8 +3202,12 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
   }
   if (compute_dt && G.kdtl == 0) orc_chrono_global(dt);
   orc_rbord(v, ps, temp, cson);
-  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol);
-  if (G.ns) orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+  if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol, temp);
+  if (G.ns) {
+    orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
+    /* atsch_num.f90:579-604: the wall law of the 'lp2' walls */
+    if (has_lp2()) orc_cllparoi1(v, SA.dist, mu, mut, tau, temp);
+  }
 #pragma omp parallel for schedule(dynamic, 1)
   for (int l = 1; l <= G.nblk; ++l) {
     /* atsch_num.f90:628-983: the flux family by ischema */

@@ -35,9 +35,10 @@
 extern "C" {
 #endif
 
-/* boundary condition kinds (rbord.f90:144-424) */
+/* boundary condition kinds (rbord.f90:144-424); ORC_BC_LP2: the adiabatic
+ * wall with the wall law ('lp2') */
 enum { ORC_BC_EXTR = 1, ORC_BC_RC = 2, ORC_BC_PARA = 3, ORC_BC_IDD = 4,
-       ORC_BC_PRD = 5 };
+       ORC_BC_PRD = 5, ORC_BC_LP2 = 6 };
 
 int  orc_setup(int nblk, const int32_t *dims /* 3*nblk: ni,nj,nk nodes */, int64_t ld);
 int64_t orc_npc(int l);
@@ -161,7 +162,15 @@ void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double
                 int harten, double epsroe, double sigma, double *fd, double *ts,
                 double *cfke);
 void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
-                 double *mut, const double *sn, const double *vol);
+                 double *mut, const double *sn, const double *vol, const double *temp);
+/* wall law of the 'lp2' walls: lpsa.f90 -> lpsa1.f90 on block l (v is
+ * (ld, 7); epsk the floor of rho nu~) and cllparoi1.f90 -> lparoi1.f90 on
+ * every 'lp2' wall (tau (ld, 9)) */
+void orc_lpsa(int l, double *v, const double *mu, double *mut, const double *dist,
+              const double *temp, double epsk);
+void orc_cllparoi1(const double *v, const double *dist, const double *mu, const double *mut,
+                   double *tau, const double *temp);
+double orc_asin(double x);
 /* non-reference option of met_smsa: the modified vorticity of Allmaras,
  * Johnson & Spalart 2012 and a derivative guarded where r is clipped
  * (0 = reference) */

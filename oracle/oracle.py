@@ -84,7 +84,11 @@ def lib():
         L.orc_set_sa.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                  C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                  C.c_void_p]
-        L.orc_met_num.argtypes = [_d] * 8
+        L.orc_met_num.argtypes = [_d] * 9
+        L.orc_lpsa.argtypes = [C.c_int] + [_d] * 5 + [C.c_double]
+        L.orc_cllparoi1.argtypes = [_d] * 6
+        L.orc_asin.argtypes = [C.c_double]
+        L.orc_asin.restype = C.c_double
         L.orc_set_sa_fix.argtypes = [C.c_int]
         L.orc_set_block_scheme.argtypes = [C.c_void_p] * 3
         L.orc_sch_hllc_euler.argtypes = [C.c_int, _d, _d, _d, _d]

@@ -23,6 +23,19 @@ CASES = {
     "channel": lambda: cases.channel_case([9, 6, 7], 8, 5, seed=13, reynz=1.0e3, ilim=0),
 }
 
+# the wall law of the 'lp2' walls (lpsa1, lparoi1, the implicit freeze)
+WALL_LAW = {
+    # log law (rho u y / mu above yp0^2 in every first cell); the k faces are
+    # wall-law walls too, so the corner cells take two walls' laws in order
+    "plate_wl": lambda: cases.flat_plate_case((14, 10, 4), reynz=1.0e6, dy1=2e-3, ratio=1.2,
+                                              seed=5, noise=0.01, wall_kind=cases.BC_LP2,
+                                              side_walls=True),
+    # linear law, three blocks
+    "channel_wl": lambda: cases.channel_case([9, 6, 7], 8, 5, seed=13, reynz=1.0e3, ilim=0,
+                                             wall_kind=cases.BC_LP2),
+}
+ALL = {**CASES, **WALL_LAW}
+
 
 def _seven(case, seed=71):
     """the case's state with seeded transport columns when it has only 5"""
@@ -51,9 +64,9 @@ def _t(torch, a):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(ALL))
 def test_atcaldis3_parity(cuda, name):
-    case = CASES[name]()
+    case = ALL[name]()
     orc, st = oracle_prepared(case)
     s = _gpu(case)
     d_o = np.full(case.layout.ld, -1.0)
@@ -75,10 +88,10 @@ def test_atcaldis3_needs_a_wall(cuda):
     s.close()
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(ALL))
 def test_met_bord_parity(cuda, name):
     torch = cuda
-    case = _seven(CASES[name]())
+    case = _seven(ALL[name]())
     orc, st = oracle_prepared(case)
     s = _gpu(case)
     v_o = st.v.copy()
@@ -179,11 +192,11 @@ def _sa_pair(case):
     return orc, st, s
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(ALL))
 def test_met_num_parity(cuda, name):
     """one transport step (met_num for 1SA) on the state after the mean-flow
     thermodynamics, time step and boundary conditions"""
-    case = _seven(CASES[name]())
+    case = _seven(ALL[name]())
     orc, st, s = _sa_pair(case)
     L = orc_lib()
     ld = case.layout.ld
@@ -199,7 +212,7 @@ def test_met_num_parity(cuda, name):
         getattr(s, name_).copy_(s.torch.as_tensor(a))
     s.torch.cuda.synchronize()
     s.sync()
-    L.orc_met_num(st.v, st.u, st.d, st.dt, st.mu, st.mut, st.sn, st.vol)
+    L.orc_met_num(st.v, st.u, st.d, st.dt, st.mu, st.mut, st.sn, st.vol, st.temp)
     s.met_num()
     s.sync()
     rc = case.layout.real_cells()
@@ -211,11 +224,11 @@ def test_met_num_parity(cuda, name):
     s.close()
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(ALL))
 def test_fused_rans_iterations_parity(cuda, name):
     """fused FP64 iterations with the SA step against the oracle's
     atsch_num + met_num sequence"""
-    case = _seven(CASES[name]())
+    case = _seven(ALL[name]())
     orc, st, s = _sa_pair(case)
     for _ in range(3):
         orc.step(st)
@@ -333,4 +346,61 @@ def test_fused_rans_iterations_stilde_fix_parity(cuda):
     v_g = s.v.cpu().numpy().reshape(7, ld)[:, rc]
     v_o = st.v.reshape(7, ld)[:, rc]
     assert_equal_bits(v_g[:6], v_o[:6], "state after 3 iterations")
+    s.close()
+
+
+def _lp2_first_cells(case):
+    ba = case.boundary_arrays()
+    sel = np.flatnonzero(ba["type"] == cases.BC_LP2)
+    return np.concatenate([ba["ncin"][ba["mpb"][b]:ba["mpb"][b] + ba["mmb"][b]] for b in sel])
+
+
+@pytest.mark.parametrize("name", sorted(WALL_LAW))
+def test_wall_law_parity(cuda, name):
+    """lpsa (block by block) and cllparoi1 after zvisqc, from the same
+    prepared state and a seeded eddy viscosity, bit for bit on every cell"""
+    torch = cuda
+    case = _seven(WALL_LAW[name]())
+    orc, st = oracle_prepared(case)
+    L = orc_lib()
+    ld = case.layout.ld
+    dist = np.zeros(ld)
+    assert L.orc_atcaldis3(st.x, st.y, st.z, dist) == 0
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_zpres(l, st.v, st.ps, st.temp, st.cson)
+        L.orc_zvismo(l, st.mu, st.temp)
+    L.orc_rbord(st.v, st.ps, st.temp, st.cson)
+    st.mut[:] = st.mu * (0.5 + cases.splitmix64_uniform(91, ld))
+    s = _gpu(case)
+    s.set_sa(_t(torch, dist), case.meta["rokinf"], 0.0, 1e-8)
+    g = {k: _t(torch, a) for k, a in (("v", st.v), ("mu", st.mu), ("mut", st.mut),
+                                      ("temp", st.temp), ("dist", dist))}
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_lpsa(l, st.v, st.mu, st.mut, dist, st.temp, 1e-8)
+        s.lpsa(l, g["v"], g["mu"], g["mut"], g["dist"], g["temp"])
+    s.sync()
+    ni = _lp2_first_cells(case)
+    assert np.isfinite(st.v.reshape(7, ld)[5, ni]).all()
+    assert_equal_bits(g["v"].cpu().numpy(), st.v, "v after lpsa")
+    assert_equal_bits(g["mut"].cpu().numpy(), st.mut, "mut after lpsa")
+    # the mean-flow stresses: zvisqc, then the wall law
+    L.orc_zvisqc(st.v, st.mu, st.mut, st.tau, st.sn, st.vol, st.temp)
+    tau = torch.zeros(9 * ld, dtype=torch.float64, device="cuda")
+    s.zvisqc(g["v"], g["mu"], g["mut"], tau, s.sn, s.vol, g["temp"])
+    tau_before = st.tau.copy()
+    L.orc_cllparoi1(st.v, dist, st.mu, st.mut, st.tau, st.temp)
+    s.cllparoi1(g["v"], g["dist"], g["mu"], g["mut"], tau, g["temp"])
+    s.sync()
+    assert not np.array_equal(tau_before.reshape(9, ld)[:, ni], st.tau.reshape(9, ld)[:, ni])
+    assert_equal_bits(tau.cpu().numpy(), st.tau, "tau after cllparoi1")
+    s.close()
+
+
+def test_wall_law_needs_the_wall_distance(cuda):
+    """the mean-flow wall law reads the wall distance of set_sa"""
+    from codens_b200 import abi
+    s = _gpu(WALL_LAW["channel_wl"]())
+    with pytest.raises(abi.CnsError) as ei:
+        s.atsch_num(1)
+    assert ei.value.code == abi.CNS_ENOTREADY
     s.close()

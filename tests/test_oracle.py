@@ -361,3 +361,18 @@ def test_portable_pow_and_exp_against_libm():
     assert worst["pow"] <= 8, worst
     assert L.orc_pow(0.0, 3.5) == 0.0 and L.orc_pow(2.0, 0.0) == 1.0
     assert math.isnan(L.orc_pow(-1.0, 0.5)) and L.orc_exp(-800.0) == 0.0
+
+
+def test_portable_asin_against_libm():
+    """the wall laws' Van Driest transform asin (cns_pmath.h: Taylor series
+    below 1/2, the half-angle identity above) within a few ulp of libm"""
+    L = lib()
+    rng = np.random.default_rng(4)
+    worst = 0
+    for x in np.concatenate([rng.uniform(-1.0, 1.0, 20000), rng.uniform(0.45, 0.55, 2000),
+                             rng.uniform(0.99, 1.0, 2000)]):
+        worst = max(worst, _ulps(L.orc_asin(x), math.asin(x)))
+    assert worst <= 4, worst
+    for x in (0.0, 0.5, 1.0, -1.0, 1e-300):
+        assert L.orc_asin(x) == math.asin(x)
+    assert math.copysign(1.0, L.orc_asin(-0.0)) < 0 and math.isnan(L.orc_asin(1.5))
