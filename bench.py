@@ -688,13 +688,20 @@ def run_adjoint(args):
         t_prep = time.perf_counter() - t0
         _, gW, _, _ = g.value_and_partials()
         g.solve_adjoint(gW)
-        g.adj_max = k
-        torch.cuda.synchronize()
-        a.record(g.s.stream)
-        g.solve_adjoint(gW)
-        e.record(g.s.stream)
-        e.synchronize()
-        ms_adj = a.elapsed_time(e) / k
+
+        def adjoint_ms(n):
+            # one solve of n iterations: set-up, an eager first iteration and
+            # the graph capture, then n - 1 replays
+            g.adj_max = n
+            torch.cuda.synchronize()
+            a.record(g.s.stream)
+            g.solve_adjoint(gW)
+            e.record(g.s.stream)
+            e.synchronize()
+            return a.elapsed_time(e)
+        # the per-iteration cost without the solve's fixed set-up: the
+        # difference of a 3k- and a k-iteration solve over 2k iterations
+        ms_adj = (adjoint_ms(3 * k) - adjoint_ms(k)) / (2 * k)
         g.close()
         # converged totals on a reduced channel
         dr = adjoint.Design(ni=128, nj=64, nk=4, precision=prec)

@@ -38,7 +38,8 @@ class Scheme_t(C.Structure):
                 ("qfix_dfez", c_i32), ("precision", c_i32), ("kdefect", c_i32),
                 ("ischema", c_i32), ("ki2", c_f64), ("ki4", c_f64), ("ncychro", c_i32),
                 ("icychr0", c_i32), ("kfmg", c_i32), ("kdualns", c_i32),
-                ("eta_l", P(c_f64)), ("ki2_l", P(c_f64)), ("ki4_l", P(c_f64))]
+                ("eta_l", P(c_f64)), ("ki2_l", P(c_f64)), ("ki4_l", P(c_f64)),
+                ("weno_fix", c_i32)]
 
 
 class Bnd_t(C.Structure):
@@ -78,6 +79,7 @@ EXPORTS = [
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
     "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
     "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov", "cns_sch_ausmp",
+    "cns_sch_weno5_3d",
 ]
 
 _lib = None
@@ -171,6 +173,7 @@ def load(build_if_missing: bool = True):
     L.cns_sch_hllc_euler.argtypes = L.cns_sch_roe_euler.argtypes
     L.cns_sch_hllc.argtypes = L.cns_sch_roe.argtypes
     L.cns_sch_rusanov.argtypes = L.cns_sch_roe.argtypes
+    L.cns_sch_weno5_3d.argtypes = L.cns_sch_roe.argtypes[:-2] + [vp]
     L.cns_sch_ausmp.argtypes = ([vp, C.c_int, C.c_int, vp, vp, vp, vp] + [vp] * 9 +
                                 [cs, vp, i64] + [vp] * 11)
     L.cns_set_cycle.argtypes = [vp, c_i64, c_i64]

@@ -88,6 +88,7 @@ class Scheme:
     eta_l: Optional[Sequence[float]] = None   # per block eta(lm) (else eta for all)
     ki2_l: Optional[Sequence[float]] = None   # per block ki2(lm)
     ki4_l: Optional[Sequence[float]] = None   # per block ki4(lm)
+    weno_fix: int = 0    # non-reference: WENO5 sums all three candidates everywhere
 
 
 @dataclass

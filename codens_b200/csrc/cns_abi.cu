@@ -285,6 +285,11 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
                      const double* tau, const double* sn, const double* ps) {
   const long long ld = c->lay.ld;
   cudaError_t e = cudaSuccess;
+  // WENO5 (no limiter) reads the stresses whatever the equations; NULL: the
+  // zero stresses the Euler equations leave (inivec.f90:93, zvisqc not run)
+  if (c->sc.ischema == 12)
+    return launch_weno5(c->d_blks, c->cells.view(l0), c->ph, c->sc.weno_fix, v, ld, ps,
+                        tau ? tau : c->w.tau0, sn, c->w.G, c->w.V, u, nullptr, c->st);
   if (c->sc.ns && c->sc.ilim == 1)
     e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
   if (e == cudaSuccess && c->res_fused && residual_fused_ok(c->sc))
@@ -453,11 +458,18 @@ cudaError_t forcing_add(cns_ctx* c, int l, const double* u, const double* ff, do
   return cudaGetLastError();
 }
 
-// the HLLC viscous halves (sch_hllc with the stresses), allocated when the
-// scheme first asks for them (never inside a graph capture)
+// the viscous halves of the HLLC faces (sch_hllc with the stresses) and of
+// the WENO5 faces, and WENO5's zero stresses for the Euler equations,
+// allocated when the scheme first asks for them (never inside a graph
+// capture)
 cudaError_t ensure_hllc_v(cns_ctx* c) {
-  if (c->w.V || c->sc.ischema != 14 || !c->sc.ns) return cudaSuccess;
-  return dev_alloc(c, &c->w.V, (size_t)(12 * c->lay.ld));
+  const bool weno = c->sc.ischema == 12;
+  if (!c->w.V && (weno || (c->sc.ischema == 14 && c->sc.ns))) {
+    cudaError_t e = dev_alloc(c, &c->w.V, (size_t)(12 * c->lay.ld));
+    if (e != cudaSuccess) return e;
+  }
+  if (!c->w.tau0 && weno && !c->sc.ns) return dev_alloc(c, &c->w.tau0, (size_t)(9 * c->lay.ld));
+  return cudaSuccess;
 }
 
 cudaError_t ensure_dis(cns_ctx* c) {
@@ -653,7 +665,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
       e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
                              s.pression, s.tau, s.sn, c->w.dis, c->w.G, s.u, nullptr, c->st);
     else
-      e = residual(c, -1, s.u, s.v, s.tau, s.sn, s.pression);
+      e = residual(c, -1, s.u, s.v, c->sc.ns ? s.tau : nullptr, s.sn, s.pression);
   }
   if (e == cudaSuccess && c->sc.kfmg == 3) e = enqueue_dual(c, nullptr);
   if (e == cudaSuccess)
@@ -761,6 +773,10 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
       if (e == cudaSuccess)
         e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
                                s.pression, s.tau, s.sn, w.dis, w.G, s.u, w.u32, c->st);
+    } else if (c->sc.ischema == 12) {
+      if (e == cudaSuccess)
+        e = launch_weno5(c->d_blks, all, c->ph, c->sc.weno_fix, s.v, ld, s.pression,
+                         c->sc.ns ? s.tau : w.tau0, s.sn, w.G, w.V, s.u, w.u32, c->st);
     } else {
       if (e == cudaSuccess && lim)
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
@@ -1237,14 +1253,15 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   if (s->lmax < 0 || s->muscl < 0 || (s->ilim != 0 && s->ilim != 1) ||
       s->precision < 0 || s->precision > 2 || (s->precision == 2 && s->kdefect < 1) ||
       (s->ischema != 1 && s->ischema != 7 && s->ischema != 9 && s->ischema != 14 &&
-       s->ischema != 5) ||
+       s->ischema != 5 && s->ischema != 12) ||
       (s->ischema == 5 && !s->ns) ||
       (s->ischema != 7 && s->precision == 2) ||
       (s->kfmg != 0 && s->kfmg != 3) ||
       (s->kfmg == 3 && (!(s->dt1min > 0.) || s->kdualns < 0 || s->kdualns > 2)))
     return fail(c, CNS_EINVAL,
                 "scheme: lmax >= 0, muscl >= 0, ilim in {0,1}, precision in {0,1,2}, "
-                "kdefect >= 1, ischema in {1,5,7,9,14} (5: ns only; defect correction: Roe only), kfmg in "
+                "kdefect >= 1, ischema in {1,5,7,9,12,14} (5: ns only; defect correction: Roe "
+                "only), kfmg in "
                 "{0,3} (3: dt1min > 0, kdualns in {0,1,2})");
   c->sc.ns = s->ns;
   c->sc.muscl = s->muscl;
@@ -1264,6 +1281,7 @@ int cns_set_scheme(cns_ctx* c, const cns_scheme_t* s) {
   c->sc.icychr0 = s->icychr0;
   c->sc.kfmg = s->kfmg;
   c->sc.kdualns = s->kdualns;
+  c->sc.weno_fix = s->weno_fix ? 1 : 0;
   // eta(lm), ki2(lm), ki4(lm): per block when given, else the scalars
   for (size_t b = 0; b < c->lay.blks.size(); ++b) {
     Blk& B = c->lay.blks[b];
@@ -1516,6 +1534,17 @@ int cns_sch_rusanov(cns_ctx* c, int lm, int ityprk, double* u, const double* v, 
   // sch_rusanov.f90 reads the stresses whatever the equations (zero for Euler)
   const double* t9[9] = {CNS_TAU9};
   return flux_entry(c, lm, ityprk, 9, equat && equat[0] == 'n', u, v, ff, t9, equat, sn,
+                    lgsnlt, ps);
+}
+
+int cns_sch_weno5_3d(cns_ctx* c, int lm, int ityprk, double* u, const double* v, double* ff,
+                     CNS_TAU9_ARGS, const char* equat, const double* sn, int64_t lgsnlt,
+                     double* fxx, double* fyy, double* fzz, double* fxy, double* fxz, double* fyz,
+                     double* fex, double* fey, double* fez, const double* ps) {
+  (void)fxx, (void)fyy, (void)fzz, (void)fxy, (void)fxz, (void)fyz, (void)fex, (void)fey,
+      (void)fez;
+  const double* t9[9] = {CNS_TAU9};
+  return flux_entry(c, lm, ityprk, 12, equat && equat[0] == 'n', u, v, ff, t9, equat, sn,
                     lgsnlt, ps);
 }
 

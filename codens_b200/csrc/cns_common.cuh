@@ -55,6 +55,7 @@ struct Scheme {
   double ki2, ki4;  // Jameson dissipation coefficients
   int ncychro, icychr0;  // time-step update frequency of the fused iteration
   int kfmg, kdualns;     // 3: dual time stepping (dt1min = physical step); its order
+  int weno_fix;          // WENO5: all three candidates in every direction (non-reference)
 };
 
 // 2.5D tiles of the implicit sweeps: tile t = (block, i0, j0, k0) covers

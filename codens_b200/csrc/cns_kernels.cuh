@@ -122,7 +122,8 @@ struct Work {
   double* dtpart = nullptr;   // global time step: per-tile minima + the result
   double* G = nullptr;        // face fluxes, [3][5][ld]
   double* R = nullptr;        // limiter ratios, [3][5][ld]
-  double* V = nullptr;        // HLLC viscous halves, [3][4][ld] (ischema 14 with ns)
+  double* V = nullptr;        // viscous halves, [3][4][ld] (ischema 14 with ns, ischema 12)
+  double* tau0 = nullptr;     // zero stresses [9][ld] (ischema 12 with the Euler equations)
   double* coefe = nullptr;    // [3][ld]
   double* coefdiag = nullptr; // [ld]
   double* rv = nullptr;       // [ld]
@@ -411,6 +412,17 @@ inline cudaError_t launch_face_flux(const Blk* blks, const SpaceBuf* faces, int 
   return launch_face_flux_t<double>(blks, faces, l0, ph, sc, v, prim, ld, ps, tau, sn, R, G,
                                     st, V);
 }
+// WENO5 residual (sch_weno5_3d.f90, ischema 12) over the real cells of the
+// space: u = the flux balance (every real cell written); tau: the nine
+// stress arrays (zero for the Euler equations); G [3][5][ld] and
+// V [3][4][ld]: face scratch; u32 (optional): u rounded to FP32 for the
+// mixed sweeps; fix: the non-reference option that sums all three weighted
+// candidates in every direction and flux component
+cudaError_t launch_weno5(const Blk* blks, Space cells, Phys ph, int fix, const double* v,
+                         long long ld,
+                         const double* ps, const double* tau, const double* sn, double* G,
+                         double* V, double* u, float* u32, cudaStream_t st);
+
 inline cudaError_t launch_accumulate(const Blk* blks, Space sp, const double* G,
                                      long long ld, double* u, cudaStream_t st,
                                      const double* V = nullptr) {

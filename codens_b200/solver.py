@@ -166,7 +166,8 @@ class CodeNS:
                             int(getattr(s, "ncychro", 1)), int(getattr(s, "icychr0", 0)),
                             int(getattr(s, "kfmg", 0)), int(getattr(s, "kdualns", 0)),
                             *(C.cast(keep[n], C.POINTER(C.c_double)) if keep[n] is not None
-                              else None for n in ("eta_l", "ki2_l", "ki4_l")))
+                              else None for n in ("eta_l", "ki2_l", "ki4_l")),
+                            int(getattr(s, "weno_fix", 0)))
 
     def _check(self, rc: int, where: str):
         if rc:
@@ -313,6 +314,14 @@ class CodeNS:
     def sch_hllc(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
         self._flux_ns(self.lib.cns_sch_hllc, "cns_sch_hllc", l, u, v, tau, sn, ps, ityprk, ff,
                       equat)
+
+    def sch_weno5_3d(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
+        """the WENO5 residual of block l (sch_weno5_3d.f90; tau is read with
+        either equations, zero for Euler)"""
+        snp, lg = self._sn(l, sn)
+        self._check(self.lib.cns_sch_weno5_3d(self.ctx, l, ityprk, _arr(u), _arr(v), _arr(ff),
+                                              *self._tau9(tau), equat or b"ns3d   ", snp, lg,
+                                              *([None] * 9), _arr(ps)), "cns_sch_weno5_3d")
 
     def sch_rusanov(self, l, u, v, tau, sn, ps, ityprk=0, ff=None, equat=None):
         self._flux_ns(self.lib.cns_sch_rusanov, "cns_sch_rusanov", l, u, v, tau, sn, ps, ityprk,

@@ -120,7 +120,8 @@ typedef struct {
                             the FP32 rounding level of the fluxes) */
   int32_t kdefect;       /* precision 2: the FP64 residual and the correction
                             R64 - R32 are refreshed every kdefect iterations */
-  int32_t ischema;       /* 7: Roe (sch_roe, sch_roe_euler); 14: HLLC; 9: Rusanov; 5: AUSM+; 1: Jameson
+  int32_t ischema;       /* 7: Roe (sch_roe, sch_roe_euler); 14: HLLC; 9: Rusanov; 5: AUSM+;
+                            12: WENO5 (sch_weno5_3d); 1: Jameson
                             (dissip_jameson + sch_jameson, kprec = 0) */
   double ki2, ki4;       /* Jameson 2nd/4th-difference coefficients (ki2(lm),
                             ki4(lm); one value for every block) */
@@ -137,6 +138,11 @@ typedef struct {
   const double *eta_l;   /* [nblk] eta(lm) of each block, or NULL: eta for all */
   const double *ki2_l;   /* [nblk] ki2(lm), or NULL: ki2 for all */
   const double *ki4_l;   /* [nblk] ki4(lm), or NULL: ki4 for all */
+  int32_t weno_fix;      /* non-reference option of ischema 12 (0 = reference):
+                            every characteristic flux sums its three weighted
+                            candidates; the reference sums only the first two
+                            in the j and k directions and in the z flux of the
+                            i direction, which no uniform flow survives */
 } cns_scheme_t;
 
 /* boundary lists (boundary module: mpb, mmb, ncbd, ncin, bceqt, ...) */
@@ -418,6 +424,23 @@ int cns_sch_rusanov(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v
                     const char *equat, const double *sn, int64_t lgsnlt, double *rhol,
                     double *ul, double *vl, double *wl, double *pl, double *rhor, double *ur,
                     double *vr, double *wr, double *prr, const double *ps);
+/* ischema 12 = WENO5 (sch_weno5_3d.f90:4-12, the 'xx3d' form of
+ * atsch_num.f90:898-919): Jiang & Shu's fifth-order reconstruction of the
+ * characteristic fluxes on Roe-averaged eigenvectors, upwinded by the sign
+ * of each eigenvalue, Henrick's mapped weights; the stresses tau enter
+ * whatever the equations (zero for Euler), a boundary face takes the flux of
+ * its ghost cell.  Near a block face the stencil reads the spare slots of
+ * the cell arrays (i = ni + 1, j = nj + 1, k = nk + 1) as the reference
+ * does; at the first interior k face its point k = -1 lies before the block,
+ * where the reference reads out of bounds, and this build reads the ghost
+ * plane k = 0 there.  fxx..fez: the reference's flux work arrays, not used */
+int cns_sch_weno5_3d(cns_ctx *ctx, int lm, int ityprk, double *u, const double *v, double *ff,
+                     const double *toxx, const double *toxy, const double *toxz,
+                     const double *toyy, const double *toyz, const double *tozz,
+                     const double *qcx, const double *qcy, const double *qcz,
+                     const char *equat, const double *sn, int64_t lgsnlt, double *fxx,
+                     double *fyy, double *fzz, double *fxy, double *fxz, double *fyz,
+                     double *fex, double *fey, double *fez, const double *ps);
 /* ischema 5 = AUSM+ (sch_ausmp.f90:4-11; the reference runs it for the
  * Navier-Stokes equations only: with the minmod limiter of ilim = 1, the
  * work and heat-flux terms of sch_ausmp.f90:81-83 from tau on the fly; d is

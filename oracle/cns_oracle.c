@@ -44,6 +44,7 @@ static struct {
   double *eta_l, *ki2_l, *ki4_l;
   /* dual time stepping (kfmg = 3): dt1min is the physical time step */
   int kfmg, kdualns, icycle;
+  int weno_fix; /* non-reference: WENO5 sums its three candidates everywhere */
   double *ptdual;
   /* boundary */
   int nbnd;
@@ -1766,6 +1767,251 @@ void orc_sch_rusanov(int l, double *u, const double *v, const double *tau, const
 }
 
 /* ------------------------------------------------------------------------ */
+/* WENO5 (sch_weno5_3d.f90, ischema 12): Jiang & Shu's fifth-order scheme,   */
+/* characteristic-wise on Roe-averaged eigenvectors, each field upwinded by  */
+/* the sign of its eigenvalue, with Henrick's mapped weights                 */
+/* ------------------------------------------------------------------------ */
+
+/* sch_weno5_3d.f90:148-166: the cell's flux tensor as the five values the
+ * projection reads per component c (0 x, 1 y, 2 z): rho u_c and the c-th
+ * column of the momentum and energy fluxes */
+static void weno_cell_flux(const double *v, const double *ps, int64_t n, double f[3][5]) {
+  const int64_t L = G.ld;
+  const double v1 = v[n], v2 = v[L + n], v3 = v[2 * L + n], v4 = v[3 * L + n],
+               v5 = v[4 * L + n], p = ps[n], pinfl = G.pinfl;
+  const double fxx = v2 * (v2 / v1) + p - pinfl, fxy = v3 * (v2 / v1), fxz = v4 * (v2 / v1);
+  const double fyy = v3 * (v3 / v1) + p - pinfl, fyz = v4 * (v3 / v1);
+  const double fzz = v4 * (v4 / v1) + p - pinfl;
+  const double fex = (v5 + p - pinfl) * v2 / v1, fey = (v5 + p - pinfl) * v3 / v1,
+               fez = (v5 + p - pinfl) * v4 / v1;
+  const double t[3][5] = {{v2, fxx, fxy, fxz, fex}, {v3, fxy, fyy, fyz, fey},
+                          {v4, fxz, fyz, fzz, fez}};
+  memcpy(f, t, sizeof(t));
+}
+
+/* Henrick's map g(w) = w (ga + ga^2 - 3 ga w + w^2) / (ga^2 + w (1 - 2 ga)):
+ * the numerator's and denominator's factors as sch_weno5_3d.f90:530-535
+ * writes them */
+static inline double weno_map_num(double ga, double w) {
+  return ga + ga * ga - 3. * ga * w + w * w;
+}
+static inline double weno_map_den(double ga, double w) { return ga * ga + w * (1. - 2. * ga); }
+
+/* one characteristic field (sch_weno5_3d.f90:333-620 for field 1): q holds
+ * its projected flux at the six points i-2..i+3; the three third-order
+ * candidates on the stencils upwind of the eigenvalue lam, their smoothness
+ * indicators (squared), the normalised weights mapped by Henrick's g and
+ * normalised again; the weighted sum of the first nterm candidates (the
+ * reference keeps three in the x and y fluxes of the i direction, two
+ * everywhere else) */
+static double weno_field(const double q[6], double lam, int nterm) {
+  const double c20 = 1. / 3., c21 = -7. / 6., c22 = 11. / 6., c10 = -1. / 6., c11 = 5. / 6.;
+  const double ga1 = 0.1, ga2 = 0.6, ga3 = 0.3, c1 = 13. / 12., c2 = 0.25, eps = 1.e-6;
+  const double sg = copysign(1., lam);
+  const double up = 0.5 * (1. + sg), dn = 0.5 * (1. - sg);
+  const double f1 = up * (q[0] * c20 + q[1] * c21 + q[2] * c22) +
+                    dn * (q[1] * c10 + q[2] * c11 + q[3] * c20);
+  const double f2 = up * (q[1] * c10 + q[2] * c11 + q[3] * c20) +
+                    dn * (q[2] * c20 + q[3] * c11 + q[4] * c10);
+  const double f3 = up * (q[2] * c20 + q[3] * c11 + q[4] * c10) +
+                    dn * (q[3] * c22 + q[4] * c21 + q[5] * c20);
+  const double s1 = sq(q[5] - 2. * q[4] + q[3]), s2 = sq(q[4] - 2. * q[3] + q[2]),
+               s3 = sq(q[3] - 2. * q[2] + q[1]), s4 = sq(q[2] - 2. * q[1] + q[0]);
+  const double t1 = sq(q[5] - 4. * q[4] + 3. * q[3]), t2 = sq(q[4] - 4. * q[3] + 3. * q[2]),
+               t3 = sq(q[4] - q[2]), t4 = sq(q[3] - q[1]),
+               t5 = sq(3. * q[3] - 4. * q[2] + q[1]), t6 = sq(3. * q[2] - 4. * q[1] + q[0]);
+  /* (...)**iexp with iexp = 2 */
+  const double b1 = sq(up * (c1 * s4 + c2 * t6) + dn * (c1 * s3 + c2 * t5) + eps);
+  const double b2 = sq(up * (c1 * s3 + c2 * t4) + dn * (c1 * s2 + c2 * t3) + eps);
+  const double b3 = sq(up * (c1 * s2 + c2 * t2) + dn * (c1 * s1 + c2 * t1) + eps);
+  const double ww1 = up * (ga1 / b1) + dn * (ga3 / b1);
+  const double ww2 = ga2 / b2;
+  const double ww3 = up * (ga3 / b3) + dn * (ga1 / b3);
+  const double sw = ww1 + ww2 + ww3;
+  const double w1 = ww1 / sw, w2 = ww2 / sw, w3 = ww3 / sw;
+  const double m1 = w1 * 0.5 * (1. + sg) * weno_map_num(ga1, w1) / weno_map_den(ga1, w1) +
+                    w1 * 0.5 * (1. - sg) * weno_map_num(ga3, w1) / weno_map_den(ga3, w1);
+  const double m2 = w2 * weno_map_num(ga2, w2) / weno_map_den(ga2, w2);
+  const double m3 = w3 * 0.5 * (1. + sg) * weno_map_num(ga3, w3) / weno_map_den(ga3, w3) +
+                    w3 * 0.5 * (1. - sg) * weno_map_num(ga1, w3) / weno_map_den(ga1, w3);
+  const double swm = m1 + m2 + m3;
+  const double x1 = m1 / swm, x2 = m2 / swm, x3 = m3 / swm;
+  return nterm == 3 ? x1 * f1 + x2 * f2 + x3 * f3 : x1 * f1 + x2 * f2;
+}
+
+/* the stencil point s (-2..3) of face n | n + ninc along dir: the flat index
+ * n + s ninc, as the reference forms it.  Near a block face it lands in the
+ * block's spare slots (i = ni + 1 of the row before or of the same row,
+ * j = nj + 1 of the plane before or of the same plane, k = nk + 1), which
+ * no cell routine writes; at the first interior k face (k = 1) the point
+ * k = -1 lies before the block, where the reference's flux work arrays are
+ * read out of bounds (undefined), and this restatement takes the ghost plane
+ * k = 0 there */
+static int64_t weno_point(const blk_t *b, int dir, int64_t n, int k, int s) {
+  if (dir == 2 && k + s < 0) return n - (int64_t)k * b->nijd;
+  return n + s * NINC(b, dir);
+}
+
+/* the interior face n | n1 = n + ninc (sch_weno5_3d.f90:240-1252): Roe
+ * average, left (Q) and right (P) eigenvectors, the x, y and z fluxes of the
+ * six stencil points reconstructed field by field, back to the conserved
+ * variables and projected on the face; fv the central viscous flux (times 2) */
+static void weno5_face(const blk_t *b, int dir, int64_t n, int k, const double *v,
+                       const double *ps, const double *tau, const double *sn, double df[5],
+                       double fv[5]) {
+  const int64_t L = G.ld, ninc = NINC(b, dir), n1 = n + ninc, m1 = n1 - b->npc;
+  const double gam = G.gam, gam1 = G.gam1;
+  const double s1 = SN(sn, b, m1, dir, 0), s2 = SN(sn, b, m1, dir, 1), s3 = SN(sn, b, m1, dir, 2);
+  const double cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const double nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
+  const double ul = v[L + n] / v[n], vl = v[2 * L + n] / v[n], wl = v[3 * L + n] / v[n];
+  const double ur = v[L + n1] / v[n1], vr = v[2 * L + n1] / v[n1], wr = v[3 * L + n1] / v[n1];
+  const double al = sqrt(gam * ps[n] / v[n]), ar = sqrt(gam * ps[n1] / v[n1]);
+  const double hl = al * al / gam1 + 0.5 * (ul * ul + vl * vl + wl * wl);
+  const double hr = ar * ar / gam1 + 0.5 * (ur * ur + vr * vr + wr * wr);
+  const double gd = sqrt(v[n1] / v[n]), gd1 = 1. / (1. + gd), gd2 = gd * gd1;
+  const double rhom = sqrt(v[n] * v[n1]), rhomi = 1. / rhom;
+  const double um = gd1 * ul + gd2 * ur, vm = gd1 * vl + gd2 * vr, wm = gd1 * wl + gd2 * wr;
+  const double hm = gd1 * hl + gd2 * hr;
+  const double vitm2 = 0.5 * (um * um + vm * vm + wm * wm);
+  const double am = sqrt(fabs(gam1 * (hm - vitm2)));
+  const double am2i = 1. / (am * am);
+  const double vn = um * nx + vm * ny + wm * nz;
+  const double rhoiam = rhom / am, rhoami = am2i / rhoiam;
+  const double lam[5] = {vn, vn, vn, vn + am, vn - am};
+  const double Q[5][5] = {
+      {(1. - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi, gam1 * um * nx * am2i,
+       gam1 * vm * nx * am2i + nz * rhomi, gam1 * wm * nx * am2i - ny * rhomi,
+       -gam1 * nx * am2i},
+      {(1. - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi,
+       gam1 * um * ny * am2i - nz * rhomi, gam1 * vm * ny * am2i,
+       gam1 * wm * ny * am2i + nx * rhomi, -gam1 * ny * am2i},
+      {(1. - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi,
+       gam1 * um * nz * am2i + ny * rhomi, gam1 * vm * nz * am2i - nx * rhomi,
+       gam1 * wm * nz * am2i, -gam1 * nz * am2i},
+      {gam1 * vitm2 * rhoami - vn * rhomi, nx * rhomi - gam1 * um * rhoami,
+       ny * rhomi - gam1 * vm * rhoami, nz * rhomi - gam1 * wm * rhoami, gam1 * rhoami},
+      {gam1 * vitm2 * rhoami + vn * rhomi, -nx * rhomi - gam1 * um * rhoami,
+       -ny * rhomi - gam1 * vm * rhoami, -nz * rhomi - gam1 * wm * rhoami, gam1 * rhoami}};
+  const double P[5][5] = {
+      {nx, ny, nz, 0.5 * rhoiam, 0.5 * rhoiam},
+      {um * nx, um * ny - rhom * nz, um * nz + rhom * ny, 0.5 * rhoiam * (um + nx * am),
+       0.5 * rhoiam * (um - nx * am)},
+      {vm * nx + rhom * nz, vm * ny, vm * nz - rhom * nx, 0.5 * rhoiam * (vm + ny * am),
+       0.5 * rhoiam * (vm - ny * am)},
+      {wm * nx - rhom * ny, wm * ny + rhom * nx, wm * nz, 0.5 * rhoiam * (wm + nz * am),
+       0.5 * rhoiam * (wm - nz * am)},
+      {vitm2 * nx + rhom * (vm * nz - wm * ny), vitm2 * ny + rhom * (wm * nx - um * nz),
+       vitm2 * nz + rhom * (um * ny - vm * nx), 0.5 * rhoiam * (hm + am * vn),
+       0.5 * rhoiam * (hm - am * vn)}};
+  double fl[6][3][5];
+  for (int p = 0; p < 6; ++p) weno_cell_flux(v, ps, weno_point(b, dir, n, k, p - 2), fl[p]);
+  double out[3][5];
+  for (int c = 0; c < 3; ++c) {
+    /* three candidates in the x and y fluxes of the i direction, two
+       elsewhere (sch_weno5_3d.f90:616, 911, 1206, 1639, 1934, 2229, 2662,
+       2957, 3252); the flagged fix sums three everywhere */
+    const int nterm = (G.weno_fix || (dir == 0 && c < 2)) ? 3 : 2;
+    double fc[5];
+    for (int kf = 0; kf < 5; ++kf) {
+      double q[6];
+      for (int p = 0; p < 6; ++p)
+        q[p] = Q[kf][0] * fl[p][c][0] + Q[kf][1] * fl[p][c][1] + Q[kf][2] * fl[p][c][2] +
+               Q[kf][3] * fl[p][c][3] + Q[kf][4] * fl[p][c][4];
+      fc[kf] = weno_field(q, lam[kf], nterm);
+    }
+    for (int r = 0; r < 5; ++r)
+      out[c][r] = fc[0] * P[r][0] + fc[1] * P[r][1] + fc[2] * P[r][2] + fc[3] * P[r][3] +
+                  fc[4] * P[r][4];
+  }
+  for (int r = 0; r < 5; ++r) df[r] = out[0][r] * s1 + out[1][r] * s2 + out[2][r] * s3;
+  const double *txx = tau, *txy = tau + L, *txz = tau + 2 * L, *tyy = tau + 3 * L,
+               *tyz = tau + 4 * L, *tzz = tau + 5 * L, *qx = tau + 6 * L, *qy = tau + 7 * L,
+               *qz = tau + 8 * L;
+  fv[0] = 0.;
+  fv[1] = (txx[n] + txx[n1]) * s1 + (txy[n] + txy[n1]) * s2 + (txz[n] + txz[n1]) * s3;
+  fv[2] = (txy[n] + txy[n1]) * s1 + (tyy[n] + tyy[n1]) * s2 + (tyz[n] + tyz[n1]) * s3;
+  fv[3] = (txz[n] + txz[n1]) * s1 + (tyz[n] + tyz[n1]) * s2 + (tzz[n] + tzz[n1]) * s3;
+  fv[4] = (txx[n] * ul + txy[n] * vl + txz[n] * wl + qx[n] + txx[n1] * ur + txy[n1] * vr +
+           txz[n1] * wr + qx[n1]) * s1 +
+          (txy[n] * ul + tyy[n] * vl + tyz[n] * wl + qy[n] + txy[n1] * ur + tyy[n1] * vr +
+           tyz[n1] * wr + qy[n1]) * s2 +
+          (txz[n] * ul + tyz[n] * vl + tzz[n] * wl + qz[n] + txz[n1] * ur + tyz[n1] * vr +
+           tzz[n1] * wr + qz[n1]) * s3;
+}
+
+/* sch_weno5_3d.f90:3302-3500: the flux through a boundary face from the
+ * ghost cell g alone (convective minus viscous), face vector s */
+static void weno5_boundary(int64_t g, const double *v, const double *ps, const double *tau,
+                           double s1, double s2, double s3, double f[5]) {
+  const int64_t L = G.ld;
+  double fl[3][5];
+  weno_cell_flux(v, ps, g, fl);
+  const double fxx = fl[0][1], fxy = fl[0][2], fxz = fl[0][3], fex = fl[0][4];
+  const double fyy = fl[1][2], fyz = fl[1][3], fey = fl[1][4], fzz = fl[2][3], fez = fl[2][4];
+  const double txx = tau[g], txy = tau[L + g], txz = tau[2 * L + g], tyy = tau[3 * L + g],
+               tyz = tau[4 * L + g], tzz = tau[5 * L + g], qx = tau[6 * L + g],
+               qy = tau[7 * L + g], qz = tau[8 * L + g];
+  const double v1 = v[g], v2 = v[L + g], v3 = v[2 * L + g], v4 = v[3 * L + g];
+  f[0] = v2 * s1 + v3 * s2 + v4 * s3;
+  f[1] = (fxx - txx) * s1 + (fxy - txy) * s2 + (fxz - txz) * s3;
+  f[2] = (fxy - txy) * s1 + (fyy - tyy) * s2 + (fyz - tyz) * s3;
+  f[3] = (fxz - txz) * s1 + (fyz - tyz) * s2 + (fzz - tzz) * s3;
+  f[4] = (fex - (txx * v2 + txy * v3 + txz * v4) / v1 - qx) * s1 +
+         (fey - (txy * v2 + tyy * v3 + tyz * v4) / v1 - qy) * s2 +
+         (fez - (txz * v2 + tyz * v3 + tzz * v4) / v1 - qz) * s3;
+}
+
+/* sch_weno5_3d.f90:146-3500 (ityprk = 0): u zeroed over the block; the
+ * interior faces of i (i = 1..ni-2), j, k in the reference's loop order, each
+ * adding to its upper cell first (u - df + fv/2) then its lower one
+ * (u + df - fv/2); then the boundary faces i1, i2, j1, j2, k1, k2 from their
+ * ghost cells.  tau: the nine stress and heat-flux arrays (zero for Euler) */
+void orc_set_weno_fix(int on) { G.weno_fix = on ? 1 : 0; }
+
+void orc_sch_weno5_3d(int l, double *u, const double *v, const double *tau, const double *sn,
+                      const double *ps) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc;
+  zero_u(b, u);
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    int hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+    hi[dir] -= 1;
+    for (int k = 1; k <= hi[2]; ++k)
+      for (int j = 1; j <= hi[1]; ++j)
+        for (int i = 1; i <= hi[0]; ++i) {
+          const int64_t n = IC(b, i, j, k), n1 = n + ninc;
+          double df[5], fv[5];
+          weno5_face(b, dir, n, k, v, ps, tau, sn, df, fv);
+          u[n1] = u[n1] - df[0];
+          for (int a = 1; a < 5; ++a) u[a * L + n1] = u[a * L + n1] - df[a] + 0.5 * fv[a];
+          u[n] = u[n] + df[0];
+          for (int a = 1; a < 5; ++a) u[a * L + n] = u[a * L + n] + df[a] - 0.5 * fv[a];
+        }
+  }
+  for (int dir = 0; dir < 3; ++dir) {
+    const int64_t ninc = NINC(b, dir);
+    const int nd = NDIR(b, dir);
+    for (int side = 0; side < 2; ++side) {
+      int lo[3] = {1, 1, 1}, hi[3] = {b->ni - 1, b->nj - 1, b->nk - 1};
+      lo[dir] = hi[dir] = side ? nd - 1 : 1;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            const int64_t n = IC(b, i, j, k), g = side ? n + ninc : n - ninc;
+            const int64_t mf = (side ? n + ninc : n) - n0;
+            double f[5];
+            weno5_boundary(g, v, ps, tau, SN(sn, b, mf, dir, 0), SN(sn, b, mf, dir, 1),
+                           SN(sn, b, mf, dir, 2), f);
+            for (int a = 0; a < 5; ++a)
+              u[a * L + n] = side ? u[a * L + n] + f[a] : u[a * L + n] - f[a];
+          }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
 /* viscous stresses                                                          */
 /* ------------------------------------------------------------------------ */
 
@@ -3213,6 +3459,8 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
     /* atsch_num.f90:628-983: the flux family by ischema */
     if (G.ischema == 9)
       orc_sch_rusanov(l, u, v, tau, sn, ps);
+    else if (G.ischema == 12)
+      orc_sch_weno5_3d(l, u, v, tau, sn, ps);
     else if (G.ischema == 5)
       orc_sch_ausmp(l, u, v, tau, sn, ps);
     else if (G.ischema == 14 && G.ns)

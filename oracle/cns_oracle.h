@@ -193,6 +193,14 @@ void orc_sch_hllc(int l, double *u, const double *v, const double *tau, const do
                   const double *ps);
 void orc_sch_rusanov(int l, double *u, const double *v, const double *tau, const double *sn,
                      const double *ps);
+/* ischema 12, WENO5 (sch_weno5_3d.f90; tau read whatever the equations,
+ * zero for Euler; the k = -1 stencil point, before the block, taken at the
+ * ghost plane k = 0) */
+void orc_sch_weno5_3d(int l, double *u, const double *v, const double *tau, const double *sn,
+                      const double *ps);
+/* non-reference option (0 = reference): every WENO5 characteristic flux
+ * sums its three weighted candidates */
+void orc_set_weno_fix(int on);
 /* ischema 5, AUSM+ (sch_ausmp.f90; Navier-Stokes only) */
 void orc_sch_ausmp(int l, double *u, const double *v, const double *tau, const double *sn,
                    const double *ps);

@@ -94,6 +94,8 @@ def lib():
         L.orc_sch_hllc_euler.argtypes = [C.c_int, _d, _d, _d, _d]
         L.orc_sch_hllc.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_sch_rusanov.argtypes = [C.c_int, _d, _d, _d, _d, _d]
+        L.orc_sch_weno5_3d.argtypes = [C.c_int, _d, _d, _d, _d, _d]
+        L.orc_set_weno_fix.argtypes = [C.c_int]
         L.orc_sch_ausmp.argtypes = [C.c_int, _d, _d, _d, _d, _d]
         L.orc_set_dual.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_sch_dual.argtypes = [C.c_int, _d, _d, C.c_int, _d, _d]
@@ -164,6 +166,7 @@ class Oracle:
                              s.dt1min, s.lmax, int(getattr(s, "qfix_dfez", 0)))
         lib().orc_set_dissipation(int(getattr(s, "ischema", 7)), float(getattr(s, "ki2", 0.5)),
                                   float(getattr(s, "ki4", 1.0 / 32.0)))
+        lib().orc_set_weno_fix(int(getattr(s, "weno_fix", 0)))
         self.jameson = int(getattr(s, "ischema", 7)) <= 4
         self._block = [None if getattr(s, n, None) is None
                        else np.ascontiguousarray(getattr(s, n), dtype=np.float64)
