@@ -42,6 +42,10 @@ class Scheme_t(C.Structure):
                 ("weno_fix", c_i32)]
 
 
+class Ke_t(C.Structure):
+    _fields_ = [("rokinf", c_f64), ("roeinf", c_f64), ("epsk", c_f64), ("epse", c_f64)]
+
+
 class Bnd_t(C.Structure):
     _fields_ = [("nbnd", c_i32), ("type", P(c_i32)), ("blk", P(c_i32)),
                 ("face", P(c_i32)), ("mpb", P(c_i64)), ("mmb", P(c_i32)),
@@ -75,7 +79,8 @@ EXPORTS = [
     "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
     "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
     "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
-    "cns_set_sa", "cns_met_num", "cns_lpsa", "cns_cllparoi1",
+    "cns_set_sa", "cns_met_num", "cns_lpsa", "cns_cllparoi1", "cns_set_ke", "cns_met_prod",
+    "cns_met_smke", "cns_met_kemut", "cns_met_cutke",
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
     "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
     "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov", "cns_sch_ausmp",
@@ -157,6 +162,11 @@ def load(build_if_missing: bool = True):
     L.cns_set_sa.argtypes = [vp, P(Sa_t)]
     L.cns_met_num.argtypes = [vp]
     L.cns_lpsa.argtypes = [vp, C.c_int] + [vp] * 5
+    L.cns_set_ke.argtypes = [vp, C.POINTER(Ke_t)]
+    L.cns_met_prod.argtypes = [vp, C.c_int, C.c_int] + [vp] * 4
+    L.cns_met_smke.argtypes = [vp, C.c_int] + [vp] * 10
+    L.cns_met_kemut.argtypes = [vp, C.c_int] + [vp] * 3
+    L.cns_met_cutke.argtypes = [vp, C.c_int, vp, c_f64, c_f64]
     L.cns_cllparoi1.argtypes = [vp] * 7
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_set_residual_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int]

@@ -23,7 +23,8 @@ LIB = os.path.join(HERE, "libcodens_b200.so")
 # only; its FP64 residual keeps IEEE division), which the mixed form's FP64
 # fixed point does not depend on.
 SOURCES = ["cns_geom.cu", "cns_flow.cu", "cns_jameson.cu", "cns_turb.cu", "cns_sa.cu",
-           "cns_adjoint.cu", "cns_abi.cu", "cns_noalloc.cu", "cns_io.cu", "cns_weno.cu"]
+           "cns_adjoint.cu", "cns_abi.cu", "cns_noalloc.cu", "cns_io.cu", "cns_weno.cu",
+           "cns_ke.cu"]
 SOURCES_FMA = ["cns_mixed.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 OBJDIR = os.path.join(HERE, "_build")

@@ -36,6 +36,12 @@ struct cns_ctx {
   double* sa_fd = nullptr;          // diffusion densities fd5x..fd6z [6][ld]
   double* sa_ts = nullptr;          // sources ts6, ts7 [2][ld]
   double* sa_cfke = nullptr;        // source-derivative bound [ld]
+  // k-epsilon transport step of the fused iteration (cns_set_ke); it shares
+  // the SA step's gradient, diffusion-density, source and line scratch
+  bool ke_on = false;
+  double ke_rokinf = 0., ke_roeinf = 0., ke_epsk = 0., ke_epse = 0.;
+  double* ke_tprod = nullptr;       // production of k [ld]
+  double* ke_w = nullptr;           // met_smke scratch [14][ld]
   long long n_wall_ent = 0;
   long long* d_wall_ents = nullptr;  // list entries of the wall boundaries
   // the wall-law walls 'lp2' in list order: first list entry, count, block
@@ -285,11 +291,10 @@ cudaError_t residual(cns_ctx* c, int l0, double* u, const double* v,
                      const double* tau, const double* sn, const double* ps) {
   const long long ld = c->lay.ld;
   cudaError_t e = cudaSuccess;
-  // WENO5 (no limiter) reads the stresses whatever the equations; NULL: the
-  // zero stresses the Euler equations leave (inivec.f90:93, zvisqc not run)
+  // WENO5 (no limiter) reads the stresses whatever the equations
   if (c->sc.ischema == 12)
-    return launch_weno5(c->d_blks, c->cells.view(l0), c->ph, c->sc.weno_fix, v, ld, ps,
-                        tau ? tau : c->w.tau0, sn, c->w.G, c->w.V, u, nullptr, c->st);
+    return launch_weno5(c->d_blks, c->cells.view(l0), c->ph, c->sc.weno_fix, v, ld, ps, tau, sn,
+                        c->w.G, c->w.V, u, nullptr, c->st);
   if (c->sc.ns && c->sc.ilim == 1)
     e = launch_ratio(c->d_blks, c->lines, l0, v, c->w.prim, ld, ps, c->w.R, c->st);
   if (e == cudaSuccess && c->res_fused && residual_fused_ok(c->sc))
@@ -472,6 +477,11 @@ cudaError_t ensure_hllc_v(cns_ctx* c) {
   return cudaSuccess;
 }
 
+// the fused iteration of WENO5 with the Euler equations reads the zero
+// stresses the reference leaves there (inivec.f90:93; zvisqc does not run),
+// not the bound stress array
+bool weno_euler(const cns_ctx* c) { return c->sc.ischema == 12 && !c->sc.ns; }
+
 cudaError_t ensure_dis(cns_ctx* c) {
   if (c->w.dis) return cudaSuccess;
   return dev_alloc(c, &c->w.dis, (size_t)(5 * c->lay.ld));
@@ -571,7 +581,64 @@ cudaError_t enqueue_cllparoi1(cns_ctx* c, const double* v, const double* mu, con
   return e;
 }
 
+// met_num.f90:145-790 for '2JL ' on the bound (ld, 7) state, after rbord:
+// met_bord; per block teq_gradv, met_prod, met_gradtr, met_smke (met_exgr,
+// met_bark, met_bare, met_smkes) and met_fludc; met_rbse + met_rbsc; then
+// over all blocks met_roe2o(h), sch_turb, impli2_eqt_3d (cmt = 1,
+// impli2_eqt_3d.f90:85), met_cutke; met_kemut
+cudaError_t enqueue_met_num_ke(cns_ctx* c) {
+  const cns_state_t& s = c->state;
+  const long long ld = c->lay.ld;
+  const int nb = (int)c->lay.blks.size();
+  double* fd = c->sa_fd;
+  double* const fdw[6] = {fd, fd + ld, fd + 2 * ld, fd + 3 * ld, fd + 4 * ld, fd + 5 * ld};
+  const double* const fdr[6] = {fdw[0], fdw[1], fdw[2], fdw[3], fdw[4], fdw[5]};
+  double* ts6 = c->sa_ts;
+  double* ts7 = c->sa_ts + ld;
+  cudaError_t e = launch_turb_bord(c->bd, s.v, ld, c->ke_rokinf, c->ke_roeinf, c->st);
+  for (int b = 0; b < nb && e == cudaSuccess; ++b) {
+    const Space cb = c->cells.view(b);
+    long long b0, b1, n0, n1;
+    block_range(c, b + 1, b0, b1);
+    fludc_range(c, b + 1, n0, n1);
+    e = launch_teq_grads(c->d_blks, cb, 0, 3, s.v, nullptr, ld, s.sn, s.vol, c->sa_dv, c->sa_sc,
+                         b0, b1, c->st);
+    if (e == cudaSuccess)
+      e = launch_met_prod(c->d_blks, cb, ld, s.mut, s.v, c->sa_dv, c->ke_tprod, c->st);
+    for (int q = 0; q < 6 && e == cudaSuccess; ++q)
+      e = cudaMemsetAsync(fdw[q] + n0, 0, sizeof(double) * (size_t)(n1 - n0 + 1), c->st);
+    if (e == cudaSuccess)
+      e = launch_teq_grads(c->d_blks, cb, 2, 2, s.v, nullptr, ld, s.sn, s.vol, fd, c->sa_sc, b0,
+                           b1, c->st);
+    if (e == cudaSuccess) e = launch_exgr(c->lay.blks[b], ld, c->sa_dv, c->st);
+    if (e == cudaSuccess)
+      e = launch_smke(c->d_blks, cb, ld, s.v, s.mu, s.mut, s.sn, s.vol, c->ke_tprod, c->sa_dv,
+                      c->ke_w, ts6, ts7, c->sa_cfke, b0, b1, c->st);
+    if (e == cudaSuccess) e = launch_fludc(n0, n1, s.mu, s.mut, fdw, c->alfak, c->alfae, c->st);
+  }
+  if (e == cudaSuccess) e = launch_fd_ghosts(c->bd, fdw, c->st);
+  const Space all = c->cells.view(-1);
+  if (e == cudaSuccess)
+    e = launch_roe2o(c->d_blks, c->faces, c->cells_ext.view(-1), -1, sa_harten(c), c->epsroe,
+                     c->ph.gam, c->ph.gam1, s.v, ld, s.sn, c->w.G, s.d, c->st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(s.u + 5 * ld, 0, sizeof(double) * c->lay.ncells, c->st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(s.u + 6 * ld, 0, sizeof(double) * c->lay.ncells, c->st);
+  if (e == cudaSuccess)
+    e = launch_sch_turb(c->d_blks, c->faces, all, -1, s.v, ld, fdr, ts6, ts7, s.d, s.sn, s.vol,
+                        c->w.G, s.u, c->st);
+  if (e == cudaSuccess)
+    e = launch_impli2(c->d_blks, c->faces, c->lines, all, -1, ld, s.u, s.dt, s.v, s.mu, s.mut,
+                      c->sa_cfke, s.sn, s.vol, 1.0, c->sa_w, c->sc.precision != 0, nullptr, 0,
+                      c->st);
+  if (e == cudaSuccess) e = launch_cutke(c->d_blks, all, ld, s.v, c->ke_epsk, c->ke_epse, c->st);
+  if (e == cudaSuccess) e = launch_kemut(c->d_blks, all, ld, s.v, s.mu, s.mut, c->st);
+  return e;
+}
+
 cudaError_t enqueue_met_num(cns_ctx* c) {
+  if (c->ke_on) return enqueue_met_num_ke(c);
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   const int nb = (int)c->lay.blks.size();
@@ -651,7 +718,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
-  if (e == cudaSuccess && c->sa_on) e = enqueue_met_num(c);
+  if (e == cudaSuccess && (c->sa_on || c->ke_on)) e = enqueue_met_num(c);
   if (e == cudaSuccess) e = launch_prim(0, c->lay.ncells, s.v, ld, c->w.prim, c->st);
   if (e == cudaSuccess && c->sc.ns) {
     e = launch_grad(c->d_blks, all, c->ph, s.v, c->w.prim, ld, s.mu, s.mut, s.tau, s.sn,
@@ -665,7 +732,7 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
       e = launch_sch_jameson(c->d_blks, c->faces, all, -1, c->sc.ns, c->ph.pinfl, s.v, ld,
                              s.pression, s.tau, s.sn, c->w.dis, c->w.G, s.u, nullptr, c->st);
     else
-      e = residual(c, -1, s.u, s.v, c->sc.ns ? s.tau : nullptr, s.sn, s.pression);
+      e = residual(c, -1, s.u, s.v, weno_euler(c) ? c->w.tau0 : s.tau, s.sn, s.pression);
   }
   if (e == cudaSuccess && c->sc.kfmg == 3) e = enqueue_dual(c, nullptr);
   if (e == cudaSuccess)
@@ -738,7 +805,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
-  if (e == cudaSuccess && c->sa_on) e = enqueue_met_num(c);
+  if (e == cudaSuccess && (c->sa_on || c->ke_on)) e = enqueue_met_num(c);
   if (e == cudaSuccess)
     e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression, w.v32, w.prim32,
                            w.ps32, c->st);
@@ -776,7 +843,7 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
     } else if (c->sc.ischema == 12) {
       if (e == cudaSuccess)
         e = launch_weno5(c->d_blks, all, c->ph, c->sc.weno_fix, s.v, ld, s.pression,
-                         c->sc.ns ? s.tau : w.tau0, s.sn, w.G, w.V, s.u, w.u32, c->st);
+                         weno_euler(c) ? w.tau0 : s.tau, s.sn, w.G, w.V, s.u, w.u32, c->st);
     } else {
       if (e == cudaSuccess && lim)
         e = launch_ratio(c->d_blks, c->lines, -1, s.v, w.prim, ld, s.pression, w.R, c->st);
@@ -1898,13 +1965,77 @@ int cns_set_sa(cns_ctx* c, const cns_sa_t* sa) {
   c->sa_epsk = sa->epsk;
   c->sa_fix = sa->stilde_fix ? 1 : 0;
   c->sa_on = true;
+  c->ke_on = false;
+  return CNS_OK;
+}
+
+int cns_set_ke(cns_ctx* c, const cns_ke_t* ke) {
+  if (!c) return CNS_EINVAL;
+  drop_graphs(c);
+  if (!ke) {
+    c->ke_on = false;
+    return CNS_OK;
+  }
+  if (!c->sc.ns)
+    return fail(c, CNS_EINVAL, "the k-epsilon step needs the Navier-Stokes equations");
+  if (!c->lp2.empty())
+    return fail(c, CNS_EINVAL, "the k-epsilon step has no wall law ('lp2' walls)");
+  if (!(ke->epsk > 0.) || !(ke->epse > 0.))
+    return fail(c, CNS_EINVAL, "k-epsilon: epsk and epse must be positive");
+  CK(ensure_sa_step(c));
+  const size_t ld = (size_t)c->lay.ld;
+  if (!c->ke_tprod) CK(dev_alloc(c, &c->ke_tprod, ld));
+  if (!c->ke_w) CK(dev_alloc(c, &c->ke_w, 14 * ld));
+  c->ke_rokinf = ke->rokinf;
+  c->ke_roeinf = ke->roeinf;
+  c->ke_epsk = ke->epsk;
+  c->ke_epse = ke->epse;
+  c->ke_on = true;
+  c->sa_on = false;
+  c->sa_dist = nullptr;
+  return CNS_OK;
+}
+
+int cns_met_prod(cns_ctx* c, int l, int ncyc, const double* mut, const double* s,
+                 const double* dv, double* tprod) {
+  (void)ncyc;  // in met_prod.f90:4-8's argument list, not read
+  if (!c || bad_block(c, l) || !mut || !s || !dv || !tprod) return CNS_EINVAL;
+  CK(launch_met_prod(c->d_blks, c->cells.view(l - 1), c->lay.ld, mut, s, dv, tprod, c->st));
+  return CNS_OK;
+}
+
+int cns_met_smke(cns_ctx* c, int l, const double* sn, const double* vol, const double* v,
+                 const double* mu, const double* mut, const double* tprod, double* cfke,
+                 double* dv, double* qcxts5, double* qcyts6) {
+  if (!c || bad_block(c, l) || !sn || !vol || !v || !mu || !mut || !tprod || !cfke || !dv ||
+      !qcxts5 || !qcyts6)
+    return CNS_EINVAL;
+  CK(ensure_sa(c));
+  if (!c->ke_w) CK(dev_alloc(c, &c->ke_w, 14 * (size_t)c->lay.ld));
+  long long b0, b1;
+  block_range(c, l, b0, b1);
+  CK(launch_exgr(c->lay.blks[l - 1], c->lay.ld, dv, c->st));
+  CK(launch_smke(c->d_blks, c->cells.view(l - 1), c->lay.ld, v, mu, mut, sn, vol, tprod, dv,
+                 c->ke_w, qcxts5, qcyts6, cfke, b0, b1, c->st));
+  return CNS_OK;
+}
+
+int cns_met_kemut(cns_ctx* c, int l, const double* v, const double* mu, double* mut) {
+  if (!c || bad_block(c, l) || !v || !mu || !mut) return CNS_EINVAL;
+  CK(launch_kemut(c->d_blks, c->cells.view(l - 1), c->lay.ld, v, mu, mut, c->st));
+  return CNS_OK;
+}
+
+int cns_met_cutke(cns_ctx* c, int l, double* v, double epsk, double epse) {
+  if (!c || bad_block(c, l) || !v) return CNS_EINVAL;
+  CK(launch_cutke(c->d_blks, c->cells.view(l - 1), c->lay.ld, v, epsk, epse, c->st));
   return CNS_OK;
 }
 
 int cns_met_num(cns_ctx* c) {
   if (!c) return CNS_EINVAL;
-  if (!c->bound || !c->sa_on)
-    return fail(c, CNS_ENOTREADY, "bind the state and enable the Spalart-Allmaras step first");
+  if (!c->bound || !(c->sa_on || c->ke_on))
+    return fail(c, CNS_ENOTREADY, "bind the state and enable a turbulence step first");
   CK(enqueue_met_num(c));
   return CNS_OK;
 }
@@ -2113,7 +2244,8 @@ int cns_atsch_num_launch(cns_ctx* c, int nsteps) {
     const cns_state_t& s = c->state;
     if (!s.ptdual || !s.vdual || !s.vdual1 || !s.vdual2)
       return fail(c, CNS_ENOTREADY, "dual time stepping: bind ptdual, vdual, vdual1, vdual2");
-    if (c->sa_on) return fail(c, CNS_EINVAL, "dual time stepping with the SA step");
+    if (c->sa_on || c->ke_on)
+      return fail(c, CNS_EINVAL, "dual time stepping with a turbulence step");
   }
   if (c->sc.ns && !c->lp2.empty() && !c->sa_dist)
     return fail(c, CNS_ENOTREADY, "the wall law of the 'lp2' walls needs the wall distance "
@@ -2261,8 +2393,8 @@ int cns_atsch_num_step(cns_ctx* c, int nsteps, double* norms) {
 int cns_atsch_num_step_host(cns_ctx* c, double* v_host, int nsteps, double* norms) {
   if (!c || !v_host) return CNS_EINVAL;
   if (!c->bound) return fail(c, CNS_ENOTREADY, "bind the state first");
-  // the (ld, 5) state, or (ld, 7) with the Spalart-Allmaras step
-  const size_t bytes = sizeof(double) * (c->sa_on ? 7 : 5) * (size_t)c->lay.ld;
+  // the (ld, 5) state, or (ld, 7) with a turbulence step
+  const size_t bytes = sizeof(double) * (c->sa_on || c->ke_on ? 7 : 5) * (size_t)c->lay.ld;
   CK(cudaMemcpyAsync(c->state.v, v_host, bytes, cudaMemcpyHostToDevice, c->st));
   int rc = cns_atsch_num_step(c, nsteps, norms);
   if (rc) return rc;

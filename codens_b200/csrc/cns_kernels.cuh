@@ -316,7 +316,8 @@ cudaError_t launch_sch_turb(const Blk* blks, const SpaceBuf* faces, Space cells,
 
 // teq_grads over the cells of the space into out[3 nsc][ld]: mode 0 = the
 // velocity (nsc 3), mode 1 = the fields f[q][ld], mode 2 = the transport
-// variables per unit mass s6/s1, s7/s1 (nsc 2, met_gradtr); modes 0 and 2
+// variables per unit mass s6/s1, s7/s1 (nsc 2, met_gradtr), mode 3 =
+// sqrt(s6/s1) (nsc 1, met_bark); modes 0, 2 and 3
 // evaluate their scalars once into sc[nsc][ld] over the flat range [n0, n1)
 // covering the cells of the space and their ghosts.  met_smsa with its
 // gradients of rho nu~ (grt) and rho (grr)
@@ -360,6 +361,23 @@ cudaError_t launch_wall_dist(const Bnd& bd, const Blk* blks, Space cells,
                              const long long* went, long long nw, const double* x,
                              const double* y, const double* z, double* par, double* dist,
                              cudaStream_t st);
+// the k-epsilon model of Jones & Launder ('2JL'): met_prod (tprod [ld]),
+// met_exgr on the nine velocity gradients dv [9][ld] of block B, met_smke
+// (met_bark + met_bare + met_smkes: ts6, ts7, cfke; w: 14 ld scratch; the
+// flat range [n0, n1) holds the block's cells), met_kemut, met_cutke
+cudaError_t launch_met_prod(const Blk* blks, Space cells, long long ld, const double* mut,
+                            const double* s, const double* dv, double* tprod, cudaStream_t st);
+cudaError_t launch_exgr(const Blk& B, long long ld, double* dv, cudaStream_t st);
+cudaError_t launch_smke(const Blk* blks, Space cells, long long ld, const double* s,
+                        const double* mu, const double* mut, const double* sn,
+                        const double* vol, const double* tprod, const double* dv, double* w,
+                        double* ts6, double* ts7, double* cfke, long long n0, long long n1,
+                        cudaStream_t st);
+cudaError_t launch_kemut(const Blk* blks, Space cells, long long ld, const double* v,
+                         const double* mu, double* mut, cudaStream_t st);
+cudaError_t launch_cutke(const Blk* blks, Space cells, long long ld, double* v, double epsk,
+                         double epse, cudaStream_t st);
+
 // met_bord (kparoi 0) on v(:,6:7); met_rbse + met_rbsc on fd[6][ld];
 // met_cutsa on the real cells
 cudaError_t launch_turb_bord(const Bnd& bd, double* v, long long ld, double rokinf,

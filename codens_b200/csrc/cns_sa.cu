@@ -34,12 +34,14 @@ __device__ __forceinline__ double pow6(double x) {  // gcc's x**6: x3 * x3
 
 // scalar q of cell n: mode 0 = the velocity component q (teq_gradv.f90:
 // t(:,q+1) / max(t(:,1), 1e-20)), mode 1 = the field f, mode 2 = the
-// transport variable q per unit mass (met_gradtr.f90:78-84: s(:,6+q) / s(:,1))
+// transport variable q per unit mass (met_gradtr.f90:78-84: s(:,6+q) / s(:,1)),
+// mode 3 = sqrt(s(:,6) / s(:,1)) (met_bark.f90:91-99)
 __device__ __forceinline__ double scalar_of(int mode, const double* __restrict__ v,
                                             const double* __restrict__ f, long long ld,
                                             long long n, int q) {
   if (mode == 0) return v[(q + 1) * ld + n] / fmax(v[n], 1.e-20);
   if (mode == 2) return v[(5 + q) * ld + n] / v[n];
+  if (mode == 3) return sqrt(v[5 * ld + n] / v[n]);
   return f[q * ld + n];
 }
 

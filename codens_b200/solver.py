@@ -448,8 +448,35 @@ class CodeNS:
                                    int(stilde_fix)))
         self._check(self.lib.cns_set_sa(self.ctx, C.byref(self._sa[1])), "cns_set_sa")
 
+    def set_ke(self, rokinf=None, roeinf=0.0, epsk=1e-10, epse=1e-10):
+        """enable the k-epsilon step of Jones & Launder ('2JL') in the fused
+        iteration (rokinf None disables it); the state must have 7 columns"""
+        if rokinf is None:
+            self._check(self.lib.cns_set_ke(self.ctx, None), "cns_set_ke")
+            return
+        if self.ncol != 7:
+            raise ValueError("the k-epsilon step needs a (ld, 7) state")
+        ke = abi.Ke_t(rokinf, roeinf, epsk, epse)
+        self._check(self.lib.cns_set_ke(self.ctx, C.byref(ke)), "cns_set_ke")
+
     def met_num(self):
         self._check(self.lib.cns_met_num(self.ctx), "cns_met_num")
+
+    def met_prod(self, l, mut, s, dv, tprod, ncyc=1):
+        self._check(self.lib.cns_met_prod(self.ctx, l, ncyc, _ptr(mut), _ptr(s), _ptr(dv),
+                                          _ptr(tprod)), "cns_met_prod")
+
+    def met_smke(self, l, sn, vol, v, mu, mut, tprod, cfke, dv, ts6, ts7):
+        self._check(self.lib.cns_met_smke(self.ctx, l, _ptr(sn), _ptr(vol), _ptr(v), _ptr(mu),
+                                          _ptr(mut), _ptr(tprod), _ptr(cfke), _ptr(dv),
+                                          _ptr(ts6), _ptr(ts7)), "cns_met_smke")
+
+    def met_kemut(self, l, v, mu, mut):
+        self._check(self.lib.cns_met_kemut(self.ctx, l, _ptr(v), _ptr(mu), _ptr(mut)),
+                    "cns_met_kemut")
+
+    def met_cutke(self, l, v, epsk, epse):
+        self._check(self.lib.cns_met_cutke(self.ctx, l, _ptr(v), epsk, epse), "cns_met_cutke")
 
     def lpsa(self, l, v, mu, mut, dist, ztemp):
         """the wall law's rho nu~ and mut of block l's 'lp2' first cells

@@ -327,6 +327,38 @@ int cns_lpsa(cns_ctx *ctx, int l, double *v, const double *mu, double *mut, cons
 int cns_cllparoi1(cns_ctx *ctx, const double *v, const double *dist, const double *mu,
                   const double *mut, double *tau, const double *ztemp);
 int cns_set_sa(cns_ctx *ctx, const cns_sa_t *sa);
+/* The k-epsilon transport step of Jones & Launder (met_num.f90 for equat
+ * '2JL ': kcutke 1, kfludis 1, ksecmb 1, kcmut 1, kparoi 0, kesst 0; cke1
+ * 1.55, cke2 2, cmu 0.09, atlecdon.f90:113-128; met_fludc with the alfak,
+ * alfae of cns_set_turbulence; no wall law), bit-exact in FP64:
+ *   cns_met_prod   met_prod.f90:41-66: tprod = the production of k from the
+ *                  velocity gradients dv (9 x ld, cns_teq_gradv) and mut
+ *   cns_met_smke   met_smke.f90:93-118: met_exgr on dv's ghosts (in place),
+ *                  met_bark (-2 mu |grad sqrt(k)|^2), met_bare (2 mut mu /
+ *                  rho times the squared gradients of dv), met_smkes:
+ *                  qcxts5, qcyts6 = the sources of k and epsilon, cfke the
+ *                  bound of their derivative, on the real cells
+ *   cns_met_kemut  met_kemut.f90:52-65: mut = exp(-2.5 / (1 + Re_t / 50))
+ *                  cmu rho k^2 / eps
+ *   cns_met_cutke  met_cutke.f90:43-60: k < epsk or eps < epse resets both
+ *                  (i = 1..ni: the upper i ghost too)
+ * Arrays are device arrays with the global cell index (dv, tprod, cfke:
+ * 9 ld, ld, ld).  cns_set_ke enables the whole step in the fused iteration
+ * (after rbord, as cns_set_sa does; v, u, d with 7 columns) and disables the
+ * Spalart-Allmaras one; NULL disables it.  cns_met_num runs the enabled
+ * step once on the bound state. */
+typedef struct {
+  double rokinf, roeinf; /* v(:,6), v(:,7) of the injection ghosts */
+  double epsk, epse;     /* met_cutke floors of v(:,6), v(:,7) */
+} cns_ke_t;
+int cns_set_ke(cns_ctx *ctx, const cns_ke_t *ke);
+int cns_met_prod(cns_ctx *ctx, int l, int ncyc, const double *mut, const double *s,
+                 const double *dv, double *tprod);
+int cns_met_smke(cns_ctx *ctx, int l, const double *sn, const double *vol, const double *v,
+                 const double *mu, const double *mut, const double *tprod, double *cfke,
+                 double *dv, double *qcxts5, double *qcyts6);
+int cns_met_kemut(cns_ctx *ctx, int l, const double *v, const double *mu, double *mut);
+int cns_met_cutke(cns_ctx *ctx, int l, double *v, double epsk, double epse);
 int cns_met_num(cns_ctx *ctx);
 
 /* Discrete adjoint of the FP64 Euler Roe iteration (sch_roe_euler with

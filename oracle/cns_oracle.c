@@ -3368,6 +3368,242 @@ void orc_cllparoi1(const double *v, const double *dist, const double *mu, const 
 
 double orc_asin(double x) { return cns_asin(x); }
 
+/* ------------------------------------------------------------------------ */
+/* k-epsilon of Jones & Launder (equat '2JL', atlecdon.f90:113-128: kcutke  */
+/* 1, kfludis 1, ksecmb 1, kcmut 1, kparoi 0, kesst 0; cke1 1.55, cke2 2,    */
+/* cmu 0.09; no wall law)                                                    */
+/* ------------------------------------------------------------------------ */
+
+#define KE_CKE1 1.55
+#define KE_CKE2 2.
+#define KE_CMU 0.09
+
+/* met_prod.f90:41-66: the production of k, -rho u'u' : grad u with the
+ * Boussinesq stresses; dv and tprod [nnn] block-local */
+void orc_met_prod(int l, const double *mut, const double *s, const double *dv, double *tprod) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  const double *dxx = dv, *dxy = dv + nnn, *dxz = dv + 2 * nnn, *dyx = dv + 3 * nnn,
+               *dyy = dv + 4 * nnn, *dyz = dv + 5 * nnn, *dzx = dv + 6 * nnn,
+               *dzy = dv + 7 * nnn, *dzz = dv + 8 * nnn;
+  const double ds3 = 2. / 3.;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        const double torxx = ds3 * (-s[5 * L + n] - mut[n] * (-2 * dxx[m] + dyy[m] + dzz[m]));
+        const double toryy = ds3 * (-s[5 * L + n] - mut[n] * (-2 * dyy[m] + dxx[m] + dzz[m]));
+        const double torzz = ds3 * (-s[5 * L + n] - mut[n] * (-2 * dzz[m] + dyy[m] + dxx[m]));
+        const double torxy = mut[n] * (dxy[m] + dyx[m]);
+        const double torxz = mut[n] * (dxz[m] + dzx[m]);
+        const double toryz = mut[n] * (dzy[m] + dyz[m]);
+        tprod[m] = dxx[m] * torxx + dyy[m] * toryy + dzz[m] * torzz +
+                   torxy * (dxy[m] + dyx[m]) + torxz * (dxz[m] + dzx[m]) +
+                   toryz * (dzy[m] + dyz[m]);
+      }
+}
+
+/* met_exgr.f90:60-100 with ex1 = 1, ex2 = 0: a gradient's ghost values
+ * from the neighbouring cell -- the k ghosts of the real (i, j), then the
+ * i ghosts of every k plane, then the j ghosts of every (i, k) */
+static void met_exgr(const blk_t *b, double *ds) {
+  const int64_t nci = 1, ncj = b->nid, nck = b->nijd, n0 = b->npc;
+  const double ex1 = 1., ex2 = 0.;
+  for (int side = 0; side < 2; ++side) {
+    const int k = side ? b->nk : 0;
+    const int64_t ks = side ? -1 : 1;
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t m = IC(b, i, j, k) - n0;
+        ds[m] = ex1 * ds[m + ks * nck] + ex2 * ds[m + 2 * ks * nck];
+      }
+  }
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int side = 0; side < 2; ++side) {
+        const int i = side ? b->ni : 0;
+        const int64_t is = side ? -1 : 1;
+        const int64_t m = IC(b, i, j, k) - n0;
+        ds[m] = ex1 * ds[m + is * nci] + ex2 * ds[m + 2 * is * nci];
+      }
+  for (int k = 0; k <= b->nk; ++k)
+    for (int side = 0; side < 2; ++side) {
+      const int j = side ? b->nj : 0;
+      const int64_t js = side ? -1 : 1;
+      for (int i = 0; i <= b->ni; ++i) {
+        const int64_t m = IC(b, i, j, k) - n0;
+        ds[m] = ex1 * ds[m + js * ncj] + ex2 * ds[m + 2 * js * ncj];
+      }
+    }
+}
+
+/* met_smke.f90:93-118 for equat '2JL ' (met_exgr on the nine velocity
+ * gradients, met_bark, met_bare, met_smkes): ts6, ts7 (qcxts5, qcyts6)
+ * the k and epsilon sources and cfke the bound of their derivative, on the
+ * real cells (global index); dv [9][nnn] block-local, its ghosts
+ * extrapolated in place */
+void orc_met_smke(int l, const double *sn, const double *vol, const double *v,
+                  const double *mu, const double *mut, const double *tprod, double *dv,
+                  double *ts6, double *ts7, double *cfke) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  for (int c = 0; c < 9; ++c) met_exgr(b, dv + c * nnn);
+  double *t = calloc((size_t)nnn, sizeof(double)), *bark = calloc((size_t)nnn, sizeof(double)),
+         *bare = calloc((size_t)nnn, sizeof(double));
+  double *dx = calloc((size_t)nnn, sizeof(double)), *dy = calloc((size_t)nnn, sizeof(double)),
+         *dz = calloc((size_t)nnn, sizeof(double));
+  /* met_bark.f90:91-126: bark = -2 mu |grad sqrt(k)|^2 (k per unit mass) */
+  for (int k = 0; k <= b->nk; ++k)
+    for (int j = 0; j <= b->nj; ++j)
+      for (int i = 0; i <= b->ni; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        t[n - n0] = sqrt(v[5 * L + n] / v[n]);
+      }
+  teq_grads(b, sn, vol, t, dx, dy, dz);
+  int64_t r0, r1;
+  flat_real_range(b, &r0, &r1);
+  for (int64_t n = r0; n <= r1; ++n) {
+    const int64_t m = n - n0;
+    bark[m] = dx[m] * dx[m] + dy[m] * dy[m] + dz[m] * dz[m];
+    bark[m] = -2. * mu[n] * bark[m];
+  }
+  /* met_bare.f90:64-318: bare = 2 mut mu / rho * sum of the squared
+   * gradients of the nine velocity gradients, in the order xx .. zz */
+  for (int c = 0; c < 9; ++c) {
+    teq_grads(b, sn, vol, dv + c * nnn, dx, dy, dz);
+    for (int k = 1; k <= b->nk - 1; ++k)
+      for (int j = 1; j <= b->nj - 1; ++j)
+        for (int i = 1; i <= b->ni - 1; ++i) {
+          const int64_t m = IC(b, i, j, k) - n0;
+          bare[m] = bare[m] + dx[m] * dx[m] + dy[m] * dy[m] + dz[m] * dz[m];
+        }
+  }
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        bare[m] = 2. * mut[n] * mu[n] * bare[m] / v[n];
+      }
+  /* met_smkes.f90:45-73 (f1 = 1; lparoi = 0) */
+  const double f1 = 1.;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        const double s6 = v[5 * L + n], s7 = v[6 * L + n];
+        const double retur = sq(s6) / (s7 * mu[n]);
+        const double arg = -sq(retur);
+        const double f2 = 1. - 0.3 * cns_exp(arg);
+        const double esk = s7 / s6;
+        const double roe2sk = (s7 * s7) / s6;
+        ts6[n] = tprod[m] - s7 + bark[m];
+        ts7[n] = KE_CKE1 * f1 * tprod[m] * esk - KE_CKE2 * f2 * roe2sk + bare[m];
+        const double c1f1 = KE_CKE1 * f1, c2f2 = KE_CKE2 * f2;
+        const double d = -bark[m];
+        const double x = c1f1 * tprod[m] - c2f2 * s7;
+        const double g = fmax(0., d * (d - 2. * (x - c2f2 * s7)));
+        const double rdelta = sqrt(sq(x - c2f2 * s7) + 4 * x * s7 + g);
+        const double bb = x - c2f2 * s7 - d;
+        const double xl1 = 0.5 * (bb + rdelta) / s6, xl2 = 0.5 * (bb - rdelta) / s6;
+        cfke[n] = fmax(fabs(xl1), fabs(xl2));
+      }
+  free(t); free(bark); free(bare); free(dx); free(dy); free(dz);
+}
+
+/* met_kemut.f90:52-65 ('2JL', kesst = 0, lparoi = 0): mut = f_mu cmu
+ * rho k^2 / eps, f_mu = exp(-2.5 / (1 + Re_t / 50)), Re_t = rho k^2 / (mu eps) */
+void orc_met_kemut(int l, const double *v, const double *mu, double *mut) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        const double retur = sq(v[5 * L + n]) / (v[6 * L + n] * mu[n]);
+        const double mut0 = KE_CMU * retur * mu[n];
+        const double fmu = cns_exp(-2.5 / (1. + retur / 50.));
+        mut[n] = fmu * mut0;
+      }
+}
+
+/* met_cutke.f90:43-60: k below epsk or epsilon below epse resets both, on
+ * i = 1..ni (the upper i ghost included), the real j and k */
+void orc_met_cutke(int l, double *s, double epsk, double epse) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld;
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        if (s[5 * L + n] < epsk) {
+          s[5 * L + n] = epsk;
+          s[6 * L + n] = epse;
+        }
+        if (s[6 * L + n] < epse) {
+          s[5 * L + n] = epsk;
+          s[6 * L + n] = epse;
+        }
+      }
+}
+
+static struct {
+  int on;
+  double rokinf, roeinf, epsk, epse, alfak, alfae;
+  int harten;
+  double epsroe;
+  double *fd, *ts, *cfke; /* 6 ld, 2 ld, ld */
+} KE;
+
+void orc_set_ke(int on, double rokinf, double roeinf, double epsk, double epse, double alfak,
+                double alfae, int harten, double epsroe, double *fd, double *ts, double *cfke) {
+  KE.on = on;
+  KE.rokinf = rokinf;
+  KE.roeinf = roeinf;
+  KE.epsk = epsk;
+  KE.epse = epse;
+  KE.alfak = alfak;
+  KE.alfae = alfae;
+  KE.harten = harten;
+  KE.epsroe = epsroe;
+  KE.fd = fd;
+  KE.ts = ts;
+  KE.cfke = cfke;
+}
+
+/* met_num.f90:145-790 for '2JL ': turbulence ghosts; per block velocity
+ * gradients, production, grad(k/rho) and grad(eps/rho), the sources and
+ * the diffusion densities; their ghosts; per block Roe dissipation,
+ * explicit balance, implicit line Jacobi (cmt = 1, impli2_eqt_3d.f90:85)
+ * and the clip; mut of the model.  v, u, d are (ld, 7). */
+void orc_met_num_ke(double *v, double *u, double *d, const double *dt, const double *mu,
+                    double *mut, const double *sn, const double *vol) {
+  const int64_t L = G.ld;
+  double *fd = KE.fd, *ts6 = KE.ts, *ts7 = KE.ts + L;
+  double *f5x = fd, *f5y = fd + L, *f5z = fd + 2 * L, *f6x = fd + 3 * L, *f6y = fd + 4 * L,
+         *f6z = fd + 5 * L;
+  orc_met_bord(v, KE.rokinf, KE.roeinf);
+  for (int l = 1; l <= G.nblk; ++l) {
+    const blk_t *b = &G.b[l - 1];
+    double *dv = calloc((size_t)(9 * b->nnn), sizeof(double));
+    double *tprod = calloc((size_t)b->nnn, sizeof(double));
+    orc_teq_gradv(l, sn, vol, v, dv);
+    orc_met_prod(l, mut, v, dv, tprod);
+    orc_met_gradtr(l, sn, vol, v, f5x, f5y, f5z, f6x, f6y, f6z);
+    orc_met_smke(l, sn, vol, v, mu, mut, tprod, dv, ts6, ts7, KE.cfke);
+    orc_met_fludc(l, mu, mut, f5x, f5y, f5z, f6x, f6y, f6z, KE.alfak, KE.alfae);
+    free(dv);
+    free(tprod);
+  }
+  orc_met_rbse(f5x, f5y, f5z, f6x, f6y, f6z);
+  for (int l = 1; l <= G.nblk; ++l) {
+    orc_met_roe2o(l, v, d, sn, KE.harten, KE.epsroe);
+    orc_sch_turb(l, u, v, d, f5x, f5y, f5z, f6x, f6y, f6z, ts6, ts7, sn, vol);
+    orc_impli2_eqt_3d(l, u, dt, v, mu, mut, KE.cfke, sn, vol, 1.0);
+    orc_met_cutke(l, v, KE.epsk, KE.epse);
+  }
+  for (int l = 1; l <= G.nblk; ++l) orc_met_kemut(l, v, mu, mut);
+}
+
 /* met_num.f90:145-790 for 1SA, after rbord: turbulence ghosts; per block
  * (in block order, which met_smsa.f90:177's block-local read of txxf5x
  * depends on) velocity gradients, grad(nu~), source, diffusion densities;
@@ -3419,6 +3655,7 @@ int orc_step_jameson(double *v, double *u, double *d, double *dis, double *dt,
   for (int l = 1; l <= G.nblk; ++l) orc_dissip_jameson(l, v, dis, sn, ps, cson);
   orc_rbord(v, ps, temp, cson);
   if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol, temp);
+  if (KE.on) orc_met_num_ke(v, u, d, dt, mu, mut, sn, vol);
   if (G.ns) {
     orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
     /* atsch_num.f90:579-604: the wall law of the 'lp2' walls */
@@ -3449,6 +3686,7 @@ int orc_step(double *v, double *u, double *d, double *dt, const double *sn,
   if (compute_dt && G.kdtl == 0) orc_chrono_global(dt);
   orc_rbord(v, ps, temp, cson);
   if (SA.on) orc_met_num(v, u, d, dt, mu, mut, sn, vol, temp);
+  if (KE.on) orc_met_num_ke(v, u, d, dt, mu, mut, sn, vol);
   if (G.ns) {
     orc_zvisqc(v, mu, mut, tau, sn, vol, temp);
     /* atsch_num.f90:579-604: the wall law of the 'lp2' walls */

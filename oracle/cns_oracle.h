@@ -163,6 +163,20 @@ void orc_set_sa(int on, const double *dist, double rokinf, double roeinf, double
                 double *cfke);
 void orc_met_num(double *v, double *u, double *d, const double *dt, const double *mu,
                  double *mut, const double *sn, const double *vol, const double *temp);
+/* k-epsilon of Jones & Launder ('2JL'): met_prod (dv, tprod block-local
+ * [9][nnn], [nnn]), met_smke (dv's ghosts extrapolated in place; ts6, ts7,
+ * cfke global), met_kemut, met_cutke, the whole met_num; orc_set_ke(on, ...)
+ * makes orc_step run it after rbord (fd 6 ld, ts 2 ld, cfke ld scratch) */
+void orc_met_prod(int l, const double *mut, const double *s, const double *dv, double *tprod);
+void orc_met_smke(int l, const double *sn, const double *vol, const double *v,
+                  const double *mu, const double *mut, const double *tprod, double *dv,
+                  double *ts6, double *ts7, double *cfke);
+void orc_met_kemut(int l, const double *v, const double *mu, double *mut);
+void orc_met_cutke(int l, double *s, double epsk, double epse);
+void orc_set_ke(int on, double rokinf, double roeinf, double epsk, double epse, double alfak,
+                double alfae, int harten, double epsroe, double *fd, double *ts, double *cfke);
+void orc_met_num_ke(double *v, double *u, double *d, const double *dt, const double *mu,
+                    double *mut, const double *sn, const double *vol);
 /* wall law of the 'lp2' walls: lpsa.f90 -> lpsa1.f90 on block l (v is
  * (ld, 7); epsk the floor of rho nu~) and cllparoi1.f90 -> lparoi1.f90 on
  * every 'lp2' wall (tau (ld, 9)) */

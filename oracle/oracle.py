@@ -85,6 +85,13 @@ def lib():
                                  C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                  C.c_void_p]
         L.orc_met_num.argtypes = [_d] * 9
+        L.orc_met_prod.argtypes = [C.c_int] + [_d] * 4
+        L.orc_met_smke.argtypes = [C.c_int] + [_d] * 10
+        L.orc_met_kemut.argtypes = [C.c_int, _d, _d, _d]
+        L.orc_met_cutke.argtypes = [C.c_int, _d, C.c_double, C.c_double]
+        L.orc_set_ke.argtypes = ([C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_double] +
+                                 [C.c_void_p] * 3)
+        L.orc_met_num_ke.argtypes = [_d] * 8
         L.orc_lpsa.argtypes = [C.c_int] + [_d] * 5 + [C.c_double]
         L.orc_cllparoi1.argtypes = [_d] * 6
         L.orc_asin.argtypes = [C.c_double]
@@ -187,6 +194,18 @@ class Oracle:
                          a["fd"].ctypes.data, a["ts"].ctypes.data, a["cfke"].ctypes.data)
         lib().orc_set_sa_fix(int(stilde_fix))
 
+    def set_ke(self, st: OracleState, rokinf: float, roeinf: float, epsk: float = 1e-10,
+               epse: float = 1e-10, epsroe: float = 0.0, alfak: float = 1.0,
+               alfae: float = 1.3):
+        """run the k-epsilon step of Jones & Launder (met_num, '2JL') in every
+        iteration from now on"""
+        ld = self.case.layout.ld
+        self._ke = dict(fd=np.zeros(6 * ld), ts=np.zeros(2 * ld), cfke=np.zeros(ld))
+        harten = int(abs(epsroe) > 1.17549435082228751e-38)
+        a = self._ke
+        lib().orc_set_ke(1, rokinf, roeinf, epsk, epse, alfak, alfae, harten, epsroe,
+                         a["fd"].ctypes.data, a["ts"].ctypes.data, a["cfke"].ctypes.data)
+
     def set_dual(self, st: OracleState, kdualns: int = 0):
         """dual time stepping (kfmg = 3; the scheme's dt1min is the physical
         time step): allocates ptdual, vdual, vdual1, vdual2 on the state and
@@ -207,7 +226,9 @@ class Oracle:
     def clear_sa(self):
         lib().orc_set_sa(0, None, 0.0, 0.0, 0.0, 0, 0.0, 1.0, None, None, None)
         lib().orc_set_sa_fix(0)
+        lib().orc_set_ke(0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0, 0.0, None, None, None)
         self._sa = None
+        self._ke = None
 
     def metric(self, st: OracleState):
         lib().orc_metric(st.x, st.y, st.z, st.sn, st.vol)
