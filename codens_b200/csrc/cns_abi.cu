@@ -54,7 +54,7 @@ struct cns_ctx {
   long long n_lp2_ni = 0;
   double* wall_par = nullptr;        // wall facet centres [3][n_wall_ent]
   double* adj_J = nullptr;   // adjoint: face-flux Jacobians [3][27][5][ld]
-  double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld]
+  double* adj_z = nullptr;   // adjoint: transposed-sweep scratch [2][5][ld] + 1 / cd [ld]
   double* tau_pack = nullptr;  // nine separate stress arrays packed as (ld, 9)
   double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
   int* sched32 = nullptr;      // tile counter pair of the persistent FP32 sweep
@@ -2054,7 +2054,7 @@ int cns_adjoint_prepare(cns_ctx* c) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   if (!c->adj_J) CK(dev_alloc(c, &c->adj_J, (size_t)(3 * 27 * 5) * ld, false));
-  if (!c->adj_z) CK(dev_alloc(c, &c->adj_z, (size_t)(2 * 5) * ld));
+  if (!c->adj_z) CK(dev_alloc(c, &c->adj_z, (size_t)(2 * 5 + 1) * ld));
   const Space all = c->cells.view(-1);
   // the iteration's inputs at the bound (converged) state: thermodynamics,
   // time steps, ghost cells, velocities, implicit coefficients
@@ -2101,11 +2101,11 @@ int cns_adjoint_lt(cns_ctx* c, const double* y, double* out) {
     float* z = reinterpret_cast<float*>(c->adj_z);
     CK(launch_precond_ta<float>(c->d_blks, c->cells.view(-1), ld, s.v, s.pression, c->w.sn32,
                                 c->w.coefe32, c->w.coefdiag32, c->ph.gam1, c->ph.pinfl, lmx, y,
-                                z, z + 5 * ld, out, c->st));
+                                z, z + 5 * ld, z + 10 * ld, out, c->st));
   } else {
     CK(launch_precond_ta<double>(c->d_blks, c->cells.view(-1), ld, s.v, s.pression, s.sn,
                                  c->w.coefe, c->w.coefdiag, c->ph.gam1, c->ph.pinfl, lmx, y,
-                                 c->adj_z, c->adj_z + 5 * ld, out, c->st));
+                                 c->adj_z, c->adj_z + 5 * ld, c->adj_z + 10 * ld, out, c->st));
   }
   return CNS_OK;
 }

@@ -214,16 +214,27 @@ __global__ void __launch_bounds__(kTile) k_adj_gather(const Blk* __restrict__ bl
   for (int c = 0; c < 6; ++c) wbar[c * ld + m] = acc[c];
 }
 
+// 1 / cd of every real cell, once per transposed solve (the sweeps take it
+// seven times a cell each)
+template <class T>
+__global__ void __launch_bounds__(kTile) k_inv_cd(const Blk* __restrict__ blks, Space sp,
+                                                  const T* __restrict__ cd, T* __restrict__ icd) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long c = cell_index(blks[b], i, j, k);
+  icd[c] = T(1.) / cd[c];
+}
+
 template <class T>
 __global__ void __launch_bounds__(kTile) k_scale_cd(const Blk* __restrict__ blks, Space sp,
-                                                    long long ld, const T* __restrict__ cd,
+                                                    long long ld, const T* __restrict__ icd,
                                                     const double* __restrict__ y,
                                                     const T* __restrict__ z,
                                                     double* __restrict__ out) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const long long c = cell_index(blks[b], i, j, k);
-  const T ic = T(1.) / cd[c];
+  const T ic = icd[c];
 #pragma unroll
   for (int a = 0; a < 5; ++a)
     out[a * ld + c] = (double)((z ? z[a * ld + c] : (T)y[a * ld + c]) * ic);
@@ -246,7 +257,7 @@ __global__ void __launch_bounds__(kTile) k_sweep_ta(const Blk* __restrict__ blks
                                                     const double* __restrict__ ps,
                                                     const T* __restrict__ sn,
                                                     const T* __restrict__ coefe,
-                                                    const T* __restrict__ cd,
+                                                    const T* __restrict__ icd,
                                                     const double* __restrict__ y,
                                                     const T* __restrict__ z,
                                                     T* __restrict__ out, T gam1, T pinfl) {
@@ -255,7 +266,7 @@ __global__ void __launch_bounds__(kTile) k_sweep_ta(const Blk* __restrict__ blks
   const Blk& B = blks[b];
   const long long c = cell_index(B, i, j, k);
   auto wof = [&](long long e, T wv[5]) {
-    const T ie = T(1.) / cd[e];
+    const T ie = icd[e];
 #pragma unroll
     for (int a = 0; a < 5; ++a) wv[a] = (z ? z[a * ld + e] : (T)y[a * ld + e]) * ie;
   };
@@ -366,26 +377,27 @@ template <class T>
 cudaError_t launch_precond_ta(const Blk* blks, Space cells, long long ld, const double* v,
                               const double* ps, const T* sn, const T* coefe, const T* cd,
                               double gam1, double pinfl, int lmax, const double* y, T* z0,
-                              T* z1, double* out, cudaStream_t st) {
+                              T* z1, T* icd, double* out, cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
+  k_inv_cd<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, cd, icd);
   const T* cur = nullptr;  // the first sweep's iterate: y
   T* bufs[2] = {z0, z1};
   for (int l = 1; l < lmax; ++l) {
     T* nxt = bufs[l & 1];
-    k_sweep_ta<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, v, ps, sn, coefe, cd, y,
+    k_sweep_ta<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, v, ps, sn, coefe, icd, y,
                                                     cur, nxt, (T)gam1, (T)pinfl);
     cur = nxt;
   }
-  k_scale_cd<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, cd, y, cur, out);
+  k_scale_cd<T><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, icd, y, cur, out);
   return cudaGetLastError();
 }
 template cudaError_t launch_precond_ta<double>(const Blk*, Space, long long, const double*,
                                                const double*, const double*, const double*,
                                                const double*, double, double, int,
                                                const double*, double*, double*, double*,
-                                               cudaStream_t);
+                                               double*, cudaStream_t);
 template cudaError_t launch_precond_ta<float>(const Blk*, Space, long long, const double*,
                                               const double*, const float*, const float*,
                                               const float*, double, double, int, const double*,
-                                              float*, float*, double*, cudaStream_t);
+                                              float*, float*, float*, double*, cudaStream_t);
 }  // namespace cns

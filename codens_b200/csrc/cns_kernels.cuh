@@ -297,13 +297,14 @@ cudaError_t launch_adj_gather(const Blk* blks, Space cells_ext, const double* J,
                               cudaStream_t st);
 // out = L^T y over lmax transposed sweeps of the linearised Euler Jacobi
 // update (implimf_eu with qfix), from the flux Jacobians of each cell's state
-// (z0, z1: scratch [5][ld]); T = float: face areas, coefficients and the
-// sweep iterates in FP32 (the reduced-precision forms)
+// (z0, z1: scratch [5][ld]; icd: scratch [ld] for 1 / cd); T = float: face
+// areas, coefficients and the sweep iterates in FP32 (the reduced-precision
+// forms)
 template <class T>
 cudaError_t launch_precond_ta(const Blk* blks, Space cells, long long ld, const double* v,
                               const double* ps, const T* sn, const T* coefe, const T* cd,
                               double gam1, double pinfl, int lmax, const double* y, T* z0,
-                              T* z1, double* out, cudaStream_t st);
+                              T* z1, T* icd, double* out, cudaStream_t st);
 
 // met_samut (real cells of block l0's space) and sch_turb (u, v, d: (ld, 7))
 cudaError_t launch_samut(const Blk* blks, Space cells, const double* v6, const double* mu,
