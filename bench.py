@@ -95,16 +95,19 @@ def parse():
                    help="TI,TJ,KC: fix the Jacobi sweep tiling instead of autotuning it")
     p.add_argument("--eta", type=float, default=5.0,
                    help="CFL number of the local time step (AUSM+ needs 2 on the channel)")
-    p.add_argument("--flux", default="roe", choices=["roe", "hllc", "rusanov", "ausm"],
-                   help="flux family of the channel workload (ischema 7, 14, 9, 5)")
+    p.add_argument("--flux", default="roe", choices=["roe", "hllc", "rusanov", "ausm", "weno5"],
+                   help="flux family of the channel workload (ischema 7, 14, 9, 5, 12; "
+                        "WENO5 with its flagged three-candidate fix, the reference form "
+                        "reaching no steady state)")
     p.add_argument("--ilim", type=int, default=0,
                    help="0: plain kappa=-1 MUSCL (default: the reference's limiter "
                         "recurrence stalls this channel at L2 ~1e-3); 1: minmod limiter")
     return p.parse_args()
 
 
-FLUX = {"roe": 7, "hllc": 14, "rusanov": 9, "ausm": 5}
-FLUX_NAME = {"roe": "Roe", "hllc": "HLLC", "rusanov": "Rusanov", "ausm": "AUSM+"}
+FLUX = {"roe": 7, "hllc": 14, "rusanov": 9, "ausm": 5, "weno5": 12}
+FLUX_NAME = {"roe": "Roe", "hllc": "HLLC", "rusanov": "Rusanov", "ausm": "AUSM+",
+             "weno5": "WENO5 (three-candidate fix)"}
 
 
 def make_case(args):
@@ -116,6 +119,7 @@ def make_case(args):
     case.scheme.lmax = args.lmax
     case.scheme.ilim = args.ilim
     case.scheme.ischema = FLUX[args.flux]
+    case.scheme.weno_fix = int(args.flux == "weno5")
     case.scheme.eta = args.eta
     case.scheme.precision = PRECISION[args.precision]
     case.scheme.kdefect = args.kdefect
@@ -125,7 +129,8 @@ def make_case(args):
 def config_of(case, args, n):
     m = case.meta
     return {
-        "workload": f"laminar NS bump channel, 8 uneven blocks, {FLUX_NAME[args.flux]}-MUSCL"
+        "workload": f"laminar NS bump channel, 8 uneven blocks, {FLUX_NAME[args.flux]}"
+                    f"{'' if args.flux == 'weno5' else '-MUSCL'}"
                     f"{' minmod' if args.ilim else ''} + viscous, "
                     f"implicit point-Jacobi lmax={args.lmax}, {args.precision}"
         if not args.small else "laminar NS bump channel, 3 blocks of 64x64x96 cells",
@@ -298,6 +303,8 @@ def _residual_ms(s, torch, reps=5):
     for _ in range(reps):
         if ischema == 9:
             s.sch_rusanov(0, s.u, s.v, s.tau, s.sn, s.pression)
+        elif ischema == 12:
+            s.sch_weno5_3d(0, s.u, s.v, s.tau, s.sn, s.pression)
         elif ischema == 5:
             s.sch_ausmp(0, s.u, s.v, s.tau, s.sn, s.pression)
         elif ischema == 14 and s.case.scheme.ns:

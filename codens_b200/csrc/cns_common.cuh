@@ -106,10 +106,11 @@ enum BcKind { BC_EXTR = 1, BC_RC = 2, BC_PARA = 3, BC_IDD = 4, BC_PRD = 5, BC_LP
 
 __device__ __forceinline__ double sq(double a) { return a * a; }
 
-// element of the tile handled by this thread; false when past the block end
-__device__ __forceinline__ bool space_elem(const Space& sp, int lane, int& b,
-                                           int& i, int& j, int& k) {
-  const int t = sp.tile0 + blockIdx.x;
+// element lane of tile t (counted from the launch's first tile); false
+// when past the block end
+__device__ __forceinline__ bool space_elem_at(const Space& sp, int tile, int lane, int& b,
+                                              int& i, int& j, int& k) {
+  const int t = sp.tile0 + tile;
   b = sp.tile_blk[t];
   const long long e = sp.tile_start[t] + lane;
   const int ex = sp.ext[3 * b], ey = sp.ext[3 * b + 1], ez = sp.ext[3 * b + 2];
@@ -123,6 +124,13 @@ __device__ __forceinline__ bool space_elem(const Space& sp, int lane, int& b,
   j += 1;
   k += 1;
   return true;
+}
+
+// element of the tile handled by this thread (a CTA per tile); false when
+// past the block end
+__device__ __forceinline__ bool space_elem(const Space& sp, int lane, int& b, int& i, int& j,
+                                           int& k) {
+  return space_elem_at(sp, blockIdx.x, lane, b, i, j, k);
 }
 
 __device__ __forceinline__ long long cell_index(const Blk& B, int i, int j, int k) {

@@ -304,13 +304,17 @@ __global__ void __launch_bounds__(kTile) k_i2_rhs(
 // covers an HBM round trip).  Few threads run it, so it may use up to 255
 // registers a thread for the two chunks in flight.
 constexpr int kLineUnroll = 8;
+// CTAs of kLineCta threads, kTile / kLineCta per tile of lines: a direction
+// has only as many threads as lines (8192 i-lines on a 256x128x64 block),
+// so small CTAs spread them over every SM instead of a third of them
+constexpr int kLineCta = 32;
 
 // RCP: the reduced-precision forms' variant, one division per step (the
 // reciprocal of the pivot times each numerator).  The sweep only shapes the
 // pseudo-time increment, so the fixed point is unchanged; the dependent
 // chain per step shrinks from three divisions to one.
 template <bool RCP>
-__global__ void __launch_bounds__(kTile, 1) k_i2_line(const Blk* __restrict__ blks, Space sp,
+__global__ void __launch_bounds__(kLineCta, 1) k_i2_line(const Blk* __restrict__ blks, Space sp,
                                                       int dir, const double* __restrict__ ta,
                                                       const double* __restrict__ tb,
                                                       const double* __restrict__ tc,
@@ -322,7 +326,10 @@ __global__ void __launch_bounds__(kTile, 1) k_i2_line(const Blk* __restrict__ bl
                                                       double* __restrict__ n6,
                                                       double* __restrict__ n7) {
   int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  constexpr int kSub = kTile / kLineCta;
+  if (!space_elem_at(sp, blockIdx.x / kSub, (blockIdx.x % kSub) * kLineCta + threadIdx.x, b, i,
+                     j, k))
+    return;
   const Blk& B = blks[b];
   const long long inc = ninc_of(B, dir);
   const int nc = nd_of(B, dir) - 1;             // cells on the line
@@ -822,12 +829,13 @@ cudaError_t launch_impli2(const Blk* blks, const SpaceBuf* faces, const SpaceBuf
     for (int sw = 0; sw < 2; ++sw) {
       k_i2_rhs<<<grid_of(cells), kTile, 0, st>>>(blks, cells, dir, ld, u, uf, ce, cd,
                                                  it[cur][0], it[cur][1], ta, tb, tc, d6, d7);
+      const int lg = grid_of(sp) * (kTile / kLineCta);
       if (sp.ntiles > 0 && rcp)
-        k_i2_line<true><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al, b6,
-                                                       b7, it[1 - cur][0], it[1 - cur][1]);
+        k_i2_line<true><<<lg, kLineCta, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al, b6, b7,
+                                                 it[1 - cur][0], it[1 - cur][1]);
       else if (sp.ntiles > 0)
-        k_i2_line<false><<<grid_of(sp), kTile, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al,
-                                                        b6, b7, it[1 - cur][0], it[1 - cur][1]);
+        k_i2_line<false><<<lg, kLineCta, 0, st>>>(blks, sp, dir, ta, tb, tc, d6, d7, al, b6,
+                                                  b7, it[1 - cur][0], it[1 - cur][1]);
       cur = 1 - cur;
     }
   }
