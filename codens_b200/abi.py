@@ -80,7 +80,8 @@ EXPORTS = [
     "cns_met_samut", "cns_sch_turb", "cns_teq_gradv", "cns_met_smsa", "cns_impli2_eqt_3d",
     "cns_atcaldis3", "cns_met_bord", "cns_met_gradtr", "cns_met_rbse", "cns_met_cutsa",
     "cns_set_sa", "cns_met_num", "cns_lpsa", "cns_cllparoi1", "cns_set_ke", "cns_met_prod",
-    "cns_met_smke", "cns_met_kemut", "cns_met_cutke",
+    "cns_met_smke", "cns_met_kemut", "cns_met_cutke", "cns_met_inisa", "cns_met_inmut",
+    "cns_met_ini",
     "cns_set_subrecord_length", "cns_readdg", "cns_writdg", "cns_readda", "cns_writda",
     "cns_set_cycle", "cns_sch_duin", "cns_sch_duup", "cns_set_dual_cycle", "cns_sch_dual",
     "cns_sch_hllc_euler", "cns_sch_hllc", "cns_sch_rusanov", "cns_sch_ausmp",
@@ -167,6 +168,9 @@ def load(build_if_missing: bool = True):
     L.cns_met_smke.argtypes = [vp, C.c_int] + [vp] * 10
     L.cns_met_kemut.argtypes = [vp, C.c_int] + [vp] * 3
     L.cns_met_cutke.argtypes = [vp, C.c_int, vp, c_f64, c_f64]
+    L.cns_met_inisa.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.cns_met_inmut.argtypes = [vp, C.c_int, vp, vp]
+    L.cns_met_ini.argtypes = [vp, C.c_int] + [vp] * 6
     L.cns_cllparoi1.argtypes = [vp] * 7
     L.cns_set_sweep_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cns_set_residual_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int]

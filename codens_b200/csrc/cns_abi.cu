@@ -2032,6 +2032,36 @@ int cns_met_cutke(cns_ctx* c, int l, double* v, double epsk, double epse) {
   return CNS_OK;
 }
 
+int cns_met_inisa(cns_ctx* c, int l, double* v, const double* mut, const double* mu) {
+  (void)mu;  // in met_inisa.f90:4's argument list, not read
+  if (!c || bad_block(c, l) || !v || !mut) return CNS_EINVAL;
+  CK(launch_turb_init(c->d_blks, c->cells.view(l - 1), 0, c->lay.ld, v, const_cast<double*>(mut),
+                      nullptr, nullptr, c->st));
+  return CNS_OK;
+}
+
+int cns_met_inmut(cns_ctx* c, int l, const double* mu, double* mut) {
+  if (!c || bad_block(c, l) || !mu || !mut) return CNS_EINVAL;
+  CK(launch_turb_init(c->d_blks, c->cells.view(l - 1), 1, c->lay.ld, nullptr, mut, mu, nullptr,
+                      c->st));
+  return CNS_OK;
+}
+
+int cns_met_ini(cns_ctx* c, int l, double* v, const double* mut, const double* mu,
+                const double* sn, const double* vol, double* dv) {
+  (void)mu;  // in met_ini.f90:4-8's argument list, not read
+  if (!c || bad_block(c, l) || !v || !mut || !sn || !vol || !dv) return CNS_EINVAL;
+  CK(ensure_sa(c));
+  long long n0, n1;
+  block_range(c, l, n0, n1);
+  const Space cb = c->cells.view(l - 1);
+  CK(launch_teq_grads(c->d_blks, cb, 0, 3, v, nullptr, c->lay.ld, sn, vol, dv, c->sa_sc, n0, n1,
+                      c->st));
+  CK(launch_turb_init(c->d_blks, cb, 2, c->lay.ld, v, const_cast<double*>(mut), nullptr, dv,
+                      c->st));
+  return CNS_OK;
+}
+
 int cns_met_num(cns_ctx* c) {
   if (!c) return CNS_EINVAL;
   if (!c->bound || !(c->sa_on || c->ke_on))

@@ -189,9 +189,43 @@ __global__ void __launch_bounds__(kTile) k_cutke(const Blk* __restrict__ blks, S
   if (i == B.ni - 1) cutke_cell(v, ld, n + 1, epsk, epse);
 }
 
+// the turbulence initialisation of the first cycle (atsch_num.f90:256-345)
+// on the real cells: mode 0 met_inisa.f90:36-44 (rho nu~ = mut), mode 1
+// met_inmut.f90 (mut = mu / 10), mode 2 met_brad.f90:37-51 (Bradshaw:
+// rho k = mut |omega| / sqrt(cmu), rho eps = mut |omega|^2; dv the velocity
+// gradients, global index)
+__global__ void __launch_bounds__(kTile) k_turb_init(const Blk* __restrict__ blks, Space sp,
+                                                     int mode, long long ld, double* v,
+                                                     double* mut, const double* __restrict__ mu,
+                                                     const double* __restrict__ dv) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const long long n = cell_index(blks[b], i, j, k);
+  if (mode == 0) {
+    v[5 * ld + n] = mut[n];
+  } else if (mode == 1) {
+    mut[n] = mu[n] * 1.e-1;
+  } else {
+    const double cmu1 = 1. / sqrt(kCmu);
+    const double a1 = dv[7 * ld + n] - dv[5 * ld + n];  // dvzy - dvyz
+    const double a2 = dv[2 * ld + n] - dv[6 * ld + n];  // dvxz - dvzx
+    const double a3 = dv[3 * ld + n] - dv[ld + n];      // dvyx - dvxy
+    const double omeg = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+    v[5 * ld + n] = cmu1 * mut[n] * omeg;
+    v[6 * ld + n] = mut[n] * omeg * omeg;
+  }
+}
+
 inline int grid_of(const Space& s) { return s.ntiles; }
 
 }  // namespace
+
+cudaError_t launch_turb_init(const Blk* blks, Space cells, int mode, long long ld, double* v,
+                             double* mut, const double* mu, const double* dv, cudaStream_t st) {
+  if (cells.ntiles > 0)
+    k_turb_init<<<grid_of(cells), kTile, 0, st>>>(blks, cells, mode, ld, v, mut, mu, dv);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_met_prod(const Blk* blks, Space cells, long long ld, const double* mut,
                             const double* s, const double* dv, double* tprod, cudaStream_t st) {

@@ -378,6 +378,11 @@ cudaError_t launch_kemut(const Blk* blks, Space cells, long long ld, const doubl
                          const double* mu, double* mut, cudaStream_t st);
 cudaError_t launch_cutke(const Blk* blks, Space cells, long long ld, double* v, double epsk,
                          double epse, cudaStream_t st);
+// first-cycle turbulence initialisation on the real cells: mode 0 met_inisa
+// (v6 = mut), 1 met_inmut (mut = mu / 10), 2 met_brad (v6, v7 from mut and
+// the vorticity of dv [9][ld])
+cudaError_t launch_turb_init(const Blk* blks, Space cells, int mode, long long ld, double* v,
+                             double* mut, const double* mu, const double* dv, cudaStream_t st);
 
 // met_bord (kparoi 0) on v(:,6:7); met_rbse + met_rbsc on fd[6][ld];
 // met_cutsa on the real cells

@@ -478,6 +478,17 @@ class CodeNS:
     def met_cutke(self, l, v, epsk, epse):
         self._check(self.lib.cns_met_cutke(self.ctx, l, _ptr(v), epsk, epse), "cns_met_cutke")
 
+    def met_inisa(self, l, v, mut, mu):
+        self._check(self.lib.cns_met_inisa(self.ctx, l, _ptr(v), _ptr(mut), _ptr(mu)),
+                    "cns_met_inisa")
+
+    def met_inmut(self, l, mu, mut):
+        self._check(self.lib.cns_met_inmut(self.ctx, l, _ptr(mu), _ptr(mut)), "cns_met_inmut")
+
+    def met_ini(self, l, v, mut, mu, sn, vol, dv):
+        self._check(self.lib.cns_met_ini(self.ctx, l, _ptr(v), _ptr(mut), _ptr(mu), _ptr(sn),
+                                         _ptr(vol), _ptr(dv)), "cns_met_ini")
+
     def lpsa(self, l, v, mu, mut, dist, ztemp):
         """the wall law's rho nu~ and mut of block l's 'lp2' first cells
         (lpsa.f90; the floor is set_sa's epsk)"""

@@ -359,6 +359,17 @@ int cns_met_smke(cns_ctx *ctx, int l, const double *sn, const double *vol, const
                  double *dv, double *qcxts5, double *qcyts6);
 int cns_met_kemut(cns_ctx *ctx, int l, const double *v, const double *mu, double *mut);
 int cns_met_cutke(cns_ctx *ctx, int l, double *v, double epsk, double epse);
+/* The first cycle's turbulence initialisation (atsch_num.f90:256-345), on
+ * the real cells of block l (device arrays):
+ *   cns_met_inisa  met_inisa.f90:36-44: v(:,6) = mut (Spalart-Allmaras)
+ *   cns_met_inmut  met_inmut.f90: mut = mu / 10 (keinit = 2)
+ *   cns_met_ini    met_ini.f90 (k-epsilon, kinke = 1): teq_gradv into dv
+ *                  (9 x ld), then met_brad.f90:37-51: v(:,6) = mut |omega| /
+ *                  sqrt(cmu), v(:,7) = mut |omega|^2 */
+int cns_met_inisa(cns_ctx *ctx, int l, double *v, const double *mut, const double *mu);
+int cns_met_inmut(cns_ctx *ctx, int l, const double *mu, double *mut);
+int cns_met_ini(cns_ctx *ctx, int l, double *v, const double *mut, const double *mu,
+                const double *sn, const double *vol, double *dv);
 int cns_met_num(cns_ctx *ctx);
 
 /* Discrete adjoint of the FP64 Euler Roe iteration (sch_roe_euler with

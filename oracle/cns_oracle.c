@@ -3546,6 +3546,48 @@ void orc_met_cutke(int l, double *s, double epsk, double epse) {
       }
 }
 
+/* the first cycle's turbulence initialisation (atsch_num.f90:256-345) on
+ * the real cells: met_inisa.f90:36-44 (v6 = mut), met_inmut.f90 (mut =
+ * mu / 10), met_ini.f90 = teq_gradv + met_brad.f90:37-51 (v6 = mut |omega| /
+ * sqrt(cmu), v7 = mut |omega|^2; dv [9][nnn] block-local) */
+void orc_met_inisa(int l, double *v, const double *mut) {
+  const blk_t *b = &G.b[l - 1];
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        v[5 * G.ld + n] = mut[n];
+      }
+}
+
+void orc_met_inmut(int l, const double *mu, double *mut) {
+  const blk_t *b = &G.b[l - 1];
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k);
+        mut[n] = mu[n] * 1.e-1;
+      }
+}
+
+void orc_met_ini(int l, double *v, const double *mut, const double *sn, const double *vol,
+                 double *dv) {
+  const blk_t *b = &G.b[l - 1];
+  const int64_t L = G.ld, n0 = b->npc, nnn = b->nnn;
+  orc_teq_gradv(l, sn, vol, v, dv);
+  const double cmu1 = 1. / sqrt(KE_CMU);
+  for (int k = 1; k <= b->nk - 1; ++k)
+    for (int j = 1; j <= b->nj - 1; ++j)
+      for (int i = 1; i <= b->ni - 1; ++i) {
+        const int64_t n = IC(b, i, j, k), m = n - n0;
+        const double omeg = sqrt(sq(dv[7 * nnn + m] - dv[5 * nnn + m]) +
+                                 sq(dv[2 * nnn + m] - dv[6 * nnn + m]) +
+                                 sq(dv[3 * nnn + m] - dv[nnn + m]));
+        v[5 * L + n] = cmu1 * mut[n] * omeg;
+        v[6 * L + n] = mut[n] * omeg * omeg;
+      }
+}
+
 static struct {
   int on;
   double rokinf, roeinf, epsk, epse, alfak, alfae;

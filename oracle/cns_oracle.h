@@ -177,6 +177,12 @@ void orc_set_ke(int on, double rokinf, double roeinf, double epsk, double epse, 
                 double alfae, int harten, double epsroe, double *fd, double *ts, double *cfke);
 void orc_met_num_ke(double *v, double *u, double *d, const double *dt, const double *mu,
                     double *mut, const double *sn, const double *vol);
+/* first-cycle initialisation: met_inisa, met_inmut, met_ini (teq_gradv +
+ * met_brad; dv [9][nnn] block-local) */
+void orc_met_inisa(int l, double *v, const double *mut);
+void orc_met_inmut(int l, const double *mu, double *mut);
+void orc_met_ini(int l, double *v, const double *mut, const double *sn, const double *vol,
+                 double *dv);
 /* wall law of the 'lp2' walls: lpsa.f90 -> lpsa1.f90 on block l (v is
  * (ld, 7); epsk the floor of rho nu~) and cllparoi1.f90 -> lparoi1.f90 on
  * every 'lp2' wall (tau (ld, 9)) */

@@ -92,6 +92,9 @@ def lib():
         L.orc_set_ke.argtypes = ([C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_double] +
                                  [C.c_void_p] * 3)
         L.orc_met_num_ke.argtypes = [_d] * 8
+        L.orc_met_inisa.argtypes = [C.c_int, _d, _d]
+        L.orc_met_inmut.argtypes = [C.c_int, _d, _d]
+        L.orc_met_ini.argtypes = [C.c_int] + [_d] * 5
         L.orc_lpsa.argtypes = [C.c_int] + [_d] * 5 + [C.c_double]
         L.orc_cllparoi1.argtypes = [_d] * 6
         L.orc_asin.argtypes = [C.c_double]

@@ -130,6 +130,35 @@ def test_met_prod_smke_kemut_cutke_parity(cuda, name):
     s.close()
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_turbulence_initialisation_parity(cuda, name):
+    """met_inmut, met_inisa and met_ini (teq_gradv + met_brad) of every block"""
+    torch = cuda
+    case = CASES[name]()
+    orc, st = _prepared(case)
+    s = _gpu(case)
+    L = orc_lib()
+    ld = case.layout.ld
+    g = {k: _t(torch, a) for k, a in (("v", st.v), ("mu", st.mu), ("mut", st.mut))}
+    dv_g = torch.zeros(9 * ld, dtype=torch.float64, device="cuda")
+    v_o, mut_o = st.v.copy(), st.mut.copy()
+    for l in range(1, case.layout.nblk + 1):
+        b = case.layout.blocks[l - 1]
+        L.orc_met_inmut(l, st.mu, mut_o)
+        s.met_inmut(l, g["mu"], g["mut"])
+        L.orc_met_ini(l, v_o, mut_o, st.sn, st.vol, np.zeros(9 * b.nnn))
+        s.met_ini(l, g["v"], g["mut"], g["mu"], s.sn, s.vol, dv_g)
+    s.sync()
+    assert_equal_bits(g["mut"].cpu().numpy(), mut_o, "mut = mu / 10")
+    assert_equal_bits(g["v"].cpu().numpy(), v_o, "v after met_ini")
+    for l in range(1, case.layout.nblk + 1):
+        L.orc_met_inisa(l, v_o, mut_o)
+        s.met_inisa(l, g["v"], g["mut"], g["mu"])
+    s.sync()
+    assert_equal_bits(g["v"].cpu().numpy(), v_o, "v after met_inisa")
+    s.close()
+
+
 def _ke_pair(case):
     orc, st = oracle_prepared(case)
     orc.set_ke(st, case.meta["rokinf"], case.meta["roeinf"])
