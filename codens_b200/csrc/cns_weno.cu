@@ -99,6 +99,98 @@ __device__ __forceinline__ double weno_field(const double q[6], double lam, int 
   return nterm == 3 ? x1 * f1 + x2 * f2 + x3 * f3 : x1 * f1 + x2 * f2;
 }
 
+// the Roe-averaged state of a face and the derived scalars its left (Q) and
+// right (P) eigenvector matrices are built from (sch_weno5_3d.f90:240-332)
+struct RoeState {
+  double nx, ny, nz, um, vm, wm, hm, vitm2, am, am2i, vn, rhom, rhomi, rhoiam, rhoami, gam1;
+};
+
+// row kf of Q (sch_weno5_3d.f90:282-306)
+__device__ __forceinline__ void q_row(const RoeState& R, int kf, double q[5]) {
+  const double nx = R.nx, ny = R.ny, nz = R.nz, um = R.um, vm = R.vm, wm = R.wm;
+  const double gam1 = R.gam1, vitm2 = R.vitm2, am2i = R.am2i, rhomi = R.rhomi,
+               rhoami = R.rhoami, vn = R.vn;
+  switch (kf) {
+    case 0:
+      q[0] = (1. - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi;
+      q[1] = gam1 * um * nx * am2i;
+      q[2] = gam1 * vm * nx * am2i + nz * rhomi;
+      q[3] = gam1 * wm * nx * am2i - ny * rhomi;
+      q[4] = -gam1 * nx * am2i;
+      break;
+    case 1:
+      q[0] = (1. - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi;
+      q[1] = gam1 * um * ny * am2i - nz * rhomi;
+      q[2] = gam1 * vm * ny * am2i;
+      q[3] = gam1 * wm * ny * am2i + nx * rhomi;
+      q[4] = -gam1 * ny * am2i;
+      break;
+    case 2:
+      q[0] = (1. - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi;
+      q[1] = gam1 * um * nz * am2i + ny * rhomi;
+      q[2] = gam1 * vm * nz * am2i - nx * rhomi;
+      q[3] = gam1 * wm * nz * am2i;
+      q[4] = -gam1 * nz * am2i;
+      break;
+    case 3:
+      q[0] = gam1 * vitm2 * rhoami - vn * rhomi;
+      q[1] = nx * rhomi - gam1 * um * rhoami;
+      q[2] = ny * rhomi - gam1 * vm * rhoami;
+      q[3] = nz * rhomi - gam1 * wm * rhoami;
+      q[4] = gam1 * rhoami;
+      break;
+    default:
+      q[0] = gam1 * vitm2 * rhoami + vn * rhomi;
+      q[1] = -nx * rhomi - gam1 * um * rhoami;
+      q[2] = -ny * rhomi - gam1 * vm * rhoami;
+      q[3] = -nz * rhomi - gam1 * wm * rhoami;
+      q[4] = gam1 * rhoami;
+  }
+}
+
+// column kf of P (sch_weno5_3d.f90:308-332)
+__device__ __forceinline__ void p_col(const RoeState& R, int kf, double p[5]) {
+  const double nx = R.nx, ny = R.ny, nz = R.nz, um = R.um, vm = R.vm, wm = R.wm;
+  const double rhom = R.rhom, rhoiam = R.rhoiam, am = R.am, hm = R.hm, vitm2 = R.vitm2,
+               vn = R.vn;
+  switch (kf) {
+    case 0:
+      p[0] = nx;
+      p[1] = um * nx;
+      p[2] = vm * nx + rhom * nz;
+      p[3] = wm * nx - rhom * ny;
+      p[4] = vitm2 * nx + rhom * (vm * nz - wm * ny);
+      break;
+    case 1:
+      p[0] = ny;
+      p[1] = um * ny - rhom * nz;
+      p[2] = vm * ny;
+      p[3] = wm * ny + rhom * nx;
+      p[4] = vitm2 * ny + rhom * (wm * nx - um * nz);
+      break;
+    case 2:
+      p[0] = nz;
+      p[1] = um * nz + rhom * ny;
+      p[2] = vm * nz - rhom * nx;
+      p[3] = wm * nz;
+      p[4] = vitm2 * nz + rhom * (um * ny - vm * nx);
+      break;
+    case 3:
+      p[0] = 0.5 * rhoiam;
+      p[1] = 0.5 * rhoiam * (um + nx * am);
+      p[2] = 0.5 * rhoiam * (vm + ny * am);
+      p[3] = 0.5 * rhoiam * (wm + nz * am);
+      p[4] = 0.5 * rhoiam * (hm + am * vn);
+      break;
+    default:
+      p[0] = 0.5 * rhoiam;
+      p[1] = 0.5 * rhoiam * (um - nx * am);
+      p[2] = 0.5 * rhoiam * (vm - ny * am);
+      p[3] = 0.5 * rhoiam * (wm - nz * am);
+      p[4] = 0.5 * rhoiam * (hm - am * vn);
+  }
+}
+
 // interior faces of direction DIR: the thread of real cell (i, j, k) with
 // index p <= nd - 2 along DIR computes the face to its upper neighbour
 // (sch_weno5_3d.f90:240-1252) into G[DIR][5][ld] and half the viscous flux
@@ -139,32 +231,8 @@ __global__ void __launch_bounds__(kTile) k_weno_face(const Blk* __restrict__ blk
   const double am2i = 1. / (am * am);
   const double vn = um * nx + vm * ny + wm * nz;
   const double rhoiam = rhom / am, rhoami = am2i / rhoiam;
-  const double lam[5] = {vn, vn, vn, vn + am, vn - am};
-  const double Q[5][5] = {
-      {(1. - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi, gam1 * um * nx * am2i,
-       gam1 * vm * nx * am2i + nz * rhomi, gam1 * wm * nx * am2i - ny * rhomi,
-       -gam1 * nx * am2i},
-      {(1. - gam1 * vitm2 * am2i) * ny - (wm * nx - um * nz) * rhomi,
-       gam1 * um * ny * am2i - nz * rhomi, gam1 * vm * ny * am2i,
-       gam1 * wm * ny * am2i + nx * rhomi, -gam1 * ny * am2i},
-      {(1. - gam1 * vitm2 * am2i) * nz - (um * ny - vm * nx) * rhomi,
-       gam1 * um * nz * am2i + ny * rhomi, gam1 * vm * nz * am2i - nx * rhomi,
-       gam1 * wm * nz * am2i, -gam1 * nz * am2i},
-      {gam1 * vitm2 * rhoami - vn * rhomi, nx * rhomi - gam1 * um * rhoami,
-       ny * rhomi - gam1 * vm * rhoami, nz * rhomi - gam1 * wm * rhoami, gam1 * rhoami},
-      {gam1 * vitm2 * rhoami + vn * rhomi, -nx * rhomi - gam1 * um * rhoami,
-       -ny * rhomi - gam1 * vm * rhoami, -nz * rhomi - gam1 * wm * rhoami, gam1 * rhoami}};
-  const double P[5][5] = {
-      {nx, ny, nz, 0.5 * rhoiam, 0.5 * rhoiam},
-      {um * nx, um * ny - rhom * nz, um * nz + rhom * ny, 0.5 * rhoiam * (um + nx * am),
-       0.5 * rhoiam * (um - nx * am)},
-      {vm * nx + rhom * nz, vm * ny, vm * nz - rhom * nx, 0.5 * rhoiam * (vm + ny * am),
-       0.5 * rhoiam * (vm - ny * am)},
-      {wm * nx - rhom * ny, wm * ny + rhom * nx, wm * nz, 0.5 * rhoiam * (wm + nz * am),
-       0.5 * rhoiam * (wm - nz * am)},
-      {vitm2 * nx + rhom * (vm * nz - wm * ny), vitm2 * ny + rhom * (wm * nx - um * nz),
-       vitm2 * nz + rhom * (um * ny - vm * nx), 0.5 * rhoiam * (hm + am * vn),
-       0.5 * rhoiam * (hm - am * vn)}};
+  const RoeState R{nx, ny, nz, um, vm, wm, hm, vitm2, am, am2i, vn, rhom, rhomi, rhoiam, rhoami,
+                   gam1};
   // the six stencil points n + s ninc (s = -2..3); k = -1 (below the
   // block) is taken at the ghost plane k = 0
   long long pt[6];
@@ -181,23 +249,27 @@ __global__ void __launch_bounds__(kTile) k_weno_face(const Blk* __restrict__ blk
     double fl[6][5];
 #pragma unroll
     for (int s = 0; s < 6; ++s) weno_cell_flux(v, ps, ld, pt[s], c, ph.pinfl, fl[s]);
-    double fc[5];
-#pragma unroll
+    // field by field: its row of Q, its reconstructed flux, and its share
+    // of P times the fluxes (summed over the fields in order, as the
+    // reference's fc1*p11 + fc2*p12 + ... rounds)
+    double oc[5];
+#pragma unroll 1
     for (int kf = 0; kf < 5; ++kf) {
+      double qr[5], pc[5];
+      q_row(R, kf, qr);
+      p_col(R, kf, pc);
       double q[6];
 #pragma unroll
       for (int s = 0; s < 6; ++s)
-        q[s] = Q[kf][0] * fl[s][0] + Q[kf][1] * fl[s][1] + Q[kf][2] * fl[s][2] +
-               Q[kf][3] * fl[s][3] + Q[kf][4] * fl[s][4];
-      fc[kf] = weno_field(q, lam[kf], nterm);
+        q[s] = qr[0] * fl[s][0] + qr[1] * fl[s][1] + qr[2] * fl[s][2] + qr[3] * fl[s][3] +
+               qr[4] * fl[s][4];
+      const double fck = weno_field(q, kf < 3 ? vn : (kf == 3 ? vn + am : vn - am), nterm);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) oc[r] = kf == 0 ? fck * pc[r] : oc[r] + fck * pc[r];
     }
     const double sc = c == 0 ? s1 : (c == 1 ? s2 : s3);
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const double o = fc[0] * P[r][0] + fc[1] * P[r][1] + fc[2] * P[r][2] + fc[3] * P[r][3] +
-                       fc[4] * P[r][4];
-      df[r] = c == 0 ? o * sc : df[r] + o * sc;
-    }
+    for (int r = 0; r < 5; ++r) df[r] = c == 0 ? oc[r] * sc : df[r] + oc[r] * sc;
   }
 #pragma unroll
   for (int r = 0; r < 5; ++r) G[(DIR * 5 + r) * ld + n] = df[r];
