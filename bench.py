@@ -93,6 +93,8 @@ def parse():
                    help="sweep-tiling cache file: a tiling found there is used without timing")
     p.add_argument("--tiles", default=None,
                    help="TI,TJ,KC: fix the Jacobi sweep tiling instead of autotuning it")
+    p.add_argument("--sweep-staging", type=int, default=0, choices=[0, 1],
+                   help="FP32 sweep plane staging: 0 tensor boxes (TMA), 1 cp.async copies")
     p.add_argument("--eta", type=float, default=5.0,
                    help="CFL number of the local time step (AUSM+ needs 2 on the channel)")
     p.add_argument("--flux", default="roe", choices=["roe", "hllc", "rusanov", "ausm", "weno5"],
@@ -143,6 +145,7 @@ def config_of(case, args, n):
         "residual": (f"fused kernel, tiles {args.residual_tiles}" if args.residual_tiles
                      else "face kernels + accumulation"),
         "flux": args.flux,
+        "sweep_staging": "cp.async" if args.sweep_staging else "tensor boxes (TMA)",
         "eta": args.eta,
         "l2_flush": "inputs larger than L2 (state and scratch ~GBs)",
         "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
@@ -408,6 +411,8 @@ def run_ours(args):
         s.set_tune_cache(args.tune_cache)
     if args.residual_tiles:
         s.set_residual_tiles(*(int(x) for x in args.residual_tiles.split(",")))
+    if args.sweep_staging:
+        s.set_sweep_staging(args.sweep_staging)
     if args.tiles:
         ti, tj, kc = (int(x) for x in args.tiles.split(","))
         s.set_sweep_tiles(PRECISION[args.precision], ti, tj, kc)

@@ -74,6 +74,7 @@ EXPORTS = [
     "cns_atsch_num_launch", "cns_last_norms", "cns_atsch_num_step_host",
     "cns_sch_roe_euler_noalloc", "cns_sweep_tiles", "cns_set_sweep_tiles",
     "cns_set_residual_tiles", "cns_residual_tiles", "cns_set_tune_cache",
+    "cns_set_sweep_staging", "cns_sweep_staging",
     "cns_rfve", "cns_rfvc", "cns_dissip_jameson", "cns_sch_jameson",
     "cns_chrono_global", "cns_adjoint_prepare", "cns_adjoint_rt", "cns_adjoint_lt",
     "cns_set_turbulence", "cns_met_fludc", "cns_met_fludcsa", "cns_met_roe2o", "cns_met_roe2oh",
@@ -176,6 +177,8 @@ def load(build_if_missing: bool = True):
     L.cns_set_residual_tiles.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     L.cns_set_tune_cache.argtypes = [vp, C.c_char_p]
     L.cns_residual_tiles.argtypes = [vp, P(c_i32)]
+    L.cns_set_sweep_staging.argtypes = [vp, C.c_int]
+    L.cns_sweep_staging.argtypes = [vp, P(c_i32)]
     L.cns_atsch_num_step_host.argtypes = [vp, vp, C.c_int, P(c_f64)]
     L.cns_sch_roe_euler_noalloc.argtypes = [c_i32, c_i32, c_i32, c_i64, c_f64, c_f64, c_i32,
                                             c_f64, vp, vp, vp, vp, vp]

@@ -58,6 +58,7 @@ struct cns_ctx {
   double* tau_pack = nullptr;  // nine separate stress arrays packed as (ld, 9)
   double* u_forced = nullptr;  // implimf right-hand side u + ff (ityprk != 0) [5][ld]
   int* sched32 = nullptr;      // tile counter pair of the persistent FP32 sweep
+  int staging32 = 0;           // FP32 sweep staging: 0 tensor boxes (TMA), 1 cp.async
   std::string tune_cache;      // sweep-tiling cache file ("" = none)
   int tune_src64 = 0, tune_src32 = 0;  // tiling source: 0 default or set, 1 timed, 2 cache
   int nsm = 0;                 // streaming multiprocessors of the device
@@ -201,7 +202,8 @@ cudaError_t build_tiles(cns_ctx* c, TileBuf& t, int ti, int tj, int kc) {
 // the FP32 sweep tiles run as a persistent launch: one CTA per resident slot
 // of the GPU (every SM times the kernel's CTAs per SM), taking tiles in turn
 void persistent_sweep32(cns_ctx* c) {
-  const int per_sm = sweep_f32_blocks_per_sm(c->tiles32.ti, c->tiles32.tj, !c->sc.ns);
+  const int per_sm =
+      sweep_f32_blocks_per_sm(c->tiles32.ti, c->tiles32.tj, !c->sc.ns, c->staging32 == 0);
   c->tiles32.sched = (c->sched32 && per_sm > 0 && c->nsm > 0) ? c->sched32 : nullptr;
   c->tiles32.grid = per_sm * c->nsm;
   c->tiles32.faces = c->w.snc32;
@@ -273,6 +275,7 @@ int check_status(cns_ctx* c) {
     *c->h_status = 0;
     CK(cudaMemsetAsync(c->w.status, 0, sizeof(int), c->st));
     if (bits & 1) return fail(c, CNS_ETEMP, "non-positive temperature (zvismo)");
+    if (bits & 4) return fail(c, CNS_ECUDA, "FP32 sweep: a staged box did not arrive");
     return fail(c, CNS_EDT, "global time step below dt1min (chrono)");
   }
   return CNS_OK;
@@ -746,6 +749,19 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
   return e;
 }
 
+// the FP32 sweep's arguments (box staging unless cp.async staging is selected)
+Sweep32 sweep32_args(cns_ctx* c) {
+  Sweep32 a{};
+  a.u = c->w.u32;
+  a.st = c->w.st32;
+  a.coefdiag = c->w.coefdiag32;
+  a.maps = c->staging32 == 0 ? c->w.sweep_maps : nullptr;
+  a.map_st = nullptr;
+  a.nblk = (int)c->lay.blks.size();
+  a.status = c->w.status;
+  return a;
+}
+
 // the single-precision scratch of the mixed form, allocated on first use
 cudaError_t ensure_mixed(cns_ctx* c) {
   Work& w = c->w;
@@ -761,8 +777,16 @@ cudaError_t ensure_mixed(cns_ctx* c) {
   if (e == cudaSuccess) e = dev_alloc(c, &w.u32, (size_t)(5 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &w.coefe32, (size_t)(3 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &w.coefdiag32, (size_t)ld);
-  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
-    e = dev_alloc(c, &w.d32pp[q], (size_t)(5 * ld));
+  // the sweep's padded arrays (zeroed: their padding and ghost cells are
+  // never written, and the sweep masks them)
+  const long long ldp = c->lay.ldp;
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) e = dev_alloc(c, &w.d32pp[q], (size_t)(5 * ldp));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.st32, (size_t)(6 * ldp));
+  if (e == cudaSuccess) {
+    std::vector<unsigned char> maps;
+    e = encode_sweep32_maps(c->lay.blks, w.st32, w.d32pp, maps);
+    if (e == cudaSuccess) e = upload(c, reinterpret_cast<unsigned char**>(&w.sweep_maps),
+                                     maps.data(), maps.size());
   }
   if (e == cudaSuccess) e = dev_alloc(c, &w.corr, (size_t)(5 * ld));
   if (e == cudaSuccess) e = dev_alloc(c, &w.ur32, (size_t)(5 * ld));
@@ -807,8 +831,9 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
                      c->d_idd_ents, c->d_idd_masks, c->st);
   if (e == cudaSuccess && (c->sa_on || c->ke_on)) e = enqueue_met_num(c);
   if (e == cudaSuccess)
-    e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression, w.v32, w.prim32,
-                           w.ps32, c->st);
+    e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression,
+                           mode == kMixed ? nullptr : w.v32, w.prim32, w.ps32, c->d_blks,
+                           (int)c->lay.blks.size(), w.st32, c->st);
   if (e == cudaSuccess && c->sc.ns) {
     e = launch_grad(c->d_blks, all, c->ph, s.v, w.prim, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
                     s.ztemp, c->st);
@@ -873,13 +898,11 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
                               w.snc32, c->st);
   int cur = 0;
   if (e == cudaSuccess)
-    e = launch_sweeps_t<float>(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
-                               c->sc.lmax, ld, w.u32,
-                               w.v32, w.prim32, w.ps32, w.sn32, w.coefe32, w.coefdiag32,
-                               w.d32pp, &cur, c->st);
+    e = launch_sweeps32(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
+                        c->sc.lmax, ld, c->lay.ldp, sweep32_args(c), w.sn32, w.coefe32,
+                        w.d32pp, &cur, c->st);
   if (e == cudaSuccess)
-    e = launch_update_t<float>(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, nullptr,
-                               w.normpart, c->st);
+    e = launch_update32(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, w.normpart, c->st);
   if (e == cudaSuccess)
     e = launch_norm_finalize(c->d_blks, c->d_cells_tile0, 0, (int)c->lay.blks.size(),
                              w.normpart, w.blocksum, w.norms, c->st);
@@ -904,6 +927,23 @@ cudaError_t time_sweep(cns_ctx* c, Tiles tl, const T* u, const T* v, const T* pr
   for (int r = 0; r < 3 && e == cudaSuccess; ++r)
     e = launch_jacobi_25d_t<T>(c->d_blks, tl, c->ph, q, !c->sc.ns, ld, u, v, prim, ps, sn,
                                coefe, coefdiag, din, dout, c->st);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, c->st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+  return e;
+}
+
+// the FP32 sweep timed the same way (iterate 0 -> iterate 1)
+cudaError_t time_sweep32(cns_ctx* c, Tiles tl, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  const int q = c->sc.ns ? 0 : c->sc.qfix_dfez;
+  const long long ld = c->lay.ld;
+  const Sweep32 a = sweep32_args(c);
+  float* const* d = c->w.d32pp;
+  cudaError_t e = launch_sweep32_25d(c->d_blks, tl, c->ph, q, !c->sc.ns, ld, a, 0, d[0], d[1],
+                                     c->st);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, c->st);
+  for (int r = 0; r < 3 && e == cudaSuccess; ++r)
+    e = launch_sweep32_25d(c->d_blks, tl, c->ph, q, !c->sc.ns, ld, a, 0, d[0], d[1], c->st);
   if (e == cudaSuccess) e = cudaEventRecord(e1, c->st);
   if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
@@ -992,15 +1032,15 @@ cudaError_t tune_sweeps(cns_ctx* c, bool fp32) {
       e = build_tiles(c, cand, kSweepShape[sh][0], kSweepShape[sh][1], kc);
       if (e != cudaSuccess) break;
       if (fp32) {  // timed as it runs: the persistent launch
-        const int per_sm = sweep_f32_blocks_per_sm(cand.ti, cand.tj, !c->sc.ns);
+        const int per_sm =
+            sweep_f32_blocks_per_sm(cand.ti, cand.tj, !c->sc.ns, c->staging32 == 0);
         cand.sched = per_sm > 0 && c->nsm > 0 ? c->sched32 : nullptr;
         cand.grid = per_sm * c->nsm;
         cand.faces = w.snc32;
       }
       float ms = 0.f;
       if (fp32)
-        e = time_sweep<float>(c, cand.view(-1), w.u32, w.v32, w.prim32, w.ps32, w.sn32,
-                              w.coefe32, w.coefdiag32, w.d32pp[0], w.d32pp[1], e0, e1, &ms);
+        e = time_sweep32(c, cand.view(-1), e0, e1, &ms);
       else
         e = time_sweep<double>(c, cand.view(-1), s.u, s.v, w.prim, s.pression, s.sn, w.coefe,
                                w.coefdiag, w.dpp[0], w.dpp[1], e0, e1, &ms);
@@ -1096,8 +1136,9 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
   cns_ctx* c = new cns_ctx();
   *out = nullptr;
   CK(cudaGetDevice(&c->device));
-  // layout (crdms.f90:125-158)
-  long long off = 0, nreal = 0;
+  // layout (crdms.f90:125-158), and the padded layout of the FP32 sweep
+  // arrays (a multiple of four cells per row, so of 16 bytes per plane too)
+  long long off = 0, nreal = 0, poff = 0;
   for (int l = 0; l < layout->nblk; ++l) {
     Blk B{};
     B.ni = layout->dims[3 * l];
@@ -1114,11 +1155,17 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     B.nnn = B.nijd * B.nkd;
     B.npc = off;
     off += B.nnn;
+    B.pid = (B.nid + 3) / 4 * 4;
+    B.pnijd = (long long)B.pid * B.njd;
+    B.ppc = poff;
+    poff += B.pnijd * B.nkd;
     nreal += (long long)(B.ni - 1) * (B.nj - 1) * (B.nk - 1);
     c->lay.blks.push_back(B);
   }
   c->lay.ncells = off;
   c->lay.nreal = nreal;
+  c->lay.ldp = poff;
+  for (Blk& B : c->lay.blks) B.pld = poff;
   c->lay.ld = layout->ld > 0 ? layout->ld : off;
   if (c->lay.ld < off) {
     delete c;
@@ -2370,6 +2417,21 @@ int cns_set_sweep_tiles(cns_ctx* c, int precision, int ti, int tj, int kc) {
   (precision == 0 ? c->tuned64 : c->tuned32) = true;
   (precision == 0 ? c->tune_src64 : c->tune_src32) = 0;
   drop_graphs(c);
+  return CNS_OK;
+}
+
+int cns_set_sweep_staging(cns_ctx* c, int mode) {
+  if (!c || mode < 0 || mode > 1) return CNS_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  c->staging32 = mode;
+  persistent_sweep32(c);
+  drop_graphs(c);
+  return CNS_OK;
+}
+
+int cns_sweep_staging(cns_ctx* c, int32_t* mode) {
+  if (!c || !mode) return CNS_EINVAL;
+  *mode = c->staging32;
   return CNS_OK;
 }
 

@@ -32,7 +32,18 @@ struct Blk {
   long long npc;            // flat offset of the block
   long long nijd, nnn;
   double eta, ki2, ki4;     // the block's eta(lm), ki2(lm), ki4(lm) (schemanum)
+  // the padded layout of the mixed form's FP32 sweep arrays (this build's
+  // own, never the caller's): rows of pid = nid rounded up to a multiple of
+  // four cells, so that every row and plane starts on 16 bytes (the tensor
+  // copies' rule); cell (i, j, k) at ppc + i + j pid + k pnijd
+  int pid;
+  long long pnijd, ppc;
+  long long pld;  // the padded arrays' component stride (the same in every block)
 };
+
+__host__ __device__ __forceinline__ long long pad_index(const Blk& B, int i, int j, int k) {
+  return B.ppc + (long long)i + (long long)j * B.pid + (long long)k * B.pnijd;
+}
 
 // index space over all blocks: element e of block b has extents ext[3b..3b+2]
 // and maps to (i,j,k) = (1,1,1) + unflatten(e)

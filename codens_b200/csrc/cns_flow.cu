@@ -89,7 +89,9 @@ __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
                                              const double* __restrict__ ps,
                                              float* __restrict__ v32,
                                              float* __restrict__ prim32,
-                                             float* __restrict__ ps32) {
+                                             float* __restrict__ ps32,
+                                             const Blk* __restrict__ blks, int nblk,
+                                             float* __restrict__ st32) {
   const long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= n1) return;
   const double r = v[n];
@@ -98,15 +100,45 @@ __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
   prim[ld + n] = q1;
   prim[2 * ld + n] = q2;
   if (SHADOW) {
-    // single-precision copies of the state, velocities and pressure for
-    // the reduced-precision sweeps
-    v32[n] = (float)r;
+    // single-precision velocities (the FP32 implicit coefficients), and the
+    // FP32 state and pressure of the defect form's face fluxes (v32, ps32)
+    // and of the FP32 sweeps (st32: rho, rho E, p, u, v, w in the padded
+    // layout), each value rounded once from FP64
+    const float r32 = (float)r, e32 = (float)v[4 * ld + n], p32 = (float)ps[n];
+    const float u32 = (float)q0, w1 = (float)q1, w2 = (float)q2;
+    prim32[n] = u32;
+    prim32[ld + n] = w1;
+    prim32[2 * ld + n] = w2;
+    if (v32) {
+      v32[n] = r32;
 #pragma unroll
-    for (int a = 1; a < 5; ++a) v32[a * ld + n] = (float)v[a * ld + n];
-    prim32[n] = (float)q0;
-    prim32[ld + n] = (float)q1;
-    prim32[2 * ld + n] = (float)q2;
-    ps32[n] = (float)ps[n];
+      for (int a = 1; a < 4; ++a) v32[a * ld + n] = (float)v[a * ld + n];
+      v32[4 * ld + n] = e32;
+      ps32[n] = p32;
+    }
+    if (st32) {
+      // the cell's block (blocks in increasing npc) and (i, j, k) in it
+      int lo = 0, hi = nblk - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (blks[mid].npc <= n) lo = mid;
+        else hi = mid - 1;
+      }
+      const Blk& B = blks[lo];
+      const long long q = n - B.npc;
+      if (q < B.nnn) {
+        const int k = (int)(q / B.nijd);
+        const long long rem = q - (long long)k * B.nijd;
+        const int j = (int)(rem / B.nid), i = (int)(rem - (long long)j * B.nid);
+        const long long pn = pad_index(B, i, j, k);
+        st32[pn] = r32;
+        st32[B.pld + pn] = e32;
+        st32[2 * B.pld + pn] = p32;
+        st32[3 * B.pld + pn] = u32;
+        st32[4 * B.pld + pn] = w1;
+        st32[5 * B.pld + pn] = w2;
+      }
+    }
   }
 }
 
@@ -633,17 +665,17 @@ cudaError_t launch_zvismo(const Blk* blks, Space sp, Phys ph, double* mu,
 cudaError_t launch_prim(long long n0, long long n1, const double* v, long long ld,
                         double* prim, cudaStream_t st) {
   if (n1 > n0)
-    k_prim<false><<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(n0, n1, v, ld, prim, nullptr,
-                                                                nullptr, nullptr, nullptr);
+    k_prim<false><<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(
+        n0, n1, v, ld, prim, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
                                const double* ps, float* v32, float* prim32, float* ps32,
-                               cudaStream_t st) {
+                               const Blk* blks, int nblk, float* st32, cudaStream_t st) {
   if (ncells > 0)
     k_prim<true><<<(int)((ncells + 255) / 256), 256, 0, st>>>(0, ncells, v, ld, prim, ps, v32,
-                                                              prim32, ps32);
+                                                              prim32, ps32, blks, nblk, st32);
   return cudaGetLastError();
 }
 

@@ -1079,7 +1079,8 @@ __device__ __forceinline__ void face_tn(const T du[5], const T dl[5], const T fu
   }
 }
 
-template <class T, bool EU, bool FIRST>
+// PAD: d_out in the padded layout (pad_index; the FP32 first sweep)
+template <class T, bool EU, bool FIRST, bool PAD = false>
 __global__ void __launch_bounds__(kTile) k_jacobi_rc(
     const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
@@ -1137,9 +1138,12 @@ __global__ void __launch_bounds__(kTile) k_jacobi_rc(
 #pragma unroll
     for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
   }
+  static_assert(FIRST || !PAD, "the padded form writes the first sweep only");
   const T cd = coefdiag[n];
+  const long long dn = PAD ? pad_index(B, i, j, k) : n;
+  const long long dld = PAD ? B.pld : ld;
 #pragma unroll
-  for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
+  for (int a = 0; a < 5; ++a) d_out[a * dld + dn] = d2w[a] / cd;
 }
 
 // ---------------------------------------------------------------------------
@@ -1560,8 +1564,9 @@ __device__ __forceinline__ void norm_tile_reduce(const double res[5], bool valid
 }
 
 // v += d on the real cells (FP64 state update of implimf_*.f90), the residual
-// norm partials and, when requested, the final increment copied to d_out
-template <class T>
+// norm partials and, when requested, the final increment copied to d_out.
+// PAD: d in the padded layout (the FP32 iterates)
+template <class T, bool PAD = false>
 __global__ void __launch_bounds__(kTile) k_update(const Blk* __restrict__ blks,
                                                   Space sp, long long ld,
                                                   const T* __restrict__ d,
@@ -1572,11 +1577,14 @@ __global__ void __launch_bounds__(kTile) k_update(const Blk* __restrict__ blks,
   const bool valid = space_elem(sp, threadIdx.x, b, i, j, k);
   double res[5] = {0., 0., 0., 0., 0.};
   if (valid) {
-    const long long n = cell_index(blks[b], i, j, k);
+    const Blk& B = blks[b];
+    const long long n = cell_index(B, i, j, k);
+    const long long dn = PAD ? pad_index(B, i, j, k) : n;
+    const long long dld = PAD ? B.pld : ld;
     const double t = dt[n];
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
-      const double vo = v[a * ld + n], dd = (double)d[a * ld + n];
+      const double vo = v[a * ld + n], dd = (double)d[a * dld + dn];
       const double vn = vo + dd;
       v[a * ld + n] = vn;
       if (d_out) d_out[a * ld + n] = dd;

@@ -21,6 +21,7 @@ constexpr int kSweepShape[kSweepShapes][2] = {{32, 4}, {32, 8}, {16, 8}, {16, 16
 struct HostLayout {
   std::vector<Blk> blks;
   long long ld = 0, ncells = 0, nreal = 0;
+  long long ldp = 0;  // cells of the padded layout (Blk::pid), a multiple of 4
 };
 
 // an index space with its tile work list on the device
@@ -137,7 +138,9 @@ struct Work {
   float *v32 = nullptr, *prim32 = nullptr, *ps32 = nullptr, *tau32 = nullptr;
   float *sn32 = nullptr, *G32 = nullptr, *R32 = nullptr, *u32 = nullptr;
   float *coefe32 = nullptr, *coefdiag32 = nullptr;
-  float* d32pp[2] = {nullptr, nullptr};
+  float* d32pp[2] = {nullptr, nullptr};  // FP32 iterates, padded [5][ldp] each
+  float* st32 = nullptr;      // the FP32 sweep's state, padded [6][ldp]
+  void* sweep_maps = nullptr; // the box staging's tensor maps (device)
   double *corr = nullptr, *ur32 = nullptr;
   float4* snc32 = nullptr;  // [ld][3]: half lower-face areas and their coefficients
 };
@@ -220,18 +223,50 @@ cudaError_t launch_update_t(const Blk* blks, Space cells, long long ld, const T*
   template <>                                                                               \
   cudaError_t launch_accumulate_t<T>(const Blk*, Space, const T*, long long,               \
                                      const double*, double*, float*, cudaStream_t,         \
-                                     const T*);                                             \
-  template <>                                                                               \
-  cudaError_t launch_sweeps_t<T>(const Blk*, Space, Tiles, Phys, Scheme, int, int, long long, \
-                                 const T*, const T*, const T*, const T*, const T*,          \
-                                 const T*, const T*, T* const[2], int*,                     \
-                                 cudaStream_t);                                             \
-  template <>                                                                               \
-  cudaError_t launch_update_t<T>(const Blk*, Space, long long, const T*, double*,          \
-                                 const double*, double*, double*, cudaStream_t);
+                                     const T*);
 CNS_DECLARE_HOT(double)
 CNS_DECLARE_HOT(float)
 #undef CNS_DECLARE_HOT
+template <>
+cudaError_t launch_sweeps_t<double>(const Blk*, Space, Tiles, Phys, Scheme, int, int, long long,
+                                    const double*, const double*, const double*, const double*,
+                                    const double*, const double*, const double*,
+                                    double* const[2], int*, cudaStream_t);
+template <>
+cudaError_t launch_update_t<double>(const Blk*, Space, long long, const double*, double*,
+                                    const double*, double*, double*, cudaStream_t);
+
+// The FP32 sweeps of the mixed forms (cns_mixed.cu).  The iterates and the
+// sweep's per-cell state st (rho, rho E, p, u, v, w of the real cells, six
+// components) are in the padded layout (pad_index, component stride
+// Blk::pld); u and coefdiag in the flat one.  maps: the device tensor maps
+// of encode_sweep32_maps (box staging), or null (cp.async staging).
+struct Sweep32 {
+  const float* u;
+  const float* st;
+  const float* coefdiag;
+  const void* maps;    // [(shape * 3 + array) * nblk + block], array 0 st, 1 dpp[0], 2 dpp[1]
+  const void* map_st;  // set per launch: the state maps of the launch's shape
+  int nblk;
+  int* status;         // bit 4: a box wait gave up
+};
+// lmx sweeps (the first per cell, the others 2.5D over tl); the final
+// iterate in dpp[*cur_out]; ldp: the padded arrays' component stride
+cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
+                            int lmx, long long ld, long long ldp, const Sweep32& a,
+                            const float* sn, const float* coefe, float* const dpp[2],
+                            int* cur_out, cudaStream_t st);
+// one 2.5D sweep d_in (= dpp[din_sel]) -> d_out over the tiles tl
+cudaError_t launch_sweep32_25d(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                               long long ld, const Sweep32& a, int din_sel, const float* d_in,
+                               float* d_out, cudaStream_t st);
+// v += d (d padded FP32) and the norm partials
+cudaError_t launch_update32(const Blk* blks, Space cells, long long ld, const float* d,
+                            double* v, const double* dt, double* normpart, cudaStream_t st);
+// the tensor maps of the box staging for every sweep shape and block (host
+// bytes, kSweepShapes * 3 * nblk maps of 128 bytes)
+cudaError_t encode_sweep32_maps(const std::vector<Blk>& blks, const float* st,
+                                float* const dpp[2], std::vector<unsigned char>& out);
 
 // one sweep of the 2.5D kernel over the tiles tl (d_in -> d_out); every
 // sweep but the first of launch_sweeps_t runs through it
@@ -245,11 +280,6 @@ cudaError_t launch_jacobi_25d_t<double>(const Blk*, Tiles, Phys, int, int, long 
                                         const double*, const double*, const double*,
                                         const double*, const double*, const double*,
                                         const double*, const double*, double*, cudaStream_t);
-template <>
-cudaError_t launch_jacobi_25d_t<float>(const Blk*, Tiles, Phys, int, int, long long,
-                                       const float*, const float*, const float*, const float*,
-                                       const float*, const float*, const float*, const float*,
-                                       float*, cudaStream_t);
 // chrono.f90:113-151 (kdtl = 0): dt = min(dt1min, min over real cells) on
 // [0, ncells); status bit 2 when below dt1min; part: one double per cell tile
 cudaError_t launch_dt_global(const Blk* blks, Space cells, long long ncells, double dt1min,
@@ -396,7 +426,7 @@ cudaError_t launch_cutsa(const Blk* blks, Space cells, double* v, long long ld, 
 // per device, before the first launch)
 cudaError_t init_jacobi_25d();
 // resident CTAs per SM of the FP32 sweep kernel of patch ti x tj (persistent launch size)
-int sweep_f32_blocks_per_sm(int ti, int tj, int eu);
+int sweep_f32_blocks_per_sm(int ti, int tj, int eu, int box);
 cudaError_t init_jacobi_25d_float();
 
 inline cudaError_t launch_ratio(const Blk* blks, const SpaceBuf* lines, int l0,
@@ -463,11 +493,13 @@ cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
                                          float* coefe32, float* coefdiag32,
                                          cudaStream_t st);
 
-// primitive velocities over the flat range [0, ncells) together with the
-// single-precision copies of v, prim and ps the reduced-precision sweeps read
+// primitive velocities over the flat range [0, ncells) together with their
+// single-precision copy prim32, the FP32 sweep state st32 (padded layout)
+// and, when v32 is given, the single-precision state v32 and pressure ps32
+// of the defect form's face fluxes
 cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
                                const double* ps, float* v32, float* prim32, float* ps32,
-                               cudaStream_t st);
+                               const Blk* blks, int nblk, float* st32, cudaStream_t st);
 cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t st);
 // corr = u64 - u_r32 on the real cells (defect correction)
 cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const double* u64,

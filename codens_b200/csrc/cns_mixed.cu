@@ -16,6 +16,8 @@
 // accelerator, not a steady-state solver.
 //
 // Built with FMA contraction (the FP32 path is not a parity path).
+#include <cuda.h>
+
 #include "cns_kernels.cuh"
 #include "cns_hot.cuh"
 
@@ -286,110 +288,236 @@ __device__ __forceinline__ void phi_acc(const Inc& x, float w0, float w1, float 
   acc[4] = fmaf(x.f[3], w0, fmaf(x.f[6], w1, fmaf(x.f[8], w2, fmaf(ce, x.d[4], acc[4]))));
 }
 
-constexpr int kRawF32 = 11;  // staged inputs of one increment: d(5), rho, rho E, p, velocity
-
+// The sweep's staged plane: the padded arrays are read as boxes of
+// (TI + 4) x (TJ + 2) points per component (the patch, its one-cell ring and
+// two columns of overhang that keep the box rows a multiple of 16 bytes);
+// the iterate's five components and the six state values each form one box
+// stack, [component][row][column] in shared memory.
 template <int TI, int TJ>
-constexpr size_t sweep_f32_smem() {
-  return sizeof(float4) * 2 * 4 * (TI + 2) * (TJ + 2) +
-         sizeof(float) * 2 * kRawF32 * (TI + 2) * (TJ + 2);
+struct Sw32 {
+  static constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ;
+  static constexpr int NXP = TI + 4;          // box row (floats)
+  static constexpr int PL = NY * NXP;         // one component's box (floats)
+  static constexpr int RD = (5 * PL * 4 + 127) / 128 * 128;  // iterate boxes (bytes)
+  static constexpr int RS = (6 * PL * 4 + 127) / 128 * 128;  // state boxes (bytes)
+  static constexpr int TX = 11 * PL * 4;      // bytes one plane's boxes deliver
+  static constexpr size_t QUAD = sizeof(float4) * 2 * 4 * NP;
+  // 128 bytes of slack align the dynamic shared memory by hand
+  static constexpr size_t SMEM = 128 + QUAD + 2 * (size_t)(RD + RS);
+  static_assert(NXP * 4 % 16 == 0, "box rows must be a multiple of 16 bytes");
+  static_assert(QUAD % 128 == 0, "the raw boxes start 128-byte aligned");
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
 }
 
-// one tile (patch t of a block, kc planes) of the sweep
-template <bool EU, int TI, int TJ>
-__device__ __forceinline__ void sweep_f32_tile(
-    const int4 t, const Blk* __restrict__ blks, const Tiles& tl, Phys ph64, int qfix,
-    long long ld, const float* __restrict__ u, const float* __restrict__ v,
-    const float* __restrict__ prim, const float* __restrict__ ps, const float* __restrict__ sn,
-    const float* __restrict__ coefe, const float* __restrict__ coefdiag,
-    const float* __restrict__ d_in, float* __restrict__ d_out, unsigned char* smem_raw) {
-  constexpr int NX = TI + 2, NY = TJ + 2, NP = NX * NY, NT = TI * TJ, NR = kRawF32;
-  float4* sq = reinterpret_cast<float4*>(smem_raw);    // [2 planes][4 quads][NP]
-  float* sraw = reinterpret_cast<float*>(sq + 2 * 4 * NP);  // [2 planes][NR][NP]
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// about two seconds at the B200's clocks: a box that has not landed by then
+// never will, and the sweep gives up (status bit 4) instead of spinning
+constexpr long long kBoxWaitCycles = 4000000000LL;
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kBoxWaitCycles) return false;
+  return true;
+}
+
+// one 4D box (x, y, z, component) of a tensor map into shared memory,
+// completing on the transaction count of bar
+__device__ __forceinline__ void box_load(void* dst, const CUtensorMap* map,
+                                         unsigned long long* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(0),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+// the sweep's shared state of one CTA: the two quad planes, the two raw
+// planes and (box staging) one transaction barrier per raw plane
+struct Sw32Smem {
+  float4* sq;
+  unsigned char* raw;
+  unsigned long long* bar;
+};
+
+// one tile (patch t of a block, kc planes) of the sweep.  Returns false
+// (every thread alike) when a box wait gave up.
+template <bool EU, int TI, int TJ, bool BOX>
+__device__ __forceinline__ bool sweep_f32_tile(const int4 t, const Blk* __restrict__ blks,
+                                               const Tiles& tl, Phys ph64, int qfix,
+                                               long long ld, const Sweep32& a,
+                                               const float* __restrict__ d_in,
+                                               float* __restrict__ d_out,
+                                               const CUtensorMap* map_d, Sw32Smem sm,
+                                               unsigned& phase) {
+  using S = Sw32<TI, TJ>;
+  constexpr int NX = S::NX, NP = S::NP, NT = S::NT, NXP = S::NXP, PL = S::PL;
   const Blk B = blks[t.x];
+  const long long pld = B.pld;
+  const float* __restrict__ u = a.u;
+  const float* __restrict__ st = a.st;
   const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
   const int i = t.y + tx, j = t.z + ty;
   const int kbeg = t.w, kend = min(t.w + tl.kc, B.nk);
   const bool own = i <= B.ni - 1 && j <= B.nj - 1;
   const float gam1 = (float)ph64.gam1, pinfl = (float)ph64.pinfl;
+  const int x0 = t.y - 1, y0 = t.z - 1;
 
-  // the patch-and-ring points this thread stages and fills (at most two for
-  // every shape: NP <= 2 NT): whether the column is inside the block's real
-  // cells, and its flat index at k = 0
+  // the patch-and-ring points this thread fills (at most two for every
+  // shape: NP <= 2 NT): whether the column is inside the block's real cells
+  // and its offset in a component's box
   constexpr int NQ = (NP + NT - 1) / NT;
-  static_assert(NQ <= 2, "a thread stages at most two ring points");
+  static_assert(NQ <= 2, "a thread fills at most two ring points");
   bool colin[NQ];
-  long long col0[NQ];
+  int boxo[NQ];
 #pragma unroll
   for (int r = 0; r < NQ; ++r) {
     const int q = threadIdx.x + r * NT;
-    const int ii = t.y - 1 + q % NX, jj = t.z - 1 + q / NX;
+    const int qx = q % NX, qy = q / NX;
+    const int ii = x0 + qx, jj = y0 + qy;
     colin[r] = q < NP && ii >= 1 && ii <= B.ni - 1 && jj >= 1 && jj <= B.nj - 1;
-    col0[r] = colin[r] ? cell_index(B, ii, jj, 0) : 0;
+    boxo[r] = qy * NXP + qx;
   }
-  // the increment inputs of plane kk (patch and ring) into raw buffer b;
-  // cells outside the block's real cells are zero-filled
+  auto raw_d = [&](int b) { return reinterpret_cast<float*>(sm.raw + b * (S::RD + S::RS)); };
+  auto raw_s = [&](int b) {
+    return reinterpret_cast<float*>(sm.raw + b * (S::RD + S::RS) + S::RD);
+  };
+  // the increment inputs of plane kk (patch and ring) into raw plane b
   auto stage = [&](int kk, int b) {
-    float* r = sraw + b * NR * NP;
-    const bool kin = kk >= 1 && kk <= B.nk - 1;
+    if (BOX) {
+      if (threadIdx.x == 0) {
+        // the generic-proxy reads of this raw plane (before the barrier
+        // that precedes this call) are ordered before the boxes' writes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&sm.bar[b], S::TX);
+        box_load(raw_d(b), map_d + t.x, &sm.bar[b], x0, y0, kk);
+        box_load(raw_s(b), static_cast<const CUtensorMap*>(a.map_st) + t.x, &sm.bar[b], x0,
+                 y0, kk);
+      }
+    } else {
+      float* rd = raw_d(b);
+      float* rs = raw_s(b);
+      const bool kin = kk >= 1 && kk <= B.nk - 1;
 #pragma unroll
-    for (int rr = 0; rr < NQ; ++rr) {
-      const int q = threadIdx.x + rr * NT;
-      if (q >= NP) break;
-      const bool in = colin[rr] && kin;
-      const long long m = in ? col0[rr] + (long long)kk * B.nijd : 0;
+      for (int rr = 0; rr < NQ; ++rr) {
+        const int q = threadIdx.x + rr * NT;
+        if (q >= NP) break;
+        const bool in = colin[rr] && kin;
+        const long long m = in ? pad_index(B, x0 + q % NX, y0 + q / NX, kk) : B.ppc;
+        const int o = boxo[rr];
 #pragma unroll
-      for (int a = 0; a < 5; ++a) cp_async_elem(r + a * NP + q, d_in + a * ld + m, in);
-      cp_async_elem(r + 5 * NP + q, v + m, in);
-      cp_async_elem(r + 6 * NP + q, v + 4 * ld + m, in);
-      cp_async_elem(r + 7 * NP + q, ps + m, in);
+        for (int c = 0; c < 5; ++c) cp_async_elem(rd + c * PL + o, d_in + c * pld + m, in);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) cp_async_elem(r + (8 + a) * NP + q, prim + a * ld + m, in);
+        for (int c = 0; c < 6; ++c) cp_async_elem(rs + c * PL + o, st + c * pld + m, in);
+      }
+      cp_async_commit();
     }
   };
-  // increments of the staged plane in raw buffer b into quad buffer b
+  // raw plane b of plane kk has landed (box staging: every thread waits on
+  // the plane's barrier; cp.async: on its own copies).  Then a block-wide
+  // vote: false when any thread's wait gave up.
+  auto arrived = [&](int b, bool last_in_flight) -> bool {
+    bool ok = true;
+    if (BOX) {
+      ok = mbar_wait_bounded(&sm.bar[b], (phase >> b) & 1u);
+      phase ^= 1u << b;
+    } else if (last_in_flight) {
+      cp_async_wait<0>();
+    } else {
+      cp_async_wait<1>();
+    }
+    return !__syncthreads_or(!ok);
+  };
+  // increments of the staged plane in raw plane b into quad plane b; cells
+  // outside the block's real cells are zero
   auto fill = [&](int kk, int b) {
-    const float* r = sraw + b * NR * NP;
-    float4* s = sq + b * 4 * NP;
+    const float* rd = raw_d(b);
+    const float* rs = raw_s(b);
+    float4* s = sm.sq + b * 4 * NP;
     const bool kin = kk >= 1 && kk <= B.nk - 1;
 #pragma unroll
     for (int rr = 0; rr < NQ; ++rr) {
       const int q = threadIdx.x + rr * NT;
       if (q >= NP) break;
       const bool in = colin[rr] && kin;
+      const int o = boxo[rr];
       float dd[5], f[9];
 #pragma unroll
-      for (int a = 0; a < 5; ++a) dd[a] = r[a * NP + q];
+      for (int c = 0; c < 5; ++c) dd[c] = in ? rd[c * PL + o] : 0.f;
       if (in) {
-        df_diff<float, EU>(dd, r[5 * NP + q], r[6 * NP + q], r[7 * NP + q], r[8 * NP + q],
-                           r[9 * NP + q], r[10 * NP + q], gam1, pinfl, qfix, f);
+        df_diff<float, EU>(dd, rs[o], rs[PL + o], rs[2 * PL + o], rs[3 * PL + o],
+                           rs[4 * PL + o], rs[5 * PL + o], gam1, pinfl, qfix, f);
       } else {
 #pragma unroll
-        for (int a = 0; a < 9; ++a) f[a] = 0.f;
+        for (int c = 0; c < 9; ++c) f[c] = 0.f;
       }
       quad_store(s, NP, q, dd, f);
     }
   };
+  // a failed wait: the boxes still in flight are waited for (bounded) before
+  // the CTA gives up, so none lands in shared memory it no longer owns
+  auto drain = [&](unsigned pending) {
+    if (!BOX) {
+      cp_async_wait<0>();
+      return;
+    }
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+      if (pending & (1u << b)) (void)mbar_wait_bounded(&sm.bar[b], (phase >> b) & 1u);
+  };
 
-  // the own column's plane kbeg-1 (registers), and the lower k face area
+  // the own column's plane kbeg-1 (registers), read from global memory
   Inc pk;
   if (own && kbeg >= 2) {
-    cell_df<float, EU, 1>(v, prim, ps, d_in, ld, cell_index(B, i, j, kbeg - 1), gam1, pinfl,
-                          qfix, pk.d, pk.f);
+    const long long pm = pad_index(B, i, j, kbeg - 1);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) pk.d[c] = d_in[c * pld + pm];
+    df_diff<float, EU>(pk.d, st[pm], st[pld + pm], st[2 * pld + pm], st[3 * pld + pm],
+                       st[4 * pld + pm], st[5 * pld + pm], gam1, pinfl, qfix, pk.f);
   } else {
 #pragma unroll
-    for (int a = 0; a < 5; ++a) pk.d[a] = 0.f;
+    for (int c = 0; c < 5; ++c) pk.d[c] = 0.f;
 #pragma unroll
-    for (int a = 0; a < 9; ++a) pk.f[a] = 0.f;
+    for (int c = 0; c < 9; ++c) pk.f[c] = 0.f;
   }
   stage(kbeg, kbeg & 1);
-  cp_async_commit();
   stage(kbeg + 1, (kbeg + 1) & 1);
-  cp_async_commit();
-  cp_async_wait<1>();
-  __syncthreads();
+  if (!arrived(kbeg & 1, false)) {
+    drain(1u << ((kbeg + 1) & 1));
+    return false;
+  }
   fill(kbeg, kbeg & 1);
   __syncthreads();
   const int q0 = (ty + 1) * NX + tx + 1;
+  // the lower k face of the own cell, carried from plane to plane (the
+  // upper k face of plane k is the lower one of plane k+1)
+  float4 fkc = own ? tl.faces[3 * cell_index(B, i, j, kbeg) + 2]
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int k = kbeg; k < kend; ++k) {
     // this cell's own inputs, in flight across the barrier
     const long long n = cell_index(B, own ? i : 1, own ? j : 1, k);
@@ -398,34 +526,37 @@ __device__ __forceinline__ void sweep_f32_tile(
     // neighbours (its upper faces); 0.5 S is exact, so the sums below equal
     // the unpacked form's bit for bit
     float uu[5], cd = 1.f;
-    float4 fi, fj, fk, fiu, fju, fku;
-    fi = fj = fk = fiu = fju = fku = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 fi, fj, fiu, fju, fku;
+    const float4 fk = fkc;
+    fi = fj = fiu = fju = fku = make_float4(0.f, 0.f, 0.f, 0.f);
     if (own) {
 #pragma unroll
-      for (int a = 0; a < 5; ++a) uu[a] = u[a * ld + n];
+      for (int c = 0; c < 5; ++c) uu[c] = u[c * ld + n];
       fi = tl.faces[3 * n];
       fj = tl.faces[3 * n + 1];
-      fk = tl.faces[3 * n + 2];
       fiu = tl.faces[3 * (n + 1)];
       fju = tl.faces[3 * (n + B.nid) + 1];
       fku = tl.faces[3 * (n + B.nijd) + 2];
-      cd = coefdiag[n];
+      cd = a.coefdiag[n];
     }
-    cp_async_wait<0>();
-    __syncthreads();
-    // plane k+2's inputs go into the raw buffer plane k's used
+    fkc = fku;
+    // plane k+1 has landed; plane k's raw plane is free
+    if (!arrived((k + 1) & 1, true)) {
+      drain(0u);
+      return false;
+    }
+    // plane k+2's inputs go into the raw plane that plane k used
     stage(k + 2, k & 1);
-    cp_async_commit();
     fill(k + 1, (k + 1) & 1);
     __syncthreads();
-    const float4* s = sq + (k & 1) * 4 * NP;
-    const float4* su = sq + ((k + 1) & 1) * 4 * NP;
+    const float4* s = sm.sq + (k & 1) * 4 * NP;
+    const float4* su = sm.sq + ((k + 1) & 1) * 4 * NP;
     Inc c0, x;
     quad_load(s, NP, q0, c0);
     if (own) {
       float acc[5];
 #pragma unroll
-      for (int a = 0; a < 5; ++a) acc[a] = -uu[a];
+      for (int c = 0; c < 5; ++c) acc[c] = -uu[c];
       // the cell itself: Phi(c) . (sum of lower minus upper areas) / 2
       phi_acc(c0, (fi.x - fiu.x) + (fj.x - fju.x) + (fk.x - fku.x),
               (fi.y - fiu.y) + (fj.y - fju.y) + (fk.y - fku.y),
@@ -442,41 +573,62 @@ __device__ __forceinline__ void sweep_f32_tile(
       quad_load(su, NP, q0, x);
       phi_acc(x, -fku.x, -fku.y, -fku.z, fku.w, acc);
       const float rc = 1.f / cd;
+      const long long pn = pad_index(B, i, j, k);
 #pragma unroll
-      for (int a = 0; a < 5; ++a) d_out[a * ld + n] = acc[a] * rc;
+      for (int c = 0; c < 5; ++c) d_out[c * pld + pn] = acc[c] * rc;
     }
     pk = c0;
   }
-  cp_async_wait<0>();
+  // plane kend+1 (staged by the last plane) is still in flight
+  if (!arrived((kend + 1) & 1, true)) return false;
+  return true;
 }
 
 // The sweep over the tile list.  With tl.sched set it is a persistent
 // launch: tl.grid CTAs take tiles in turn from the counter sched[0] (each
 // tile's result does not depend on the CTA that runs it), and the last CTA
 // to finish resets the counter pair for the next launch on the stream.
-// Without it, one CTA per tile.
-template <bool EU, int TI, int TJ>
-__global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
-    const Blk* __restrict__ blks, Tiles tl, Phys ph64, int qfix, long long ld,
-    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ prim,
-    const float* __restrict__ ps, const float* __restrict__ sn, const float* __restrict__ coefe,
-    const float* __restrict__ coefdiag, const float* __restrict__ d_in,
-    float* __restrict__ d_out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// Without it, one CTA per tile.  A CTA whose box wait gave up sets status
+// bit 4 and takes no further tile.
+template <bool EU, int TI, int TJ, bool BOX>
+__global__ void __launch_bounds__(TI * TJ) k_sweep_f32(const Blk* __restrict__ blks, Tiles tl,
+                                                      Phys ph64, int qfix, long long ld,
+                                                      Sweep32 a, const float* __restrict__ d_in,
+                                                      float* __restrict__ d_out,
+                                                      const CUtensorMap* __restrict__ map_d) {
+  extern __shared__ unsigned char smem_dyn[];
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int s_next;
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  Sw32Smem sm{reinterpret_cast<float4*>(base), base + Sw32<TI, TJ>::QUAD, bar};
+  if (BOX) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+  }
+  unsigned phase = 0;
   if (!tl.sched) {
-    sweep_f32_tile<EU, TI, TJ>(tl.tile[tl.tile0 + blockIdx.x], blks, tl, ph64, qfix, ld, u, v,
-                               prim, ps, sn, coefe, coefdiag, d_in, d_out, smem_raw);
+    if (!sweep_f32_tile<EU, TI, TJ, BOX>(tl.tile[tl.tile0 + blockIdx.x], blks, tl, ph64, qfix,
+                                         ld, a, d_in, d_out, map_d, sm, phase) &&
+        threadIdx.x == 0)
+      atomicOr(a.status, 4);
     return;
   }
-  __shared__ int s_next;
   for (;;) {
     if (threadIdx.x == 0) s_next = atomicAdd(&tl.sched[0], 1);
     __syncthreads();
     const int tt = s_next;
     __syncthreads();  // every thread has read s_next before it is taken again
     if (tt >= tl.ntiles) break;
-    sweep_f32_tile<EU, TI, TJ>(tl.tile[tl.tile0 + tt], blks, tl, ph64, qfix, ld, u, v, prim,
-                               ps, sn, coefe, coefdiag, d_in, d_out, smem_raw);
+    if (!sweep_f32_tile<EU, TI, TJ, BOX>(tl.tile[tl.tile0 + tt], blks, tl, ph64, qfix, ld, a,
+                                         d_in, d_out, map_d, sm, phase)) {
+      if (threadIdx.x == 0) atomicOr(a.status, 4);
+      break;
+    }
     __syncthreads();  // the shared buffers are free for the next tile
   }
   if (threadIdx.x == 0) {
@@ -490,47 +642,70 @@ __global__ void __launch_bounds__(TI * TJ) k_sweep_f32(
 }
 
 template <int TI, int TJ>
-cudaError_t sweep_f32_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu, long long ld,
-                            const float* u, const float* v, const float* prim, const float* ps,
-                            const float* sn, const float* coefe, const float* coefdiag,
-                            const float* d_in, float* d_out, cudaStream_t st) {
-  constexpr size_t sm = sweep_f32_smem<TI, TJ>();
+int shape_index() {
+  for (int sh = 0; sh < kSweepShapes; ++sh)
+    if (kSweepShape[sh][0] == TI && kSweepShape[sh][1] == TJ) return sh;
+  return -1;
+}
+
+template <int TI, int TJ, bool BOX>
+cudaError_t sweep_f32_launch(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                             long long ld, const Sweep32& a, const float* d_in, float* d_out,
+                             const CUtensorMap* map_d, cudaStream_t st) {
+  constexpr size_t sm = Sw32<TI, TJ>::SMEM;
   const int grid = tl.sched ? min(tl.grid, tl.ntiles) : tl.ntiles;
   if (grid <= 0 || !tl.faces) return cudaErrorInvalidValue;
   if (eu)
-    k_sweep_f32<true, TI, TJ><<<grid, TI * TJ, sm, st>>>(
-        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+    k_sweep_f32<true, TI, TJ, BOX><<<grid, TI * TJ, sm, st>>>(blks, tl, ph, qfix, ld, a, d_in,
+                                                               d_out, map_d);
   else
-    k_sweep_f32<false, TI, TJ><<<grid, TI * TJ, sm, st>>>(
-        blks, tl, ph, qfix, ld, u, v, prim, ps, sn, coefe, coefdiag, d_in, d_out);
+    k_sweep_f32<false, TI, TJ, BOX><<<grid, TI * TJ, sm, st>>>(blks, tl, ph, qfix, ld, a, d_in,
+                                                                d_out, map_d);
   return cudaGetLastError();
 }
 
 template <int TI, int TJ>
+cudaError_t sweep_f32_shape(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu, long long ld,
+                            const Sweep32& a, int din_sel, const float* d_in, float* d_out,
+                            cudaStream_t st) {
+  if (a.maps) {
+    const CUtensorMap* m = static_cast<const CUtensorMap*>(a.maps) +
+                           (long long)(shape_index<TI, TJ>() * 3 + 1 + din_sel) * a.nblk;
+    Sweep32 b = a;
+    b.map_st = static_cast<const CUtensorMap*>(a.maps) +
+               (long long)(shape_index<TI, TJ>() * 3) * a.nblk;
+    return sweep_f32_launch<TI, TJ, true>(blks, tl, ph, qfix, eu, ld, b, d_in, d_out, m, st);
+  }
+  return sweep_f32_launch<TI, TJ, false>(blks, tl, ph, qfix, eu, ld, a, d_in, d_out, nullptr,
+                                         st);
+}
+
+template <int TI, int TJ>
 cudaError_t sweep_f32_attr() {
-  cudaError_t e = cudaFuncSetAttribute(k_sweep_f32<true, TI, TJ>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sweep_f32_smem<TI, TJ>());
+  const int sm = (int)Sw32<TI, TJ>::SMEM;
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_f32<true, TI, TJ, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep_f32<false, TI, TJ>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sweep_f32_smem<TI, TJ>());
+    e = cudaFuncSetAttribute(k_sweep_f32<false, TI, TJ, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_f32<true, TI, TJ, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_f32<false, TI, TJ, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   return e;
 }
 
 }  // namespace
 
-template <>
-cudaError_t launch_jacobi_25d_t<float>(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
-                                       long long ld, const float* u, const float* v,
-                                       const float* prim, const float* ps, const float* sn,
-                                       const float* coefe, const float* coefdiag,
-                                       const float* d_in, float* d_out, cudaStream_t st) {
+cudaError_t launch_sweep32_25d(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
+                               long long ld, const Sweep32& a, int din_sel, const float* d_in,
+                               float* d_out, cudaStream_t st) {
   if (tl.ntiles == 0) return cudaSuccess;
 #define CNS_SHAPE(A, B)                                                                   \
   if (tl.ti == A && tl.tj == B)                                                           \
-    return sweep_f32_shape<A, B>(blks, tl, ph, qfix, eu, ld, u, v, prim, ps, sn, coefe,   \
-                                 coefdiag, d_in, d_out, st);
+    return sweep_f32_shape<A, B>(blks, tl, ph, qfix, eu, ld, a, din_sel, d_in, d_out, st);
   CNS_SHAPE(32, 4)
   CNS_SHAPE(32, 8)
   CNS_SHAPE(16, 8)
@@ -540,23 +715,25 @@ cudaError_t launch_jacobi_25d_t<float>(const Blk* blks, Tiles tl, Phys ph, int q
 }
 
 // resident CTAs per SM of the FP32 sweep with patch ti x tj (0: unknown shape)
-int sweep_f32_blocks_per_sm(int ti, int tj, int eu) {
+int sweep_f32_blocks_per_sm(int ti, int tj, int eu, int box) {
   int n = 0;
-#define CNS_OCC(A, B)                                                                      \
-  if (ti == A && tj == B) {                                                                \
-    if (eu)                                                                                \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_f32<true, A, B>, A * B,   \
-                                                    sweep_f32_smem<A, B>());               \
-    else                                                                                   \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_f32<false, A, B>, A * B,  \
-                                                    sweep_f32_smem<A, B>());               \
-    return n;                                                                              \
+#define CNS_OCC1(A, B, E, X)                                                              \
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_f32<E, A, B, X>, A * B,       \
+                                                Sw32<A, B>::SMEM)
+#define CNS_OCC(A, B)                                                                     \
+  if (ti == A && tj == B) {                                                               \
+    if (eu && box) CNS_OCC1(A, B, true, true);                                            \
+    else if (eu) CNS_OCC1(A, B, true, false);                                             \
+    else if (box) CNS_OCC1(A, B, false, true);                                            \
+    else CNS_OCC1(A, B, false, false);                                                    \
+    return n;                                                                             \
   }
   CNS_OCC(32, 4)
   CNS_OCC(32, 8)
   CNS_OCC(16, 8)
   CNS_OCC(16, 16)
 #undef CNS_OCC
+#undef CNS_OCC1
   return 0;
 }
 
@@ -568,18 +745,63 @@ cudaError_t init_jacobi_25d_float() {
   return e;
 }
 
+// The tensor maps of the box staging: for every patch shape and block, the
+// state st and the two iterates as 4D tensors (column, row, plane,
+// component) of the block's padded box, boxes of (ti + 4) x (tj + 2) x 1 x
+// ncomp.  Reads outside the block's padded box fill with zeros (never used:
+// such points lie outside the real cells).
+cudaError_t encode_sweep32_maps(const std::vector<Blk>& blks, const float* st,
+                                float* const dpp[2], std::vector<unsigned char>& out) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess) return e;
+  if (!fn || q != cudaDriverEntryPointSuccess) return cudaErrorNotSupported;
+  const Encode encode = reinterpret_cast<Encode>(fn);
+  const size_t nblk = blks.size();
+  out.assign(sizeof(CUtensorMap) * kSweepShapes * 3 * nblk, 0);
+  CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(out.data());
+  for (int sh = 0; sh < kSweepShapes; ++sh)
+    for (int arr = 0; arr < 3; ++arr)
+      for (size_t b = 0; b < nblk; ++b) {
+        const Blk& B = blks[b];
+        const float* base = arr == 0 ? st : dpp[arr - 1];
+        const cuuint32_t ncomp = arr == 0 ? 6 : 5;
+        void* addr = const_cast<float*>(base + B.ppc);
+        const cuuint64_t dims[4] = {(cuuint64_t)B.pid, (cuuint64_t)B.njd, (cuuint64_t)B.nkd,
+                                    ncomp};
+        const cuuint64_t strides[3] = {(cuuint64_t)B.pid * 4, (cuuint64_t)B.pnijd * 4,
+                                       (cuuint64_t)B.pld * 4};
+        const cuuint32_t box[4] = {(cuuint32_t)kSweepShape[sh][0] + 4,
+                                   (cuuint32_t)kSweepShape[sh][1] + 2, 1, ncomp};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        if ((reinterpret_cast<uintptr_t>(addr) & 15) || (strides[0] & 15) ||
+            (strides[1] & 15) || (strides[2] & 15))
+          return cudaErrorInvalidValue;
+        const CUresult r = encode(&maps[(sh * 3 + arr) * nblk + b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                  4, addr, dims, strides, box, estr,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+      }
+  return cudaSuccess;
+}
+
 // the FP32 sweeps of the mixed forms: the first per cell, the others
 // 2.5D-blocked with the increments in difference form (no stored increments)
-template <>
-cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc,
-                                   int eu, int lmx, long long ld, const float* u,
-                                   const float* v, const float* prim, const float* ps,
-                                   const float* sn, const float* coefe, const float* coefdiag,
-                                   float* const dpp[2], int* cur_out, cudaStream_t st) {
+cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
+                            int lmx, long long ld, long long ldp, const Sweep32& a,
+                            const float* sn, const float* coefe, float* const dpp[2],
+                            int* cur_out, cudaStream_t st) {
   const int g = grid_of(cells);
   int cur = 0;
   if (lmx == 0) {
-    cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(float) * 5 * ld, st);
+    cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(float) * 5 * ldp, st);
     if (e0 != cudaSuccess) return e0;
   }
   const int q = eu ? sc.qfix_dfez : 0;
@@ -588,19 +810,19 @@ cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Tiles tl, Phys 
     const float* din = dpp[cur];
     float* dout = dpp[nxt];
     if (ls == 1) {
+      // the first sweep (zero previous iterate) reads no increment
       if (g > 0) {
         if (eu)
-          k_jacobi_rc<float, true, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
-                                                              prim, ps, sn, coefe, coefdiag,
-                                                              din, dout);
+          k_jacobi_rc<float, true, true, true><<<g, kTile, 0, st>>>(
+              blks, cells, ph, q, ld, a.u, nullptr, nullptr, nullptr, sn, coefe, a.coefdiag,
+              nullptr, dout);
         else
-          k_jacobi_rc<float, false, true><<<g, kTile, 0, st>>>(blks, cells, ph, q, ld, u, v,
-                                                               prim, ps, sn, coefe, coefdiag,
-                                                               din, dout);
+          k_jacobi_rc<float, false, true, true><<<g, kTile, 0, st>>>(
+              blks, cells, ph, q, ld, a.u, nullptr, nullptr, nullptr, sn, coefe, a.coefdiag,
+              nullptr, dout);
       }
     } else {
-      cudaError_t e1 = launch_jacobi_25d_t<float>(blks, tl, ph, q, eu, ld, u, v, prim, ps, sn,
-                                                  coefe, coefdiag, din, dout, st);
+      cudaError_t e1 = launch_sweep32_25d(blks, tl, ph, q, eu, ld, a, cur, din, dout, st);
       if (e1 != cudaSuccess) return e1;
     }
     cur = nxt;
@@ -609,13 +831,11 @@ cudaError_t launch_sweeps_t<float>(const Blk* blks, Space cells, Tiles tl, Phys 
   return cudaGetLastError();
 }
 
-template <>
-cudaError_t launch_update_t<float>(const Blk* blks, Space cells, long long ld, const float* d,
-                                   double* v, const double* dt, double* d_out,
-                                   double* normpart, cudaStream_t st) {
+cudaError_t launch_update32(const Blk* blks, Space cells, long long ld, const float* d,
+                            double* v, const double* dt, double* normpart, cudaStream_t st) {
   if (cells.ntiles > 0)
-    k_update<float><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, d, v, dt, d_out,
-                                                      normpart);
+    k_update<float, true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, d, v, dt, nullptr,
+                                                            normpart);
   return cudaGetLastError();
 }
 

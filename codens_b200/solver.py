@@ -220,6 +220,18 @@ class CodeNS:
         self._check(self.lib.cns_residual_tiles(self.ctx, cfg), "cns_residual_tiles")
         return tuple(int(x) for x in cfg)
 
+    @property
+    def sweep_staging(self) -> int:
+        """how the FP32 sweeps stage a plane: 0 tensor boxes, 1 cp.async"""
+        m = C.c_int32()
+        self._check(self.lib.cns_sweep_staging(self.ctx, C.byref(m)), "cns_sweep_staging")
+        return int(m.value)
+
+    def set_sweep_staging(self, mode: int):
+        """0: tensor-box staging (the default); 1: cp.async element copies
+        (the same bits)"""
+        self._check(self.lib.cns_set_sweep_staging(self.ctx, mode), "cns_set_sweep_staging")
+
     def set_residual_tiles(self, ti: int, tj: int = 0, kc: int = 0):
         """ti = 0: the face kernels + accumulation; else the fused kernel"""
         self._check(self.lib.cns_set_residual_tiles(self.ctx, ti, tj, kc),

@@ -572,6 +572,14 @@ int cns_sch_dual(cns_ctx *ctx, int l, double *u, const double *v, int icycle,
 int cns_sweep_tiles(cns_ctx *ctx, int precision, int32_t *cfg);
 int cns_set_sweep_tiles(cns_ctx *ctx, int precision, int ti, int tj, int kc);
 int cns_set_tune_cache(cns_ctx *ctx, const char *path);
+/* How the FP32 sweeps (precision 1 and 2) stage each plane of a patch in
+ * shared memory (no counterpart in the reference): mode 0 (the default)
+ * copies it as tensor boxes (cp.async.bulk.tensor, one per array and plane,
+ * completing on an mbarrier; a wait that gives up after about two seconds
+ * makes the next status check return CNS_ECUDA), mode 1 with per-thread
+ * cp.async element copies.  Both give the same bits. */
+int cns_set_sweep_staging(cns_ctx *ctx, int mode);
+int cns_sweep_staging(cns_ctx *ctx, int32_t *mode);
 /* Residual kernel variant (no counterpart in the reference): ti = 0 selects
  * the face kernels (one launch per direction into a face buffer, then the
  * per-cell accumulation); ti x tj = 32 x 4 or 16 x 8 selects the fused kernel

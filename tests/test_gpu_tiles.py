@@ -1,7 +1,8 @@
 """The 2.5D Jacobi sweep tiling: every patch shape and plane count gives the
 same FP64 iteration bit for bit (each cell's arithmetic does not depend on
 the tiling), the autotuner runs on the first fused iteration, and the
-reduced-precision forms are tiling-independent bit for bit too."""
+reduced-precision forms are tiling-independent bit for bit too, with the
+planes staged as tensor boxes (the default) or by cp.async element copies."""
 from __future__ import annotations
 
 import numpy as np
@@ -14,12 +15,15 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(32, 4), (32, 8), (16, 8), (16, 16)]
 
 
-def _run(name, precision, tiles, nsteps=3):
+def _run(name, precision, tiles, nsteps=3, staging=0):
     from codens_b200.solver import CodeNS
     case = SMALL[name]()
     case.scheme.precision = precision
     s = CodeNS(case)
     s.metric()
+    if staging:
+        s.set_sweep_staging(staging)
+        assert s.sweep_staging == staging
     if tiles is not None:
         s.set_sweep_tiles(0 if precision == 0 else 1, *tiles)
     s.atsch_num(nsteps)
@@ -52,6 +56,9 @@ def test_reduced_precision_iteration_independent_of_tiling(cuda, name, precision
         for kc in (1, 2, 3, 8):
             v, _ = _run(name, precision, (ti, tj, kc))
             assert_equal_bits(v, ref, f"precision {precision} tiles {ti}x{tj}x{kc}")
+        for kc in (2, 3):
+            v, _ = _run(name, precision, (ti, tj, kc), staging=1)
+            assert_equal_bits(v, ref, f"cp.async staging, tiles {ti}x{tj}x{kc}")
 
 
 def test_rejects_unknown_shape(cuda):
@@ -119,4 +126,15 @@ def test_tuning_cache(cuda, tmp_path):
     s.set_tune_cache(path)
     s.atsch_num(1)
     assert s.sweep_tiles(1)[3] == 1
+    s.close()
+
+
+def test_staging_mode_is_checked(cuda):
+    from codens_b200 import abi
+    from codens_b200.solver import CodeNS
+    s = CodeNS(SMALL["box_ns"]())
+    assert s.sweep_staging == 0
+    with pytest.raises(abi.CnsError) as e:
+        s.set_sweep_staging(2)
+    assert e.value.code == abi.CNS_EINVAL
     s.close()
