@@ -55,7 +55,7 @@ SWEEP_KERNEL = {"fp64": "k_jacobi_25d<double> (2.5D point-Jacobi sweep, recomput
 # DRAM bytes per cell of one 2.5D sweep launch, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 1.18M-cell channel;
 # traffic grows with the cells processed, so a full launch is this x cells
-SWEEP_TRAFFIC_PER_CELL = {"fp64": 326.4, "mixed": 146.6, "defect": 146.6}
+SWEEP_TRAFFIC_PER_CELL = {"fp64": 326.4, "mixed": 152.0, "defect": 152.0}
 FALLBACK_HBM_GBS = 6650.0
 
 
