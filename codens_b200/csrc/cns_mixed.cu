@@ -19,6 +19,9 @@
 #include <cuda.h>
 
 #include "cns_kernels.cuh"
+// the Roe dissipation of this translation unit's face fluxes with one
+// reciprocal per divisor (the hot kernels are internal to each unit)
+#define CNS_RECIP_DIV 1
 #include "cns_hot.cuh"
 
 namespace cns {
@@ -82,8 +85,6 @@ __global__ void __launch_bounds__(kTile) k_coef32(
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const long long n = cell_index(B, i, j, k);
-  // the coefficient lane of the sweep's face pack: float 4 (3 m + dir) + 3
-  float* const sncw = reinterpret_cast<float*>(snc);
   const float gp = (float)(ph.gam / ph.pr), gpt = (float)(ph.gam / ph.prt);
   auto rv_of = [&](long long m, bool real) -> float {
     if (EU || !real) return 0.f;
@@ -108,8 +109,13 @@ __global__ void __launch_bounds__(kTile) k_coef32(
     coefe[(long long)dir * ld + n] = cel;
     if (p == nd - 1) coefe[(long long)dir * ld + nu] = ceu;
     if (snc) {
-      sncw[4 * (3 * n + dir) + 3] = cel;
-      if (p == nd - 1) sncw[4 * (3 * nu + dir) + 3] = ceu;
+      // the sweep's face pack, whole 16-byte entries (half the face's area
+      // vector, as k_pack_faces32 writes it, and its coefficient): a store of
+      // the coefficient lane alone would make the memory system fetch the
+      // rest of each entry first
+      snc[3 * n + dir] = make_float4(0.5f * s0[n], 0.5f * s1[n], 0.5f * s2[n], cel);
+      if (p == nd - 1)
+        snc[3 * nu + dir] = make_float4(0.5f * s0[nu], 0.5f * s1[nu], 0.5f * s2[nu], ceu);
     }
     cd = cd + cel + ceu;
   }
