@@ -178,14 +178,17 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   const T one = T(1.), h = T(0.5);
   const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
   const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
-  const T cnds = sqrt(sx * sx + sy * sy + sz * sz);
+  const T s2 = sx * sx + sy * sy + sz * sz;
   const T q2l = sqT(ul) + sqT(vl) + sqT(wl);
   const T q2r = sqT(ur) + sqT(vr) + sqT(wr);
 #ifdef CNS_RECIP_DIV
   // the mixed form's residual (not a parity path): one reciprocal per
-  // distinct divisor and products with it, 7 divisions instead of 17; the
-  // same quantities to FP64 rounding
-  const T icnds = one / cnds, irl = one / rhol, irr = one / rhor, igam1 = one / gam1;
+  // distinct divisor and products with it, and a reciprocal square root
+  // where both a root and its inverse are used (|S|, the Roe density and
+  // sound speed): 4 divisions, 3 roots and 3 reciprocal roots instead of 17
+  // divisions and 6 roots; the same quantities to FP64 rounding
+  const T icnds = rsqrt(s2), cnds = s2 * icnds;
+  const T irl = one / rhol, irr = one / rhor, igam1 = one / gam1;
   const T nx = sx * icnds, ny = sy * icnds, nz = sz * icnds;
   const T al = sqrt(gam * pl * irl);
   const T ar = sqrt(gam * prr * irr);
@@ -195,6 +198,7 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   er = prr * igam1 * irr + h * q2r + pinfl * irr;
   const T gd = sqrt(rhor * irl);
 #else
+  const T cnds = sqrt(s2);
   const T nx = sx / cnds, ny = sy / cnds, nz = sz / cnds;
   const T al = sqrt(gam * pl / rhol);
   const T ar = sqrt(gam * prr / rhor);
@@ -206,21 +210,26 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
 #endif
   const T gd1 = one / (one + gd);
   const T gd2 = gd * gd1;
+#ifdef CNS_RECIP_DIV
+  const T rlr = rhol * rhor, rhomi = rsqrt(rlr), rhom = rlr * rhomi;
+#else
   const T rhom = sqrt(rhol * rhor);
   const T rhomi = one / rhom;
+#endif
   const T um = gd1 * ul + gd2 * ur;
   const T vm = gd1 * vl + gd2 * vr;
   const T wm = gd1 * wl + gd2 * wr;
   const T hm = gd1 * hl + gd2 * hr;
   const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
-  const T am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
   const T vn = um * nx + vm * ny + wm * nz;
 #ifdef CNS_RECIP_DIV
-  const T iam = one / am;
+  const T am2 = absam ? fabs(gam1 * (hm - vitm2)) : gam1 * (hm - vitm2);
+  const T iam = rsqrt(am2), am = am2 * iam;
   const T am2i = iam * iam;
   const T rhoiam = rhom * iam;
   const T rhoami = iam * rhomi;
 #else
+  const T am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
   const T am2i = one / (am * am);
   const T rhoiam = rhom / am;
   const T rhoami = am2i / rhoiam;
