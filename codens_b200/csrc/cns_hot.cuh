@@ -182,21 +182,38 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   const T q2l = sqT(ul) + sqT(vl) + sqT(wl);
   const T q2r = sqT(ur) + sqT(vr) + sqT(wr);
 #ifdef CNS_RECIP_DIV
-  // the mixed form's residual (not a parity path): one reciprocal per
-  // distinct divisor and products with it, and a reciprocal square root
-  // where both a root and its inverse are used (|S|, the Roe density and
-  // sound speed): 4 divisions, 3 roots and 3 reciprocal roots instead of 17
-  // divisions and 6 roots; the same quantities to FP64 rounding
+  // the mixed form's residual (not a parity path): reciprocal square roots
+  // where a root and its inverse are both used (|S|, the Roe density
+  // sqrt(rho_L rho_R) and sound speed), the inverse densities and the
+  // density ratio from 1/sqrt(rho_L rho_R), products with reciprocals
+  // instead of divisions: 2 divisions and 3 reciprocal roots per face
+  // instead of 17 divisions and 6 roots; the same quantities to FP64
+  // rounding
   const T icnds = rsqrt(s2), cnds = s2 * icnds;
-  const T irl = one / rhol, irr = one / rhor, igam1 = one / gam1;
   const T nx = sx * icnds, ny = sy * icnds, nz = sz * icnds;
-  const T al = sqrt(gam * pl * irl);
-  const T ar = sqrt(gam * prr * irr);
-  const T hl = al * al * igam1 + h * q2l;
-  const T hr = ar * ar * igam1 + h * q2r;
+  const T rlr = rhol * rhor, rhomi = rsqrt(rlr), rhom = rlr * rhomi;
+  const T ilr = rhomi * rhomi;                  // 1 / (rho_L rho_R)
+  const T irl = rhor * ilr, irr = rhol * ilr;   // 1 / rho_L, 1 / rho_R
+  const T igam1 = one / gam1;
+  const T al2 = gam * pl * irl, ar2 = gam * prr * irr;
+  const T hl = al2 * igam1 + h * q2l;
+  const T hr = ar2 * igam1 + h * q2r;
   el = pl * igam1 * irl + h * q2l + pinfl * irl;
   er = prr * igam1 * irr + h * q2r + pinfl * irr;
-  const T gd = sqrt(rhor * irl);
+  const T gd = rhor * rhomi;                    // sqrt(rho_R / rho_L)
+  const T gd1 = one / (one + gd);
+  const T gd2 = gd * gd1;
+  const T um = gd1 * ul + gd2 * ur;
+  const T vm = gd1 * vl + gd2 * vr;
+  const T wm = gd1 * wl + gd2 * wr;
+  const T hm = gd1 * hl + gd2 * hr;
+  const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
+  const T vn = um * nx + vm * ny + wm * nz;
+  const T am2 = absam ? fabs(gam1 * (hm - vitm2)) : gam1 * (hm - vitm2);
+  const T iam = rsqrt(am2), am = am2 * iam;
+  const T am2i = iam * iam;
+  const T rhoiam = rhom * iam;
+  const T rhoami = iam * rhomi;
 #else
   const T cnds = sqrt(s2);
   const T nx = sx / cnds, ny = sy / cnds, nz = sz / cnds;
@@ -207,30 +224,18 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
   er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
   const T gd = sqrt(rhor / rhol);
-#endif
   const T gd1 = one / (one + gd);
   const T gd2 = gd * gd1;
-#ifdef CNS_RECIP_DIV
-  const T rlr = rhol * rhor, rhomi = rsqrt(rlr), rhom = rlr * rhomi;
-#else
   const T rhom = sqrt(rhol * rhor);
   const T rhomi = one / rhom;
-#endif
   const T um = gd1 * ul + gd2 * ur;
   const T vm = gd1 * vl + gd2 * vr;
   const T wm = gd1 * wl + gd2 * wr;
   const T hm = gd1 * hl + gd2 * hr;
   const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
-  const T vn = um * nx + vm * ny + wm * nz;
-#ifdef CNS_RECIP_DIV
-  const T am2 = absam ? fabs(gam1 * (hm - vitm2)) : gam1 * (hm - vitm2);
-  const T iam = rsqrt(am2), am = am2 * iam;
-  const T am2i = iam * iam;
-  const T rhoiam = rhom * iam;
-  const T rhoami = iam * rhomi;
-#else
   const T am = absam ? sqrt(fabs(gam1 * (hm - vitm2))) : sqrt(gam1 * (hm - vitm2));
   const T am2i = one / (am * am);
+  const T vn = um * nx + vm * ny + wm * nz;
   const T rhoiam = rhom / am;
   const T rhoami = am2i / rhoiam;
 #endif
