@@ -711,11 +711,12 @@ cudaError_t enqueue_step(cns_ctx* c, bool first, bool dt_on) {
   const cns_state_t& s = c->state;
   const long long ld = c->lay.ld;
   const Space all = c->cells.view(-1);
-  cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
-                               s.ztemp, s.cson, s.mu, c->w.status, c->st);
-  if (e == cudaSuccess && dt_on)
-    e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
-                       s.vol, s.cson, c->st);
+  // zpres (+ zvismo), and chronos when the time step is recomputed, in one pass
+  cudaError_t e =
+      dt_on ? launch_zpres_chronos(c->d_blks, all, c->ph, c->sc, s.v, ld, s.pression, s.ztemp,
+                                   s.cson, s.mu, s.mut, s.dt, s.sn, s.vol, c->w.status, c->st)
+            : launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression, s.ztemp,
+                           s.cson, s.mu, c->w.status, c->st);
   if (e == cudaSuccess && dt_on) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
@@ -782,6 +783,8 @@ cudaError_t ensure_mixed(cns_ctx* c) {
   const long long ldp = c->lay.ldp;
   for (int q = 0; q < 2 && e == cudaSuccess; ++q) e = dev_alloc(c, &w.d32pp[q], (size_t)(5 * ldp));
   if (e == cudaSuccess) e = dev_alloc(c, &w.st32, (size_t)(6 * ldp));
+  if (e == cudaSuccess) e = dev_alloc(c, &w.cq32, (size_t)ld);
+  if (e == cudaSuccess) e = dev_alloc(c, &w.cv32, (size_t)ld);
   if (e == cudaSuccess) {
     std::vector<unsigned char> maps;
     e = encode_sweep32_maps(c->lay.blks, w.st32, w.d32pp, maps);
@@ -819,21 +822,37 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
   const long long ld = c->lay.ld;
   const Space all = c->cells.view(-1);
   const bool lim = c->sc.ns && c->sc.ilim == 1;
-  cudaError_t e = launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression,
-                               s.ztemp, s.cson, s.mu, w.status, c->st);
-  if (e == cudaSuccess && dt_on)
-    e = launch_chronos(c->d_blks, all, c->ph, c->sc, s.mu, s.mut, s.v, ld, s.dt, s.sn,
-                       s.vol, s.cson, c->st);
+  // zpres (+ zvismo), and chronos when the time step is recomputed, in one pass
+  cudaError_t e =
+      dt_on ? launch_zpres_chronos(c->d_blks, all, c->ph, c->sc, s.v, ld, s.pression, s.ztemp,
+                                   s.cson, s.mu, s.mut, s.dt, s.sn, s.vol, w.status, c->st)
+            : launch_zpres(c->d_blks, all, c->ph, c->sc.ns, s.v, ld, s.pression, s.ztemp,
+                           s.cson, s.mu, w.status, c->st);
   if (e == cudaSuccess && dt_on) e = global_dt(c);
   if (e == cudaSuccess && jameson(c)) e = jameson_dissipation(c, first);
   if (e == cudaSuccess)
     e = launch_rbord(c->bd, c->ph, s.v, ld, s.pression, s.ztemp, s.cson, c->n_idd_ent,
                      c->d_idd_ents, c->d_idd_masks, c->st);
   if (e == cudaSuccess && (c->sa_on || c->ke_on)) e = enqueue_met_num(c);
-  if (e == cudaSuccess)
-    e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression,
-                           mode == kMixed ? nullptr : w.v32, w.prim32, w.ps32, c->d_blks,
-                           (int)c->lay.blks.size(), w.st32, c->st);
+  if (e == cudaSuccess) {
+    PrimShadow sh{};
+    sh.v32 = mode == kMixed ? nullptr : w.v32;
+    sh.prim32 = w.prim32;
+    sh.ps32 = w.ps32;
+    sh.blks = c->d_blks;
+    sh.nblk = (int)c->lay.blks.size();
+    sh.st32 = w.st32;
+    sh.cq32 = w.cq32;
+    sh.cv32 = w.cv32;
+    sh.cson = s.cson;
+    sh.mu = s.mu;
+    sh.mut = s.mut;
+    sh.vol = s.vol;
+    sh.gp = (float)(c->ph.gam / c->ph.pr);
+    sh.gpt = (float)(c->ph.gam / c->ph.prt);
+    sh.eu = !c->sc.ns;
+    e = launch_prim_shadow(c->lay.ncells, s.v, ld, w.prim, s.pression, sh, c->st);
+  }
   if (e == cudaSuccess && c->sc.ns) {
     e = launch_grad(c->d_blks, all, c->ph, s.v, w.prim, ld, s.mu, s.mut, s.tau, s.sn, s.vol,
                     s.ztemp, c->st);
@@ -892,10 +911,9 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
   if (e == cudaSuccess && c->sc.kfmg == 3) e = enqueue_dual(c, w.u32);
   // single-precision coefficients and implicit sweeps, FP64 update
   if (e == cudaSuccess)
-    e = launch_coefficients32(c->d_blks, all, c->ph, !c->sc.ns, ld,
-                              c->sc.kfmg == 3 ? c->sc.dt1min : 0., s.dt, s.v, w.prim32,
-                              s.mu, s.mut, w.sn32, s.vol, s.cson, w.coefe32, w.coefdiag32,
-                              w.snc32, c->st);
+    e = launch_coefficients32(c->d_blks, all, !c->sc.ns, ld,
+                              c->sc.kfmg == 3 ? c->sc.dt1min : 0., s.dt, s.vol, w.cq32,
+                              w.cv32, w.sn32, w.coefe32, w.coefdiag32, w.snc32, c->st);
   int cur = 0;
   if (e == cudaSuccess)
     e = launch_sweeps32(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,

@@ -27,7 +27,39 @@ inline int grid_of(const Space& s) { return s.ntiles; }
 // thermodynamics
 // ---------------------------------------------------------------------------
 
-// zpres.f90:66-79 and, for the Navier-Stokes equations, zvismo.f90:77-104
+// zpres.f90:66-79 and, for the Navier-Stokes equations, zvismo.f90:77-104,
+// of cell n; returns c (and mu through *mu_n when with_mu)
+__device__ __forceinline__ double zpres_cell(Phys ph, int with_mu,
+                                             const double* __restrict__ v, long long ld,
+                                             long long n, double* ps, double* temp,
+                                             double* cson, double* mu, int* status,
+                                             double* mu_n) {
+  const double v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n],
+               v5 = v[4 * ld + n];
+  const double rhoe = v5 - 0.5 * (sq(v2) + sq(v3) + sq(v4)) / v1;
+  const double p = ph.gam1 * (rhoe - ph.pinfl);
+  const double t = ph.gam * p / v1;
+  ps[n] = p;
+  temp[n] = t;
+  const double c = sqrt(t);
+  cson[n] = c;
+  if (with_mu) {
+    // the reference aborts on T <= 0 (zvismo.f90:123-127); here the status
+    // word records it and the host turns it into an error code
+    double m;
+    if (t <= 0.) {
+      m = 0.;
+      atomicOr(status, 1);
+    } else {
+      const double usrey = 1. / ph.reynz, a = ph.suth_a;
+      m = usrey * t * sqrt(t) * (1. + a) / (t + a);
+    }
+    mu[n] = m;
+    *mu_n = m;
+  }
+  return c;
+}
+
 __global__ void __launch_bounds__(kTile) k_zpres(const Blk* __restrict__ blks,
                                                  Space sp, Phys ph, int with_mu,
                                                  const double* __restrict__ v,
@@ -36,27 +68,9 @@ __global__ void __launch_bounds__(kTile) k_zpres(const Blk* __restrict__ blks,
                                                  double* mu, int* status) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long n = cell_index(B, i, j, k);
-  const double v1 = v[n], v2 = v[ld + n], v3 = v[2 * ld + n], v4 = v[3 * ld + n],
-               v5 = v[4 * ld + n];
-  const double rhoe = v5 - 0.5 * (sq(v2) + sq(v3) + sq(v4)) / v1;
-  const double p = ph.gam1 * (rhoe - ph.pinfl);
-  const double t = ph.gam * p / v1;
-  ps[n] = p;
-  temp[n] = t;
-  cson[n] = sqrt(t);
-  if (with_mu) {
-    // the reference aborts on T <= 0 (zvismo.f90:123-127); here the status
-    // word records it and the host turns it into an error code
-    if (t <= 0.) {
-      mu[n] = 0.;
-      atomicOr(status, 1);
-    } else {
-      const double usrey = 1. / ph.reynz, a = ph.suth_a;
-      mu[n] = usrey * t * sqrt(t) * (1. + a) / (t + a);
-    }
-  }
+  const long long n = cell_index(blks[b], i, j, k);
+  double m;
+  (void)zpres_cell(ph, with_mu, v, ld, n, ps, temp, cson, mu, status, &m);
 }
 
 // zvismo.f90:77-104 alone (temperature already known)
@@ -86,12 +100,7 @@ template <bool SHADOW>
 __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
                                              const double* __restrict__ v,
                                              long long ld, double* __restrict__ prim,
-                                             const double* __restrict__ ps,
-                                             float* __restrict__ v32,
-                                             float* __restrict__ prim32,
-                                             float* __restrict__ ps32,
-                                             const Blk* __restrict__ blks, int nblk,
-                                             float* __restrict__ st32) {
+                                             const double* __restrict__ ps, PrimShadow sh) {
   const long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= n1) return;
   const double r = v[n];
@@ -100,21 +109,25 @@ __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
   prim[ld + n] = q1;
   prim[2 * ld + n] = q2;
   if (SHADOW) {
-    // single-precision velocities (the FP32 implicit coefficients), and the
-    // FP32 state and pressure of the defect form's face fluxes (v32, ps32)
-    // and of the FP32 sweeps (st32: rho, rho E, p, u, v, w in the padded
-    // layout), each value rounded once from FP64
+    // the single-precision copies (PrimShadow)
     const float r32 = (float)r, e32 = (float)v[4 * ld + n], p32 = (float)ps[n];
     const float u32 = (float)q0, w1 = (float)q1, w2 = (float)q2;
-    prim32[n] = u32;
-    prim32[ld + n] = w1;
-    prim32[2 * ld + n] = w2;
-    if (v32) {
-      v32[n] = r32;
+    const Blk* __restrict__ blks = sh.blks;
+    const int nblk = sh.nblk;
+    float* __restrict__ st32 = sh.st32;
+    sh.cq32[n] = make_float4(u32, w1, w2, (float)sh.cson[n]);
+    sh.cv32[n] = make_float2(
+        (float)sh.vol[n],
+        sh.eu ? 0.f : (sh.gp * (float)sh.mu[n] + sh.gpt * (float)sh.mut[n]) / r32);
+    if (sh.v32) {
+      sh.prim32[n] = u32;
+      sh.prim32[ld + n] = w1;
+      sh.prim32[2 * ld + n] = w2;
+      sh.v32[n] = r32;
 #pragma unroll
-      for (int a = 1; a < 4; ++a) v32[a * ld + n] = (float)v[a * ld + n];
-      v32[4 * ld + n] = e32;
-      ps32[n] = p32;
+      for (int a = 1; a < 4; ++a) sh.v32[a * ld + n] = (float)v[a * ld + n];
+      sh.v32[4 * ld + n] = e32;
+      sh.ps32[n] = p32;
     }
     if (st32) {
       // the cell's block (blocks in increasing npc) and (i, j, k) in it
@@ -143,16 +156,13 @@ __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
 }
 
 // chronos.f90:110-194 (kprec = 0)
-__global__ void __launch_bounds__(kTile) k_chronos(
-    const Blk* __restrict__ blks, Space sp, Phys ph, Scheme sc,
-    const double* __restrict__ mu, const double* __restrict__ mut,
-    const double* __restrict__ t, long long ld, double* dt,
-    const double* __restrict__ sn, const double* __restrict__ vol,
-    const double* __restrict__ cson) {
-  int b, i, j, k;
-  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
-  const Blk& B = blks[b];
-  const long long nc = cell_index(B, i, j, k);
+// the local time step of cell nc (chronos.f90:110-194, kprec = 0) from its
+// state t (rho, rho u, rho v, rho w), sound speed c and viscosities mu, mut
+__device__ __forceinline__ double chronos_cell(const Blk& B, Phys ph, Scheme sc,
+                                               const double* __restrict__ t, long long ld,
+                                               long long nc, const double* __restrict__ sn,
+                                               const double* __restrict__ vol, double c,
+                                               double mu_c, double mut_c) {
   double sf[3][2];
 #pragma unroll
   for (int dir = 0; dir < 3; ++dir) {
@@ -171,15 +181,46 @@ __global__ void __launch_bounds__(kTile) k_chronos(
   const double ro = t[nc];
   const double qq = (sq(t[ld + nc]) + sq(t[2 * ld + nc]) + sq(t[3 * ld + nc])) / sq(ro);
   const double q = sqrt(qq);
-  const double dte = dism / (q + cson[nc]);
+  const double dte = dism / (q + c);
   double d = B.eta * dte;
   if (sc.ns) {
-    const double rv1 = ph.gam * (mu[nc] / ph.pr + mut[nc] / ph.prt) / t[nc];
-    const double rv = fmax(rv1, 4. / 3. * (mu[nc] + mut[nc]) / t[nc]);
+    const double rv1 = ph.gam * (mu_c / ph.pr + mut_c / ph.prt) / t[nc];
+    const double rv = fmax(rv1, 4. / 3. * (mu_c + mut_c) / t[nc]);
     const double dtv = B.eta * 0.25 * sq(dism) / rv;
     d = fmin(d, dtv);
   }
-  dt[nc] = d;
+  return d;
+}
+
+__global__ void __launch_bounds__(kTile) k_chronos(
+    const Blk* __restrict__ blks, Space sp, Phys ph, Scheme sc,
+    const double* __restrict__ mu, const double* __restrict__ mut,
+    const double* __restrict__ t, long long ld, double* dt,
+    const double* __restrict__ sn, const double* __restrict__ vol,
+    const double* __restrict__ cson) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long nc = cell_index(B, i, j, k);
+  dt[nc] = chronos_cell(B, ph, sc, t, ld, nc, sn, vol, cson[nc], sc.ns ? mu[nc] : 0.,
+                        sc.ns ? mut[nc] : 0.);
+}
+
+// zpres (+ zvismo) and chronos of each real cell in one pass: the time step
+// takes the sound speed and viscosity just computed (the values the separate
+// kernels store and re-read)
+__global__ void __launch_bounds__(kTile) k_zpres_chronos(
+    const Blk* __restrict__ blks, Space sp, Phys ph, Scheme sc, const double* __restrict__ v,
+    long long ld, double* ps, double* temp, double* cson, double* mu,
+    const double* __restrict__ mut, double* dt, const double* __restrict__ sn,
+    const double* __restrict__ vol, int* status) {
+  int b, i, j, k;
+  if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
+  const Blk& B = blks[b];
+  const long long n = cell_index(B, i, j, k);
+  double m = 0.;
+  const double c = zpres_cell(ph, sc.ns, v, ld, n, ps, temp, cson, mu, status, &m);
+  dt[n] = chronos_cell(B, ph, sc, v, ld, n, sn, vol, c, m, sc.ns ? mut[n] : 0.);
 }
 
 // ---------------------------------------------------------------------------
@@ -665,17 +706,15 @@ cudaError_t launch_zvismo(const Blk* blks, Space sp, Phys ph, double* mu,
 cudaError_t launch_prim(long long n0, long long n1, const double* v, long long ld,
                         double* prim, cudaStream_t st) {
   if (n1 > n0)
-    k_prim<false><<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(
-        n0, n1, v, ld, prim, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr);
+    k_prim<false><<<(int)((n1 - n0 + 255) / 256), 256, 0, st>>>(n0, n1, v, ld, prim, nullptr,
+                                                                PrimShadow{});
   return cudaGetLastError();
 }
 
 cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
-                               const double* ps, float* v32, float* prim32, float* ps32,
-                               const Blk* blks, int nblk, float* st32, cudaStream_t st) {
+                               const double* ps, const PrimShadow& sh, cudaStream_t st) {
   if (ncells > 0)
-    k_prim<true><<<(int)((ncells + 255) / 256), 256, 0, st>>>(0, ncells, v, ld, prim, ps, v32,
-                                                              prim32, ps32, blks, nblk, st32);
+    k_prim<true><<<(int)((ncells + 255) / 256), 256, 0, st>>>(0, ncells, v, ld, prim, ps, sh);
   return cudaGetLastError();
 }
 
@@ -732,6 +771,17 @@ cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
   if (sp.ntiles > 0)
     k_chronos<<<grid_of(sp), kTile, 0, st>>>(blks, sp, ph, sc, mu, mut, v, ld, dt,
                                              sn, vol, cson);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zpres_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
+                                 const double* v, long long ld, double* ps, double* temp,
+                                 double* cson, double* mu, const double* mut, double* dt,
+                                 const double* sn, const double* vol, int* status,
+                                 cudaStream_t st) {
+  if (sp.ntiles > 0)
+    k_zpres_chronos<<<grid_of(sp), kTile, 0, st>>>(blks, sp, ph, sc, v, ld, ps, temp, cson, mu,
+                                                   mut, dt, sn, vol, status);
   return cudaGetLastError();
 }
 

@@ -140,6 +140,8 @@ struct Work {
   float *coefe32 = nullptr, *coefdiag32 = nullptr;
   float* d32pp[2] = {nullptr, nullptr};  // FP32 iterates, padded [5][ldp] each
   float* st32 = nullptr;      // the FP32 sweep's state, padded [6][ldp]
+  float4* cq32 = nullptr;     // the FP32 coefficients' inputs (u, v, w, c) [ld]
+  float2* cv32 = nullptr;     // and (vol, rv) [ld]
   void* sweep_maps = nullptr; // the box staging's tensor maps (device)
   double *corr = nullptr, *ur32 = nullptr;
   float4* snc32 = nullptr;  // [ld][3]: half lower-face areas and their coefficients
@@ -157,6 +159,13 @@ cudaError_t launch_zpres(const Blk* blks, Space sp, Phys ph, int with_mu,
 cudaError_t launch_zvismo(const Blk* blks, Space sp, Phys ph, double* mu,
                           const double* temp, int* status, cudaStream_t st);
 
+// launch_zpres (with mu for the Navier-Stokes equations) and launch_chronos
+// in one pass over the real cells sp, the same values
+cudaError_t launch_zpres_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
+                                 const double* v, long long ld, double* ps, double* temp,
+                                 double* cson, double* mu, const double* mut, double* dt,
+                                 const double* sn, const double* vol, int* status,
+                                 cudaStream_t st);
 cudaError_t launch_chronos(const Blk* blks, Space sp, Phys ph, Scheme sc,
                            const double* mu, const double* mut, const double* v,
                            long long ld, double* dt, const double* sn,
@@ -493,25 +502,41 @@ cudaError_t launch_implicit_coefficients(const Blk* blks, Space cells,
                                          float* coefe32, float* coefdiag32,
                                          cudaStream_t st);
 
-// primitive velocities over the flat range [0, ncells) together with their
-// single-precision copy prim32, the FP32 sweep state st32 (padded layout)
-// and, when v32 is given, the single-precision state v32 and pressure ps32
-// of the defect form's face fluxes
+// The single-precision copies the primitive-velocity kernel writes for the
+// reduced-precision forms, each value rounded once from FP64:
+//  - st32: the FP32 sweep state rho, rho E, p, u, v, w (padded layout);
+//  - cq32 = (u, v, w, c) and cv32 = (vol, rv) per cell: the inputs of the
+//    FP32 implicit coefficients, rv = (gam/pr mu + gam/prt mut) / rho the
+//    viscous factor of implimf_3d.f90:95-105 (0 for the Euler equations);
+//  - when v32 is given (defect form), v32, prim32 and ps32 for the FP32
+//    face fluxes.
+struct PrimShadow {
+  float *v32, *prim32, *ps32;
+  const Blk* blks;
+  int nblk;
+  float* st32;
+  float4* cq32;
+  float2* cv32;
+  const double *cson, *mu, *mut, *vol;
+  float gp, gpt;  // gam / pr, gam / prt
+  int eu;
+};
+// primitive velocities over the flat range [0, ncells) together with the
+// copies of sh
 cudaError_t launch_prim_shadow(long long ncells, const double* v, long long ld, double* prim,
-                               const double* ps, float* v32, float* prim32, float* ps32,
-                               const Blk* blks, int nblk, float* st32, cudaStream_t st);
+                               const double* ps, const PrimShadow& sh, cudaStream_t st);
 cudaError_t launch_to_float(const double* a, float* b, long long n, cudaStream_t st);
 // corr = u64 - u_r32 on the real cells (defect correction)
 cudaError_t launch_defect(const Blk* blks, Space cells, long long ld, const double* u64,
                           const double* ur32, double* corr, cudaStream_t st);
 // the FP32 implicit coefficients (coefe32 per face, coefdiag32 per cell) of
 // the mixed sweeps in one pass over the real cells
-cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
-                                  double dtpas,
-                                  const double* dt, const double* v, const float* prim32,
-                                  const double* mu, const double* mut, const float* sn32,
-                                  const double* vol, const double* cson, float* coefe32,
-                                  float* coefdiag32, float4* snc32, cudaStream_t st);
+// (the per-cell inputs cq32, cv32 of PrimShadow)
+cudaError_t launch_coefficients32(const Blk* blks, Space cells, int eu, long long ld,
+                                  double dtpas, const double* dt, const double* vol,
+                                  const float4* cq32, const float2* cv32, const float* sn32,
+                                  float* coefe32, float* coefdiag32, float4* snc32,
+                                  cudaStream_t st);
 // the face lanes of the FP32 sweep's pack: snc[3n + dir].xyz = S/2 of cell n's
 // lower face in dir (exact halves of sn32), .w = 0 until k_coef32 writes it
 cudaError_t launch_pack_faces32(const Blk* blks, int nblk, long long ncells, const float* sn32,

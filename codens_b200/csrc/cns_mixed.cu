@@ -48,23 +48,21 @@ __global__ void __launch_bounds__(kTile) k_defect(const Blk* __restrict__ blks, 
   for (int a = 0; a < 5; ++a) corr[a * ld + n] = u64[a * ld + n] - ur32[a * ld + n];
 }
 
-// spectral radius of the face between cells nh (upper side) and nl; rvh, rvl
-// the viscous factors (zero off the real cells, as the reference's zeroed rv)
+// spectral radius of the face between cells h (upper side) and l, from their
+// packed inputs q = (u, v, w, c) and (vol, rv); rvh, rvl the viscous factors
+// (zero off the real cells, as the reference's zeroed rv)
 template <bool EU>
-__device__ __forceinline__ float face_coef(const float* __restrict__ prim, long long ld,
-                                           const double* __restrict__ vol,
-                                           const double* __restrict__ cson, long long nh,
-                                           long long nl, float sx, float sy, float sz,
+__device__ __forceinline__ float face_coef(const float4 qh, const float4 ql, float volh,
+                                           float voll, float sx, float sy, float sz,
                                            float rvh, float rvl) {
   const float cnds = sx * sx + sy * sy + sz * sz;
-  const float cc = 0.5f * ((float)cson[nh] + (float)cson[nl]);
-  const float uu = 0.5f * (prim[nh] + prim[nl]);
-  const float vv = 0.5f * (prim[ld + nh] + prim[ld + nl]);
-  const float ww = 0.5f * (prim[2 * ld + nh] + prim[2 * ld + nl]);
+  const float cc = 0.5f * (qh.w + ql.w);
+  const float uu = 0.5f * (qh.x + ql.x);
+  const float vv = 0.5f * (qh.y + ql.y);
+  const float ww = 0.5f * (qh.z + ql.z);
   const float vn = uu * sx + vv * sy + ww * sz;
   if (EU) return 0.5f * fabsf(vn) + sqrtf(cnds) * cc;
-  return 0.5f * (fabsf(vn) + sqrtf(cnds) * cc) +
-         (rvh + rvl) * cnds / (float)(vol[nh] + vol[nl]);
+  return 0.5f * (fabsf(vn) + sqrtf(cnds) * cc) + (rvh + rvl) * cnds / (volh + voll);
 }
 
 // the implicit coefficients of the FP32 sweeps in one pass (the FP32 form of
@@ -72,25 +70,22 @@ __device__ __forceinline__ float face_coef(const float* __restrict__ prim, long 
 // the spectral radii of its six faces, stores the lower faces (and the upper
 // one at the end of each line) and sums the diagonal in the reference order.
 // Every interior face is evaluated by both its cells (cheaper than a second
-// pass over memory).
+// pass over memory); a neighbour's inputs are two vector loads of the packed
+// cq32 = (u, v, w, c) and cv32 = (vol, rv) the primitive kernel writes.
 template <bool EU>
 __global__ void __launch_bounds__(kTile) k_coef32(
-    const Blk* __restrict__ blks, Space sp, Phys ph, long long ld, double dtpas,
-    const double* __restrict__ dt, const double* __restrict__ v,
-    const float* __restrict__ prim, const double* __restrict__ mu,
-    const double* __restrict__ mut, const float* __restrict__ sn,
-    const double* __restrict__ vol, const double* __restrict__ cson,
-    float* __restrict__ coefe, float* __restrict__ coefdiag, float4* __restrict__ snc) {
+    const Blk* __restrict__ blks, Space sp, long long ld, double dtpas,
+    const double* __restrict__ dt, const double* __restrict__ vol,
+    const float4* __restrict__ cq, const float2* __restrict__ cv,
+    const float* __restrict__ sn, float* __restrict__ coefe, float* __restrict__ coefdiag,
+    float4* __restrict__ snc) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
   const long long n = cell_index(B, i, j, k);
-  const float gp = (float)(ph.gam / ph.pr), gpt = (float)(ph.gam / ph.prt);
-  auto rv_of = [&](long long m, bool real) -> float {
-    if (EU || !real) return 0.f;
-    return (gp * (float)mu[m] + gpt * (float)mut[m]) / (float)v[m];
-  };
-  const float rv0 = rv_of(n, true);
+  const float4 q0 = cq[n];
+  const float2 c0 = cv[n];
+  const float rv0 = EU ? 0.f : c0.y;
   // dtpas > 0: dual time stepping (implimf_eu.f90:82-85, implimf_3d.f90:213-224)
   float cd = (float)(EU && dtpas > 0. ? vol[n] * (1.5 / dtpas + 1. / dt[n]) : vol[n] / dt[n]);
 #pragma unroll
@@ -102,10 +97,12 @@ __global__ void __launch_bounds__(kTile) k_coef32(
     const float* s1 = sn_ptr(sn, B, dir, 1);
     const float* s2 = sn_ptr(sn, B, dir, 2);
     const long long nl = n - inc, nu = n + inc;
-    const float cel = face_coef<EU>(prim, ld, vol, cson, n, nl, s0[n], s1[n], s2[n], rv0,
-                                    rv_of(nl, p > 1));
-    const float ceu = face_coef<EU>(prim, ld, vol, cson, nu, n, s0[nu], s1[nu], s2[nu],
-                                    rv_of(nu, p < nd - 1), rv0);
+    const float4 ql = cq[nl], qu = cq[nu];
+    const float2 cl = cv[nl], cu = cv[nu];
+    const float rvl = (EU || p <= 1) ? 0.f : cl.y;
+    const float rvu = (EU || p >= nd - 1) ? 0.f : cu.y;
+    const float cel = face_coef<EU>(q0, ql, c0.x, cl.x, s0[n], s1[n], s2[n], rv0, rvl);
+    const float ceu = face_coef<EU>(qu, q0, cu.x, c0.x, s0[nu], s1[nu], s2[nu], rvu, rv0);
     coefe[(long long)dir * ld + n] = cel;
     if (p == nd - 1) coefe[(long long)dir * ld + nu] = ceu;
     if (snc) {
@@ -125,21 +122,18 @@ __global__ void __launch_bounds__(kTile) k_coef32(
 
 }  // namespace
 
-cudaError_t launch_coefficients32(const Blk* blks, Space cells, Phys ph, int eu, long long ld,
-                                  double dtpas,
-                                  const double* dt, const double* v, const float* prim32,
-                                  const double* mu, const double* mut, const float* sn32,
-                                  const double* vol, const double* cson, float* coefe32,
-                                  float* coefdiag32, float4* snc32, cudaStream_t st) {
+cudaError_t launch_coefficients32(const Blk* blks, Space cells, int eu, long long ld,
+                                  double dtpas, const double* dt, const double* vol,
+                                  const float4* cq32, const float2* cv32, const float* sn32,
+                                  float* coefe32, float* coefdiag32, float4* snc32,
+                                  cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
   if (eu)
-    k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
-                                                     mut, sn32, vol, cson, coefe32,
-                                                     coefdiag32, snc32);
+    k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, dtpas, dt, vol, cq32,
+                                                     cv32, sn32, coefe32, coefdiag32, snc32);
   else
-    k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ph, ld, dtpas, dt, v, prim32, mu,
-                                                      mut, sn32, vol, cson, coefe32,
-                                                      coefdiag32, snc32);
+    k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, dtpas, dt, vol, cq32,
+                                                      cv32, sn32, coefe32, coefdiag32, snc32);
   return cudaGetLastError();
 }
 
