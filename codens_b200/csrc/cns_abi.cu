@@ -913,12 +913,13 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
   if (e == cudaSuccess)
     e = launch_coefficients32(c->d_blks, all, !c->sc.ns, ld,
                               c->sc.kfmg == 3 ? c->sc.dt1min : 0., s.dt, s.vol, w.cq32,
-                              w.cv32, w.sn32, w.coefe32, w.coefdiag32, w.snc32, c->st);
+                              w.cv32, w.sn32, w.coefe32, w.coefdiag32, w.snc32, w.u32,
+                              c->sc.lmax >= 1 ? w.d32pp[0] : nullptr, c->st);
   int cur = 0;
   if (e == cudaSuccess)
     e = launch_sweeps32(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
                         c->sc.lmax, ld, c->lay.ldp, sweep32_args(c), w.sn32, w.coefe32,
-                        w.d32pp, &cur, c->st);
+                        w.d32pp, &cur, c->st, true);
   if (e == cudaSuccess)
     e = launch_update32(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, w.normpart, c->st);
   if (e == cudaSuccess)

@@ -260,11 +260,12 @@ struct Sweep32 {
   int* status;         // bit 4: a box wait gave up
 };
 // lmx sweeps (the first per cell, the others 2.5D over tl); the final
-// iterate in dpp[*cur_out]; ldp: the padded arrays' component stride
+// iterate in dpp[*cur_out]; ldp: the padded arrays' component stride;
+// first_done: dpp[0] already holds the first iterate (launch_coefficients32)
 cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
                             int lmx, long long ld, long long ldp, const Sweep32& a,
                             const float* sn, const float* coefe, float* const dpp[2],
-                            int* cur_out, cudaStream_t st);
+                            int* cur_out, cudaStream_t st, bool first_done = false);
 // one 2.5D sweep d_in (= dpp[din_sel]) -> d_out over the tiles tl
 cudaError_t launch_sweep32_25d(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
                                long long ld, const Sweep32& a, int din_sel, const float* d_in,
@@ -536,7 +537,7 @@ cudaError_t launch_coefficients32(const Blk* blks, Space cells, int eu, long lon
                                   double dtpas, const double* dt, const double* vol,
                                   const float4* cq32, const float2* cv32, const float* sn32,
                                   float* coefe32, float* coefdiag32, float4* snc32,
-                                  cudaStream_t st);
+                                  const float* u32, float* d1, cudaStream_t st);
 // the face lanes of the FP32 sweep's pack: snc[3n + dir].xyz = S/2 of cell n's
 // lower face in dir (exact halves of sn32), .w = 0 until k_coef32 writes it
 cudaError_t launch_pack_faces32(const Blk* blks, int nblk, long long ncells, const float* sn32,

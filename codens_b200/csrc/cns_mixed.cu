@@ -72,13 +72,17 @@ __device__ __forceinline__ float face_coef(const float4 qh, const float4 ql, flo
 // Every interior face is evaluated by both its cells (cheaper than a second
 // pass over memory); a neighbour's inputs are two vector loads of the packed
 // cq32 = (u, v, w, c) and cv32 = (vol, rv) the primitive kernel writes.
+// With d1 given, the cell's first Jacobi iterate too: with a zero previous
+// iterate every face term of the first sweep is zero, so d1 = -u / cd
+// (the value k_jacobi_rc<FIRST> computes, up to the sign of a zero), in
+// the padded layout.
 template <bool EU>
 __global__ void __launch_bounds__(kTile) k_coef32(
     const Blk* __restrict__ blks, Space sp, long long ld, double dtpas,
     const double* __restrict__ dt, const double* __restrict__ vol,
     const float4* __restrict__ cq, const float2* __restrict__ cv,
     const float* __restrict__ sn, float* __restrict__ coefe, float* __restrict__ coefdiag,
-    float4* __restrict__ snc) {
+    float4* __restrict__ snc, const float* __restrict__ u32, float* __restrict__ d1) {
   int b, i, j, k;
   if (!space_elem(sp, threadIdx.x, b, i, j, k)) return;
   const Blk& B = blks[b];
@@ -118,6 +122,11 @@ __global__ void __launch_bounds__(kTile) k_coef32(
   }
   if (!EU && dtpas > 0.) cd = cd + (float)(1.5 * vol[n] / dtpas);
   coefdiag[n] = cd;
+  if (d1) {
+    const long long pn = pad_index(B, i, j, k);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) d1[a * B.pld + pn] = -u32[a * ld + n] / cd;
+  }
 }
 
 }  // namespace
@@ -126,14 +135,16 @@ cudaError_t launch_coefficients32(const Blk* blks, Space cells, int eu, long lon
                                   double dtpas, const double* dt, const double* vol,
                                   const float4* cq32, const float2* cv32, const float* sn32,
                                   float* coefe32, float* coefdiag32, float4* snc32,
-                                  cudaStream_t st) {
+                                  const float* u32, float* d1, cudaStream_t st) {
   if (cells.ntiles == 0) return cudaSuccess;
   if (eu)
     k_coef32<true><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, dtpas, dt, vol, cq32,
-                                                     cv32, sn32, coefe32, coefdiag32, snc32);
+                                                     cv32, sn32, coefe32, coefdiag32, snc32,
+                                                     u32, d1);
   else
     k_coef32<false><<<grid_of(cells), kTile, 0, st>>>(blks, cells, ld, dtpas, dt, vol, cq32,
-                                                      cv32, sn32, coefe32, coefdiag32, snc32);
+                                                      cv32, sn32, coefe32, coefdiag32, snc32,
+                                                      u32, d1);
   return cudaGetLastError();
 }
 
@@ -797,7 +808,7 @@ cudaError_t encode_sweep32_maps(const std::vector<Blk>& blks, const float* st,
 cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
                             int lmx, long long ld, long long ldp, const Sweep32& a,
                             const float* sn, const float* coefe, float* const dpp[2],
-                            int* cur_out, cudaStream_t st) {
+                            int* cur_out, cudaStream_t st, bool first_done) {
   const int g = grid_of(cells);
   int cur = 0;
   if (lmx == 0) {
@@ -810,8 +821,9 @@ cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Sch
     const float* din = dpp[cur];
     float* dout = dpp[nxt];
     if (ls == 1) {
-      // the first sweep (zero previous iterate) reads no increment
-      if (g > 0) {
+      // the first sweep (zero previous iterate) reads no increment; the
+      // coefficient kernel may have written it already
+      if (g > 0 && !first_done) {
         if (eu)
           k_jacobi_rc<float, true, true, true><<<g, kTile, 0, st>>>(
               blks, cells, ph, q, ld, a.u, nullptr, nullptr, nullptr, sn, coefe, a.coefdiag,
