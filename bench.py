@@ -281,18 +281,21 @@ def _timed_steps(s, torch, steps):
 
 
 def _sweep_ms(s, torch, scheme, lmax, steps):
-    """one Jacobi sweep, timed live on the solver's stream as the difference
-    of the fused iteration with lmax sweeps and with none, over `steps`
-    iterations each (ms per sweep)"""
+    """one 2.5D Jacobi sweep (every sweep but the first, which is a cheaper
+    per-cell kernel or part of the coefficient kernel), timed live on the
+    solver's stream as the difference of the fused iteration with lmax
+    sweeps and with one, over `steps` iterations each (ms per sweep)"""
+    if lmax < 2:
+        return float("nan")
     t_l, _ = _timed_steps(s, torch, steps)
-    scheme.lmax = 0
+    scheme.lmax = 1
     s.set_scheme(scheme)
     s.atsch_num_launch(3)
-    t_0, _ = _timed_steps(s, torch, steps)
+    t_1, _ = _timed_steps(s, torch, steps)
     scheme.lmax = lmax
     s.set_scheme(scheme)
     s.atsch_num_launch(3)
-    return max((t_l - t_0) / steps / max(lmax, 1), 1e-9)
+    return max((t_l - t_1) / steps / (lmax - 1), 1e-9)
 
 
 def _residual_ms(s, torch, reps=5):
