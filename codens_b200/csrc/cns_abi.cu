@@ -1172,6 +1172,11 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     B.nkd = B.nk + 2;
     B.nijd = (long long)B.nid * B.njd;
     B.nnn = B.nijd * B.nkd;
+    // the kernels index a block's cells with 32-bit offsets
+    if (B.nnn >= (1LL << 31)) {
+      delete c;
+      return CNS_EINVAL;
+    }
     B.npc = off;
     off += B.nnn;
     B.pid = (B.nid + 3) / 4 * 4;

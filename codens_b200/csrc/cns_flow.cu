@@ -140,9 +140,10 @@ __global__ void __launch_bounds__(256) k_prim(long long n0, long long n1,
       const Blk& B = blks[lo];
       const long long q = n - B.npc;
       if (q < B.nnn) {
-        const int k = (int)(q / B.nijd);
-        const long long rem = q - (long long)k * B.nijd;
-        const int j = (int)(rem / B.nid), i = (int)(rem - (long long)j * B.nid);
+        // (i, j, k) by 32-bit divisions (a block holds fewer than 2^31 cells)
+        const unsigned q32 = (unsigned)q, nijd = (unsigned)B.nijd, nid = (unsigned)B.nid;
+        const unsigned k = q32 / nijd, rem = q32 - k * nijd;
+        const unsigned j = rem / nid, i = rem - j * nid;
         const long long pn = pad_index(B, i, j, k);
         st32[pn] = r32;
         st32[B.pld + pn] = e32;

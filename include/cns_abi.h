@@ -89,7 +89,8 @@ typedef struct cns_ctx cns_ctx;
 /* maillage: block dimensions (ii2, jj2, kk2 = real node counts) */
 typedef struct {
   int32_t nblk;
-  const int32_t *dims;   /* [3*nblk]: ni, nj, nk of each block */
+  const int32_t *dims;   /* [3*nblk]: ni, nj, nk of each block (each >= 2,
+                            (ni+2)(nj+2)(nk+2) < 2^31, else CNS_EINVAL) */
   int64_t ld;            /* ip11: leading dimension of the state arrays */
 } cns_layout_t;
 
