@@ -917,9 +917,8 @@ cudaError_t enqueue_step_mixed(cns_ctx* c, MixedMode mode, bool first, bool dt_o
                               c->sc.lmax >= 1 ? w.d32pp[0] : nullptr, c->st);
   int cur = 0;
   if (e == cudaSuccess)
-    e = launch_sweeps32(c->d_blks, all, c->tiles32.view(-1), c->ph, c->sc, !c->sc.ns,
-                        c->sc.lmax, ld, c->lay.ldp, sweep32_args(c), w.sn32, w.coefe32,
-                        w.d32pp, &cur, c->st, true);
+    e = launch_sweeps32(c->tiles32.view(-1), c->d_blks, c->ph, c->sc, !c->sc.ns, c->sc.lmax,
+                        ld, c->lay.ldp, sweep32_args(c), w.d32pp, &cur, c->st);
   if (e == cudaSuccess)
     e = launch_update32(c->d_blks, all, ld, w.d32pp[cur], s.v, s.dt, w.normpart, c->st);
   if (e == cudaSuccess)

@@ -1115,8 +1115,7 @@ __device__ __forceinline__ void face_tn(const T du[5], const T dl[5], const T fu
   }
 }
 
-// PAD: d_out in the padded layout (pad_index; the FP32 first sweep)
-template <class T, bool EU, bool FIRST, bool PAD = false>
+template <class T, bool EU, bool FIRST>
 __global__ void __launch_bounds__(kTile) k_jacobi_rc(
     const Blk* __restrict__ blks, Space sp, Phys ph64, int qfix, long long ld,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ prim,
@@ -1174,12 +1173,9 @@ __global__ void __launch_bounds__(kTile) k_jacobi_rc(
 #pragma unroll
     for (int a = 0; a < 5; ++a) d2w[a] = d2w[a] - tn[a];
   }
-  static_assert(FIRST || !PAD, "the padded form writes the first sweep only");
   const T cd = coefdiag[n];
-  const long long dn = PAD ? pad_index(B, i, j, k) : n;
-  const long long dld = PAD ? B.pld : ld;
 #pragma unroll
-  for (int a = 0; a < 5; ++a) d_out[a * dld + dn] = d2w[a] / cd;
+  for (int a = 0; a < 5; ++a) d_out[a * ld + n] = d2w[a] / cd;
 }
 
 // ---------------------------------------------------------------------------

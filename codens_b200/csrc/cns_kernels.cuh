@@ -259,13 +259,12 @@ struct Sweep32 {
   int nblk;
   int* status;         // bit 4: a box wait gave up
 };
-// lmx sweeps (the first per cell, the others 2.5D over tl); the final
-// iterate in dpp[*cur_out]; ldp: the padded arrays' component stride;
-// first_done: dpp[0] already holds the first iterate (launch_coefficients32)
-cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
-                            int lmx, long long ld, long long ldp, const Sweep32& a,
-                            const float* sn, const float* coefe, float* const dpp[2],
-                            int* cur_out, cudaStream_t st, bool first_done = false);
+// sweeps 2..lmx, 2.5D over tl, after launch_coefficients32 has written the
+// first iterate into dpp[0] (lmx = 0: dpp[0] is zeroed); the final iterate
+// in dpp[*cur_out]; ldp: the padded arrays' component stride
+cudaError_t launch_sweeps32(Tiles tl, const Blk* blks, Phys ph, Scheme sc, int eu, int lmx,
+                            long long ld, long long ldp, const Sweep32& a,
+                            float* const dpp[2], int* cur_out, cudaStream_t st);
 // one 2.5D sweep d_in (= dpp[din_sel]) -> d_out over the tiles tl
 cudaError_t launch_sweep32_25d(const Blk* blks, Tiles tl, Phys ph, int qfix, int eu,
                                long long ld, const Sweep32& a, int din_sel, const float* d_in,

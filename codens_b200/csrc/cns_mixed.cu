@@ -803,41 +803,23 @@ cudaError_t encode_sweep32_maps(const std::vector<Blk>& blks, const float* st,
   return cudaSuccess;
 }
 
-// the FP32 sweeps of the mixed forms: the first per cell, the others
-// 2.5D-blocked with the increments in difference form (no stored increments)
-cudaError_t launch_sweeps32(const Blk* blks, Space cells, Tiles tl, Phys ph, Scheme sc, int eu,
-                            int lmx, long long ld, long long ldp, const Sweep32& a,
-                            const float* sn, const float* coefe, float* const dpp[2],
-                            int* cur_out, cudaStream_t st, bool first_done) {
-  const int g = grid_of(cells);
+// the FP32 sweeps of the mixed forms after the first, whose iterate the
+// coefficient kernel writes into dpp[0] (launch_coefficients32): 2.5D-blocked,
+// with the increments in difference form (no stored increments)
+cudaError_t launch_sweeps32(Tiles tl, const Blk* blks, Phys ph, Scheme sc, int eu, int lmx,
+                            long long ld, long long ldp, const Sweep32& a,
+                            float* const dpp[2], int* cur_out, cudaStream_t st) {
   int cur = 0;
   if (lmx == 0) {
     cudaError_t e0 = cudaMemsetAsync(dpp[0], 0, sizeof(float) * 5 * ldp, st);
     if (e0 != cudaSuccess) return e0;
   }
   const int q = eu ? sc.qfix_dfez : 0;
-  for (int ls = 1; ls <= lmx; ++ls) {
-    const int nxt = (ls == 1) ? 0 : 1 - cur;
-    const float* din = dpp[cur];
-    float* dout = dpp[nxt];
-    if (ls == 1) {
-      // the first sweep (zero previous iterate) reads no increment; the
-      // coefficient kernel may have written it already
-      if (g > 0 && !first_done) {
-        if (eu)
-          k_jacobi_rc<float, true, true, true><<<g, kTile, 0, st>>>(
-              blks, cells, ph, q, ld, a.u, nullptr, nullptr, nullptr, sn, coefe, a.coefdiag,
-              nullptr, dout);
-        else
-          k_jacobi_rc<float, false, true, true><<<g, kTile, 0, st>>>(
-              blks, cells, ph, q, ld, a.u, nullptr, nullptr, nullptr, sn, coefe, a.coefdiag,
-              nullptr, dout);
-      }
-    } else {
-      cudaError_t e1 = launch_sweep32_25d(blks, tl, ph, q, eu, ld, a, cur, din, dout, st);
-      if (e1 != cudaSuccess) return e1;
-    }
-    cur = nxt;
+  for (int ls = 2; ls <= lmx; ++ls) {
+    cudaError_t e1 = launch_sweep32_25d(blks, tl, ph, q, eu, ld, a, cur, dpp[cur], dpp[1 - cur],
+                                        st);
+    if (e1 != cudaSuccess) return e1;
+    cur = 1 - cur;
   }
   *cur_out = cur;
   return cudaGetLastError();
