@@ -1153,7 +1153,10 @@ int cns_create(const cns_layout_t* layout, const cns_phys_t* phys,
     return CNS_EINVAL;
   cns_ctx* c = new cns_ctx();
   *out = nullptr;
-  CK(cudaGetDevice(&c->device));
+  if (cudaGetDevice(&c->device) != cudaSuccess) {
+    delete c;
+    return CNS_ECUDA;
+  }
   // layout (crdms.f90:125-158), and the padded layout of the FP32 sweep
   // arrays (a multiple of four cells per row, so of 16 bytes per plane too)
   long long off = 0, nreal = 0, poff = 0;

@@ -144,3 +144,19 @@ def test_mixed_rejects_bad_precision(cuda):
         s.set_scheme(case.scheme)
     assert ei.value.code == abi.CNS_EINVAL
     s.close()
+
+
+def test_create_rejects_a_block_of_2_31_cells(cuda):
+    """the kernels index a block's cells with 32-bit offsets: cns_create
+    refuses a block whose (ni+2)(nj+2)(nk+2) reaches 2^31, before it
+    allocates anything"""
+    import ctypes as C
+    from codens_b200 import abi
+    s = _solver(SMALL["box_ns"](), 1)
+    dims = np.array([2000, 1100, 1000], dtype=np.int32)
+    lay = abi.Layout_t(1, dims.ctypes.data_as(C.POINTER(C.c_int32)), 0)
+    ctx = C.c_void_p()
+    rc = s.lib.cns_create(C.byref(lay), C.byref(s._phys), C.byref(s._scheme),
+                          C.byref(s._bnd), C.byref(ctx))
+    assert rc == abi.CNS_EINVAL and not ctx.value
+    s.close()
