@@ -385,15 +385,30 @@ __device__ __forceinline__ void hllc_flux(const T WL[5], const T WR[5], T s1, T 
   const T one = T(1.), h = T(0.5), zero = T(0.);
   const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
   const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
-  const T cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const T ss = s1 * s1 + s2 * s2 + s3 * s3;
+  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
+#ifdef CNS_RECIP_DIV
+  // the mixed form's residual (not a parity path): the reciprocal-root and
+  // reciprocal forms of the Roe dissipation (roe_dissipation)
+  const T icnds = rsqrt(ss), cnds = ss * icnds;
+  const T nx = s1 * icnds, ny = s2 * icnds, nz = s3 * icnds;
+  const T rlr = rhol * rhor, irlr = rsqrt(rlr), ilr = irlr * irlr;
+  const T irl = rhor * ilr, irr = rhol * ilr, igam1 = one / gam1;
+  const T hl = gam * pl * irl * igam1 + h * q2l, hr = gam * prr * irr * igam1 + h * q2r;
+  const T el = pl * igam1 * irl + h * q2l + pinfl * irl;
+  const T er = prr * igam1 * irr + h * q2r + pinfl * irr;
+  const T gd = rhor * irlr;
+#else
+  const T cnds = sqrt(ss);
   const T nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
   const T al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
-  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
   const T hl = al * al / gam1 + h * q2l, hr = ar * ar / gam1 + h * q2r;
   const T el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
   const T er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
+  const T gd = sqrt(rhor / rhol);
+#endif
   const T vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
-  const T gd = sqrt(rhor / rhol), gd1 = one / (one + gd), gd2 = gd * gd1;
+  const T gd1 = one / (one + gd), gd2 = gd * gd1;
   const T um = gd1 * ul + gd2 * ur, vm = gd1 * vl + gd2 * vr, wm = gd1 * wl + gd2 * wr;
   const T hm = gd1 * hl + gd2 * hr;
   const T vitm2 = h * (sqT(um) + sqT(vm) + sqT(wm));
@@ -447,12 +462,24 @@ __device__ __forceinline__ void rusanov_dissipation(const T WL[5], const T WR[5]
   const T gam = ph.gam, gam1 = ph.gam1, pinfl = ph.pinfl, h = T(0.5);
   const T rhol = WL[0], ul = WL[1], vl = WL[2], wl = WL[3], pl = WL[4];
   const T rhor = WR[0], ur = WR[1], vr = WR[2], wr = WR[3], prr = WR[4];
-  const T cnds = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+  const T ss = s1 * s1 + s2 * s2 + s3 * s3;
+  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
+#ifdef CNS_RECIP_DIV
+  // the mixed form's residual: reciprocal forms as in roe_dissipation
+  const T icnds = rsqrt(ss), cnds = ss * icnds;
+  const T nx = s1 * icnds, ny = s2 * icnds, nz = s3 * icnds;
+  const T irlr = rsqrt(rhol * rhor), ilr = irlr * irlr;
+  const T irl = rhor * ilr, irr = rhol * ilr, igam1 = T(1.) / gam1;
+  const T al = sqrt(gam * pl * irl), ar = sqrt(gam * prr * irr);
+  el = pl * igam1 * irl + h * q2l + pinfl * irl;
+  er = prr * igam1 * irr + h * q2r + pinfl * irr;
+#else
+  const T cnds = sqrt(ss);
   const T nx = s1 / cnds, ny = s2 / cnds, nz = s3 / cnds;
   const T al = sqrt(gam * pl / rhol), ar = sqrt(gam * prr / rhor);
-  const T q2l = sqT(ul) + sqT(vl) + sqT(wl), q2r = sqT(ur) + sqT(vr) + sqT(wr);
   el = pl / (gam1 * rhol) + h * q2l + pinfl / rhol;
   er = prr / (gam1 * rhor) + h * q2r + pinfl / rhor;
+#endif
   const T vnl = ul * nx + vl * ny + wl * nz, vnr = ur * nx + vr * ny + wr * nz;
   const T al1 = fabs(vnl + al), ar1 = fabs(vnr + ar);
   const T rm = cnds * (al1 >= ar1 ? al1 : ar1);
