@@ -242,6 +242,36 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   const T lam1 = fabs(vn * cnds);
   const T lam4 = fabs(vn * cnds + am * cnds);
   const T lam5 = fabs(vn * cnds - am * cnds);
+  T dw[5];
+  dw[0] = rhor - rhol;
+  dw[1] = rhor * ur - rhol * ul;
+  dw[2] = rhor * vr - rhol * vl;
+  dw[3] = rhor * wr - rhol * wl;
+  dw[4] = rhor * er - rhol * el;
+#ifdef CNS_RECIP_DIV
+  // the mixed form: (P Lambda Q) dW associated as P (Lambda (Q dW)) -- the
+  // rows of Q dotted with dW in closed form, then each row of P with the
+  // five weighted characteristic amplitudes: ~50 multiply-adds instead of
+  // ~150 and no 5x5 Q held in registers (the same product to rounding)
+  T w[5];
+  {
+    const T S = um * dw[1] + vm * dw[2] + wm * dw[3] - dw[4];
+    const T A = (one - gam1 * vitm2 * am2i) * dw[0] + gam1 * am2i * S;
+    const T B = gam1 * rhoami * (vitm2 * dw[0] - S);
+    const T C = rhomi * (nx * dw[1] + ny * dw[2] + nz * dw[3] - vn * dw[0]);
+    w[0] = lam1 * (nx * A + rhomi * (nz * dw[2] - ny * dw[3] - (vm * nz - wm * ny) * dw[0]));
+    w[1] = lam1 * (ny * A + rhomi * (nx * dw[3] - nz * dw[1] - (wm * nx - um * nz) * dw[0]));
+    w[2] = lam1 * (nz * A + rhomi * (ny * dw[1] - nx * dw[2] - (um * ny - vm * nx) * dw[0]));
+    w[3] = lam4 * (B + C);
+    w[4] = lam5 * (B - C);
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    T p[5];
+    p_row(r, nx, ny, nz, um, vm, wm, hm, am, vn, vitm2, rhom, rhoiam, p);
+    di[r] = p[0] * w[0] + p[1] * w[1] + p[2] * w[2] + p[3] * w[3] + p[4] * w[4];
+  }
+#else
   T q[5][5];
   q[0][0] = (one - gam1 * vitm2 * am2i) * nx - (vm * nz - wm * ny) * rhomi;
   q[0][1] = gam1 * um * nx * am2i;
@@ -268,12 +298,6 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
   q[4][2] = -ny * rhomi - gam1 * vm * rhoami;
   q[4][3] = -nz * rhomi - gam1 * wm * rhoami;
   q[4][4] = gam1 * rhoami;
-  T dw[5];
-  dw[0] = rhor - rhol;
-  dw[1] = rhor * ur - rhol * ul;
-  dw[2] = rhor * vr - rhol * vl;
-  dw[3] = rhor * wr - rhol * wl;
-  dw[4] = rhor * er - rhol * el;
   const T lam[5] = {lam1, lam1, lam1, lam4, lam5};
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
@@ -292,6 +316,7 @@ __device__ __forceinline__ void roe_dissipation(const T WL[5], const T WR[5], T 
     }
     di[r] = acc;
   }
+#endif
 }
 
 // flux families of the face kernel (atsch_num.f90:628-983 by ischema)
